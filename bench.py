@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: ns/day of the nonbonded hot path on the 96,000-atom solvated PME box.
+
+One step = what one MD step of SPONGE spends in the path (SPONGE/main.cu:162-210, :376): the
+neighbor-list update by its policy (rebuild every 20 steps), LJ + PME direct, the long-range
+correction, the exclusion correction and PME reciprocal space, for 96,000 atoms (31,000 rigid
+waters + 3,000 solute atoms, 98.6 A box, rc 10 A, skin 2 A, PME 96^3). ns/day = steps/s * 2 fs *
+86400 / 1e6. The integrator and constraints are not part of the path and are not timed.
+
+  value   device time per step (CUDA events on the launching stream), inputs resident in HBM,
+          L2 flushed (256 MiB write) before every timed step
+  e2e     the same through the public C-ABI call with HOST buffers: pinned coordinates copied
+          in, fixed-point conversion, step, forces copied out, every step
+  --impl reference  the CPU baseline: the FP64 multithreaded restatement of the same path
+          (SPONGE has no CPU implementation) on the host cores, one full evaluation per step
+
+Multi-GPU: independent replicas (one system per rank, no collective in the data path).
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+DT_FS = 2.0
+FLOP_PER_PAIR = 50.0       # in-cutoff pair (SURVEY-derived breakdown)
+FLOP_PER_CANDIDATE = 10.0  # list pair beyond the cutoff
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal at max SM clock
+
+
+def ns_per_day(sec_per_step):
+    return DT_FS * 86400.0 / 1e6 / sec_per_step
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def pair_counts(system, uc):
+    """List pairs (rc+skin) and in-cutoff pairs from the FP64 oracle (algorithmic work)."""
+    import oracle
+    keys = oracle.pairs(uc, system, "cells")
+    _, _, d = oracle.direct(uc, system, keys, oracle.get_beta(system["cutoff"]))
+    return int(keys.size), int(d["n_in_cutoff"])
+
+
+def run_reference(args, rank, world):
+    """CPU baseline: FP64 multithreaded restatement of the path, one evaluation per step."""
+    if rank != 0:
+        return
+    import oracle
+    from sponge_b200 import systems
+    s = systems.config1()
+    uc = oracle.crd_to_uint(oracle.periodic_map(s["crd"], s["box"]), s["box"])
+    beta = oracle.get_beta(s["cutoff"])
+    nthreads = oracle.threads()
+    for _ in range(max(0, min(args.warmup, 1))):
+        oracle.nonbonded(uc, s, beta)
+    times = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        oracle.nonbonded(uc, s, beta)
+        times.append(time.perf_counter() - t)
+    total = time.perf_counter() - t0
+    sec = total / max(1, args.steps)
+    v = ns_per_day(sec)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ns/day",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(),
+        "cpu_baseline": {"value": v, "unit": "ns/day", "cores": nthreads, "kind": "port",
+                         "sample": "one full FP64 evaluation of the 96,000-atom path per step "
+                                   "(cell list + LJ/Ewald direct + exclusions + SPME 96^3)"},
+        "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "ns/day, 96k-atom PME water, 1 B200 (nonbonded path, fixed-point form)"
+
+
+def workload_config():
+    return {"workload": "solvated96k_pme96: 31,000 rigid waters + 3,000 solute atoms (20 LJ "
+                        "types), 98.6 A cube, rc 10 A, skin 2 A, PME 96^3, list rebuilt every "
+                        "20 steps, dt 2 fs",
+            "atoms": 96000, "l2": "flushed (256 MiB write) before every timed step",
+            "parallelism": "replicas"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="fixed", choices=["fixed", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import sponge_b200
+    from sponge_b200 import FORM_FIXED, FORM_PLAIN, NonbondedEngine, systems
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    s = systems.config1()
+    form = FORM_FIXED if args.form == "fixed" else FORM_PLAIN
+    eng = NonbondedEngine(s, form=form, refresh_interval=20)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    eng.update_list(forced=1)
+    eng.to_uint()
+
+    def one_step():
+        eng.frc.zero_()
+        eng.step(need_energy=0, need_virial=0)
+
+    for _ in range(max(3, args.warmup)):
+        one_step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_wall = time.perf_counter()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        one_step()
+        ev[k][1].record(stream)
+    barrier()
+    t_wall = time.perf_counter() - t_wall
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+
+    # e2e through the public API with host buffers
+    crd_host = torch.from_numpy(s["crd"].copy()).pin_memory()
+    frc_host = torch.empty((eng.n, 3), dtype=torch.float32).pin_memory()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev2[k][0].record(stream)
+        eng.crd.copy_(crd_host, non_blocking=True)
+        eng.to_uint()
+        one_step()
+        frc_host.copy_(eng.frc, non_blocking=True)
+        ev2[k][1].record(stream)
+    barrier()
+    clk = clocks.stop()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in ev2)
+
+    # roofline of the dominant kernel (LJ + Ewald direct pair kernel), timed in isolation
+    evp = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(20)]
+    for k in range(20):
+        flush.fill_(float(k))
+        evp[k][0].record(stream)
+        eng.forces(parts=("direct",))
+        evp[k][1].record(stream)
+    torch.cuda.synchronize()
+    pair_ms = float(np.mean([a.elapsed_time(b) for a, b in evp]))
+
+    ms = dev_ms / args.steps
+    if dist is not None:
+        t = torch.tensor([ms, e2e_ms / args.steps], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_step_ms = t.tolist()
+    else:
+        e2e_step_ms = e2e_ms / args.steps
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    uc = eng.uint_crd.cpu().numpy().view(np.uint32)
+    n_list, n_cut = pair_counts(s, uc)
+    flops = FLOP_PER_PAIR * n_cut + FLOP_PER_CANDIDATE * (n_list - n_cut)
+    achieved = flops / (pair_ms * 1e-3) / 1e12
+    rebuilds_per_step = 1.0 / 20
+    launches_force = 11
+    launches_rebuild = 6
+    line = {
+        "metric": METRIC,
+        "value": world * ns_per_day(ms * 1e-3),
+        "unit": "ns/day",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 pair math, int64 fixed-point accumulation, f64 energies" if form == FORM_FIXED
+                 else "f32 float atomics",
+        "data": "synthetic (seeded generator, sponge_b200.systems.config1)",
+        "config": dict(workload_config(), form=args.form),
+        "e2e": {"value": world * ns_per_day(e2e_step_ms * 1e-3), "unit": "ns/day",
+                "h2d_bytes_per_step": int(eng.n * 12), "d2h_bytes_per_step": int(eng.n * 12)},
+        "gpu_launches": int(round(args.steps * (launches_force + launches_rebuild * rebuilds_per_step))),
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
+                     "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": None,
+                     "kernel": "k_pair_fixed (LJ + Ewald direct; timed with its pack/finalize)",
+                     "kernel_ms": pair_ms, "pairs_in_cutoff": n_cut, "pairs_in_list": n_list,
+                     "peak_note": "nominal FP32 peak 148 SM x 128 lanes x 2 x 1.965 GHz"},
+        "clocks": clk,
+        "wall_s": t_wall,
+    }
+    if not args.no_plain and form == FORM_FIXED:
+        del eng
+        torch.cuda.synchronize()
+        pe = NonbondedEngine(s, form=FORM_PLAIN, refresh_interval=20)
+        pe.update_list(forced=1)
+        pe.to_uint()
+        for _ in range(5):
+            pe.frc.zero_()
+            pe.step()
+        torch.cuda.synchronize()
+        evq = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(min(args.steps, 100))]
+        for k in range(len(evq)):
+            flush.fill_(float(k))
+            evq[k][0].record(stream)
+            pe.frc.zero_()
+            pe.step()
+            evq[k][1].record(stream)
+        torch.cuda.synchronize()
+        pms = float(np.mean([a.elapsed_time(b) for a, b in evq]))
+        line["plain_form"] = {"value": ns_per_day(pms * 1e-3), "unit": "ns/day",
+                              "ms_per_step": pms,
+                              "speedup_fixed_over_plain": pms / ms}
+    if not args.no_cpu_baseline:
+        import oracle
+        beta = oracle.get_beta(s["cutoff"])
+        t = time.perf_counter()
+        oracle.nonbonded(uc, s, beta)
+        sec = time.perf_counter() - t
+        line["cpu_baseline"] = {"value": ns_per_day(sec), "unit": "ns/day",
+                                "cores": oracle.threads(), "kind": "port",
+                                "sample": "one full FP64 evaluation of the same 96,000-atom path "
+                                          "(%.2f s)" % sec}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

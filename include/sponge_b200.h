@@ -1,0 +1,226 @@
+/*
+ * sponge_b200 — C ABI of a B200 (sm_100a) implementation of SPONGE's nonbonded hot path:
+ * the cell-grid neighbor-list rebuild, the Lennard-Jones + PME direct-space pair
+ * force/energy/virial, and PME reciprocal space.
+ *
+ * The three handle types mirror SPONGE's three module structs; every entry point names the
+ * reference method it replaces (paths relative to the SPONGE project root, SPONGE/...).
+ * Plain pointers and sizes only: device pointers are prefixed d_, host pointers h_. Streams are
+ * passed as void* holding a cudaStream_t (NULL = legacy default stream, as the reference uses).
+ *
+ * Units and layouts follow the reference: lengths in Angstrom, energies in kcal/mol, charges
+ * pre-multiplied by 18.2223, coordinates as unsigned-int fixed point (3 x uint32 per atom,
+ * UNSIGNED_INT_VECTOR), forces as float VECTOR (3 x float per atom) accumulated with +=,
+ * per-atom energies/virials as float[N] accumulated with +=, d_virial / d_potential as single
+ * device floats accumulated with +=.
+ *
+ * Every function returns SB_OK (0) or an SB_ERR_* code; sb_last_error() gives the message.
+ */
+#ifndef SPONGE_B200_H
+#define SPONGE_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SB_API __attribute__((visibility("default")))
+#else
+#define SB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB_OK 0
+#define SB_ERR_ARG 1      /* invalid argument (null handle, bad size, mismatched atom count) */
+#define SB_ERR_CUDA 2     /* a CUDA runtime call or kernel launch failed */
+#define SB_ERR_ALLOC 3    /* device or host allocation failed */
+#define SB_ERR_OVERFLOW 4 /* a fixed-capacity buffer overflowed (see sb_nl_status) */
+#define SB_ERR_STATE 5    /* call order violated (e.g. force before the first list build) */
+
+/* Accumulation forms (the `form` argument of the create functions). */
+#define SB_FORM_FIXED 0 /* FP32 pair math, 64-bit fixed-point accumulation: bit-identical runs */
+#define SB_FORM_PLAIN 1 /* FP32 pair math, float atomics, per-atom lists, library FFT */
+
+/* Status flags reported by sb_nl_status (OR-ed). */
+#define SB_STATUS_LIST_OVERFLOW 1    /* a cluster's pair-entry capacity was exceeded */
+#define SB_STATUS_COLUMN_OVERFLOW 2  /* a sort column held more atoms than the sort capacity */
+#define SB_STATUS_ATOMGROUP_OVERFLOW 4 /* an atom exceeded max_neighbor_numbers in the export */
+
+/* Particle_Mesh_Ewald::PME_ENERGY_PART (SPONGE/PME_force/PME_force.cuh:86-93) */
+#define SB_PME_TOTAL 0
+#define SB_PME_DIRECT 1
+#define SB_PME_RECIPROCAL 2
+#define SB_PME_CORRECTION 3
+#define SB_PME_SELF 4
+
+typedef struct sb_neighbor_list sb_neighbor_list;
+typedef struct sb_lennard_jones sb_lennard_jones;
+typedef struct sb_pme sb_pme;
+
+/* Library version (integer) and the message of the last failed call on this host thread. */
+SB_API int sb_version(void);
+SB_API const char* sb_last_error(void);
+
+/* ------------------------------------------------------------------------------------------
+ * Neighbor list — replaces NEIGHBOR_LIST (SPONGE/neighbor_list/neighbor_list.cuh:44-106)
+ * ---------------------------------------------------------------------------------------- */
+
+/* NEIGHBOR_LIST::Initial (SPONGE/neighbor_list/neighbor_list.cu:688-750). skin_permit is the
+ * mdin value (the reference doubles it internally, :718); pass 0.5 for the reference default.
+ * max_neighbor_numbers sizes the ATOM_GROUP compatibility export (reference default 800). */
+SB_API int sb_nl_create(int atom_numbers, const float box_length[3], float cutoff, float skin,
+                 int refresh_interval, float skin_permit, int max_neighbor_numbers, int form,
+                 sb_neighbor_list** out);
+
+/* NEIGHBOR_LIST::Clear (neighbor_list.cu:767-819) */
+SB_API int sb_nl_destroy(sb_neighbor_list* nl);
+
+/* NEIGHBOR_LIST::Neighbor_List_Update (neighbor_list.cu:618-664). d_crd is VECTOR[N] and is
+ * wrapped into the box in place on every rebuild, as the reference does. The exclusion CSR is
+ * SPONGE's (MD_core/MD_core.cu:308-351): for atom i, d_excluded_list[start[i] .. start[i] +
+ * numbers[i]) lists the excluded partners j > i. Policy: forced_update rebuilds; else with
+ * refresh_interval > 0 and !forced_check every refresh_interval-th call rebuilds; else the
+ * rebuild happens when an atom moved more than skin_permit*skin/2 since the last rebuild. */
+SB_API int sb_nl_update(sb_neighbor_list* nl, float* d_crd, const int* d_excluded_list_start,
+                 const int* d_excluded_list, const int* d_excluded_numbers, int forced_update,
+                 int forced_check, void* stream);
+
+/* NEIGHBOR_LIST::Update_Volume (neighbor_list.cu:753-764): box change without re-gridding.
+ * The next update call rebuilds. */
+SB_API int sb_nl_update_volume(sb_neighbor_list* nl, const float box_length[3]);
+
+/* Materialises the reference's public member `ATOM_GROUP* d_nl` (neighbor_list.cuh:75): an
+ * ATOM_GROUP[N] device array ({int atom_numbers; int* atom_serial}) whose per-atom lists hold
+ * the same half pair set (j > i, exclusions removed, within cutoff+skin). The array and its
+ * serial storage are owned by the handle; *d_atom_group receives its device address. Consumers
+ * that read d_nl directly (Get_Energy, FEP_CORE, TI_CORE) use this. */
+SB_API int sb_nl_atom_group(sb_neighbor_list* nl, void** d_atom_group, void* stream);
+
+/* Number of half pairs currently in the list (synchronises the stream). */
+SB_API int sb_nl_pair_count(sb_neighbor_list* nl, int64_t* h_count, void* stream);
+
+/* Copies the half pair set as sorted keys i*N + j (i < j, original atom ids) into h_keys
+ * (capacity cap). *h_count receives the count; fails with SB_ERR_OVERFLOW if cap is short. */
+SB_API int sb_nl_export_pairs(sb_neighbor_list* nl, int64_t* h_keys, int64_t cap, int64_t* h_count,
+                       void* stream);
+
+/* OR of SB_STATUS_* flags raised since the last call (synchronises the stream, clears them). */
+SB_API int sb_nl_status(sb_neighbor_list* nl, int* h_flags, void* stream);
+
+/* The list's own fixed-point coordinates (UNSIGNED_INT_VECTOR[N], NEIGHBOR_LIST::uint_crd). */
+SB_API int sb_nl_uint_crd(sb_neighbor_list* nl, const uint32_t** d_uint_crd);
+
+/* ------------------------------------------------------------------------------------------
+ * Lennard-Jones + PME direct space — replaces LENNARD_JONES_INFORMATION
+ * (SPONGE/Lennard_Jones_force/Lennard_Jones_force.cuh:41-149)
+ * ---------------------------------------------------------------------------------------- */
+
+/* LENNARD_JONES_INFORMATION::Initial (Lennard_Jones_force.cu:1067-1139). h_LJ_A / h_LJ_B are
+ * the lower-triangular tables as the module stores them (already x12 and x6, pair index
+ * max*(max+1)/2 + min), h_atom_LJ_type the per-atom type. The long-range correction factor is
+ * computed in FP64 from type counts. */
+SB_API int sb_lj_create(int atom_numbers, int atom_type_numbers, const float* h_LJ_A,
+                 const float* h_LJ_B, const int* h_atom_LJ_type, float cutoff,
+                 const float box_length[3], int form, sb_lennard_jones** out);
+
+/* LENNARD_JONES_INFORMATION::Clear (Lennard_Jones_force.cu:1141-1176) */
+SB_API int sb_lj_destroy(sb_lennard_jones* lj);
+
+/* LENNARD_JONES_INFORMATION::LJ_PME_Direct_Force_With_Atom_Energy_And_Virial
+ * (Lennard_Jones_force.cu:1318-1352): LJ + Ewald direct force over the list of `nl`, added to
+ * d_frc. need_atom_energy adds LJ + direct Coulomb energy per atom into d_atom_energy;
+ * need_virial adds the LJ virial per atom into d_atom_lj_virial and overwrites
+ * d_atom_direct_pme_energy with the direct Coulomb energy per atom. */
+SB_API int sb_lj_pme_direct_force(sb_lennard_jones* lj, sb_neighbor_list* nl, int atom_numbers,
+                           const uint32_t* d_uint_crd, const float* d_charge, float* d_frc,
+                           float pme_beta, int need_atom_energy, float* d_atom_energy,
+                           int need_virial, float* d_atom_lj_virial,
+                           float* d_atom_direct_pme_energy, void* stream);
+
+/* LENNARD_JONES_INFORMATION::Long_Range_Correction (Lennard_Jones_force.cu:1178-1191) */
+SB_API int sb_lj_long_range_correction(sb_lennard_jones* lj, int need_pressure, float* d_virial,
+                                int need_potential, float* d_potential, void* stream);
+
+/* LENNARD_JONES_INFORMATION::Get_Energy (Lennard_Jones_force.cu:1407-1433): LJ energy within
+ * the cutoff over the list plus the long-range correction, reduced in FP64. */
+SB_API int sb_lj_get_energy(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                     float* h_energy, void* stream);
+
+/* LENNARD_JONES_INFORMATION::Update_Volume */
+SB_API int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[3]);
+
+/* Public members read by other modules: long_range_factor (FP64-computed, returned as float). */
+SB_API int sb_lj_long_range_factor(sb_lennard_jones* lj, float* h_factor);
+
+/* ------------------------------------------------------------------------------------------
+ * PME — replaces Particle_Mesh_Ewald (SPONGE/PME_force/PME_force.cuh:25-123)
+ * ---------------------------------------------------------------------------------------- */
+
+/* Particle_Mesh_Ewald::Initial (PME_force.cu:108-306). fft* <= 0 picks the size as the
+ * reference's Get_Fft_Patameter does; tolerance is PME_Direct_Tolerance (default 1e-5). The
+ * B-spline moduli and the Green's-function table are computed in FP64. */
+SB_API int sb_pme_create(int atom_numbers, const float box_length[3], float cutoff, float tolerance,
+                  int fftx, int ffty, int fftz, int form, sb_pme** out);
+
+/* Particle_Mesh_Ewald::Clear */
+SB_API int sb_pme_destroy(sb_pme* pme);
+
+/* Public members beta, fftx/ffty/fftz, and the device arrays d_direct_atom_energy (filled by
+ * sb_lj_pme_direct_force with need_virial) and d_correction_atom_energy (filled by
+ * sb_pme_excluded_force), which the reference reads in its energy and virial sums. */
+SB_API int sb_pme_info(sb_pme* pme, float* h_beta, int* h_fft3);
+SB_API int sb_pme_atom_energy_arrays(sb_pme* pme, float** d_direct_atom_energy,
+                              float** d_correction_atom_energy);
+
+/* Particle_Mesh_Ewald::PME_Excluded_Force_With_Atom_Energy (PME_force.cu:697-708): Ewald
+ * correction for every exclusion CSR entry, force added to d_frc, per-atom correction energy
+ * written (reset then +=) to d_atom_energy (the reference passes d_correction_atom_energy). */
+SB_API int sb_pme_excluded_force(sb_pme* pme, const uint32_t* d_uint_crd, const float scaler[3],
+                          const float* d_charge, const int* d_excluded_list_start,
+                          const int* d_excluded_list, const int* d_excluded_numbers,
+                          float* d_frc, float* d_atom_energy, void* stream);
+
+/* Particle_Mesh_Ewald::PME_Reciprocal_Force_With_Energy_And_Virial (PME_force.cu:722-773):
+ * B-spline spread, 3D real FFT, Green's-function convolution, inverse FFT, force gather (added
+ * to d_frc). need_energy adds correction + self + reciprocal energy to *d_potential;
+ * need_virial adds direct + correction + self + reciprocal energy to *d_virial. */
+SB_API int sb_pme_reciprocal_force(sb_pme* pme, const uint32_t* d_uint_crd, const float* d_charge,
+                            float* d_frc, int need_virial, int need_energy, float* d_virial,
+                            float* d_potential, void* stream);
+
+/* Particle_Mesh_Ewald::Get_Energy (PME_force.cu:892-994). which_part is SB_PME_*. The DIRECT
+ * part is evaluated over the list of `nl` (may be NULL for other parts). h_parts (optional,
+ * 5 doubles) receives total, direct, reciprocal, correction, self as computed (FP64). */
+SB_API int sb_pme_get_energy(sb_pme* pme, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                      const float* d_charge, const float scaler[3],
+                      const int* d_excluded_list_start, const int* d_excluded_list,
+                      const int* d_excluded_numbers, int which_part, float* h_energy,
+                      double* h_parts, void* stream);
+
+/* Particle_Mesh_Ewald::Update_Box_Length / Update_Volume (PME_force.cu:996-1042) */
+SB_API int sb_pme_update_box(sb_pme* pme, const float box_length[3]);
+
+/* ------------------------------------------------------------------------------------------
+ * Whole nonbonded force evaluation of one MD step, as Main_Calculate_Force + Main_Iteration
+ * call the three modules (SPONGE/main.cu:180-193 and :376): list update by its policy, LJ +
+ * direct, long-range correction, exclusion correction, reciprocal space. Forces are added to
+ * d_frc. The flags and outputs have the meanings of the module calls above.
+ * ---------------------------------------------------------------------------------------- */
+SB_API int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme, float* d_crd,
+                      const uint32_t* d_uint_crd, const float* d_charge,
+                      const int* d_excluded_list_start, const int* d_excluded_list,
+                      const int* d_excluded_numbers, float* d_frc, int need_energy,
+                      int need_virial, float* d_atom_energy, float* d_atom_virial,
+                      float* d_virial, float* d_potential, void* stream);
+
+/* Crd_To_Uint_Crd (SPONGE/common.cu:264-287) with the quarter coefficient 0.25*2^32/L, as
+ * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */
+SB_API int sb_crd_to_uint_crd(int atom_numbers, const float box_length[3], const float* d_crd,
+                       uint32_t* d_uint_crd, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPONGE_B200_H */

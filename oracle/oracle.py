@@ -1,0 +1,271 @@
+"""ctypes wrappers around ``liboracle.so`` (built from ``oracle.cpp`` by ``oracle/Makefile``).
+
+Test infrastructure only: see the package docstring. Each wrapper names the reference code it
+restates; the C++ file carries the full citations.
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+
+
+def build(force=False):
+    """Compile liboracle.so with the committed Makefile (g++ only)."""
+    so = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "oracle.cpp")
+    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(so):
+            build()
+        L = ctypes.CDLL(so)
+        L.orc_periodic_map.argtypes = [ctypes.c_int, _f32p, _f32p]
+        L.orc_crd_to_uint.argtypes = [ctypes.c_int, _f32p, _f32p, _u32p]
+        L.orc_get_beta.argtypes = [ctypes.c_float, ctypes.c_float]
+        L.orc_get_beta.restype = ctypes.c_float
+        L.orc_fft_size.argtypes = [ctypes.c_float]
+        L.orc_fft_size.restype = ctypes.c_int
+        L.orc_bspline_moduli.argtypes = [ctypes.c_int, _f64p]
+        pairfn = [ctypes.c_int, _u32p, _f32p, ctypes.c_float, ctypes.c_float, _i32p, _i32p,
+                  _i32p, _i64p, ctypes.c_long, ctypes.c_int]
+        for f in (L.orc_pairs_bruteforce, L.orc_pairs_cells):
+            f.argtypes = pairfn
+            f.restype = ctypes.c_long
+        L.orc_direct.argtypes = [ctypes.c_int, _u32p, _f32p, _i32p, _f32p, _f32p, _f32p,
+                                 ctypes.c_float, ctypes.c_double, _i64p, ctypes.c_long, _f64p,
+                                 _f64p, _f64p, ctypes.c_int]
+        L.orc_lrc_factor.argtypes = [ctypes.c_int, _i32p, ctypes.c_int, _f32p, ctypes.c_float]
+        L.orc_lrc_factor.restype = ctypes.c_double
+        L.orc_excluded.argtypes = [ctypes.c_int, _u32p, _f32p, _f32p, ctypes.c_double, _i32p,
+                                   _i32p, _i32p, _f64p, _f64p, _f64p]
+        L.orc_self_energy.argtypes = [ctypes.c_int, _f32p, ctypes.c_double, ctypes.c_double]
+        L.orc_self_energy.restype = ctypes.c_double
+        L.orc_fft3.argtypes = [_f64p, _i32p, ctypes.c_int, ctypes.c_int]
+        L.orc_pme.argtypes = [ctypes.c_int, _u32p, _f32p, _f32p, _i32p, ctypes.c_double, _f64p,
+                              _f64p, ctypes.c_void_p, ctypes.c_int]
+        L.orc_ewald_recip.argtypes = [ctypes.c_int, _u32p, _f32p, _f32p, ctypes.c_double,
+                                      ctypes.c_int, _f64p, _f64p, ctypes.c_int]
+        L.orc_nonbonded.argtypes = [ctypes.c_int, _u32p, _f32p, _i32p, _f32p, _f32p, _f32p,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_double, _i32p,
+                                    _i32p, _i32p, _i32p, _f64p, _f64p, ctypes.c_int]
+        L.orc_nonbonded.restype = ctypes.c_long
+        L.orc_threads.restype = ctypes.c_int
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        _LIB = L
+    return _LIB
+
+
+def threads():
+    return lib().orc_threads()
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def periodic_map(crd, box):
+    """Crd_Periodic_Map (SPONGE/common.cu:299-352); returns a wrapped copy."""
+    c = np.ascontiguousarray(crd, np.float32).copy()
+    lib().orc_periodic_map(c.shape[0], c.reshape(-1), np.ascontiguousarray(box, np.float32))
+    return c
+
+
+def crd_to_uint(crd, box):
+    """Crd_To_Uint_Crd with the quarter coefficient (SPONGE/common.cu:264-287)."""
+    c = np.ascontiguousarray(crd, np.float32)
+    out = np.empty((c.shape[0], 3), np.uint32)
+    lib().orc_crd_to_uint(c.shape[0], c.reshape(-1), np.ascontiguousarray(box, np.float32),
+                          out.reshape(-1))
+    return out
+
+
+def get_beta(cutoff, tolerance=1e-5):
+    """Get_Beta (SPONGE/PME_force/PME_force.cu:71-100)."""
+    return float(lib().orc_get_beta(cutoff, tolerance))
+
+
+def fft_size(length):
+    """Get_Fft_Patameter (SPONGE/common.cu:513-534)."""
+    return int(lib().orc_fft_size(length))
+
+
+def bspline_moduli(K):
+    out = np.empty(K, np.float64)
+    lib().orc_bspline_moduli(K, out)
+    return out
+
+
+def _excl(sys):
+    return (np.ascontiguousarray(sys["excl_start"], np.int32),
+            np.ascontiguousarray(sys["excl_numbers"], np.int32),
+            np.ascontiguousarray(sys["excl_list"], np.int32) if len(sys["excl_list"])
+            else np.zeros(1, np.int32))
+
+
+def pairs(uc, sys, method="cells", cap=None, nthreads=0):
+    """Half pair set {i<j} as sorted int64 keys i*N+j under the pinned FP32 criterion."""
+    n = uc.shape[0]
+    if cap is None:
+        cap = max(1024, n * 800)
+    out = np.empty(cap, np.int64)
+    es, en, el = _excl(sys)
+    f = lib().orc_pairs_bruteforce if method == "brute" else lib().orc_pairs_cells
+    cnt = f(n, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+            np.ascontiguousarray(sys["box"], np.float32), sys["cutoff"], sys["skin"],
+            es, en, el, out, cap, nthreads)
+    if cnt > cap:
+        return pairs(uc, sys, method, cap=int(cnt) + 16, nthreads=nthreads)
+    return out[:cnt].copy()
+
+
+def scaled_tables(sys):
+    """h_LJ_A * 12 and h_LJ_B * 6 in float, as the LJ module stores them (Lennard_Jones_force.cu:1092-1098)."""
+    A12 = (np.asarray(sys["lj_A"], np.float32) * np.float32(12.0)).astype(np.float32)
+    B6 = (np.asarray(sys["lj_B"], np.float32) * np.float32(6.0)).astype(np.float32)
+    return A12, B6
+
+
+def direct(uc, sys, pair_keys, beta, nthreads=0):
+    """LJ + Ewald direct force/energies/virial over a pair set in FP64.
+
+    Returns (frc [N,3] f64, atom_energy [N] f64, dict(e_lj, e_direct, virial_lj, n_in_cutoff))."""
+    n = uc.shape[0]
+    A12, B6 = scaled_tables(sys)
+    frc = np.zeros(3 * n, np.float64)
+    ae = np.zeros(n, np.float64)
+    out = np.zeros(4, np.float64)
+    pk = np.ascontiguousarray(pair_keys, np.int64)
+    if pk.size == 0:
+        pk = np.zeros(1, np.int64)
+        npairs = 0
+    else:
+        npairs = pk.size
+    lib().orc_direct(n, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                     np.ascontiguousarray(sys["charge"], np.float32),
+                     np.ascontiguousarray(sys["lj_type"], np.int32), A12, B6,
+                     np.ascontiguousarray(sys["box"], np.float32), sys["cutoff"], beta, pk,
+                     npairs, frc, ae, out, nthreads)
+    return frc.reshape(n, 3), ae, dict(e_lj=out[0], e_direct=out[1], virial_lj=out[2],
+                                       n_in_cutoff=int(out[3]))
+
+
+def lrc_factor(sys):
+    _, B6 = scaled_tables(sys)
+    return float(lib().orc_lrc_factor(len(sys["lj_type"]),
+                                      np.ascontiguousarray(sys["lj_type"], np.int32),
+                                      int(sys["n_types"]), B6, sys["cutoff"]))
+
+
+def excluded(uc, sys, beta):
+    """Exclusion correction (SPONGE/PME_force/PME_force.cu:620-695)."""
+    n = uc.shape[0]
+    frc = np.zeros(3 * n, np.float64)
+    ae = np.zeros(n, np.float64)
+    out = np.zeros(1, np.float64)
+    es, en, el = _excl(sys)
+    lib().orc_excluded(n, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                       np.ascontiguousarray(sys["charge"], np.float32),
+                       np.ascontiguousarray(sys["box"], np.float32), beta, es, en, el, frc, ae,
+                       out)
+    return frc.reshape(n, 3), ae, float(out[0])
+
+
+def self_energy(sys, beta):
+    box = np.asarray(sys["box"], np.float64)
+    return float(lib().orc_self_energy(len(sys["charge"]),
+                                       np.ascontiguousarray(sys["charge"], np.float32), beta,
+                                       float(box[0] * box[1] * box[2])))
+
+
+def fft3(grid, sign):
+    """Unnormalised 3D FFT (sign -1 forward, +1 inverse) of a complex128 grid."""
+    g = np.ascontiguousarray(grid, np.complex128).copy()
+    K = np.array(g.shape, np.int32)
+    lib().orc_fft3(g.view(np.float64).reshape(-1), K, int(sign), 0)
+    return g
+
+
+def pme(uc, sys, beta, fft=None, want_grid=False, nthreads=0):
+    """SPME reciprocal force and energy in FP64. Returns (frc [N,3], E_rec[, Q grid])."""
+    n = uc.shape[0]
+    K = np.array(fft if fft is not None else sys["fft"], np.int32)
+    frc = np.zeros(3 * n, np.float64)
+    out = np.zeros(1, np.float64)
+    grid = np.zeros(int(K.prod()), np.float64) if want_grid else None
+    lib().orc_pme(n, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                  np.ascontiguousarray(sys["charge"], np.float32),
+                  np.ascontiguousarray(sys["box"], np.float32), K, beta, frc, out,
+                  grid.ctypes.data if grid is not None else None, nthreads)
+    if want_grid:
+        return frc.reshape(n, 3), float(out[0]), grid.reshape(tuple(K))
+    return frc.reshape(n, 3), float(out[0])
+
+
+def ewald_recip(uc, sys, beta, kmax, nthreads=0):
+    """Classic Ewald reciprocal sum (no grid): converged reference for the SPME method error."""
+    n = uc.shape[0]
+    frc = np.zeros(3 * n, np.float64)
+    out = np.zeros(1, np.float64)
+    lib().orc_ewald_recip(n, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                          np.ascontiguousarray(sys["charge"], np.float32),
+                          np.ascontiguousarray(sys["box"], np.float32), beta, kmax, frc, out,
+                          nthreads)
+    return frc.reshape(n, 3), float(out[0])
+
+
+def nonbonded(uc, sys, beta, nthreads=0):
+    """Whole FP64 evaluation (cell list + direct + exclusions + SPME): the CPU baseline.
+
+    Returns (frc [N,3], dict of energies, pair count)."""
+    n = uc.shape[0]
+    A12, B6 = scaled_tables(sys)
+    frc = np.zeros(3 * n, np.float64)
+    out = np.zeros(7, np.float64)
+    es, en, el = _excl(sys)
+    npairs = lib().orc_nonbonded(n, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                                 np.ascontiguousarray(sys["charge"], np.float32),
+                                 np.ascontiguousarray(sys["lj_type"], np.int32), A12, B6,
+                                 np.ascontiguousarray(sys["box"], np.float32), sys["cutoff"],
+                                 sys["skin"], beta, np.array(sys["fft"], np.int32), es, en, el,
+                                 frc, out, nthreads)
+    if npairs < 0:
+        raise MemoryError("oracle pair buffer allocation failed")
+    keys = ("e_lj", "e_direct", "e_corr", "e_rec", "e_self", "virial_lj", "n_in_cutoff")
+    return frc.reshape(n, 3), dict(zip(keys, out.tolist())), int(npairs)
+
+
+def reference_energies(sys, uc=None, nthreads=0):
+    """All FP64 quantities for a system in one call (convenience for tests)."""
+    if uc is None:
+        uc = crd_to_uint(periodic_map(sys["crd"], sys["box"]), sys["box"])
+    beta = get_beta(sys["cutoff"], sys["tolerance"])
+    pk = pairs(uc, sys, nthreads=nthreads)
+    fd, ae, d = direct(uc, sys, pk, beta, nthreads)
+    fe, aee, ecorr = excluded(uc, sys, beta)
+    fr, erec = pme(uc, sys, beta, nthreads=nthreads)
+    box = np.asarray(sys["box"], np.float64)
+    V = float(box.prod())
+    f = lrc_factor(sys)
+    res = dict(beta=beta, pairs=pk, uc=uc, f_direct=fd, f_excl=fe, f_rec=fr,
+               e_lj=d["e_lj"], e_direct=d["e_direct"], virial_lj=d["virial_lj"],
+               n_in_cutoff=d["n_in_cutoff"], e_corr=ecorr, e_rec=erec,
+               e_self=self_energy(sys, beta), lrc_factor=f, e_lrc=f / V, virial_lrc=6 * f / V)
+    res["f_total"] = fd + fe + fr
+    return res

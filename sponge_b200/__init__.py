@@ -1,0 +1,378 @@
+"""sponge_b200: B200-native nonbonded hot path of SPONGE behind its module API.
+
+Python mirror of the three SPONGE module structs, calling the C ABI of libsponge_b200.so
+(include/sponge_b200.h) with torch CUDA tensors as device memory:
+
+* ``NeighborList``      <- NEIGHBOR_LIST              (SPONGE/neighbor_list/neighbor_list.cuh:44-106)
+* ``LennardJones``      <- LENNARD_JONES_INFORMATION  (SPONGE/Lennard_Jones_force/Lennard_Jones_force.cuh:41-149)
+* ``ParticleMeshEwald`` <- Particle_Mesh_Ewald        (SPONGE/PME_force/PME_force.cuh:25-123)
+
+Method names, argument meaning and accumulation semantics (+= into forces, per-atom energies
+and the single-float virial/potential) are the reference's. There is no CPU path: every call
+needs the compiled library and a CUDA device, and fails loudly otherwise.
+
+Coordinates in fixed point are held in torch.int32 tensors carrying the uint32 bit pattern
+(torch has no general uint32 arithmetic); shape [N, 3].
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBPATH = os.path.join(_HERE, "libsponge_b200.so")
+_LIB = None
+
+FORM_FIXED = 0
+FORM_PLAIN = 1
+
+PME_TOTAL, PME_DIRECT, PME_RECIPROCAL, PME_CORRECTION, PME_SELF = range(5)
+
+STATUS_LIST_OVERFLOW = 1
+STATUS_COLUMN_OVERFLOW = 2
+STATUS_ATOMGROUP_OVERFLOW = 4
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_f = ctypes.c_float
+
+# name -> argtypes (restype int unless stated)
+_SIGS = {
+    "sb_version": [],
+    "sb_last_error": [],
+    "sb_nl_create": [_i, _vp, _f, _f, _i, _f, _i, _i, _vp],
+    "sb_nl_destroy": [_vp],
+    "sb_nl_update": [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp],
+    "sb_nl_update_volume": [_vp, _vp],
+    "sb_nl_atom_group": [_vp, _vp, _vp],
+    "sb_nl_pair_count": [_vp, _vp, _vp],
+    "sb_nl_export_pairs": [_vp, _vp, ctypes.c_int64, _vp, _vp],
+    "sb_nl_status": [_vp, _vp, _vp],
+    "sb_nl_uint_crd": [_vp, _vp],
+    "sb_lj_create": [_i, _i, _vp, _vp, _vp, _f, _vp, _i, _vp],
+    "sb_lj_destroy": [_vp],
+    "sb_lj_pme_direct_force": [_vp, _vp, _i, _vp, _vp, _vp, _f, _i, _vp, _i, _vp, _vp, _vp],
+    "sb_lj_long_range_correction": [_vp, _i, _vp, _i, _vp, _vp],
+    "sb_lj_get_energy": [_vp, _vp, _vp, _vp, _vp],
+    "sb_lj_update_volume": [_vp, _vp],
+    "sb_lj_long_range_factor": [_vp, _vp],
+    "sb_pme_create": [_i, _vp, _f, _f, _i, _i, _i, _i, _vp],
+    "sb_pme_destroy": [_vp],
+    "sb_pme_info": [_vp, _vp, _vp],
+    "sb_pme_atom_energy_arrays": [_vp, _vp, _vp],
+    "sb_pme_excluded_force": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_pme_reciprocal_force": [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
+    "sb_pme_get_energy": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp],
+    "sb_pme_update_box": [_vp, _vp],
+    "sb_nonbonded_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp,
+                          _vp, _vp, _vp],
+    "sb_crd_to_uint_crd": [_i, _vp, _vp, _vp, _vp],
+}
+
+
+class SpongeError(RuntimeError):
+    pass
+
+
+def library_path():
+    return _LIBPATH
+
+
+def lib():
+    """Load libsponge_b200.so (built in-tree by ``python -m sponge_b200.build``)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(_LIBPATH):
+            raise SpongeError("libsponge_b200.so is not built: run `python -m sponge_b200.build`")
+        L = ctypes.CDLL(_LIBPATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        L.sb_last_error.restype = ctypes.c_char_p
+        _LIB = L
+    return _LIB
+
+
+def _check(status):
+    if status != 0:
+        msg = lib().sb_last_error()
+        raise SpongeError("sponge_b200 error %d: %s" % (status, msg.decode() if msg else ""))
+
+
+def _require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise SpongeError("sponge_b200 needs a CUDA device; there is no CPU path")
+    return torch
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda:
+        raise SpongeError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise SpongeError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return stream if isinstance(stream, int) else stream.cuda_stream
+
+
+def _box3(box):
+    return (ctypes.c_float * 3)(*[float(v) for v in np.broadcast_to(np.asarray(box, np.float64), 3)])
+
+
+class DeviceArray:
+    """Zero-copy view of library-owned device memory (``torch.as_tensor(x, device='cuda')``)."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def crd_to_uint_crd(crd, box, out=None, stream=None):
+    """Crd_To_Uint_Crd with the quarter coefficient (SPONGE/common.cu:264-287)."""
+    torch = _require_cuda()
+    n = crd.shape[0]
+    if out is None:
+        out = torch.empty((n, 3), dtype=torch.int32, device=crd.device)
+    _check(lib().sb_crd_to_uint_crd(n, _box3(box), _ptr(crd), _ptr(out), _stream(stream)))
+    return out
+
+
+class NeighborList:
+    """NEIGHBOR_LIST. ``Neighbor_List_Update`` wraps ``crd`` into the box in place on rebuilds."""
+
+    CONDITIONAL_UPDATE, FORCED_UPDATE = 0, 1
+    CONDITIONAL_CHECK, FORCED_CHECK = 0, 1
+
+    def __init__(self, atom_numbers, box_length, cutoff, skin, refresh_interval=0,
+                 skin_permit=0.5, max_neighbor_numbers=800, form=FORM_FIXED):
+        _require_cuda()
+        self.atom_numbers = int(atom_numbers)
+        self.cutoff, self.skin = float(cutoff), float(skin)
+        self.box_length = np.asarray(box_length, np.float32)
+        self.max_neighbor_numbers = int(max_neighbor_numbers)
+        self.handle = ctypes.c_void_p()
+        _check(lib().sb_nl_create(self.atom_numbers, _box3(box_length), self.cutoff, self.skin,
+                                  int(refresh_interval), float(skin_permit),
+                                  self.max_neighbor_numbers, int(form), ctypes.byref(self.handle)))
+
+    def Neighbor_List_Update(self, crd, excluded_list_start=None, excluded_list=None,
+                             excluded_numbers=None, forced_update=0, forced_check=0, stream=None):
+        _check(lib().sb_nl_update(self.handle, _ptr(crd), _ptr(excluded_list_start),
+                                  _ptr(excluded_list), _ptr(excluded_numbers), int(forced_update),
+                                  int(forced_check), _stream(stream)))
+
+    def Update_Volume(self, box_length):
+        self.box_length = np.asarray(box_length, np.float32)
+        _check(lib().sb_nl_update_volume(self.handle, _box3(box_length)))
+
+    @property
+    def d_nl(self):
+        """Device address of the ATOM_GROUP[N] compatibility list (materialised on demand)."""
+        p = ctypes.c_void_p()
+        _check(lib().sb_nl_atom_group(self.handle, ctypes.byref(p), _stream(None)))
+        return p.value
+
+    def pair_count(self):
+        c = ctypes.c_int64()
+        _check(lib().sb_nl_pair_count(self.handle, ctypes.byref(c), _stream(None)))
+        return c.value
+
+    def export_pairs(self):
+        """Half pair set as sorted int64 keys i*N + j (i < j)."""
+        n = self.pair_count()
+        keys = np.empty(max(n, 1), np.int64)
+        c = ctypes.c_int64()
+        _check(lib().sb_nl_export_pairs(self.handle, keys.ctypes.data, n, ctypes.byref(c),
+                                        _stream(None)))
+        return keys[:c.value]
+
+    def status(self):
+        f = ctypes.c_int()
+        _check(lib().sb_nl_status(self.handle, ctypes.byref(f), _stream(None)))
+        return f.value
+
+    def uint_crd(self):
+        torch = _require_cuda()
+        p = ctypes.c_void_p()
+        _check(lib().sb_nl_uint_crd(self.handle, ctypes.byref(p)))
+        return torch.as_tensor(DeviceArray(p.value, (self.atom_numbers, 3), "<i4"), device="cuda")
+
+    def Clear(self):
+        if self.handle:
+            lib().sb_nl_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+
+class LennardJones:
+    """LENNARD_JONES_INFORMATION. ``LJ_A``/``LJ_B`` are the lower-triangular tables already
+    multiplied by 12 and 6 (h_LJ_A / h_LJ_B of the reference)."""
+
+    def __init__(self, atom_numbers, atom_type_numbers, LJ_A, LJ_B, atom_LJ_type, cutoff,
+                 box_length, form=FORM_FIXED):
+        _require_cuda()
+        self.atom_numbers = int(atom_numbers)
+        self.atom_type_numbers = int(atom_type_numbers)
+        self.h_LJ_A = np.ascontiguousarray(LJ_A, np.float32)
+        self.h_LJ_B = np.ascontiguousarray(LJ_B, np.float32)
+        self.h_atom_LJ_type = np.ascontiguousarray(atom_LJ_type, np.int32)
+        self.cutoff = float(cutoff)
+        self.handle = ctypes.c_void_p()
+        _check(lib().sb_lj_create(self.atom_numbers, self.atom_type_numbers,
+                                  self.h_LJ_A.ctypes.data, self.h_LJ_B.ctypes.data,
+                                  self.h_atom_LJ_type.ctypes.data, self.cutoff,
+                                  _box3(box_length), int(form), ctypes.byref(self.handle)))
+
+    @property
+    def long_range_factor(self):
+        f = ctypes.c_float()
+        _check(lib().sb_lj_long_range_factor(self.handle, ctypes.byref(f)))
+        return f.value
+
+    def LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(self, atom_numbers, uint_crd, charge, frc,
+                                                        nl, pme_beta, need_atom_energy=0,
+                                                        atom_energy=None, need_virial=0,
+                                                        atom_lj_virial=None,
+                                                        atom_direct_pme_energy=None,
+                                                        stream=None):
+        _check(lib().sb_lj_pme_direct_force(self.handle, nl.handle, int(atom_numbers),
+                                            _ptr(uint_crd), _ptr(charge), _ptr(frc),
+                                            float(pme_beta), int(need_atom_energy),
+                                            _ptr(atom_energy), int(need_virial),
+                                            _ptr(atom_lj_virial), _ptr(atom_direct_pme_energy),
+                                            _stream(stream)))
+
+    def Long_Range_Correction(self, need_pressure, d_virial, need_potential, d_potential,
+                              stream=None):
+        _check(lib().sb_lj_long_range_correction(self.handle, int(need_pressure), _ptr(d_virial),
+                                                 int(need_potential), _ptr(d_potential),
+                                                 _stream(stream)))
+
+    def Get_Energy(self, uint_crd, nl, stream=None):
+        e = ctypes.c_float()
+        _check(lib().sb_lj_get_energy(self.handle, nl.handle, _ptr(uint_crd), ctypes.byref(e),
+                                      _stream(stream)))
+        return e.value
+
+    def Update_Volume(self, box_length):
+        _check(lib().sb_lj_update_volume(self.handle, _box3(box_length)))
+
+    def Clear(self):
+        if self.handle:
+            lib().sb_lj_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+
+class ParticleMeshEwald:
+    """Particle_Mesh_Ewald. ``fft`` entries <= 0 pick the size as Get_Fft_Patameter does."""
+
+    TOTAL, DIRECT, RECIPROCAL, CORRECTION, SELF = range(5)
+
+    def __init__(self, atom_numbers, box_length, cutoff, tolerance=1e-5, fft=(-1, -1, -1),
+                 form=FORM_FIXED):
+        torch = _require_cuda()
+        self.atom_numbers = int(atom_numbers)
+        self.box_length = np.asarray(box_length, np.float32)
+        self.handle = ctypes.c_void_p()
+        f = [int(v) if v is not None else -1 for v in (fft if fft is not None else (-1, -1, -1))]
+        _check(lib().sb_pme_create(self.atom_numbers, _box3(box_length), float(cutoff),
+                                   float(tolerance), f[0], f[1], f[2], int(form),
+                                   ctypes.byref(self.handle)))
+        b = ctypes.c_float()
+        k = (ctypes.c_int * 3)()
+        _check(lib().sb_pme_info(self.handle, ctypes.byref(b), k))
+        self.beta = b.value
+        self.fftx, self.ffty, self.fftz = k[0], k[1], k[2]
+        pd, pc = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib().sb_pme_atom_energy_arrays(self.handle, ctypes.byref(pd), ctypes.byref(pc)))
+        self.d_direct_atom_energy = torch.as_tensor(
+            DeviceArray(pd.value, (self.atom_numbers,), "<f4"), device="cuda")
+        self.d_correction_atom_energy = torch.as_tensor(
+            DeviceArray(pc.value, (self.atom_numbers,), "<f4"), device="cuda")
+
+    def scaler(self):
+        return (np.float32(1.0) / np.float32(4294967296.0)) * self.box_length
+
+    def PME_Excluded_Force_With_Atom_Energy(self, uint_crd, scaler, charge, excluded_list_start,
+                                            excluded_list, excluded_numbers, frc, atom_energy,
+                                            stream=None):
+        _check(lib().sb_pme_excluded_force(self.handle, _ptr(uint_crd), _box3(scaler),
+                                           _ptr(charge), _ptr(excluded_list_start),
+                                           _ptr(excluded_list), _ptr(excluded_numbers),
+                                           _ptr(frc), _ptr(atom_energy), _stream(stream)))
+
+    def PME_Reciprocal_Force_With_Energy_And_Virial(self, uint_crd, charge, force, need_virial=0,
+                                                    need_energy=0, d_virial=None,
+                                                    d_potential=None, stream=None):
+        _check(lib().sb_pme_reciprocal_force(self.handle, _ptr(uint_crd), _ptr(charge),
+                                             _ptr(force), int(need_virial), int(need_energy),
+                                             _ptr(d_virial), _ptr(d_potential), _stream(stream)))
+
+    def Get_Energy(self, uint_crd, charge, nl, scaler, excluded_list_start, excluded_list,
+                   excluded_numbers, which_part=0, parts=False, stream=None):
+        e = ctypes.c_float()
+        p = (ctypes.c_double * 5)()
+        _check(lib().sb_pme_get_energy(self.handle, nl.handle if nl is not None else None,
+                                       _ptr(uint_crd), _ptr(charge), _box3(scaler),
+                                       _ptr(excluded_list_start), _ptr(excluded_list),
+                                       _ptr(excluded_numbers), int(which_part), ctypes.byref(e),
+                                       p, _stream(stream)))
+        if parts:
+            return e.value, dict(zip(("total", "direct", "reciprocal", "correction", "self"),
+                                     list(p)))
+        return e.value
+
+    def Update_Box_Length(self, box_length):
+        self.box_length = np.asarray(box_length, np.float32)
+        _check(lib().sb_pme_update_box(self.handle, _box3(box_length)))
+
+    Update_Volume = Update_Box_Length
+
+    def Clear(self):
+        if self.handle:
+            lib().sb_pme_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+
+def nonbonded_step(nl, lj, pme, crd, uint_crd, charge, excl, frc, need_energy=0, need_virial=0,
+                   atom_energy=None, atom_virial=None, d_virial=None, d_potential=None,
+                   stream=None):
+    """One MD step's nonbonded forces through the fused C entry point (sb_nonbonded_step)."""
+    es, el, en = excl
+    _check(lib().sb_nonbonded_step(nl.handle, lj.handle, pme.handle, _ptr(crd), _ptr(uint_crd),
+                                   _ptr(charge), _ptr(es), _ptr(el), _ptr(en), _ptr(frc),
+                                   int(need_energy), int(need_virial), _ptr(atom_energy),
+                                   _ptr(atom_virial), _ptr(d_virial), _ptr(d_potential),
+                                   _stream(stream)))
+
+
+from .engine import NonbondedEngine  # noqa: E402,F401

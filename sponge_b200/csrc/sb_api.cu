@@ -1,0 +1,89 @@
+// C ABI glue: error reporting, allocation, FP64 reductions and the whole-step entry point.
+
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "sb_internal.cuh"
+
+static thread_local char g_err[1024] = "";
+
+void sb_set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+extern "C" const char* sb_last_error(void) { return g_err; }
+
+extern "C" int sb_version(void) { return 100; }
+
+int sb_malloc(void** p, size_t bytes, const char* what) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        sb_set_error("cudaMalloc of %zu bytes for %s failed: %s", bytes, what,
+                     cudaGetErrorString(e));
+        return SB_ERR_ALLOC;
+    }
+    return SB_OK;
+}
+
+void sb_free(void* p) {
+    if (p) cudaFree(p);
+}
+
+__global__ void __launch_bounds__(1024) k_reduce_f32(const float* __restrict__ x, int n,
+                                                     double* __restrict__ out) {
+    __shared__ double red[1024];
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)x[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = red[0];
+}
+
+int sb_reduce_sum_f32(const float* d_x, int n, double* d_out, cudaStream_t s) {
+    k_reduce_f32<<<1, 1024, 0, s>>>(d_x, n, d_out);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+extern "C" int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
+                                 float* d_crd, const uint32_t* d_uint_crd, const float* d_charge,
+                                 const int* es, const int* el, const int* en, float* d_frc,
+                                 int need_energy, int need_virial, float* d_atom_energy,
+                                 float* d_atom_virial, float* d_virial, float* d_potential,
+                                 void* stream) {
+    if (!nl || !lj || !pme || !d_crd || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_nonbonded_step: null argument");
+        return SB_ERR_ARG;
+    }
+    // Main_Iteration's list update follows the previous step's integration; the list built
+    // here is used for this step's forces (the order a driver calling update then force sees)
+    SB_TRY(sb_nl_update(nl, d_crd, es, el, en, 0, 0, stream));
+    float* d_direct = nullptr;
+    float* d_corr = nullptr;
+    SB_TRY(sb_pme_atom_energy_arrays(pme, &d_direct, &d_corr));
+    SB_TRY(sb_lj_pme_direct_force(lj, nl, lj->n, d_uint_crd, d_charge, d_frc, pme->beta,
+                                  need_energy, d_atom_energy, need_virial, d_atom_virial,
+                                  d_direct, stream));
+    SB_TRY(sb_lj_long_range_correction(lj, need_virial, d_virial, need_energy, d_potential,
+                                       stream));
+    const float sc[3] = {(1.0f / 4294967296.0f) * pme->box[0],
+                         (1.0f / 4294967296.0f) * pme->box[1],
+                         (1.0f / 4294967296.0f) * pme->box[2]};
+    SB_TRY(sb_pme_excluded_force(pme, d_uint_crd, sc, d_charge, es, el, en, d_frc, d_corr,
+                                 stream));
+    SB_TRY(sb_pme_reciprocal_force(pme, d_uint_crd, d_charge, d_frc, need_virial, need_energy,
+                                   d_virial, d_potential, stream));
+    return SB_OK;
+}

@@ -1,0 +1,525 @@
+// Hand-written shared-memory 3D real FFT + Green's-function convolution for PME reciprocal
+// space (replaces cufftExecR2C / PME_BCFQ / cufftExecC2R, SPONGE/PME_force/PME_force.cu:741-747).
+//
+// Three kernels per convolution, each touching the grid once (the grids are L2-resident):
+//   k_plane_fwd   one block per x-plane: reads the int64 fixed-point charge grid (and clears it
+//                 for the next step), real-to-complex along z (length K2 via a K2/2 complex FFT,
+//                 decimation in time, digit-reversed load), then forward along y (decimation in
+//                 frequency, digit-reversed store) -> half spectrum C[x][ky][kz], kz <= K2/2.
+//   k_xconv       one block per (ky, 16 kz columns): forward along x (DIT), multiply by
+//                 BC(kx,ky,kz) and accumulate the FP64 reciprocal energy, inverse along x (DIF).
+//   k_plane_inv   one block per x-plane: inverse along y (DIT), complex-to-real along z (DIF)
+//                 -> real potential grid theta[x][y][z].
+// Mixed radix 2/3/4/5/7. DIT with stage radices r1..rS applied to digit-reversed input and DIF
+// with the mirrored order both use one permutation table per axis, so no pass needs a second
+// buffer or an explicit transpose. All transforms are unnormalised, as cuFFT's are.
+
+#include <stdio.h>
+
+#include <cmath>
+#include <vector>
+
+#include "sb_internal.cuh"
+
+struct FftAxisDev {
+    int n;
+    int nrad;
+    int rad[SB_FFT_MAX_STAGES];
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 tw_at(const float2* tw, int e, bool inv) {
+    float2 w = tw[e];
+    return inv ? conjf2(w) : w;
+}
+
+// in-register R-point DFT: y[q] <- sum_j y[j] W_R^{jq}, W_R = e^{-+2 pi i / R}
+template <int R>
+__device__ __forceinline__ void dft_r(float2* y, const float2* tw, int n, bool inv) {
+    if (R == 2) {
+        float2 a = y[0], b = y[1];
+        y[0] = cadd(a, b);
+        y[1] = csub(a, b);
+    } else if (R == 4) {
+        float2 a = y[0], b = y[1], c = y[2], d = y[3];
+        float2 s0 = cadd(a, c), s1 = csub(a, c), s2 = cadd(b, d), s3 = csub(b, d);
+        // -i * s3 (forward) / +i * s3 (inverse)
+        float2 js3 = inv ? make_float2(-s3.y, s3.x) : make_float2(s3.y, -s3.x);
+        y[0] = cadd(s0, s2);
+        y[2] = csub(s0, s2);
+        y[1] = cadd(s1, js3);
+        y[3] = csub(s1, js3);
+    } else if (R == 3) {
+        const float c = -0.5f, s0 = inv ? -0.86602540378443865f : 0.86602540378443865f;
+        float2 a = y[0], b = y[1], d = y[2];
+        float2 t1 = cadd(b, d), t2 = csub(b, d);
+        float2 m = make_float2(a.x + c * t1.x, a.y + c * t1.y);
+        // -i s0 t2
+        float2 st = make_float2(s0 * t2.y, -s0 * t2.x);
+        y[0] = cadd(a, t1);
+        y[1] = cadd(m, st);
+        y[2] = csub(m, st);
+    } else {
+        float2 x[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) x[j] = y[j];
+        const int st = n / R;
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            float2 acc = x[0];
+#pragma unroll
+            for (int j = 1; j < R; j++) acc = cadd(acc, cmul(x[j], tw_at(tw, ((j * q) % R) * st, inv)));
+            y[q] = acc;
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void dit_stage(float2* buf, int nl, int ls, int es, int n, int m,
+                                          const float2* tw, bool inv) {
+    const int L = m * R;
+    const int step = n / L;
+    const int nb = n / R;
+    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
+        const int l = t / nb, b = t - l * nb;
+        const int blk = b / m, k = b - blk * m;
+        float2* p = buf + l * ls + (blk * L + k) * es;
+        float2 y[R];
+        y[0] = p[0];
+#pragma unroll
+        for (int j = 1; j < R; j++) y[j] = cmul(p[j * m * es], tw_at(tw, j * k * step, inv));
+        dft_r<R>(y, tw, n, inv);
+#pragma unroll
+        for (int q = 0; q < R; q++) p[q * m * es] = y[q];
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void dif_stage(float2* buf, int nl, int ls, int es, int n, int Lb,
+                                          const float2* tw, bool inv) {
+    const int m = Lb / R;
+    const int step = n / Lb;
+    const int nb = n / R;
+    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
+        const int l = t / nb, b = t - l * nb;
+        const int blk = b / m, n1 = b - blk * m;
+        float2* p = buf + l * ls + (blk * Lb + n1) * es;
+        float2 y[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) y[j] = p[j * m * es];
+        dft_r<R>(y, tw, n, inv);
+        p[0] = y[0];
+#pragma unroll
+        for (int q = 1; q < R; q++) p[q * m * es] = cmul(y[q], tw_at(tw, n1 * q * step, inv));
+    }
+}
+
+// in-place transforms of nl lines (line l at buf + l*ls, element stride es)
+__device__ void fft_dit(float2* buf, int nl, int ls, int es, const FftAxisDev& A,
+                        const float2* tw, bool inv) {
+    int m = 1;
+    for (int s = 0; s < A.nrad; s++) {
+        const int r = A.rad[s];
+        switch (r) {
+            case 2: dit_stage<2>(buf, nl, ls, es, A.n, m, tw, inv); break;
+            case 3: dit_stage<3>(buf, nl, ls, es, A.n, m, tw, inv); break;
+            case 4: dit_stage<4>(buf, nl, ls, es, A.n, m, tw, inv); break;
+            case 5: dit_stage<5>(buf, nl, ls, es, A.n, m, tw, inv); break;
+            default: dit_stage<7>(buf, nl, ls, es, A.n, m, tw, inv); break;
+        }
+        m *= r;
+        __syncthreads();
+    }
+}
+
+__device__ void fft_dif(float2* buf, int nl, int ls, int es, const FftAxisDev& A,
+                        const float2* tw, bool inv) {
+    int Lb = A.n;
+    for (int s = A.nrad - 1; s >= 0; s--) {
+        const int r = A.rad[s];
+        switch (r) {
+            case 2: dif_stage<2>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
+            case 3: dif_stage<3>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
+            case 4: dif_stage<4>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
+            case 5: dif_stage<5>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
+            default: dif_stage<7>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
+        }
+        Lb /= r;
+        __syncthreads();
+    }
+}
+
+// shared-memory table layout helper: [perm_a int[na]][perm_b int[nb]][tw_a f2[na]][tw_b f2[nb]][post f2[M]]
+struct SmemTables {
+    int* perm_a;
+    int* perm_b;
+    float2* tw_a;
+    float2* tw_b;
+    float2* post;
+    float2* data;
+};
+
+__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__device__ SmemTables carve(char* sm, int na, int nb, int npost) {
+    SmemTables T;
+    size_t o = 0;
+    T.perm_a = (int*)(sm + o); o = align16(o + sizeof(int) * na);
+    T.perm_b = (int*)(sm + o); o = align16(o + sizeof(int) * nb);
+    T.tw_a = (float2*)(sm + o); o = align16(o + sizeof(float2) * na);
+    T.tw_b = (float2*)(sm + o); o = align16(o + sizeof(float2) * nb);
+    T.post = (float2*)(sm + o); o = align16(o + sizeof(float2) * npost);
+    T.data = (float2*)(sm + o);
+    return T;
+}
+
+static size_t carve_bytes(int na, int nb, int npost) {
+    auto a16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    size_t o = 0;
+    o = a16(o + sizeof(int) * na);
+    o = a16(o + sizeof(int) * nb);
+    o = a16(o + sizeof(float2) * na);
+    o = a16(o + sizeof(float2) * nb);
+    o = a16(o + sizeof(float2) * npost);
+    return o;
+}
+
+__device__ void load_tables(SmemTables& T, const int* pa, const int* pb, const float2* ta,
+                            const float2* tb, const float2* post, int na, int nb, int npost) {
+    for (int t = threadIdx.x; t < na; t += blockDim.x) {
+        T.perm_a[t] = pa[t];
+        T.tw_a[t] = ta[t];
+    }
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        T.perm_b[t] = pb[t];
+        T.tw_b[t] = tb[t];
+    }
+    for (int t = threadIdx.x; t < npost; t += blockDim.x) T.post[t] = post[t];
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------------
+// forward plane pass: z (real, via M = K2/2 complex) then y; A = z axis (length M), B = y axis
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_plane_fwd(FftAxisDev Az, FftAxisDev Ay,
+                                                   const int* __restrict__ pz,
+                                                   const int* __restrict__ py,
+                                                   const float2* __restrict__ twz,
+                                                   const float2* __restrict__ twy,
+                                                   const float2* __restrict__ post,
+                                                   long long* __restrict__ qfix,
+                                                   float2* __restrict__ spec, int K1, int K2) {
+    extern __shared__ __align__(16) char sm[];
+    const int M = K2 / 2, H = M + 1;
+    SmemTables T = carve(sm, M, K1, M);
+    load_tables(T, pz, py, twz, twy, post, M, K1, M);
+    float2* D = T.data;  // [K1][H]
+    const int x = blockIdx.x;
+    long long* q = qfix + (size_t)x * K1 * K2;
+    // digit-reversed load of z = x_even + i x_odd, clearing the charge grid behind us
+    for (int t = threadIdx.x; t < K1 * M; t += blockDim.x) {
+        const int y = t / M, p = t - y * M;
+        const int nn = T.perm_a[p];
+        long long* g = q + (size_t)y * K2 + 2 * nn;
+        const long long a = g[0], b = g[1];
+        g[0] = 0;
+        g[1] = 0;
+        D[y * H + p] = make_float2((float)a * SB_GRID_UNSCALE, (float)b * SB_GRID_UNSCALE);
+    }
+    __syncthreads();
+    fft_dit(D, K1, H, 1, Az, T.tw_a, false);
+    // real-transform post-processing: X[k] = E[k] + W_K2^k O[k], k = 0..M
+    const int half = M / 2;
+    for (int t = threadIdx.x; t < K1 * (half + 1); t += blockDim.x) {
+        const int y = t / (half + 1), k = t - y * (half + 1);
+        float2* row = D + y * H;
+        if (k == 0) {
+            const float2 z0 = row[0];
+            row[0] = make_float2(z0.x + z0.y, 0.f);
+            row[M] = make_float2(z0.x - z0.y, 0.f);
+        } else {
+            const int k2 = M - k;
+            const float2 a = row[k], b = row[k2];
+            // E[k] = (Z[k] + conj Z[M-k]) / 2, O[k] = (Z[k] - conj Z[M-k]) / 2i
+            const float2 Ek = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+            const float2 Ok = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
+            const float2 Xk = cadd(Ek, cmul(T.post[k], Ok));
+            if (k2 != k) {
+                // E[M-k] = conj E[k], O[M-k] = conj O[k]; W^{M-k} = -conj(W^k)
+                const float2 w2 = make_float2(-T.post[k].x, T.post[k].y);
+                const float2 Xk2 = cadd(conjf2(Ek), cmul(w2, conjf2(Ok)));
+                row[k2] = Xk2;
+            }
+            row[k] = Xk;
+        }
+    }
+    __syncthreads();
+    // forward along y for every kz column, natural in -> digit-reversed out
+    fft_dif(D, H, 1, H, Ay, T.tw_b, false);
+    float2* out = spec + (size_t)x * K1 * H;
+    for (int t = threadIdx.x; t < K1 * H; t += blockDim.x) {
+        const int p = t / H, kz = t - p * H;
+        out[(size_t)T.perm_b[p] * H + kz] = D[p * H + kz];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// x pass with the convolution: forward x (DIT), * BC, energy, inverse x (DIF)
+// ---------------------------------------------------------------------------------------------
+#define SB_XCONV_T 16
+__global__ void __launch_bounds__(256) k_xconv(FftAxisDev Ax, const int* __restrict__ px,
+                                               const float2* __restrict__ twx,
+                                               float2* __restrict__ spec,
+                                               const float* __restrict__ bc,
+                                               double* __restrict__ epart, int K0, int K1,
+                                               int H, int K2) {
+    extern __shared__ __align__(16) char sm[];
+    SmemTables T = carve(sm, K0, 0, 0);
+    load_tables(T, px, px, twx, twx, twx, K0, 0, 0);
+    float2* D = T.data;  // [K0][SB_XCONV_T]
+    const int y = blockIdx.x;
+    const int kz0 = blockIdx.y * SB_XCONV_T;
+    const int nt = min(SB_XCONV_T, H - kz0);
+    const size_t pstride = (size_t)K1 * H;
+    for (int t = threadIdx.x; t < K0 * SB_XCONV_T; t += blockDim.x) {
+        const int p = t / SB_XCONV_T, c = t - p * SB_XCONV_T;
+        float2 v = make_float2(0.f, 0.f);
+        if (c < nt) v = spec[(size_t)T.perm_a[p] * pstride + (size_t)y * H + kz0 + c];
+        D[p * SB_XCONV_T + c] = v;
+    }
+    __syncthreads();
+    fft_dit(D, SB_XCONV_T, 1, SB_XCONV_T, Ax, T.tw_a, false);
+    double e = 0.0;
+    for (int t = threadIdx.x; t < K0 * SB_XCONV_T; t += blockDim.x) {
+        const int kx = t / SB_XCONV_T, c = t - kx * SB_XCONV_T;
+        if (c < nt) {
+            const int kz = kz0 + c;
+            const float g = bc[((size_t)kx * K1 + y) * H + kz];
+            float2 v = D[t];
+            if (epart) {
+                const double w = (kz == 0 || 2 * kz == K2) ? 1.0 : 2.0;
+                e += w * (double)g * ((double)v.x * v.x + (double)v.y * v.y);
+            }
+            D[t] = make_float2(v.x * g, v.y * g);
+        }
+    }
+    __syncthreads();
+    fft_dif(D, SB_XCONV_T, 1, SB_XCONV_T, Ax, T.tw_a, true);
+    for (int t = threadIdx.x; t < K0 * SB_XCONV_T; t += blockDim.x) {
+        const int p = t / SB_XCONV_T, c = t - p * SB_XCONV_T;
+        if (c < nt) spec[(size_t)T.perm_a[p] * pstride + (size_t)y * H + kz0 + c] = D[t];
+    }
+    if (epart) {
+        // deterministic block reduction (fixed tree)
+        __shared__ double red[256];
+        red[threadIdx.x] = e;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) epart[blockIdx.y * gridDim.x + blockIdx.x] = 0.5 * red[0];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// inverse plane pass: y inverse (DIT) then z complex-to-real (DIF)
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_plane_inv(FftAxisDev Az, FftAxisDev Ay,
+                                                   const int* __restrict__ pz,
+                                                   const int* __restrict__ py,
+                                                   const float2* __restrict__ twz,
+                                                   const float2* __restrict__ twy,
+                                                   const float2* __restrict__ post,
+                                                   const float2* __restrict__ spec,
+                                                   float* __restrict__ real, int K1, int K2) {
+    extern __shared__ __align__(16) char sm[];
+    const int M = K2 / 2, H = M + 1;
+    SmemTables T = carve(sm, M, K1, M);
+    load_tables(T, pz, py, twz, twy, post, M, K1, M);
+    float2* D = T.data;
+    const int x = blockIdx.x;
+    const float2* in = spec + (size_t)x * K1 * H;
+    for (int t = threadIdx.x; t < K1 * H; t += blockDim.x) {
+        const int p = t / H, kz = t - p * H;
+        D[p * H + kz] = in[(size_t)T.perm_b[p] * H + kz];
+    }
+    __syncthreads();
+    fft_dit(D, H, 1, H, Ay, T.tw_b, true);
+    // C2R pre-processing: Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_K2^{-k}
+    const int half = M / 2;
+    for (int t = threadIdx.x; t < K1 * (half + 1); t += blockDim.x) {
+        const int y = t / (half + 1), k = t - y * (half + 1);
+        float2* row = D + y * H;
+        const int k2 = M - k;
+        const float2 a = row[k], b = row[k2];  // k = 0 pairs X[0] with X[M]
+        const float2 wk = conjf2(T.post[k]);   // W^{-k}
+        const float2 E = cadd(a, conjf2(b));
+        const float2 O = cmul(csub(a, conjf2(b)), wk);
+        const float2 Zk = make_float2(E.x - O.y, E.y + O.x);  // E + i O
+        if (k != 0 && k2 != k) {
+            // Z[M-k] from X[M-k], X[k]: W^{-(M-k)} = -conj(W^{-k}) ... computed directly
+            const float2 w2 = make_float2(-wk.x, wk.y);
+            const float2 E2 = cadd(b, conjf2(a));
+            const float2 O2 = cmul(csub(b, conjf2(a)), w2);
+            row[k2] = make_float2(E2.x - O2.y, E2.y + O2.x);
+        }
+        row[k] = Zk;
+    }
+    __syncthreads();
+    fft_dif(D, K1, H, 1, Az, T.tw_a, true);
+    float* out = real + (size_t)x * K1 * K2;
+    for (int t = threadIdx.x; t < K1 * M; t += blockDim.x) {
+        const int y = t / M, p = t - y * M;
+        const float2 v = D[y * H + p];
+        const int nn = T.perm_a[p];
+        out[(size_t)y * K2 + 2 * nn] = v.x;
+        out[(size_t)y * K2 + 2 * nn + 1] = v.y;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host: plans
+// ---------------------------------------------------------------------------------------------
+static int axis_radices(int n, int* rad) {
+    int k = 0;
+    const int pr[5] = {4, 2, 3, 5, 7};
+    for (int p : pr)
+        while (n % p == 0) {
+            if (k >= SB_FFT_MAX_STAGES) return -1;
+            rad[k++] = p;
+            n /= p;
+        }
+    return n == 1 ? k : -1;
+}
+
+static int axis_create(SbFftAxis* a, int n) {
+    a->n = n;
+    a->nrad = axis_radices(n, a->rad);
+    if (a->nrad < 0) {
+        sb_set_error("FFT length %d is not 2^a 3^b 5^c 7^d", n);
+        return SB_ERR_ARG;
+    }
+    std::vector<int> perm(n);
+    std::vector<int> L(a->nrad + 1, 1);
+    for (int s = 0; s < a->nrad; s++) L[s + 1] = L[s] * a->rad[s];
+    for (int p = 0; p < n; p++) {
+        int q = p, src = 0, mul = 1;
+        std::vector<int> d(a->nrad);
+        for (int s = a->nrad - 1; s >= 0; s--) {
+            d[s] = q / L[s];
+            q %= L[s];
+        }
+        for (int s = a->nrad - 1; s >= 0; s--) {
+            src += d[s] * mul;
+            mul *= a->rad[s];
+        }
+        perm[p] = src;
+    }
+    std::vector<float2> tw(n);
+    for (int t = 0; t < n; t++) {
+        double ang = -2.0 * M_PI * (double)t / n;
+        tw[t] = make_float2((float)cos(ang), (float)sin(ang));
+    }
+    SB_TRY(sb_malloc((void**)&a->d_perm, sizeof(int) * n, "fft perm"));
+    SB_TRY(sb_malloc((void**)&a->d_tw, sizeof(float2) * n, "fft twiddles"));
+    SB_CHECK_CUDA(cudaMemcpy(a->d_perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    SB_CHECK_CUDA(cudaMemcpy(a->d_tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+    return SB_OK;
+}
+
+static FftAxisDev axis_dev(const SbFftAxis& a) {
+    FftAxisDev d;
+    d.n = a.n;
+    d.nrad = a.nrad;
+    for (int i = 0; i < SB_FFT_MAX_STAGES; i++) d.rad[i] = a.rad[i];
+    return d;
+}
+
+int sb_fft_plan_create(SbFftPlan* p, const int K[3]) {
+    for (int d = 0; d < 3; d++) p->K[d] = K[d];
+    if (K[2] % 2 != 0 || K[2] < 4 || K[0] < 2 || K[1] < 2) {
+        sb_set_error("PME grid %dx%dx%d: fftz must be even and every size >= 2", K[0], K[1], K[2]);
+        return SB_ERR_ARG;
+    }
+    p->H = K[2] / 2 + 1;
+    SB_TRY(axis_create(&p->z, K[2] / 2));
+    SB_TRY(axis_create(&p->y, K[1]));
+    SB_TRY(axis_create(&p->x, K[0]));
+    const int M = K[2] / 2;
+    std::vector<float2> post(M);
+    for (int k = 0; k < M; k++) {
+        double ang = -2.0 * M_PI * (double)k / K[2];
+        post[k] = make_float2((float)cos(ang), (float)sin(ang));
+    }
+    SB_TRY(sb_malloc((void**)&p->d_post, sizeof(float2) * M, "fft post twiddles"));
+    SB_CHECK_CUDA(cudaMemcpy(p->d_post, post.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+    p->plane_smem = carve_bytes(M, K[1], M) + sizeof(float2) * (size_t)K[1] * p->H;
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (optin <= 0) optin = 227 * 1024;
+    if (p->plane_smem > (size_t)optin) {
+        sb_set_error("PME grid plane %dx%d needs %zu B of shared memory (> %d)", K[1], K[2],
+                     p->plane_smem, optin);
+        return SB_ERR_ARG;
+    }
+    cudaFuncSetAttribute(k_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)p->plane_smem);
+    cudaFuncSetAttribute(k_plane_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)p->plane_smem);
+    size_t xs = carve_bytes(K[0], 0, 0) + sizeof(float2) * (size_t)K[0] * SB_XCONV_T;
+    if (xs > 48 * 1024)
+        cudaFuncSetAttribute(k_xconv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xs);
+    return SB_OK;
+}
+
+void sb_fft_plan_destroy(SbFftPlan* p) {
+    SbFftAxis* ax[3] = {&p->z, &p->y, &p->x};
+    for (SbFftAxis* a : ax) {
+        sb_free(a->d_perm);
+        sb_free(a->d_tw);
+        a->d_perm = nullptr;
+        a->d_tw = nullptr;
+    }
+    sb_free(p->d_post);
+    p->d_post = nullptr;
+}
+
+int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, cudaStream_t s) {
+    k_plane_fwd<<<p->K[0], 512, p->plane_smem, s>>>(axis_dev(p->z), axis_dev(p->y), p->z.d_perm,
+                                                    p->y.d_perm, p->z.d_tw, p->y.d_tw, p->d_post,
+                                                    d_qfix, d_spec, p->K[1], p->K[2]);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+int sb_fft_xconv_parts(const SbFftPlan* p) {
+    return p->K[1] * ((p->H + SB_XCONV_T - 1) / SB_XCONV_T);
+}
+
+int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
+                      int want_energy, cudaStream_t s, int* nparts_out) {
+    dim3 grid(p->K[1], (p->H + SB_XCONV_T - 1) / SB_XCONV_T);
+    size_t xs = carve_bytes(p->K[0], 0, 0) + sizeof(float2) * (size_t)p->K[0] * SB_XCONV_T;
+    k_xconv<<<grid, 256, xs, s>>>(axis_dev(p->x), p->x.d_perm, p->x.d_tw, d_spec, d_bc,
+                                  want_energy ? d_epart : nullptr, p->K[0], p->K[1], p->H,
+                                  p->K[2]);
+    SB_CHECK_LAUNCH();
+    if (nparts_out) *nparts_out = grid.x * grid.y;
+    return SB_OK;
+}
+
+int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real,
+                         cudaStream_t s) {
+    k_plane_inv<<<p->K[0], 512, p->plane_smem, s>>>(axis_dev(p->z), axis_dev(p->y), p->z.d_perm,
+                                                    p->y.d_perm, p->z.d_tw, p->y.d_tw, p->d_post,
+                                                    d_spec, d_real, p->K[1], p->K[2]);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}

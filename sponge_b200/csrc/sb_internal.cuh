@@ -1,0 +1,205 @@
+// Internal definitions shared by the sponge_b200 CUDA sources (sm_100a).
+//
+// Data layout in HBM (chosen form):
+//   * original atom order (caller-owned): uint_crd[3N] u32, charge[N] f32, frc[3N] f32
+//   * cell-sorted "slots": atoms are bucketed into xy columns (~ (8/rho)^(1/3) wide), sorted
+//     by (z, atom id) inside each column, and every column is padded to a multiple of 8 slots.
+//     Slot s holds atom slot_atom[s] (-1 for padding). 8 consecutive slots form a cluster.
+//   * per-call packed SoA in slot order: xq[s] = {ux, uy, uz, float_bits(q)} (uint4, one
+//     128-bit load) and stype[s] (int)
+//   * cluster pair list: for cluster c, cl_count[c] entries at cl_ent[c*ent_cap ...]; entry =
+//     (slot j) | (mask << 24), mask bit k set iff pair (slot 8c+k, j) is in the half list
+//     (slot j > slot 8c+k, not excluded, FP32 distance^2 < (rc+skin)^2)
+//   * fixed-point accumulators: int64 fx/fy/fz per slot, 2^-32 kcal/mol/A per unit
+//   * PME: int64 charge grid [K0][K1][K2] (2^-40 e*18.2223 per unit), complex half spectrum
+//     [K0][K1][K2/2+1] float2, real potential grid [K0][K1][K2] float
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/sponge_b200.h"
+
+#define SB_FORCE_SCALE 4294967296.0f          // 2^32 units per kcal/mol/A
+#define SB_FORCE_UNSCALE (1.0 / 4294967296.0)  // double
+#define SB_GRID_SCALE 1099511627776.0f        // 2^40 units per charge unit on the PME grid
+#define SB_GRID_UNSCALE (1.0f / 1099511627776.0f)
+
+#define SB_CLUSTER 8
+#define SB_MAX_SLOTS (1 << 24)  // slot index must fit 24 bits of a list entry
+#define SB_COLUMN_SORT_CAP 4096 // max atoms per sort column (bitonic sort in shared memory)
+#define SB_MAX_RADIX 8
+#define SB_FFT_MAX_STAGES 12
+
+// ---------------------------------------------------------------------------------------------
+// error handling
+// ---------------------------------------------------------------------------------------------
+void sb_set_error(const char* fmt, ...);
+
+#define SB_CHECK_CUDA(call)                                                              \
+    do {                                                                                 \
+        cudaError_t _e = (call);                                                         \
+        if (_e != cudaSuccess) {                                                         \
+            sb_set_error("%s failed at %s:%d: %s", #call, __FILE__, __LINE__,            \
+                         cudaGetErrorString(_e));                                        \
+            return SB_ERR_CUDA;                                                          \
+        }                                                                                \
+    } while (0)
+
+#define SB_CHECK_LAUNCH()                                                                \
+    do {                                                                                 \
+        cudaError_t _e = cudaGetLastError();                                             \
+        if (_e != cudaSuccess) {                                                         \
+            sb_set_error("kernel launch failed at %s:%d: %s", __FILE__, __LINE__,        \
+                         cudaGetErrorString(_e));                                        \
+            return SB_ERR_CUDA;                                                          \
+        }                                                                                \
+    } while (0)
+
+#define SB_TRY(expr)                  \
+    do {                              \
+        int _s = (expr);              \
+        if (_s != SB_OK) return _s;   \
+    } while (0)
+
+int sb_malloc(void** p, size_t bytes, const char* what);
+void sb_free(void* p);
+
+// ---------------------------------------------------------------------------------------------
+// FFT plan (hand-written mixed-radix shared-memory FFT)
+// ---------------------------------------------------------------------------------------------
+struct SbFftAxis {
+    int n = 0;
+    int nrad = 0;
+    int rad[SB_FFT_MAX_STAGES] = {0};
+    int* d_perm = nullptr;     // DIT input position p holds element perm[p]; DIF output likewise
+    float2* d_tw = nullptr;    // e^{-2 pi i t / n}, t < n (FP64-computed)
+};
+
+struct SbFftPlan {
+    int K[3] = {0, 0, 0};
+    int H = 0;                 // K2/2 + 1
+    SbFftAxis z;               // complex length K2/2 (real transform along z via the half trick)
+    SbFftAxis y;               // length K1
+    SbFftAxis x;               // length K0
+    float2* d_post = nullptr;  // e^{-2 pi i k / K2}, k < K2/2 (real-transform twiddles)
+    size_t plane_smem = 0;     // bytes of the plane kernels' dynamic shared memory
+};
+
+int sb_fft_plan_create(SbFftPlan* p, const int K[3]);
+void sb_fft_plan_destroy(SbFftPlan* p);
+
+// forward plane pass: int64 charge grid -> half spectrum (z R2C + y forward); clears the grid
+int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, cudaStream_t s);
+// x pass: forward x, multiply by the Green's function table, energy partials, inverse x
+int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
+                      int want_energy, cudaStream_t s, int* nparts_out);
+// inverse plane pass: half spectrum -> real grid (y inverse + z C2R)
+int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real,
+                         cudaStream_t s);
+int sb_fft_xconv_parts(const SbFftPlan* p);
+
+// ---------------------------------------------------------------------------------------------
+// module structs
+// ---------------------------------------------------------------------------------------------
+struct sb_neighbor_list {
+    int n = 0;
+    float box[3];
+    float cutoff = 10.f, skin = 2.f, cs = 12.f, cs2 = 144.f;
+    int refresh_interval = 0, refresh_count = 0;
+    float skin_permit = 1.f;        // internal value (2x the mdin value, neighbor_list.cu:718)
+    float half_skin_square = 1.f;
+    int form = SB_FORM_FIXED;
+    int max_neighbor_numbers = 800;
+    // column grid
+    int ncx = 1, ncy = 1, ncol = 1;
+    int nxr = 1, nyr = 1;
+    int slot_cap = 0;               // n + 8*ncol
+    int clu_cap = 0;                // slot_cap / 8
+    int ent_cap = 0;                // entries per cluster
+    // device buffers
+    float* old_crd = nullptr;       // VECTOR[N]
+    uint32_t* ucrd = nullptr;       // UNSIGNED_INT_VECTOR[N] of the last rebuild
+    int* col_of = nullptr;          // [N]
+    int* col_rank = nullptr;        // [N]
+    int* col_count = nullptr;       // [ncol] real atoms
+    int* col_start = nullptr;       // [ncol+1] padded slot starts
+    unsigned long long* sort_tmp = nullptr;  // [slot_cap] (z << 32 | atom) scatter buffer
+    int* slot_atom = nullptr;       // [slot_cap]
+    int* atom_slot = nullptr;       // [N]
+    uint32_t* slot_u = nullptr;     // [3*slot_cap] fixed-point coordinates at build, slot order
+    int* excl_lo = nullptr;         // [N] min / max exclusion partner (INT_MAX / -1 if none)
+    int* excl_hi = nullptr;
+    int* cl_count = nullptr;        // [clu_cap]
+    uint32_t* cl_ent = nullptr;     // [clu_cap * ent_cap]
+    int* meta = nullptr;            // [0] clusters, [1] status flags, [2] refresh flag,
+                                    // [3] padded slots, [4..5] pair count (int64)
+    // per force call packed data
+    uint4* xq = nullptr;            // [slot_cap]
+    int* stype = nullptr;           // [slot_cap]
+    long long* fix = nullptr;       // [3*slot_cap] x,y,z planes
+    // ATOM_GROUP compatibility export
+    void* ag = nullptr;             // ATOM_GROUP[N]
+    int* ag_serial = nullptr;       // [N * max_neighbor_numbers]
+    int ag_valid = 0;
+    int built = 0;
+    int needs_rebuild = 0;
+    unsigned long long build_id = 0;
+};
+
+struct sb_lennard_jones {
+    int n = 0;
+    int ntypes = 0;
+    int form = SB_FORM_FIXED;
+    float cutoff = 10.f;
+    float box[3];
+    float volume = 1.f;
+    double long_range_factor = 0;
+    float* d_A = nullptr;           // lower-triangular x12
+    float* d_B = nullptr;           // lower-triangular x6
+    float2* d_AB = nullptr;         // full square [ntypes*ntypes] {A12, B6}
+    int* d_type = nullptr;          // [N]
+    double* d_red = nullptr;        // FP64 reduction scratch
+    float* d_energy_atom = nullptr; // [N] scratch for Get_Energy
+};
+
+struct sb_pme {
+    int n = 0;
+    int form = SB_FORM_FIXED;
+    float box[3];
+    float cutoff = 10.f, tolerance = 1e-5f;
+    float beta = 0.f;
+    int K[3];
+    size_t G = 0;                   // K0*K1*K2
+    size_t Gh = 0;                  // K0*K1*(K2/2+1)
+    double neutralizing_factor = 0; // -pi/(2 beta^2 V)
+    SbFftPlan plan;
+    long long* d_qfix = nullptr;    // int64 charge grid (chosen form), kept zero between calls
+    float* d_qf = nullptr;          // float charge grid (plain form)
+    float2* d_spec = nullptr;       // half spectrum
+    float* d_theta = nullptr;       // real convolved grid
+    float* d_bc = nullptr;          // [K0][K1][H] Green's function x B-spline moduli (FP64-built)
+    double* d_epart = nullptr;      // per-block reciprocal energy partials
+    int nparts = 0;
+    double* d_ered = nullptr;       // [8] FP64 energy slots: rec, self, direct, corr
+    float* d_direct_atom_energy = nullptr;
+    float* d_correction_atom_energy = nullptr;
+    long long* d_fix = nullptr;     // [3N] exclusion-correction accumulator (original order)
+    void* cufft_r2c = nullptr;      // plain form: cuFFT handles (stored as int)
+    void* cufft_c2r = nullptr;
+    int cufft_ok = 0;
+};
+
+// kernels/launchers shared across files
+int sb_nl_ensure_built(sb_neighbor_list* nl);
+int sb_nl_pack(sb_neighbor_list* nl, const uint32_t* d_uint_crd, const float* d_charge,
+               const int* d_type, cudaStream_t s);
+int sb_nl_finalize_forces(sb_neighbor_list* nl, float* d_frc, cudaStream_t s);
+int sb_nl_build_atom_group(sb_neighbor_list* nl, cudaStream_t s);
+
+// FP64 reduction helpers (deterministic: fixed block/thread order)
+int sb_reduce_sum_f32(const float* d_x, int n, double* d_out, cudaStream_t s);
+
+static inline cudaStream_t sb_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }

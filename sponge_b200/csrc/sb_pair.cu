@@ -1,0 +1,585 @@
+// LJ + PME direct-space pair force/energy/virial — replaces LENNARD_JONES_INFORMATION
+// (SPONGE/Lennard_Jones_force/Lennard_Jones_force.cu).
+//
+// Chosen form (k_pair_fixed): one warp per 8-atom i-cluster. Each lane takes one list entry
+// (a j atom plus an 8-bit mask of the i atoms it pairs with), loads j with one 128-bit load,
+// and loops over the 8 i atoms held in registers. Positions are taken relative to the
+// cluster's first atom: the fixed-point difference is exact, its float conversion is done once
+// per j instead of once per pair, and close pairs keep full relative precision. The j force is
+// complete after the 8-i loop and goes out as three 64-bit fixed-point atomics; the i forces
+// stay in registers for the whole list and are reduced across the warp once. Fixed-point sums
+// are order independent, so forces are bit-identical run to run.
+//
+// Pair math (Lennard_Jones_force.cu:83-139): for dr = r_j - r_i and r < rc,
+//   F_i += [ (B6 - A12 r^-6) r^-8  -  qq (erfc(br) + 2br/sqrt(pi) e^{-b^2r^2}) r^-3 ] dr
+// with the Coulomb bracket evaluated as qq (r^-3 - b^3 G(b^2 r^2)) (sb_ewald.cuh).
+// Energies (:508-513): A12/12 r^-12 - B6/6 r^-6 + qq erfc(br)/r; LJ virial -(LJ scalar) r^2.
+//
+// Plain form (k_pair_plain): the reference's structure on the per-atom ATOM_GROUP list — one
+// warp per atom i, lanes striding over its j list, float atomicAdd on every j, erfcf/expf.
+
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "sb_ewald.cuh"
+#include "sb_internal.cuh"
+
+struct SbAtomGroupP {
+    int atom_numbers;
+    int* atom_serial;
+};
+
+struct PairParams {
+    float sx, sy, sz;
+    float rc2, rc;
+    float beta, beta2, beta3;
+    int nt;
+    int slot_cap;
+    int ent_cap;
+};
+
+#define SB_EV_ENERGY 1
+#define SB_EV_VIRIAL 2
+
+__device__ __forceinline__ void red_fix(long long* p, float v) {
+    long long q = __float2ll_rn(v * SB_FORCE_SCALE);
+    if (q) atomicAdd((unsigned long long*)p, (unsigned long long)q);
+}
+
+template <int EV>
+__global__ void __launch_bounds__(128) k_pair_fixed(
+    PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
+    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
+    const int* __restrict__ stype, const float2* __restrict__ AB,
+    const int* __restrict__ slot_atom, long long* __restrict__ fix,
+    float* __restrict__ atom_energy, float* __restrict__ atom_virial,
+    float* __restrict__ atom_direct) {
+    extern __shared__ float2 sAB[];
+    const int ntt = P.nt * P.nt;
+    for (int t = threadIdx.x; t < ntt; t += blockDim.x) sAB[t] = AB[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= meta[0]) return;
+    const int base = c * SB_CLUSTER;
+
+    const uint4 my = lane < SB_CLUSTER ? xq[base + lane] : make_uint4(0, 0, 0, 0);
+    const int myt = lane < SB_CLUSTER ? stype[base + lane] : 0;
+    const uint32_t rx = __shfl_sync(0xffffffffu, my.x, 0);
+    const uint32_t ry = __shfl_sync(0xffffffffu, my.y, 0);
+    const uint32_t rz = __shfl_sync(0xffffffffu, my.z, 0);
+    const float mxr = __int2float_rn((int)(my.x - rx)) * P.sx;
+    const float myr = __int2float_rn((int)(my.y - ry)) * P.sy;
+    const float mzr = __int2float_rn((int)(my.z - rz)) * P.sz;
+
+    float xi[SB_CLUSTER], yi[SB_CLUSTER], zi[SB_CLUSTER], qi[SB_CLUSTER];
+    int ti[SB_CLUSTER];
+    float fxi[SB_CLUSTER], fyi[SB_CLUSTER], fzi[SB_CLUSTER];
+    float ei[SB_CLUSTER], vi[SB_CLUSTER], di[SB_CLUSTER];
+#pragma unroll
+    for (int k = 0; k < SB_CLUSTER; k++) {
+        xi[k] = __shfl_sync(0xffffffffu, mxr, k);
+        yi[k] = __shfl_sync(0xffffffffu, myr, k);
+        zi[k] = __shfl_sync(0xffffffffu, mzr, k);
+        qi[k] = __uint_as_float(__shfl_sync(0xffffffffu, my.w, k));
+        ti[k] = __shfl_sync(0xffffffffu, myt, k) * P.nt;
+        fxi[k] = fyi[k] = fzi[k] = 0.f;
+        if (EV) ei[k] = vi[k] = di[k] = 0.f;
+    }
+
+    const int cnt = cl_count[c];
+    const uint32_t* __restrict__ ents = cl_ent + (size_t)c * P.ent_cap;
+    for (int e = lane; e < cnt; e += 32) {
+        const uint32_t v = ents[e];
+        const int j = (int)(v & 0xffffffu);
+        const uint32_t m = v >> 24;
+        const uint4 xj = xq[j];
+        const int tj = stype[j];
+        const float xjr = __int2float_rn((int)(xj.x - rx)) * P.sx;
+        const float yjr = __int2float_rn((int)(xj.y - ry)) * P.sy;
+        const float zjr = __int2float_rn((int)(xj.z - rz)) * P.sz;
+        const float qj = __uint_as_float(xj.w);
+        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+#pragma unroll
+        for (int k = 0; k < SB_CLUSTER; k++) {
+            const float dx = xjr - xi[k];
+            const float dy = yjr - yi[k];
+            const float dz = zjr - zi[k];
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (((m >> k) & 1u) && r2 < P.rc2) {
+                const float ri = rsqrtf(r2);
+                const float ri2 = ri * ri;
+                const float ri6 = ri2 * ri2 * ri2;
+                const float2 ab = sAB[ti[k] + tj];
+                const float flj = (ab.y - ab.x * ri6) * ri6 * ri2;
+                const float qq = qi[k] * qj;
+                const float z = P.beta2 * r2;
+                const float G = sb_ewald_G(z);
+                const float fc = qq * (ri * ri2 - P.beta3 * G);
+                const float fs = flj - fc;
+                const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
+                fxi[k] += tx;
+                fyi[k] += ty;
+                fzi[k] += tz;
+                fjx -= tx;
+                fjy -= ty;
+                fjz -= tz;
+                if (EV & SB_EV_ENERGY) {
+                    const float ec = qq * erfcf(P.beta * r2 * ri) * ri;
+                    ei[k] += (0.083333333f * ab.x * ri6 - 0.166666667f * ab.y) * ri6 + ec;
+                    di[k] += ec;
+                }
+                if (EV & SB_EV_VIRIAL) {
+                    vi[k] -= flj * r2;
+                    if (!(EV & SB_EV_ENERGY)) di[k] += qq * erfcf(P.beta * r2 * ri) * ri;
+                }
+            }
+        }
+        red_fix(&fix[j], fjx);
+        red_fix(&fix[P.slot_cap + j], fjy);
+        red_fix(&fix[2 * P.slot_cap + j], fjz);
+    }
+    // warp reduction of the i forces: lane k ends with cluster atom k's totals
+#pragma unroll
+    for (int k = 0; k < SB_CLUSTER; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            fxi[k] += __shfl_xor_sync(0xffffffffu, fxi[k], o);
+            fyi[k] += __shfl_xor_sync(0xffffffffu, fyi[k], o);
+            fzi[k] += __shfl_xor_sync(0xffffffffu, fzi[k], o);
+            if (EV) {
+                ei[k] += __shfl_xor_sync(0xffffffffu, ei[k], o);
+                vi[k] += __shfl_xor_sync(0xffffffffu, vi[k], o);
+                di[k] += __shfl_xor_sync(0xffffffffu, di[k], o);
+            }
+        }
+    }
+    float ox = 0.f, oy = 0.f, oz = 0.f, oe = 0.f, ov = 0.f, od = 0.f;
+#pragma unroll
+    for (int k = 0; k < SB_CLUSTER; k++)
+        if (lane == k) {
+            ox = fxi[k];
+            oy = fyi[k];
+            oz = fzi[k];
+            if (EV) {
+                oe = ei[k];
+                ov = vi[k];
+                od = di[k];
+            }
+        }
+    if (lane < SB_CLUSTER) {
+        const int s = base + lane;
+        const int a = slot_atom[s];
+        if (a >= 0) {
+            red_fix(&fix[s], ox);
+            red_fix(&fix[P.slot_cap + s], oy);
+            red_fix(&fix[2 * P.slot_cap + s], oz);
+            if (EV & SB_EV_ENERGY) atom_energy[a] += oe;
+            if (EV & SB_EV_VIRIAL) {
+                atom_virial[a] += ov;
+                atom_direct[a] = od;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// plain form: reference structure (warp per atom, float atomics), Lennard_Jones_force.cu:47-158
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ int lj_pair_index(int a, int b) {
+    int M = max(a, b), m = min(a, b);
+    return (M * (M + 1) >> 1) + m;
+}
+
+template <int EV>
+__global__ void __launch_bounds__(1024) k_pair_plain(
+    int n, const SbAtomGroupP* __restrict__ nl, const uint32_t* __restrict__ uc,
+    const float* __restrict__ q, const int* __restrict__ type, const float* __restrict__ A,
+    const float* __restrict__ B, float sx, float sy, float sz, float cutoff, float beta,
+    float* __restrict__ frc, float* __restrict__ atom_energy, float* __restrict__ atom_virial,
+    float* __restrict__ atom_direct) {
+    const int i = blockIdx.x * blockDim.y + threadIdx.y;
+    if (i >= n) return;
+    const SbAtomGroupP g = nl[i];
+    const uint32_t ux = uc[3 * i], uy = uc[3 * i + 1], uz = uc[3 * i + 2];
+    const float qi = q[i];
+    const int ti = type[i];
+    float fx = 0.f, fy = 0.f, fz = 0.f, el = 0.f, ed = 0.f, vr = 0.f;
+    for (int t = threadIdx.x; t < g.atom_numbers; t += blockDim.x) {
+        const int j = g.atom_serial[t];
+        const float dx = (float)(int)(uc[3 * j] - ux) * sx;
+        const float dy = (float)(int)(uc[3 * j + 1] - uy) * sy;
+        const float dz = (float)(int)(uc[3 * j + 2] - uz) * sz;
+        const float r = norm3df(dx, dy, dz);
+        if (r < cutoff) {
+            const float ri = 1.0f / r;
+            const float ri2 = ri * ri;
+            const float ri4 = ri2 * ri2;
+            const float ri6 = ri4 * ri2;
+            const float ri8 = ri4 * ri4;
+            const int k = lj_pair_index(ti, type[j]);
+            const float a = A[k], b = B[k];
+            float fs = (-a * ri6 + b) * ri8;
+            const float br = beta * r;
+            const float ec = erfcf(br);
+            const float qq = qi * q[j];
+            const float fc = qq * (br * 1.1283791670218446f * expf(-br * br) + ec) * ri2 * ri;
+            if (EV & SB_EV_ENERGY) {
+                ed += qq * ec * ri;
+                el += (0.083333333f * a * ri6 - 0.166666666f * b) * ri6;
+            }
+            if (EV & SB_EV_VIRIAL) {
+                vr -= fs * r * r;
+                if (!(EV & SB_EV_ENERGY)) ed += qq * ec * ri;
+            }
+            fs -= fc;
+            const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
+            fx += tx;
+            fy += ty;
+            fz += tz;
+            atomicAdd(&frc[3 * j], -tx);
+            atomicAdd(&frc[3 * j + 1], -ty);
+            atomicAdd(&frc[3 * j + 2], -tz);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        fx += __shfl_down_sync(0xffffffffu, fx, o);
+        fy += __shfl_down_sync(0xffffffffu, fy, o);
+        fz += __shfl_down_sync(0xffffffffu, fz, o);
+        if (EV) {
+            el += __shfl_down_sync(0xffffffffu, el, o);
+            ed += __shfl_down_sync(0xffffffffu, ed, o);
+            vr += __shfl_down_sync(0xffffffffu, vr, o);
+        }
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&frc[3 * i], fx);
+        atomicAdd(&frc[3 * i + 1], fy);
+        atomicAdd(&frc[3 * i + 2], fz);
+        if (EV & SB_EV_ENERGY) atom_energy[i] += el + ed;
+        if (EV & SB_EV_VIRIAL) {
+            atom_virial[i] += vr;
+            atom_direct[i] = ed;
+        }
+    }
+}
+
+// LJ energy only (LJ_Energy_CUDA, Lennard_Jones_force.cu:964-1025) over the cluster list
+__global__ void __launch_bounds__(128) k_lj_energy_fixed(
+    PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
+    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
+    const int* __restrict__ stype, const float2* __restrict__ AB,
+    const int* __restrict__ slot_atom, float* __restrict__ atom_energy) {
+    const int lane = threadIdx.x & 31;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= meta[0]) return;
+    const int base = c * SB_CLUSTER;
+    const uint32_t* __restrict__ ents = cl_ent + (size_t)c * P.ent_cap;
+    const int cnt = cl_count[c];
+    for (int k = 0; k < SB_CLUSTER; k++) {
+        const uint4 xi = xq[base + k];
+        const int ti = stype[base + k] * P.nt;
+        float e = 0.f;
+        for (int t = lane; t < cnt; t += 32) {
+            const uint32_t v = ents[t];
+            if (!((v >> (24 + k)) & 1u)) continue;
+            const int j = (int)(v & 0xffffffu);
+            const uint4 xj = xq[j];
+            const float dx = __int2float_rn((int)(xj.x - xi.x)) * P.sx;
+            const float dy = __int2float_rn((int)(xj.y - xi.y)) * P.sy;
+            const float dz = __int2float_rn((int)(xj.z - xi.z)) * P.sz;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (r2 < P.rc2) {
+                const float ri2 = 1.0f / r2;
+                const float ri6 = ri2 * ri2 * ri2;
+                const float2 ab = AB[ti + stype[j]];
+                e += (0.083333333f * ab.x * ri6 - 0.166666667f * ab.y) * ri6;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        if (lane == 0) {
+            const int a = slot_atom[base + k];
+            if (a >= 0) atom_energy[a] += e;
+        }
+    }
+}
+
+__global__ void k_device_add(float* p, float v) { p[0] += v; }
+
+__global__ void k_zero_f32(int n, float* p) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = 0.f;
+}
+
+// ---------------------------------------------------------------------------------------------
+// host API
+// ---------------------------------------------------------------------------------------------
+extern "C" int sb_lj_create(int atom_numbers, int atom_type_numbers, const float* h_A,
+                            const float* h_B, const int* h_type, float cutoff,
+                            const float box_length[3], int form, sb_lennard_jones** out) {
+    if (!out || atom_numbers <= 0 || atom_type_numbers <= 0 || !h_A || !h_B || !h_type ||
+        !box_length || cutoff <= 0) {
+        sb_set_error("sb_lj_create: invalid argument");
+        return SB_ERR_ARG;
+    }
+    const int nt = atom_type_numbers;
+    for (int i = 0; i < atom_numbers; i++)
+        if (h_type[i] < 0 || h_type[i] >= nt) {
+            sb_set_error("sb_lj_create: atom %d has LJ type %d outside [0, %d)", i, h_type[i], nt);
+            return SB_ERR_ARG;
+        }
+    sb_lennard_jones* lj = new sb_lennard_jones();
+    lj->n = atom_numbers;
+    lj->ntypes = nt;
+    lj->form = form;
+    lj->cutoff = cutoff;
+    for (int d = 0; d < 3; d++) lj->box[d] = box_length[d];
+    lj->volume = box_length[0] * box_length[1] * box_length[2];
+    const int np = nt * (nt + 1) / 2;
+    std::vector<float2> ab((size_t)nt * nt);
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++) {
+            int M = std::max(a, b), m = std::min(a, b);
+            int k = M * (M + 1) / 2 + m;
+            ab[(size_t)a * nt + b] = make_float2(h_A[k], h_B[k]);
+        }
+    // long-range correction factor, FP64 over type counts (Lennard_Jones_force.cu:1119-1130)
+    std::vector<double> cnt(nt, 0.0);
+    for (int i = 0; i < atom_numbers; i++) cnt[h_type[i]] += 1.0;
+    double sumB = 0;
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++) sumB += cnt[a] * cnt[b] * (double)ab[(size_t)a * nt + b].y;
+    lj->long_range_factor = sumB * (-2.0 / 3.0 * M_PI / ((double)cutoff * cutoff * cutoff) / 6.0);
+    int st = SB_OK;
+    if ((st = sb_malloc((void**)&lj->d_A, sizeof(float) * np, "LJ_A")) ||
+        (st = sb_malloc((void**)&lj->d_B, sizeof(float) * np, "LJ_B")) ||
+        (st = sb_malloc((void**)&lj->d_AB, sizeof(float2) * nt * nt, "LJ_AB")) ||
+        (st = sb_malloc((void**)&lj->d_type, sizeof(int) * atom_numbers, "LJ type")) ||
+        (st = sb_malloc((void**)&lj->d_red, sizeof(double) * 8, "LJ reduce")) ||
+        (st = sb_malloc((void**)&lj->d_energy_atom, sizeof(float) * atom_numbers, "LJ energy"))) {
+        sb_lj_destroy(lj);
+        return st;
+    }
+    cudaMemcpy(lj->d_A, h_A, sizeof(float) * np, cudaMemcpyHostToDevice);
+    cudaMemcpy(lj->d_B, h_B, sizeof(float) * np, cudaMemcpyHostToDevice);
+    cudaMemcpy(lj->d_AB, ab.data(), sizeof(float2) * nt * nt, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(lj->d_type, h_type, sizeof(int) * atom_numbers,
+                               cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        sb_set_error("sb_lj_create: %s", cudaGetErrorString(e));
+        sb_lj_destroy(lj);
+        return SB_ERR_CUDA;
+    }
+    *out = lj;
+    return SB_OK;
+}
+
+extern "C" int sb_lj_destroy(sb_lennard_jones* lj) {
+    if (!lj) return SB_OK;
+    sb_free(lj->d_A);
+    sb_free(lj->d_B);
+    sb_free(lj->d_AB);
+    sb_free(lj->d_type);
+    sb_free(lj->d_red);
+    sb_free(lj->d_energy_atom);
+    delete lj;
+    return SB_OK;
+}
+
+static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list* nl,
+                              float beta) {
+    PairParams P;
+    P.sx = (1.0f / 4294967296.0f) * nl->box[0];
+    P.sy = (1.0f / 4294967296.0f) * nl->box[1];
+    P.sz = (1.0f / 4294967296.0f) * nl->box[2];
+    P.rc = lj->cutoff;
+    P.rc2 = lj->cutoff * lj->cutoff;
+    P.beta = beta;
+    P.beta2 = beta * beta;
+    P.beta3 = beta * beta * beta;
+    P.nt = lj->ntypes;
+    P.slot_cap = nl->slot_cap;
+    P.ent_cap = nl->ent_cap;
+    return P;
+}
+
+static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float beta, int ev,
+                             float* ae, float* av, float* ad, cudaStream_t s) {
+    PairParams P = pair_params(lj, nl, beta);
+    const int warps = 4;
+    const int blocks = (nl->clu_cap + warps - 1) / warps;
+    const size_t smem = sizeof(float2) * lj->ntypes * lj->ntypes;
+    if (smem > 96 * 1024) {
+        sb_set_error("LJ type table too large for shared memory (%d types)", lj->ntypes);
+        return SB_ERR_ARG;
+    }
+#define SB_LAUNCH_PAIR(EVV)                                                                   \
+    do {                                                                                      \
+        if (smem > 48 * 1024)                                                                 \
+            cudaFuncSetAttribute(k_pair_fixed<EVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)smem);                                                  \
+        k_pair_fixed<EVV><<<blocks, 32 * warps, smem, s>>>(P, nl->meta, nl->cl_count,          \
+                                                          nl->cl_ent, nl->xq, nl->stype,      \
+                                                          lj->d_AB, nl->slot_atom, nl->fix,   \
+                                                          ae, av, ad);                        \
+    } while (0)
+    switch (ev) {
+        case 0: SB_LAUNCH_PAIR(0); break;
+        case 1: SB_LAUNCH_PAIR(1); break;
+        case 2: SB_LAUNCH_PAIR(2); break;
+        default: SB_LAUNCH_PAIR(3); break;
+    }
+#undef SB_LAUNCH_PAIR
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+static int launch_pair_plain(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* uc,
+                             const float* q, float* frc, float beta, int ev, float* ae,
+                             float* av, float* ad, cudaStream_t s) {
+    SB_TRY(sb_nl_build_atom_group(nl, s));
+    const float sx = (1.0f / 4294967296.0f) * nl->box[0];
+    const float sy = (1.0f / 4294967296.0f) * nl->box[1];
+    const float sz = (1.0f / 4294967296.0f) * nl->box[2];
+    dim3 thr(32, 32);
+    dim3 grid((lj->n + 31) / 32);
+    const SbAtomGroupP* g = (const SbAtomGroupP*)nl->ag;
+    switch (ev) {
+        case 0:
+            k_pair_plain<0><<<grid, thr, 0, s>>>(lj->n, g, uc, q, lj->d_type, lj->d_A, lj->d_B,
+                                                 sx, sy, sz, lj->cutoff, beta, frc, ae, av, ad);
+            break;
+        case 1:
+            k_pair_plain<1><<<grid, thr, 0, s>>>(lj->n, g, uc, q, lj->d_type, lj->d_A, lj->d_B,
+                                                 sx, sy, sz, lj->cutoff, beta, frc, ae, av, ad);
+            break;
+        case 2:
+            k_pair_plain<2><<<grid, thr, 0, s>>>(lj->n, g, uc, q, lj->d_type, lj->d_A, lj->d_B,
+                                                 sx, sy, sz, lj->cutoff, beta, frc, ae, av, ad);
+            break;
+        default:
+            k_pair_plain<3><<<grid, thr, 0, s>>>(lj->n, g, uc, q, lj->d_type, lj->d_A, lj->d_B,
+                                                 sx, sy, sz, lj->cutoff, beta, frc, ae, av, ad);
+            break;
+    }
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+extern "C" int sb_lj_pme_direct_force(sb_lennard_jones* lj, sb_neighbor_list* nl,
+                                      int atom_numbers, const uint32_t* d_uint_crd,
+                                      const float* d_charge, float* d_frc, float pme_beta,
+                                      int need_atom_energy, float* d_atom_energy,
+                                      int need_virial, float* d_atom_lj_virial,
+                                      float* d_atom_direct_pme_energy, void* stream) {
+    if (!lj || !nl || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_lj_pme_direct_force: null argument");
+        return SB_ERR_ARG;
+    }
+    if (atom_numbers != lj->n || nl->n != lj->n) {
+        sb_set_error("sb_lj_pme_direct_force: atom count %d does not match the modules (%d, %d)",
+                     atom_numbers, lj->n, nl->n);
+        return SB_ERR_ARG;
+    }
+    if ((need_atom_energy > 0 && !d_atom_energy) ||
+        (need_virial > 0 && (!d_atom_lj_virial || !d_atom_direct_pme_energy))) {
+        sb_set_error("sb_lj_pme_direct_force: energy/virial output missing");
+        return SB_ERR_ARG;
+    }
+    SB_TRY(sb_nl_ensure_built(nl));
+    cudaStream_t s = sb_stream(stream);
+    const int ev = (need_atom_energy > 0 ? SB_EV_ENERGY : 0) | (need_virial > 0 ? SB_EV_VIRIAL : 0);
+    if (lj->form == SB_FORM_PLAIN) {
+        if (ev & SB_EV_VIRIAL) {
+            int tb = 1024;
+            k_zero_f32<<<(lj->n + tb - 1) / tb, tb, 0, s>>>(lj->n, d_atom_direct_pme_energy);
+            SB_CHECK_LAUNCH();
+        }
+        return launch_pair_plain(lj, nl, d_uint_crd, d_charge, d_frc, pme_beta, ev,
+                                 d_atom_energy, d_atom_lj_virial, d_atom_direct_pme_energy, s);
+    }
+    SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
+    SB_TRY(launch_pair_fixed(lj, nl, pme_beta, ev, d_atom_energy, d_atom_lj_virial,
+                             d_atom_direct_pme_energy, s));
+    SB_TRY(sb_nl_finalize_forces(nl, d_frc, s));
+    return SB_OK;
+}
+
+extern "C" int sb_lj_long_range_correction(sb_lennard_jones* lj, int need_pressure,
+                                           float* d_virial, int need_potential,
+                                           float* d_potential, void* stream) {
+    if (!lj) {
+        sb_set_error("sb_lj_long_range_correction: null handle");
+        return SB_ERR_ARG;
+    }
+    cudaStream_t s = sb_stream(stream);
+    const double V = (double)lj->box[0] * lj->box[1] * lj->box[2];
+    if (need_pressure > 0) {
+        if (!d_virial) {
+            sb_set_error("sb_lj_long_range_correction: d_virial is NULL");
+            return SB_ERR_ARG;
+        }
+        k_device_add<<<1, 1, 0, s>>>(d_virial, (float)(lj->long_range_factor * 6.0 / V));
+        SB_CHECK_LAUNCH();
+    }
+    if (need_potential > 0) {
+        if (!d_potential) {
+            sb_set_error("sb_lj_long_range_correction: d_potential is NULL");
+            return SB_ERR_ARG;
+        }
+        k_device_add<<<1, 1, 0, s>>>(d_potential, (float)(lj->long_range_factor / V));
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_lj_get_energy(sb_lennard_jones* lj, sb_neighbor_list* nl,
+                                const uint32_t* d_uint_crd, float* h_energy, void* stream) {
+    if (!lj || !nl || !d_uint_crd) {
+        sb_set_error("sb_lj_get_energy: null argument");
+        return SB_ERR_ARG;
+    }
+    SB_TRY(sb_nl_ensure_built(nl));
+    cudaStream_t s = sb_stream(stream);
+    int tb = 1024;
+    k_zero_f32<<<(lj->n + tb - 1) / tb, tb, 0, s>>>(lj->n, lj->d_energy_atom);
+    SB_CHECK_LAUNCH();
+    // charges are irrelevant for the LJ energy; pack with the type table only
+    SB_TRY(sb_nl_pack(nl, d_uint_crd, nullptr, lj->d_type, s));
+    PairParams P = pair_params(lj, nl, 0.f);
+    const int warps = 4;
+    k_lj_energy_fixed<<<(nl->clu_cap + warps - 1) / warps, 32 * warps, 0, s>>>(
+        P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB, nl->slot_atom,
+        lj->d_energy_atom);
+    SB_CHECK_LAUNCH();
+    SB_TRY(sb_reduce_sum_f32(lj->d_energy_atom, lj->n, lj->d_red, s));
+    double e = 0;
+    SB_CHECK_CUDA(cudaMemcpyAsync(&e, lj->d_red, sizeof(double), cudaMemcpyDeviceToHost, s));
+    SB_CHECK_CUDA(cudaStreamSynchronize(s));
+    const double V = (double)lj->box[0] * lj->box[1] * lj->box[2];
+    e += lj->long_range_factor / V;
+    if (h_energy) *h_energy = (float)e;
+    return SB_OK;
+}
+
+extern "C" int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[3]) {
+    if (!lj || !box_length) {
+        sb_set_error("sb_lj_update_volume: null argument");
+        return SB_ERR_ARG;
+    }
+    for (int d = 0; d < 3; d++) lj->box[d] = box_length[d];
+    lj->volume = box_length[0] * box_length[1] * box_length[2];
+    return SB_OK;
+}
+
+extern "C" int sb_lj_long_range_factor(sb_lennard_jones* lj, float* h_factor) {
+    if (!lj || !h_factor) {
+        sb_set_error("sb_lj_long_range_factor: null argument");
+        return SB_ERR_ARG;
+    }
+    *h_factor = (float)lj->long_range_factor;
+    return SB_OK;
+}

@@ -1,0 +1,713 @@
+// PME reciprocal space and the Ewald exclusion correction — replaces Particle_Mesh_Ewald
+// (SPONGE/PME_force/PME_force.cu).
+//
+// Grid convention (PME_force.cu:367-421): u = uint * K / 2^32, base = floor(u), fr = u - base;
+// grid point (base - k) mod K receives weight w_k(fr), k = 0..3, with the 4th-order cardinal
+// B-spline polynomials of PME_force.cu:8-14. Here base and fr come from an exact 64-bit
+// integer product instead of the reference's FP32 product, so the stencil never flips at a
+// rounding boundary.
+//
+// Chosen form: spread with int64 fixed-point atomics (order independent), the hand-written
+// FFT + convolution of sb_fft.cu, gather with one thread per atom (one writer per atom).
+// Plain form: float atomicAdd spread into a float grid, cuFFT R2C/C2R with a separate BC
+// multiply, same gather.
+// Energies (PME_force.cu:753-771) are reduced in FP64 in fixed order.
+
+#include <cufft.h>
+#include <stdio.h>
+
+#include <cmath>
+#include <vector>
+
+#include "sb_ewald.cuh"
+#include "sb_internal.cuh"
+
+__device__ __forceinline__ void grid_coord(uint32_t u, int K, int& base, float& fr) {
+    const unsigned long long p = (unsigned long long)u * (unsigned)K;
+    base = (int)(p >> 32);
+    fr = (float)(uint32_t)(p & 0xffffffffull) * 2.3283064365386963e-10f;
+}
+
+__device__ __forceinline__ void bspline4(float f, float w[4]) {
+    const float f2 = f * f, f3 = f2 * f;
+    w[0] = f3 * (1.0f / 6.0f);
+    w[1] = -0.5f * f3 + 0.5f * f2 + 0.5f * f + (1.0f / 6.0f);
+    w[2] = 0.5f * f3 - f2 + (2.0f / 3.0f);
+    w[3] = -f3 * (1.0f / 6.0f) + 0.5f * f2 - 0.5f * f + (1.0f / 6.0f);
+}
+
+__device__ __forceinline__ void bspline4d(float f, float d[4]) {
+    const float f2 = f * f;
+    d[0] = 0.5f * f2;
+    d[1] = -1.5f * f2 + f + 0.5f;
+    d[2] = 1.5f * f2 - 2.0f * f;
+    d[3] = -0.5f * f2 + f - 0.5f;
+}
+
+// 4 threads per atom; thread t handles x-offset t and the 16 (y, z) points
+template <bool FIXED>
+__global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __restrict__ q,
+                         int K0, int K1, int K2, long long* __restrict__ gfix,
+                         float* __restrict__ gf) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gt >> 2, kx = gt & 3;
+    if (i >= n) return;
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(uc[3 * i], K0, b0, f0);
+    grid_coord(uc[3 * i + 1], K1, b1, f1);
+    grid_coord(uc[3 * i + 2], K2, b2, f2);
+    float wx[4], wy[4], wz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    const float qw = q[i] * wx[kx];
+    int gx = b0 - kx;
+    if (gx < 0) gx += K0;
+    const size_t rowx = (size_t)gx * K1;
+#pragma unroll
+    for (int ky = 0; ky < 4; ky++) {
+        int gy = b1 - ky;
+        if (gy < 0) gy += K1;
+        const size_t row = (rowx + gy) * K2;
+        const float qwy = qw * wy[ky];
+#pragma unroll
+        for (int kz = 0; kz < 4; kz++) {
+            int gz = b2 - kz;
+            if (gz < 0) gz += K2;
+            const float v = qwy * wz[kz];
+            if (FIXED) {
+                const long long f = __float2ll_rn(v * SB_GRID_SCALE);
+                if (f) atomicAdd((unsigned long long*)&gfix[row + gz], (unsigned long long)f);
+            } else {
+                atomicAdd(&gf[row + gz], v);
+            }
+        }
+    }
+}
+
+// force interpolation (PME_Final, PME_force.cu:485-550); one thread per atom, one writer
+__global__ void k_gather(int n, const uint32_t* __restrict__ uc, const float* __restrict__ q,
+                         const float* __restrict__ theta, int K0, int K1, int K2, float ix,
+                         float iy, float iz, float* __restrict__ frc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(uc[3 * i], K0, b0, f0);
+    grid_coord(uc[3 * i + 1], K1, b1, f1);
+    grid_coord(uc[3 * i + 2], K2, b2, f2);
+    float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    bspline4d(f0, dx);
+    bspline4d(f1, dy);
+    bspline4d(f2, dz);
+    int gz[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int g = b2 - k;
+        gz[k] = g < 0 ? g + K2 : g;
+    }
+    float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+#pragma unroll
+    for (int kx = 0; kx < 4; kx++) {
+        int gx = b0 - kx;
+        if (gx < 0) gx += K0;
+#pragma unroll
+        for (int ky = 0; ky < 4; ky++) {
+            int gy = b1 - ky;
+            if (gy < 0) gy += K1;
+            const float* row = theta + ((size_t)gx * K1 + gy) * K2;
+            float sw = 0.f, sd = 0.f;
+#pragma unroll
+            for (int kz = 0; kz < 4; kz++) {
+                const float t = row[gz[kz]];
+                sw = fmaf(t, wz[kz], sw);
+                sd = fmaf(t, dz[kz], sd);
+            }
+            Fx = fmaf(dx[kx] * wy[ky], sw, Fx);
+            Fy = fmaf(wx[kx] * dy[ky], sw, Fy);
+            Fz = fmaf(wx[kx] * wy[ky], sd, Fz);
+        }
+    }
+    const float s = -q[i];
+    frc[3 * i] += s * Fx * ix;
+    frc[3 * i + 1] += s * Fy * iy;
+    frc[3 * i + 2] += s * Fz * iz;
+}
+
+// plain form: FQ *= BC on the cuFFT half spectrum (PME_BCFQ, PME_force.cu:473-483)
+__global__ void k_bcfq(size_t nh, float2* __restrict__ fq, const float* __restrict__ bc) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nh) {
+        const float g = bc[i];
+        float2 v = fq[i];
+        fq[i] = make_float2(v.x * g, v.y * g);
+    }
+}
+
+// plain form energy: 1/2 sum Q * theta over the real grid (PME_Energy_Product, :553-566)
+__global__ void k_grid_dot(size_t G, const float* __restrict__ a, const float* __restrict__ b,
+                           double* __restrict__ part) {
+    __shared__ double red[256];
+    double s = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < G;
+         i += (size_t)gridDim.x * blockDim.x)
+        s += (double)a[i] * (double)b[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = 0.5 * red[0];
+}
+
+// exclusion correction (PME_Excluded_Force_With_Atom_Energy_Correction, PME_force.cu:620-695)
+template <bool FIXED>
+__global__ void k_excluded(int n, const uint32_t* __restrict__ uc, float sx, float sy, float sz,
+                           const float* __restrict__ q, float beta, float beta2, float beta3,
+                           const int* __restrict__ es, const int* __restrict__ el,
+                           const int* __restrict__ en, long long* __restrict__ fix,
+                           float* __restrict__ frc, float* __restrict__ ene) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int cnt = en[i];
+    if (cnt <= 0) return;
+    const int s0 = es[i];
+    const uint32_t ux = uc[3 * i], uy = uc[3 * i + 1], uz = uc[3 * i + 2];
+    const float qi = q[i];
+    float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f;
+    for (int k = s0; k < s0 + cnt; k++) {
+        const int j = el[k];
+        const float dx = __int2float_rn((int)(uc[3 * j] - ux)) * sx;
+        const float dy = __int2float_rn((int)(uc[3 * j + 1] - uy)) * sy;
+        const float dz = __int2float_rn((int)(uc[3 * j + 2] - uz)) * sz;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float r = sqrtf(r2);
+        const float qq = qi * q[j];
+        float fs;
+        if (FIXED) {
+            fs = qq * beta3 * sb_ewald_G(beta2 * r2);
+        } else {
+            const float br = beta * r;
+            float t = br * 1.1283791670218446f * expf(-br * br) + erfcf(br);
+            fs = -qq * (t - 1.0f) / r2 / r;
+        }
+        const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
+        fx += tx;
+        fy += ty;
+        fz += tz;
+        e -= qq * erff(beta * r) / r;
+        if (FIXED) {
+            atomicAdd((unsigned long long*)&fix[3 * j], (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
+            atomicAdd((unsigned long long*)&fix[3 * j + 1], (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
+            atomicAdd((unsigned long long*)&fix[3 * j + 2], (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
+        } else {
+            atomicAdd(&frc[3 * j], -tx);
+            atomicAdd(&frc[3 * j + 1], -ty);
+            atomicAdd(&frc[3 * j + 2], -tz);
+        }
+    }
+    if (FIXED) {
+        atomicAdd((unsigned long long*)&fix[3 * i], (unsigned long long)__float2ll_rn(fx * SB_FORCE_SCALE));
+        atomicAdd((unsigned long long*)&fix[3 * i + 1], (unsigned long long)__float2ll_rn(fy * SB_FORCE_SCALE));
+        atomicAdd((unsigned long long*)&fix[3 * i + 2], (unsigned long long)__float2ll_rn(fz * SB_FORCE_SCALE));
+    } else {
+        atomicAdd(&frc[3 * i], fx);
+        atomicAdd(&frc[3 * i + 1], fy);
+        atomicAdd(&frc[3 * i + 2], fz);
+    }
+    if (ene) atomicAdd(&ene[i], e);
+}
+
+__global__ void k_fix_to_frc(int n, long long* __restrict__ fix, float* __restrict__ frc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * n) return;
+    const long long v = fix[t];
+    if (v) {
+        fix[t] = 0;
+        frc[t] += (float)((double)v * SB_FORCE_UNSCALE);
+    }
+}
+
+__global__ void k_zero_f(int n, float* p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = 0.f;
+}
+
+// FP64 fixed-order block reduction helper
+__device__ double block_sum(double v, double* red) {
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// ered: [0] reciprocal, [1] self (+neutralising), [2] direct, [3] correction
+__global__ void __launch_bounds__(1024) k_pme_energy_finish(
+    int n, const float* __restrict__ q, const double* __restrict__ epart, int nparts,
+    const float* __restrict__ direct, const float* __restrict__ corr, double beta,
+    double neutral, double* __restrict__ ered, int need_virial, int need_energy,
+    float* __restrict__ d_virial, float* __restrict__ d_potential) {
+    __shared__ double red[1024];
+    double a = 0, b = 0, c = 0, d = 0, e = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double qi = q[i];
+        a += qi * qi;
+        b += qi;
+        if (direct) c += direct[i];
+        if (corr) d += corr[i];
+    }
+    for (int p = threadIdx.x; p < nparts; p += blockDim.x) e += epart[p];
+    const double s2 = block_sum(a, red);
+    const double s1 = block_sum(b, red);
+    const double sd = block_sum(c, red);
+    const double sc = block_sum(d, red);
+    const double er = block_sum(e, red);
+    if (threadIdx.x == 0) {
+        const double self = -beta / sqrt(M_PI) * s2 + neutral * s1 * s1;
+        ered[0] = er;
+        ered[1] = self;
+        ered[2] = sd;
+        ered[3] = sc;
+        if (need_energy && d_potential) d_potential[0] += (float)(sc + self + er);
+        if (need_virial && d_virial) d_virial[0] += (float)(sd + sc + self + er);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------------------------
+static int check_2357(int number) {
+    const int primes[4] = {2, 3, 5, 7};
+    for (int p : primes) {
+        while (number > 0) {
+            if (number == 1) return 1;
+            int t = number / p;
+            if (t * p != number) break;
+            number = t;
+        }
+    }
+    return number == 1;
+}
+
+// Get_Fft_Patameter (SPONGE/common.cu:513-534)
+static int fft_size(float length) {
+    int t = ((int)ceil(length + 3.0f)) >> 2 << 2;
+    if (t >= 60 && t <= 68) t = 64;
+    else if (t >= 120 && t <= 136) t = 128;
+    else if (t >= 240 && t <= 272) t = 256;
+    else if (t >= 480 && t <= 544) t = 512;
+    else if (t >= 960 && t <= 1088) t = 1024;
+    while (!check_2357(t)) t += 4;
+    return t;
+}
+
+// Get_Beta (PME_force.cu:71-100) with the same float/double mix
+static float get_beta(float cutoff, float tolerance) {
+    float beta = 0, low, high, tempf;
+    int ilow, ihigh;
+    high = 1.0f;
+    ihigh = 1;
+    while (1) {
+        float hc = high * cutoff;
+        tempf = (float)(erfc((double)hc) / (double)cutoff);
+        if (tempf <= tolerance) break;
+        high *= 2;
+        ihigh++;
+    }
+    ihigh += 50;
+    low = 0.0f;
+    for (ilow = 1; ilow < ihigh; ilow++) {
+        beta = (low + high) / 2;
+        float bc = beta * cutoff;
+        tempf = (float)(erfc((double)bc) / (double)cutoff);
+        if (tempf >= tolerance)
+            low = beta;
+        else
+            high = beta;
+    }
+    return beta;
+}
+
+// FP64 B-spline moduli and Green's function table on the half spectrum (PME_force.cu:45-67,
+// :253-286): BC = B1 B2 B3 exp(-pi^2 m^2 / beta^2) / (pi m^2 V), BC(0) = 0
+static int build_bc(sb_pme* p) {
+    const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2], H = K2 / 2 + 1;
+    std::vector<double> B[3];
+    for (int d = 0; d < 3; d++) {
+        B[d].resize(p->K[d]);
+        for (int k = 0; k < p->K[d]; k++) {
+            double re = 0, im = 0;
+            const double M4[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
+            for (int j = 0; j < 3; j++) {
+                double a = 2 * M_PI * j * (double)k / p->K[d];
+                re += M4[j] * cos(a);
+                im += M4[j] * sin(a);
+            }
+            B[d][k] = 1.0 / (re * re + im * im);
+        }
+    }
+    const double Lx = p->box[0], Ly = p->box[1], Lz = p->box[2];
+    const double V = Lx * Ly * Lz;
+    const double beta = p->beta;
+    std::vector<float> bc((size_t)K0 * K1 * H);
+    for (int x = 0; x < K0; x++) {
+        const int mx = x > K0 / 2 ? K0 - x : x;
+        for (int y = 0; y < K1; y++) {
+            const int my = y > K1 / 2 ? K1 - y : y;
+            for (int z = 0; z < H; z++) {
+                const int mz = z;
+                double v = 0;
+                if (x + y + z != 0) {
+                    const double m2 = mx * mx / (Lx * Lx) + my * my / (Ly * Ly) + mz * mz / (Lz * Lz);
+                    v = B[0][x] * B[1][y] * B[2][z] * exp(-M_PI * M_PI * m2 / (beta * beta)) /
+                        (M_PI * m2 * V);
+                }
+                bc[((size_t)x * K1 + y) * H + z] = (float)v;
+            }
+        }
+    }
+    SB_CHECK_CUDA(cudaMemcpy(p->d_bc, bc.data(), sizeof(float) * bc.size(), cudaMemcpyHostToDevice));
+    p->neutralizing_factor = -0.5 * M_PI / (beta * beta * V);
+    return SB_OK;
+}
+
+extern "C" int sb_pme_create(int atom_numbers, const float box_length[3], float cutoff,
+                             float tolerance, int fftx, int ffty, int fftz, int form,
+                             sb_pme** out) {
+    if (!out || atom_numbers <= 0 || !box_length || cutoff <= 0) {
+        sb_set_error("sb_pme_create: invalid argument");
+        return SB_ERR_ARG;
+    }
+    sb_pme* p = new sb_pme();
+    p->n = atom_numbers;
+    p->form = form;
+    for (int d = 0; d < 3; d++) p->box[d] = box_length[d];
+    p->cutoff = cutoff;
+    p->tolerance = tolerance > 0 ? tolerance : 1e-5f;
+    p->K[0] = fftx > 0 ? fftx : fft_size(box_length[0]);
+    p->K[1] = ffty > 0 ? ffty : fft_size(box_length[1]);
+    p->K[2] = fftz > 0 ? fftz : fft_size(box_length[2]);
+    p->beta = get_beta(cutoff, p->tolerance);
+    p->G = (size_t)p->K[0] * p->K[1] * p->K[2];
+    p->Gh = (size_t)p->K[0] * p->K[1] * (p->K[2] / 2 + 1);
+    int st = SB_OK;
+    auto fail = [&](int s) {
+        sb_pme_destroy(p);
+        return s;
+    };
+    if (form == SB_FORM_FIXED) {
+        if ((st = sb_fft_plan_create(&p->plan, p->K))) return fail(st);
+        if ((st = sb_malloc((void**)&p->d_qfix, sizeof(long long) * p->G, "PME grid"))) return fail(st);
+        cudaMemset(p->d_qfix, 0, sizeof(long long) * p->G);
+        p->nparts = sb_fft_xconv_parts(&p->plan);
+    } else {
+        if ((st = sb_malloc((void**)&p->d_qf, sizeof(float) * p->G, "PME grid"))) return fail(st);
+        cufftHandle a, b;
+        if (cufftPlan3d(&a, p->K[0], p->K[1], p->K[2], CUFFT_R2C) != CUFFT_SUCCESS ||
+            cufftPlan3d(&b, p->K[0], p->K[1], p->K[2], CUFFT_C2R) != CUFFT_SUCCESS) {
+            sb_set_error("sb_pme_create: cuFFT plan creation failed");
+            return fail(SB_ERR_CUDA);
+        }
+        p->cufft_r2c = (void*)(intptr_t)a;
+        p->cufft_c2r = (void*)(intptr_t)b;
+        p->cufft_ok = 1;
+        p->nparts = 1184;
+    }
+    if ((st = sb_malloc((void**)&p->d_spec, sizeof(float2) * p->Gh, "PME spectrum")) ||
+        (st = sb_malloc((void**)&p->d_theta, sizeof(float) * p->G, "PME potential grid")) ||
+        (st = sb_malloc((void**)&p->d_bc, sizeof(float) * p->Gh, "PME BC")) ||
+        (st = sb_malloc((void**)&p->d_epart, sizeof(double) * std::max(p->nparts, 1), "PME parts")) ||
+        (st = sb_malloc((void**)&p->d_ered, sizeof(double) * 8, "PME energies")) ||
+        (st = sb_malloc((void**)&p->d_direct_atom_energy, sizeof(float) * atom_numbers, "direct E")) ||
+        (st = sb_malloc((void**)&p->d_correction_atom_energy, sizeof(float) * atom_numbers, "corr E")) ||
+        (st = sb_malloc((void**)&p->d_fix, sizeof(long long) * 3 * atom_numbers, "excl fix")))
+        return fail(st);
+    cudaMemset(p->d_fix, 0, sizeof(long long) * 3 * atom_numbers);
+    cudaMemset(p->d_direct_atom_energy, 0, sizeof(float) * atom_numbers);
+    cudaMemset(p->d_correction_atom_energy, 0, sizeof(float) * atom_numbers);
+    cudaMemset(p->d_ered, 0, sizeof(double) * 8);
+    if ((st = build_bc(p))) return fail(st);
+    *out = p;
+    return SB_OK;
+}
+
+extern "C" int sb_pme_destroy(sb_pme* p) {
+    if (!p) return SB_OK;
+    cudaDeviceSynchronize();
+    sb_fft_plan_destroy(&p->plan);
+    if (p->cufft_ok) {
+        cufftDestroy((cufftHandle)(intptr_t)p->cufft_r2c);
+        cufftDestroy((cufftHandle)(intptr_t)p->cufft_c2r);
+    }
+    void* ps[] = {p->d_qfix, p->d_qf, p->d_spec, p->d_theta, p->d_bc, p->d_epart, p->d_ered,
+                  p->d_direct_atom_energy, p->d_correction_atom_energy, p->d_fix};
+    for (void* x : ps) sb_free(x);
+    delete p;
+    return SB_OK;
+}
+
+extern "C" int sb_pme_info(sb_pme* p, float* h_beta, int* h_fft3) {
+    if (!p) {
+        sb_set_error("sb_pme_info: null handle");
+        return SB_ERR_ARG;
+    }
+    if (h_beta) *h_beta = p->beta;
+    if (h_fft3)
+        for (int d = 0; d < 3; d++) h_fft3[d] = p->K[d];
+    return SB_OK;
+}
+
+extern "C" int sb_pme_atom_energy_arrays(sb_pme* p, float** d_direct, float** d_corr) {
+    if (!p) {
+        sb_set_error("sb_pme_atom_energy_arrays: null handle");
+        return SB_ERR_ARG;
+    }
+    if (d_direct) *d_direct = p->d_direct_atom_energy;
+    if (d_corr) *d_corr = p->d_correction_atom_energy;
+    return SB_OK;
+}
+
+static int excluded_force(sb_pme* p, const uint32_t* uc, const float scaler[3], const float* q,
+                          const int* es, const int* el, const int* en, float* frc, float* ene,
+                          cudaStream_t s) {
+    const int n = p->n, tb = 128;
+    const float b = p->beta;
+    if (p->form == SB_FORM_FIXED) {
+        k_excluded<true><<<(n + tb - 1) / tb, tb, 0, s>>>(n, uc, scaler[0], scaler[1], scaler[2],
+                                                          q, b, b * b, b * b * b, es, el, en,
+                                                          p->d_fix, frc, ene);
+        SB_CHECK_LAUNCH();
+        k_fix_to_frc<<<(3 * n + 255) / 256, 256, 0, s>>>(n, p->d_fix, frc);
+        SB_CHECK_LAUNCH();
+    } else {
+        k_excluded<false><<<(n + tb - 1) / tb, tb, 0, s>>>(n, uc, scaler[0], scaler[1],
+                                                           scaler[2], q, b, b * b, b * b * b, es,
+                                                           el, en, p->d_fix, frc, ene);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_pme_excluded_force(sb_pme* p, const uint32_t* d_uint_crd, const float scaler[3],
+                                     const float* d_charge, const int* es, const int* el,
+                                     const int* en, float* d_frc, float* d_atom_energy,
+                                     void* stream) {
+    if (!p || !d_uint_crd || !scaler || !d_charge || !d_frc) {
+        sb_set_error("sb_pme_excluded_force: null argument");
+        return SB_ERR_ARG;
+    }
+    cudaStream_t s = sb_stream(stream);
+    // Reset_List(d_correction_atom_energy) precedes the kernel as in PME_force.cu:701
+    k_zero_f<<<(p->n + 1023) / 1024, 1024, 0, s>>>(p->n, p->d_correction_atom_energy);
+    SB_CHECK_LAUNCH();
+    if (!es || !el || !en) return SB_OK;
+    return excluded_force(p, d_uint_crd, scaler, d_charge, es, el, en, d_frc, d_atom_energy, s);
+}
+
+// returns a status; *nparts_out receives the number of reciprocal-energy partials written
+static int reciprocal(sb_pme* p, const uint32_t* uc, const float* q, float* frc, int want_e,
+                      cudaStream_t s, int* nparts_out) {
+    const int n = p->n;
+    const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
+    int nparts = 0;
+    if (p->form == SB_FORM_FIXED) {
+        k_spread<true><<<(4 * n + 255) / 256, 256, 0, s>>>(n, uc, q, K0, K1, K2, p->d_qfix, nullptr);
+        SB_CHECK_LAUNCH();
+        SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
+        SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_e, s, &nparts));
+        SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+    } else {
+        SB_CHECK_CUDA(cudaMemsetAsync(p->d_qf, 0, sizeof(float) * p->G, s));
+        k_spread<false><<<(4 * n + 255) / 256, 256, 0, s>>>(n, uc, q, K0, K1, K2, nullptr, p->d_qf);
+        SB_CHECK_LAUNCH();
+        cufftHandle a = (cufftHandle)(intptr_t)p->cufft_r2c, b = (cufftHandle)(intptr_t)p->cufft_c2r;
+        if (cufftSetStream(a, s) != CUFFT_SUCCESS || cufftSetStream(b, s) != CUFFT_SUCCESS ||
+            cufftExecR2C(a, p->d_qf, (cufftComplex*)p->d_spec) != CUFFT_SUCCESS) {
+            sb_set_error("cuFFT R2C failed");
+            return SB_ERR_CUDA;
+        }
+        k_bcfq<<<(unsigned)((p->Gh + 1023) / 1024), 1024, 0, s>>>(p->Gh, p->d_spec, p->d_bc);
+        SB_CHECK_LAUNCH();
+        if (cufftExecC2R(b, (cufftComplex*)p->d_spec, p->d_theta) != CUFFT_SUCCESS) {
+            sb_set_error("cuFFT C2R failed");
+            return SB_ERR_CUDA;
+        }
+        if (want_e) {
+            nparts = p->nparts;
+            k_grid_dot<<<nparts, 256, 0, s>>>(p->G, p->d_qf, p->d_theta, p->d_epart);
+            SB_CHECK_LAUNCH();
+        }
+    }
+    k_gather<<<(n + 127) / 128, 128, 0, s>>>(n, uc, q, p->d_theta, K0, K1, K2,
+                                             (float)K0 / p->box[0], (float)K1 / p->box[1],
+                                             (float)K2 / p->box[2], frc);
+    SB_CHECK_LAUNCH();
+    *nparts_out = nparts;
+    return SB_OK;
+}
+
+extern "C" int sb_pme_reciprocal_force(sb_pme* p, const uint32_t* d_uint_crd,
+                                       const float* d_charge, float* d_frc, int need_virial,
+                                       int need_energy, float* d_virial, float* d_potential,
+                                       void* stream) {
+    if (!p || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_pme_reciprocal_force: null argument");
+        return SB_ERR_ARG;
+    }
+    cudaStream_t s = sb_stream(stream);
+    const int want = (need_virial > 0 || need_energy > 0);
+    int nparts = 0;
+    SB_TRY(reciprocal(p, d_uint_crd, d_charge, d_frc, want, s, &nparts));
+    if (want) {
+        k_pme_energy_finish<<<1, 1024, 0, s>>>(p->n, d_charge, p->d_epart, nparts,
+                                               p->d_direct_atom_energy,
+                                               p->d_correction_atom_energy, (double)p->beta,
+                                               p->neutralizing_factor, p->d_ered, need_virial > 0,
+                                               need_energy > 0, d_virial, d_potential);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_pme_update_box(sb_pme* p, const float box_length[3]) {
+    if (!p || !box_length) {
+        sb_set_error("sb_pme_update_box: null argument");
+        return SB_ERR_ARG;
+    }
+    for (int d = 0; d < 3; d++) p->box[d] = box_length[d];
+    return build_bc(p);
+}
+
+// direct-space Coulomb energy over the list (PME_Direct_Atom_Energy, PME_force.cu:570-617)
+__global__ void k_direct_energy_list(int n, const void* __restrict__ agv,
+                                     const uint32_t* __restrict__ uc, const float* __restrict__ q,
+                                     float sx, float sy, float sz, float beta, float rc2,
+                                     float* __restrict__ out) {
+    struct AG {
+        int atom_numbers;
+        int* atom_serial;
+    };
+    const AG* ag = (const AG*)agv;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const AG g = ag[i];
+    float e = 0.f;
+    for (int t = 0; t < g.atom_numbers; t++) {
+        const int j = g.atom_serial[t];
+        const float dx = __int2float_rn((int)(uc[3 * j] - uc[3 * i])) * sx;
+        const float dy = __int2float_rn((int)(uc[3 * j + 1] - uc[3 * i + 1])) * sy;
+        const float dz = __int2float_rn((int)(uc[3 * j + 2] - uc[3 * i + 2])) * sz;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (r2 < rc2) {
+            const float r = sqrtf(r2);
+            e += q[i] * q[j] * erfcf(beta * r) / r;
+        }
+    }
+    out[i] = e;
+}
+
+extern "C" int sb_pme_get_energy(sb_pme* p, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                                 const float* d_charge, const float scaler[3], const int* es,
+                                 const int* el, const int* en, int which_part, float* h_energy,
+                                 double* h_parts, void* stream) {
+    if (!p || !d_uint_crd || !d_charge || !scaler) {
+        sb_set_error("sb_pme_get_energy: null argument");
+        return SB_ERR_ARG;
+    }
+    if (which_part < 0 || which_part > 4) {
+        sb_set_error("sb_pme_get_energy: energy part %d is not allowed", which_part);
+        return SB_ERR_ARG;
+    }
+    cudaStream_t s = sb_stream(stream);
+    const int n = p->n;
+    const int all = which_part == SB_PME_TOTAL;
+    int nparts = 0;
+    float* scratch_frc = nullptr;
+    if (all || which_part == SB_PME_RECIPROCAL) {
+        // the reciprocal energy comes with a force evaluation into a scratch array
+        SB_TRY(sb_malloc((void**)&scratch_frc, sizeof(float) * 3 * n, "energy scratch"));
+        cudaMemsetAsync(scratch_frc, 0, sizeof(float) * 3 * n, s);
+        int st = reciprocal(p, d_uint_crd, d_charge, scratch_frc, 1, s, &nparts);
+        if (st) {
+            sb_free(scratch_frc);
+            return st;
+        }
+    }
+    float* direct = nullptr;
+    float* corr = nullptr;
+    if (all || which_part == SB_PME_DIRECT) {
+        if (!nl) {
+            sb_free(scratch_frc);
+            sb_set_error("sb_pme_get_energy: the DIRECT part needs the neighbor list");
+            return SB_ERR_ARG;
+        }
+        int st = sb_nl_build_atom_group(nl, s);
+        if (st) {
+            sb_free(scratch_frc);
+            return st;
+        }
+        k_direct_energy_list<<<(n + 127) / 128, 128, 0, s>>>(n, nl->ag, d_uint_crd, d_charge,
+                                                             scaler[0], scaler[1], scaler[2],
+                                                             p->beta, p->cutoff * p->cutoff,
+                                                             p->d_direct_atom_energy);
+        direct = p->d_direct_atom_energy;
+    }
+    if (all || which_part == SB_PME_CORRECTION) {
+        k_zero_f<<<(n + 1023) / 1024, 1024, 0, s>>>(n, p->d_correction_atom_energy);
+        if (!scratch_frc) {
+            SB_TRY(sb_malloc((void**)&scratch_frc, sizeof(float) * 3 * n, "energy scratch"));
+            cudaMemsetAsync(scratch_frc, 0, sizeof(float) * 3 * n, s);
+        }
+        if (es && el && en) {
+            int st = excluded_force(p, d_uint_crd, scaler, d_charge, es, el, en, scratch_frc,
+                                    p->d_correction_atom_energy, s);
+            if (st) {
+                sb_free(scratch_frc);
+                return st;
+            }
+        }
+        corr = p->d_correction_atom_energy;
+    }
+    k_pme_energy_finish<<<1, 1024, 0, s>>>(n, d_charge, p->d_epart, nparts, direct, corr,
+                                           (double)p->beta, p->neutralizing_factor, p->d_ered, 0,
+                                           0, nullptr, nullptr);
+    cudaError_t e = cudaGetLastError();
+    double parts[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(parts, p->d_ered, sizeof(double) * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    sb_free(scratch_frc);
+    if (e != cudaSuccess) {
+        sb_set_error("sb_pme_get_energy: %s", cudaGetErrorString(e));
+        return SB_ERR_CUDA;
+    }
+    const double rec = parts[0], self = parts[1], dir = parts[2], cor = parts[3];
+    const double tot = rec + self + dir + cor;
+    double v = tot;
+    switch (which_part) {
+        case SB_PME_DIRECT: v = dir; break;
+        case SB_PME_RECIPROCAL: v = rec; break;
+        case SB_PME_CORRECTION: v = cor; break;
+        case SB_PME_SELF: v = self; break;
+        default: break;
+    }
+    if (h_energy) *h_energy = (float)v;
+    if (h_parts) {
+        h_parts[0] = tot;
+        h_parts[1] = dir;
+        h_parts[2] = rec;
+        h_parts[3] = cor;
+        h_parts[4] = self;
+    }
+    return SB_OK;
+}

@@ -1,0 +1,103 @@
+"""NonbondedEngine: the three modules wired together the way SPONGE's MD driver calls them.
+
+Main_Calculate_Force (SPONGE/main.cu:162-210) calls, in order, LJ + PME direct
+(``LJ_PME_Direct_Force_With_Atom_Energy_And_Virial``), the LJ long-range correction, the PME
+exclusion correction and PME reciprocal space; Main_Iteration (main.cu:376) then updates the
+neighbor list. The engine owns device copies of one system's arrays (from
+``sponge_b200.systems``) and exposes both the per-module sequence and the fused C entry point.
+"""
+
+import numpy as np
+
+from . import (FORM_FIXED, LennardJones, NeighborList, ParticleMeshEwald, _require_cuda,
+               crd_to_uint_crd, nonbonded_step)
+
+
+def scaled_lj_tables(system):
+    """The LJ module's h_LJ_A * 12 and h_LJ_B * 6 in float (Lennard_Jones_force.cu:1092-1098)."""
+    A12 = (np.asarray(system["lj_A"], np.float32) * np.float32(12.0)).astype(np.float32)
+    B6 = (np.asarray(system["lj_B"], np.float32) * np.float32(6.0)).astype(np.float32)
+    return A12, B6
+
+
+class NonbondedEngine:
+    def __init__(self, system, form=FORM_FIXED, refresh_interval=20, max_neighbor_numbers=1200,
+                 device="cuda"):
+        torch = _require_cuda()
+        self.torch = torch
+        self.system = system
+        self.n = n = int(len(system["charge"]))
+        self.box = np.asarray(system["box"], np.float32)
+        dev = torch.device(device)
+        self.crd = torch.tensor(np.asarray(system["crd"], np.float32), device=dev)
+        self.charge = torch.tensor(np.asarray(system["charge"], np.float32), device=dev)
+        self.excl_start = torch.tensor(system["excl_start"], dtype=torch.int32, device=dev)
+        self.excl_numbers = torch.tensor(system["excl_numbers"], dtype=torch.int32, device=dev)
+        el = system["excl_list"] if len(system["excl_list"]) else np.zeros(1, np.int32)
+        self.excl_list = torch.tensor(el, dtype=torch.int32, device=dev)
+        self.uint_crd = torch.empty((n, 3), dtype=torch.int32, device=dev)
+        A12, B6 = scaled_lj_tables(system)
+        self.nl = NeighborList(n, self.box, system["cutoff"], system["skin"], refresh_interval,
+                               max_neighbor_numbers=max_neighbor_numbers, form=form)
+        self.lj = LennardJones(n, system["n_types"], A12, B6, system["lj_type"],
+                               system["cutoff"], self.box, form=form)
+        fft = system.get("fft") or (-1, -1, -1)
+        self.pme = ParticleMeshEwald(n, self.box, system["cutoff"], system["tolerance"], fft,
+                                     form=form)
+        self.frc = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+        self.atom_energy = torch.zeros(n, dtype=torch.float32, device=dev)
+        self.atom_virial = torch.zeros(n, dtype=torch.float32, device=dev)
+        self.d_virial = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.d_potential = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
+
+    @property
+    def excl(self):
+        return (self.excl_start, self.excl_list, self.excl_numbers)
+
+    def update_list(self, forced=0, stream=None):
+        self.nl.Neighbor_List_Update(self.crd, self.excl_start, self.excl_list, self.excl_numbers,
+                                     forced_update=forced, stream=stream)
+
+    def to_uint(self, stream=None):
+        crd_to_uint_crd(self.crd, self.box, out=self.uint_crd, stream=stream)
+
+    def reset(self):
+        self.frc.zero_()
+        self.atom_energy.zero_()
+        self.atom_virial.zero_()
+        self.d_virial.zero_()
+        self.d_potential.zero_()
+
+    def forces(self, need_energy=0, need_virial=0, parts=("direct", "lrc", "excluded",
+                                                          "reciprocal"), stream=None):
+        """Module-by-module force evaluation (adds into self.frc)."""
+        if "direct" in parts:
+            self.lj.LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(
+                self.n, self.uint_crd, self.charge, self.frc, self.nl, self.pme.beta,
+                need_energy, self.atom_energy, need_virial, self.atom_virial,
+                self.pme.d_direct_atom_energy, stream=stream)
+        if "lrc" in parts:
+            self.lj.Long_Range_Correction(need_virial, self.d_virial, need_energy,
+                                          self.d_potential, stream=stream)
+        if "excluded" in parts:
+            self.pme.PME_Excluded_Force_With_Atom_Energy(
+                self.uint_crd, self.scaler, self.charge, self.excl_start, self.excl_list,
+                self.excl_numbers, self.frc, self.pme.d_correction_atom_energy, stream=stream)
+        if "reciprocal" in parts:
+            self.pme.PME_Reciprocal_Force_With_Energy_And_Virial(
+                self.uint_crd, self.charge, self.frc, need_virial, need_energy, self.d_virial,
+                self.d_potential, stream=stream)
+
+    def step(self, need_energy=0, need_virial=0, stream=None):
+        """Fused C entry point: list update by policy + all force terms."""
+        nonbonded_step(self.nl, self.lj, self.pme, self.crd, self.uint_crd, self.charge,
+                       self.excl, self.frc, need_energy, need_virial, self.atom_energy,
+                       self.atom_virial, self.d_virial, self.d_potential, stream=stream)
+
+    def potential(self):
+        """Total potential as MD_core sums it: sum(atom_energy) + d_potential (FP64 sum)."""
+        return float(self.atom_energy.double().sum().item() + self.d_potential.double().item())
+
+    def virial(self):
+        return float(self.atom_virial.double().sum().item() + self.d_virial.double().item())
