@@ -1,0 +1,78 @@
+"""Runs the reference harness (oracle/_ref/ref_harness) on a generated system (test infrastructure).
+
+The reference kernels have no bounds checks on their fixed-capacity buffers (per-atom lists of
+max_neighbor_numbers, cell buckets of max_atom_in_grid_numbers: neighbor_list.cu:297-329,
+:378-386), so the capacities passed here are computed from the system first (largest half list
+and fullest cell, with margin): the harness never runs with a capacity the system can overflow.
+The list is refreshed on a fixed interval so the device-side launch path is not exercised.
+"""
+
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BIN = os.path.join(os.path.dirname(HERE), "_ref", "ref_harness")
+
+
+def available():
+    return os.path.exists(BIN)
+
+
+def safe_capacities(system, uc, pair_keys):
+    n = uc.shape[0]
+    per_atom = np.bincount((pair_keys // n).astype(np.int64), minlength=n)
+    max_nb = int(per_atom.max()) if per_atom.size else 0
+    cs = np.float32(system["cutoff"]) + np.float32(system["skin"])
+    box = np.asarray(system["box"], np.float64)
+    N = np.maximum(1, np.floor(box / (0.5 * float(cs))).astype(np.int64))
+    cell = [((uc[:, d].astype(np.uint64) * np.uint64(N[d])) >> np.uint64(32)).astype(np.int64)
+            for d in range(3)]
+    key = (cell[2] * N[1] + cell[1]) * N[0] + cell[0]
+    max_cell = int(np.bincount(key).max())
+    return int(max_nb * 1.25) + 64, int(max_cell * 1.5) + 16
+
+
+def write_input(path, system, max_nb, max_grid, refresh_interval=20):
+    n = len(system["charge"])
+    T = int(system["n_types"])
+    fft = system.get("fft") or (-1, -1, -1)
+    el = np.asarray(system["excl_list"], np.int32)
+    with open(path, "wb") as f:
+        np.array([n, T, el.size, fft[0], fft[1], fft[2], refresh_interval, max_nb, max_grid],
+                 np.int32).tofile(f)
+        np.array([*system["box"], system["cutoff"], system["skin"], system["tolerance"]],
+                 np.float32).tofile(f)
+        np.asarray(system["crd"], np.float32).tofile(f)
+        np.asarray(system["charge"], np.float32).tofile(f)
+        np.asarray(system["lj_type"], np.int32).tofile(f)
+        np.asarray(system["lj_A"], np.float32).tofile(f)
+        np.asarray(system["lj_B"], np.float32).tofile(f)
+        np.asarray(system["excl_start"], np.int32).tofile(f)
+        np.asarray(system["excl_numbers"], np.int32).tofile(f)
+        el.tofile(f)
+
+
+def run(system, uc, pair_keys, timing_steps=0, outdir=None, timeout=900):
+    """Runs the harness; returns dict(frc, frc_plain, pairs, summary)."""
+    max_nb, max_grid = safe_capacities(system, uc, pair_keys)
+    outdir = outdir or tempfile.mkdtemp(prefix="refh_")
+    os.makedirs(outdir, exist_ok=True)
+    inp = os.path.join(outdir, "in.bin")
+    write_input(inp, system, max_nb, max_grid)
+    r = subprocess.run([BIN, inp, outdir, str(int(timing_steps))], stdin=subprocess.DEVNULL,
+                       capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("reference harness failed (%d): %s" % (r.returncode, r.stderr[-2000:]))
+    n = len(system["charge"])
+    summ = {}
+    for line in open(os.path.join(outdir, "summary.txt")):
+        k, v = line.split()
+        summ[k] = float(v)
+    return dict(
+        frc=np.fromfile(os.path.join(outdir, "frc.f32"), np.float32).reshape(n, 3),
+        frc_plain=np.fromfile(os.path.join(outdir, "frc_plain.f32"), np.float32).reshape(n, 3),
+        pairs=np.fromfile(os.path.join(outdir, "pairs.i64"), np.int64),
+        summary=summ, capacities=(max_nb, max_grid), outdir=outdir)

