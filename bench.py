@@ -41,6 +41,17 @@ def ns_per_day(sec_per_step):
     return DT_FS * 86400.0 / 1e6 / sec_per_step
 
 
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Element-wise max of per-rank timings (every rank gets the result); identity without a
+    process group. Replicas report the slowest rank, as the driver's clock would see it."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -247,13 +258,7 @@ def main():
     torch.cuda.synchronize()
     pair_ms = float(np.mean([a.elapsed_time(b) for a, b in evp]))
 
-    ms = dev_ms / args.steps
-    if dist is not None:
-        t = torch.tensor([ms, e2e_ms / args.steps], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_step_ms = t.tolist()
-    else:
-        e2e_step_ms = e2e_ms / args.steps
+    ms, e2e_step_ms = max_over_ranks([dev_ms / args.steps, e2e_ms / args.steps], dist, "cuda")
     if rank != 0:
         if dist is not None:
             dist.barrier()

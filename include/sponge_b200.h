@@ -150,6 +150,16 @@ SB_API int sb_lj_get_energy(sb_lennard_jones* lj, sb_neighbor_list* nl, const ui
 /* LENNARD_JONES_INFORMATION::Update_Volume */
 SB_API int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[3]);
 
+/* Pair-kernel shape of the fixed-point form (no reference counterpart; a tuning knob):
+ * i atoms held per lane, 8 (one lane per list entry) or 4 (two lanes per entry, fewer registers,
+ * more resident warps). Results are identical to FP32 rounding either way. */
+SB_API int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane);
+
+/* Autotuner: times each pair-kernel shape on the current list and keeps the fastest; writes the
+ * choice to *h_chosen. Synchronises the stream; leaves d_frc untouched. */
+SB_API int sb_lj_tune(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                      const float* d_charge, float pme_beta, int* h_chosen, void* stream);
+
 /* Public members read by other modules: long_range_factor (FP64-computed, returned as float). */
 SB_API int sb_lj_long_range_factor(sb_lennard_jones* lj, float* h_factor);
 

@@ -57,6 +57,8 @@ _SIGS = {
     "sb_lj_get_energy": [_vp, _vp, _vp, _vp, _vp],
     "sb_lj_update_volume": [_vp, _vp],
     "sb_lj_long_range_factor": [_vp, _vp],
+    "sb_lj_set_kernel_variant": [_vp, _i],
+    "sb_lj_tune": [_vp, _vp, _vp, _vp, _f, _vp, _vp],
     "sb_pme_create": [_i, _vp, _f, _f, _i, _i, _i, _i, _vp],
     "sb_pme_destroy": [_vp],
     "sb_pme_info": [_vp, _vp, _vp],
@@ -273,6 +275,17 @@ class LennardJones:
 
     def Update_Volume(self, box_length):
         _check(lib().sb_lj_update_volume(self.handle, _box3(box_length)))
+
+    def set_kernel_variant(self, atoms_per_lane):
+        """Pair-kernel shape: 8 or 4 i atoms per lane (a tuning knob; same results)."""
+        _check(lib().sb_lj_set_kernel_variant(self.handle, int(atoms_per_lane)))
+
+    def tune(self, nl, uint_crd, charge, pme_beta, stream=None):
+        """Time each pair-kernel shape on the current list and keep the fastest."""
+        c = ctypes.c_int()
+        _check(lib().sb_lj_tune(self.handle, nl.handle, _ptr(uint_crd), _ptr(charge),
+                                float(pme_beta), ctypes.byref(c), _stream(stream)))
+        return c.value
 
     def Clear(self):
         if self.handle:

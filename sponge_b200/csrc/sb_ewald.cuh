@@ -25,3 +25,33 @@ __device__ __forceinline__ float sb_ewald_G(float z) {
     float x = sqrtf(z);
     return (erff(x) - 1.1283791670955126f * x * expf(-z)) / (z * x);
 }
+
+// The numerator coefficients of G, in Horner order (highest degree first).
+#define SB_EWALD_P5 -4.234642899e-07
+#define SB_EWALD_P4 3.557744695e-05
+#define SB_EWALD_P3 -2.489903094e-05
+#define SB_EWALD_P2 1.708683818e-02
+#define SB_EWALD_P1 -2.884509870e-02
+#define SB_EWALD_P0 7.522527883e-01
+
+// beta^3 G(z) with the numerator coefficients pre-multiplied by beta^3 (gp[0] = beta^3 P5 ...
+// gp[5] = beta^3 P0, filled on the host), one multiply fewer per pair.
+__device__ __forceinline__ float sb_ewald_G_scaled(float z, const float* gp) {
+    if (z <= 12.0f) {
+        float p = gp[0];
+        p = fmaf(p, z, gp[1]);
+        p = fmaf(p, z, gp[2]);
+        p = fmaf(p, z, gp[3]);
+        p = fmaf(p, z, gp[4]);
+        p = fmaf(p, z, gp[5]);
+        float q = 1.255407394e-04f;
+        q = fmaf(q, z, 2.169710712e-03f);
+        q = fmaf(q, z, 2.242775561e-02f);
+        q = fmaf(q, z, 1.454184461e-01f);
+        q = fmaf(q, z, 5.616555609e-01f);
+        q = fmaf(q, z, 1.0f);
+        return __fdividef(p, q);
+    }
+    // beta^3 = gp[5] / P0
+    return (gp[5] * (float)(1.0 / SB_EWALD_P0)) * sb_ewald_G(z);
+}

@@ -86,7 +86,9 @@ __device__ __forceinline__ void dit_stage(float2* buf, int nl, int ls, int es, i
     const int step = n / L;
     const int nb = n / R;
     for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-        const int l = t / nb, b = t - l * nb;
+        // consecutive threads take consecutive lines: for column lines (ls == 1) the threads of
+        // a warp touch adjacent words and shared-memory bank conflicts disappear
+        const int b = t / nl, l = t - b * nl;
         const int blk = b / m, k = b - blk * m;
         float2* p = buf + l * ls + (blk * L + k) * es;
         float2 y[R];
@@ -106,7 +108,9 @@ __device__ __forceinline__ void dif_stage(float2* buf, int nl, int ls, int es, i
     const int step = n / Lb;
     const int nb = n / R;
     for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-        const int l = t / nb, b = t - l * nb;
+        // consecutive threads take consecutive lines: for column lines (ls == 1) the threads of
+        // a warp touch adjacent words and shared-memory bank conflicts disappear
+        const int b = t / nl, l = t - b * nl;
         const int blk = b / m, n1 = b - blk * m;
         float2* p = buf + l * ls + (blk * Lb + n1) * es;
         float2 y[R];

@@ -36,6 +36,7 @@ struct PairParams {
     float sx, sy, sz;
     float rc2, rc;
     float beta, beta2, beta3;
+    float gp[6];  // beta^3 x numerator coefficients of the Ewald rational (sb_ewald.cuh)
     int nt;
     int slot_cap;
     int ent_cap;
@@ -49,201 +50,7 @@ __device__ __forceinline__ void red_fix(long long* p, float v) {
     if (q) atomicAdd((unsigned long long*)p, (unsigned long long)q);
 }
 
-template <int EV, bool EXACT>
-__device__ __forceinline__ void pair_entries(
-    const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
-    const uint4* __restrict__ xq, const int* __restrict__ stype, const float2* sAB,
-    long long* __restrict__ fix, const int base, const uint32_t rx, const uint32_t ry,
-    const uint32_t rz, const float (&xi)[SB_CLUSTER], const float (&yi)[SB_CLUSTER],
-    const float (&zi)[SB_CLUSTER], const float (&qi)[SB_CLUSTER], const int (&ti)[SB_CLUSTER],
-    float (&fxi)[SB_CLUSTER], float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER],
-    float (&ei)[SB_CLUSTER], float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER], const int lane);
-
-template <int EV>
-__device__ __forceinline__ void finish_cluster(
-    const PairParams& P, const int base, const int lane, const int* __restrict__ slot_atom,
-    long long* __restrict__ fix, float* __restrict__ atom_energy,
-    float* __restrict__ atom_virial, float* __restrict__ atom_direct, float (&fxi)[SB_CLUSTER],
-    float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER], float (&ei)[SB_CLUSTER],
-    float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER]);
-
-template <int EV>
-__global__ void __launch_bounds__(128) k_pair_fixed(
-    PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
-    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
-    const int* __restrict__ stype, const float2* __restrict__ AB,
-    const int* __restrict__ slot_atom, long long* __restrict__ fix,
-    float* __restrict__ atom_energy, float* __restrict__ atom_virial,
-    float* __restrict__ atom_direct) {
-    extern __shared__ float2 sAB[];
-    const int ntt = P.nt * P.nt;
-    for (int t = threadIdx.x; t < ntt; t += blockDim.x) sAB[t] = AB[t];
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (c >= meta[0]) return;
-    const int base = c * SB_CLUSTER;
-
-    const uint4 my = lane < SB_CLUSTER ? xq[base + lane] : make_uint4(0, 0, 0, 0);
-    const int myt = lane < SB_CLUSTER ? stype[base + lane] : 0;
-    const uint32_t rx = __shfl_sync(0xffffffffu, my.x, 0);
-    const uint32_t ry = __shfl_sync(0xffffffffu, my.y, 0);
-    const uint32_t rz = __shfl_sync(0xffffffffu, my.z, 0);
-    const float mxr = __int2float_rn((int)(my.x - rx)) * P.sx;
-    const float myr = __int2float_rn((int)(my.y - ry)) * P.sy;
-    const float mzr = __int2float_rn((int)(my.z - rz)) * P.sz;
-
-    float xi[SB_CLUSTER], yi[SB_CLUSTER], zi[SB_CLUSTER], qi[SB_CLUSTER];
-    int ti[SB_CLUSTER];
-    float fxi[SB_CLUSTER], fyi[SB_CLUSTER], fzi[SB_CLUSTER];
-    float ei[SB_CLUSTER], vi[SB_CLUSTER], di[SB_CLUSTER];
-#pragma unroll
-    for (int k = 0; k < SB_CLUSTER; k++) {
-        xi[k] = __shfl_sync(0xffffffffu, mxr, k);
-        yi[k] = __shfl_sync(0xffffffffu, myr, k);
-        zi[k] = __shfl_sync(0xffffffffu, mzr, k);
-        qi[k] = __uint_as_float(__shfl_sync(0xffffffffu, my.w, k));
-        ti[k] = __shfl_sync(0xffffffffu, myt, k) * P.nt;
-        fxi[k] = fyi[k] = fzi[k] = 0.f;
-        if (EV) ei[k] = vi[k] = di[k] = 0.f;
-    }
-
-    const int cntf = cl_count[c];
-    const int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
-    if (cntf & SB_CL_EXACT)
-        pair_entries<EV, true>(P, cnt, cl_ent + (size_t)c * P.ent_cap, xq,
-                               stype, sAB, fix, base, rx, ry, rz, xi, yi, zi, qi, ti, fxi, fyi,
-                               fzi, ei, vi, di, lane);
-    else
-        pair_entries<EV, false>(P, cnt, cl_ent + (size_t)c * P.ent_cap, xq,
-                                stype, sAB, fix, base, rx, ry, rz, xi, yi, zi, qi, ti, fxi, fyi,
-                                fzi, ei, vi, di, lane);
-    finish_cluster<EV>(P, base, lane, slot_atom, fix, atom_energy, atom_virial, atom_direct, fxi,
-                       fyi, fzi, ei, vi, di);
-}
-
-// The list walk of one cluster. EXACT (set by the search for clusters whose extent plus the
-// list radius reaches half a box length) converts every pair's fixed-point difference instead of
-// using the cluster-relative frame, so minimum image stays exact in small boxes.
-template <int EV, bool EXACT>
-__device__ __forceinline__ void pair_entries(
-    const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
-    const uint4* __restrict__ xq, const int* __restrict__ stype, const float2* sAB,
-    long long* __restrict__ fix, const int base, const uint32_t rx, const uint32_t ry,
-    const uint32_t rz, const float (&xi)[SB_CLUSTER], const float (&yi)[SB_CLUSTER],
-    const float (&zi)[SB_CLUSTER], const float (&qi)[SB_CLUSTER], const int (&ti)[SB_CLUSTER],
-    float (&fxi)[SB_CLUSTER], float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER],
-    float (&ei)[SB_CLUSTER], float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER], const int lane) {
-    for (int e = lane; e < cnt; e += 32) {
-        const uint32_t v = ents[e];
-        const int j = (int)(v & 0xffffffu);
-        const uint32_t m = v >> 24;
-        const uint4 xj = xq[j];
-        const int tj = stype[j];
-        const float xjr = __int2float_rn((int)(xj.x - rx)) * P.sx;
-        const float yjr = __int2float_rn((int)(xj.y - ry)) * P.sy;
-        const float zjr = __int2float_rn((int)(xj.z - rz)) * P.sz;
-        const float qj = __uint_as_float(xj.w);
-        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-#pragma unroll
-        for (int k = 0; k < SB_CLUSTER; k++) {
-            float dx, dy, dz;
-            if (EXACT) {
-                const uint4 xk = xq[base + k];
-                dx = __int2float_rn((int)(xj.x - xk.x)) * P.sx;
-                dy = __int2float_rn((int)(xj.y - xk.y)) * P.sy;
-                dz = __int2float_rn((int)(xj.z - xk.z)) * P.sz;
-            } else {
-                dx = xjr - xi[k];
-                dy = yjr - yi[k];
-                dz = zjr - zi[k];
-            }
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            if (((m >> k) & 1u) && r2 < P.rc2) {
-                const float ri = rsqrtf(r2);
-                const float ri2 = ri * ri;
-                const float ri6 = ri2 * ri2 * ri2;
-                const float2 ab = sAB[ti[k] + tj];
-                const float flj = (ab.y - ab.x * ri6) * ri6 * ri2;
-                const float qq = qi[k] * qj;
-                const float z = P.beta2 * r2;
-                const float G = sb_ewald_G(z);
-                const float fc = qq * (ri * ri2 - P.beta3 * G);
-                const float fs = flj - fc;
-                const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
-                fxi[k] += tx;
-                fyi[k] += ty;
-                fzi[k] += tz;
-                fjx -= tx;
-                fjy -= ty;
-                fjz -= tz;
-                if (EV & SB_EV_ENERGY) {
-                    const float ec = qq * erfcf(P.beta * r2 * ri) * ri;
-                    ei[k] += (0.083333333f * ab.x * ri6 - 0.166666667f * ab.y) * ri6 + ec;
-                    di[k] += ec;
-                }
-                if (EV & SB_EV_VIRIAL) {
-                    vi[k] -= flj * r2;
-                    if (!(EV & SB_EV_ENERGY)) di[k] += qq * erfcf(P.beta * r2 * ri) * ri;
-                }
-            }
-        }
-        red_fix(&fix[j], fjx);
-        red_fix(&fix[P.slot_cap + j], fjy);
-        red_fix(&fix[2 * P.slot_cap + j], fjz);
-    }
-}
-
-// warp reduction of the i forces (lane k ends with cluster atom k's totals) and their output
-template <int EV>
-__device__ __forceinline__ void finish_cluster(
-    const PairParams& P, const int base, const int lane, const int* __restrict__ slot_atom,
-    long long* __restrict__ fix, float* __restrict__ atom_energy,
-    float* __restrict__ atom_virial, float* __restrict__ atom_direct, float (&fxi)[SB_CLUSTER],
-    float (&fyi)[SB_CLUSTER], float (&fzi)[SB_CLUSTER], float (&ei)[SB_CLUSTER],
-    float (&vi)[SB_CLUSTER], float (&di)[SB_CLUSTER]) {
-#pragma unroll
-    for (int k = 0; k < SB_CLUSTER; k++) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            fxi[k] += __shfl_xor_sync(0xffffffffu, fxi[k], o);
-            fyi[k] += __shfl_xor_sync(0xffffffffu, fyi[k], o);
-            fzi[k] += __shfl_xor_sync(0xffffffffu, fzi[k], o);
-            if (EV) {
-                ei[k] += __shfl_xor_sync(0xffffffffu, ei[k], o);
-                vi[k] += __shfl_xor_sync(0xffffffffu, vi[k], o);
-                di[k] += __shfl_xor_sync(0xffffffffu, di[k], o);
-            }
-        }
-    }
-    float ox = 0.f, oy = 0.f, oz = 0.f, oe = 0.f, ov = 0.f, od = 0.f;
-#pragma unroll
-    for (int k = 0; k < SB_CLUSTER; k++)
-        if (lane == k) {
-            ox = fxi[k];
-            oy = fyi[k];
-            oz = fzi[k];
-            if (EV) {
-                oe = ei[k];
-                ov = vi[k];
-                od = di[k];
-            }
-        }
-    if (lane < SB_CLUSTER) {
-        const int s = base + lane;
-        const int a = slot_atom[s];
-        if (a >= 0) {
-            red_fix(&fix[s], ox);
-            red_fix(&fix[P.slot_cap + s], oy);
-            red_fix(&fix[2 * P.slot_cap + s], oz);
-            if (EV & SB_EV_ENERGY) atom_energy[a] += oe;
-            if (EV & SB_EV_VIRIAL) {
-                atom_virial[a] += ov;
-                atom_direct[a] = od;
-            }
-        }
-    }
-}
+#include "sb_pair_fixed.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // plain form: reference structure (warp per atom, float atomics), Lennard_Jones_force.cu:47-158
@@ -459,6 +266,10 @@ static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list
     P.beta = beta;
     P.beta2 = beta * beta;
     P.beta3 = beta * beta * beta;
+    const double b3 = (double)beta * beta * beta;
+    const double pc[6] = {SB_EWALD_P5, SB_EWALD_P4, SB_EWALD_P3,
+                          SB_EWALD_P2, SB_EWALD_P1, SB_EWALD_P0};
+    for (int k = 0; k < 6; k++) P.gp[k] = (float)(b3 * pc[k]);
     P.nt = lj->ntypes;
     P.slot_cap = nl->slot_cap;
     P.ent_cap = nl->ent_cap;
@@ -475,21 +286,29 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
         sb_set_error("LJ type table too large for shared memory (%d types)", lj->ntypes);
         return SB_ERR_ARG;
     }
-#define SB_LAUNCH_PAIR(EVV)                                                                   \
+#define SB_LAUNCH_PAIR(EVV, IPLV)                                                             \
     do {                                                                                      \
         if (smem > 48 * 1024)                                                                 \
-            cudaFuncSetAttribute(k_pair_fixed<EVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)smem);                                                  \
-        k_pair_fixed<EVV><<<blocks, 32 * warps, smem, s>>>(P, nl->meta, nl->cl_count,          \
-                                                          nl->cl_ent, nl->xq, nl->stype,      \
-                                                          lj->d_AB, nl->slot_atom, nl->fix,   \
-                                                          ae, av, ad);                        \
+            cudaFuncSetAttribute(k_pair_fixed<EVV, IPLV>,                                     \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+        k_pair_fixed<EVV, IPLV><<<blocks, 32 * warps, smem, s>>>(                             \
+            P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
+            nl->slot_atom, nl->fix, ae, av, ad);                                              \
     } while (0)
-    switch (ev) {
-        case 0: SB_LAUNCH_PAIR(0); break;
-        case 1: SB_LAUNCH_PAIR(1); break;
-        case 2: SB_LAUNCH_PAIR(2); break;
-        default: SB_LAUNCH_PAIR(3); break;
+    if (lj->ipl == 4) {
+        switch (ev) {
+            case 0: SB_LAUNCH_PAIR(0, 4); break;
+            case 1: SB_LAUNCH_PAIR(1, 4); break;
+            case 2: SB_LAUNCH_PAIR(2, 4); break;
+            default: SB_LAUNCH_PAIR(3, 4); break;
+        }
+    } else {
+        switch (ev) {
+            case 0: SB_LAUNCH_PAIR(0, 8); break;
+            case 1: SB_LAUNCH_PAIR(1, 8); break;
+            case 2: SB_LAUNCH_PAIR(2, 8); break;
+            default: SB_LAUNCH_PAIR(3, 8); break;
+        }
     }
 #undef SB_LAUNCH_PAIR
     SB_CHECK_LAUNCH();
@@ -631,6 +450,58 @@ extern "C" int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[
     }
     for (int d = 0; d < 3; d++) lj->box[d] = box_length[d];
     lj->volume = box_length[0] * box_length[1] * box_length[2];
+    return SB_OK;
+}
+
+extern "C" int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane) {
+    if (!lj || (atoms_per_lane != 4 && atoms_per_lane != 8)) {
+        sb_set_error("sb_lj_set_kernel_variant: atoms_per_lane must be 4 or 8");
+        return SB_ERR_ARG;
+    }
+    lj->ipl = atoms_per_lane;
+    return SB_OK;
+}
+
+extern "C" int sb_lj_tune(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                          const float* d_charge, float pme_beta, int* h_chosen, void* stream) {
+    if (!lj || !nl || !d_uint_crd || !d_charge) {
+        sb_set_error("sb_lj_tune: null argument");
+        return SB_ERR_ARG;
+    }
+    SB_TRY(sb_nl_ensure_built(nl));
+    if (lj->form != SB_FORM_FIXED) {
+        if (h_chosen) *h_chosen = 0;
+        return SB_OK;
+    }
+    cudaStream_t s = sb_stream(stream);
+    SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
+    const int cand[2] = {4, 8};
+    float best = 1e30f;
+    int pick = lj->ipl;
+    cudaEvent_t a, b;
+    SB_CHECK_CUDA(cudaEventCreate(&a));
+    SB_CHECK_CUDA(cudaEventCreate(&b));
+    for (int c = 0; c < 2; c++) {
+        lj->ipl = cand[c];
+        SB_TRY(launch_pair_fixed(lj, nl, pme_beta, 0, nullptr, nullptr, nullptr, s));
+        SB_CHECK_CUDA(cudaEventRecord(a, s));
+        for (int r = 0; r < 3; r++)
+            SB_TRY(launch_pair_fixed(lj, nl, pme_beta, 0, nullptr, nullptr, nullptr, s));
+        SB_CHECK_CUDA(cudaEventRecord(b, s));
+        SB_CHECK_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) {
+            best = ms;
+            pick = cand[c];
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    lj->ipl = pick;
+    // the timing runs accumulated into the fixed-point buffers: clear them
+    SB_CHECK_CUDA(cudaMemsetAsync(nl->fix, 0, sizeof(long long) * 3 * nl->slot_cap, s));
+    if (h_chosen) *h_chosen = pick;
     return SB_OK;
 }
 

@@ -1,0 +1,102 @@
+"""The oracle pinned against the REFERENCE's own outputs (CPU test).
+
+tests/golden/reference_*.npz were produced by running SPONGE's unchanged NEIGHBOR_LIST,
+LENNARD_JONES_INFORMATION and Particle_Mesh_Ewald modules on a B200 (tests/golden/make_golden.py
+through oracle/ref_harness). The systems are regenerated here from their seeds.
+
+Tolerances: the reference computes in FP32 with float atomics, so its forces are compared at
+relative RMS 1e-5 against the FP64 oracle; its FP32 energy reductions at relative 1e-4; its
+long-range LJ factor (an FP32 atomic sum over all N^2 atom pairs) at 1e-3. Its pair list may
+differ from the pinned criterion only in pairs within FP32 rounding of the threshold.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from sponge_b200 import systems
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = {
+    "small": lambda: systems.small_water(),
+    "config0": systems.config0,
+    "config3": systems.config3,
+}
+
+
+def fixture(name):
+    path = os.path.join(HERE, "reference_%s.npz" % name)
+    if not os.path.exists(path):
+        pytest.fail("missing golden fixture %s (run tests/golden/make_golden.py on a GPU)" % path)
+    return np.load(path)
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request, oracle_lib):
+    s = CASES[request.param]()
+    uc = oracle_lib.crd_to_uint(oracle_lib.periodic_map(s["crd"], s["box"]), s["box"])
+    ref = oracle_lib.reference_energies(s, uc=uc)
+    return request.param, s, uc, ref, fixture(request.param)
+
+
+def boundary_r2(uc, keys, s):
+    """FP32 r^2 of pairs (pinned expression) and the list threshold."""
+    n = uc.shape[0]
+    i, j = keys // n, keys % n
+    sc = (np.float32(1.0) / np.float32(4294967296.0)) * np.asarray(s["box"], np.float32)
+    with np.errstate(over="ignore"):
+        d = [(uc[j, k].astype(np.int64) - uc[i, k].astype(np.int64)).astype(np.int32)
+             .astype(np.float32) * sc[k] for k in range(3)]
+    r2 = (d[0] * d[0] + d[1] * d[1]).astype(np.float32) + (d[2] * d[2]).astype(np.float32)
+    cs = np.float32(s["cutoff"]) + np.float32(s["skin"])
+    return r2.astype(np.float32), np.float32(cs * cs)
+
+
+def test_pair_list_matches_reference(case):
+    name, s, uc, ref, g = case
+    if "pairs" in g.files:
+        rp = g["pairs"]
+        only_ref = np.setdiff1d(rp, ref["pairs"])
+        only_orc = np.setdiff1d(ref["pairs"], rp)
+    else:
+        only_ref, only_orc = g["pairs_only_ref"], g["pairs_only_oracle"]
+        assert int(g["n_pairs"]) == ref["pairs"].size + only_ref.size - only_orc.size
+    # every disagreement is a pair within FP32 rounding of (rc+skin)^2
+    for keys in (only_ref, only_orc):
+        if keys.size:
+            r2, thr = boundary_r2(uc, keys, s)
+            assert np.all(np.abs(r2 - thr) <= 4 * np.spacing(thr))
+    assert only_ref.size + only_orc.size <= max(2, ref["pairs"].size // 100000)
+
+
+def test_reference_forces_match_oracle(case):
+    name, s, uc, ref, g = case
+    for key in ("frc", "frc_plain"):
+        f = g[key].astype(np.float64)
+        err = np.sqrt(((f - ref["f_total"]) ** 2).sum() / (ref["f_total"] ** 2).sum())
+        assert err < 1e-5, (key, err)
+
+
+def test_reference_energies_match_oracle(case):
+    name, s, uc, ref, g = case
+    get = lambda k: float(g["summary_" + k])  # noqa: E731
+    assert get("beta") == pytest.approx(ref["beta"], rel=1e-7)
+    assert get("e_rec") == pytest.approx(ref["e_rec"], rel=1e-4)
+    assert get("e_self") == pytest.approx(ref["e_self"], rel=1e-4)
+    assert get("e_direct") == pytest.approx(ref["e_direct"], rel=1e-4, abs=1e-2)
+    assert get("e_corr") == pytest.approx(ref["e_corr"], rel=1e-4)
+    assert get("long_range_factor") == pytest.approx(ref["lrc_factor"], rel=1e-3)
+    V = float(np.prod(np.asarray(s["box"], np.float64)))
+    lrc_ref = get("long_range_factor") / V
+    assert get("e_lj_with_lrc") - lrc_ref == pytest.approx(ref["e_lj"], rel=1e-4, abs=1e-2)
+    assert get("atom_virial_sum") == pytest.approx(ref["virial_lj"], rel=1e-4, abs=1e-2)
+    # d_potential = LRC + correction + self + reciprocal; d_virial = 6 LRC + direct + those
+    pot = lrc_ref + ref["e_corr"] + ref["e_self"] + ref["e_rec"]
+    vir = 6 * lrc_ref + ref["e_direct"] + ref["e_corr"] + ref["e_self"] + ref["e_rec"]
+    scale = abs(ref["e_self"]) + abs(ref["e_corr"])
+    assert abs(get("d_potential") - pot) < 1e-5 * scale + 1e-4 * abs(pot)
+    assert abs(get("d_virial") - vir) < 1e-5 * scale + 1e-4 * abs(vir)
+    # per-atom energy sum = LJ + direct Coulomb
+    assert get("atom_energy_sum") == pytest.approx(ref["e_lj"] + ref["e_direct"], rel=1e-4,
+                                                    abs=1e-2)

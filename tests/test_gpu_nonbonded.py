@@ -99,8 +99,16 @@ def _forces(eng, parts, need_energy=0, need_virial=0):
 
 def test_direct_force(case):
     name, s, eng, ref = case
-    f = _forces(eng, ("direct",))
-    assert rel_rms(f, ref["f_direct"]) < FORCE_TOL
+    out = {}
+    for ipl in (8, 4):  # both pair-kernel shapes
+        eng.lj.set_kernel_variant(ipl)
+        out[ipl] = _forces(eng, ("direct",))
+        assert rel_rms(out[ipl], ref["f_direct"]) < FORCE_TOL
+    assert rel_rms(out[4], out[8]) < 1e-6
+    chosen = eng.lj.tune(eng.nl, eng.uint_crd, eng.charge, eng.pme.beta)
+    assert chosen in (4, 8)
+    # tuning leaves no residue in the accumulators
+    assert np.array_equal(_forces(eng, ("direct",)), out[chosen])
 
 
 def test_excluded_force(case):
