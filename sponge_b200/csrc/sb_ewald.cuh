@@ -34,6 +34,25 @@ __device__ __forceinline__ float sb_ewald_G(float z) {
 #define SB_EWALD_P1 -2.884509870e-02
 #define SB_EWALD_P0 7.522527883e-01
 
+// beta^3 G(z) by the rational alone, no branch: valid for z <= 12. The pair kernel uses it when
+// (beta rc)^2 <= 12 (every tolerance above ~1e-7), where in-cutoff pairs never leave the fitted
+// range and out-of-range values only reach pairs that are discarded.
+__device__ __forceinline__ float sb_ewald_G_rational(float z, const float* gp) {
+    float p = gp[0];
+    p = fmaf(p, z, gp[1]);
+    p = fmaf(p, z, gp[2]);
+    p = fmaf(p, z, gp[3]);
+    p = fmaf(p, z, gp[4]);
+    p = fmaf(p, z, gp[5]);
+    float q = 1.255407394e-04f;
+    q = fmaf(q, z, 2.169710712e-03f);
+    q = fmaf(q, z, 2.242775561e-02f);
+    q = fmaf(q, z, 1.454184461e-01f);
+    q = fmaf(q, z, 5.616555609e-01f);
+    q = fmaf(q, z, 1.0f);
+    return __fdividef(p, q);
+}
+
 // beta^3 G(z) with the numerator coefficients pre-multiplied by beta^3 (gp[0] = beta^3 P5 ...
 // gp[5] = beta^3 P0, filled on the host), one multiply fewer per pair.
 __device__ __forceinline__ float sb_ewald_G_scaled(float z, const float* gp) {

@@ -208,71 +208,6 @@ __device__ void load_tables(SmemTables& T, const int* pa, const int* pb, const f
 }
 
 // ---------------------------------------------------------------------------------------------
-// forward plane pass: z (real, via M = K2/2 complex) then y; A = z axis (length M), B = y axis
-// ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_plane_fwd(FftAxisDev Az, FftAxisDev Ay,
-                                                   const int* __restrict__ pz,
-                                                   const int* __restrict__ py,
-                                                   const float2* __restrict__ twz,
-                                                   const float2* __restrict__ twy,
-                                                   const float2* __restrict__ post,
-                                                   long long* __restrict__ qfix,
-                                                   float2* __restrict__ spec, int K1, int K2) {
-    extern __shared__ __align__(16) char sm[];
-    const int M = K2 / 2, H = M + 1;
-    SmemTables T = carve(sm, M, K1, M);
-    load_tables(T, pz, py, twz, twy, post, M, K1, M);
-    float2* D = T.data;  // [K1][H]
-    const int x = blockIdx.x;
-    long long* q = qfix + (size_t)x * K1 * K2;
-    // digit-reversed load of z = x_even + i x_odd, clearing the charge grid behind us
-    for (int t = threadIdx.x; t < K1 * M; t += blockDim.x) {
-        const int y = t / M, p = t - y * M;
-        const int nn = T.perm_a[p];
-        long long* g = q + (size_t)y * K2 + 2 * nn;
-        const long long a = g[0], b = g[1];
-        g[0] = 0;
-        g[1] = 0;
-        D[y * H + p] = make_float2((float)a * SB_GRID_UNSCALE, (float)b * SB_GRID_UNSCALE);
-    }
-    __syncthreads();
-    fft_dit(D, K1, H, 1, Az, T.tw_a, false);
-    // real-transform post-processing: X[k] = E[k] + W_K2^k O[k], k = 0..M
-    const int half = M / 2;
-    for (int t = threadIdx.x; t < K1 * (half + 1); t += blockDim.x) {
-        const int y = t / (half + 1), k = t - y * (half + 1);
-        float2* row = D + y * H;
-        if (k == 0) {
-            const float2 z0 = row[0];
-            row[0] = make_float2(z0.x + z0.y, 0.f);
-            row[M] = make_float2(z0.x - z0.y, 0.f);
-        } else {
-            const int k2 = M - k;
-            const float2 a = row[k], b = row[k2];
-            // E[k] = (Z[k] + conj Z[M-k]) / 2, O[k] = (Z[k] - conj Z[M-k]) / 2i
-            const float2 Ek = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
-            const float2 Ok = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
-            const float2 Xk = cadd(Ek, cmul(T.post[k], Ok));
-            if (k2 != k) {
-                // E[M-k] = conj E[k], O[M-k] = conj O[k]; W^{M-k} = -conj(W^k)
-                const float2 w2 = make_float2(-T.post[k].x, T.post[k].y);
-                const float2 Xk2 = cadd(conjf2(Ek), cmul(w2, conjf2(Ok)));
-                row[k2] = Xk2;
-            }
-            row[k] = Xk;
-        }
-    }
-    __syncthreads();
-    // forward along y for every kz column, natural in -> digit-reversed out
-    fft_dif(D, H, 1, H, Ay, T.tw_b, false);
-    float2* out = spec + (size_t)x * K1 * H;
-    for (int t = threadIdx.x; t < K1 * H; t += blockDim.x) {
-        const int p = t / H, kz = t - p * H;
-        out[(size_t)T.perm_b[p] * H + kz] = D[p * H + kz];
-    }
-}
-
-// ---------------------------------------------------------------------------------------------
 // x pass with the convolution: forward x (DIT), * BC, energy, inverse x (DIF)
 // ---------------------------------------------------------------------------------------------
 #define SB_XCONV_T 16
@@ -332,42 +267,90 @@ __global__ void __launch_bounds__(256) k_xconv(FftAxisDev Ax, const int* __restr
 }
 
 // ---------------------------------------------------------------------------------------------
-// inverse plane pass: y inverse (DIT) then z complex-to-real (DIF)
+// z passes: SB_ZROWS rows of K2 reals per block. Global reads and writes are coalesced along a
+// row; the digit reversal happens on the shared-memory side through the inverse permutation.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_plane_inv(FftAxisDev Az, FftAxisDev Ay,
-                                                   const int* __restrict__ pz,
-                                                   const int* __restrict__ py,
-                                                   const float2* __restrict__ twz,
-                                                   const float2* __restrict__ twy,
-                                                   const float2* __restrict__ post,
-                                                   const float2* __restrict__ spec,
-                                                   float* __restrict__ real, int K1, int K2) {
+#define SB_ZROWS 32
+
+// real-to-complex along z: int64 charge grid rows (cleared behind) -> half-spectrum rows
+__global__ void __launch_bounds__(256) k_zfwd(FftAxisDev Az, const int* __restrict__ ipz,
+                                              const float2* __restrict__ twz,
+                                              const float2* __restrict__ post,
+                                              long long* __restrict__ qfix,
+                                              float2* __restrict__ spec, int nrows, int K2) {
     extern __shared__ __align__(16) char sm[];
     const int M = K2 / 2, H = M + 1;
-    SmemTables T = carve(sm, M, K1, M);
-    load_tables(T, pz, py, twz, twy, post, M, K1, M);
+    SmemTables T = carve(sm, M, 0, M);
+    load_tables(T, ipz, ipz, twz, twz, post, M, 0, M);
     float2* D = T.data;
-    const int x = blockIdx.x;
-    const float2* in = spec + (size_t)x * K1 * H;
-    for (int t = threadIdx.x; t < K1 * H; t += blockDim.x) {
-        const int p = t / H, kz = t - p * H;
-        D[p * H + kz] = in[(size_t)T.perm_b[p] * H + kz];
+    float* Df = reinterpret_cast<float*>(D);
+    const int r0 = blockIdx.x * SB_ZROWS;
+    const int nr = min(SB_ZROWS, nrows - r0);
+    long long* q = qfix + (size_t)r0 * K2;
+    for (int t = threadIdx.x; t < nr * K2; t += blockDim.x) {
+        const int r = t / K2, col = t - r * K2;
+        const long long v = q[t];
+        if (v) q[t] = 0;
+        Df[2 * (r * H + T.perm_a[col >> 1]) + (col & 1)] = (float)v * SB_GRID_UNSCALE;
     }
     __syncthreads();
-    fft_dit(D, H, 1, H, Ay, T.tw_b, true);
-    // C2R pre-processing: Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_K2^{-k}
+    fft_dit(D, nr, H, 1, Az, T.tw_a, false);
+    // X[k] = E[k] + W_K2^k O[k], k = 0..M, from Z = FFT_M(x_even + i x_odd)
     const int half = M / 2;
-    for (int t = threadIdx.x; t < K1 * (half + 1); t += blockDim.x) {
-        const int y = t / (half + 1), k = t - y * (half + 1);
-        float2* row = D + y * H;
+    for (int t = threadIdx.x; t < nr * (half + 1); t += blockDim.x) {
+        const int k = t / nr, r = t - k * nr;
+        float2* row = D + r * H;
+        if (k == 0) {
+            const float2 z0 = row[0];
+            row[0] = make_float2(z0.x + z0.y, 0.f);
+            row[M] = make_float2(z0.x - z0.y, 0.f);
+        } else {
+            const int k2 = M - k;
+            const float2 a = row[k], b = row[k2];
+            const float2 Ek = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+            const float2 Ok = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
+            const float2 Xk = cadd(Ek, cmul(T.post[k], Ok));
+            if (k2 != k) {
+                const float2 w2 = make_float2(-T.post[k].x, T.post[k].y);
+                row[k2] = cadd(conjf2(Ek), cmul(w2, conjf2(Ok)));
+            }
+            row[k] = Xk;
+        }
+    }
+    __syncthreads();
+    float2* out = spec + (size_t)r0 * H;
+    for (int t = threadIdx.x; t < nr * H; t += blockDim.x) out[t] = D[t];
+}
+
+// complex-to-real along z: half-spectrum rows -> real rows
+__global__ void __launch_bounds__(256) k_zinv(FftAxisDev Az, const int* __restrict__ ipz,
+                                              const float2* __restrict__ twz,
+                                              const float2* __restrict__ post,
+                                              const float2* __restrict__ spec,
+                                              float* __restrict__ real, int nrows, int K2) {
+    extern __shared__ __align__(16) char sm[];
+    const int M = K2 / 2, H = M + 1;
+    SmemTables T = carve(sm, M, 0, M);
+    load_tables(T, ipz, ipz, twz, twz, post, M, 0, M);
+    float2* D = T.data;
+    const float* Df = reinterpret_cast<const float*>(D);
+    const int r0 = blockIdx.x * SB_ZROWS;
+    const int nr = min(SB_ZROWS, nrows - r0);
+    const float2* in = spec + (size_t)r0 * H;
+    for (int t = threadIdx.x; t < nr * H; t += blockDim.x) D[t] = in[t];
+    __syncthreads();
+    // Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_K2^{-k}, k = 0..M-1
+    const int half = M / 2;
+    for (int t = threadIdx.x; t < nr * (half + 1); t += blockDim.x) {
+        const int k = t / nr, r = t - k * nr;
+        float2* row = D + r * H;
         const int k2 = M - k;
-        const float2 a = row[k], b = row[k2];  // k = 0 pairs X[0] with X[M]
-        const float2 wk = conjf2(T.post[k]);   // W^{-k}
+        const float2 a = row[k], b = row[k2];
+        const float2 wk = conjf2(T.post[k]);
         const float2 E = cadd(a, conjf2(b));
         const float2 O = cmul(csub(a, conjf2(b)), wk);
-        const float2 Zk = make_float2(E.x - O.y, E.y + O.x);  // E + i O
+        const float2 Zk = make_float2(E.x - O.y, E.y + O.x);
         if (k != 0 && k2 != k) {
-            // Z[M-k] from X[M-k], X[k]: W^{-(M-k)} = -conj(W^{-k}) ... computed directly
             const float2 w2 = make_float2(-wk.x, wk.y);
             const float2 E2 = cadd(b, conjf2(a));
             const float2 O2 = cmul(csub(b, conjf2(a)), w2);
@@ -376,14 +359,38 @@ __global__ void __launch_bounds__(512) k_plane_inv(FftAxisDev Az, FftAxisDev Ay,
         row[k] = Zk;
     }
     __syncthreads();
-    fft_dif(D, K1, H, 1, Az, T.tw_a, true);
-    float* out = real + (size_t)x * K1 * K2;
-    for (int t = threadIdx.x; t < K1 * M; t += blockDim.x) {
-        const int y = t / M, p = t - y * M;
-        const float2 v = D[y * H + p];
-        const int nn = T.perm_a[p];
-        out[(size_t)y * K2 + 2 * nn] = v.x;
-        out[(size_t)y * K2 + 2 * nn + 1] = v.y;
+    fft_dif(D, nr, H, 1, Az, T.tw_a, true);
+    float* o = real + (size_t)r0 * K2;
+    for (int t = threadIdx.x; t < nr * K2; t += blockDim.x) {
+        const int r = t / K2, col = t - r * K2;
+        o[t] = Df[2 * (r * H + T.perm_a[col >> 1]) + (col & 1)];
+    }
+}
+
+// y pass (forward or inverse) on a tile of SB_YT adjacent kz columns of one x-plane: DIT with a
+// digit-reversed load, natural-order store
+#define SB_YT 16
+__global__ void __launch_bounds__(256) k_ypass(FftAxisDev Ay, const int* __restrict__ py,
+                                               const float2* __restrict__ twy,
+                                               float2* __restrict__ spec, int K1, int H,
+                                               int inv) {
+    extern __shared__ __align__(16) char sm[];
+    SmemTables T = carve(sm, K1, 0, 0);
+    load_tables(T, py, py, twy, twy, twy, K1, 0, 0);
+    float2* D = T.data;  // [K1][SB_YT]
+    const int x = blockIdx.x;
+    const int kz0 = blockIdx.y * SB_YT;
+    const int nt = min(SB_YT, H - kz0);
+    float2* base = spec + (size_t)x * K1 * H + kz0;
+    for (int t = threadIdx.x; t < K1 * SB_YT; t += blockDim.x) {
+        const int p = t / SB_YT, c = t - p * SB_YT;
+        D[t] = c < nt ? base[(size_t)T.perm_a[p] * H + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_dit(D, SB_YT, 1, SB_YT, Ay, T.tw_a, inv != 0);
+    for (int t = threadIdx.x; t < K1 * SB_YT; t += blockDim.x) {
+        const int p = t / SB_YT, c = t - p * SB_YT;
+        if (c < nt) base[(size_t)p * H + c] = D[t];
     }
 }
 
@@ -430,9 +437,13 @@ static int axis_create(SbFftAxis* a, int n) {
         double ang = -2.0 * M_PI * (double)t / n;
         tw[t] = make_float2((float)cos(ang), (float)sin(ang));
     }
+    std::vector<int> iperm(n);
+    for (int p = 0; p < n; p++) iperm[perm[p]] = p;
     SB_TRY(sb_malloc((void**)&a->d_perm, sizeof(int) * n, "fft perm"));
+    SB_TRY(sb_malloc((void**)&a->d_iperm, sizeof(int) * n, "fft inverse perm"));
     SB_TRY(sb_malloc((void**)&a->d_tw, sizeof(float2) * n, "fft twiddles"));
     SB_CHECK_CUDA(cudaMemcpy(a->d_perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    SB_CHECK_CUDA(cudaMemcpy(a->d_iperm, iperm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     SB_CHECK_CUDA(cudaMemcpy(a->d_tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
     return SB_OK;
 }
@@ -463,22 +474,28 @@ int sb_fft_plan_create(SbFftPlan* p, const int K[3]) {
     }
     SB_TRY(sb_malloc((void**)&p->d_post, sizeof(float2) * M, "fft post twiddles"));
     SB_CHECK_CUDA(cudaMemcpy(p->d_post, post.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
-    p->plane_smem = carve_bytes(M, K[1], M) + sizeof(float2) * (size_t)K[1] * p->H;
+    // shared memory of the three tile shapes (z rows, y columns, x columns)
+    p->plane_smem = carve_bytes(M, 0, M) + sizeof(float2) * (size_t)SB_ZROWS * p->H;
+    const size_t ys = carve_bytes(K[1], 0, 0) + sizeof(float2) * (size_t)K[1] * SB_YT;
+    const size_t xs = carve_bytes(K[0], 0, 0) + sizeof(float2) * (size_t)K[0] * SB_XCONV_T;
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (optin <= 0) optin = 227 * 1024;
-    if (p->plane_smem > (size_t)optin) {
-        sb_set_error("PME grid plane %dx%d needs %zu B of shared memory (> %d)", K[1], K[2],
-                     p->plane_smem, optin);
+    if (p->plane_smem > (size_t)optin || ys > (size_t)optin || xs + 2048 > (size_t)optin) {
+        sb_set_error("PME grid %dx%dx%d needs more shared memory per block than %d B", K[0],
+                     K[1], K[2], optin);
         return SB_ERR_ARG;
     }
-    cudaFuncSetAttribute(k_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)p->plane_smem);
-    cudaFuncSetAttribute(k_plane_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)p->plane_smem);
-    size_t xs = carve_bytes(K[0], 0, 0) + sizeof(float2) * (size_t)K[0] * SB_XCONV_T;
-    if (xs > 48 * 1024)
+    if (p->plane_smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)p->plane_smem);
+        cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)p->plane_smem);
+    }
+    if (ys > 48 * 1024)
+        cudaFuncSetAttribute(k_ypass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
+    if (xs > 46 * 1024)
         cudaFuncSetAttribute(k_xconv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xs);
     return SB_OK;
 }
@@ -487,8 +504,10 @@ void sb_fft_plan_destroy(SbFftPlan* p) {
     SbFftAxis* ax[3] = {&p->z, &p->y, &p->x};
     for (SbFftAxis* a : ax) {
         sb_free(a->d_perm);
+        sb_free(a->d_iperm);
         sb_free(a->d_tw);
         a->d_perm = nullptr;
+        a->d_iperm = nullptr;
         a->d_tw = nullptr;
     }
     sb_free(p->d_post);
@@ -496,9 +515,14 @@ void sb_fft_plan_destroy(SbFftPlan* p) {
 }
 
 int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, cudaStream_t s) {
-    k_plane_fwd<<<p->K[0], 512, p->plane_smem, s>>>(axis_dev(p->z), axis_dev(p->y), p->z.d_perm,
-                                                    p->y.d_perm, p->z.d_tw, p->y.d_tw, p->d_post,
-                                                    d_qfix, d_spec, p->K[1], p->K[2]);
+    const int rows = p->K[0] * p->K[1];
+    k_zfwd<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
+        axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_qfix, d_spec, rows, p->K[2]);
+    SB_CHECK_LAUNCH();
+    const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * SB_YT;
+    dim3 grid(p->K[0], (p->H + SB_YT - 1) / SB_YT);
+    k_ypass<<<grid, 256, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec, p->K[1], p->H,
+                                  0);
     SB_CHECK_LAUNCH();
     return SB_OK;
 }
@@ -521,9 +545,14 @@ int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, dou
 
 int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real,
                          cudaStream_t s) {
-    k_plane_inv<<<p->K[0], 512, p->plane_smem, s>>>(axis_dev(p->z), axis_dev(p->y), p->z.d_perm,
-                                                    p->y.d_perm, p->z.d_tw, p->y.d_tw, p->d_post,
-                                                    d_spec, d_real, p->K[1], p->K[2]);
+    const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * SB_YT;
+    dim3 grid(p->K[0], (p->H + SB_YT - 1) / SB_YT);
+    k_ypass<<<grid, 256, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw,
+                                  const_cast<float2*>(d_spec), p->K[1], p->H, 1);
+    SB_CHECK_LAUNCH();
+    const int rows = p->K[0] * p->K[1];
+    k_zinv<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
+        axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_spec, d_real, rows, p->K[2]);
     SB_CHECK_LAUNCH();
     return SB_OK;
 }

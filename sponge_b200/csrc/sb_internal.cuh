@@ -77,6 +77,7 @@ struct SbFftAxis {
     int nrad = 0;
     int rad[SB_FFT_MAX_STAGES] = {0};
     int* d_perm = nullptr;     // DIT input position p holds element perm[p]; DIF output likewise
+    int* d_iperm = nullptr;    // inverse: element e sits at position iperm[e]
     float2* d_tw = nullptr;    // e^{-2 pi i t / n}, t < n (FP64-computed)
 };
 

@@ -37,6 +37,7 @@ struct PairParams {
     float rc2, rc;
     float beta, beta2, beta3;
     float gp[6];  // beta^3 x numerator coefficients of the Ewald rational (sb_ewald.cuh)
+    int wide;     // (beta rc)^2 > 12: in-cutoff pairs can leave the rational's fitted range
     int nt;
     int slot_cap;
     int ent_cap;
@@ -270,6 +271,8 @@ static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list
     const double pc[6] = {SB_EWALD_P5, SB_EWALD_P4, SB_EWALD_P3,
                           SB_EWALD_P2, SB_EWALD_P1, SB_EWALD_P0};
     for (int k = 0; k < 6; k++) P.gp[k] = (float)(b3 * pc[k]);
+    const double brc = (double)beta * lj->cutoff;
+    P.wide = brc * brc > 11.9;
     P.nt = lj->ntypes;
     P.slot_cap = nl->slot_cap;
     P.ent_cap = nl->ent_cap;

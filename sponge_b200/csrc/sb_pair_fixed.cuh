@@ -16,7 +16,7 @@ struct PairLane {
     static constexpr int EPW = 32 / LPE;          // entries per warp iteration
 };
 
-template <int EV, bool EXACT, int IPL>
+template <int EV, bool EXACT, int IPL, bool WIDE>
 __device__ __forceinline__ void pair_walk(
     const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
     const uint4* __restrict__ xq, const int* __restrict__ stype, const float2* sAB,
@@ -64,7 +64,9 @@ __device__ __forceinline__ void pair_walk(
             const float2 ab = sAB[ti[k] + tj];
             const float flj = (ab.y - ab.x * ri6) * (ri6 * ri2);
             const float qq = qi[k] * qj;
-            const float fc = qq * (ri * ri2 - sb_ewald_G_scaled(P.beta2 * r2, P.gp));
+            const float bg = WIDE ? sb_ewald_G_scaled(P.beta2 * r2, P.gp)
+                                  : sb_ewald_G_rational(P.beta2 * r2, P.gp);
+            const float fc = qq * (ri * ri2 - bg);
             const float fs = act ? flj - fc : 0.f;
             fxi[k] = fmaf(fs, dx, fxi[k]);
             fyi[k] = fmaf(fs, dy, fyi[k]);
@@ -139,12 +141,24 @@ __global__ void __launch_bounds__(128) k_pair_fixed(
     const int cntf = cl_count[c];
     const int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
     const uint32_t* ents = cl_ent + (size_t)c * P.ent_cap;
-    if (cntf & SB_CL_EXACT)
-        pair_walk<EV, true, IPL>(P, cnt, ents, xq, stype, sAB, fix, base, h, eslot, rx, ry, rz,
-                                 xi, yi, zi, qi, ti, fxi, fyi, fzi, ei, vi, di);
-    else
-        pair_walk<EV, false, IPL>(P, cnt, ents, xq, stype, sAB, fix, base, h, eslot, rx, ry, rz,
-                                  xi, yi, zi, qi, ti, fxi, fyi, fzi, ei, vi, di);
+    // (beta rc)^2 > 12 ("wide") needs the exact Ewald expression beyond the fitted range; the
+    // common case runs the branch-free rational so the IPL pair chains interleave
+    if (P.wide) {
+        if (cntf & SB_CL_EXACT)
+            pair_walk<EV, true, IPL, true>(P, cnt, ents, xq, stype, sAB, fix, base, h, eslot, rx,
+                                           ry, rz, xi, yi, zi, qi, ti, fxi, fyi, fzi, ei, vi, di);
+        else
+            pair_walk<EV, false, IPL, true>(P, cnt, ents, xq, stype, sAB, fix, base, h, eslot, rx,
+                                            ry, rz, xi, yi, zi, qi, ti, fxi, fyi, fzi, ei, vi, di);
+    } else {
+        if (cntf & SB_CL_EXACT)
+            pair_walk<EV, true, IPL, false>(P, cnt, ents, xq, stype, sAB, fix, base, h, eslot, rx,
+                                            ry, rz, xi, yi, zi, qi, ti, fxi, fyi, fzi, ei, vi, di);
+        else
+            pair_walk<EV, false, IPL, false>(P, cnt, ents, xq, stype, sAB, fix, base, h, eslot,
+                                             rx, ry, rz, xi, yi, zi, qi, ti, fxi, fyi, fzi, ei, vi,
+                                             di);
+    }
 
     // reduce over the lanes that hold the same i atoms (same h); lanes 0..LPE-1 end with totals
 #pragma unroll
