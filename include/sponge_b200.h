@@ -57,6 +57,7 @@ extern "C" {
 typedef struct sb_neighbor_list sb_neighbor_list;
 typedef struct sb_lennard_jones sb_lennard_jones;
 typedef struct sb_pme sb_pme;
+typedef struct sb_adjoint sb_adjoint;
 
 /* Library version (integer) and the message of the last failed call on this host thread. */
 SB_API int sb_version(void);
@@ -228,6 +229,39 @@ SB_API int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme*
  * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */
 SB_API int sb_crd_to_uint_crd(int atom_numbers, const float box_length[3], const float* d_crd,
                        uint32_t* d_uint_crd, void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Differentiation for force-field fitting (no reference counterpart: SPONGE has no gradients
+ * with respect to parameters). Fixed-point form of all three modules only.
+ * ---------------------------------------------------------------------------------------- */
+
+/* Parameter update for fitting: replaces the LJ pair tables (same layout and scaling as
+ * sb_lj_create: lower-triangular, already x12 and x6) and recomputes the long-range correction
+ * factor. The atom types are unchanged. Copies from the host (synchronous). */
+SB_API int sb_lj_set_tables(sb_lennard_jones* lj, const float* h_LJ_A, const float* h_LJ_B);
+
+/* Adjoint context for one set of modules (scratch sized from them; re-create it after any of
+ * the modules is re-created). */
+SB_API int sb_adjoint_create(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
+                             sb_adjoint** out);
+SB_API int sb_adjoint_destroy(sb_adjoint* adj);
+
+/* Jacobian-vector product of the nonbonded energy E and forces F (the sum of what the LJ,
+ * long-range-correction, exclusion and reciprocal calls produce) at d_uint_crd with the current
+ * list of nl: for L with dL/dE = grad_energy and dL/dF = d_grad_frc [3N] float, writes
+ *   d_grad_crd    [3N] double  dL/dx in (unit of L)/A
+ *   d_grad_charge [N]  double  dL/dq per atom (charges in the module's scaled units)
+ *   d_grad_lj     [2 * ntypes^2] double  dL/dA12 then dL/dB6, square [type_i][type_j] tables
+ *                 of the scaled values A*12, B*6; an entry (a, b) collects the half-list pairs
+ *                 whose first atom has type a, so a symmetric table's gradient is g[a][b] +
+ *                 g[b][a] (a != b)
+ * Outputs are overwritten. The list must be current for d_uint_crd (as for the force calls). */
+SB_API int sb_adjoint_backward(sb_adjoint* adj, sb_neighbor_list* nl, sb_lennard_jones* lj,
+                               sb_pme* pme, const uint32_t* d_uint_crd, const float* d_charge,
+                               const int* d_excluded_list_start, const int* d_excluded_list,
+                               const int* d_excluded_numbers, double grad_energy,
+                               const float* d_grad_frc, double* d_grad_crd,
+                               double* d_grad_charge, double* d_grad_lj, void* stream);
 
 #ifdef __cplusplus
 }

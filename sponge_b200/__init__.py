@@ -70,6 +70,11 @@ _SIGS = {
     "sb_nonbonded_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp,
                           _vp, _vp, _vp],
     "sb_crd_to_uint_crd": [_i, _vp, _vp, _vp, _vp],
+    "sb_lj_set_tables": [_vp, _vp, _vp],
+    "sb_adjoint_create": [_vp, _vp, _vp, _vp],
+    "sb_adjoint_destroy": [_vp],
+    "sb_adjoint_backward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp,
+                            _vp, _vp, _vp, _vp],
 }
 
 

@@ -121,6 +121,7 @@ def _finish(crd, charge_e, lj_type, sig, eps, excl, box, cutoff, skin, fft, tole
         lj_type=np.asarray(lj_type, np.int32),
         n_types=len(sig),
         lj_A=A, lj_B=B,
+        lj_sigma=np.asarray(sig, np.float64), lj_eps=np.asarray(eps, np.float64),
         excl_start=start.astype(np.int32), excl_numbers=numbers.astype(np.int32),
         excl_list=lst.astype(np.int32),
         box=box, cutoff=float(cutoff), skin=float(skin),
@@ -239,6 +240,30 @@ def config3(seed=1003):
     10.5 A sphere: 3,200 atoms, rc 8, skin 2, PME 32^3 (differentiation case)."""
     return _solvated(200, 10.5, 1000, 31.04, 12, seed, 8.0, 2.0, (32, 32, 32),
                      name="water_solute3k_pme32")
+
+
+def config3_fit(n_frames=16, seed=1003, jitter=0.05, noise=0.05):
+    """Force-field fitting workload on the config-3 system.
+
+    Returns (system, frames, target) where ``frames`` are ``n_frames`` seeded configurations
+    (the base coordinates with independent Gaussian displacements of ``jitter`` A per
+    coordinate, wrapped into the box) and ``target`` holds the parameter set the target
+    energies and forces are computed with: per-type sigma/epsilon and per-atom charges each
+    multiplied by (1 + ``noise`` N(0, 1)), seeded."""
+    s = config3(seed)
+    rng = np.random.default_rng(seed + 5000)
+    box = np.asarray(s["box"], np.float64)
+    frames = []
+    for _ in range(n_frames):
+        c = s["crd"].astype(np.float64) + rng.normal(0.0, jitter, s["crd"].shape)
+        c = np.mod(c, box)
+        c = np.where(c >= box, 0.0, c)
+        frames.append(c.astype(np.float32))
+    sig = s["lj_sigma"] * (1.0 + noise * rng.normal(size=s["lj_sigma"].shape))
+    eps = s["lj_eps"] * (1.0 + noise * rng.normal(size=s["lj_eps"].shape))
+    q = s["charge"].astype(np.float64) * (1.0 + noise * rng.normal(size=s["charge"].shape))
+    target = dict(lj_sigma=sig, lj_eps=eps, charge=q.astype(np.float32))
+    return s, frames, target
 
 
 def small_water(n_side=4, spacing=3.104, seed=7, cutoff=5.0, skin=1.0, fft=(16, 16, 16)):
