@@ -76,8 +76,8 @@ def _function():
             if model._key != ctx.key:
                 model._forward(crd, charge, A, B, force_eval=False)
             g_crd, g_q, g_A, g_B = model._backward(gE, gF)
-            return (g_crd.to(crd.dtype), g_q.to(charge.dtype), g_A.to(A.dtype),
-                    g_B.to(B.dtype), None)
+            return (g_crd.to(crd.device, crd.dtype), g_q.to(charge.device, charge.dtype),
+                    g_A.to(A.device, A.dtype), g_B.to(B.device, B.dtype), None)
 
     _NonbondedFunction.cls = NonbondedFunction
     return NonbondedFunction

@@ -32,6 +32,8 @@
 #define SB_CL_COUNT_MASK 0xffffff
 #define SB_MAX_SLOTS (1 << 24)  // slot index must fit 24 bits of a list entry
 #define SB_COLUMN_SORT_CAP 4096 // max atoms per sort column (bitonic sort in shared memory)
+#define SB_ZBIN_SHIFT 25        // z bins per column: the top 7 bits of the fixed-point z
+#define SB_ZBINS (1 << (32 - SB_ZBIN_SHIFT))
 #define SB_MAX_RADIX 8
 #define SB_FFT_MAX_STAGES 12
 
@@ -135,6 +137,7 @@ struct sb_neighbor_list {
     uint32_t* slot_u = nullptr;     // [3*slot_cap] fixed-point coordinates at build, slot order
     int* excl_lo = nullptr;         // [N] min / max exclusion partner (INT_MAX / -1 if none)
     int* excl_hi = nullptr;
+    int* zbin = nullptr;            // [ncol][SB_ZBINS+1] first slot of each z bin of a column
     int* cl_count = nullptr;        // [clu_cap]
     uint32_t* cl_ent = nullptr;     // [clu_cap * ent_cap]
     int* meta = nullptr;            // [0] clusters, [1] status flags, [2] refresh flag,

@@ -8,9 +8,10 @@
 //   2. k_colscan   padded exclusive scan: every column starts on a multiple of 8 slots.
 //   3. k_scatter   (z << 32 | atom) keys into their column.
 //   4. k_colsort   per-column bitonic sort in shared memory -> deterministic slot order
-//                  (z, atom id); writes slot_atom / atom_slot / slot-order coordinates.
+//                  (z, atom id); writes slot_atom / atom_slot / slot-order coordinates and a
+//                  per-column index of 128 z bins.
 //   5. k_search    one warp per 8-atom cluster walks the columns around it (half shell in
-//                  slot order), binary-searches the z window, and tests every candidate pair
+//                  slot order), takes the z window from the z-bin index, and tests every candidate pair
 //                  with the pinned FP32 criterion; surviving j become entries (j | mask << 24).
 //
 // The pair set represented is exactly the reference's half list: pairs within (rc+skin) under
@@ -136,7 +137,7 @@ __global__ void k_colsort(int ncol, const int* __restrict__ col_count,
                           const unsigned long long* __restrict__ tmp,
                           const uint32_t* __restrict__ ucrd, int* __restrict__ slot_atom,
                           int* __restrict__ atom_slot, uint32_t* __restrict__ slot_u,
-                          int slot_cap, int* __restrict__ meta,
+                          int slot_cap, int* __restrict__ meta, int* __restrict__ zbin,
                           const int* __restrict__ refresh_flag) {
     if (refresh_flag && refresh_flag[0] == 0) return;
     extern __shared__ unsigned long long keys[];
@@ -172,6 +173,17 @@ __global__ void k_colsort(int ncol, const int* __restrict__ col_count,
             }
             __syncthreads();
         }
+    }
+    // z-bin index of the sorted column: zbin[b] = first slot whose z >= b 2^SB_ZBIN_SHIFT
+    for (int b = threadIdx.x; b <= SB_ZBINS; b += blockDim.x) {
+        const unsigned long long zb = (unsigned long long)b << SB_ZBIN_SHIFT;
+        int lo = 0, hi = cnt;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((keys[mid] >> 32) < zb) lo = mid + 1;
+            else hi = mid;
+        }
+        zbin[(size_t)col * (SB_ZBINS + 1) + b] = start + lo;
     }
     int sz = slot_cap;
     for (int t = threadIdx.x; t < padded; t += blockDim.x) {
@@ -224,15 +236,6 @@ __device__ __forceinline__ bool excluded_pair(int a, int b, const int* __restric
     return false;
 }
 
-__device__ __forceinline__ int lower_bound_u(const uint32_t* __restrict__ z, int a, int b,
-                                             uint32_t v) {
-    while (a < b) {
-        int m = (a + b) >> 1;
-        if (z[m] < v) a = m + 1; else b = m;
-    }
-    return a;
-}
-
 struct SearchParams {
     int ncx, ncy, nxr, nyr, fullx, fully;
     float sx, sy, sz, cs2, colwx, colwy, cs, lx, ly, lz;
@@ -246,6 +249,7 @@ __global__ void __launch_bounds__(128) k_search(
     const uint32_t* __restrict__ slot_u, const int* __restrict__ slot_atom,
     const int* __restrict__ excl_lo, const int* __restrict__ excl_hi,
     const int* __restrict__ es, const int* __restrict__ en, const int* __restrict__ el,
+    const int* __restrict__ zbin,
     int* __restrict__ cl_count, uint32_t* __restrict__ cl_ent, int* __restrict__ meta,
     const int* __restrict__ refresh_flag) {
     if (refresh_flag && refresh_flag[0] == 0) return;
@@ -341,8 +345,11 @@ __global__ void __launch_bounds__(128) k_search(
             int s0 = col_start[col2];
             int s1 = s0 + col_count[col2];
             for (int w = 0; w < nwin; w++) {
-                int a = lower_bound_u(UZ, s0, s1, wa[w]);
-                int b = (wb[w] == 0xffffffffu) ? s1 : lower_bound_u(UZ, a, s1, wb[w] + 1u);
+                // candidate range from the column's z-bin index: a superset of the z window
+                // (whole bins); the exact pair test filters
+                const int* zb = zbin + (size_t)col2 * (SB_ZBINS + 1);
+                int a = max(zb[wa[w] >> SB_ZBIN_SHIFT], s0);
+                int b = min(zb[(wb[w] >> SB_ZBIN_SHIFT) + 1], s1);
                 if (col2 == col) a = max(a, base + 1);
                 for (int j0 = a; j0 < b; j0 += 32) {
                     int j = j0 + lane;
@@ -559,6 +566,8 @@ static int nl_alloc(sb_neighbor_list* nl) {
     SB_TRY(sb_malloc((void**)&nl->excl_lo, sizeof(int) * n, "excl_lo"));
     SB_TRY(sb_malloc((void**)&nl->excl_hi, sizeof(int) * n, "excl_hi"));
     SB_TRY(sb_malloc((void**)&nl->cl_count, sizeof(int) * nl->clu_cap, "cl_count"));
+    SB_TRY(sb_malloc((void**)&nl->zbin, sizeof(int) * (size_t)nl->ncol * (SB_ZBINS + 1),
+                     "z bins"));
     SB_TRY(sb_malloc((void**)&nl->cl_ent, sizeof(uint32_t) * (size_t)nl->clu_cap * nl->ent_cap,
                      "cluster list"));
     SB_TRY(sb_malloc((void**)&nl->meta, sizeof(int) * 8, "meta"));
@@ -576,7 +585,7 @@ static void nl_free(sb_neighbor_list* nl) {
     void* ps[] = {nl->old_crd, nl->ucrd, nl->col_of, nl->col_rank, nl->col_count, nl->col_start,
                   nl->sort_tmp, nl->slot_atom, nl->atom_slot, nl->slot_u, nl->excl_lo,
                   nl->excl_hi, nl->cl_count, nl->cl_ent, nl->meta, nl->xq, nl->stype, nl->fix,
-                  nl->ag, nl->ag_serial};
+                  nl->ag, nl->ag_serial, nl->zbin};
     for (void* p : ps) sb_free(p);
 }
 
@@ -651,7 +660,7 @@ static int nl_rebuild(sb_neighbor_list* nl, float* d_crd, const int* es, const i
     // sort capacity: largest power of two needed is bounded by SB_COLUMN_SORT_CAP
     k_colsort<<<nl->ncol, 256, SB_COLUMN_SORT_CAP * sizeof(unsigned long long), s>>>(
         nl->ncol, nl->col_count, nl->col_start, nl->sort_tmp, nl->ucrd, nl->slot_atom,
-        nl->atom_slot, nl->slot_u, nl->slot_cap, nl->meta, dflag);
+        nl->atom_slot, nl->slot_u, nl->slot_cap, nl->meta, nl->zbin, dflag);
     SB_CHECK_LAUNCH();
     k_excl_range<<<(n + tb - 1) / tb, tb, 0, s>>>(n, es, en, el, nl->excl_lo, nl->excl_hi, dflag);
     SB_CHECK_LAUNCH();
@@ -681,7 +690,7 @@ static int nl_rebuild(sb_neighbor_list* nl, float* d_crd, const int* es, const i
     int blocks = (nl->clu_cap + warps_per_block - 1) / warps_per_block;
     k_search<<<blocks, 32 * warps_per_block, 0, s>>>(
         P, nl->col_start, nl->col_count, nl->slot_u, nl->slot_atom, nl->excl_lo, nl->excl_hi,
-        es, en, el, nl->cl_count, nl->cl_ent, nl->meta, dflag);
+        es, en, el, nl->zbin, nl->cl_count, nl->cl_ent, nl->meta, dflag);
     SB_CHECK_LAUNCH();
     nl->ag_valid = 0;
     nl->build_id++;
