@@ -209,6 +209,25 @@ SB_API int sb_pme_get_energy(sb_pme* pme, sb_neighbor_list* nl, const uint32_t* 
                       const int* d_excluded_numbers, int which_part, float* h_energy,
                       double* h_parts, void* stream);
 
+/* Allocation-free variant of sb_pme_get_energy (no counterpart in the reference). Same
+ * arguments and results. sb_pme_get_energy allocates and frees a 3N-float array on every call
+ * for the forces its reciprocal and exclusion passes produce and then discard; this variant uses
+ * a fixed 1.5 MiB device block that the library reserves when it is loaded, for callers that
+ * cannot allocate: programs whose device memory is all handed to their own pool allocator, and
+ * loops that must not pay for cudaFree, which waits for the whole device.
+ *   - at most 131072 atoms (larger modules are rejected with SB_ERR_ARG);
+ *   - the first call on each device looks up the block's device address (with that device
+ *     current); make that first call before beginning any stream capture;
+ *   - the DIRECT part (and TOTAL) reads the list's ATOM_GROUP export, which allocates on first
+ *     use: call sb_nl_atom_group once beforehand, or the call fails with SB_ERR_STATE;
+ *   - every call on a device shares the one block: calls whose GPU work overlaps (other streams,
+ *     other host threads) race on it. Each call clears the part it uses before use. */
+SB_API int sb_pme_get_energy_noalloc(sb_pme* pme, sb_neighbor_list* nl,
+                      const uint32_t* d_uint_crd, const float* d_charge, const float scaler[3],
+                      const int* d_excluded_list_start, const int* d_excluded_list,
+                      const int* d_excluded_numbers, int which_part, float* h_energy,
+                      double* h_parts, void* stream);
+
 /* Particle_Mesh_Ewald::Update_Box_Length / Update_Volume (PME_force.cu:996-1042) */
 SB_API int sb_pme_update_box(sb_pme* pme, const float box_length[3]);
 

@@ -66,6 +66,7 @@ _SIGS = {
     "sb_pme_excluded_force": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "sb_pme_reciprocal_force": [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
     "sb_pme_get_energy": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp],
+    "sb_pme_get_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp],
     "sb_pme_update_box": [_vp, _vp],
     "sb_nonbonded_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp,
                           _vp, _vp, _vp],

@@ -17,6 +17,7 @@
 #include <stdio.h>
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "sb_ewald.cuh"
@@ -691,6 +692,144 @@ extern "C" int sb_pme_get_energy(sb_pme* p, sb_neighbor_list* nl, const uint32_t
         sb_set_error("sb_pme_get_energy: %s", cudaGetErrorString(e));
         return SB_ERR_CUDA;
     }
+    const double rec = parts[0], self = parts[1], dir = parts[2], cor = parts[3];
+    const double tot = rec + self + dir + cor;
+    double v = tot;
+    switch (which_part) {
+        case SB_PME_DIRECT: v = dir; break;
+        case SB_PME_RECIPROCAL: v = rec; break;
+        case SB_PME_CORRECTION: v = cor; break;
+        case SB_PME_SELF: v = self; break;
+        default: break;
+    }
+    if (h_energy) *h_energy = (float)v;
+    if (h_parts) {
+        h_parts[0] = tot;
+        h_parts[1] = dir;
+        h_parts[2] = rec;
+        h_parts[3] = cor;
+        h_parts[4] = self;
+    }
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free energy query
+//
+// sb_pme_get_energy needs a 3N-float force array to run the reciprocal and exclusion passes
+// (their forces are thrown away; only the energies are kept) and obtains it with cudaMalloc /
+// cudaFree on every call. Some callers cannot do that: a host program whose device memory is
+// fully handed to its own pool allocator, or a driver loop that must not pay for cudaFree, which
+// waits for the whole device. sb_pme_get_energy_noalloc takes that array from a fixed block of
+// device memory that this library reserves at load time instead.
+// ---------------------------------------------------------------------------------------------
+#define SB_NOALLOC_MAX_ATOMS 131072  // 3 x 131072 floats = 1.5 MiB, held by every GPU that loads
+                                     // the library until the process exits
+#define SB_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) float g_noalloc_frc[3 * SB_NOALLOC_MAX_ATOMS];
+
+// Host code may not hand g_noalloc_frc itself to a kernel (on the host it only names a stand-in
+// object); its device address is looked up once per device, with that device current.
+static float* g_noalloc_frc_addr[SB_NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(float** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        sb_set_error("sb_pme_get_energy_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+        return SB_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= SB_NOALLOC_MAX_DEVICES) {
+        sb_set_error("sb_pme_get_energy_noalloc: device %d is beyond the %d devices supported", dev,
+                     SB_NOALLOC_MAX_DEVICES);
+        return SB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_frc_addr[dev]) {
+        void* addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_noalloc_frc);
+        if (e != cudaSuccess || !addr) {
+            sb_set_error("sb_pme_get_energy_noalloc: cudaGetSymbolAddress failed: %s",
+                         cudaGetErrorString(e));
+            return SB_ERR_CUDA;
+        }
+        g_noalloc_frc_addr[dev] = (float*)addr;
+    }
+    *out = g_noalloc_frc_addr[dev];
+    return SB_OK;
+}
+
+extern "C" int sb_pme_get_energy_noalloc(sb_pme* p, sb_neighbor_list* nl,
+                                         const uint32_t* d_uint_crd, const float* d_charge,
+                                         const float scaler[3], const int* es, const int* el,
+                                         const int* en, int which_part, float* h_energy,
+                                         double* h_parts, void* stream) {
+    if (!p || !d_uint_crd || !d_charge || !scaler) {
+        sb_set_error("sb_pme_get_energy_noalloc: null argument");
+        return SB_ERR_ARG;
+    }
+    if (which_part < 0 || which_part > 4) {
+        sb_set_error("sb_pme_get_energy_noalloc: energy part %d is not allowed", which_part);
+        return SB_ERR_ARG;
+    }
+    const int n = p->n;
+    if (n > SB_NOALLOC_MAX_ATOMS) {
+        sb_set_error("sb_pme_get_energy_noalloc: %d atoms exceed the maximum of %d; use "
+                     "sb_pme_get_energy", n, SB_NOALLOC_MAX_ATOMS);
+        return SB_ERR_ARG;
+    }
+    const int all = which_part == SB_PME_TOTAL;
+    const int want_rec = all || which_part == SB_PME_RECIPROCAL;
+    const int want_dir = all || which_part == SB_PME_DIRECT;
+    const int want_cor = all || which_part == SB_PME_CORRECTION;
+    if (want_dir) {
+        if (!nl) {
+            sb_set_error("sb_pme_get_energy_noalloc: the DIRECT part needs the neighbor list");
+            return SB_ERR_ARG;
+        }
+        if (!nl->ag) {
+            // the list's ATOM_GROUP export is allocated on its first use
+            sb_set_error("sb_pme_get_energy_noalloc: the DIRECT part reads the list's ATOM_GROUP "
+                         "export, which allocates on first use; call sb_nl_atom_group once first");
+            return SB_ERR_STATE;
+        }
+    }
+    float* scratch = nullptr;
+    SB_TRY(noalloc_scratch(&scratch));
+    cudaStream_t s = sb_stream(stream);
+    // the thrown-away forces accumulate here: clear the part this call uses
+    if (want_rec || want_cor)
+        SB_CHECK_CUDA(cudaMemsetAsync(scratch, 0, sizeof(float) * 3 * n, s));
+    int nparts = 0;
+    if (want_rec) SB_TRY(reciprocal(p, d_uint_crd, d_charge, scratch, 1, s, &nparts));
+    float* direct = nullptr;
+    float* corr = nullptr;
+    if (want_dir) {
+        SB_TRY(sb_nl_build_atom_group(nl, s));
+        k_direct_energy_list<<<(n + 127) / 128, 128, 0, s>>>(n, nl->ag, d_uint_crd, d_charge,
+                                                             scaler[0], scaler[1], scaler[2],
+                                                             p->beta, p->cutoff * p->cutoff,
+                                                             p->d_direct_atom_energy);
+        SB_CHECK_LAUNCH();
+        direct = p->d_direct_atom_energy;
+    }
+    if (want_cor) {
+        k_zero_f<<<(n + 1023) / 1024, 1024, 0, s>>>(n, p->d_correction_atom_energy);
+        SB_CHECK_LAUNCH();
+        if (es && el && en)
+            SB_TRY(excluded_force(p, d_uint_crd, scaler, d_charge, es, el, en, scratch,
+                                  p->d_correction_atom_energy, s));
+        corr = p->d_correction_atom_energy;
+    }
+    k_pme_energy_finish<<<1, 1024, 0, s>>>(n, d_charge, p->d_epart, nparts, direct, corr,
+                                           (double)p->beta, p->neutralizing_factor, p->d_ered, 0,
+                                           0, nullptr, nullptr);
+    SB_CHECK_LAUNCH();
+    double parts[4] = {0, 0, 0, 0};
+    SB_CHECK_CUDA(cudaMemcpyAsync(parts, p->d_ered, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+    SB_CHECK_CUDA(cudaStreamSynchronize(s));
     const double rec = parts[0], self = parts[1], dir = parts[2], cor = parts[3];
     const double tot = rec + self + dir + cor;
     double v = tot;
