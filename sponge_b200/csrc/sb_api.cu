@@ -73,6 +73,23 @@ extern "C" int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_
     float* d_direct = nullptr;
     float* d_corr = nullptr;
     SB_TRY(sb_pme_atom_energy_arrays(pme, &d_direct, &d_corr));
+    if (lj->form == SB_FORM_FIXED && pme->form == SB_FORM_FIXED && nl->form == SB_FORM_FIXED &&
+        lj->n == nl->n && pme->n == nl->n) {
+        // fused fixed form: pair and exclusion forces meet in the list's slot-order fixed-point
+        // buffer; the reciprocal gather finalises it into d_frc
+        SB_TRY(sb_nl_ensure_built(nl));
+        cudaStream_t s = sb_stream(stream);
+        const int ev = need_energy > 0 || need_virial > 0;
+        SB_TRY(sb_lj_fused_direct(lj, nl, d_uint_crd, d_charge, pme->beta, need_energy,
+                                  d_atom_energy, need_virial, d_atom_virial, d_direct, s));
+        SB_TRY(sb_lj_long_range_correction(lj, need_virial, d_virial, need_energy, d_potential,
+                                           stream));
+        // the per-atom correction energy is only read on energy/virial steps
+        SB_TRY(sb_pme_fused_excluded(pme, nl, d_uint_crd, d_charge, es, el, en,
+                                     ev ? d_corr : nullptr, s));
+        return sb_pme_fused_reciprocal(pme, nl, d_frc, d_charge, need_virial, need_energy,
+                                       d_virial, d_potential, s);
+    }
     SB_TRY(sb_lj_pme_direct_force(lj, nl, lj->n, d_uint_crd, d_charge, d_frc, pme->beta,
                                   need_energy, d_atom_energy, need_virial, d_atom_virial,
                                   d_direct, stream));

@@ -206,6 +206,20 @@ int sb_nl_pack(sb_neighbor_list* nl, const uint32_t* d_uint_crd, const float* d_
 int sb_nl_finalize_forces(sb_neighbor_list* nl, float* d_frc, cudaStream_t s);
 int sb_nl_build_atom_group(sb_neighbor_list* nl, cudaStream_t s);
 
+// fused fixed-form step pieces: the pair kernel and the exclusion correction accumulate into the
+// list's slot-order fixed-point buffer; the reciprocal spread reads the list's packed slot data
+// and its gather finalises the buffer into d_frc
+int sb_lj_fused_direct(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                       const float* d_charge, float pme_beta, int need_atom_energy,
+                       float* d_atom_energy, int need_virial, float* d_atom_lj_virial,
+                       float* d_atom_direct_pme_energy, cudaStream_t s);
+int sb_pme_fused_excluded(sb_pme* pme, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                          const float* d_charge, const int* es, const int* el, const int* en,
+                          float* d_atom_energy, cudaStream_t s);
+int sb_pme_fused_reciprocal(sb_pme* pme, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
+                            int need_virial, int need_energy, float* d_virial, float* d_potential,
+                            cudaStream_t s);
+
 // FP64 reduction helpers (deterministic: fixed block/thread order)
 int sb_reduce_sum_f32(const float* d_x, int n, double* d_out, cudaStream_t s);
 

@@ -714,6 +714,205 @@ extern "C" int sb_pme_get_energy(sb_pme* p, sb_neighbor_list* nl, const uint32_t
 }
 
 // ---------------------------------------------------------------------------------------------
+// fused fixed-form step: slot-order kernels sharing the neighbor list's packed data and its
+// fixed-point force buffer (x, y, z planes of slot_cap int64 each)
+// ---------------------------------------------------------------------------------------------
+
+// exclusion correction as k_excluded<true>, accumulating at the atoms' slots
+__global__ void k_excluded_slot(int n, const uint32_t* __restrict__ uc, float sx, float sy,
+                                float sz, const float* __restrict__ q, float beta2, float beta3,
+                                float beta, const int* __restrict__ es,
+                                const int* __restrict__ el, const int* __restrict__ en,
+                                const int* __restrict__ atom_slot, int slot_cap,
+                                long long* __restrict__ fix, float* __restrict__ ene) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int cnt = en[i];
+    if (cnt <= 0) return;
+    const int s0 = es[i];
+    const uint32_t ux = uc[3 * i], uy = uc[3 * i + 1], uz = uc[3 * i + 2];
+    const float qi = q[i];
+    float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f;
+    for (int k = s0; k < s0 + cnt; k++) {
+        const int j = el[k];
+        const float dx = __int2float_rn((int)(uc[3 * j] - ux)) * sx;
+        const float dy = __int2float_rn((int)(uc[3 * j + 1] - uy)) * sy;
+        const float dz = __int2float_rn((int)(uc[3 * j + 2] - uz)) * sz;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float qq = qi * q[j];
+        const float fs = qq * beta3 * sb_ewald_G(beta2 * r2);
+        const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
+        fx += tx;
+        fy += ty;
+        fz += tz;
+        if (ene) {
+            const float r = sqrtf(r2);
+            e -= qq * erff(beta * r) / r;
+        }
+        const int sj = atom_slot[j];
+        atomicAdd((unsigned long long*)&fix[sj], (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
+        atomicAdd((unsigned long long*)&fix[slot_cap + sj], (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
+        atomicAdd((unsigned long long*)&fix[2 * slot_cap + sj], (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
+    }
+    const int si = atom_slot[i];
+    atomicAdd((unsigned long long*)&fix[si], (unsigned long long)__float2ll_rn(fx * SB_FORCE_SCALE));
+    atomicAdd((unsigned long long*)&fix[slot_cap + si], (unsigned long long)__float2ll_rn(fy * SB_FORCE_SCALE));
+    atomicAdd((unsigned long long*)&fix[2 * slot_cap + si], (unsigned long long)__float2ll_rn(fz * SB_FORCE_SCALE));
+    if (ene) atomicAdd(&ene[i], e);
+}
+
+// charge spread from the packed slot data {ux, uy, uz, q}; 4 threads per slot (x offset)
+__global__ void k_spread_slot(const int* __restrict__ meta, const uint4* __restrict__ xq, int K0,
+                              int K1, int K2, long long* __restrict__ gfix) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int sl = gt >> 2, kx = gt & 3;
+    if (sl >= meta[3]) return;
+    const uint4 v = xq[sl];
+    const float q = __uint_as_float(v.w);
+    if (q == 0.f) return;  // padding slots and uncharged atoms add nothing
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(v.x, K0, b0, f0);
+    grid_coord(v.y, K1, b1, f1);
+    grid_coord(v.z, K2, b2, f2);
+    float wx[4], wy[4], wz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    const float qw = q * wx[kx];
+    int gx = b0 - kx;
+    if (gx < 0) gx += K0;
+    const size_t rowx = (size_t)gx * K1;
+#pragma unroll
+    for (int ky = 0; ky < 4; ky++) {
+        int gy = b1 - ky;
+        if (gy < 0) gy += K1;
+        const size_t row = (rowx + gy) * K2;
+        const float qwy = qw * wy[ky];
+#pragma unroll
+        for (int kz = 0; kz < 4; kz++) {
+            int gz = b2 - kz;
+            if (gz < 0) gz += K2;
+            const long long f = __float2ll_rn(qwy * wz[kz] * SB_GRID_SCALE);
+            if (f) atomicAdd((unsigned long long*)&gfix[row + gz], (unsigned long long)f);
+        }
+    }
+}
+
+// reciprocal force gather per slot, fused with the conversion of the slot's fixed-point
+// accumulators (pair + exclusion forces) into the caller's float forces; clears the buffer
+__global__ void k_gather_finalize(const int* __restrict__ meta, const int* __restrict__ slot_atom,
+                                  const uint4* __restrict__ xq, const float* __restrict__ theta,
+                                  int K0, int K1, int K2, float ix, float iy, float iz,
+                                  long long* __restrict__ fix, int slot_cap,
+                                  float* __restrict__ frc) {
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= meta[3]) return;
+    const long long ax = fix[sl], ay = fix[slot_cap + sl], az = fix[2 * slot_cap + sl];
+    if (ax | ay | az) {
+        fix[sl] = 0;
+        fix[slot_cap + sl] = 0;
+        fix[2 * slot_cap + sl] = 0;
+    }
+    const int a = slot_atom[sl];
+    if (a < 0) return;
+    const uint4 v = xq[sl];
+    const float q = __uint_as_float(v.w);
+    float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+    if (q != 0.f) {
+        int b0, b1, b2;
+        float f0, f1, f2;
+        grid_coord(v.x, K0, b0, f0);
+        grid_coord(v.y, K1, b1, f1);
+        grid_coord(v.z, K2, b2, f2);
+        float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+        bspline4(f0, wx);
+        bspline4(f1, wy);
+        bspline4(f2, wz);
+        bspline4d(f0, dx);
+        bspline4d(f1, dy);
+        bspline4d(f2, dz);
+        int gz[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int g = b2 - k;
+            gz[k] = g < 0 ? g + K2 : g;
+        }
+#pragma unroll
+        for (int kx = 0; kx < 4; kx++) {
+            int gx = b0 - kx;
+            if (gx < 0) gx += K0;
+#pragma unroll
+            for (int ky = 0; ky < 4; ky++) {
+                int gy = b1 - ky;
+                if (gy < 0) gy += K1;
+                const float* row = theta + ((size_t)gx * K1 + gy) * K2;
+                float sw = 0.f, sd = 0.f;
+#pragma unroll
+                for (int kz = 0; kz < 4; kz++) {
+                    const float t = row[gz[kz]];
+                    sw = fmaf(t, wz[kz], sw);
+                    sd = fmaf(t, dz[kz], sd);
+                }
+                Fx = fmaf(dx[kx] * wy[ky], sw, Fx);
+                Fy = fmaf(wx[kx] * dy[ky], sw, Fy);
+                Fz = fmaf(wx[kx] * wy[ky], sd, Fz);
+            }
+        }
+    }
+    const float sq = -q;
+    frc[3 * a] += (float)((double)ax * SB_FORCE_UNSCALE) + sq * Fx * ix;
+    frc[3 * a + 1] += (float)((double)ay * SB_FORCE_UNSCALE) + sq * Fy * iy;
+    frc[3 * a + 2] += (float)((double)az * SB_FORCE_UNSCALE) + sq * Fz * iz;
+}
+
+int sb_pme_fused_excluded(sb_pme* p, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                          const float* d_charge, const int* es, const int* el, const int* en,
+                          float* d_atom_energy, cudaStream_t s) {
+    const int n = p->n;
+    if (d_atom_energy) {
+        k_zero_f<<<(n + 1023) / 1024, 1024, 0, s>>>(n, d_atom_energy);
+        SB_CHECK_LAUNCH();
+    }
+    if (!es || !el || !en) return SB_OK;
+    const float b = p->beta;
+    const float sx = (1.0f / 4294967296.0f) * p->box[0], sy = (1.0f / 4294967296.0f) * p->box[1],
+                sz = (1.0f / 4294967296.0f) * p->box[2];
+    k_excluded_slot<<<(n + 127) / 128, 128, 0, s>>>(n, d_uint_crd, sx, sy, sz, d_charge, b * b,
+                                                    b * b * b, b, es, el, en, nl->atom_slot,
+                                                    nl->slot_cap, nl->fix, d_atom_energy);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+int sb_pme_fused_reciprocal(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
+                            int need_virial, int need_energy, float* d_virial, float* d_potential,
+                            cudaStream_t s) {
+    const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
+    const int want = need_virial > 0 || need_energy > 0;
+    int nparts = 0;
+    k_spread_slot<<<(4 * nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->meta, nl->xq, K0, K1, K2,
+                                                                 p->d_qfix);
+    SB_CHECK_LAUNCH();
+    SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
+    SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want, s, &nparts));
+    SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+    k_gather_finalize<<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
+        nl->meta, nl->slot_atom, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
+        (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, d_frc);
+    SB_CHECK_LAUNCH();
+    if (want) {
+        k_pme_energy_finish<<<1, 1024, 0, s>>>(p->n, d_charge, p->d_epart, nparts,
+                                               p->d_direct_atom_energy,
+                                               p->d_correction_atom_energy, (double)p->beta,
+                                               p->neutralizing_factor, p->d_ered, need_virial > 0,
+                                               need_energy > 0, d_virial, d_potential);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Allocation-free energy query
 //
 // sb_pme_get_energy needs a 3N-float force array to run the reciprocal and exclusion passes
