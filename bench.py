@@ -201,6 +201,9 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     eng.update_list(forced=1)
     eng.to_uint()
+    # autotuner: time each pair-kernel shape on this list and keep the fastest
+    pair_shape = eng.lj.tune(eng.nl, eng.uint_crd, eng.charge, eng.pme.beta) \
+        if form == FORM_FIXED else None
 
     def one_step():
         eng.frc.zero_()
@@ -286,7 +289,7 @@ def main():
         "dtype": "f32 pair math, int64 fixed-point accumulation, f64 energies" if form == FORM_FIXED
                  else "f32 float atomics",
         "data": "synthetic (seeded generator, sponge_b200.systems.config1)",
-        "config": dict(workload_config(), form=args.form),
+        "config": dict(workload_config(), form=args.form, pair_kernel_shape=pair_shape),
         "e2e": {"value": world * ns_per_day(e2e_step_ms * 1e-3), "unit": "ns/day",
                 "h2d_bytes_per_step": int(eng.n * 12), "d2h_bytes_per_step": int(eng.n * 12)},
         "gpu_launches": int(round(args.steps * (launches_force + launches_rebuild * rebuilds_per_step))),

@@ -153,7 +153,9 @@ SB_API int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[3]);
 
 /* Pair-kernel shape of the fixed-point form (no reference counterpart; a tuning knob):
  * i atoms held per lane, 8 (one lane per list entry) or 4 (two lanes per entry, fewer registers,
- * more resident warps). Results are identical to FP32 rounding either way. */
+ * more resident warps), or 1: the compacted kernel, which first filters each batch of entries to
+ * the pairs inside the cutoff and then evaluates one such pair per lane. Results are identical to
+ * FP32 rounding whichever shape runs. */
 SB_API int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane);
 
 /* Autotuner: times each pair-kernel shape on the current list and keeps the fastest; writes the

@@ -52,6 +52,7 @@ __device__ __forceinline__ void red_fix(long long* p, float v) {
 }
 
 #include "sb_pair_fixed.cuh"
+#include "sb_pair_compact.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // plain form: reference structure (warp per atom, float atomics), Lennard_Jones_force.cu:47-158
@@ -298,7 +299,24 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
             P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
             nl->slot_atom, nl->fix, ae, av, ad);                                              \
     } while (0)
-    if (lj->ipl == 4) {
+#define SB_LAUNCH_COMPACT(EVV)                                                                \
+    do {                                                                                      \
+        if (smem + sizeof(CompactSmem<EVV>) > 48 * 1024)                                      \
+            cudaFuncSetAttribute(k_pair_compact<EVV>,                                         \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+        k_pair_compact<EVV><<<(nl->clu_cap + SB_CP_WARPS - 1) / SB_CP_WARPS,                  \
+                              32 * SB_CP_WARPS, smem, s>>>(                                   \
+            P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
+            nl->slot_atom, nl->fix, ae, av, ad);                                              \
+    } while (0)
+    if (lj->ipl == 1) {
+        switch (ev) {
+            case 0: SB_LAUNCH_COMPACT(0); break;
+            case 1: SB_LAUNCH_COMPACT(1); break;
+            case 2: SB_LAUNCH_COMPACT(2); break;
+            default: SB_LAUNCH_COMPACT(3); break;
+        }
+    } else if (lj->ipl == 4) {
         switch (ev) {
             case 0: SB_LAUNCH_PAIR(0, 4); break;
             case 1: SB_LAUNCH_PAIR(1, 4); break;
@@ -314,6 +332,7 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
         }
     }
 #undef SB_LAUNCH_PAIR
+#undef SB_LAUNCH_COMPACT
     SB_CHECK_LAUNCH();
     return SB_OK;
 }
@@ -474,8 +493,8 @@ extern "C" int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[
 }
 
 extern "C" int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane) {
-    if (!lj || (atoms_per_lane != 4 && atoms_per_lane != 8)) {
-        sb_set_error("sb_lj_set_kernel_variant: atoms_per_lane must be 4 or 8");
+    if (!lj || (atoms_per_lane != 1 && atoms_per_lane != 4 && atoms_per_lane != 8)) {
+        sb_set_error("sb_lj_set_kernel_variant: atoms_per_lane must be 1, 4 or 8");
         return SB_ERR_ARG;
     }
     lj->ipl = atoms_per_lane;
@@ -495,13 +514,13 @@ extern "C" int sb_lj_tune(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint
     }
     cudaStream_t s = sb_stream(stream);
     SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
-    const int cand[2] = {4, 8};
+    const int cand[3] = {1, 4, 8};
     float best = 1e30f;
     int pick = lj->ipl;
     cudaEvent_t a, b;
     SB_CHECK_CUDA(cudaEventCreate(&a));
     SB_CHECK_CUDA(cudaEventCreate(&b));
-    for (int c = 0; c < 2; c++) {
+    for (int c = 0; c < 3; c++) {
         lj->ipl = cand[c];
         SB_TRY(launch_pair_fixed(lj, nl, pme_beta, 0, nullptr, nullptr, nullptr, s));
         SB_CHECK_CUDA(cudaEventRecord(a, s));
