@@ -32,9 +32,12 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 DT_FS = 2.0
-FLOP_PER_PAIR = 50.0       # in-cutoff pair (SURVEY-derived breakdown)
+FLOP_PER_PAIR = 50.0       # in-cutoff pair: dr 3, r^2 5, rsqrt 1, powers 4, LJ 3, Ewald 26, scale 3, accumulate 6
 FLOP_PER_CANDIDATE = 10.0  # list pair beyond the cutoff
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal at max SM clock
+# DRAM bytes read + written by one launch of the pair kernel on this workload, from an ncu
+# capture (profiles/k_pair_fixed_solvated96k.md): the list plus the packed coordinates
+PAIR_DRAM_BYTES = 32.63e6
 
 
 def ns_per_day(sec_per_step):
@@ -273,7 +276,7 @@ def main():
     flops = FLOP_PER_PAIR * n_cut + FLOP_PER_CANDIDATE * (n_list - n_cut)
     achieved = flops / (pair_ms * 1e-3) / 1e12
     rebuilds_per_step = 1.0 / 20
-    launches_force = 11
+    launches_force = 10  # pack, pair, exclusion, spread, 5 FFT passes, gather+finalize
     launches_rebuild = 6
     line = {
         "metric": METRIC,
@@ -294,7 +297,7 @@ def main():
                 "h2d_bytes_per_step": int(eng.n * 12), "d2h_bytes_per_step": int(eng.n * 12)},
         "gpu_launches": int(round(args.steps * (launches_force + launches_rebuild * rebuilds_per_step))),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
-                     "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": PAIR_DRAM_BYTES,
                      "kernel": "k_pair_fixed (LJ + Ewald direct; timed with its pack/finalize)",
                      "kernel_ms": pair_ms, "pairs_in_cutoff": n_cut, "pairs_in_list": n_list,
                      "peak_note": "nominal FP32 peak 148 SM x 128 lanes x 2 x 1.965 GHz"},
