@@ -725,4 +725,167 @@ long orc_nonbonded(int n, const uint32_t* uc, const float* q, const int* type, c
     return np;
 }
 
+// ------------------------------------------------------------------------------------------
+// FEP / TI: soft-core LJ + direct Coulomb (LJ_soft_core.cu:159-317 forces, :320-664 energies,
+// :1137-1283 dH/dlambda) and the TI cross terms of PME (TI_core.cu:670-730)
+// ------------------------------------------------------------------------------------------
+
+// Over a half pair list, at coupling lambda: forces (accumulated into frc) and
+// out[0] = E_LJ, out[1] = E_direct_coulomb, out[2] = dH/dlambda (LJ), out[3] = dH/dlambda
+// (direct Coulomb, including the charge change dq = q_B - q_A at fixed geometry).
+// q holds the charges at lambda. Tables are lower-triangular and scaled (x12, x6): AA/AB of
+// the A state indexed by A types, BA/BB of the B state indexed by B types. A pair is soft-core
+// when its two atoms differ in mask or when exactly one end state has LJ; then
+//   r_A^6 = r^6 + alpha lambda^p sigma_A^6,  r_B^6 = r^6 + alpha (1-lambda)^p sigma_B^6,
+//   E = (1-l) [AA/12 r_A^-12 - AB/6 r_A^-6 + qq erfc(b r_A)/r_A] + l [same with B and r_B],
+// sigma^6 = max(AA/(2 AB), sigma_min^6) (sigma^6 if either coefficient vanishes); otherwise the
+// tables are mixed linearly in lambda and r is not softened. dH/dlambda is the exact derivative
+// of that energy (the soft-cored radii depend on lambda).
+void orc_softcore(int n, const uint32_t* uc, const float* q, const float* dq, const int* ta,
+                  const int* tb, const int* mask, const float* AA, const float* AB,
+                  const float* BA, const float* BB, const float* box, float cutoff, double beta,
+                  double lambda, double alpha, double p, double sigma6, double sigma6_min,
+                  const int64_t* pairs, long npairs, double* frc, double* out) {
+    float s[3];
+    scaler_of(box, s);
+    const float rc2 = cutoff * cutoff;
+    const double tsp = 2.0 / std::sqrt(M_PI);
+    const double l = lambda, l_ = 1.0 - lambda;
+    const double cA0 = alpha * std::pow(l, p), cB0 = alpha * std::pow(l_, p);
+    const double dcA0 = alpha * p * std::pow(l, p - 1.0), dcB0 = -alpha * p * std::pow(l_, p - 1.0);
+    double elj = 0, edir = 0, hlj = 0, hdir = 0;
+    for (long k = 0; k < npairs; k++) {
+        const int i = (int)(pairs[k] / n), j = (int)(pairs[k] % n);
+        const uint32_t* a = uc + 3 * (long)i;
+        const uint32_t* c = uc + 3 * (long)j;
+        if (!(pair_r2_f32(a[0], c[0], a[1], c[1], a[2], c[2], s) < rc2)) continue;
+        double dr[3];
+        dr_f64(a, c, s, dr);  // r_j - r_i
+        const double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+        const double r = std::sqrt(r2);
+        const int pa = pair_type(ta[i], ta[j]), pb = pair_type(tb[i], tb[j]);
+        const double Aa = AA[pa], Ab = AB[pa], Ba = BA[pb], Bb = BB[pb];
+        const double qq = (double)q[i] * q[j];
+        const double dqq = (double)dq[j] * q[i] + (double)q[j] * dq[i];
+        const bool soft = mask[i] != mask[j] || (Ba > 1e-6 && Aa < 1e-6) || (Ba < 1e-6 && Aa > 1e-6);
+        double fs;
+        if (!soft) {
+            const double ri2 = 1.0 / r2, ri6 = ri2 * ri2 * ri2;
+            const double Am = l_ * Aa + l * Ba, Bm = l_ * Ab + l * Bb;
+            const double flj = (-Am * ri6 + Bm) * ri6 * ri2;
+            const double br = beta * r, ec = std::erfc(br);
+            const double fc = qq * (br * tsp * std::exp(-br * br) + ec) * ri2 / r;
+            fs = flj - fc;
+            elj += (Am / 12.0 * ri6 - Bm / 6.0) * ri6;
+            edir += qq * ec / r;
+            hlj += ((Ba - Aa) / 12.0 * ri6 - (Bb - Ab) / 6.0) * ri6;
+            hdir += dqq * ec / r;
+        } else {
+            const double r4 = r2 * r2, r6 = r4 * r2;
+            const double sgA = (Aa < 1e-6 || Ab < 1e-6) ? sigma6 : std::max(0.5 * Aa / Ab, sigma6_min);
+            const double sgB = (Ba < 1e-6 || Bb < 1e-6) ? sigma6 : std::max(0.5 * Ba / Bb, sigma6_min);
+            const double sA = 1.0 / (r6 + cA0 * sgA), sB = 1.0 / (r6 + cB0 * sgB);
+            const double rA = std::pow(r6 + cA0 * sgA, 1.0 / 6.0), rB = std::pow(r6 + cB0 * sgB, 1.0 / 6.0);
+            const double flj = r4 * (l_ * (Ab - Aa * sA) * sA * sA + l * (Bb - Ba * sB) * sB * sB);
+            const double gA = beta * tsp * std::exp(-beta * beta * rA * rA);
+            const double gB = beta * tsp * std::exp(-beta * beta * rB * rB);
+            const double phA = std::erfc(beta * rA) / rA, phB = std::erfc(beta * rB) / rB;
+            const double fc = qq * r4 * (l_ * (gA + phA) * sA + l * (gB + phB) * sB);
+            fs = flj - fc;
+            const double EA = Aa / 12.0 * sA * sA - Ab / 6.0 * sA;
+            const double EB = Ba / 12.0 * sB * sB - Bb / 6.0 * sB;
+            elj += l_ * EA + l * EB;
+            edir += qq * (l_ * phA + l * phB);
+            const double dEA = (Aa / 6.0 * sA - Ab / 6.0) * (-sA * sA * dcA0 * sgA);
+            const double dEB = (Ba / 6.0 * sB - Bb / 6.0) * (-sB * sB * dcB0 * sgB);
+            hlj += EB - EA + l_ * dEA + l * dEB;
+            const double dphA = -(gA + phA) * sA / 6.0 * dcA0 * sgA;
+            const double dphB = -(gB + phB) * sB / 6.0 * dcB0 * sgB;
+            hdir += qq * (phB - phA + l_ * dphA + l * dphB) + dqq * (l_ * phA + l * phB);
+        }
+        for (int d = 0; d < 3; d++) {
+            frc[3 * (size_t)i + d] += fs * dr[d];
+            frc[3 * (size_t)j + d] -= fs * dr[d];
+        }
+    }
+    out[0] = elj;
+    out[1] = edir;
+    out[2] = hlj;
+    out[3] = hdir;
+}
+
+// TI cross terms of PME for charges q (at lambda) changing by dq per unit lambda:
+// out[0] = sum_i dq_i phi_i (reciprocal; phi the SPME potential of q at atom i),
+// out[1] = d/dlambda of the self + neutralising energy, out[2] = d/dlambda of the exclusion
+// correction energy at fixed geometry.
+void orc_ti_cross(int n, const uint32_t* uc, const float* q, const float* dq, const float* box,
+                  const int* K, double beta, const int* es, const int* en, const int* el,
+                  double* out) {
+    const size_t G = (size_t)K[0] * K[1] * K[2];
+    std::vector<cplx> Q(G, cplx(0, 0));
+    for (int i = 0; i < n; i++) {
+        int b[3];
+        double fr[3], w[3][4], dw[3][4];
+        for (int d = 0; d < 3; d++) {
+            grid_coord(uc[3 * (size_t)i + d], K[d], b[d], fr[d]);
+            bspline4(fr[d], w[d], dw[d]);
+        }
+        for (int kx = 0; kx < 4; kx++)
+            for (int ky = 0; ky < 4; ky++)
+                for (int kz = 0; kz < 4; kz++) {
+                    const int gx = ((b[0] - kx) % K[0] + K[0]) % K[0];
+                    const int gy = ((b[1] - ky) % K[1] + K[1]) % K[1];
+                    const int gz = ((b[2] - kz) % K[2] + K[2]) % K[2];
+                    Q[((size_t)gx * K[1] + gy) * K[2] + gz] +=
+                        (double)q[i] * w[0][kx] * w[1][ky] * w[2][kz];
+                }
+    }
+    fft3(Q.data(), K, -1, 0);
+    std::vector<double> bc;
+    bc_table(K, box, beta, bc);
+    for (size_t g = 0; g < G; g++) Q[g] *= bc[g];
+    fft3(Q.data(), K, +1, 0);
+    double rec = 0;
+    for (int i = 0; i < n; i++) {
+        int b[3];
+        double fr[3], w[3][4], dw[3][4];
+        for (int d = 0; d < 3; d++) {
+            grid_coord(uc[3 * (size_t)i + d], K[d], b[d], fr[d]);
+            bspline4(fr[d], w[d], dw[d]);
+        }
+        double phi = 0;
+        for (int kx = 0; kx < 4; kx++)
+            for (int ky = 0; ky < 4; ky++)
+                for (int kz = 0; kz < 4; kz++) {
+                    const int gx = ((b[0] - kx) % K[0] + K[0]) % K[0];
+                    const int gy = ((b[1] - ky) % K[1] + K[1]) % K[1];
+                    const int gz = ((b[2] - kz) % K[2] + K[2]) % K[2];
+                    phi += w[0][kx] * w[1][ky] * w[2][kz] * Q[((size_t)gx * K[1] + gy) * K[2] + gz].real();
+                }
+        rec += (double)dq[i] * phi;
+    }
+    double sqq = 0, sq = 0, sdq = 0;
+    for (int i = 0; i < n; i++) {
+        sqq += (double)q[i] * dq[i];
+        sq += q[i];
+        sdq += dq[i];
+    }
+    const double V = (double)box[0] * box[1] * box[2];
+    const double nf = -0.5 * M_PI / (beta * beta * V);
+    float s[3];
+    scaler_of(box, s);
+    double corr = 0;
+    for (int i = 0; i < n; i++)
+        for (int k = es[i]; k < es[i] + en[i]; k++) {
+            const int j = el[k];
+            double dr[3];
+            dr_f64(uc + 3 * (long)i, uc + 3 * (long)j, s, dr);
+            const double r = std::sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+            corr -= ((double)q[i] * dq[j] + (double)dq[i] * q[j]) * std::erf(beta * r) / r;
+        }
+    out[0] = rec;
+    out[1] = -2.0 * beta / std::sqrt(M_PI) * sqq + 2.0 * nf * sq * sdq;
+    out[2] = corr;
+}
+
 }  // extern "C"

@@ -66,6 +66,13 @@ def lib():
                                     ctypes.c_float, ctypes.c_float, ctypes.c_double, _i32p,
                                     _i32p, _i32p, _i32p, _f64p, _f64p, ctypes.c_int]
         L.orc_nonbonded.restype = ctypes.c_long
+        L.orc_softcore.argtypes = [ctypes.c_int, _u32p, _f32p, _f32p, _i32p, _i32p, _i32p,
+                                   _f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_float,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, _i64p,
+                                   ctypes.c_long, _f64p, _f64p]
+        L.orc_ti_cross.argtypes = [ctypes.c_int, _u32p, _f32p, _f32p, _f32p, _i32p,
+                                   ctypes.c_double, _i32p, _i32p, _i32p, _f64p]
         L.orc_threads.restype = ctypes.c_int
         L.orc_set_threads.argtypes = [ctypes.c_int]
         _LIB = L
@@ -269,3 +276,111 @@ def reference_energies(sys, uc=None, nthreads=0):
                e_self=self_energy(sys, beta), lrc_factor=f, e_lrc=f / V, virial_lrc=6 * f / V)
     res["f_total"] = fd + fe + fr
     return res
+
+
+# ---------------------------------------------------------------------------------------------
+# FEP / TI (soft-core LJ, LJ_soft_core.cu; PME cross terms, TI_core.cu:670-730)
+# ---------------------------------------------------------------------------------------------
+def fep_tables(sys):
+    """Scaled (x12, x6) lower-triangular tables of the A and B states."""
+    f32 = np.float32
+    A12 = (np.asarray(sys["lj_A"], f32) * f32(12.0)).astype(f32)
+    B6 = (np.asarray(sys["lj_B"], f32) * f32(6.0)).astype(f32)
+    A12b = (np.asarray(sys["lj_A_B"], f32) * f32(12.0)).astype(f32)
+    B6b = (np.asarray(sys["lj_B_B"], f32) * f32(6.0)).astype(f32)
+    return A12, B6, A12b, B6b
+
+
+def sc_sigma6(sys):
+    return float(sys["sc_sigma"]) ** 6, float(sys["sc_sigma_min"]) ** 6
+
+
+def softcore(uc, sys, pair_keys, beta, lam=None, charge=None):
+    """Soft-core LJ + direct Coulomb at lambda over a half pair set in FP64.
+
+    Returns (frc [N,3], dict(e_lj, e_direct, dhdl_lj, dhdl_direct))."""
+    n = uc.shape[0]
+    lam = sys["lam"] if lam is None else lam
+    q = np.ascontiguousarray(sys["charge"] if charge is None else charge, np.float32)
+    AA, AB, BA, BB = fep_tables(sys)
+    s6, s6m = sc_sigma6(sys)
+    pk = np.ascontiguousarray(pair_keys, np.int64)
+    npairs = pk.size
+    if npairs == 0:
+        pk = np.zeros(1, np.int64)
+    frc = np.zeros(3 * n, np.float64)
+    out = np.zeros(4, np.float64)
+    lib().orc_softcore(n, np.ascontiguousarray(uc, np.uint32).reshape(-1), q,
+                       np.ascontiguousarray(sys["dq"], np.float32),
+                       np.ascontiguousarray(sys["lj_type"], np.int32),
+                       np.ascontiguousarray(sys["lj_type_B"], np.int32),
+                       np.ascontiguousarray(sys["mask"], np.int32), AA, AB, BA, BB,
+                       np.ascontiguousarray(sys["box"], np.float32), sys["cutoff"], beta, lam,
+                       sys["sc_alpha"], sys["sc_p"], s6, s6m, pk, npairs, frc, out)
+    return frc.reshape(n, 3), dict(e_lj=out[0], e_direct=out[1], dhdl_lj=out[2],
+                                   dhdl_direct=out[3])
+
+
+def ti_cross(uc, sys, beta, charge=None):
+    """PME cross terms of dH/dlambda: reciprocal sum dq_i phi_i, self, exclusion correction."""
+    n = uc.shape[0]
+    q = np.ascontiguousarray(sys["charge"] if charge is None else charge, np.float32)
+    es, en, el = _excl(sys)
+    out = np.zeros(3, np.float64)
+    lib().orc_ti_cross(n, np.ascontiguousarray(uc, np.uint32).reshape(-1), q,
+                       np.ascontiguousarray(sys["dq"], np.float32),
+                       np.ascontiguousarray(sys["box"], np.float32),
+                       np.array(sys["fft"], np.int32), beta, es, en, el, out)
+    return dict(rec=out[0], self=out[1], corr=out[2])
+
+
+def fep_lrc(sys, lam=None):
+    """LJ long-range correction of the soft-core module: the factor at lambda (B6 mixed
+    linearly between the states, LJ_soft_core.cu:85-120) and its lambda derivative
+    (:123-156), both times -(2 pi/3)/rc^3/6; energy = factor/V."""
+    lam = sys["lam"] if lam is None else lam
+    _, B6a, _, B6b = fep_tables(sys)
+    ta = np.asarray(sys["lj_type"], np.int64)
+    tb = np.asarray(sys["lj_type_B"], np.int64)
+    combos, cnt = np.unique(np.stack([ta, tb], 1), axis=0, return_counts=True)
+    a = combos[:, 0]
+    b = combos[:, 1]
+
+    def tri(x, y):
+        M = np.maximum(x, y)
+        m = np.minimum(x, y)
+        return M * (M + 1) // 2 + m
+    w = np.outer(cnt, cnt).astype(np.float64)
+    sa = (w * B6a[tri(a[:, None], a[None, :])].astype(np.float64)).sum()
+    sb = (w * B6b[tri(b[:, None], b[None, :])].astype(np.float64)).sum()
+    kappa = -2.0 / 3.0 * np.pi / float(sys["cutoff"]) ** 3 / 6.0
+    return kappa * ((1.0 - lam) * sa + lam * sb), kappa * (sb - sa)
+
+
+def fep_reference(sys, uc=None, lam=None):
+    """FP64 forces, potential energy U(lambda) and dU/dlambda of an FEP box (soft-core LJ +
+    direct, exclusion correction, self, SPME reciprocal, long-range correction) with the
+    charges at lambda."""
+    lam = sys["lam"] if lam is None else lam
+    if uc is None:
+        uc = crd_to_uint(periodic_map(sys["crd"], sys["box"]), sys["box"])
+    q = ((1.0 - lam) * np.asarray(sys["charge_A"], np.float64) +
+         lam * np.asarray(sys["charge_B"], np.float64)).astype(np.float32)
+    sq = dict(sys)
+    sq["charge"] = q
+    beta = get_beta(sys["cutoff"], sys["tolerance"])
+    pk = pairs(uc, sys)
+    fs, p = softcore(uc, sys, pk, beta, lam=lam, charge=q)
+    fe, _, ecorr = excluded(uc, sq, beta)
+    fr, erec = pme(uc, sq, beta)
+    eself = self_energy(sq, beta)
+    V = float(np.prod(np.asarray(sys["box"], np.float64)))
+    flrc, flrc_ti = fep_lrc(sys, lam)
+    x = ti_cross(uc, sys, beta, charge=q)
+    U = p["e_lj"] + p["e_direct"] + ecorr + eself + erec + flrc / V
+    dU = p["dhdl_lj"] + p["dhdl_direct"] + x["rec"] + x["self"] + x["corr"] + flrc_ti / V
+    return dict(uc=uc, beta=beta, pairs=pk, charge=q, f_total=fs + fe + fr, f_sc=fs, U=U,
+                dU=dU, e_lj=p["e_lj"], e_direct=p["e_direct"], e_corr=ecorr, e_self=eself,
+                e_rec=erec, e_lrc=flrc / V, dhdl_lj=p["dhdl_lj"], dhdl_direct=p["dhdl_direct"],
+                cross_rec=x["rec"], cross_self=x["self"], cross_corr=x["corr"],
+                dhdl_lrc=flrc_ti / V)

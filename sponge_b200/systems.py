@@ -154,7 +154,7 @@ def config0(seed=1000):
 
 def _solvated(n_solute, radius, n_water, box, n_side, seed, cutoff, skin, fft,
               solute_q_sigma=0.4, n_types=20, min_dist=2.2, clear=2.6, name="",
-              center=None):
+              center=None, neutral=True):
     rng = np.random.default_rng(seed)
     if center is None:
         center = np.full(3, box / 2)
@@ -212,7 +212,8 @@ def _solvated(n_solute, radius, n_water, box, n_side, seed, cutoff, skin, fft,
     eps = list(rng.uniform(0.05, 0.25, n_types))
     stype = rng.integers(0, n_types, n_solute) + 2
     sq = rng.normal(0.0, solute_q_sigma, n_solute)
-    sq -= sq.mean()
+    if neutral:
+        sq -= sq.mean()
     crd = np.concatenate([solute, wcrd])
     q = np.concatenate([sq, np.tile([Q_O, Q_H, Q_H], n_water)])
     t = np.concatenate([stype, np.tile([0, 1, 1], n_water)])
@@ -264,6 +265,66 @@ def config3_fit(n_frames=16, seed=1003, jitter=0.05, noise=0.05):
     q = s["charge"].astype(np.float64) * (1.0 + noise * rng.normal(size=s["charge"].shape))
     target = dict(lj_sigma=sig, lj_eps=eps, charge=q.astype(np.float32))
     return s, frames, target
+
+
+WATER_VOLUME = 18.01528 / (0.997 * 0.602214076)  # A^3 per molecule at 0.997 g/cm^3
+
+
+def fft_smooth(n):
+    """Smallest 2-3-5-smooth integer >= n (an FFT-friendly grid size)."""
+    k = max(int(n), 1)
+    while True:
+        m = k
+        for f in (2, 3, 5):
+            while m % f == 0:
+                m //= f
+        if m == 1:
+            return k
+        k += 1
+
+
+def fep_box(n_water, lam, seed, n_solute=20, q_sigma=0.3, cutoff=9.0, skin=2.0, alpha=0.5,
+            p=1.0, sigma=3.0, sigma_min=0.0, name=""):
+    """A water box at 0.997 g/cm^3 holding a perturbed solute of ``n_solute`` atoms for FEP/TI.
+
+    The solute (20 LJ types as in the 96k-atom system, charges N(0, q_sigma) e, not neutralised)
+    is fully coupled in state A and vanishes in state B: B-state LJ type ``n_types`` has no LJ
+    and B-state charges are zero, so the charges at ``lam`` are (1 - lam) q_A. Waters are
+    unperturbed. Soft-core parameters follow LJ_SOFT_CORE::Initial's keys (alpha, p, sigma,
+    sigma_min; LJ_soft_core.cu:1420-1610). PME grid ~1 A, 2-3-5-smooth."""
+    L = float((n_water * WATER_VOLUME) ** (1.0 / 3.0))
+    k = fft_smooth(int(np.ceil(L)))
+    n_side = int(np.ceil((n_water * 1.12) ** (1.0 / 3.0)))
+    s = _solvated(n_solute, 4.5, n_water, L, n_side, seed, cutoff, skin, (k, k, k),
+                  solute_q_sigma=q_sigma, name=name, neutral=False)
+    nt = int(s["n_types"])
+    n = len(s["charge"])
+    mask = np.zeros(n, np.int32)
+    mask[:n_solute] = 1
+    type_b = s["lj_type"].copy()
+    type_b[:n_solute] = nt
+    A_b, B_b = _lj_tables(list(s["lj_sigma"]) + [1.0], list(s["lj_eps"]) + [0.0])
+    q_a = s["charge"].astype(np.float32)
+    q_b = q_a.copy()
+    q_b[:n_solute] = 0.0
+    s.update(
+        lj_type_B=type_b.astype(np.int32), n_types_B=nt + 1, lj_A_B=A_b, lj_B_B=B_b, mask=mask,
+        charge_A=q_a, charge_B=q_b,
+        charge=((1.0 - lam) * q_a.astype(np.float64) + lam * q_b).astype(np.float32),
+        dq=(q_b.astype(np.float64) - q_a).astype(np.float32),
+        lam=float(lam), sc_alpha=float(alpha), sc_p=float(p), sc_sigma=float(sigma),
+        sc_sigma_min=float(sigma_min))
+    return s
+
+
+def config4(box_index, n_boxes=48, seed=1004):
+    """Box ``box_index`` of the batched FEP/TI workload: water counts U[500, 8000] (seeded),
+    lambda = box_index / (n_boxes - 1), rc 9 A, skin 2 A."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(500, 8001, n_boxes)
+    lam = box_index / (n_boxes - 1) if n_boxes > 1 else 0.0
+    return fep_box(int(counts[box_index]), lam, seed * 1000 + box_index,
+                   name="fep%02d_w%d" % (box_index, counts[box_index]))
 
 
 def small_water(n_side=4, spacing=3.104, seed=7, cutoff=5.0, skin=1.0, fft=(16, 16, 16)):
