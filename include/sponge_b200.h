@@ -58,6 +58,7 @@ typedef struct sb_neighbor_list sb_neighbor_list;
 typedef struct sb_lennard_jones sb_lennard_jones;
 typedef struct sb_pme sb_pme;
 typedef struct sb_adjoint sb_adjoint;
+typedef struct sb_softcore sb_softcore;
 
 /* Library version (integer) and the message of the last failed call on this host thread. */
 SB_API int sb_version(void);
@@ -250,6 +251,70 @@ SB_API int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme*
  * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */
 SB_API int sb_crd_to_uint_crd(int atom_numbers, const float box_length[3], const float* d_crd,
                        uint32_t* d_uint_crd, void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Soft-core LJ for FEP/TI — replaces LJ_SOFT_CORE (SPONGE/Lennard_Jones_force/LJ_soft_core.cuh:
+ * 42-159) and the PME cross terms of TI_CORE (SPONGE/TI_core/TI_core.cu:670-730)
+ * ---------------------------------------------------------------------------------------- */
+
+/* LJ_SOFT_CORE::Initial (LJ_soft_core.cu:1420-1610). Two end states A and B with their own type
+ * sets: h_LJ_AA / h_LJ_AB the lower-triangular A-state tables (x12, x6 as the LJ module stores
+ * them) over atom_type_numbers_A types, h_LJ_BA / h_LJ_BB the B-state tables; per atom the A and B
+ * types, the perturbation mask (pairs whose masks differ are soft-cored) and the charge change
+ * h_charge_B_A = q_B - q_A. Soft core: r_A^6 = r^6 + alpha lambda^p sigma_A^6 and
+ * r_B^6 = r^6 + alpha (1 - lambda)^p sigma_B^6 with sigma^6 = max(A/(2B), sigma_min^6) of the
+ * pair (sigma^6 when either coefficient is zero). lambda is lambda_lj. */
+SB_API int sb_sc_create(int atom_numbers, int atom_type_numbers_A, const float* h_LJ_AA,
+                        const float* h_LJ_AB, int atom_type_numbers_B, const float* h_LJ_BA,
+                        const float* h_LJ_BB, const int* h_atom_LJ_type_A,
+                        const int* h_atom_LJ_type_B, const int* h_mask,
+                        const float* h_charge_B_A, float cutoff, const float box_length[3],
+                        float lambda, float alpha, float p, float sigma, float sigma_min, int form,
+                        sb_softcore** out);
+SB_API int sb_sc_destroy(sb_softcore* sc);
+
+/* Moves the module to another coupling parameter (one lambda window); recomputes the
+ * lambda-mixed long-range correction factor. */
+SB_API int sb_sc_set_lambda(sb_softcore* sc, float lambda);
+
+/* LJ_SOFT_CORE::LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial: soft-core LJ + Ewald
+ * direct force over the list of `nl` added to d_frc (d_charge holds the charges at lambda), with
+ * the per-atom energy / LJ virial / direct energy outputs of sb_lj_pme_direct_force. */
+SB_API int sb_sc_pme_direct_force(sb_softcore* sc, sb_neighbor_list* nl, int atom_numbers,
+                                  const uint32_t* d_uint_crd, const float* d_charge, float* d_frc,
+                                  float pme_beta, int need_atom_energy, float* d_atom_energy,
+                                  int need_virial, float* d_atom_lj_virial,
+                                  float* d_atom_direct_pme_energy, void* stream);
+
+/* LJ_SOFT_CORE::Long_Range_Correction with the lambda-mixed dispersion factor. */
+SB_API int sb_sc_long_range_correction(sb_softcore* sc, int need_pressure, float* d_virial,
+                                       int need_potential, float* d_potential, void* stream);
+
+/* LJ_SOFT_CORE::Get_Partial_H_Partial_Lambda_With_Columb_Direct (LJ_soft_core.cu:1137-1283) and
+ * Partial_H_Partial_Lambda_Long_Range_Correction (:1939-1953): h_dhdl[0] = LJ, h_dhdl[1] = direct
+ * Coulomb (including the charge change at fixed geometry), h_dhdl[2] = long-range correction.
+ * Exact derivatives of the soft-core energy (FP64 sums). Synchronises the stream. */
+SB_API int sb_sc_dh_dlambda(sb_softcore* sc, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                            const float* d_charge, float pme_beta, double* h_dhdl, void* stream);
+
+/* TI_CORE::Get_Cross_PME_Partial_H_Partial_Lambda: for charges d_charge changing by
+ * d_charge_B_A per unit lambda, h_parts[0] = reciprocal sum_i dq_i phi_i (phi the SPME potential),
+ * h_parts[1] = self + neutralising derivative, h_parts[2] = exclusion-correction derivative.
+ * Synchronises the stream. */
+SB_API int sb_pme_ti_cross(sb_pme* pme, const uint32_t* d_uint_crd, const float* d_charge,
+                           const float* d_charge_B_A, const int* d_excluded_list_start,
+                           const int* d_excluded_list, const int* d_excluded_numbers,
+                           double* h_parts, void* stream);
+
+/* One FEP force evaluation at the module's lambda with dU/dlambda, fixed-point form, no host
+ * synchronisation: soft-core LJ + direct, long-range correction, exclusion correction and
+ * reciprocal space (charges d_charge at lambda) added to d_frc; *d_dudl (one device double)
+ * receives dU/dlambda = soft-core LJ + direct + PME cross terms + long-range correction. The list
+ * of `nl` must be current (sb_nl_update is not called). */
+SB_API int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
+                       const uint32_t* d_uint_crd, const float* d_charge,
+                       const int* d_excluded_list_start, const int* d_excluded_list,
+                       const int* d_excluded_numbers, float* d_frc, double* d_dudl, void* stream);
 
 /* ------------------------------------------------------------------------------------------
  * Differentiation for force-field fitting (no reference counterpart: SPONGE has no gradients

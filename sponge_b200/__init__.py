@@ -76,6 +76,15 @@ _SIGS = {
     "sb_adjoint_destroy": [_vp],
     "sb_adjoint_backward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp,
                             _vp, _vp, _vp, _vp],
+    "sb_sc_create": [_i, _i, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _f, _vp, _f, _f, _f,
+                     _f, _f, _i, _vp],
+    "sb_sc_destroy": [_vp],
+    "sb_sc_set_lambda": [_vp, _f],
+    "sb_sc_pme_direct_force": [_vp, _vp, _i, _vp, _vp, _vp, _f, _i, _vp, _i, _vp, _vp, _vp],
+    "sb_sc_long_range_correction": [_vp, _i, _vp, _i, _vp, _vp],
+    "sb_sc_dh_dlambda": [_vp, _vp, _vp, _vp, _f, _vp, _vp],
+    "sb_pme_ti_cross": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_fep_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }
 
 
@@ -396,3 +405,86 @@ def nonbonded_step(nl, lj, pme, crd, uint_crd, charge, excl, frc, need_energy=0,
 
 
 from .engine import NonbondedEngine  # noqa: E402,F401
+
+
+class SoftCore:
+    """LJ_SOFT_CORE (SPONGE/Lennard_Jones_force/LJ_soft_core.cuh:42-159). Tables are the
+    lower-triangular A/B coefficients of each end state already multiplied by 12 and 6."""
+
+    def __init__(self, atom_numbers, LJ_AA, LJ_AB, LJ_BA, LJ_BB, atom_LJ_type_A, atom_LJ_type_B,
+                 mask, charge_B_A, cutoff, box_length, lambda_lj, alpha=0.5, p=1.0, sigma=3.0,
+                 sigma_min=0.0, form=FORM_FIXED, n_types_A=None, n_types_B=None):
+        _require_cuda()
+        self.atom_numbers = int(atom_numbers)
+        f32, i32 = np.float32, np.int32
+        self.h = [np.ascontiguousarray(x, t) for x, t in
+                  ((LJ_AA, f32), (LJ_AB, f32), (LJ_BA, f32), (LJ_BB, f32),
+                   (atom_LJ_type_A, i32), (atom_LJ_type_B, i32), (mask, i32), (charge_B_A, f32))]
+        ntA = int(n_types_A) if n_types_A is not None else int(self.h[4].max()) + 1
+        ntB = int(n_types_B) if n_types_B is not None else int(self.h[5].max()) + 1
+        self.lambda_lj = float(lambda_lj)
+        self.handle = ctypes.c_void_p()
+        _check(lib().sb_sc_create(self.atom_numbers, ntA, self.h[0].ctypes.data,
+                                  self.h[1].ctypes.data, ntB, self.h[2].ctypes.data,
+                                  self.h[3].ctypes.data, self.h[4].ctypes.data,
+                                  self.h[5].ctypes.data, self.h[6].ctypes.data,
+                                  self.h[7].ctypes.data, float(cutoff), _box3(box_length),
+                                  self.lambda_lj, float(alpha), float(p), float(sigma),
+                                  float(sigma_min), int(form), ctypes.byref(self.handle)))
+
+    def set_lambda(self, lambda_lj):
+        self.lambda_lj = float(lambda_lj)
+        _check(lib().sb_sc_set_lambda(self.handle, self.lambda_lj))
+
+    def LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial(
+            self, atom_numbers, uint_crd, charge, frc, nl, pme_beta, need_atom_energy=0,
+            atom_energy=None, need_virial=0, atom_lj_virial=None, atom_direct_pme_energy=None,
+            stream=None):
+        _check(lib().sb_sc_pme_direct_force(self.handle, nl.handle, int(atom_numbers),
+                                            _ptr(uint_crd), _ptr(charge), _ptr(frc),
+                                            float(pme_beta), int(need_atom_energy),
+                                            _ptr(atom_energy), int(need_virial),
+                                            _ptr(atom_lj_virial), _ptr(atom_direct_pme_energy),
+                                            _stream(stream)))
+
+    def Long_Range_Correction(self, need_pressure, d_virial, need_potential, d_potential,
+                              stream=None):
+        _check(lib().sb_sc_long_range_correction(self.handle, int(need_pressure), _ptr(d_virial),
+                                                 int(need_potential), _ptr(d_potential),
+                                                 _stream(stream)))
+
+    def Get_Partial_H_Partial_Lambda(self, uint_crd, charge, nl, pme_beta, stream=None):
+        """(LJ, direct Coulomb, long-range correction) parts of dH/dlambda (FP64)."""
+        h = (ctypes.c_double * 3)()
+        _check(lib().sb_sc_dh_dlambda(self.handle, nl.handle, _ptr(uint_crd), _ptr(charge),
+                                      float(pme_beta), h, _stream(stream)))
+        return tuple(h)
+
+    def Clear(self):
+        if self.handle:
+            lib().sb_sc_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+
+def pme_ti_cross(pme, uint_crd, charge, charge_B_A, excl, stream=None):
+    """TI_CORE::Get_Cross_PME_Partial_H_Partial_Lambda: (reciprocal, self, correction)."""
+    h = (ctypes.c_double * 3)()
+    es, el, en = excl
+    _check(lib().sb_pme_ti_cross(pme.handle, _ptr(uint_crd), _ptr(charge), _ptr(charge_B_A),
+                                 _ptr(es), _ptr(el), _ptr(en), h, _stream(stream)))
+    return tuple(h)
+
+
+def fep_step(nl, sc, pme, uint_crd, charge, excl, frc, dudl=None, stream=None):
+    """One FEP force evaluation (forces += into frc) with dU/dlambda into the device double
+    ``dudl`` (a 1-element float64 CUDA tensor, optional)."""
+    es, el, en = excl
+    _check(lib().sb_fep_step(nl.handle, sc.handle, pme.handle, _ptr(uint_crd), _ptr(charge),
+                             _ptr(es), _ptr(el), _ptr(en), _ptr(frc), _ptr(dudl),
+                             _stream(stream)))

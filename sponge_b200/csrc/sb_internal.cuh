@@ -220,6 +220,12 @@ int sb_pme_fused_reciprocal(sb_pme* pme, sb_neighbor_list* nl, float* d_frc, con
                             int need_virial, int need_energy, float* d_virial, float* d_potential,
                             cudaStream_t s);
 
+// FEP step: PME cross terms of dU/dlambda after sb_pme_fused_reciprocal (acc[0] reciprocal,
+// acc[1] exclusion correction, 2^32 fixed point)
+int sb_pme_ti_terms_slot(sb_pme* p, sb_neighbor_list* nl, const float* slot_dq,
+                         const uint32_t* uc, const float* q, const float* dq, const int* es,
+                         const int* el, const int* en, long long* acc, cudaStream_t s);
+
 // FP64 reduction helpers (deterministic: fixed block/thread order)
 int sb_reduce_sum_f32(const float* d_x, int n, double* d_out, cudaStream_t s);
 

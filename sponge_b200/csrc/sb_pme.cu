@@ -913,6 +913,202 @@ int sb_pme_fused_reciprocal(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const
 }
 
 // ---------------------------------------------------------------------------------------------
+// TI cross terms of PME (TI_core.cu:670-730): for charges changing by dq per unit lambda,
+// d E_rec / d lambda = sum_i dq_i phi_i with phi the SPME potential of the current charges (the
+// reference spreads dq onto a second grid and dots it with the convolved grid; the same number),
+// and the exclusion-correction derivative at fixed geometry. Accumulated as 2^32 fixed point.
+// ---------------------------------------------------------------------------------------------
+#define SB_TI_SCALE 4294967296.0f
+#define SB_TI_UNSCALE (1.0 / 4294967296.0)
+
+__device__ __forceinline__ float phi_at(uint32_t ux, uint32_t uy, uint32_t uz,
+                                        const float* __restrict__ theta, int K0, int K1, int K2) {
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(ux, K0, b0, f0);
+    grid_coord(uy, K1, b1, f1);
+    grid_coord(uz, K2, b2, f2);
+    float wx[4], wy[4], wz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    float phi = 0.f;
+#pragma unroll
+    for (int kx = 0; kx < 4; kx++) {
+        int gx = b0 - kx;
+        if (gx < 0) gx += K0;
+#pragma unroll
+        for (int ky = 0; ky < 4; ky++) {
+            int gy = b1 - ky;
+            if (gy < 0) gy += K1;
+            const float* row = theta + ((size_t)gx * K1 + gy) * K2;
+            float sw = 0.f;
+#pragma unroll
+            for (int kz = 0; kz < 4; kz++) {
+                int gz = b2 - kz;
+                if (gz < 0) gz += K2;
+                sw = fmaf(row[gz], wz[kz], sw);
+            }
+            phi = fmaf(wx[kx] * wy[ky], sw, phi);
+        }
+    }
+    return phi;
+}
+
+__device__ __forceinline__ void ti_red(long long* p, float v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) {
+        const long long q = __float2ll_rn(v * SB_TI_SCALE);
+        if (q) atomicAdd((unsigned long long*)p, (unsigned long long)q);
+    }
+}
+
+// sum dq phi over atoms in original order (n) or over packed slots (xq != null, n = slots)
+__global__ void k_ti_rec(int n, const int* __restrict__ meta, const uint32_t* __restrict__ uc,
+                         const uint4* __restrict__ xq, const float* __restrict__ dq,
+                         const float* __restrict__ theta, int K0, int K1, int K2,
+                         long long* __restrict__ acc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lim = meta ? meta[3] : n;
+    float v = 0.f;
+    if (i < lim) {
+        const float d = dq[i];
+        if (d != 0.f) {
+            if (xq) {
+                const uint4 u = xq[i];
+                v = d * phi_at(u.x, u.y, u.z, theta, K0, K1, K2);
+            } else {
+                v = d * phi_at(uc[3 * i], uc[3 * i + 1], uc[3 * i + 2], theta, K0, K1, K2);
+            }
+        }
+    }
+    ti_red(acc, v);
+}
+
+// d/dlambda of the exclusion correction -qq erf(beta r)/r at fixed geometry
+__global__ void k_ti_corr(int n, const uint32_t* __restrict__ uc, float sx, float sy, float sz,
+                          const float* __restrict__ q, const float* __restrict__ dq, float beta,
+                          const int* __restrict__ es, const int* __restrict__ el,
+                          const int* __restrict__ en, long long* __restrict__ acc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float v = 0.f;
+    if (i < n) {
+        const int cnt = en[i], s0 = es[i];
+        const float qi = q[i], dqi = dq[i];
+        for (int k = s0; k < s0 + cnt; k++) {
+            const int j = el[k];
+            const float dqq = qi * dq[j] + dqi * q[j];
+            if (dqq == 0.f) continue;
+            const float dx = __int2float_rn((int)(uc[3 * j] - uc[3 * i])) * sx;
+            const float dy = __int2float_rn((int)(uc[3 * j + 1] - uc[3 * i + 1])) * sy;
+            const float dz = __int2float_rn((int)(uc[3 * j + 2] - uc[3 * i + 2])) * sz;
+            const float r = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+            v -= dqq * erff(beta * r) / r;
+        }
+    }
+    ti_red(acc, v);
+}
+
+__global__ void k_ti_zero(long long* a, int n) {
+    if ((int)threadIdx.x < n) a[threadIdx.x] = 0;
+}
+
+__global__ void __launch_bounds__(1024) k_ti_finish(int n, const float* __restrict__ q,
+                                                    const float* __restrict__ dq,
+                                                    const long long* __restrict__ acc,
+                                                    double self_coef, double neutral2,
+                                                    double* __restrict__ out) {
+    __shared__ double r1[1024], r2[1024], r3[1024];
+    double a = 0, b = 0, c = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a += (double)q[i] * dq[i];
+        b += q[i];
+        c += dq[i];
+    }
+    r1[threadIdx.x] = a;
+    r2[threadIdx.x] = b;
+    r3[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            r1[threadIdx.x] += r1[threadIdx.x + o];
+            r2[threadIdx.x] += r2[threadIdx.x + o];
+            r3[threadIdx.x] += r3[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = (double)acc[0] * SB_TI_UNSCALE;
+        out[1] = self_coef * r1[0] + neutral2 * r2[0] * r3[0];
+        out[2] = (double)acc[1] * SB_TI_UNSCALE;
+    }
+}
+
+// fused FEP step: reciprocal and exclusion cross terms after sb_pme_fused_reciprocal left the
+// convolved grid in d_theta; adds into acc[0] (reciprocal) and acc[1] (correction)
+int sb_pme_ti_terms_slot(sb_pme* p, sb_neighbor_list* nl, const float* slot_dq,
+                         const uint32_t* uc, const float* q, const float* dq, const int* es,
+                         const int* el, const int* en, long long* acc, cudaStream_t s) {
+    k_ti_rec<<<(nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->slot_cap, nl->meta, nullptr, nl->xq,
+                                                        slot_dq, p->d_theta, p->K[0], p->K[1],
+                                                        p->K[2], acc);
+    SB_CHECK_LAUNCH();
+    if (es && el && en) {
+        const float sx = (1.0f / 4294967296.0f) * p->box[0], sy = (1.0f / 4294967296.0f) * p->box[1],
+                    sz = (1.0f / 4294967296.0f) * p->box[2];
+        k_ti_corr<<<(p->n + 255) / 256, 256, 0, s>>>(p->n, uc, sx, sy, sz, q, dq, p->beta, es, el,
+                                                     en, acc + 1);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_pme_ti_cross(sb_pme* p, const uint32_t* d_uint_crd, const float* d_charge,
+                               const float* d_dq, const int* es, const int* el, const int* en,
+                               double* h_parts, void* stream) {
+    if (!p || !d_uint_crd || !d_charge || !d_dq || !h_parts) {
+        sb_set_error("sb_pme_ti_cross: null argument");
+        return SB_ERR_ARG;
+    }
+    if (p->form != SB_FORM_FIXED) {
+        sb_set_error("sb_pme_ti_cross: needs the fixed-point form");
+        return SB_ERR_ARG;
+    }
+    cudaStream_t s = sb_stream(stream);
+    const int n = p->n;
+    // two int64 accumulators in the FP64 energy slots 4 and 5; the results go to slots 0..2
+    long long* acc = (long long*)(p->d_ered + 4);
+    k_ti_zero<<<1, 32, 0, s>>>(acc, 2);
+    SB_CHECK_LAUNCH();
+    // theta of the current charges (recomputed, as TI_CORE does)
+    k_spread<true><<<(4 * n + 255) / 256, 256, 0, s>>>(n, d_uint_crd, d_charge, p->K[0], p->K[1],
+                                                      p->K[2], p->d_qfix, nullptr);
+    SB_CHECK_LAUNCH();
+    int nparts = 0;
+    SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
+    SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, 0, s, &nparts));
+    SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+    k_ti_rec<<<(n + 255) / 256, 256, 0, s>>>(n, nullptr, d_uint_crd, nullptr, d_dq, p->d_theta,
+                                             p->K[0], p->K[1], p->K[2], acc);
+    SB_CHECK_LAUNCH();
+    if (es && el && en) {
+        const float sx = (1.0f / 4294967296.0f) * p->box[0], sy = (1.0f / 4294967296.0f) * p->box[1],
+                    sz = (1.0f / 4294967296.0f) * p->box[2];
+        k_ti_corr<<<(n + 255) / 256, 256, 0, s>>>(n, d_uint_crd, sx, sy, sz, d_charge, d_dq,
+                                                  p->beta, es, el, en, acc + 1);
+        SB_CHECK_LAUNCH();
+    }
+    k_ti_finish<<<1, 1024, 0, s>>>(n, d_charge, d_dq, acc, -2.0 * (double)p->beta / sqrt(M_PI),
+                                   2.0 * p->neutralizing_factor, p->d_ered);
+    SB_CHECK_LAUNCH();
+    double h[3];
+    SB_CHECK_CUDA(cudaMemcpyAsync(h, p->d_ered, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
+    SB_CHECK_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < 3; k++) h_parts[k] = h[k];
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Allocation-free energy query
 //
 // sb_pme_get_energy needs a 3N-float force array to run the reciprocal and exclusion passes

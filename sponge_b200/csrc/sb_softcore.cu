@@ -1,0 +1,831 @@
+// Soft-core LJ + Ewald direct space for FEP/TI — replaces LJ_SOFT_CORE
+// (SPONGE/Lennard_Jones_force/LJ_soft_core.cu) — and the FEP force step with dU/dlambda.
+//
+// Two end states A and B. A pair is soft-cored when its atoms' perturbation masks differ or
+// when exactly one end state has LJ between them (LJ_soft_core.cu:243-297); then
+//   r_A^6 = r^6 + alpha lambda^p sigma_A^6,   r_B^6 = r^6 + alpha (1-lambda)^p sigma_B^6,
+//   E = (1-l) [A_A/12 r_A^-12 - B_A/6 r_A^-6 + qq erfc(b r_A)/r_A] + l [same, B state, r_B],
+// sigma^6 = max(A/(2B), sigma_min^6), or sigma^6 when either coefficient vanishes. Other pairs
+// use the tables mixed linearly in lambda at the plain distance. qq is the product of the charges
+// at lambda (the caller's charge array). dH/dlambda is the exact lambda derivative of that
+// energy at fixed geometry, including the charge change dq = q_B - q_A.
+//
+// Chosen form: the cluster list of the neighbor list (warp per 8-atom cluster, one lane per
+// entry), forces and dH/dlambda accumulated as 64-bit fixed point. Plain form: the per-atom
+// ATOM_GROUP list with float atomics (the reference's structure).
+
+#include <math.h>
+
+#include <vector>
+
+#include "sb_ewald.cuh"
+#include "sb_internal.cuh"
+
+#define SB_DHDL_SCALE 4294967296.0f      // 2^32 fixed-point units per kcal/mol
+#define SB_DHDL_UNSCALE (1.0 / 4294967296.0)
+#define SB_EV_ENERGY_SC 1
+#define SB_EV_VIRIAL_SC 2
+
+struct sb_softcore {
+    int n = 0;
+    int ntA = 0, ntB = 0;
+    int form = SB_FORM_FIXED;
+    float cutoff = 10.f;
+    float box[3];
+    float lambda = 0.f, alpha = 0.5f, p = 1.f, sigma = 3.f, sigma_min = 0.f;
+    std::vector<float> hA12a, hB6a, hA12b, hB6b;  // lower-triangular tables (x12, x6)
+    std::vector<int> htA, htB;
+    double lrc_factor = 0, lrc_ti = 0;             // x kappa; energy = factor / V
+    float2* d_ABa = nullptr;   // [ntA^2] {A12, B6} of state A
+    float2* d_ABb = nullptr;   // [ntB^2] of state B
+    float* d_Aa = nullptr;     // lower-triangular copies for the plain form
+    float* d_Ba = nullptr;
+    float* d_Ab = nullptr;
+    float* d_Bb = nullptr;
+    int* d_typeA = nullptr;
+    int* d_typeB = nullptr;
+    int* d_mask = nullptr;
+    float* d_dq = nullptr;
+    int slot_cap = 0;
+    int* d_slot_ext = nullptr;     // [slot_cap] typeB | mask << 16
+    float* d_slot_dq = nullptr;    // [slot_cap]
+    long long* d_hfix = nullptr;   // [4] fixed-point dH/dlambda: LJ, direct, reciprocal, correction
+    double* d_red = nullptr;       // [8] FP64 scratch
+    float* d_scratch_frc = nullptr;  // [3N] plain-form dH/dlambda pass (forces discarded)
+};
+
+struct ScParams {
+    float sx, sy, sz, rc2;
+    float beta, beta2, tsp_beta;  // 2 beta / sqrt(pi)
+    float l, l_;                  // lambda, 1 - lambda
+    float cA, cB;                 // alpha lambda^p, alpha (1-lambda)^p
+    float dcA, dcB;               // their lambda derivatives
+    float s6, s6min;
+    float gp[6];
+    int wide;
+    int ntA, ntB;
+    int slot_cap, ent_cap;
+};
+
+// force factor fs (force on i = fs (r_j - r_i)) of one pair inside the cutoff, with the optional
+// energy, LJ virial and dH/dlambda contributions
+template <bool EV, bool DH>
+__device__ __forceinline__ float sc_pair(const ScParams& P, float r2, float qq, float dqq,
+                                         bool soft, float2 a, float2 b, float& e_lj, float& e_c,
+                                         float& v_lj, float& h_lj, float& h_c) {
+    if (!soft) {
+        const float ri = rsqrtf(r2);
+        const float ri2 = ri * ri, ri6 = ri2 * ri2 * ri2;
+        const float Am = P.l_ * a.x + P.l * b.x, Bm = P.l_ * a.y + P.l * b.y;
+        const float flj = (Bm - Am * ri6) * (ri6 * ri2);
+        const float bg = P.wide ? sb_ewald_G_scaled(P.beta2 * r2, P.gp)
+                                : sb_ewald_G_rational(P.beta2 * r2, P.gp);
+        const float fc = qq * (ri * ri2 - bg);
+        if (EV || DH) {
+            const float ec = (EV || dqq != 0.f) ? erfcf(P.beta * r2 * ri) * ri : 0.f;
+            if (EV) {
+                e_lj += (0.083333333f * Am * ri6 - 0.166666667f * Bm) * ri6;
+                e_c += qq * ec;
+                v_lj -= flj * r2;
+            }
+            if (DH) {
+                h_lj += (0.083333333f * (b.x - a.x) * ri6 - 0.166666667f * (b.y - a.y)) * ri6;
+                h_c += dqq * ec;
+            }
+        }
+        return flj - fc;
+    }
+    const float r4 = r2 * r2, r6 = r4 * r2;
+    const float sgA = (a.x < 1e-6f || a.y < 1e-6f) ? P.s6 : fmaxf(0.5f * a.x / a.y, P.s6min);
+    const float sgB = (b.x < 1e-6f || b.y < 1e-6f) ? P.s6 : fmaxf(0.5f * b.x / b.y, P.s6min);
+    const float sA = 1.0f / (r6 + P.cA * sgA), sB = 1.0f / (r6 + P.cB * sgB);
+    const float flj = r4 * (P.l_ * (a.y - a.x * sA) * sA * sA + P.l * (b.y - b.x * sB) * sB * sB);
+    const float rAi = powf(sA, 1.0f / 6.0f), rBi = powf(sB, 1.0f / 6.0f);  // 1/r_A, 1/r_B
+    const float gA = P.tsp_beta * expf(-P.beta2 / (rAi * rAi));
+    const float gB = P.tsp_beta * expf(-P.beta2 / (rBi * rBi));
+    const float phA = erfcf(P.beta / rAi) * rAi, phB = erfcf(P.beta / rBi) * rBi;
+    const float fc = qq * r4 * (P.l_ * (gA + phA) * sA + P.l * (gB + phB) * sB);
+    const float EA = (0.083333333f * a.x * sA - 0.166666667f * a.y) * sA;
+    const float EB = (0.083333333f * b.x * sB - 0.166666667f * b.y) * sB;
+    if (EV) {
+        e_lj += P.l_ * EA + P.l * EB;
+        e_c += qq * (P.l_ * phA + P.l * phB);
+        v_lj -= flj * r2;
+    }
+    if (DH) {
+        const float dEA = (0.166666667f * a.x * sA - 0.166666667f * a.y) * (-sA * sA * P.dcA * sgA);
+        const float dEB = (0.166666667f * b.x * sB - 0.166666667f * b.y) * (-sB * sB * P.dcB * sgB);
+        h_lj += EB - EA + P.l_ * dEA + P.l * dEB;
+        const float dphA = -(gA + phA) * sA * 0.166666667f * P.dcA * sgA;
+        const float dphB = -(gB + phB) * sB * 0.166666667f * P.dcB * sgB;
+        h_c += qq * (phB - phA + P.l_ * dphA + P.l * dphB) + dqq * (P.l_ * phA + P.l * phB);
+    }
+    return flj - fc;
+}
+
+__device__ __forceinline__ bool sc_is_soft(int mi, int mj, float2 a, float2 b) {
+    return mi != mj || (b.x > 1e-6f && a.x < 1e-6f) || (b.x < 1e-6f && a.x > 1e-6f);
+}
+
+__device__ __forceinline__ void red_fix_sc(long long* p, float v, float scale) {
+    const long long q = __float2ll_rn(v * scale);
+    if (q) atomicAdd((unsigned long long*)p, (unsigned long long)q);
+}
+
+// per-slot B type, mask and charge change
+__global__ void k_sc_pack(const int* __restrict__ meta, const int* __restrict__ slot_atom,
+                          const int* __restrict__ typeB, const int* __restrict__ mask,
+                          const float* __restrict__ dq, int* __restrict__ ext,
+                          float* __restrict__ sdq) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= meta[3]) return;
+    const int a = slot_atom[s];
+    ext[s] = a >= 0 ? (typeB[a] | (mask[a] << 16)) : 0;
+    sdq[s] = a >= 0 ? dq[a] : 0.f;
+}
+
+// chosen form: warp per cluster, one lane per list entry, the 8 cluster atoms in registers
+template <int EV, bool DH>
+__global__ void __launch_bounds__(128) k_pair_sc(
+    ScParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
+    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
+    const int* __restrict__ stype, const int* __restrict__ sext, const float* __restrict__ sdq,
+    const float2* __restrict__ ABa, const float2* __restrict__ ABb,
+    const int* __restrict__ slot_atom, long long* __restrict__ fix,
+    long long* __restrict__ hfix, float* __restrict__ atom_energy,
+    float* __restrict__ atom_virial, float* __restrict__ atom_direct) {
+    extern __shared__ float2 sAB[];  // [ntA^2] A tables, then [ntB^2] B tables
+    __shared__ int s_ta[4][SB_CLUSTER], s_tb[4][SB_CLUSTER], s_m[4][SB_CLUSTER];
+    __shared__ float s_dq[4][SB_CLUSTER];
+    const int na = P.ntA * P.ntA, nb = P.ntB * P.ntB;
+    for (int t = threadIdx.x; t < na; t += blockDim.x) sAB[t] = ABa[t];
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) sAB[na + t] = ABb[t];
+    __syncthreads();
+    const float2* sA = sAB;
+    const float2* sB = sAB + na;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int c = blockIdx.x * 4 + w;
+    if (c >= meta[0]) return;
+    const int base = c * SB_CLUSTER;
+    const uint4 my = lane < SB_CLUSTER ? xq[base + lane] : make_uint4(0, 0, 0, 0);
+    if (lane < SB_CLUSTER) {
+        const int ex = sext[base + lane];
+        s_ta[w][lane] = stype[base + lane] * P.ntA;
+        s_tb[w][lane] = (ex & 0xffff) * P.ntB;
+        s_m[w][lane] = ex >> 16;
+        s_dq[w][lane] = sdq[base + lane];
+    }
+    __syncwarp();
+    const bool exact = (cl_count[c] & SB_CL_EXACT) != 0;
+    float xi[SB_CLUSTER], yi[SB_CLUSTER], zi[SB_CLUSTER], qi[SB_CLUSTER];
+    uint32_t ux[SB_CLUSTER], uy[SB_CLUSTER], uz[SB_CLUSTER];
+    float fxi[SB_CLUSTER], fyi[SB_CLUSTER], fzi[SB_CLUSTER];
+    float el[SB_CLUSTER], ec[SB_CLUSTER], ev[SB_CLUSTER];
+#pragma unroll
+    for (int k = 0; k < SB_CLUSTER; k++) {
+        ux[k] = __shfl_sync(0xffffffffu, my.x, k);
+        uy[k] = __shfl_sync(0xffffffffu, my.y, k);
+        uz[k] = __shfl_sync(0xffffffffu, my.z, k);
+        qi[k] = __uint_as_float(__shfl_sync(0xffffffffu, my.w, k));
+        xi[k] = __int2float_rn((int)(ux[k] - ux[0])) * P.sx;
+        yi[k] = __int2float_rn((int)(uy[k] - uy[0])) * P.sy;
+        zi[k] = __int2float_rn((int)(uz[k] - uz[0])) * P.sz;
+        fxi[k] = fyi[k] = fzi[k] = 0.f;
+        el[k] = ec[k] = ev[k] = 0.f;
+    }
+    float h_lj = 0.f, h_c = 0.f;
+    const int cnt = min(cl_count[c] & SB_CL_COUNT_MASK, P.ent_cap);
+    const uint32_t* ents = cl_ent + (size_t)c * P.ent_cap;
+    for (int e = lane; e < cnt; e += 32) {
+        const uint32_t v = ents[e];
+        const int j = (int)(v & 0xffffffu);
+        const uint32_t m = v >> 24;
+        const uint4 xj = xq[j];
+        const int tja = stype[j];
+        const int exj = sext[j];
+        const int tjb = exj & 0xffff, mj = exj >> 16;
+        const float qj = __uint_as_float(xj.w), dqj = sdq[j];
+        const float xjr = __int2float_rn((int)(xj.x - ux[0])) * P.sx;
+        const float yjr = __int2float_rn((int)(xj.y - uy[0])) * P.sy;
+        const float zjr = __int2float_rn((int)(xj.z - uz[0])) * P.sz;
+        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+#pragma unroll
+        for (int k = 0; k < SB_CLUSTER; k++) {
+            if (!((m >> k) & 1u)) continue;
+            float dx, dy, dz;
+            if (exact) {
+                dx = __int2float_rn((int)(xj.x - ux[k])) * P.sx;
+                dy = __int2float_rn((int)(xj.y - uy[k])) * P.sy;
+                dz = __int2float_rn((int)(xj.z - uz[k])) * P.sz;
+            } else {
+                dx = xjr - xi[k];
+                dy = yjr - yi[k];
+                dz = zjr - zi[k];
+            }
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (!(r2 < P.rc2)) continue;
+            const float2 a = sA[s_ta[w][k] + tja];
+            const float2 b = sB[s_tb[w][k] + tjb];
+            const bool soft = sc_is_soft(s_m[w][k], mj, a, b);
+            const float qq = qi[k] * qj;
+            const float dqq = dqj * qi[k] + qj * s_dq[w][k];
+            float e1 = 0.f, e2 = 0.f, v1 = 0.f;
+            const float fs = sc_pair<EV != 0, DH>(P, r2, qq, dqq, soft, a, b, e1, e2, v1, h_lj, h_c);
+            fxi[k] = fmaf(fs, dx, fxi[k]);
+            fyi[k] = fmaf(fs, dy, fyi[k]);
+            fzi[k] = fmaf(fs, dz, fzi[k]);
+            fjx = fmaf(-fs, dx, fjx);
+            fjy = fmaf(-fs, dy, fjy);
+            fjz = fmaf(-fs, dz, fjz);
+            if (EV) {
+                el[k] += e1;
+                ec[k] += e2;
+                ev[k] += v1;
+            }
+        }
+        red_fix_sc(&fix[j], fjx, SB_FORCE_SCALE);
+        red_fix_sc(&fix[P.slot_cap + j], fjy, SB_FORCE_SCALE);
+        red_fix_sc(&fix[2 * P.slot_cap + j], fjz, SB_FORCE_SCALE);
+    }
+#pragma unroll
+    for (int k = 0; k < SB_CLUSTER; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            fxi[k] += __shfl_xor_sync(0xffffffffu, fxi[k], o);
+            fyi[k] += __shfl_xor_sync(0xffffffffu, fyi[k], o);
+            fzi[k] += __shfl_xor_sync(0xffffffffu, fzi[k], o);
+            if (EV) {
+                el[k] += __shfl_xor_sync(0xffffffffu, el[k], o);
+                ec[k] += __shfl_xor_sync(0xffffffffu, ec[k], o);
+                ev[k] += __shfl_xor_sync(0xffffffffu, ev[k], o);
+            }
+        }
+        if (lane == k) {
+            const int s = base + k;
+            const int a = slot_atom[s];
+            if (a >= 0) {
+                red_fix_sc(&fix[s], fxi[k], SB_FORCE_SCALE);
+                red_fix_sc(&fix[P.slot_cap + s], fyi[k], SB_FORCE_SCALE);
+                red_fix_sc(&fix[2 * P.slot_cap + s], fzi[k], SB_FORCE_SCALE);
+                if (EV & SB_EV_ENERGY_SC) atom_energy[a] += el[k] + ec[k];
+                if (EV & SB_EV_VIRIAL_SC) {
+                    atom_virial[a] += ev[k];
+                    atom_direct[a] = ec[k];
+                }
+            }
+        }
+    }
+    if (DH) {
+        for (int o = 16; o > 0; o >>= 1) {
+            h_lj += __shfl_xor_sync(0xffffffffu, h_lj, o);
+            h_c += __shfl_xor_sync(0xffffffffu, h_c, o);
+        }
+        if (lane == 0) {
+            red_fix_sc(&hfix[0], h_lj, SB_DHDL_SCALE);
+            red_fix_sc(&hfix[1], h_c, SB_DHDL_SCALE);
+        }
+    }
+}
+
+// plain form: warp per atom over the ATOM_GROUP half list, float atomics (the reference's
+// LJ_Soft_Core_Force_With_Direct_CF_CUDA structure, LJ_soft_core.cu:159-317)
+struct ScAtomGroup {
+    int atom_numbers;
+    int* atom_serial;
+};
+
+__device__ __forceinline__ int sc_tri(int a, int b) {
+    const int M = max(a, b), m = min(a, b);
+    return (M * (M + 1) >> 1) + m;
+}
+
+template <int EV, bool DH>
+__global__ void __launch_bounds__(256) k_pair_sc_plain(
+    ScParams P, int n, const ScAtomGroup* __restrict__ nl, const uint32_t* __restrict__ uc,
+    const float* __restrict__ q, const float* __restrict__ dq, const int* __restrict__ ta,
+    const int* __restrict__ tb, const int* __restrict__ mask, const float* __restrict__ Aa,
+    const float* __restrict__ Ba, const float* __restrict__ Ab, const float* __restrict__ Bb,
+    float* __restrict__ frc, float* __restrict__ hsum, float* __restrict__ atom_energy,
+    float* __restrict__ atom_virial, float* __restrict__ atom_direct) {
+    const int i = blockIdx.x * blockDim.y + threadIdx.y;
+    if (i >= n) return;
+    const ScAtomGroup g = nl[i];
+    const uint32_t ux = uc[3 * i], uy = uc[3 * i + 1], uz = uc[3 * i + 2];
+    const float qi = q[i], dqi = dq[i];
+    const int tai = ta[i], tbi = tb[i], mi = mask[i];
+    float fx = 0.f, fy = 0.f, fz = 0.f, e1 = 0.f, e2 = 0.f, v1 = 0.f, h1 = 0.f, h2 = 0.f;
+    for (int t = threadIdx.x; t < g.atom_numbers; t += blockDim.x) {
+        const int j = g.atom_serial[t];
+        const float dx = (float)(int)(uc[3 * j] - ux) * P.sx;
+        const float dy = (float)(int)(uc[3 * j + 1] - uy) * P.sy;
+        const float dz = (float)(int)(uc[3 * j + 2] - uz) * P.sz;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (!(r2 < P.rc2)) continue;
+        const int ka = sc_tri(tai, ta[j]), kb = sc_tri(tbi, tb[j]);
+        const float2 a = make_float2(Aa[ka], Ba[ka]);
+        const float2 b = make_float2(Ab[kb], Bb[kb]);
+        const bool soft = sc_is_soft(mi, mask[j], a, b);
+        const float qj = q[j];
+        const float fs = sc_pair<EV != 0, DH>(P, r2, qi * qj, dq[j] * qi + qj * dqi, soft, a, b,
+                                              e1, e2, v1, h1, h2);
+        const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
+        fx += tx;
+        fy += ty;
+        fz += tz;
+        atomicAdd(&frc[3 * j], -tx);
+        atomicAdd(&frc[3 * j + 1], -ty);
+        atomicAdd(&frc[3 * j + 2], -tz);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        fx += __shfl_down_sync(0xffffffffu, fx, o);
+        fy += __shfl_down_sync(0xffffffffu, fy, o);
+        fz += __shfl_down_sync(0xffffffffu, fz, o);
+        if (EV) {
+            e1 += __shfl_down_sync(0xffffffffu, e1, o);
+            e2 += __shfl_down_sync(0xffffffffu, e2, o);
+            v1 += __shfl_down_sync(0xffffffffu, v1, o);
+        }
+        if (DH) {
+            h1 += __shfl_down_sync(0xffffffffu, h1, o);
+            h2 += __shfl_down_sync(0xffffffffu, h2, o);
+        }
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&frc[3 * i], fx);
+        atomicAdd(&frc[3 * i + 1], fy);
+        atomicAdd(&frc[3 * i + 2], fz);
+        if (EV & SB_EV_ENERGY_SC) atom_energy[i] += e1 + e2;
+        if (EV & SB_EV_VIRIAL_SC) {
+            atom_virial[i] += v1;
+            atom_direct[i] = e2;
+        }
+        if (DH) {
+            atomicAdd(&hsum[0], h1);
+            atomicAdd(&hsum[1], h2);
+        }
+    }
+}
+
+__global__ void k_sc_zero(long long* __restrict__ h, int n) {
+    const int t = threadIdx.x;
+    if (t < n) h[t] = 0;
+}
+
+// PME cross-term and total: hfix [LJ, direct, reciprocal, correction] (fixed point) + self term
+// from FP64 sums of q dq, q, dq + long-range term -> out (FP64); optionally parts[7]
+__global__ void __launch_bounds__(1024) k_fep_finish(int n, const float* __restrict__ q,
+                                                     const float* __restrict__ dq,
+                                                     const long long* __restrict__ hfix,
+                                                     double self_coef, double neutral2,
+                                                     double lrc, double* __restrict__ out,
+                                                     double* __restrict__ parts) {
+    __shared__ double r1[1024], r2[1024], r3[1024];
+    double a = 0, b = 0, c = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a += (double)q[i] * dq[i];
+        b += q[i];
+        c += dq[i];
+    }
+    r1[threadIdx.x] = a;
+    r2[threadIdx.x] = b;
+    r3[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            r1[threadIdx.x] += r1[threadIdx.x + o];
+            r2[threadIdx.x] += r2[threadIdx.x + o];
+            r3[threadIdx.x] += r3[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double lj = (double)hfix[0] * SB_DHDL_UNSCALE, dir = (double)hfix[1] * SB_DHDL_UNSCALE;
+        const double rec = (double)hfix[2] * SB_DHDL_UNSCALE, cor = (double)hfix[3] * SB_DHDL_UNSCALE;
+        const double self = self_coef * r1[0] + neutral2 * r2[0] * r3[0];
+        if (out) out[0] = lj + dir + rec + cor + self + lrc;
+        if (parts) {
+            parts[0] = lj;
+            parts[1] = dir;
+            parts[2] = rec;
+            parts[3] = self;
+            parts[4] = cor;
+            parts[5] = lrc;
+            parts[6] = lj + dir + rec + cor + self + lrc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------------------------
+static void sc_lrc(sb_softcore* sc) {
+    // dispersion factor mixed linearly in lambda over atom-pair types (LJ_soft_core.cu:85-156)
+    const int nt2 = sc->ntA > sc->ntB ? sc->ntA : sc->ntB;
+    (void)nt2;
+    std::vector<double> cnt((size_t)sc->ntA * sc->ntB, 0.0);
+    for (int i = 0; i < sc->n; i++) cnt[(size_t)sc->htA[i] * sc->ntB + sc->htB[i]] += 1.0;
+    double sa = 0, sb = 0;
+    for (int a1 = 0; a1 < sc->ntA; a1++)
+        for (int b1 = 0; b1 < sc->ntB; b1++) {
+            const double c1 = cnt[(size_t)a1 * sc->ntB + b1];
+            if (c1 == 0) continue;
+            for (int a2 = 0; a2 < sc->ntA; a2++)
+                for (int b2 = 0; b2 < sc->ntB; b2++) {
+                    const double c2 = cnt[(size_t)a2 * sc->ntB + b2];
+                    if (c2 == 0) continue;
+                    const int ka = a1 > a2 ? a1 * (a1 + 1) / 2 + a2 : a2 * (a2 + 1) / 2 + a1;
+                    const int kb = b1 > b2 ? b1 * (b1 + 1) / 2 + b2 : b2 * (b2 + 1) / 2 + b1;
+                    sa += c1 * c2 * (double)sc->hB6a[ka];
+                    sb += c1 * c2 * (double)sc->hB6b[kb];
+                }
+        }
+    const double rc = sc->cutoff;
+    const double kappa = -2.0 / 3.0 * M_PI / (rc * rc * rc) / 6.0;
+    sc->lrc_factor = kappa * ((1.0 - sc->lambda) * sa + sc->lambda * sb);
+    sc->lrc_ti = kappa * (sb - sa);
+}
+
+static ScParams sc_params(const sb_softcore* sc, const sb_neighbor_list* nl, float beta) {
+    ScParams P;
+    P.sx = (1.0f / 4294967296.0f) * nl->box[0];
+    P.sy = (1.0f / 4294967296.0f) * nl->box[1];
+    P.sz = (1.0f / 4294967296.0f) * nl->box[2];
+    P.rc2 = sc->cutoff * sc->cutoff;
+    P.beta = beta;
+    P.beta2 = beta * beta;
+    P.tsp_beta = (float)(2.0 * beta / sqrt(M_PI));
+    P.l = sc->lambda;
+    P.l_ = 1.0f - sc->lambda;
+    const double l = sc->lambda, l_ = 1.0 - l, a = sc->alpha, p = sc->p;
+    P.cA = (float)(a * pow(l, p));
+    P.cB = (float)(a * pow(l_, p));
+    P.dcA = (float)(a * p * pow(l, p - 1.0));
+    P.dcB = (float)(-a * p * pow(l_, p - 1.0));
+    P.s6 = (float)pow((double)sc->sigma, 6.0);
+    P.s6min = (float)pow((double)sc->sigma_min, 6.0);
+    const double b3 = (double)beta * beta * beta;
+    const double pc[6] = {SB_EWALD_P5, SB_EWALD_P4, SB_EWALD_P3, SB_EWALD_P2, SB_EWALD_P1,
+                          SB_EWALD_P0};
+    for (int k = 0; k < 6; k++) P.gp[k] = (float)(b3 * pc[k]);
+    const double brc = (double)beta * sc->cutoff;
+    P.wide = brc * brc > 11.9;
+    P.ntA = sc->ntA;
+    P.ntB = sc->ntB;
+    P.slot_cap = nl->slot_cap;
+    P.ent_cap = nl->ent_cap;
+    return P;
+}
+
+extern "C" int sb_sc_destroy(sb_softcore* sc) {
+    if (!sc) return SB_OK;
+    cudaDeviceSynchronize();
+    void* ps[] = {sc->d_ABa, sc->d_ABb, sc->d_Aa, sc->d_Ba, sc->d_Ab, sc->d_Bb, sc->d_typeA,
+                  sc->d_typeB, sc->d_mask, sc->d_dq, sc->d_slot_ext, sc->d_slot_dq, sc->d_hfix,
+                  sc->d_red, sc->d_scratch_frc};
+    for (void* x : ps) sb_free(x);
+    delete sc;
+    return SB_OK;
+}
+
+static std::vector<float2> square_table(int nt, const float* A, const float* B) {
+    std::vector<float2> t((size_t)nt * nt);
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++) {
+            const int M = a > b ? a : b, m = a > b ? b : a;
+            const int k = M * (M + 1) / 2 + m;
+            t[(size_t)a * nt + b] = make_float2(A[k], B[k]);
+        }
+    return t;
+}
+
+extern "C" int sb_sc_create(int n, int ntA, const float* hAA, const float* hAB, int ntB,
+                            const float* hBA, const float* hBB, const int* htA, const int* htB,
+                            const int* hmask, const float* hdq, float cutoff,
+                            const float box_length[3], float lambda, float alpha, float p,
+                            float sigma, float sigma_min, int form, sb_softcore** out) {
+    if (!out || n <= 0 || ntA <= 0 || ntB <= 0 || !hAA || !hAB || !hBA || !hBB || !htA ||
+        !htB || !hmask || !hdq || !box_length || cutoff <= 0 || ntB > 0xffff) {
+        sb_set_error("sb_sc_create: invalid argument");
+        return SB_ERR_ARG;
+    }
+    for (int i = 0; i < n; i++)
+        if (htA[i] < 0 || htA[i] >= ntA || htB[i] < 0 || htB[i] >= ntB || hmask[i] < 0 ||
+            hmask[i] > 0x7fff) {
+            sb_set_error("sb_sc_create: atom %d has types (%d, %d) or mask %d out of range", i,
+                         htA[i], htB[i], hmask[i]);
+            return SB_ERR_ARG;
+        }
+    if ((size_t)(ntA * ntA + ntB * ntB) * sizeof(float2) > 96 * 1024) {
+        sb_set_error("sb_sc_create: LJ type tables too large for shared memory");
+        return SB_ERR_ARG;
+    }
+    sb_softcore* sc = new sb_softcore();
+    sc->n = n;
+    sc->ntA = ntA;
+    sc->ntB = ntB;
+    sc->form = form;
+    sc->cutoff = cutoff;
+    for (int d = 0; d < 3; d++) sc->box[d] = box_length[d];
+    sc->lambda = lambda;
+    sc->alpha = alpha;
+    sc->p = p;
+    sc->sigma = sigma;
+    sc->sigma_min = sigma_min;
+    const int npa = ntA * (ntA + 1) / 2, npb = ntB * (ntB + 1) / 2;
+    sc->hA12a.assign(hAA, hAA + npa);
+    sc->hB6a.assign(hAB, hAB + npa);
+    sc->hA12b.assign(hBA, hBA + npb);
+    sc->hB6b.assign(hBB, hBB + npb);
+    sc->htA.assign(htA, htA + n);
+    sc->htB.assign(htB, htB + n);
+    const std::vector<float2> ta = square_table(ntA, hAA, hAB), tb = square_table(ntB, hBA, hBB);
+    int st = SB_OK;
+    if ((st = sb_malloc((void**)&sc->d_ABa, sizeof(float2) * ta.size(), "soft-core A table")) ||
+        (st = sb_malloc((void**)&sc->d_ABb, sizeof(float2) * tb.size(), "soft-core B table")) ||
+        (st = sb_malloc((void**)&sc->d_Aa, sizeof(float) * npa, "soft-core AA")) ||
+        (st = sb_malloc((void**)&sc->d_Ba, sizeof(float) * npa, "soft-core AB")) ||
+        (st = sb_malloc((void**)&sc->d_Ab, sizeof(float) * npb, "soft-core BA")) ||
+        (st = sb_malloc((void**)&sc->d_Bb, sizeof(float) * npb, "soft-core BB")) ||
+        (st = sb_malloc((void**)&sc->d_typeA, sizeof(int) * n, "soft-core type A")) ||
+        (st = sb_malloc((void**)&sc->d_typeB, sizeof(int) * n, "soft-core type B")) ||
+        (st = sb_malloc((void**)&sc->d_mask, sizeof(int) * n, "soft-core mask")) ||
+        (st = sb_malloc((void**)&sc->d_dq, sizeof(float) * n, "soft-core dq")) ||
+        (st = sb_malloc((void**)&sc->d_hfix, sizeof(long long) * 4, "dH/dlambda")) ||
+        (st = sb_malloc((void**)&sc->d_red, sizeof(double) * 8, "soft-core reduce"))) {
+        sb_sc_destroy(sc);
+        return st;
+    }
+    cudaMemcpy(sc->d_ABa, ta.data(), sizeof(float2) * ta.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_ABb, tb.data(), sizeof(float2) * tb.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_Aa, hAA, sizeof(float) * npa, cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_Ba, hAB, sizeof(float) * npa, cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_Ab, hBA, sizeof(float) * npb, cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_Bb, hBB, sizeof(float) * npb, cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_typeA, htA, sizeof(int) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_typeB, htB, sizeof(int) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->d_mask, hmask, sizeof(int) * n, cudaMemcpyHostToDevice);
+    const cudaError_t e = cudaMemcpy(sc->d_dq, hdq, sizeof(float) * n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        sb_set_error("sb_sc_create: %s", cudaGetErrorString(e));
+        sb_sc_destroy(sc);
+        return SB_ERR_CUDA;
+    }
+    sc_lrc(sc);
+    *out = sc;
+    return SB_OK;
+}
+
+extern "C" int sb_sc_set_lambda(sb_softcore* sc, float lambda) {
+    if (!sc || !(lambda >= 0.f && lambda <= 1.f)) {
+        sb_set_error("sb_sc_set_lambda: lambda must lie in [0, 1]");
+        return SB_ERR_ARG;
+    }
+    sc->lambda = lambda;
+    sc_lrc(sc);
+    return SB_OK;
+}
+
+// per-slot extras sized for the list (re-created when a list with more slots comes along)
+static int sc_slots(sb_softcore* sc, sb_neighbor_list* nl, cudaStream_t s) {
+    if (sc->slot_cap < nl->slot_cap) {
+        sb_free(sc->d_slot_ext);
+        sb_free(sc->d_slot_dq);
+        sc->d_slot_ext = nullptr;
+        sc->d_slot_dq = nullptr;
+        sc->slot_cap = 0;
+        SB_TRY(sb_malloc((void**)&sc->d_slot_ext, sizeof(int) * nl->slot_cap, "soft-core slots"));
+        SB_TRY(sb_malloc((void**)&sc->d_slot_dq, sizeof(float) * nl->slot_cap, "soft-core slots"));
+        sc->slot_cap = nl->slot_cap;
+    }
+    k_sc_pack<<<(nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->meta, nl->slot_atom, sc->d_typeB,
+                                                         sc->d_mask, sc->d_dq, sc->d_slot_ext,
+                                                         sc->d_slot_dq);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+// fixed form: pack + soft-core pair kernel into the list's fixed-point force buffer
+static int sc_launch_fixed(sb_softcore* sc, sb_neighbor_list* nl, const uint32_t* uc,
+                           const float* q, float beta, int ev, bool dh, float* ae, float* av,
+                           float* ad, cudaStream_t s) {
+    SB_TRY(sb_nl_pack(nl, uc, q, sc->d_typeA, s));
+    SB_TRY(sc_slots(sc, nl, s));
+    const ScParams P = sc_params(sc, nl, beta);
+    const size_t smem = sizeof(float2) * (size_t)(sc->ntA * sc->ntA + sc->ntB * sc->ntB);
+    const int blocks = (nl->clu_cap + 3) / 4;
+#define SB_LAUNCH_SC(EVV, DHV)                                                                   \
+    do {                                                                                         \
+        if (smem > 40 * 1024)                                                                    \
+            cudaFuncSetAttribute(k_pair_sc<EVV, DHV>,                                            \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);        \
+        k_pair_sc<EVV, DHV><<<blocks, 128, smem, s>>>(                                           \
+            P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, sc->d_slot_ext,            \
+            sc->d_slot_dq, sc->d_ABa, sc->d_ABb, nl->slot_atom, nl->fix, sc->d_hfix, ae, av, ad); \
+    } while (0)
+    if (dh) {
+        switch (ev) {
+            case 0: SB_LAUNCH_SC(0, true); break;
+            case 1: SB_LAUNCH_SC(1, true); break;
+            case 2: SB_LAUNCH_SC(2, true); break;
+            default: SB_LAUNCH_SC(3, true); break;
+        }
+    } else {
+        switch (ev) {
+            case 0: SB_LAUNCH_SC(0, false); break;
+            case 1: SB_LAUNCH_SC(1, false); break;
+            case 2: SB_LAUNCH_SC(2, false); break;
+            default: SB_LAUNCH_SC(3, false); break;
+        }
+    }
+#undef SB_LAUNCH_SC
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+// plain form: ATOM_GROUP walk with float atomics; dH/dlambda into d_red (float pair [0..1])
+static int sc_launch_plain(sb_softcore* sc, sb_neighbor_list* nl, const uint32_t* uc,
+                           const float* q, float* frc, float beta, int ev, bool dh, float* ae,
+                           float* av, float* ad, cudaStream_t s) {
+    SB_TRY(sb_nl_build_atom_group(nl, s));
+    const ScParams P = sc_params(sc, nl, beta);
+    const dim3 blk(32, 8);
+    const int grid = (sc->n + 7) / 8;
+    float* hsum = (float*)sc->d_red;
+#define SB_LAUNCH_SCP(EVV, DHV)                                                                  \
+    k_pair_sc_plain<EVV, DHV><<<grid, blk, 0, s>>>(                                             \
+        P, sc->n, (const ScAtomGroup*)nl->ag, uc, q, sc->d_dq, sc->d_typeA, sc->d_typeB,        \
+        sc->d_mask, sc->d_Aa, sc->d_Ba, sc->d_Ab, sc->d_Bb, frc, hsum, ae, av, ad)
+    if (dh) {
+        switch (ev) {
+            case 0: SB_LAUNCH_SCP(0, true); break;
+            case 1: SB_LAUNCH_SCP(1, true); break;
+            case 2: SB_LAUNCH_SCP(2, true); break;
+            default: SB_LAUNCH_SCP(3, true); break;
+        }
+    } else {
+        switch (ev) {
+            case 0: SB_LAUNCH_SCP(0, false); break;
+            case 1: SB_LAUNCH_SCP(1, false); break;
+            case 2: SB_LAUNCH_SCP(2, false); break;
+            default: SB_LAUNCH_SCP(3, false); break;
+        }
+    }
+#undef SB_LAUNCH_SCP
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+__global__ void k_sc_zero_f(int n, float* p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = 0.f;
+}
+
+extern "C" int sb_sc_pme_direct_force(sb_softcore* sc, sb_neighbor_list* nl, int atom_numbers,
+                                      const uint32_t* d_uint_crd, const float* d_charge,
+                                      float* d_frc, float pme_beta, int need_atom_energy,
+                                      float* d_atom_energy, int need_virial,
+                                      float* d_atom_lj_virial, float* d_atom_direct_pme_energy,
+                                      void* stream) {
+    if (!sc || !nl || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_sc_pme_direct_force: null argument");
+        return SB_ERR_ARG;
+    }
+    if (atom_numbers != sc->n || nl->n != sc->n) {
+        sb_set_error("sb_sc_pme_direct_force: atom count %d does not match the modules (%d, %d)",
+                     atom_numbers, sc->n, nl->n);
+        return SB_ERR_ARG;
+    }
+    if ((need_atom_energy > 0 && !d_atom_energy) ||
+        (need_virial > 0 && (!d_atom_lj_virial || !d_atom_direct_pme_energy))) {
+        sb_set_error("sb_sc_pme_direct_force: energy/virial output missing");
+        return SB_ERR_ARG;
+    }
+    SB_TRY(sb_nl_ensure_built(nl));
+    cudaStream_t s = sb_stream(stream);
+    const int ev = (need_atom_energy > 0 ? SB_EV_ENERGY_SC : 0) |
+                   (need_virial > 0 ? SB_EV_VIRIAL_SC : 0);
+    if (sc->form == SB_FORM_PLAIN)
+        return sc_launch_plain(sc, nl, d_uint_crd, d_charge, d_frc, pme_beta, ev, false,
+                               d_atom_energy, d_atom_lj_virial, d_atom_direct_pme_energy, s);
+    SB_TRY(sc_launch_fixed(sc, nl, d_uint_crd, d_charge, pme_beta, ev, false, d_atom_energy,
+                           d_atom_lj_virial, d_atom_direct_pme_energy, s));
+    return sb_nl_finalize_forces(nl, d_frc, s);
+}
+
+__global__ void k_sc_device_add(float* p, float v) { p[0] += v; }
+
+extern "C" int sb_sc_long_range_correction(sb_softcore* sc, int need_pressure, float* d_virial,
+                                           int need_potential, float* d_potential,
+                                           void* stream) {
+    if (!sc) {
+        sb_set_error("sb_sc_long_range_correction: null handle");
+        return SB_ERR_ARG;
+    }
+    cudaStream_t s = sb_stream(stream);
+    const double V = (double)sc->box[0] * sc->box[1] * sc->box[2];
+    if (need_pressure > 0) {
+        if (!d_virial) {
+            sb_set_error("sb_sc_long_range_correction: d_virial is NULL");
+            return SB_ERR_ARG;
+        }
+        k_sc_device_add<<<1, 1, 0, s>>>(d_virial, (float)(sc->lrc_factor * 6.0 / V));
+        SB_CHECK_LAUNCH();
+    }
+    if (need_potential > 0) {
+        if (!d_potential) {
+            sb_set_error("sb_sc_long_range_correction: d_potential is NULL");
+            return SB_ERR_ARG;
+        }
+        k_sc_device_add<<<1, 1, 0, s>>>(d_potential, (float)(sc->lrc_factor / V));
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+__global__ void k_sc_hsum(const float* __restrict__ hf, const long long* __restrict__ hfix,
+                          int plain, double* __restrict__ out) {
+    if (threadIdx.x == 0) {
+        out[0] = plain ? (double)hf[0] : (double)hfix[0] * SB_DHDL_UNSCALE;
+        out[1] = plain ? (double)hf[1] : (double)hfix[1] * SB_DHDL_UNSCALE;
+    }
+}
+
+extern "C" int sb_sc_dh_dlambda(sb_softcore* sc, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                                const float* d_charge, float pme_beta, double* h_dhdl,
+                                void* stream) {
+    if (!sc || !nl || !d_uint_crd || !d_charge || !h_dhdl) {
+        sb_set_error("sb_sc_dh_dlambda: null argument");
+        return SB_ERR_ARG;
+    }
+    if (nl->n != sc->n) {
+        sb_set_error("sb_sc_dh_dlambda: the list has %d atoms, the module %d", nl->n, sc->n);
+        return SB_ERR_ARG;
+    }
+    SB_TRY(sb_nl_ensure_built(nl));
+    cudaStream_t s = sb_stream(stream);
+    const int plain = sc->form == SB_FORM_PLAIN;
+    if (plain) {
+        if (!sc->d_scratch_frc)
+            SB_TRY(sb_malloc((void**)&sc->d_scratch_frc, sizeof(float) * 3 * sc->n, "dH scratch"));
+        SB_CHECK_CUDA(cudaMemsetAsync(sc->d_red, 0, sizeof(double) * 8, s));
+        SB_TRY(sc_launch_plain(sc, nl, d_uint_crd, d_charge, sc->d_scratch_frc, pme_beta, 0, true,
+                               nullptr, nullptr, nullptr, s));
+    } else {
+        k_sc_zero<<<1, 32, 0, s>>>(sc->d_hfix, 4);
+        SB_CHECK_LAUNCH();
+        SB_TRY(sc_launch_fixed(sc, nl, d_uint_crd, d_charge, pme_beta, 0, true, nullptr, nullptr,
+                               nullptr, s));
+        // the pass also accumulated forces: discard them
+        SB_CHECK_CUDA(cudaMemsetAsync(nl->fix, 0, sizeof(long long) * 3 * nl->slot_cap, s));
+    }
+    k_sc_hsum<<<1, 32, 0, s>>>((const float*)sc->d_red, sc->d_hfix, plain, sc->d_red + 4);
+    SB_CHECK_LAUNCH();
+    double h[2];
+    SB_CHECK_CUDA(cudaMemcpyAsync(h, sc->d_red + 4, sizeof(h), cudaMemcpyDeviceToHost, s));
+    SB_CHECK_CUDA(cudaStreamSynchronize(s));
+    const double V = (double)sc->box[0] * sc->box[1] * sc->box[2];
+    h_dhdl[0] = h[0];
+    h_dhdl[1] = h[1];
+    h_dhdl[2] = sc->lrc_ti / V;
+    return SB_OK;
+}
+
+extern "C" int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
+                           const uint32_t* d_uint_crd, const float* d_charge, const int* es,
+                           const int* el, const int* en, float* d_frc, double* d_dudl,
+                           void* stream) {
+    if (!nl || !sc || !pme || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_fep_step: null argument");
+        return SB_ERR_ARG;
+    }
+    if (nl->n != sc->n || pme->n != sc->n) {
+        sb_set_error("sb_fep_step: modules disagree on the atom count");
+        return SB_ERR_ARG;
+    }
+    if (nl->form != SB_FORM_FIXED || sc->form != SB_FORM_FIXED || pme->form != SB_FORM_FIXED) {
+        sb_set_error("sb_fep_step: needs the fixed-point form of all modules");
+        return SB_ERR_ARG;
+    }
+    SB_TRY(sb_nl_ensure_built(nl));
+    cudaStream_t s = sb_stream(stream);
+    const bool dh = d_dudl != nullptr;
+    if (dh) {
+        k_sc_zero<<<1, 32, 0, s>>>(sc->d_hfix, 4);
+        SB_CHECK_LAUNCH();
+    }
+    SB_TRY(sc_launch_fixed(sc, nl, d_uint_crd, d_charge, pme->beta, 0, dh, nullptr, nullptr,
+                           nullptr, s));
+    SB_TRY(sb_pme_fused_excluded(pme, nl, d_uint_crd, d_charge, es, el, en, nullptr, s));
+    SB_TRY(sb_pme_fused_reciprocal(pme, nl, d_frc, d_charge, 0, 0, nullptr, nullptr, s));
+    if (dh) {
+        SB_TRY(sb_pme_ti_terms_slot(pme, nl, sc->d_slot_dq, d_uint_crd, d_charge, sc->d_dq, es,
+                                    el, en, sc->d_hfix + 2, s));
+        const double V = (double)sc->box[0] * sc->box[1] * sc->box[2];
+        k_fep_finish<<<1, 1024, 0, s>>>(sc->n, d_charge, sc->d_dq, sc->d_hfix,
+                                        -2.0 * (double)pme->beta / sqrt(M_PI),
+                                        2.0 * pme->neutralizing_factor, sc->lrc_ti / V, d_dudl,
+                                        nullptr);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}

@@ -1,0 +1,178 @@
+"""FEP/TI windows: one soft-core system per lambda, and many of them batched on one GPU.
+
+``FepEngine(system)`` wires NEIGHBOR_LIST, LJ_SOFT_CORE and Particle_Mesh_Ewald for one box of
+``sponge_b200.systems.fep_box`` (the charges at the box's lambda, their change per unit lambda,
+A/B LJ types and tables, the perturbation mask). ``step()`` is one force evaluation with
+dU/dlambda (``sb_fep_step``: soft-core LJ + direct, exclusion correction, reciprocal space, PME
+cross terms and the long-range correction, no host synchronisation).
+
+``FepBatch(systems)`` runs many such boxes of uneven size together: every box keeps its own
+modules and list; one force step of all boxes is captured once as a CUDA graph whose branches run
+the boxes concurrently on separate streams, and each step replays it. The number of streams the
+boxes are spread over is picked by timing (``tune``). List rebuilds run between replays.
+"""
+
+import numpy as np
+
+from . import (FORM_FIXED, NeighborList, ParticleMeshEwald, SoftCore, _require_cuda,
+               crd_to_uint_crd, fep_step, pme_ti_cross)
+
+
+def _scaled(x, f):
+    return (np.asarray(x, np.float32) * np.float32(f)).astype(np.float32)
+
+
+class FepEngine:
+    def __init__(self, system, form=FORM_FIXED, refresh_interval=20, max_neighbor_numbers=1200,
+                 device="cuda"):
+        torch = _require_cuda()
+        self.torch = torch
+        self.system = s = system
+        self.n = n = len(s["charge"])
+        self.box = np.asarray(s["box"], np.float32)
+        dev = torch.device(device)
+        self.crd = torch.tensor(np.asarray(s["crd"], np.float32), device=dev)
+        self.charge = torch.tensor(np.asarray(s["charge"], np.float32), device=dev)
+        self.dq = torch.tensor(np.asarray(s["dq"], np.float32), device=dev)
+        self.excl_start = torch.tensor(s["excl_start"], dtype=torch.int32, device=dev)
+        self.excl_numbers = torch.tensor(s["excl_numbers"], dtype=torch.int32, device=dev)
+        el = s["excl_list"] if len(s["excl_list"]) else np.zeros(1, np.int32)
+        self.excl_list = torch.tensor(el, dtype=torch.int32, device=dev)
+        self.uint_crd = torch.empty((n, 3), dtype=torch.int32, device=dev)
+        self.frc = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+        self.dudl = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.nl = NeighborList(n, self.box, s["cutoff"], s["skin"], refresh_interval,
+                               max_neighbor_numbers=max_neighbor_numbers, form=form)
+        self.sc = SoftCore(n, _scaled(s["lj_A"], 12), _scaled(s["lj_B"], 6),
+                           _scaled(s["lj_A_B"], 12), _scaled(s["lj_B_B"], 6), s["lj_type"],
+                           s["lj_type_B"], s["mask"], s["dq"], s["cutoff"], self.box, s["lam"],
+                           s["sc_alpha"], s["sc_p"], s["sc_sigma"], s["sc_sigma_min"], form=form,
+                           n_types_A=s["n_types"], n_types_B=s["n_types_B"])
+        self.pme = ParticleMeshEwald(n, self.box, s["cutoff"], s["tolerance"], s["fft"],
+                                     form=form)
+        self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
+        self.form = form
+
+    @property
+    def excl(self):
+        return (self.excl_start, self.excl_list, self.excl_numbers)
+
+    def update_list(self, forced=0, stream=None):
+        self.nl.Neighbor_List_Update(self.crd, self.excl_start, self.excl_list, self.excl_numbers,
+                                     forced_update=forced, stream=stream)
+
+    def to_uint(self, stream=None):
+        crd_to_uint_crd(self.crd, self.box, out=self.uint_crd, stream=stream)
+
+    def step(self, want_dudl=True, stream=None):
+        """Fused fixed-form FEP force step (forces += into self.frc, dU/dlambda to self.dudl)."""
+        fep_step(self.nl, self.sc, self.pme, self.uint_crd, self.charge, self.excl, self.frc,
+                 self.dudl if want_dudl else None, stream=stream)
+
+    def forces_modules(self, stream=None):
+        """The module-by-module sequence (either form): soft-core LJ + direct, exclusion
+        correction, reciprocal space, forces += into self.frc."""
+        self.sc.LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial(
+            self.n, self.uint_crd, self.charge, self.frc, self.nl, self.pme.beta, stream=stream)
+        self.pme.PME_Excluded_Force_With_Atom_Energy(
+            self.uint_crd, self.scaler, self.charge, self.excl_start, self.excl_list,
+            self.excl_numbers, self.frc, self.pme.d_correction_atom_energy, stream=stream)
+        self.pme.PME_Reciprocal_Force_With_Energy_And_Virial(self.uint_crd, self.charge,
+                                                             self.frc, stream=stream)
+
+    def dudl_parts(self, stream=None):
+        """dU/dlambda by parts through the module calls (synchronising)."""
+        lj, direct, lrc = self.sc.Get_Partial_H_Partial_Lambda(self.uint_crd, self.charge,
+                                                               self.nl, self.pme.beta,
+                                                               stream=stream)
+        parts = dict(dhdl_lj=lj, dhdl_direct=direct, dhdl_lrc=lrc)
+        if self.form == FORM_FIXED:
+            rec, slf, cor = pme_ti_cross(self.pme, self.uint_crd, self.charge, self.dq,
+                                         self.excl, stream=stream)
+            parts.update(cross_rec=rec, cross_self=slf, cross_corr=cor)
+        return parts
+
+
+class FepBatch:
+    """Many FEP boxes on one GPU, one captured CUDA graph per force step."""
+
+    def __init__(self, systems, refresh_interval=20):
+        torch = _require_cuda()
+        self.torch = torch
+        self.engines = [FepEngine(s, refresh_interval=refresh_interval) for s in systems]
+        self.refresh_interval = refresh_interval
+        self.dudl = torch.zeros(len(self.engines), dtype=torch.float64, device="cuda")
+        for k, e in enumerate(self.engines):
+            e.dudl = self.dudl[k:k + 1]
+        self.graph = None
+        self.n_streams = None
+        self.count = 0
+
+    @property
+    def atoms(self):
+        return sum(e.n for e in self.engines)
+
+    def rebuild(self):
+        for e in self.engines:
+            e.update_list(forced=1)
+            e.to_uint()
+
+    def _eager_step(self):
+        for e in self.engines:
+            e.frc.zero_()
+            e.step()
+
+    def capture(self, n_streams):
+        """Capture one force step of every box; box k runs on stream k mod n_streams."""
+        torch = self.torch
+        self._eager_step()  # first calls size per-list scratch outside the capture
+        torch.cuda.synchronize()
+        main = torch.cuda.Stream()
+        streams = [torch.cuda.Stream() for _ in range(n_streams)]
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=main):
+            cur = torch.cuda.current_stream()
+            for st in streams:
+                st.wait_stream(cur)
+            for k, e in enumerate(self.engines):
+                st = streams[k % n_streams]
+                with torch.cuda.stream(st):
+                    e.frc.zero_()
+                    e.step(stream=st)
+            for st in streams:
+                cur.wait_stream(st)
+        self.graph = g
+        self.n_streams = n_streams
+        self._streams = (main, streams)
+        return g
+
+    def step(self):
+        """One step of all boxes: list rebuild every refresh_interval steps, then the graph."""
+        if self.count % self.refresh_interval == 0:
+            self.rebuild()
+        self.graph.replay()
+        self.count += 1
+
+    def tune(self, candidates=(1, 4, 8, 16, 48), reps=5):
+        """Pick the stream count of the captured step by timing its replay."""
+        torch = self.torch
+        best = None
+        for ns in candidates:
+            if ns > len(self.engines):
+                continue
+            self.capture(ns)
+            for _ in range(2):
+                self.graph.replay()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                self.graph.replay()
+            b.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / reps
+            if best is None or ms < best[1]:
+                best = (ns, ms)
+        self.capture(best[0])
+        return best
