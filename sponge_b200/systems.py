@@ -270,10 +270,14 @@ def config3_fit(n_frames=16, seed=1003, jitter=0.05, noise=0.05):
 WATER_VOLUME = 18.01528 / (0.997 * 0.602214076)  # A^3 per molecule at 0.997 g/cm^3
 
 
-def fft_smooth(n):
-    """Smallest 2-3-5-smooth integer >= n (an FFT-friendly grid size)."""
-    k = max(int(n), 1)
+def fft_smooth(n, even=True):
+    """Smallest 2-3-5-smooth integer >= n (an FFT-friendly grid size), even by default (the
+    real-to-complex transform along z halves the last size)."""
+    k = max(int(n), 2 if even else 1)
     while True:
+        if even and k % 2:
+            k += 1
+            continue
         m = k
         for f in (2, 3, 5):
             while m % f == 0:
@@ -291,7 +295,7 @@ def fep_box(n_water, lam, seed, n_solute=20, q_sigma=0.3, cutoff=9.0, skin=2.0, 
     is fully coupled in state A and vanishes in state B: B-state LJ type ``n_types`` has no LJ
     and B-state charges are zero, so the charges at ``lam`` are (1 - lam) q_A. Waters are
     unperturbed. Soft-core parameters follow LJ_SOFT_CORE::Initial's keys (alpha, p, sigma,
-    sigma_min; LJ_soft_core.cu:1420-1610). PME grid ~1 A, 2-3-5-smooth."""
+    sigma_min; LJ_soft_core.cu:1420-1610). PME grid ~1 A, even and 2-3-5-smooth."""
     L = float((n_water * WATER_VOLUME) ** (1.0 / 3.0))
     k = fft_smooth(int(np.ceil(L)))
     n_side = int(np.ceil((n_water * 1.12) ** (1.0 / 3.0)))
