@@ -176,3 +176,21 @@ class FepBatch:
                 best = (ns, ms)
         self.capture(best[0])
         return best
+
+
+def shard_boxes(costs, world):
+    """Greedy assignment of boxes to ranks, largest first onto the least-loaded rank.
+    Returns a list of box-index lists, one per rank (each sorted)."""
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for k in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        r = min(range(world), key=lambda j: (load[j], j))
+        parts[r].append(k)
+        load[r] += costs[k]
+    return [sorted(p) for p in parts]
+
+
+def box_cost(system):
+    """Relative cost of one box's step: atoms (pair work) plus grid points (FFT work)."""
+    K = system["fft"]
+    return float(len(system["charge"])) + 0.25 * float(K[0] * K[1] * K[2])
