@@ -1,15 +1,17 @@
 // Hand-written shared-memory 3D real FFT + Green's-function convolution for PME reciprocal
 // space (replaces cufftExecR2C / PME_BCFQ / cufftExecC2R, SPONGE/PME_force/PME_force.cu:741-747).
 //
-// Three kernels per convolution, each touching the grid once (the grids are L2-resident):
-//   k_plane_fwd   one block per x-plane: reads the int64 fixed-point charge grid (and clears it
-//                 for the next step), real-to-complex along z (length K2 via a K2/2 complex FFT,
-//                 decimation in time, digit-reversed load), then forward along y (decimation in
-//                 frequency, digit-reversed store) -> half spectrum C[x][ky][kz], kz <= K2/2.
-//   k_xconv       one block per (ky, 16 kz columns): forward along x (DIT), multiply by
-//                 BC(kx,ky,kz) and accumulate the FP64 reciprocal energy, inverse along x (DIF).
-//   k_plane_inv   one block per x-plane: inverse along y (DIT), complex-to-real along z (DIF)
-//                 -> real potential grid theta[x][y][z].
+// Five passes per convolution, each touching the grid once (the grids are L2-resident):
+//   k_zfwd        32 rows per block: reads the int64 fixed-point charge grid (and clears it for
+//                 the next step), real-to-complex along z (length K2 via a K2/2 complex FFT,
+//                 decimation in time, digit-reversed load) -> half spectrum rows, kz <= K2/2
+//   k_ypass       16 (x, kz) lines per block: forward along y (DIT)
+//   k_xconv       16 (ky, kz) lines per block: forward along x (DIT), multiply by BC(kx,ky,kz)
+//                 and accumulate the FP64 reciprocal energy, inverse along x (DIF)
+//   k_ypass       inverse along y
+//   k_zinv        complex-to-real along z -> real potential grid theta[x][y][z]
+// Line tiles run across planes, so no block computes padding; the stage loops divide by the
+// butterfly span through a multiply-high with a precomputed reciprocal.
 // Mixed radix 2/3/4/5/7. DIT with stage radices r1..rS applied to digit-reversed input and DIF
 // with the mirrored order both use one permutation table per axis, so no pass needs a second
 // buffer or an explicit transpose. All transforms are unnormalised, as cuFFT's are.
@@ -25,7 +27,15 @@ struct FftAxisDev {
     int n;
     int nrad;
     int rad[SB_FFT_MAX_STAGES];
+    // m_s = rad[0] * ... * rad[s-1] (the butterfly span of stage s) and ceil(2^32 / m_s), so that
+    // b / m_s = __umulhi(b, mrec[s]) exactly for b < 2^16 (0 marks m_s = 1)
+    int m[SB_FFT_MAX_STAGES];
+    unsigned mrec[SB_FFT_MAX_STAGES];
 };
+
+__device__ __forceinline__ int div_m(int b, int m, unsigned rec) {
+    return m == 1 ? b : (int)__umulhi((unsigned)b, rec);
+}
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -79,17 +89,17 @@ __device__ __forceinline__ void dft_r(float2* y, const float2* tw, int n, bool i
     }
 }
 
-template <int R>
-__device__ __forceinline__ void dit_stage(float2* buf, int nl, int ls, int es, int n, int m,
-                                          const float2* tw, bool inv) {
+template <int R, int NL>
+__device__ __forceinline__ void dit_stage(float2* buf, int ls, int es, int n, int m,
+                                          unsigned mrec, const float2* tw, bool inv) {
     const int L = m * R;
     const int step = n / L;
     const int nb = n / R;
-    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
+    for (int t = threadIdx.x; t < NL * nb; t += blockDim.x) {
         // consecutive threads take consecutive lines: for column lines (ls == 1) the threads of
         // a warp touch adjacent words and shared-memory bank conflicts disappear
-        const int b = t / nl, l = t - b * nl;
-        const int blk = b / m, k = b - blk * m;
+        const int b = t / NL, l = t - b * NL;
+        const int blk = div_m(b, m, mrec), k = b - blk * m;
         float2* p = buf + l * ls + (blk * L + k) * es;
         float2 y[R];
         y[0] = p[0];
@@ -101,17 +111,15 @@ __device__ __forceinline__ void dit_stage(float2* buf, int nl, int ls, int es, i
     }
 }
 
-template <int R>
-__device__ __forceinline__ void dif_stage(float2* buf, int nl, int ls, int es, int n, int Lb,
-                                          const float2* tw, bool inv) {
-    const int m = Lb / R;
+template <int R, int NL>
+__device__ __forceinline__ void dif_stage(float2* buf, int ls, int es, int n, int m,
+                                          unsigned mrec, const float2* tw, bool inv) {
+    const int Lb = m * R;
     const int step = n / Lb;
     const int nb = n / R;
-    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-        // consecutive threads take consecutive lines: for column lines (ls == 1) the threads of
-        // a warp touch adjacent words and shared-memory bank conflicts disappear
-        const int b = t / nl, l = t - b * nl;
-        const int blk = b / m, n1 = b - blk * m;
+    for (int t = threadIdx.x; t < NL * nb; t += blockDim.x) {
+        const int b = t / NL, l = t - b * NL;
+        const int blk = div_m(b, m, mrec), n1 = b - blk * m;
         float2* p = buf + l * ls + (blk * Lb + n1) * es;
         float2 y[R];
 #pragma unroll
@@ -123,37 +131,37 @@ __device__ __forceinline__ void dif_stage(float2* buf, int nl, int ls, int es, i
     }
 }
 
-// in-place transforms of nl lines (line l at buf + l*ls, element stride es)
-__device__ void fft_dit(float2* buf, int nl, int ls, int es, const FftAxisDev& A,
-                        const float2* tw, bool inv) {
-    int m = 1;
+// in-place transforms of NL lines (line l at buf + l*ls, element stride es)
+template <int NL>
+__device__ __forceinline__ void fft_dit(float2* buf, int ls, int es, const FftAxisDev& A,
+                                        const float2* tw, bool inv) {
     for (int s = 0; s < A.nrad; s++) {
-        const int r = A.rad[s];
-        switch (r) {
-            case 2: dit_stage<2>(buf, nl, ls, es, A.n, m, tw, inv); break;
-            case 3: dit_stage<3>(buf, nl, ls, es, A.n, m, tw, inv); break;
-            case 4: dit_stage<4>(buf, nl, ls, es, A.n, m, tw, inv); break;
-            case 5: dit_stage<5>(buf, nl, ls, es, A.n, m, tw, inv); break;
-            default: dit_stage<7>(buf, nl, ls, es, A.n, m, tw, inv); break;
+        const int m = A.m[s];
+        const unsigned mr = A.mrec[s];
+        switch (A.rad[s]) {
+            case 2: dit_stage<2, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            case 3: dit_stage<3, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            case 4: dit_stage<4, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            case 5: dit_stage<5, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            default: dit_stage<7, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
         }
-        m *= r;
         __syncthreads();
     }
 }
 
-__device__ void fft_dif(float2* buf, int nl, int ls, int es, const FftAxisDev& A,
-                        const float2* tw, bool inv) {
-    int Lb = A.n;
+template <int NL>
+__device__ __forceinline__ void fft_dif(float2* buf, int ls, int es, const FftAxisDev& A,
+                                        const float2* tw, bool inv) {
     for (int s = A.nrad - 1; s >= 0; s--) {
-        const int r = A.rad[s];
-        switch (r) {
-            case 2: dif_stage<2>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
-            case 3: dif_stage<3>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
-            case 4: dif_stage<4>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
-            case 5: dif_stage<5>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
-            default: dif_stage<7>(buf, nl, ls, es, A.n, Lb, tw, inv); break;
+        const int m = A.m[s];
+        const unsigned mr = A.mrec[s];
+        switch (A.rad[s]) {
+            case 2: dif_stage<2, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            case 3: dif_stage<3, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            case 4: dif_stage<4, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            case 5: dif_stage<5, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
+            default: dif_stage<7, NL>(buf, ls, es, A.n, m, mr, tw, inv); break;
         }
-        Lb /= r;
         __syncthreads();
     }
 }
@@ -210,37 +218,49 @@ __device__ void load_tables(SmemTables& T, const int* pa, const int* pb, const f
 // ---------------------------------------------------------------------------------------------
 // x pass with the convolution: forward x (DIT), * BC, energy, inverse x (DIF)
 // ---------------------------------------------------------------------------------------------
+// Column passes (x and y) work on tiles of NL lines: a line is one (plane, kz) pair of the half
+// spectrum, tiles run across planes so that no block computes padding, and each line's base
+// address is computed once per block.
 #define SB_XCONV_T 16
-__global__ void __launch_bounds__(256) k_xconv(FftAxisDev Ax, const int* __restrict__ px,
-                                               const float2* __restrict__ twx,
-                                               float2* __restrict__ spec,
-                                               const float* __restrict__ bc,
-                                               double* __restrict__ epart, int K0, int K1,
-                                               int H, int K2) {
+#define SB_YT 16
+
+template <int NL>
+__global__ void __launch_bounds__(16 * NL) k_xconv(FftAxisDev Ax, const int* __restrict__ px,
+                                                   const float2* __restrict__ twx,
+                                                   float2* __restrict__ spec,
+                                                   const float* __restrict__ bc,
+                                                   double* __restrict__ epart, int K0, int K1,
+                                                   int H, int K2) {
     extern __shared__ __align__(16) char sm[];
+    __shared__ int cbase[NL], ckz[NL];
     SmemTables T = carve(sm, K0, 0, 0);
+    const int nlines = K1 * H;
+    const int l0 = blockIdx.x * NL;
+    if (threadIdx.x < NL) {
+        const int l = l0 + threadIdx.x;
+        const int y = l / H, kz = l - y * H;
+        cbase[threadIdx.x] = l < nlines ? y * H + kz : -1;
+        ckz[threadIdx.x] = kz;
+    }
     load_tables(T, px, px, twx, twx, twx, K0, 0, 0);
-    float2* D = T.data;  // [K0][SB_XCONV_T]
-    const int y = blockIdx.x;
-    const int kz0 = blockIdx.y * SB_XCONV_T;
-    const int nt = min(SB_XCONV_T, H - kz0);
+    float2* D = T.data;  // [K0][NL]
     const size_t pstride = (size_t)K1 * H;
-    for (int t = threadIdx.x; t < K0 * SB_XCONV_T; t += blockDim.x) {
-        const int p = t / SB_XCONV_T, c = t - p * SB_XCONV_T;
-        float2 v = make_float2(0.f, 0.f);
-        if (c < nt) v = spec[(size_t)T.perm_a[p] * pstride + (size_t)y * H + kz0 + c];
-        D[p * SB_XCONV_T + c] = v;
+    for (int t = threadIdx.x; t < K0 * NL; t += blockDim.x) {
+        const int p = t / NL, c = t - p * NL;
+        const int cb = cbase[c];
+        D[t] = cb >= 0 ? spec[(size_t)T.perm_a[p] * pstride + cb] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_dit(D, SB_XCONV_T, 1, SB_XCONV_T, Ax, T.tw_a, false);
+    fft_dit<NL>(D, 1, NL, Ax, T.tw_a, false);
     double e = 0.0;
-    for (int t = threadIdx.x; t < K0 * SB_XCONV_T; t += blockDim.x) {
-        const int kx = t / SB_XCONV_T, c = t - kx * SB_XCONV_T;
-        if (c < nt) {
-            const int kz = kz0 + c;
-            const float g = bc[((size_t)kx * K1 + y) * H + kz];
+    for (int t = threadIdx.x; t < K0 * NL; t += blockDim.x) {
+        const int kx = t / NL, c = t - kx * NL;
+        const int cb = cbase[c];
+        if (cb >= 0) {
+            const float g = bc[(size_t)kx * pstride + cb];
             float2 v = D[t];
             if (epart) {
+                const int kz = ckz[c];
                 const double w = (kz == 0 || 2 * kz == K2) ? 1.0 : 2.0;
                 e += w * (double)g * ((double)v.x * v.x + (double)v.y * v.y);
             }
@@ -248,21 +268,22 @@ __global__ void __launch_bounds__(256) k_xconv(FftAxisDev Ax, const int* __restr
         }
     }
     __syncthreads();
-    fft_dif(D, SB_XCONV_T, 1, SB_XCONV_T, Ax, T.tw_a, true);
-    for (int t = threadIdx.x; t < K0 * SB_XCONV_T; t += blockDim.x) {
-        const int p = t / SB_XCONV_T, c = t - p * SB_XCONV_T;
-        if (c < nt) spec[(size_t)T.perm_a[p] * pstride + (size_t)y * H + kz0 + c] = D[t];
+    fft_dif<NL>(D, 1, NL, Ax, T.tw_a, true);
+    for (int t = threadIdx.x; t < K0 * NL; t += blockDim.x) {
+        const int p = t / NL, c = t - p * NL;
+        const int cb = cbase[c];
+        if (cb >= 0) spec[(size_t)T.perm_a[p] * pstride + cb] = D[t];
     }
     if (epart) {
         // deterministic block reduction (fixed tree)
-        __shared__ double red[256];
+        __shared__ double red[16 * NL];
         red[threadIdx.x] = e;
         __syncthreads();
         for (int o = blockDim.x / 2; o > 0; o >>= 1) {
             if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
             __syncthreads();
         }
-        if (threadIdx.x == 0) epart[blockIdx.y * gridDim.x + blockIdx.x] = 0.5 * red[0];
+        if (threadIdx.x == 0) epart[blockIdx.x] = 0.5 * red[0];
     }
 }
 
@@ -287,18 +308,21 @@ __global__ void __launch_bounds__(256) k_zfwd(FftAxisDev Az, const int* __restri
     const int r0 = blockIdx.x * SB_ZROWS;
     const int nr = min(SB_ZROWS, nrows - r0);
     long long* q = qfix + (size_t)r0 * K2;
-    for (int t = threadIdx.x; t < nr * K2; t += blockDim.x) {
+    for (int t = threadIdx.x; t < SB_ZROWS * K2; t += blockDim.x) {
         const int r = t / K2, col = t - r * K2;
-        const long long v = q[t];
-        if (v) q[t] = 0;
+        long long v = 0;
+        if (r < nr) {
+            v = q[t];
+            if (v) q[t] = 0;
+        }
         Df[2 * (r * H + T.perm_a[col >> 1]) + (col & 1)] = (float)v * SB_GRID_UNSCALE;
     }
     __syncthreads();
-    fft_dit(D, nr, H, 1, Az, T.tw_a, false);
+    fft_dit<SB_ZROWS>(D, H, 1, Az, T.tw_a, false);
     // X[k] = E[k] + W_K2^k O[k], k = 0..M, from Z = FFT_M(x_even + i x_odd)
     const int half = M / 2;
-    for (int t = threadIdx.x; t < nr * (half + 1); t += blockDim.x) {
-        const int k = t / nr, r = t - k * nr;
+    for (int t = threadIdx.x; t < SB_ZROWS * (half + 1); t += blockDim.x) {
+        const int k = t / SB_ZROWS, r = t - k * SB_ZROWS;
         float2* row = D + r * H;
         if (k == 0) {
             const float2 z0 = row[0];
@@ -337,12 +361,13 @@ __global__ void __launch_bounds__(256) k_zinv(FftAxisDev Az, const int* __restri
     const int r0 = blockIdx.x * SB_ZROWS;
     const int nr = min(SB_ZROWS, nrows - r0);
     const float2* in = spec + (size_t)r0 * H;
-    for (int t = threadIdx.x; t < nr * H; t += blockDim.x) D[t] = in[t];
+    for (int t = threadIdx.x; t < SB_ZROWS * H; t += blockDim.x)
+        D[t] = t < nr * H ? in[t] : make_float2(0.f, 0.f);
     __syncthreads();
     // Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_K2^{-k}, k = 0..M-1
     const int half = M / 2;
-    for (int t = threadIdx.x; t < nr * (half + 1); t += blockDim.x) {
-        const int k = t / nr, r = t - k * nr;
+    for (int t = threadIdx.x; t < SB_ZROWS * (half + 1); t += blockDim.x) {
+        const int k = t / SB_ZROWS, r = t - k * SB_ZROWS;
         float2* row = D + r * H;
         const int k2 = M - k;
         const float2 a = row[k], b = row[k2];
@@ -359,7 +384,7 @@ __global__ void __launch_bounds__(256) k_zinv(FftAxisDev Az, const int* __restri
         row[k] = Zk;
     }
     __syncthreads();
-    fft_dif(D, nr, H, 1, Az, T.tw_a, true);
+    fft_dif<SB_ZROWS>(D, H, 1, Az, T.tw_a, true);
     float* o = real + (size_t)r0 * K2;
     for (int t = threadIdx.x; t < nr * K2; t += blockDim.x) {
         const int r = t / K2, col = t - r * K2;
@@ -367,30 +392,36 @@ __global__ void __launch_bounds__(256) k_zinv(FftAxisDev Az, const int* __restri
     }
 }
 
-// y pass (forward or inverse) on a tile of SB_YT adjacent kz columns of one x-plane: DIT with a
-// digit-reversed load, natural-order store
-#define SB_YT 16
-__global__ void __launch_bounds__(256) k_ypass(FftAxisDev Ay, const int* __restrict__ py,
-                                               const float2* __restrict__ twy,
-                                               float2* __restrict__ spec, int K1, int H,
-                                               int inv) {
+// y pass (forward or inverse) on a tile of NL (x, kz) lines: DIT with a digit-reversed load,
+// natural-order store
+template <int NL>
+__global__ void __launch_bounds__(16 * NL) k_ypass(FftAxisDev Ay, const int* __restrict__ py,
+                                                   const float2* __restrict__ twy,
+                                                   float2* __restrict__ spec, int K0, int K1,
+                                                   int H, int inv) {
     extern __shared__ __align__(16) char sm[];
+    __shared__ long long cbase[NL];
     SmemTables T = carve(sm, K1, 0, 0);
+    const int nlines = K0 * H;
+    const int l0 = blockIdx.x * NL;
+    if (threadIdx.x < NL) {
+        const int l = l0 + threadIdx.x;
+        const int x = l / H, kz = l - x * H;
+        cbase[threadIdx.x] = l < nlines ? (long long)x * K1 * H + kz : -1;
+    }
     load_tables(T, py, py, twy, twy, twy, K1, 0, 0);
-    float2* D = T.data;  // [K1][SB_YT]
-    const int x = blockIdx.x;
-    const int kz0 = blockIdx.y * SB_YT;
-    const int nt = min(SB_YT, H - kz0);
-    float2* base = spec + (size_t)x * K1 * H + kz0;
-    for (int t = threadIdx.x; t < K1 * SB_YT; t += blockDim.x) {
-        const int p = t / SB_YT, c = t - p * SB_YT;
-        D[t] = c < nt ? base[(size_t)T.perm_a[p] * H + c] : make_float2(0.f, 0.f);
+    float2* D = T.data;  // [K1][NL]
+    for (int t = threadIdx.x; t < K1 * NL; t += blockDim.x) {
+        const int p = t / NL, c = t - p * NL;
+        const long long cb = cbase[c];
+        D[t] = cb >= 0 ? spec[cb + (size_t)T.perm_a[p] * H] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_dit(D, SB_YT, 1, SB_YT, Ay, T.tw_a, inv != 0);
-    for (int t = threadIdx.x; t < K1 * SB_YT; t += blockDim.x) {
-        const int p = t / SB_YT, c = t - p * SB_YT;
-        if (c < nt) base[(size_t)p * H + c] = D[t];
+    fft_dit<NL>(D, 1, NL, Ay, T.tw_a, inv != 0);
+    for (int t = threadIdx.x; t < K1 * NL; t += blockDim.x) {
+        const int p = t / NL, c = t - p * NL;
+        const long long cb = cbase[c];
+        if (cb >= 0) spec[cb + (size_t)p * H] = D[t];
     }
 }
 
@@ -452,7 +483,14 @@ static FftAxisDev axis_dev(const SbFftAxis& a) {
     FftAxisDev d;
     d.n = a.n;
     d.nrad = a.nrad;
-    for (int i = 0; i < SB_FFT_MAX_STAGES; i++) d.rad[i] = a.rad[i];
+    int m = 1;
+    for (int i = 0; i < SB_FFT_MAX_STAGES; i++) {
+        d.rad[i] = a.rad[i];
+        d.m[i] = m;
+        // ceil(2^32 / m); b / m == umulhi(b, rec) for b < 2^16 and m < 2^16
+        d.mrec[i] = m == 1 ? 0u : (unsigned)((0x100000000ull + (unsigned long long)m - 1) / m);
+        if (i < a.nrad) m *= a.rad[i];
+    }
     return d;
 }
 
@@ -493,10 +531,11 @@ int sb_fft_plan_create(SbFftPlan* p, const int K[3]) {
         cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)p->plane_smem);
     }
-    if (ys > 48 * 1024)
-        cudaFuncSetAttribute(k_ypass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
-    if (xs > 46 * 1024)
-        cudaFuncSetAttribute(k_xconv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xs);
+    if (ys > 46 * 1024)
+        cudaFuncSetAttribute(k_ypass<SB_YT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
+    if (xs > 40 * 1024)
+        cudaFuncSetAttribute(k_xconv<SB_XCONV_T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xs);
     return SB_OK;
 }
 
@@ -520,35 +559,36 @@ int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, 
         axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_qfix, d_spec, rows, p->K[2]);
     SB_CHECK_LAUNCH();
     const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * SB_YT;
-    dim3 grid(p->K[0], (p->H + SB_YT - 1) / SB_YT);
-    k_ypass<<<grid, 256, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec, p->K[1], p->H,
-                                  0);
+    const int yblocks = (p->K[0] * p->H + SB_YT - 1) / SB_YT;
+    k_ypass<SB_YT><<<yblocks, 16 * SB_YT, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec,
+                                                   p->K[0], p->K[1], p->H, 0);
     SB_CHECK_LAUNCH();
     return SB_OK;
 }
 
 int sb_fft_xconv_parts(const SbFftPlan* p) {
-    return p->K[1] * ((p->H + SB_XCONV_T - 1) / SB_XCONV_T);
+    return (p->K[1] * p->H + SB_XCONV_T - 1) / SB_XCONV_T;
 }
 
 int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
                       int want_energy, cudaStream_t s, int* nparts_out) {
-    dim3 grid(p->K[1], (p->H + SB_XCONV_T - 1) / SB_XCONV_T);
+    const int xblocks = sb_fft_xconv_parts(p);
     size_t xs = carve_bytes(p->K[0], 0, 0) + sizeof(float2) * (size_t)p->K[0] * SB_XCONV_T;
-    k_xconv<<<grid, 256, xs, s>>>(axis_dev(p->x), p->x.d_perm, p->x.d_tw, d_spec, d_bc,
-                                  want_energy ? d_epart : nullptr, p->K[0], p->K[1], p->H,
-                                  p->K[2]);
+    k_xconv<SB_XCONV_T><<<xblocks, 16 * SB_XCONV_T, xs, s>>>(
+        axis_dev(p->x), p->x.d_perm, p->x.d_tw, d_spec, d_bc, want_energy ? d_epart : nullptr,
+        p->K[0], p->K[1], p->H, p->K[2]);
     SB_CHECK_LAUNCH();
-    if (nparts_out) *nparts_out = grid.x * grid.y;
+    if (nparts_out) *nparts_out = xblocks;
     return SB_OK;
 }
 
 int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real,
                          cudaStream_t s) {
     const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * SB_YT;
-    dim3 grid(p->K[0], (p->H + SB_YT - 1) / SB_YT);
-    k_ypass<<<grid, 256, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw,
-                                  const_cast<float2*>(d_spec), p->K[1], p->H, 1);
+    const int yblocks = (p->K[0] * p->H + SB_YT - 1) / SB_YT;
+    k_ypass<SB_YT><<<yblocks, 16 * SB_YT, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw,
+                                                   const_cast<float2*>(d_spec), p->K[0], p->K[1],
+                                                   p->H, 1);
     SB_CHECK_LAUNCH();
     const int rows = p->K[0] * p->K[1];
     k_zinv<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
