@@ -5,8 +5,8 @@
 //   k_zfwd        32 rows per block: reads the int64 fixed-point charge grid (and clears it for
 //                 the next step), real-to-complex along z (length K2 via a K2/2 complex FFT,
 //                 decimation in time, digit-reversed load) -> half spectrum rows, kz <= K2/2
-//   k_ypass       16 (x, kz) lines per block: forward along y (DIT)
-//   k_xconv       16 (ky, kz) lines per block: forward along x (DIT), multiply by BC(kx,ky,kz)
+//   k_ypass       8 or 16 (x, kz) lines per block (timed at plan set-up): forward along y
+//   k_xconv       8 or 16 (ky, kz) lines per block: forward along x (DIT), multiply by BC(kx,ky,kz)
 //                 and accumulate the FP64 reciprocal energy, inverse along x (DIF)
 //   k_ypass       inverse along y
 //   k_zinv        complex-to-real along z -> real potential grid theta[x][y][z]
@@ -221,8 +221,6 @@ __device__ void load_tables(SmemTables& T, const int* pa, const int* pb, const f
 // Column passes (x and y) work on tiles of NL lines: a line is one (plane, kz) pair of the half
 // spectrum, tiles run across planes so that no block computes padding, and each line's base
 // address is computed once per block.
-#define SB_XCONV_T 16
-#define SB_YT 16
 
 template <int NL>
 __global__ void __launch_bounds__(16 * NL) k_xconv(FftAxisDev Ax, const int* __restrict__ px,
@@ -514,8 +512,8 @@ int sb_fft_plan_create(SbFftPlan* p, const int K[3]) {
     SB_CHECK_CUDA(cudaMemcpy(p->d_post, post.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
     // shared memory of the three tile shapes (z rows, y columns, x columns)
     p->plane_smem = carve_bytes(M, 0, M) + sizeof(float2) * (size_t)SB_ZROWS * p->H;
-    const size_t ys = carve_bytes(K[1], 0, 0) + sizeof(float2) * (size_t)K[1] * SB_YT;
-    const size_t xs = carve_bytes(K[0], 0, 0) + sizeof(float2) * (size_t)K[0] * SB_XCONV_T;
+    const size_t ys = carve_bytes(K[1], 0, 0) + sizeof(float2) * (size_t)K[1] * 16;
+    const size_t xs = carve_bytes(K[0], 0, 0) + sizeof(float2) * (size_t)K[0] * 16;
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -531,11 +529,14 @@ int sb_fft_plan_create(SbFftPlan* p, const int K[3]) {
         cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)p->plane_smem);
     }
-    if (ys > 46 * 1024)
-        cudaFuncSetAttribute(k_ypass<SB_YT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
-    if (xs > 40 * 1024)
-        cudaFuncSetAttribute(k_xconv<SB_XCONV_T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)xs);
+    if (ys > 46 * 1024) {
+        cudaFuncSetAttribute(k_ypass<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
+        cudaFuncSetAttribute(k_ypass<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
+    }
+    if (xs > 40 * 1024) {
+        cudaFuncSetAttribute(k_xconv<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xs);
+        cudaFuncSetAttribute(k_xconv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xs);
+    }
     return SB_OK;
 }
 
@@ -553,43 +554,92 @@ void sb_fft_plan_destroy(SbFftPlan* p) {
     p->d_post = nullptr;
 }
 
+static int launch_ypass(const SbFftPlan* p, float2* d_spec, int inv, int yt, cudaStream_t s) {
+    const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * yt;
+    const int blocks = (p->K[0] * p->H + yt - 1) / yt;
+    if (yt == 8)
+        k_ypass<8><<<blocks, 128, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec,
+                                           p->K[0], p->K[1], p->H, inv);
+    else
+        k_ypass<16><<<blocks, 256, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec,
+                                            p->K[0], p->K[1], p->H, inv);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+static int launch_xconv(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
+                        int xt, cudaStream_t s, int* nparts_out) {
+    const int blocks = (p->K[1] * p->H + xt - 1) / xt;
+    const size_t xs = carve_bytes(p->K[0], 0, 0) + sizeof(float2) * (size_t)p->K[0] * xt;
+    if (xt == 8)
+        k_xconv<8><<<blocks, 128, xs, s>>>(axis_dev(p->x), p->x.d_perm, p->x.d_tw, d_spec, d_bc,
+                                           d_epart, p->K[0], p->K[1], p->H, p->K[2]);
+    else
+        k_xconv<16><<<blocks, 256, xs, s>>>(axis_dev(p->x), p->x.d_perm, p->x.d_tw, d_spec,
+                                            d_bc, d_epart, p->K[0], p->K[1], p->H, p->K[2]);
+    SB_CHECK_LAUNCH();
+    if (nparts_out) *nparts_out = blocks;
+    return SB_OK;
+}
+
+int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream_t s) {
+    cudaEvent_t a, b;
+    SB_CHECK_CUDA(cudaEventCreate(&a));
+    SB_CHECK_CUDA(cudaEventCreate(&b));
+    float best_y = 1e30f, best_x = 1e30f;
+    const int cand[2] = {16, 8};
+    for (int c = 0; c < 2; c++) {
+        for (int pass = 0; pass < 2; pass++) {
+            SB_TRY(launch_ypass(p, d_spec, 0, cand[c], s));  // warm-up
+            SB_CHECK_CUDA(cudaEventRecord(a, s));
+            for (int r = 0; r < 3; r++) SB_TRY(launch_ypass(p, d_spec, 0, cand[c], s));
+            SB_CHECK_CUDA(cudaEventRecord(b, s));
+            SB_CHECK_CUDA(cudaEventSynchronize(b));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            if (pass == 1 && ms < best_y) {
+                best_y = ms;
+                p->yt = cand[c];
+            }
+            SB_TRY(launch_xconv(p, d_spec, d_bc, nullptr, cand[c], s, nullptr));
+            SB_CHECK_CUDA(cudaEventRecord(a, s));
+            for (int r = 0; r < 3; r++)
+                SB_TRY(launch_xconv(p, d_spec, d_bc, nullptr, cand[c], s, nullptr));
+            SB_CHECK_CUDA(cudaEventRecord(b, s));
+            SB_CHECK_CUDA(cudaEventSynchronize(b));
+            cudaEventElapsedTime(&ms, a, b);
+            if (pass == 1 && ms < best_x) {
+                best_x = ms;
+                p->xt = cand[c];
+            }
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return SB_OK;
+}
+
 int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, cudaStream_t s) {
     const int rows = p->K[0] * p->K[1];
     k_zfwd<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
         axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_qfix, d_spec, rows, p->K[2]);
     SB_CHECK_LAUNCH();
-    const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * SB_YT;
-    const int yblocks = (p->K[0] * p->H + SB_YT - 1) / SB_YT;
-    k_ypass<SB_YT><<<yblocks, 16 * SB_YT, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec,
-                                                   p->K[0], p->K[1], p->H, 0);
-    SB_CHECK_LAUNCH();
-    return SB_OK;
+    return launch_ypass(p, d_spec, 0, p->yt, s);
 }
 
 int sb_fft_xconv_parts(const SbFftPlan* p) {
-    return (p->K[1] * p->H + SB_XCONV_T - 1) / SB_XCONV_T;
+    // the most energy partials either tile size writes
+    return (p->K[1] * p->H + 7) / 8;
 }
 
 int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
                       int want_energy, cudaStream_t s, int* nparts_out) {
-    const int xblocks = sb_fft_xconv_parts(p);
-    size_t xs = carve_bytes(p->K[0], 0, 0) + sizeof(float2) * (size_t)p->K[0] * SB_XCONV_T;
-    k_xconv<SB_XCONV_T><<<xblocks, 16 * SB_XCONV_T, xs, s>>>(
-        axis_dev(p->x), p->x.d_perm, p->x.d_tw, d_spec, d_bc, want_energy ? d_epart : nullptr,
-        p->K[0], p->K[1], p->H, p->K[2]);
-    SB_CHECK_LAUNCH();
-    if (nparts_out) *nparts_out = xblocks;
-    return SB_OK;
+    return launch_xconv(p, d_spec, d_bc, want_energy ? d_epart : nullptr, p->xt, s, nparts_out);
 }
 
 int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real,
                          cudaStream_t s) {
-    const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * SB_YT;
-    const int yblocks = (p->K[0] * p->H + SB_YT - 1) / SB_YT;
-    k_ypass<SB_YT><<<yblocks, 16 * SB_YT, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw,
-                                                   const_cast<float2*>(d_spec), p->K[0], p->K[1],
-                                                   p->H, 1);
-    SB_CHECK_LAUNCH();
+    SB_TRY(launch_ypass(p, const_cast<float2*>(d_spec), 1, p->yt, s));
     const int rows = p->K[0] * p->K[1];
     k_zinv<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
         axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_spec, d_real, rows, p->K[2]);

@@ -91,7 +91,12 @@ struct SbFftPlan {
     SbFftAxis x;               // length K0
     float2* d_post = nullptr;  // e^{-2 pi i k / K2}, k < K2/2 (real-transform twiddles)
     size_t plane_smem = 0;     // bytes of the plane kernels' dynamic shared memory
+    int yt = 16;               // lines per block of the y pass (8 or 16, picked by timing)
+    int xt = 16;               // lines per block of the x pass
 };
+
+// times both line-tile sizes of the y and x passes on the plan's grid and keeps the faster
+int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream_t s);
 
 int sb_fft_plan_create(SbFftPlan* p, const int K[3]);
 void sb_fft_plan_destroy(SbFftPlan* p);

@@ -438,6 +438,11 @@ extern "C" int sb_pme_create(int atom_numbers, const float box_length[3], float 
     cudaMemset(p->d_correction_atom_energy, 0, sizeof(float) * atom_numbers);
     cudaMemset(p->d_ered, 0, sizeof(double) * 8);
     if ((st = build_bc(p))) return fail(st);
+    if (form == SB_FORM_FIXED) {
+        // line-tile sizes of the FFT column passes, picked by timing on this grid
+        if ((st = sb_fft_plan_tune(&p->plan, p->d_spec, p->d_bc, 0))) return fail(st);
+        cudaMemset(p->d_spec, 0, sizeof(float2) * p->Gh);
+    }
     *out = p;
     return SB_OK;
 }
@@ -761,11 +766,14 @@ __global__ void k_excluded_slot(int n, const uint32_t* __restrict__ uc, float sx
     if (ene) atomicAdd(&ene[i], e);
 }
 
-// charge spread from the packed slot data {ux, uy, uz, q}; 4 threads per slot (x offset)
+// charge spread from the packed slot data {ux, uy, uz, q}; 4 threads per slot, one per z offset,
+// so that the four lanes of a slot hit four adjacent grid words of one z row (one 32-byte
+// sector) at every (x, y) offset instead of four different x planes. The value added at each
+// point is the same product, in the same order, as the atom-order spread computes.
 __global__ void k_spread_slot(const int* __restrict__ meta, const uint4* __restrict__ xq, int K0,
                               int K1, int K2, long long* __restrict__ gfix) {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int sl = gt >> 2, kx = gt & 3;
+    const int sl = gt >> 2, kz = gt & 3;
     if (sl >= meta[3]) return;
     const uint4 v = xq[sl];
     const float q = __uint_as_float(v.w);
@@ -779,22 +787,22 @@ __global__ void k_spread_slot(const int* __restrict__ meta, const uint4* __restr
     bspline4(f0, wx);
     bspline4(f1, wy);
     bspline4(f2, wz);
-    const float qw = q * wx[kx];
-    int gx = b0 - kx;
-    if (gx < 0) gx += K0;
-    const size_t rowx = (size_t)gx * K1;
+    int gz = b2 - kz;
+    if (gz < 0) gz += K2;
+    const float wzk = kz == 0 ? wz[0] : kz == 1 ? wz[1] : kz == 2 ? wz[2] : wz[3];
 #pragma unroll
-    for (int ky = 0; ky < 4; ky++) {
-        int gy = b1 - ky;
-        if (gy < 0) gy += K1;
-        const size_t row = (rowx + gy) * K2;
-        const float qwy = qw * wy[ky];
+    for (int kx = 0; kx < 4; kx++) {
+        int gx = b0 - kx;
+        if (gx < 0) gx += K0;
+        const float qw = q * wx[kx];
 #pragma unroll
-        for (int kz = 0; kz < 4; kz++) {
-            int gz = b2 - kz;
-            if (gz < 0) gz += K2;
-            const long long f = __float2ll_rn(qwy * wz[kz] * SB_GRID_SCALE);
-            if (f) atomicAdd((unsigned long long*)&gfix[row + gz], (unsigned long long)f);
+        for (int ky = 0; ky < 4; ky++) {
+            int gy = b1 - ky;
+            if (gy < 0) gy += K1;
+            const long long f = __float2ll_rn(qw * wy[ky] * wzk * SB_GRID_SCALE);
+            if (f)
+                atomicAdd((unsigned long long*)&gfix[((size_t)gx * K1 + gy) * K2 + gz],
+                          (unsigned long long)f);
         }
     }
 }
