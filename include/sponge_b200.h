@@ -247,6 +247,16 @@ SB_API int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme*
                       int need_virial, float* d_atom_energy, float* d_atom_virial,
                       float* d_virial, float* d_potential, void* stream);
 
+/* The force part of sb_nonbonded_step with the list as it stands (no update): a fixed sequence
+ * of kernel launches with no host synchronisation, so a driver may capture it in a CUDA graph
+ * and replay it between list updates. */
+SB_API int sb_nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
+                       const uint32_t* d_uint_crd, const float* d_charge,
+                       const int* d_excluded_list_start, const int* d_excluded_list,
+                       const int* d_excluded_numbers, float* d_frc, int need_energy,
+                       int need_virial, float* d_atom_energy, float* d_atom_virial,
+                       float* d_virial, float* d_potential, void* stream);
+
 /* Crd_To_Uint_Crd (SPONGE/common.cu:264-287) with the quarter coefficient 0.25*2^32/L, as
  * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */
 SB_API int sb_crd_to_uint_crd(int atom_numbers, const float box_length[3], const float* d_crd,

@@ -71,6 +71,8 @@ _SIGS = {
     "sb_nonbonded_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp,
                           _vp, _vp, _vp],
     "sb_crd_to_uint_crd": [_i, _vp, _vp, _vp, _vp],
+    "sb_nonbonded_force": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp,
+                           _vp, _vp],
     "sb_lj_set_tables": [_vp, _vp, _vp],
     "sb_adjoint_create": [_vp, _vp, _vp, _vp],
     "sb_adjoint_destroy": [_vp],
@@ -402,6 +404,19 @@ def nonbonded_step(nl, lj, pme, crd, uint_crd, charge, excl, frc, need_energy=0,
                                    int(need_energy), int(need_virial), _ptr(atom_energy),
                                    _ptr(atom_virial), _ptr(d_virial), _ptr(d_potential),
                                    _stream(stream)))
+
+
+def nonbonded_force(nl, lj, pme, uint_crd, charge, excl, frc, need_energy=0, need_virial=0,
+                    atom_energy=None, atom_virial=None, d_virial=None, d_potential=None,
+                    stream=None):
+    """The force part of a step with the list as it stands (sb_nonbonded_force); capturable
+    in a CUDA graph."""
+    es, el, en = excl
+    _check(lib().sb_nonbonded_force(nl.handle, lj.handle, pme.handle, _ptr(uint_crd),
+                                    _ptr(charge), _ptr(es), _ptr(el), _ptr(en), _ptr(frc),
+                                    int(need_energy), int(need_virial), _ptr(atom_energy),
+                                    _ptr(atom_virial), _ptr(d_virial), _ptr(d_potential),
+                                    _stream(stream)))
 
 
 from .engine import NonbondedEngine  # noqa: E402,F401

@@ -57,19 +57,12 @@ int sb_reduce_sum_f32(const float* d_x, int n, double* d_out, cudaStream_t s) {
     return SB_OK;
 }
 
-extern "C" int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
-                                 float* d_crd, const uint32_t* d_uint_crd, const float* d_charge,
-                                 const int* es, const int* el, const int* en, float* d_frc,
-                                 int need_energy, int need_virial, float* d_atom_energy,
-                                 float* d_atom_virial, float* d_virial, float* d_potential,
-                                 void* stream) {
-    if (!nl || !lj || !pme || !d_crd || !d_uint_crd || !d_charge || !d_frc) {
-        sb_set_error("sb_nonbonded_step: null argument");
-        return SB_ERR_ARG;
-    }
-    // Main_Iteration's list update follows the previous step's integration; the list built
-    // here is used for this step's forces (the order a driver calling update then force sees)
-    SB_TRY(sb_nl_update(nl, d_crd, es, el, en, 0, 0, stream));
+// force part of one step (the list is used as it stands)
+static int nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
+                           const uint32_t* d_uint_crd, const float* d_charge, const int* es,
+                           const int* el, const int* en, float* d_frc, int need_energy,
+                           int need_virial, float* d_atom_energy, float* d_atom_virial,
+                           float* d_virial, float* d_potential, void* stream) {
     float* d_direct = nullptr;
     float* d_corr = nullptr;
     SB_TRY(sb_pme_atom_energy_arrays(pme, &d_direct, &d_corr));
@@ -103,4 +96,37 @@ extern "C" int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_
     SB_TRY(sb_pme_reciprocal_force(pme, d_uint_crd, d_charge, d_frc, need_virial, need_energy,
                                    d_virial, d_potential, stream));
     return SB_OK;
+}
+
+extern "C" int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
+                                 float* d_crd, const uint32_t* d_uint_crd, const float* d_charge,
+                                 const int* es, const int* el, const int* en, float* d_frc,
+                                 int need_energy, int need_virial, float* d_atom_energy,
+                                 float* d_atom_virial, float* d_virial, float* d_potential,
+                                 void* stream) {
+    if (!nl || !lj || !pme || !d_crd || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_nonbonded_step: null argument");
+        return SB_ERR_ARG;
+    }
+    // Main_Iteration's list update follows the previous step's integration; the list built
+    // here is used for this step's forces (the order a driver calling update then force sees)
+    SB_TRY(sb_nl_update(nl, d_crd, es, el, en, 0, 0, stream));
+    return nonbonded_force(nl, lj, pme, d_uint_crd, d_charge, es, el, en, d_frc, need_energy,
+                           need_virial, d_atom_energy, d_atom_virial, d_virial, d_potential,
+                           stream);
+}
+
+extern "C" int sb_nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
+                                  const uint32_t* d_uint_crd, const float* d_charge,
+                                  const int* es, const int* el, const int* en, float* d_frc,
+                                  int need_energy, int need_virial, float* d_atom_energy,
+                                  float* d_atom_virial, float* d_virial, float* d_potential,
+                                  void* stream) {
+    if (!nl || !lj || !pme || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_nonbonded_force: null argument");
+        return SB_ERR_ARG;
+    }
+    return nonbonded_force(nl, lj, pme, d_uint_crd, d_charge, es, el, en, d_frc, need_energy,
+                           need_virial, d_atom_energy, d_atom_virial, d_virial, d_potential,
+                           stream);
 }

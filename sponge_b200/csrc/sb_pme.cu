@@ -46,12 +46,14 @@ __device__ __forceinline__ void bspline4d(float f, float d[4]) {
 }
 
 // 4 threads per atom; thread t handles x-offset t and the 16 (y, z) points
+// 4 threads per atom, one per z offset: the four lanes of an atom update adjacent words of one
+// z row at each (x, y) offset
 template <bool FIXED>
 __global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __restrict__ q,
                          int K0, int K1, int K2, long long* __restrict__ gfix,
                          float* __restrict__ gf) {
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gt >> 2, kx = gt & 3;
+    const int i = gt >> 2, kz = gt & 3;
     if (i >= n) return;
     int b0, b1, b2;
     float f0, f1, f2;
@@ -62,26 +64,26 @@ __global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __
     bspline4(f0, wx);
     bspline4(f1, wy);
     bspline4(f2, wz);
-    const float qw = q[i] * wx[kx];
-    int gx = b0 - kx;
-    if (gx < 0) gx += K0;
-    const size_t rowx = (size_t)gx * K1;
+    const float qi = q[i];
+    int gz = b2 - kz;
+    if (gz < 0) gz += K2;
+    const float wzk = kz == 0 ? wz[0] : kz == 1 ? wz[1] : kz == 2 ? wz[2] : wz[3];
 #pragma unroll
-    for (int ky = 0; ky < 4; ky++) {
-        int gy = b1 - ky;
-        if (gy < 0) gy += K1;
-        const size_t row = (rowx + gy) * K2;
-        const float qwy = qw * wy[ky];
+    for (int kx = 0; kx < 4; kx++) {
+        int gx = b0 - kx;
+        if (gx < 0) gx += K0;
+        const float qw = qi * wx[kx];
 #pragma unroll
-        for (int kz = 0; kz < 4; kz++) {
-            int gz = b2 - kz;
-            if (gz < 0) gz += K2;
-            const float v = qwy * wz[kz];
+        for (int ky = 0; ky < 4; ky++) {
+            int gy = b1 - ky;
+            if (gy < 0) gy += K1;
+            const size_t at = ((size_t)gx * K1 + gy) * K2 + gz;
+            const float v = qw * wy[ky] * wzk;
             if (FIXED) {
                 const long long f = __float2ll_rn(v * SB_GRID_SCALE);
-                if (f) atomicAdd((unsigned long long*)&gfix[row + gz], (unsigned long long)f);
+                if (f) atomicAdd((unsigned long long*)&gfix[at], (unsigned long long)f);
             } else {
-                atomicAdd(&gf[row + gz], v);
+                atomicAdd(&gf[at], v);
             }
         }
     }

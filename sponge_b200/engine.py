@@ -10,7 +10,7 @@ neighbor list. The engine owns device copies of one system's arrays (from
 import numpy as np
 
 from . import (FORM_FIXED, LennardJones, NeighborList, ParticleMeshEwald, _require_cuda,
-               crd_to_uint_crd, nonbonded_step)
+               crd_to_uint_crd, nonbonded_force, nonbonded_step)
 
 
 def scaled_lj_tables(system):
@@ -94,6 +94,32 @@ class NonbondedEngine:
         nonbonded_step(self.nl, self.lj, self.pme, self.crd, self.uint_crd, self.charge,
                        self.excl, self.frc, need_energy, need_virial, self.atom_energy,
                        self.atom_virial, self.d_virial, self.d_potential, stream=stream)
+
+    def force(self, need_energy=0, need_virial=0, stream=None):
+        """Force part only, list as it stands (sb_nonbonded_force)."""
+        nonbonded_force(self.nl, self.lj, self.pme, self.uint_crd, self.charge, self.excl,
+                        self.frc, need_energy, need_virial, self.atom_energy, self.atom_virial,
+                        self.d_virial, self.d_potential, stream=stream)
+
+    def capture_force_graph(self):
+        """Capture (frc = 0; force part) once as a CUDA graph; ``step_graph`` replays it after
+        the list update by its policy. Call once eagerly first (lazy per-list buffers)."""
+        torch = self.torch
+        self.frc.zero_()
+        self.force()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream()
+        with torch.cuda.graph(g, stream=side):
+            self.frc.zero_()
+            self.force()
+        self._graph = g
+        return g
+
+    def step_graph(self):
+        """List update by its policy (eager), then the captured force graph."""
+        self.update_list()
+        self._graph.replay()
 
     def potential(self):
         """Total potential as MD_core sums it: sum(atom_energy) + d_potential (FP64 sum)."""

@@ -263,6 +263,31 @@ def test_fused_step_matches_module_sequence(name, torch_cuda, oracle_lib):
     assert rel_rms(eng.frc.cpu().numpy(), runs[0]) < 1e-6
 
 
+@pytest.mark.parametrize("form", ["fixed", "plain"])
+def test_force_graph_replay_matches_eager_step(form, torch_cuda):
+    """The force part captured once as a CUDA graph and replayed after each list update gives
+    the eager step's forces (bit-identical in the fixed form)."""
+    from sponge_b200 import FORM_FIXED, FORM_PLAIN, NonbondedEngine
+    s = systems.config0()
+    eng = NonbondedEngine(s, form=FORM_FIXED if form == "fixed" else FORM_PLAIN,
+                          refresh_interval=3)
+    eng.update_list(forced=1)
+    eng.to_uint()
+    eng.capture_force_graph()
+    for k in range(5):  # crosses a list rebuild (every 3rd update)
+        eng.crd[:30] += 0.05
+        eng.to_uint()
+        eng.step_graph()
+        g = eng.frc.cpu().numpy().copy()
+        eng.frc.zero_()
+        eng.force()
+        e = eng.frc.cpu().numpy()
+        if form == "fixed":
+            assert np.array_equal(g, e), k
+        else:
+            assert rel_rms(g, e) < 1e-6, k
+
+
 def test_refresh_policy(torch_cuda, oracle_lib):
     """refresh_interval > 0 rebuilds on calls 0, k, 2k ...; interval 0 rebuilds only when an
     atom moved more than skin/2 (neighbor_list.cu:618-664)."""
