@@ -392,11 +392,11 @@ __global__ void __launch_bounds__(256) k_zinv(FftAxisDev Az, const int* __restri
 
 // y pass (forward or inverse) on a tile of NL (x, kz) lines: DIT with a digit-reversed load,
 // natural-order store
-template <int NL>
+template <int NL, bool INV>
 __global__ void __launch_bounds__(16 * NL) k_ypass(FftAxisDev Ay, const int* __restrict__ py,
                                                    const float2* __restrict__ twy,
                                                    float2* __restrict__ spec, int K0, int K1,
-                                                   int H, int inv) {
+                                                   int H) {
     extern __shared__ __align__(16) char sm[];
     __shared__ long long cbase[NL];
     SmemTables T = carve(sm, K1, 0, 0);
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(16 * NL) k_ypass(FftAxisDev Ay, const int* __r
         D[t] = cb >= 0 ? spec[cb + (size_t)T.perm_a[p] * H] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_dit<NL>(D, 1, NL, Ay, T.tw_a, inv != 0);
+    fft_dit<NL>(D, 1, NL, Ay, T.tw_a, INV);
     for (int t = threadIdx.x; t < K1 * NL; t += blockDim.x) {
         const int p = t / NL, c = t - p * NL;
         const long long cb = cbase[c];
@@ -530,8 +530,14 @@ int sb_fft_plan_create(SbFftPlan* p, const int K[3]) {
                              (int)p->plane_smem);
     }
     if (ys > 46 * 1024) {
-        cudaFuncSetAttribute(k_ypass<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
-        cudaFuncSetAttribute(k_ypass<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ys);
+        cudaFuncSetAttribute(k_ypass<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ys);
+        cudaFuncSetAttribute(k_ypass<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ys);
+        cudaFuncSetAttribute(k_ypass<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ys);
+        cudaFuncSetAttribute(k_ypass<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ys);
     }
     if (xs > 40 * 1024) {
         cudaFuncSetAttribute(k_xconv<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xs);
@@ -557,12 +563,22 @@ void sb_fft_plan_destroy(SbFftPlan* p) {
 static int launch_ypass(const SbFftPlan* p, float2* d_spec, int inv, int yt, cudaStream_t s) {
     const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * yt;
     const int blocks = (p->K[0] * p->H + yt - 1) / yt;
-    if (yt == 8)
-        k_ypass<8><<<blocks, 128, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec,
-                                           p->K[0], p->K[1], p->H, inv);
-    else
-        k_ypass<16><<<blocks, 256, ys, s>>>(axis_dev(p->y), p->y.d_perm, p->y.d_tw, d_spec,
-                                            p->K[0], p->K[1], p->H, inv);
+    const FftAxisDev A = axis_dev(p->y);
+    if (yt == 8) {
+        if (inv)
+            k_ypass<8, true><<<blocks, 128, ys, s>>>(A, p->y.d_perm, p->y.d_tw, d_spec, p->K[0],
+                                                     p->K[1], p->H);
+        else
+            k_ypass<8, false><<<blocks, 128, ys, s>>>(A, p->y.d_perm, p->y.d_tw, d_spec, p->K[0],
+                                                      p->K[1], p->H);
+    } else {
+        if (inv)
+            k_ypass<16, true><<<blocks, 256, ys, s>>>(A, p->y.d_perm, p->y.d_tw, d_spec, p->K[0],
+                                                      p->K[1], p->H);
+        else
+            k_ypass<16, false><<<blocks, 256, ys, s>>>(A, p->y.d_perm, p->y.d_tw, d_spec,
+                                                       p->K[0], p->K[1], p->H);
+    }
     SB_CHECK_LAUNCH();
     return SB_OK;
 }
