@@ -187,6 +187,18 @@ SB_API int sb_pme_info(sb_pme* pme, float* h_beta, int* h_fft3);
 SB_API int sb_pme_atom_energy_arrays(sb_pme* pme, float** d_direct_atom_energy,
                               float** d_correction_atom_energy);
 
+/* FFT kernel family of the fixed-point form (no reference counterpart; a tuning knob):
+ * SB_FFT_AUTO times, per pass, the register line transforms (grid sizes N = N1 * N2 with small
+ * 2/3/5-smooth factors) against the generic mixed-radix stage kernels and keeps the fastest (the
+ * default, done once at sb_pme_create); SB_FFT_GENERIC uses only the stage kernels;
+ * SB_FFT_REGISTER uses the register transforms wherever the size has one. Re-times the passes,
+ * synchronises the device and clears the spectrum buffer; call it outside stream capture.
+ * Results agree to FP32 rounding whichever family runs. */
+#define SB_FFT_AUTO 0
+#define SB_FFT_GENERIC 1
+#define SB_FFT_REGISTER 2
+SB_API int sb_pme_set_fft_variant(sb_pme* pme, int variant);
+
 /* Particle_Mesh_Ewald::PME_Excluded_Force_With_Atom_Energy (PME_force.cu:697-708): Ewald
  * correction for every exclusion CSR entry, force added to d_frc, per-atom correction energy
  * written (reset then +=) to d_atom_energy (the reference passes d_correction_atom_energy). */

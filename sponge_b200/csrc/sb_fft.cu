@@ -15,6 +15,9 @@
 // Mixed radix 2/3/4/5/7. DIT with stage radices r1..rS applied to digit-reversed input and DIF
 // with the mirrored order both use one permutation table per axis, so no pass needs a second
 // buffer or an explicit transpose. All transforms are unnormalised, as cuFFT's are.
+// Each pass also has a register form (sb_fft4.cuh) for sizes N = N1 * N2 with small smooth
+// factors: two fully unrolled in-register DFT rounds around one shared-memory exchange, natural
+// order in and out. sb_fft_plan_tune times both forms per pass and keeps the faster.
 
 #include <stdio.h>
 
@@ -22,6 +25,7 @@
 #include <vector>
 
 #include "sb_internal.cuh"
+#include "sb_fft4.cuh"
 
 struct FftAxisDev {
     int n;
@@ -508,6 +512,14 @@ int sb_fft_plan_create(SbFftPlan* p, const int K[3]) {
         double ang = -2.0 * M_PI * (double)k / K[2];
         post[k] = make_float2((float)cos(ang), (float)sin(ang));
     }
+    // e^{-2 pi i k / n} for the register transforms' small DFTs (FP64-computed)
+    std::vector<float2> small(SB_SMALL_TW);
+    for (int n = 2; n <= SB_SMALL_N; n++)
+        for (int k = 0; k < n; k++) {
+            const double ang = -2.0 * M_PI * (double)k / n;
+            small[n * (n - 1) / 2 - 1 + k] = make_float2((float)cos(ang), (float)sin(ang));
+        }
+    SB_CHECK_CUDA(cudaMemcpyToSymbol(c_small_tw, small.data(), sizeof(float2) * SB_SMALL_TW));
     SB_TRY(sb_malloc((void**)&p->d_post, sizeof(float2) * M, "fft post twiddles"));
     SB_CHECK_CUDA(cudaMemcpy(p->d_post, post.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
     // shared memory of the three tile shapes (z rows, y columns, x columns)
@@ -560,7 +572,116 @@ void sb_fft_plan_destroy(SbFftPlan* p) {
     p->d_post = nullptr;
 }
 
+// ---------------------------------------------------------------------------------------------
+// host: register line transforms (one kernel instantiation per supported size)
+// ---------------------------------------------------------------------------------------------
+#define SB_F4_HAS(N_, A_, B_) \
+    case N_:                  \
+        return true;
+static bool f4_has(int n) {
+    switch (n) {
+        SB_FFT4_SIZES(SB_F4_HAS)
+        default: return false;
+    }
+}
+static bool f4_has_z(int m) {
+    switch (m) {
+        SB_FFT4_ZSIZES(SB_F4_HAS)
+        default: return false;
+    }
+}
+#undef SB_F4_HAS
+
+template <bool INV>
+static void ypass4(int n, int blocks, const float2* tw, float2* spec, int K0, int H,
+                   cudaStream_t s) {
+#define SB_F4_Y(N_, A_, B_)                                                                  \
+    case N_:                                                                                 \
+        k_ypass4<A_, B_, INV><<<blocks, SB_F4_NL * F4<A_, B_>::T, 0, s>>>(tw, spec, K0, H); \
+        break;
+    switch (n) {
+        SB_FFT4_SIZES(SB_F4_Y)
+        default: break;
+    }
+#undef SB_F4_Y
+}
+
+static void xconv4(int n, int blocks, const float2* tw, float2* spec, const float* bc,
+                   double* epart, int K1, int H, int K2, cudaStream_t s) {
+#define SB_F4_X(N_, A_, B_)                                                               \
+    case N_:                                                                              \
+        k_xconv4<A_, B_><<<blocks, SB_F4_NL * F4<A_, B_>::T, 0, s>>>(tw, spec, bc, epart, \
+                                                                      K1, H, K2);         \
+        break;
+    switch (n) {
+        SB_FFT4_SIZES(SB_F4_X)
+        default: break;
+    }
+#undef SB_F4_X
+}
+
+static void zfwd4(int m, int blocks, const float2* tw, const float2* post, long long* qfix,
+                  float2* spec, int rows, cudaStream_t s) {
+#define SB_F4_ZF(N_, A_, B_)                                                                 \
+    case N_:                                                                                 \
+        k_zfwd4<A_, B_><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, qfix, spec, rows); \
+        break;
+    switch (m) {
+        SB_FFT4_ZSIZES(SB_F4_ZF)
+        default: break;
+    }
+#undef SB_F4_ZF
+}
+
+static void zinv4(int m, int blocks, const float2* tw, const float2* post, const float2* spec,
+                  float* real, int rows, cudaStream_t s) {
+#define SB_F4_ZI(N_, A_, B_)                                                                 \
+    case N_:                                                                                 \
+        k_zinv4<A_, B_><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, spec, real, rows); \
+        break;
+    switch (m) {
+        SB_FFT4_ZSIZES(SB_F4_ZI)
+        default: break;
+    }
+#undef SB_F4_ZI
+}
+
+static int launch_zfwd(const SbFftPlan* p, long long* d_qfix, float2* d_spec, int zt,
+                       cudaStream_t s) {
+    const int rows = p->K[0] * p->K[1];
+    if (zt == 0)
+        zfwd4(p->K[2] / 2, (rows + SB_F4_ZR - 1) / SB_F4_ZR, p->z.d_tw, p->d_post, d_qfix,
+              d_spec, rows, s);
+    else
+        k_zfwd<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
+            axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_qfix, d_spec, rows, p->K[2]);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+static int launch_zinv(const SbFftPlan* p, const float2* d_spec, float* d_real, int zt,
+                       cudaStream_t s) {
+    const int rows = p->K[0] * p->K[1];
+    if (zt == 0)
+        zinv4(p->K[2] / 2, (rows + SB_F4_ZR - 1) / SB_F4_ZR, p->z.d_tw, p->d_post, d_spec,
+              d_real, rows, s);
+    else
+        k_zinv<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
+            axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_spec, d_real, rows, p->K[2]);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
 static int launch_ypass(const SbFftPlan* p, float2* d_spec, int inv, int yt, cudaStream_t s) {
+    if (yt == 0) {
+        const int blocks = (p->K[0] * p->H + SB_F4_NL - 1) / SB_F4_NL;
+        if (inv)
+            ypass4<true>(p->K[1], blocks, p->y.d_tw, d_spec, p->K[0], p->H, s);
+        else
+            ypass4<false>(p->K[1], blocks, p->y.d_tw, d_spec, p->K[0], p->H, s);
+        SB_CHECK_LAUNCH();
+        return SB_OK;
+    }
     const size_t ys = carve_bytes(p->K[1], 0, 0) + sizeof(float2) * (size_t)p->K[1] * yt;
     const int blocks = (p->K[0] * p->H + yt - 1) / yt;
     const FftAxisDev A = axis_dev(p->y);
@@ -585,6 +706,13 @@ static int launch_ypass(const SbFftPlan* p, float2* d_spec, int inv, int yt, cud
 
 static int launch_xconv(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
                         int xt, cudaStream_t s, int* nparts_out) {
+    if (xt == 0) {
+        const int blocks = (p->K[1] * p->H + SB_F4_NL - 1) / SB_F4_NL;
+        xconv4(p->K[0], blocks, p->x.d_tw, d_spec, d_bc, d_epart, p->K[1], p->H, p->K[2], s);
+        SB_CHECK_LAUNCH();
+        if (nparts_out) *nparts_out = blocks;
+        return SB_OK;
+    }
     const int blocks = (p->K[1] * p->H + xt - 1) / xt;
     const size_t xs = carve_bytes(p->K[0], 0, 0) + sizeof(float2) * (size_t)p->K[0] * xt;
     if (xt == 8)
@@ -598,53 +726,75 @@ static int launch_xconv(const SbFftPlan* p, float2* d_spec, const float* d_bc, d
     return SB_OK;
 }
 
-int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream_t s) {
+// mean duration of `reps` launches after one warm-up launch
+template <class F>
+static int time_launches(F launch, cudaEvent_t a, cudaEvent_t b, cudaStream_t s, float* ms) {
+    SB_TRY(launch());
+    SB_CHECK_CUDA(cudaEventRecord(a, s));
+    for (int r = 0; r < 3; r++) SB_TRY(launch());
+    SB_CHECK_CUDA(cudaEventRecord(b, s));
+    SB_CHECK_CUDA(cudaEventSynchronize(b));
+    SB_CHECK_CUDA(cudaEventElapsedTime(ms, a, b));
+    return SB_OK;
+}
+
+int sb_fft_plan_tune(SbFftPlan* p, long long* d_qfix, float2* d_spec, const float* d_bc,
+                     float* d_real, cudaStream_t s) {
+    const bool gen = p->variant != SB_FFT_REGISTER, reg = p->variant != SB_FFT_GENERIC;
+    const bool ry = reg && f4_has(p->K[1]), rx = reg && f4_has(p->K[0]),
+               rz = reg && f4_has_z(p->K[2] / 2);
+    // shapes to try: the register kernel (0) where allowed, the generic tiles where allowed or
+    // where no register kernel exists
+    int cy[3], cx[3], cz[2], ny = 0, nx = 0, nz = 0;
+    if (ry) cy[ny++] = 0;
+    if (rx) cx[nx++] = 0;
+    if (rz) cz[nz++] = 0;
+    if (gen || !ry) cy[ny++] = 16, cy[ny++] = 8;
+    if (gen || !rx) cx[nx++] = 16, cx[nx++] = 8;
+    if (gen || !rz) cz[nz++] = 32;
     cudaEvent_t a, b;
     SB_CHECK_CUDA(cudaEventCreate(&a));
     SB_CHECK_CUDA(cudaEventCreate(&b));
-    float best_y = 1e30f, best_x = 1e30f;
-    const int cand[2] = {16, 8};
-    for (int c = 0; c < 2; c++) {
-        for (int pass = 0; pass < 2; pass++) {
-            SB_TRY(launch_ypass(p, d_spec, 0, cand[c], s));  // warm-up
-            SB_CHECK_CUDA(cudaEventRecord(a, s));
-            for (int r = 0; r < 3; r++) SB_TRY(launch_ypass(p, d_spec, 0, cand[c], s));
-            SB_CHECK_CUDA(cudaEventRecord(b, s));
-            SB_CHECK_CUDA(cudaEventSynchronize(b));
-            float ms = 0;
-            cudaEventElapsedTime(&ms, a, b);
-            if (pass == 1 && ms < best_y) {
-                best_y = ms;
-                p->yt = cand[c];
-            }
-            SB_TRY(launch_xconv(p, d_spec, d_bc, nullptr, cand[c], s, nullptr));
-            SB_CHECK_CUDA(cudaEventRecord(a, s));
-            for (int r = 0; r < 3; r++)
-                SB_TRY(launch_xconv(p, d_spec, d_bc, nullptr, cand[c], s, nullptr));
-            SB_CHECK_CUDA(cudaEventRecord(b, s));
-            SB_CHECK_CUDA(cudaEventSynchronize(b));
-            cudaEventElapsedTime(&ms, a, b);
-            if (pass == 1 && ms < best_x) {
-                best_x = ms;
-                p->xt = cand[c];
-            }
+    int st = SB_OK;
+    float best = 1e30f, ms = 0.f;
+    // every shape is timed twice; the second round decides (the first pays for module loading)
+    for (int round = 0; round < 2 && !st; round++) {
+        best = 1e30f;
+        for (int c = 0; c < ny && !st; c++) {
+            st = time_launches([&] { return launch_ypass(p, d_spec, 0, cy[c], s); }, a, b, s, &ms);
+            if (!st && ms < best) best = ms, p->yt = cy[c];
+        }
+        best = 1e30f;
+        for (int c = 0; c < nx && !st; c++) {
+            st = time_launches(
+                [&] { return launch_xconv(p, d_spec, d_bc, nullptr, cx[c], s, nullptr); }, a, b,
+                s, &ms);
+            if (!st && ms < best) best = ms, p->xt = cx[c];
+        }
+        best = 1e30f;
+        for (int c = 0; c < nz && !st; c++) {
+            // forward then inverse: d_qfix stays zero (the forward pass clears what it reads)
+            st = time_launches(
+                [&] {
+                    SB_TRY(launch_zfwd(p, d_qfix, d_spec, cz[c], s));
+                    return launch_zinv(p, d_spec, d_real, cz[c], s);
+                },
+                a, b, s, &ms);
+            if (!st && ms < best) best = ms, p->zt = cz[c];
         }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    return SB_OK;
+    return st;
 }
 
 int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, cudaStream_t s) {
-    const int rows = p->K[0] * p->K[1];
-    k_zfwd<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
-        axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_qfix, d_spec, rows, p->K[2]);
-    SB_CHECK_LAUNCH();
+    SB_TRY(launch_zfwd(p, d_qfix, d_spec, p->zt, s));
     return launch_ypass(p, d_spec, 0, p->yt, s);
 }
 
 int sb_fft_xconv_parts(const SbFftPlan* p) {
-    // the most energy partials either tile size writes
+    // the most energy partials any x-pass shape writes (8-line tiles)
     return (p->K[1] * p->H + 7) / 8;
 }
 
@@ -656,9 +806,5 @@ int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, dou
 int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real,
                          cudaStream_t s) {
     SB_TRY(launch_ypass(p, const_cast<float2*>(d_spec), 1, p->yt, s));
-    const int rows = p->K[0] * p->K[1];
-    k_zinv<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
-        axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_spec, d_real, rows, p->K[2]);
-    SB_CHECK_LAUNCH();
-    return SB_OK;
+    return launch_zinv(p, d_spec, d_real, p->zt, s);
 }

@@ -91,12 +91,19 @@ struct SbFftPlan {
     SbFftAxis x;               // length K0
     float2* d_post = nullptr;  // e^{-2 pi i k / K2}, k < K2/2 (real-transform twiddles)
     size_t plane_smem = 0;     // bytes of the plane kernels' dynamic shared memory
-    int yt = 16;               // lines per block of the y pass (8 or 16, picked by timing)
-    int xt = 16;               // lines per block of the x pass
+    // kernel shape of each pass, picked by timing: 0 = register line transform (sizes that have
+    // one), 8 or 16 = generic stage kernels with that many lines per block (z: 32 rows)
+    int yt = 16;
+    int xt = 16;
+    int zt = 32;
+    int variant = 0;           // SB_FFT_AUTO / SB_FFT_GENERIC / SB_FFT_REGISTER
 };
 
-// times both line-tile sizes of the y and x passes on the plan's grid and keeps the faster
-int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream_t s);
+// times the kernel shapes the plan's variant allows for every pass and keeps the fastest;
+// d_qfix must hold zeros (the forward z pass reads and clears it), d_spec and d_real are
+// overwritten
+int sb_fft_plan_tune(SbFftPlan* p, long long* d_qfix, float2* d_spec, const float* d_bc,
+                     float* d_real, cudaStream_t s);
 
 int sb_fft_plan_create(SbFftPlan* p, const int K[3]);
 void sb_fft_plan_destroy(SbFftPlan* p);

@@ -441,11 +441,31 @@ extern "C" int sb_pme_create(int atom_numbers, const float box_length[3], float 
     cudaMemset(p->d_ered, 0, sizeof(double) * 8);
     if ((st = build_bc(p))) return fail(st);
     if (form == SB_FORM_FIXED) {
-        // line-tile sizes of the FFT column passes, picked by timing on this grid
-        if ((st = sb_fft_plan_tune(&p->plan, p->d_spec, p->d_bc, 0))) return fail(st);
+        // kernel shapes of the FFT passes, picked by timing on this grid
+        if ((st = sb_fft_plan_tune(&p->plan, p->d_qfix, p->d_spec, p->d_bc, p->d_theta, 0)))
+            return fail(st);
         cudaMemset(p->d_spec, 0, sizeof(float2) * p->Gh);
     }
     *out = p;
+    return SB_OK;
+}
+
+extern "C" int sb_pme_set_fft_variant(sb_pme* p, int variant) {
+    if (!p) {
+        sb_set_error("sb_pme_set_fft_variant: null handle");
+        return SB_ERR_ARG;
+    }
+    if (variant < SB_FFT_AUTO || variant > SB_FFT_REGISTER) {
+        sb_set_error("sb_pme_set_fft_variant: variant %d is not AUTO, GENERIC or REGISTER",
+                     variant);
+        return SB_ERR_ARG;
+    }
+    if (p->form != SB_FORM_FIXED) return SB_OK;  // the plain form runs the library FFT
+    SB_CHECK_CUDA(cudaDeviceSynchronize());
+    p->plan.variant = variant;
+    SB_TRY(sb_fft_plan_tune(&p->plan, p->d_qfix, p->d_spec, p->d_bc, p->d_theta, 0));
+    SB_CHECK_CUDA(cudaMemset(p->d_spec, 0, sizeof(float2) * p->Gh));
+    SB_CHECK_CUDA(cudaDeviceSynchronize());
     return SB_OK;
 }
 

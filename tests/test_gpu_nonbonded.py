@@ -121,8 +121,19 @@ def test_excluded_force(case):
 
 def test_reciprocal_force(case):
     name, s, eng, ref = case
-    f = _forces(eng, ("reciprocal",))
-    assert rel_rms(f, ref["f_rec"]) < FORCE_TOL
+    import sponge_b200
+    out = {}
+    # both FFT kernel families (register line transforms exist for every grid here), then the
+    # timed choice, which stays in place for the other tests
+    for v in (sponge_b200.FFT_GENERIC, sponge_b200.FFT_REGISTER, sponge_b200.FFT_AUTO):
+        eng.pme.set_fft_variant(v)
+        out[v] = _forces(eng, ("reciprocal",))
+        assert rel_rms(out[v], ref["f_rec"]) < FORCE_TOL
+        assert np.array_equal(_forces(eng, ("reciprocal",)), out[v])  # bit-identical repeat
+        e, parts = eng.pme.Get_Energy(eng.uint_crd, eng.charge, eng.nl, eng.scaler, *eng.excl,
+                                      which_part=sponge_b200.PME_TOTAL, parts=True)
+        assert parts["reciprocal"] == pytest.approx(ref["e_rec"], rel=1e-5)
+    assert rel_rms(out[sponge_b200.FFT_REGISTER], out[sponge_b200.FFT_GENERIC]) < 1e-6
 
 
 def test_total_force(case):
