@@ -160,7 +160,9 @@ SB_API int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[3]);
 SB_API int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane);
 
 /* Autotuner: times each pair-kernel shape on the current list and keeps the fastest; writes the
- * choice to *h_chosen. Synchronises the stream; leaves d_frc untouched. */
+ * choice to *h_chosen. Synchronises the stream; leaves d_frc untouched. The shapes sum in
+ * different orders, so a process that needs the same bits as another sets the shape explicitly
+ * (sb_lj_set_kernel_variant) rather than tuning (the default shape is 8). */
 SB_API int sb_lj_tune(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
                       const float* d_charge, float pme_beta, int* h_chosen, void* stream);
 
@@ -188,15 +190,13 @@ SB_API int sb_pme_atom_energy_arrays(sb_pme* pme, float** d_direct_atom_energy,
                               float** d_correction_atom_energy);
 
 /* FFT kernel family of the fixed-point form (no reference counterpart; a tuning knob):
- * SB_FFT_AUTO times, per pass, the register line transforms (grid sizes N = N1 * N2 with small
- * 2/3/5-smooth factors) against the generic mixed-radix stage kernels and keeps the fastest (the
- * default, done once at sb_pme_create); SB_FFT_GENERIC uses only the stage kernels;
- * SB_FFT_REGISTER uses the register transforms wherever the size has one. Re-times the passes,
- * synchronises the device and clears the spectrum buffer; call it outside stream capture.
- * Results agree to FP32 rounding whichever family runs. */
+ * SB_FFT_AUTO (the default) runs the register line transforms on every axis whose size has one
+ * (N = N1 * N2 with small 2/3/5-smooth factors) and the generic mixed-radix stage kernels on the
+ * others; SB_FFT_GENERIC runs only the stage kernels. The choice is a fixed rule, not a timing,
+ * so the same grid gives the same bits in every process. Synchronises the device and clears the
+ * spectrum buffer; call it outside stream capture. The two families agree to FP32 rounding. */
 #define SB_FFT_AUTO 0
 #define SB_FFT_GENERIC 1
-#define SB_FFT_REGISTER 2
 SB_API int sb_pme_set_fft_variant(sb_pme* pme, int variant);
 
 /* Particle_Mesh_Ewald::PME_Excluded_Force_With_Atom_Energy (PME_force.cu:697-708): Ewald
@@ -268,6 +268,13 @@ SB_API int sb_nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme
                        const int* d_excluded_numbers, float* d_frc, int need_energy,
                        int need_virial, float* d_atom_energy, float* d_atom_virial,
                        float* d_virial, float* d_potential, void* stream);
+
+/* Overlap switch of the fixed-form force part (no reference counterpart; a scheduling knob, on
+ * by default): the exclusion correction and the reciprocal grid chain (spread, FFT, convolution,
+ * inverse FFT) run on a high-priority stream owned by the PME module, forked from and joined back
+ * to the caller's stream, concurrently with the pair kernel. Forces are bit-identical either way
+ * (integer accumulation); a graph captured from the caller's stream holds both branches. */
+SB_API int sb_nonbonded_set_overlap(sb_pme* pme, int on);
 
 /* Crd_To_Uint_Crd (SPONGE/common.cu:264-287) with the quarter coefficient 0.25*2^32/L, as
  * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */

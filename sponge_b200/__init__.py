@@ -29,7 +29,7 @@ FORM_PLAIN = 1
 
 PME_TOTAL, PME_DIRECT, PME_RECIPROCAL, PME_CORRECTION, PME_SELF = range(5)
 
-FFT_AUTO, FFT_GENERIC, FFT_REGISTER = range(3)
+FFT_AUTO, FFT_GENERIC = range(2)
 
 STATUS_LIST_OVERFLOW = 1
 STATUS_COLUMN_OVERFLOW = 2
@@ -65,6 +65,7 @@ _SIGS = {
     "sb_pme_destroy": [_vp],
     "sb_pme_info": [_vp, _vp, _vp],
     "sb_pme_set_fft_variant": [_vp, _i],
+    "sb_nonbonded_set_overlap": [_vp, _i],
     "sb_pme_atom_energy_arrays": [_vp, _vp, _vp],
     "sb_pme_excluded_force": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "sb_pme_reciprocal_force": [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp],
@@ -351,10 +352,15 @@ class ParticleMeshEwald:
         return (np.float32(1.0) / np.float32(4294967296.0)) * self.box_length
 
     def set_fft_variant(self, variant):
-        """FFT kernel family of the fixed-point form: FFT_AUTO (timed per pass, the default),
-        FFT_GENERIC (stage kernels) or FFT_REGISTER (register line transforms where the size
-        has one); a tuning knob with the same results to FP32 rounding. Synchronises."""
+        """FFT kernel family of the fixed-point form: FFT_AUTO (register line transforms where
+        the axis size has one, the default) or FFT_GENERIC (stage kernels only); a fixed rule,
+        same results to FP32 rounding. Synchronises."""
         _check(lib().sb_pme_set_fft_variant(self.handle, int(variant)))
+
+    def set_overlap(self, on):
+        """Fixed-form fused force: run the exclusion correction and the reciprocal grid chain on
+        a side stream concurrently with the pair kernel (default on; same forces either way)."""
+        _check(lib().sb_nonbonded_set_overlap(self.handle, int(bool(on))))
 
     def PME_Excluded_Force_With_Atom_Energy(self, uint_crd, scaler, charge, excluded_list_start,
                                             excluded_list, excluded_numbers, frc, atom_energy,

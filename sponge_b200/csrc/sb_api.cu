@@ -73,15 +73,34 @@ static int nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* p
         SB_TRY(sb_nl_ensure_built(nl));
         cudaStream_t s = sb_stream(stream);
         const int ev = need_energy > 0 || need_virial > 0;
-        SB_TRY(sb_lj_fused_direct(lj, nl, d_uint_crd, d_charge, pme->beta, need_energy,
-                                  d_atom_energy, need_virial, d_atom_virial, d_direct, s));
-        SB_TRY(sb_lj_long_range_correction(lj, need_virial, d_virial, need_energy, d_potential,
-                                           stream));
+        SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
+        // the exclusion correction and the reciprocal grid chain depend only on the packed
+        // slots; with overlap on they run on the module's side stream while the pair kernel
+        // runs here (the force buffer takes integer adds, so the order cannot change a bit)
+        const bool fork = pme->overlap && pme->side;
+        cudaStream_t g = fork ? pme->side : s;
+        if (fork) {
+            SB_CHECK_CUDA(cudaEventRecord(pme->ev_fork, s));
+            SB_CHECK_CUDA(cudaStreamWaitEvent(g, pme->ev_fork, 0));
+        }
         // the per-atom correction energy is only read on energy/virial steps
-        SB_TRY(sb_pme_fused_excluded(pme, nl, d_uint_crd, d_charge, es, el, en,
-                                     ev ? d_corr : nullptr, s));
-        return sb_pme_fused_reciprocal(pme, nl, d_frc, d_charge, need_virial, need_energy,
-                                       d_virial, d_potential, s);
+        int st = sb_pme_fused_excluded(pme, nl, d_uint_crd, d_charge, es, el, en,
+                                       ev ? d_corr : nullptr, g);
+        if (!st) st = sb_pme_fused_grid(pme, nl, ev, g);
+        if (fork) {
+            // join even after a failed launch so that a capture in progress stays well formed
+            SB_CHECK_CUDA(cudaEventRecord(pme->ev_join, g));
+        }
+        int st2 = sb_lj_fused_pair(lj, nl, pme->beta, need_energy, d_atom_energy, need_virial,
+                                   d_atom_virial, d_direct, s);
+        if (!st2)
+            st2 = sb_lj_long_range_correction(lj, need_virial, d_virial, need_energy,
+                                              d_potential, stream);
+        if (fork) SB_CHECK_CUDA(cudaStreamWaitEvent(s, pme->ev_join, 0));
+        if (st) return st;
+        if (st2) return st2;
+        return sb_pme_fused_finish(pme, nl, d_frc, d_charge, need_virial, need_energy, d_virial,
+                                   d_potential, s);
     }
     SB_TRY(sb_lj_pme_direct_force(lj, nl, lj->n, d_uint_crd, d_charge, d_frc, pme->beta,
                                   need_energy, d_atom_energy, need_virial, d_atom_virial,
@@ -114,6 +133,15 @@ extern "C" int sb_nonbonded_step(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_
     return nonbonded_force(nl, lj, pme, d_uint_crd, d_charge, es, el, en, d_frc, need_energy,
                            need_virial, d_atom_energy, d_atom_virial, d_virial, d_potential,
                            stream);
+}
+
+extern "C" int sb_nonbonded_set_overlap(sb_pme* pme, int on) {
+    if (!pme) {
+        sb_set_error("sb_nonbonded_set_overlap: null handle");
+        return SB_ERR_ARG;
+    }
+    pme->overlap = on ? 1 : 0;
+    return SB_OK;
 }
 
 extern "C" int sb_nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,

@@ -1,6 +1,20 @@
 // Ewald real-space helpers shared by the pair and exclusion kernels.
 #pragma once
 
+// Approximate reciprocal square root and quotient of the special-function unit, flushing
+// subnormal inputs to zero (the pair kernels only see normal operands: r^2 >= ~1e-2 for pairs
+// that count, a denominator >= 1), which spares the subnormal rescaling of the non-flushing forms.
+__device__ __forceinline__ float sb_rsqrt(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sb_fdiv(float a, float b) {
+    float y;
+    asm("div.approx.ftz.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+    return y;
+}
+
 // G(z) = [erf(x) - 2x e^{-x^2}/sqrt(pi)] / x^3 with x = sqrt(z) = beta*r.
 // Coulomb part of the pair force scalar:   qq * (1/r^3 - beta^3 G(beta^2 r^2))
 // exclusion-correction force scalar:       qq * beta^3 G(beta^2 r^2)
@@ -50,7 +64,7 @@ __device__ __forceinline__ float sb_ewald_G_rational(float z, const float* gp) {
     q = fmaf(q, z, 1.454184461e-01f);
     q = fmaf(q, z, 5.616555609e-01f);
     q = fmaf(q, z, 1.0f);
-    return __fdividef(p, q);
+    return sb_fdiv(p, q);
 }
 
 // beta^3 G(z) with the numerator coefficients pre-multiplied by beta^3 (gp[0] = beta^3 P5 ...

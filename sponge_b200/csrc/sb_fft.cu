@@ -17,7 +17,7 @@
 // buffer or an explicit transpose. All transforms are unnormalised, as cuFFT's are.
 // Each pass also has a register form (sb_fft4.cuh) for sizes N = N1 * N2 with small smooth
 // factors: two fully unrolled in-register DFT rounds around one shared-memory exchange, natural
-// order in and out. sb_fft_plan_tune times both forms per pass and keeps the faster.
+// order in and out. Plans use the register form wherever the size has one.
 
 #include <stdio.h>
 
@@ -738,49 +738,36 @@ static int time_launches(F launch, cudaEvent_t a, cudaEvent_t b, cudaStream_t s,
     return SB_OK;
 }
 
-int sb_fft_plan_tune(SbFftPlan* p, long long* d_qfix, float2* d_spec, const float* d_bc,
-                     float* d_real, cudaStream_t s) {
-    const bool gen = p->variant != SB_FFT_REGISTER, reg = p->variant != SB_FFT_GENERIC;
-    const bool ry = reg && f4_has(p->K[1]), rx = reg && f4_has(p->K[0]),
-               rz = reg && f4_has_z(p->K[2] / 2);
-    // shapes to try: the register kernel (0) where allowed, the generic tiles where allowed or
-    // where no register kernel exists
-    int cy[3], cx[3], cz[2], ny = 0, nx = 0, nz = 0;
-    if (ry) cy[ny++] = 0;
-    if (rx) cx[nx++] = 0;
-    if (rz) cz[nz++] = 0;
-    if (gen || !ry) cy[ny++] = 16, cy[ny++] = 8;
-    if (gen || !rx) cx[nx++] = 16, cx[nx++] = 8;
-    if (gen || !rz) cz[nz++] = 32;
+int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream_t s) {
+    // the register transforms round differently from the stage kernels, so the family is a fixed
+    // rule (register wherever the size has one, unless the generic family is requested) and
+    // timing only picks among the stage kernels' line tiles, which give identical bits
+    const bool reg = p->variant != SB_FFT_GENERIC;
+    p->yt = reg && f4_has(p->K[1]) ? 0 : 16;
+    p->xt = reg && f4_has(p->K[0]) ? 0 : 16;
+    p->zt = reg && f4_has_z(p->K[2] / 2) ? 0 : 32;
+    if (p->yt && p->xt) return SB_OK;
     cudaEvent_t a, b;
     SB_CHECK_CUDA(cudaEventCreate(&a));
     SB_CHECK_CUDA(cudaEventCreate(&b));
     int st = SB_OK;
-    float best = 1e30f, ms = 0.f;
+    const int cand[2] = {16, 8};
+    float best_y = 1e30f, best_x = 1e30f, ms = 0.f;
     // every shape is timed twice; the second round decides (the first pays for module loading)
     for (int round = 0; round < 2 && !st; round++) {
-        best = 1e30f;
-        for (int c = 0; c < ny && !st; c++) {
-            st = time_launches([&] { return launch_ypass(p, d_spec, 0, cy[c], s); }, a, b, s, &ms);
-            if (!st && ms < best) best = ms, p->yt = cy[c];
-        }
-        best = 1e30f;
-        for (int c = 0; c < nx && !st; c++) {
-            st = time_launches(
-                [&] { return launch_xconv(p, d_spec, d_bc, nullptr, cx[c], s, nullptr); }, a, b,
-                s, &ms);
-            if (!st && ms < best) best = ms, p->xt = cx[c];
-        }
-        best = 1e30f;
-        for (int c = 0; c < nz && !st; c++) {
-            // forward then inverse: d_qfix stays zero (the forward pass clears what it reads)
-            st = time_launches(
-                [&] {
-                    SB_TRY(launch_zfwd(p, d_qfix, d_spec, cz[c], s));
-                    return launch_zinv(p, d_spec, d_real, cz[c], s);
-                },
-                a, b, s, &ms);
-            if (!st && ms < best) best = ms, p->zt = cz[c];
+        best_y = best_x = 1e30f;
+        for (int c = 0; c < 2 && !st; c++) {
+            if (p->yt) {
+                st = time_launches([&] { return launch_ypass(p, d_spec, 0, cand[c], s); }, a, b,
+                                   s, &ms);
+                if (!st && ms < best_y) best_y = ms, p->yt = cand[c];
+            }
+            if (p->xt && !st) {
+                st = time_launches(
+                    [&] { return launch_xconv(p, d_spec, d_bc, nullptr, cand[c], s, nullptr); },
+                    a, b, s, &ms);
+                if (!st && ms < best_x) best_x = ms, p->xt = cand[c];
+            }
         }
     }
     cudaEventDestroy(a);

@@ -91,19 +91,18 @@ struct SbFftPlan {
     SbFftAxis x;               // length K0
     float2* d_post = nullptr;  // e^{-2 pi i k / K2}, k < K2/2 (real-transform twiddles)
     size_t plane_smem = 0;     // bytes of the plane kernels' dynamic shared memory
-    // kernel shape of each pass, picked by timing: 0 = register line transform (sizes that have
-    // one), 8 or 16 = generic stage kernels with that many lines per block (z: 32 rows)
+    // kernel shape of each pass: 0 = register line transform (sizes that have one, unless the
+    // generic family is requested), else the stage kernels with 8 or 16 lines per block (picked
+    // by timing; both give the same bits) or 32 rows (z)
     int yt = 16;
     int xt = 16;
     int zt = 32;
-    int variant = 0;           // SB_FFT_AUTO / SB_FFT_GENERIC / SB_FFT_REGISTER
+    int variant = 0;           // SB_FFT_AUTO / SB_FFT_GENERIC
 };
 
-// times the kernel shapes the plan's variant allows for every pass and keeps the fastest;
-// d_qfix must hold zeros (the forward z pass reads and clears it), d_spec and d_real are
-// overwritten
-int sb_fft_plan_tune(SbFftPlan* p, long long* d_qfix, float2* d_spec, const float* d_bc,
-                     float* d_real, cudaStream_t s);
+// sets the kernel shape of every pass for the plan's variant, timing the stage kernels' line
+// tiles where they run; d_spec is overwritten
+int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream_t s);
 
 int sb_fft_plan_create(SbFftPlan* p, const int K[3]);
 void sb_fft_plan_destroy(SbFftPlan* p);
@@ -209,6 +208,12 @@ struct sb_pme {
     void* cufft_r2c = nullptr;      // plain form: cuFFT handles (stored as int)
     void* cufft_c2r = nullptr;
     int cufft_ok = 0;
+    // fused step: the reciprocal grid chain runs on `side` (highest priority, non-blocking)
+    // between a fork and a join event, concurrently with the pair kernel on the caller's stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int overlap = 1;
+    int rec_nparts = 0;             // energy partials written by the last grid chain
 };
 
 // kernels/launchers shared across files
@@ -225,6 +230,17 @@ int sb_lj_fused_direct(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_
                        const float* d_charge, float pme_beta, int need_atom_energy,
                        float* d_atom_energy, int need_virial, float* d_atom_lj_virial,
                        float* d_atom_direct_pme_energy, cudaStream_t s);
+// the pair kernel alone, on coordinates already packed by sb_nl_pack
+int sb_lj_fused_pair(sb_lennard_jones* lj, sb_neighbor_list* nl, float pme_beta,
+                     int need_atom_energy, float* d_atom_energy, int need_virial,
+                     float* d_atom_lj_virial, float* d_atom_direct_pme_energy, cudaStream_t s);
+// reciprocal part in two pieces: the grid chain (spread of the packed slots, FFT, convolution,
+// inverse FFT into d_theta) and the finish (gather + fixed-point finalisation into d_frc, energy
+// and virial sums), which must follow the pair and exclusion kernels
+int sb_pme_fused_grid(sb_pme* pme, sb_neighbor_list* nl, int want_energy, cudaStream_t s);
+int sb_pme_fused_finish(sb_pme* pme, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
+                        int need_virial, int need_energy, float* d_virial, float* d_potential,
+                        cudaStream_t s);
 int sb_pme_fused_excluded(sb_pme* pme, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
                           const float* d_charge, const int* es, const int* el, const int* en,
                           float* d_atom_energy, cudaStream_t s);

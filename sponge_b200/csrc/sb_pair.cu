@@ -410,19 +410,26 @@ extern "C" int sb_lj_pme_direct_force(sb_lennard_jones* lj, sb_neighbor_list* nl
 
 // fused fixed-form step: pack + pair kernel into the list's slot-order fixed-point buffer, left
 // there for the exclusion pass and the reciprocal gather to finish
-int sb_lj_fused_direct(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
-                       const float* d_charge, float pme_beta, int need_atom_energy,
-                       float* d_atom_energy, int need_virial, float* d_atom_lj_virial,
-                       float* d_atom_direct_pme_energy, cudaStream_t s) {
+int sb_lj_fused_pair(sb_lennard_jones* lj, sb_neighbor_list* nl, float pme_beta,
+                     int need_atom_energy, float* d_atom_energy, int need_virial,
+                     float* d_atom_lj_virial, float* d_atom_direct_pme_energy, cudaStream_t s) {
     if ((need_atom_energy > 0 && !d_atom_energy) ||
         (need_virial > 0 && (!d_atom_lj_virial || !d_atom_direct_pme_energy))) {
         sb_set_error("sb_nonbonded_step: energy/virial output missing");
         return SB_ERR_ARG;
     }
     const int ev = (need_atom_energy > 0 ? SB_EV_ENERGY : 0) | (need_virial > 0 ? SB_EV_VIRIAL : 0);
-    SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
     return launch_pair_fixed(lj, nl, pme_beta, ev, d_atom_energy, d_atom_lj_virial,
                              d_atom_direct_pme_energy, s);
+}
+
+int sb_lj_fused_direct(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
+                       const float* d_charge, float pme_beta, int need_atom_energy,
+                       float* d_atom_energy, int need_virial, float* d_atom_lj_virial,
+                       float* d_atom_direct_pme_energy, cudaStream_t s) {
+    SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
+    return sb_lj_fused_pair(lj, nl, pme_beta, need_atom_energy, d_atom_energy, need_virial,
+                            d_atom_lj_virial, d_atom_direct_pme_energy, s);
 }
 
 extern "C" int sb_lj_long_range_correction(sb_lennard_jones* lj, int need_pressure,

@@ -27,15 +27,26 @@ __device__ __forceinline__ void pair_walk(
     float (&ei)[IPL], float (&vi)[IPL], float (&di)[IPL]) {
     constexpr int LPE = PairLane<IPL>::LPE;
     constexpr int EPW = PairLane<IPL>::EPW;
+    // two-deep software pipeline: list entries are loaded two batches ahead (a DRAM stream) and
+    // the j coordinates/types one batch ahead (L1/L2 gathers), so their latency overlaps the
+    // current batch's arithmetic. Past the end v = 0: j = 0 (a valid slot) and an empty mask.
+    uint32_t v1 = eslot < cnt ? ents[eslot] : 0u;
+    uint32_t v2 = eslot + EPW < cnt ? ents[eslot + EPW] : 0u;
+    uint4 xj1 = xq[v1 & 0xffffffu];
+    int tj1 = stype[v1 & 0xffffffu];
     // warp-uniform trip count so that the lanes of one entry stay converged for the shuffles
     for (int e0 = 0; e0 < cnt; e0 += EPW) {
         const int e = e0 + eslot;
         const bool valid = e < cnt;
-        const uint32_t v = valid ? ents[e] : 0u;
+        const uint32_t v = v1;
+        const uint4 xj = xj1;
+        const int tj = tj1;
+        v1 = v2;
+        v2 = e + 2 * EPW < cnt ? ents[e + 2 * EPW] : 0u;
+        xj1 = xq[v1 & 0xffffffu];
+        tj1 = stype[v1 & 0xffffffu];
         const int j = (int)(v & 0xffffffu);
         const uint32_t m = (v >> 24) >> (h * IPL);
-        const uint4 xj = xq[j];
-        const int tj = stype[j];
         const float xjr = __int2float_rn((int)(xj.x - rx)) * P.sx;
         const float yjr = __int2float_rn((int)(xj.y - ry)) * P.sy;
         const float zjr = __int2float_rn((int)(xj.z - rz)) * P.sz;
@@ -58,7 +69,7 @@ __device__ __forceinline__ void pair_walk(
             const bool act = ((m >> k) & 1u) && r2 < P.rc2;
             // evaluated for every lane and discarded by a select where inactive (r2 may be 0
             // there, so a select, not a multiply, removes the non-finite values)
-            const float ri = rsqrtf(r2);
+            const float ri = sb_rsqrt(r2);
             const float ri2 = ri * ri;
             const float ri6 = ri2 * ri2 * ri2;
             const float2 ab = sAB[ti[k] + tj];
@@ -95,8 +106,10 @@ __device__ __forceinline__ void pair_walk(
     }
 }
 
+// force-only launches are capped at 96 registers (five 4-warp blocks per SM; the few spills
+// cost less than the occupancy gains), energy/virial launches keep four blocks
 template <int EV, int IPL>
-__global__ void __launch_bounds__(128) k_pair_fixed(
+__global__ void __launch_bounds__(128, EV ? 4 : 5) k_pair_fixed(
     PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
     const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
     const int* __restrict__ stype, const float2* __restrict__ AB,

@@ -442,9 +442,17 @@ extern "C" int sb_pme_create(int atom_numbers, const float box_length[3], float 
     if ((st = build_bc(p))) return fail(st);
     if (form == SB_FORM_FIXED) {
         // kernel shapes of the FFT passes, picked by timing on this grid
-        if ((st = sb_fft_plan_tune(&p->plan, p->d_qfix, p->d_spec, p->d_bc, p->d_theta, 0)))
+        if ((st = sb_fft_plan_tune(&p->plan, p->d_spec, p->d_bc, 0)))
             return fail(st);
         cudaMemset(p->d_spec, 0, sizeof(float2) * p->Gh);
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        if (cudaStreamCreateWithPriority(&p->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+            sb_set_error("sb_pme_create: stream/event creation failed");
+            return fail(SB_ERR_CUDA);
+        }
     }
     *out = p;
     return SB_OK;
@@ -455,15 +463,14 @@ extern "C" int sb_pme_set_fft_variant(sb_pme* p, int variant) {
         sb_set_error("sb_pme_set_fft_variant: null handle");
         return SB_ERR_ARG;
     }
-    if (variant < SB_FFT_AUTO || variant > SB_FFT_REGISTER) {
-        sb_set_error("sb_pme_set_fft_variant: variant %d is not AUTO, GENERIC or REGISTER",
-                     variant);
+    if (variant != SB_FFT_AUTO && variant != SB_FFT_GENERIC) {
+        sb_set_error("sb_pme_set_fft_variant: variant %d is not AUTO or GENERIC", variant);
         return SB_ERR_ARG;
     }
     if (p->form != SB_FORM_FIXED) return SB_OK;  // the plain form runs the library FFT
     SB_CHECK_CUDA(cudaDeviceSynchronize());
     p->plan.variant = variant;
-    SB_TRY(sb_fft_plan_tune(&p->plan, p->d_qfix, p->d_spec, p->d_bc, p->d_theta, 0));
+    SB_TRY(sb_fft_plan_tune(&p->plan, p->d_spec, p->d_bc, 0));
     SB_CHECK_CUDA(cudaMemset(p->d_spec, 0, sizeof(float2) * p->Gh));
     SB_CHECK_CUDA(cudaDeviceSynchronize());
     return SB_OK;
@@ -473,6 +480,9 @@ extern "C" int sb_pme_destroy(sb_pme* p) {
     if (!p) return SB_OK;
     cudaDeviceSynchronize();
     sb_fft_plan_destroy(&p->plan);
+    if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+    if (p->ev_join) cudaEventDestroy(p->ev_join);
+    if (p->side) cudaStreamDestroy(p->side);
     if (p->cufft_ok) {
         cufftDestroy((cufftHandle)(intptr_t)p->cufft_r2c);
         cufftDestroy((cufftHandle)(intptr_t)p->cufft_c2r);
@@ -915,24 +925,27 @@ int sb_pme_fused_excluded(sb_pme* p, sb_neighbor_list* nl, const uint32_t* d_uin
     return SB_OK;
 }
 
-int sb_pme_fused_reciprocal(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
-                            int need_virial, int need_energy, float* d_virial, float* d_potential,
-                            cudaStream_t s) {
+int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s) {
     const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
-    const int want = need_virial > 0 || need_energy > 0;
-    int nparts = 0;
     k_spread_slot<<<(4 * nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->meta, nl->xq, K0, K1, K2,
                                                                  p->d_qfix);
     SB_CHECK_LAUNCH();
     SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
-    SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want, s, &nparts));
-    SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+    SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_energy, s,
+                             &p->rec_nparts));
+    return sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s);
+}
+
+int sb_pme_fused_finish(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
+                        int need_virial, int need_energy, float* d_virial, float* d_potential,
+                        cudaStream_t s) {
+    const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
     k_gather_finalize<<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
         nl->meta, nl->slot_atom, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
         (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, d_frc);
     SB_CHECK_LAUNCH();
-    if (want) {
-        k_pme_energy_finish<<<1, 1024, 0, s>>>(p->n, d_charge, p->d_epart, nparts,
+    if (need_virial > 0 || need_energy > 0) {
+        k_pme_energy_finish<<<1, 1024, 0, s>>>(p->n, d_charge, p->d_epart, p->rec_nparts,
                                                p->d_direct_atom_energy,
                                                p->d_correction_atom_energy, (double)p->beta,
                                                p->neutralizing_factor, p->d_ered, need_virial > 0,
@@ -940,6 +953,14 @@ int sb_pme_fused_reciprocal(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const
         SB_CHECK_LAUNCH();
     }
     return SB_OK;
+}
+
+int sb_pme_fused_reciprocal(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
+                            int need_virial, int need_energy, float* d_virial, float* d_potential,
+                            cudaStream_t s) {
+    SB_TRY(sb_pme_fused_grid(p, nl, need_virial > 0 || need_energy > 0, s));
+    return sb_pme_fused_finish(p, nl, d_frc, d_charge, need_virial, need_energy, d_virial,
+                               d_potential, s);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -123,9 +123,9 @@ def test_reciprocal_force(case):
     name, s, eng, ref = case
     import sponge_b200
     out = {}
-    # both FFT kernel families (register line transforms exist for every grid here), then the
-    # timed choice, which stays in place for the other tests
-    for v in (sponge_b200.FFT_GENERIC, sponge_b200.FFT_REGISTER, sponge_b200.FFT_AUTO):
+    # both FFT kernel families (register line transforms exist for every grid here); the
+    # default (register) stays in place for the other tests
+    for v in (sponge_b200.FFT_GENERIC, sponge_b200.FFT_AUTO):
         eng.pme.set_fft_variant(v)
         out[v] = _forces(eng, ("reciprocal",))
         assert rel_rms(out[v], ref["f_rec"]) < FORCE_TOL
@@ -133,7 +133,7 @@ def test_reciprocal_force(case):
         e, parts = eng.pme.Get_Energy(eng.uint_crd, eng.charge, eng.nl, eng.scaler, *eng.excl,
                                       which_part=sponge_b200.PME_TOTAL, parts=True)
         assert parts["reciprocal"] == pytest.approx(ref["e_rec"], rel=1e-5)
-    assert rel_rms(out[sponge_b200.FFT_REGISTER], out[sponge_b200.FFT_GENERIC]) < 1e-6
+    assert rel_rms(out[sponge_b200.FFT_AUTO], out[sponge_b200.FFT_GENERIC]) < 1e-6
 
 
 def test_total_force(case):
@@ -263,8 +263,16 @@ def test_fused_step_matches_module_sequence(name, torch_cuda, oracle_lib):
         runs.append(eng.frc.cpu().numpy().astype(np.float64))
     assert np.array_equal(runs[0], runs[1])
     assert rel_rms(runs[0], a) < 1e-6
-    assert eng.potential() == pytest.approx(pa, rel=1e-6)
-    assert eng.virial() == pytest.approx(va, rel=1e-6)
+    p0, v0 = eng.potential(), eng.virial()
+    assert p0 == pytest.approx(pa, rel=1e-6)
+    assert v0 == pytest.approx(va, rel=1e-6)
+    # the serial schedule (no side stream) gives the same bits as the overlapped default
+    eng.pme.set_overlap(False)
+    eng.reset()
+    eng.step(need_energy=1, need_virial=1)
+    assert np.array_equal(eng.frc.cpu().numpy().astype(np.float64), runs[0])
+    assert eng.potential() == p0 and eng.virial() == v0
+    eng.pme.set_overlap(True)
     uc = eng.uint_crd.cpu().numpy().view(np.uint32)
     ref = oracle_lib.reference_energies(s, uc=uc)
     assert rel_rms(runs[0], ref["f_total"]) < FORCE_TOL
@@ -274,14 +282,17 @@ def test_fused_step_matches_module_sequence(name, torch_cuda, oracle_lib):
     assert rel_rms(eng.frc.cpu().numpy(), runs[0]) < 1e-6
 
 
-@pytest.mark.parametrize("form", ["fixed", "plain"])
+@pytest.mark.parametrize("form", ["fixed", "fixed-serial", "plain"])
 def test_force_graph_replay_matches_eager_step(form, torch_cuda):
     """The force part captured once as a CUDA graph and replayed after each list update gives
-    the eager step's forces (bit-identical in the fixed form)."""
+    the eager step's forces (bit-identical in the fixed form, whose captured graph holds the
+    side-stream branch unless the serial schedule is chosen)."""
     from sponge_b200 import FORM_FIXED, FORM_PLAIN, NonbondedEngine
     s = systems.config0()
-    eng = NonbondedEngine(s, form=FORM_FIXED if form == "fixed" else FORM_PLAIN,
+    eng = NonbondedEngine(s, form=FORM_PLAIN if form == "plain" else FORM_FIXED,
                           refresh_interval=3)
+    if form == "fixed-serial":
+        eng.pme.set_overlap(False)
     eng.update_list(forced=1)
     eng.to_uint()
     eng.capture_force_graph()
@@ -293,7 +304,7 @@ def test_force_graph_replay_matches_eager_step(form, torch_cuda):
         eng.frc.zero_()
         eng.force()
         e = eng.frc.cpu().numpy()
-        if form == "fixed":
+        if form != "plain":
             assert np.array_equal(g, e), k
         else:
             assert rel_rms(g, e) < 1e-6, k
