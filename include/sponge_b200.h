@@ -154,15 +154,16 @@ SB_API int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[3]);
 
 /* Pair-kernel shape of the fixed-point form (no reference counterpart; a tuning knob):
  * i atoms held per lane, 8 (one lane per list entry) or 4 (two lanes per entry, fewer registers,
- * more resident warps), or 1: the compacted kernel, which first filters each batch of entries to
- * the pairs inside the cutoff and then evaluates one such pair per lane. Results are identical to
- * FP32 rounding whichever shape runs. */
+ * more resident warps); 2: the eight-atom layout evaluated two (i, j) slots at a time on the
+ * packed FP32x2 instructions (the default); or 1: the compacted kernel, which first filters each
+ * batch of entries to the pairs inside the cutoff and then evaluates one such pair per lane.
+ * Results are identical to FP32 rounding whichever shape runs. */
 SB_API int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane);
 
 /* Autotuner: times each pair-kernel shape on the current list and keeps the fastest; writes the
  * choice to *h_chosen. Synchronises the stream; leaves d_frc untouched. The shapes sum in
  * different orders, so a process that needs the same bits as another sets the shape explicitly
- * (sb_lj_set_kernel_variant) rather than tuning (the default shape is 8). */
+ * (sb_lj_set_kernel_variant) rather than tuning (the default shape is 2). */
 SB_API int sb_lj_tune(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
                       const float* d_charge, float pme_beta, int* h_chosen, void* stream);
 

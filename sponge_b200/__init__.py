@@ -298,8 +298,9 @@ class LennardJones:
         _check(lib().sb_lj_update_volume(self.handle, _box3(box_length)))
 
     def set_kernel_variant(self, atoms_per_lane):
-        """Pair-kernel shape: 8 or 4 i atoms per lane, or 1 for the compacted kernel (one
-        in-cutoff pair per lane); a tuning knob with the same results."""
+        """Pair-kernel shape: 8 or 4 i atoms per lane, 2 for eight atoms per lane on packed
+        FP32x2 slot pairs (the default), or 1 for the compacted kernel (one in-cutoff pair per
+        lane); a tuning knob with the same results to FP32 rounding."""
         _check(lib().sb_lj_set_kernel_variant(self.handle, int(atoms_per_lane)))
 
     def tune(self, nl, uint_crd, charge, pme_beta, stream=None):

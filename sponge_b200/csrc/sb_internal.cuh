@@ -180,7 +180,8 @@ struct sb_lennard_jones {
     int* d_type = nullptr;          // [N]
     double* d_red = nullptr;        // FP64 reduction scratch
     float* d_energy_atom = nullptr; // [N] scratch for Get_Energy
-    int ipl = 4;                    // pair kernel: i atoms per lane (8, or 4 with 2 lanes/entry)
+    int ipl = 2;                    // pair kernel shape: 8 or 4 i atoms per lane, 2 = packed
+                                    // FP32x2 slot pairs, 1 = compacted in-cutoff pairs
 };
 
 struct sb_pme {

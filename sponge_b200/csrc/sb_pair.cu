@@ -53,6 +53,7 @@ __device__ __forceinline__ void red_fix(long long* p, float v) {
 
 #include "sb_pair_fixed.cuh"
 #include "sb_pair_compact.cuh"
+#include "sb_pair_x2.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // plain form: reference structure (warp per atom, float atomics), Lennard_Jones_force.cu:47-158
@@ -283,7 +284,7 @@ static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list
 static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float beta, int ev,
                              float* ae, float* av, float* ad, cudaStream_t s) {
     PairParams P = pair_params(lj, nl, beta);
-    const int warps = 4;
+    const int warps = 1;  // one cluster per block (the launch bounds assume it)
     const int blocks = (nl->clu_cap + warps - 1) / warps;
     const size_t smem = sizeof(float2) * lj->ntypes * lj->ntypes;
     if (smem > 96 * 1024) {
@@ -309,7 +310,20 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
             P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
             nl->slot_atom, nl->fix, ae, av, ad);                                              \
     } while (0)
-    if (lj->ipl == 1) {
+#define SB_LAUNCH_X2(EVV)                                                                     \
+    do {                                                                                      \
+        k_pair_x2<EVV><<<nl->clu_cap, 32, sizeof(float4) * 4 * lj->ntypes, s>>>(              \
+            P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
+            nl->slot_atom, nl->fix, ae, av, ad);                                              \
+    } while (0)
+    if (lj->ipl == 2 && !P.wide) {
+        switch (ev) {
+            case 0: SB_LAUNCH_X2(0); break;
+            case 1: SB_LAUNCH_X2(1); break;
+            case 2: SB_LAUNCH_X2(2); break;
+            default: SB_LAUNCH_X2(3); break;
+        }
+    } else if (lj->ipl == 1) {
         switch (ev) {
             case 0: SB_LAUNCH_COMPACT(0); break;
             case 1: SB_LAUNCH_COMPACT(1); break;
@@ -500,8 +514,9 @@ extern "C" int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[
 }
 
 extern "C" int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane) {
-    if (!lj || (atoms_per_lane != 1 && atoms_per_lane != 4 && atoms_per_lane != 8)) {
-        sb_set_error("sb_lj_set_kernel_variant: atoms_per_lane must be 1, 4 or 8");
+    if (!lj || (atoms_per_lane != 1 && atoms_per_lane != 2 && atoms_per_lane != 4 &&
+                atoms_per_lane != 8)) {
+        sb_set_error("sb_lj_set_kernel_variant: atoms_per_lane must be 1, 2, 4 or 8");
         return SB_ERR_ARG;
     }
     lj->ipl = atoms_per_lane;
@@ -521,13 +536,13 @@ extern "C" int sb_lj_tune(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint
     }
     cudaStream_t s = sb_stream(stream);
     SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
-    const int cand[3] = {1, 4, 8};
+    const int cand[4] = {1, 4, 8, 2};
     float best = 1e30f;
     int pick = lj->ipl;
     cudaEvent_t a, b;
     SB_CHECK_CUDA(cudaEventCreate(&a));
     SB_CHECK_CUDA(cudaEventCreate(&b));
-    for (int c = 0; c < 3; c++) {
+    for (int c = 0; c < 4; c++) {
         lj->ipl = cand[c];
         SB_TRY(launch_pair_fixed(lj, nl, pme_beta, 0, nullptr, nullptr, nullptr, s));
         SB_CHECK_CUDA(cudaEventRecord(a, s));

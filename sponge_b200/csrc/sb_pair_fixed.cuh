@@ -106,10 +106,12 @@ __device__ __forceinline__ void pair_walk(
     }
 }
 
-// force-only launches are capped at 96 registers (five 4-warp blocks per SM; the few spills
-// cost less than the occupancy gains), energy/virial launches keep four blocks
+// One-warp blocks: a block's slot frees as soon as its cluster is done (no waiting on a slower
+// sibling warp), which also lets the reciprocal kernels of the side stream interleave. Force-only
+// launches are capped at 96 registers (20 warps per SM; the few spills cost less than the
+// occupancy gains), energy/virial launches at 128 (16 warps).
 template <int EV, int IPL>
-__global__ void __launch_bounds__(128, EV ? 4 : 5) k_pair_fixed(
+__global__ void __launch_bounds__(32, EV ? 16 : 20) k_pair_fixed(
     PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
     const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
     const int* __restrict__ stype, const float2* __restrict__ AB,

@@ -1,0 +1,247 @@
+// Fixed-point cluster pair kernel on packed FP32x2 arithmetic (chosen form) — included by
+// sb_pair.cu after sb_pair_fixed.cuh.
+//
+// Same work decomposition as the eight-atoms-per-lane kernel (one warp per 8-atom i-cluster, one
+// lane per list entry, j force out through three 64-bit fixed-point atomics, i forces reduced
+// over the warp once per cluster), but the eight (i, j) slots of an entry are evaluated as four
+// pairs of slots (i atoms 2p and 2p+1) on the sm_100 FP32x2 instructions (fma/mul/add .f32x2),
+// which do two single-precision operations per issue slot. Per component each operation rounds
+// exactly like its scalar counterpart; only the order of the j-force sum changes (even and odd
+// i atoms summed separately, then added).
+//
+// The LJ coefficients of a slot pair come from a per-cluster table in shared memory built when
+// the warp takes its cluster: row tj holds, for every i pair p, the float4 (-A(t_2p, tj),
+// -A(t_2p+1, tj), B(t_2p, tj), B(t_2p+1, tj)), so one 16-byte load yields both slots' packed
+// operands.
+#pragma once
+
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ float sb_rcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// -beta^3 G(z) on a pair of slots by the (5,5) rational of sb_ewald_G_rational (valid for
+// z <= 12); gp holds the numerator coefficients pre-multiplied by beta^3, highest degree first
+__device__ __forceinline__ float2 ewald_nG2(float2 z, const float* gp) {
+    float2 p = f2(-gp[0]);
+    p = f2fma(p, z, f2(-gp[1]));
+    p = f2fma(p, z, f2(-gp[2]));
+    p = f2fma(p, z, f2(-gp[3]));
+    p = f2fma(p, z, f2(-gp[4]));
+    p = f2fma(p, z, f2(-gp[5]));
+    float2 q = f2(1.255407394e-04f);
+    q = f2fma(q, z, f2(2.169710712e-03f));
+    q = f2fma(q, z, f2(2.242775561e-02f));
+    q = f2fma(q, z, f2(1.454184461e-01f));
+    q = f2fma(q, z, f2(5.616555609e-01f));
+    q = f2fma(q, z, f2(1.0f));
+    return f2mul(p, make_float2(sb_rcp(q.x), sb_rcp(q.y)));
+}
+
+template <int EV, bool EXACT>
+__device__ __forceinline__ void pair_walk_x2(
+    const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
+    const uint4* __restrict__ xq, const int* __restrict__ stype, const float4* ctab,
+    long long* __restrict__ fix, const int base, const int lane, const uint32_t rx,
+    const uint32_t ry, const uint32_t rz, const float2 (&nx)[4], const float2 (&ny)[4],
+    const float2 (&nz)[4], const float2 (&nq)[4], float2 (&fx)[4], float2 (&fy)[4],
+    float2 (&fz)[4], float (&ei)[8], float (&vi)[8], float (&di)[8]) {
+    const float2 rc2 = f2(P.rc2);
+    const float2 b2 = f2(P.beta2);
+    // two-deep software pipeline as in the scalar kernel: entries two batches ahead, j data one
+    uint32_t v1 = lane < cnt ? ents[lane] : 0u;
+    uint32_t v2 = lane + 32 < cnt ? ents[lane + 32] : 0u;
+    uint4 xj1 = xq[v1 & 0xffffffu];
+    int tj1 = stype[v1 & 0xffffffu];
+    for (int e0 = 0; e0 < cnt; e0 += 32) {
+        const int e = e0 + lane;
+        const bool valid = e < cnt;
+        const uint32_t v = v1;
+        const uint4 xj = xj1;
+        const int tj = tj1;
+        v1 = v2;
+        v2 = e + 64 < cnt ? ents[e + 64] : 0u;
+        xj1 = xq[v1 & 0xffffffu];
+        tj1 = stype[v1 & 0xffffffu];
+        const int j = (int)(v & 0xffffffu);
+        const uint32_t m = v >> 24;
+        const float2 xj2 = f2(__int2float_rn((int)(xj.x - rx)) * P.sx);
+        const float2 yj2 = f2(__int2float_rn((int)(xj.y - ry)) * P.sy);
+        const float2 zj2 = f2(__int2float_rn((int)(xj.z - rz)) * P.sz);
+        const float2 qj2 = f2(__uint_as_float(xj.w));
+        const float4* trow = ctab + tj * 4;
+        float2 gx = f2(0.f), gy = f2(0.f), gz = f2(0.f);
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+            float2 dx, dy, dz;
+            if (EXACT) {
+                const uint4 xa = xq[base + 2 * p], xb = xq[base + 2 * p + 1];
+                dx = make_float2(__int2float_rn((int)(xj.x - xa.x)) * P.sx,
+                                 __int2float_rn((int)(xj.x - xb.x)) * P.sx);
+                dy = make_float2(__int2float_rn((int)(xj.y - xa.y)) * P.sy,
+                                 __int2float_rn((int)(xj.y - xb.y)) * P.sy);
+                dz = make_float2(__int2float_rn((int)(xj.z - xa.z)) * P.sz,
+                                 __int2float_rn((int)(xj.z - xb.z)) * P.sz);
+            } else {
+                dx = f2add(xj2, nx[p]);
+                dy = f2add(yj2, ny[p]);
+                dz = f2add(zj2, nz[p]);
+            }
+            const float2 r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
+            const bool a0 = ((m >> (2 * p)) & 1u) && r2.x < rc2.x;
+            const bool a1 = ((m >> (2 * p + 1)) & 1u) && r2.y < rc2.y;
+            // evaluated on every slot and discarded by a select where inactive
+            const float2 ri = make_float2(sb_rsqrt(r2.x), sb_rsqrt(r2.y));
+            const float2 ri2 = f2mul(ri, ri);
+            const float2 ri6 = f2mul(f2mul(ri2, ri2), ri2);
+            const float4 t = trow[p];
+            const float2 l = f2fma(make_float2(t.x, t.y), ri6, make_float2(t.z, t.w));
+            const float2 flj = f2mul(l, f2mul(ri6, ri2));
+            const float2 nqq = f2mul(nq[p], qj2);
+            const float2 ngb = ewald_nG2(f2mul(b2, r2), P.gp);
+            const float2 fs2 = f2fma(nqq, f2add(f2mul(ri, ri2), ngb), flj);
+            const float2 fs = make_float2(a0 ? fs2.x : 0.f, a1 ? fs2.y : 0.f);
+            fx[p] = f2fma(fs, dx, fx[p]);
+            fy[p] = f2fma(fs, dy, fy[p]);
+            fz[p] = f2fma(fs, dz, fz[p]);
+            gx = f2fma(fs, dx, gx);
+            gy = f2fma(fs, dy, gy);
+            gz = f2fma(fs, dz, gz);
+            if (EV) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const bool act = h ? a1 : a0;
+                    if (act) {
+                        const int k = 2 * p + h;
+                        const float rr2 = h ? r2.y : r2.x, rri = h ? ri.y : ri.x;
+                        const float rri6 = h ? ri6.y : ri6.x;
+                        const float A = -(h ? t.y : t.x), B = h ? t.w : t.z;
+                        const float qq = -(h ? nqq.y : nqq.x);
+                        const float ec = qq * erfcf(P.beta * rr2 * rri) * rri;
+                        if (EV & SB_EV_ENERGY)
+                            ei[k] += (0.083333333f * A * rri6 - 0.166666667f * B) * rri6 + ec;
+                        if (EV & SB_EV_VIRIAL) vi[k] -= (h ? flj.y : flj.x) * rr2;
+                        di[k] += ec;
+                    }
+                }
+            }
+        }
+        const float fjx = -(gx.x + gx.y), fjy = -(gy.x + gy.y), fjz = -(gz.x + gz.y);
+        if (valid && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
+            red_fix(&fix[j], fjx);
+            red_fix(&fix[P.slot_cap + j], fjy);
+            red_fix(&fix[2 * P.slot_cap + j], fjz);
+        }
+    }
+}
+
+// One-warp blocks (see k_pair_fixed); dynamic shared memory: the cluster's LJ table, 4 nt float4.
+template <int EV>
+__global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
+    PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
+    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
+    const int* __restrict__ stype, const float2* __restrict__ AB,
+    const int* __restrict__ slot_atom, long long* __restrict__ fix,
+    float* __restrict__ atom_energy, float* __restrict__ atom_virial,
+    float* __restrict__ atom_direct) {
+    extern __shared__ float4 ctab[];
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x;
+    if (c >= meta[0]) return;
+    const int base = c * SB_CLUSTER;
+    const uint4 my = lane < SB_CLUSTER ? xq[base + lane] : make_uint4(0, 0, 0, 0);
+    const int myt = lane < SB_CLUSTER ? stype[base + lane] : 0;
+    // cluster LJ table: entry (tj, p) = (-A(t_2p,tj), -A(t_2p+1,tj), B(t_2p,tj), B(t_2p+1,tj))
+    const int nt = P.nt;
+    {
+        // lane l always serves pair p = l & 3, so its two i types are fetched once
+        const int p = lane & 3;
+        const int ta = __shfl_sync(0xffffffffu, myt, 2 * p) * nt;
+        const int tb = __shfl_sync(0xffffffffu, myt, 2 * p + 1) * nt;
+        for (int t = lane; t < 4 * nt; t += 32) {
+            const int tj = t >> 2;
+            const float2 a = AB[ta + tj], b = AB[tb + tj];
+            ctab[t] = make_float4(-a.x, -b.x, a.y, b.y);
+        }
+    }
+    const uint32_t rx = __shfl_sync(0xffffffffu, my.x, 0);
+    const uint32_t ry = __shfl_sync(0xffffffffu, my.y, 0);
+    const uint32_t rz = __shfl_sync(0xffffffffu, my.z, 0);
+    const float mxr = __int2float_rn((int)(my.x - rx)) * P.sx;
+    const float myr = __int2float_rn((int)(my.y - ry)) * P.sy;
+    const float mzr = __int2float_rn((int)(my.z - rz)) * P.sz;
+    const float mq = __uint_as_float(my.w);
+    float2 nx[4], ny[4], nz[4], nq[4], fx[4], fy[4], fz[4];
+    float ei[8], vi[8], di[8];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+        nx[p] = make_float2(-__shfl_sync(0xffffffffu, mxr, 2 * p),
+                            -__shfl_sync(0xffffffffu, mxr, 2 * p + 1));
+        ny[p] = make_float2(-__shfl_sync(0xffffffffu, myr, 2 * p),
+                            -__shfl_sync(0xffffffffu, myr, 2 * p + 1));
+        nz[p] = make_float2(-__shfl_sync(0xffffffffu, mzr, 2 * p),
+                            -__shfl_sync(0xffffffffu, mzr, 2 * p + 1));
+        nq[p] = make_float2(-__shfl_sync(0xffffffffu, mq, 2 * p),
+                            -__shfl_sync(0xffffffffu, mq, 2 * p + 1));
+        fx[p] = fy[p] = fz[p] = f2(0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) ei[k] = vi[k] = di[k] = 0.f;
+    __syncwarp();
+
+    const int cntf = cl_count[c];
+    const int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
+    const uint32_t* ents = cl_ent + (size_t)c * P.ent_cap;
+    if (cntf & SB_CL_EXACT)
+        pair_walk_x2<EV, true>(P, cnt, ents, xq, stype, ctab, fix, base, lane, rx, ry, rz, nx, ny,
+                               nz, nq, fx, fy, fz, ei, vi, di);
+    else
+        pair_walk_x2<EV, false>(P, cnt, ents, xq, stype, ctab, fix, base, lane, rx, ry, rz, nx,
+                                ny, nz, nq, fx, fy, fz, ei, vi, di);
+
+    // reduce each i atom's sums over the 32 lanes; lane 0 ends with the totals
+    float fxi[8], fyi[8], fzi[8];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+        fxi[2 * p] = fx[p].x, fxi[2 * p + 1] = fx[p].y;
+        fyi[2 * p] = fy[p].x, fyi[2 * p + 1] = fy[p].y;
+        fzi[2 * p] = fz[p].x, fzi[2 * p + 1] = fz[p].y;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            fxi[k] += __shfl_xor_sync(0xffffffffu, fxi[k], o);
+            fyi[k] += __shfl_xor_sync(0xffffffffu, fyi[k], o);
+            fzi[k] += __shfl_xor_sync(0xffffffffu, fzi[k], o);
+            if (EV) {
+                ei[k] += __shfl_xor_sync(0xffffffffu, ei[k], o);
+                vi[k] += __shfl_xor_sync(0xffffffffu, vi[k], o);
+                di[k] += __shfl_xor_sync(0xffffffffu, di[k], o);
+            }
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int s = base + k;
+            const int a = slot_atom[s];
+            if (a >= 0) {
+                red_fix(&fix[s], fxi[k]);
+                red_fix(&fix[P.slot_cap + s], fyi[k]);
+                red_fix(&fix[2 * P.slot_cap + s], fzi[k]);
+                if (EV & SB_EV_ENERGY) atom_energy[a] += ei[k];
+                if (EV & SB_EV_VIRIAL) {
+                    atom_virial[a] += vi[k];
+                    atom_direct[a] = di[k];
+                }
+            }
+        }
+    }
+}

@@ -100,15 +100,17 @@ def _forces(eng, parts, need_energy=0, need_virial=0):
 def test_direct_force(case):
     name, s, eng, ref = case
     out = {}
-    for ipl in (8, 4, 1):  # every pair-kernel shape (1 = compacted pairs)
+    # every pair-kernel shape (1 = compacted pairs, 2 = packed FP32x2 slot pairs)
+    for ipl in (8, 4, 2, 1):
         eng.lj.set_kernel_variant(ipl)
         out[ipl] = _forces(eng, ("direct",))
         assert rel_rms(out[ipl], ref["f_direct"]) < FORCE_TOL
         assert np.array_equal(_forces(eng, ("direct",)), out[ipl])  # bit-identical repeat
     assert rel_rms(out[4], out[8]) < 1e-6
+    assert rel_rms(out[2], out[8]) < 1e-6
     assert rel_rms(out[1], out[8]) < 1e-6
     chosen = eng.lj.tune(eng.nl, eng.uint_crd, eng.charge, eng.pme.beta)
-    assert chosen in (1, 4, 8)
+    assert chosen in (1, 2, 4, 8)
     # tuning leaves no residue in the accumulators
     assert np.array_equal(_forces(eng, ("direct",)), out[chosen])
 
@@ -144,7 +146,7 @@ def test_total_force(case):
     assert err < FORCE_TOL
 
 
-@pytest.mark.parametrize("ipl", [1, 4, 8])
+@pytest.mark.parametrize("ipl", [1, 2, 4, 8])
 def test_energies_and_virial(case, ipl):
     name, s, eng, ref = case
     torch = eng.torch
