@@ -223,14 +223,17 @@ __global__ void k_excl_range(int n, const int* __restrict__ es, const int* __res
     hi[i] = b;
 }
 
-__device__ __forceinline__ bool excluded_pair(int a, int b, const int* __restrict__ lo,
-                                              const int* __restrict__ hi,
-                                              const int* __restrict__ es,
+// {a, b} excluded: the pair's lower id p carries the other id q in its CSR list; [lo, hi] is the
+// id range of p's list (the caller holds it for both atoms), so most pairs need no list walk
+__device__ __forceinline__ bool excluded_pair(int a, int b, int lo_a, int hi_a, int lo_b,
+                                              int hi_b, const int* __restrict__ es,
                                               const int* __restrict__ en,
                                               const int* __restrict__ el) {
-    int p = min(a, b), q = max(a, b);
-    if (q < lo[p] || q > hi[p]) return false;
-    int s = es[p], e = s + en[p];
+    const bool a_low = a < b;
+    const int p = a_low ? a : b, q = a_low ? b : a;
+    const int lo = a_low ? lo_a : lo_b, hi = a_low ? hi_a : hi_b;
+    if (q < lo || q > hi) return false;
+    const int s = es[p], e = s + en[p];
     for (int k = s; k < e; k++)
         if (el[k] == q) return true;
     return false;
@@ -239,12 +242,45 @@ __device__ __forceinline__ bool excluded_pair(int a, int b, const int* __restric
 struct SearchParams {
     int ncx, ncy, nxr, nyr, fullx, fully;
     float sx, sy, sz, cs2, colwx, colwy, cs, lx, ly, lz;
-    unsigned long long rz;  // z window half-width in fixed-point units
+    float colw;            // the wider column width
+    int max_ranges;        // 2 x columns of the half-shell walk (two z windows per column)
+    float zscale;          // fixed-point units per A along z (2^32 / Lz)
     int slot_cap, ent_cap;
 };
 
-// one warp per cluster
-__global__ void __launch_bounds__(128) k_search(
+// inclusive z windows [zmin - rz, zmax + rz] with periodic wrap (one or two ranges)
+__device__ __forceinline__ int z_windows(uint32_t zmin, uint32_t zmax, unsigned long long rz,
+                                         uint32_t (&wa)[2], uint32_t (&wb)[2]) {
+    const long long zlo = (long long)zmin - (long long)rz;
+    const long long zhi = (long long)zmax + (long long)rz;
+    if (zhi - zlo >= 4294967296ll) {
+        wa[0] = 0; wb[0] = 0xffffffffu;
+        return 1;
+    }
+    if (zlo < 0) {
+        wa[0] = 0; wb[0] = (uint32_t)zhi; wa[1] = (uint32_t)(zlo + 4294967296ll); wb[1] = 0xffffffffu;
+        return 2;
+    }
+    if (zhi > 0xffffffffll) {
+        wa[0] = 0; wb[0] = (uint32_t)(zhi - 4294967296ll); wa[1] = (uint32_t)zlo; wb[1] = 0xffffffffu;
+        return 2;
+    }
+    wa[0] = (uint32_t)zlo; wb[0] = (uint32_t)zhi;
+    return 1;
+}
+
+// One warp per cluster; lanes take candidate j slots, each lane tests its j against the 8 i
+// atoms. The decision per (i, j) is the pinned FP32 criterion (pair_r2_rn < cs^2). It is
+// evaluated exactly only where it could go either way: every candidate is first placed in the
+// cluster's relative float frame (one conversion per coordinate per j). Both that r^2 and the
+// pinned one are within a few ulp per coordinate of the exact value: with R a bound on the
+// frame coordinates of any candidate (cluster extent + 2 cs + 2 column widths), the two differ
+// by at most 2 sqrt(3) cs (R 2^-21) + cs^2 2^-20 near cs^2; outside ten times that band the
+// frame's answer is the pinned answer. Clusters flagged exact (the frame may not be the minimum
+// image) use the pinned test on every pair. The z window of each column shrinks with the xy gap
+// between the cluster's column and that column.
+#define SB_SEARCH_WARPS 4
+__global__ void __launch_bounds__(32 * SB_SEARCH_WARPS) k_search(
     SearchParams P, const int* __restrict__ col_start, const int* __restrict__ col_count,
     const uint32_t* __restrict__ slot_u, const int* __restrict__ slot_atom,
     const int* __restrict__ excl_lo, const int* __restrict__ excl_hi,
@@ -252,85 +288,103 @@ __global__ void __launch_bounds__(128) k_search(
     const int* __restrict__ zbin,
     int* __restrict__ cl_count, uint32_t* __restrict__ cl_ent, int* __restrict__ meta,
     const int* __restrict__ refresh_flag) {
+    // per-warp copy of the cluster's atoms for the rarely taken per-slot paths (dynamic index)
+    __shared__ int s_ia[SB_SEARCH_WARPS][SB_CLUSTER], s_lo[SB_SEARCH_WARPS][SB_CLUSTER],
+        s_hi[SB_SEARCH_WARPS][SB_CLUSTER];
+    __shared__ uint32_t s_u[SB_SEARCH_WARPS][SB_CLUSTER], s_v[SB_SEARCH_WARPS][SB_CLUSTER],
+        s_w[SB_SEARCH_WARPS][SB_CLUSTER];
+    __shared__ float4 s_r[SB_SEARCH_WARPS][SB_CLUSTER];
+    extern __shared__ int s_ranges[];  // per warp: max_ranges starts, max_ranges + 1 prefixes
     if (refresh_flag && refresh_flag[0] == 0) return;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (c >= meta[0]) return;
     const uint32_t* __restrict__ UX = slot_u;
     const uint32_t* __restrict__ UY = slot_u + P.slot_cap;
     const uint32_t* __restrict__ UZ = slot_u + 2 * P.slot_cap;
     const int base = c * SB_CLUSTER;
-    // cluster atoms (lanes 0..7 load, all lanes receive)
-    int my_atom = lane < SB_CLUSTER ? slot_atom[base + lane] : -1;
-    uint32_t my_u = lane < SB_CLUSTER ? UX[base + lane] : 0;
-    uint32_t my_v = lane < SB_CLUSTER ? UY[base + lane] : 0;
-    uint32_t my_w = lane < SB_CLUSTER ? UZ[base + lane] : 0;
-    int ia[SB_CLUSTER];
-    uint32_t iu[SB_CLUSTER], iv[SB_CLUSTER], iw[SB_CLUSTER];
-#pragma unroll
-    for (int k = 0; k < SB_CLUSTER; k++) {
-        ia[k] = __shfl_sync(0xffffffffu, my_atom, k);
-        iu[k] = __shfl_sync(0xffffffffu, my_u, k);
-        iv[k] = __shfl_sync(0xffffffffu, my_v, k);
-        iw[k] = __shfl_sync(0xffffffffu, my_w, k);
+    // cluster atoms: lanes 0..7 load; register copies of the relative frame for all lanes
+    const int my_atom = lane < SB_CLUSTER ? slot_atom[base + lane] : -1;
+    const uint32_t my_u = lane < SB_CLUSTER ? UX[base + lane] : 0;
+    const uint32_t my_v = lane < SB_CLUSTER ? UY[base + lane] : 0;
+    const uint32_t my_w = lane < SB_CLUSTER ? UZ[base + lane] : 0;
+    if (lane < SB_CLUSTER) {
+        s_ia[wid][lane] = my_atom;
+        s_lo[wid][lane] = my_atom >= 0 ? excl_lo[my_atom] : INT_MAX;
+        s_hi[wid][lane] = my_atom >= 0 ? excl_hi[my_atom] : -1;
+        s_u[wid][lane] = my_u;
+        s_v[wid][lane] = my_v;
+        s_w[wid][lane] = my_w;
     }
+    __syncwarp();
+    const uint32_t u0 = __shfl_sync(0xffffffffu, my_u, 0);
+    const uint32_t v0 = __shfl_sync(0xffffffffu, my_v, 0);
+    const uint32_t w0 = __shfl_sync(0xffffffffu, my_w, 0);
     // z extent of the real atoms (sorted ascending in z inside the cluster)
-    uint32_t zmin = iw[0], zmax = iw[0];
+    const unsigned real = __ballot_sync(0xffffffffu, my_atom >= 0) & 0xffu;
+    const uint32_t zmin = w0;
+    const uint32_t zmax = __shfl_sync(0xffffffffu, my_w, 31 - __clz(real));
+    // relative float frame of the cluster (origin: its first atom)
+    const float mxr = __int2float_rn((int)(my_u - u0)) * P.sx;
+    const float myr = __int2float_rn((int)(my_v - v0)) * P.sy;
+    const float mzr = __int2float_rn((int)(my_w - w0)) * P.sz;
+    float ex = (lane < SB_CLUSTER && my_atom >= 0) ? fmaxf(fabsf(mxr), 0.f) : 0.f;
+    float ey = (lane < SB_CLUSTER && my_atom >= 0) ? fabsf(myr) : 0.f;
+    float ez = (lane < SB_CLUSTER && my_atom >= 0) ? fabsf(mzr) : 0.f;
 #pragma unroll
-    for (int k = 1; k < SB_CLUSTER; k++)
-        if (ia[k] >= 0) zmax = iw[k];
+    for (int o = 4; o >= 1; o >>= 1) {
+        ex = fmaxf(ex, __shfl_xor_sync(0xffffffffu, ex, o));
+        ey = fmaxf(ey, __shfl_xor_sync(0xffffffffu, ey, o));
+        ez = fmaxf(ez, __shfl_xor_sync(0xffffffffu, ez, o));
+    }
+    ex = __shfl_sync(0xffffffffu, ex, 0);
+    ey = __shfl_sync(0xffffffffu, ey, 0);
+    ez = __shfl_sync(0xffffffffu, ez, 0);
+    if (lane < SB_CLUSTER) s_r[wid][lane] = make_float4(mxr, myr, mzr, 0.f);
+    __syncwarp();
     // exact-path flag: the cluster-relative float frame of the pair kernel is a faithful
     // minimum image only while cs + (extent of the cluster from its first atom) < L/2
-    float ex = 0.f, ey = 0.f, ez = 0.f;
-#pragma unroll
-    for (int k = 1; k < SB_CLUSTER; k++)
-        if (ia[k] >= 0) {
-            ex = fmaxf(ex, fabsf(__int2float_rn((int)(iu[k] - iu[0])) * P.sx));
-            ey = fmaxf(ey, fabsf(__int2float_rn((int)(iv[k] - iv[0])) * P.sy));
-            ez = fmaxf(ez, fabsf(__int2float_rn((int)(iw[k] - iw[0])) * P.sz));
-        }
     const int exact = (ex + P.cs >= 0.49f * P.lx) || (ey + P.cs >= 0.49f * P.ly) ||
                       (ez + P.cs >= 0.49f * P.lz);
+    const float R = fmaxf(ex, fmaxf(ey, ez)) + 2.f * P.cs + 2.f * P.colw;
+    const float band = 10.f * (3.5f * P.cs * R * 4.8e-7f + P.cs2 * 9.6e-7f);
+    const float cs2_lo = P.cs2 - band, cs2_hi = P.cs2 + band;
     // own column from the first atom
-    const int cx = (int)(((unsigned long long)iu[0] * (unsigned)P.ncx) >> 32);
-    const int cy = (int)(((unsigned long long)iv[0] * (unsigned)P.ncy) >> 32);
+    const int cx = (int)(((unsigned long long)u0 * (unsigned)P.ncx) >> 32);
+    const int cy = (int)(((unsigned long long)v0 * (unsigned)P.ncy) >> 32);
     const int col = cy * P.ncx + cx;
-    int count = 0;
-    uint32_t* out = cl_ent + (size_t)c * P.ent_cap;
+    // candidate ranges: the lanes take the (dy, dx) columns of the half shell in parallel, each
+    // giving up to two slot ranges (its z window, wrapped); r = 2 (column index) + window keeps
+    // the order of a sequential walk (dy outer, dx inner, window), so the entries come out in
+    // that order. rs[r] = first slot, rp[r] = exclusive prefix of the range lengths.
     const int dy0 = P.fully ? 0 : -P.nyr, dy1 = P.fully ? P.ncy - 1 : P.nyr;
     const int dx0 = P.fullx ? 0 : -P.nxr, dx1 = P.fullx ? P.ncx - 1 : P.nxr;
-    // z window [zmin - rz, zmax + rz] with periodic wrap
-    long long zlo = (long long)zmin - (long long)P.rz;
-    long long zhi = (long long)zmax + (long long)P.rz;
-    int nwin;
-    uint32_t wa[2], wb[2];  // inclusive windows
-    if (zhi - zlo >= 4294967296ll) {
-        nwin = 1; wa[0] = 0; wb[0] = 0xffffffffu;
-    } else if (zlo < 0) {
-        nwin = 2; wa[0] = 0; wb[0] = (uint32_t)zhi; wa[1] = (uint32_t)(zlo + 4294967296ll); wb[1] = 0xffffffffu;
-    } else if (zhi > 0xffffffffll) {
-        nwin = 2; wa[0] = 0; wb[0] = (uint32_t)(zhi - 4294967296ll); wa[1] = (uint32_t)zlo; wb[1] = 0xffffffffu;
-    } else {
-        nwin = 1; wa[0] = (uint32_t)zlo; wb[0] = (uint32_t)zhi;
-    }
-    for (int dy = dy0; dy <= dy1; dy++) {
-        int cy2, ady;
-        if (P.fully) {
-            cy2 = dy;
-            int d = abs(cy2 - cy);
-            ady = min(d, P.ncy - d);
-        } else {
-            cy2 = cy + dy;
-            if (cy2 < 0) cy2 += P.ncy;
-            if (cy2 >= P.ncy) cy2 -= P.ncy;
-            ady = abs(dy);
-        }
-        float gy = fmaxf(0.f, (float)(ady - 1)) * P.colwy;
-        for (int dx = dx0; dx <= dx1; dx++) {
-            int cx2, adx;
+    const int nxw = dx1 - dx0 + 1;
+    const int ncols = (dy1 - dy0 + 1) * nxw;
+    int* rs = s_ranges + wid * (2 * P.max_ranges + 1);
+    int* rp = rs + P.max_ranges;  // max_ranges + 1 entries
+    const int nr = 2 * ncols;
+    int carry = 0;
+    for (int q0 = 0; q0 < ncols; q0 += 16) {
+        // 16 columns per round: lane l handles column q0 + l/2, window l&1
+        const int q = q0 + (lane >> 1), w = lane & 1;
+        int ra = 0, len = 0;
+        if (q < ncols) {
+            const int dy = dy0 + q / nxw, dx = dx0 + q % nxw;
+            int cy2, ady, cx2, adx;
+            if (P.fully) {
+                cy2 = dy;
+                const int d = abs(cy2 - cy);
+                ady = min(d, P.ncy - d);
+            } else {
+                cy2 = cy + dy;
+                if (cy2 < 0) cy2 += P.ncy;
+                if (cy2 >= P.ncy) cy2 -= P.ncy;
+                ady = abs(dy);
+            }
             if (P.fullx) {
                 cx2 = dx;
-                int d = abs(cx2 - cx);
+                const int d = abs(cx2 - cx);
                 adx = min(d, P.ncx - d);
             } else {
                 cx2 = cx + dx;
@@ -338,48 +392,108 @@ __global__ void __launch_bounds__(128) k_search(
                 if (cx2 >= P.ncx) cx2 -= P.ncx;
                 adx = abs(dx);
             }
-            int col2 = cy2 * P.ncx + cx2;
-            if (col2 < col) continue;  // every slot of an earlier column precedes this cluster
-            float gx = fmaxf(0.f, (float)(adx - 1)) * P.colwx;
-            if (gx * gx + gy * gy >= P.cs2) continue;
-            int s0 = col_start[col2];
-            int s1 = s0 + col_count[col2];
-            for (int w = 0; w < nwin; w++) {
-                // candidate range from the column's z-bin index: a superset of the z window
-                // (whole bins); the exact pair test filters
-                const int* zb = zbin + (size_t)col2 * (SB_ZBINS + 1);
-                int a = max(zb[wa[w] >> SB_ZBIN_SHIFT], s0);
-                int b = min(zb[(wb[w] >> SB_ZBIN_SHIFT) + 1], s1);
-                if (col2 == col) a = max(a, base + 1);
-                for (int j0 = a; j0 < b; j0 += 32) {
-                    int j = j0 + lane;
-                    unsigned mask = 0;
-                    if (j < b) {
-                        uint32_t ju = UX[j], jv = UY[j], jw = UZ[j];
-                        int ja = slot_atom[j];
-#pragma unroll
-                        for (int k = 0; k < SB_CLUSTER; k++) {
-                            if (ia[k] >= 0 && base + k < j) {
-                                float r2 = pair_r2_rn(iu[k], iv[k], iw[k], ju, jv, jw, P.sx,
-                                                      P.sy, P.sz);
-                                if (r2 < P.cs2 &&
-                                    !excluded_pair(ia[k], ja, excl_lo, excl_hi, es, en, el))
-                                    mask |= 1u << k;
-                            }
-                        }
-                    }
-                    unsigned bal = __ballot_sync(0xffffffffu, mask != 0);
-                    int pos = count + __popc(bal & ((1u << lane) - 1u));
-                    if (mask != 0) {
-                        if (pos < P.ent_cap)
-                            out[pos] = (uint32_t)j | (mask << 24);
-                        else
-                            atomicOr(&meta[1], SB_STATUS_LIST_OVERFLOW);
-                    }
-                    count += __popc(bal);
+            const int col2 = cy2 * P.ncx + cx2;
+            const float gy = fmaxf(0.f, (float)(ady - 1)) * P.colwy;
+            const float gx = fmaxf(0.f, (float)(adx - 1)) * P.colwx;
+            const float g2 = gx * gx + gy * gy;
+            // earlier columns precede this cluster in slot order; columns beyond cs are skipped
+            if (col2 >= col && g2 < P.cs2) {
+                // z reach in this column: sqrt(cs^2 - (xy gap)^2), widened for rounding
+                const float rzA = sqrtf(P.cs2 - g2) * 1.001f + 1e-3f;
+                const unsigned long long rz =
+                    (unsigned long long)((double)rzA * (double)P.zscale) + 1024ull;
+                uint32_t wa[2], wb[2];
+                const int nwin = z_windows(zmin, zmax, rz, wa, wb);
+                if (w < nwin) {
+                    const int s0 = col_start[col2];
+                    const int s1 = s0 + col_count[col2];
+                    // a superset of the z window (whole bins); the pair test filters
+                    const int* zb = zbin + (size_t)col2 * (SB_ZBINS + 1);
+                    int lo = max(zb[(w ? wa[1] : wa[0]) >> SB_ZBIN_SHIFT], s0);
+                    const int hi = min(zb[((w ? wb[1] : wb[0]) >> SB_ZBIN_SHIFT) + 1], s1);
+                    if (col2 == col) lo = max(lo, base + 1);
+                    ra = lo;
+                    len = max(hi - lo, 0);
                 }
             }
         }
+        // exclusive scan of the lengths over the warp, continuing the running carry
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int r = 2 * q0 + lane;
+        if (r < nr) {
+            rs[r] = ra;
+            rp[r] = carry + incl - len;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) rp[nr] = carry;
+    __syncwarp();
+    const int total = carry;
+    int count = 0;
+    uint32_t* out = cl_ent + (size_t)c * P.ent_cap;
+    int r = 0;  // this lane's current range (advances monotonically)
+    for (int t0 = 0; t0 < total; t0 += 32) {
+        const int t = t0 + lane;
+        unsigned mask = 0;
+        if (t < total) {
+            while (rp[r + 1] <= t) r++;
+            const int j = rs[r] + (t - rp[r]);
+            const uint32_t ju = UX[j], jv = UY[j], jw = UZ[j];
+            unsigned near = 0, border = 0xffu;
+            if (!exact) {
+                const float xj = __int2float_rn((int)(ju - u0)) * P.sx;
+                const float yj = __int2float_rn((int)(jv - v0)) * P.sy;
+                const float zj = __int2float_rn((int)(jw - w0)) * P.sz;
+                unsigned notfar = 0;
+#pragma unroll
+                for (int k = 0; k < SB_CLUSTER; k++) {
+                    const float4 rk = s_r[wid][k];
+                    const float ddx = xj - rk.x, ddy = yj - rk.y, ddz = zj - rk.z;
+                    const float r2a = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+                    near |= (r2a < cs2_lo ? 1u : 0u) << k;
+                    notfar |= (r2a <= cs2_hi ? 1u : 0u) << k;
+                }
+                border = notfar & ~near;
+            }
+            // slots the frame cannot decide: the pinned test itself
+            while (border) {
+                const int k = __ffs(border) - 1;
+                border &= border - 1u;
+                if (pair_r2_rn(s_u[wid][k], s_v[wid][k], s_w[wid][k], ju, jv, jw, P.sx, P.sy,
+                               P.sz) < P.cs2)
+                    near |= 1u << k;
+            }
+            // slots in range: padding, slot order and exclusions
+            if (near) {
+                const int ja = slot_atom[j];
+                const int jlo = ja >= 0 ? excl_lo[ja] : INT_MAX;
+                const int jhi = ja >= 0 ? excl_hi[ja] : -1;
+                while (near) {
+                    const int k = __ffs(near) - 1;
+                    near &= near - 1u;
+                    const int ak = s_ia[wid][k];
+                    if (ak >= 0 && base + k < j &&
+                        !excluded_pair(ak, ja, s_lo[wid][k], s_hi[wid][k], jlo, jhi, es, en,
+                                       el))
+                        mask |= 1u << k;
+                }
+            }
+            if (mask != 0) mask |= (unsigned)j << 8;  // carry j for the store below
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, mask != 0);
+        const int pos = count + __popc(bal & ((1u << lane) - 1u));
+        if (mask != 0) {
+            if (pos < P.ent_cap)
+                out[pos] = (mask >> 8) | ((mask & 0xffu) << 24);
+            else
+                atomicOr(&meta[1], SB_STATUS_LIST_OVERFLOW);
+        }
+        count += __popc(bal);
     }
     if (lane == 0) cl_count[c] = min(count, P.ent_cap) | (exact ? SB_CL_EXACT : 0);
 }
@@ -681,14 +795,27 @@ static int nl_rebuild(sb_neighbor_list* nl, float* d_crd, const int* es, const i
     P.lz = nl->box[2];
     P.colwx = nl->box[0] / nl->ncx;
     P.colwy = nl->box[1] / nl->ncy;
-    // z half-width: cs / (Lz 2^-32), rounded up with margin (the exact test is per pair)
-    double rz = ceil((double)nl->cs / ((double)nl->box[2] / 4294967296.0)) + 1024.0;
-    P.rz = rz > 8.0e9 ? 8000000000ull : (unsigned long long)rz;
+    // fixed-point units per A along z (the z windows are sized per column in the kernel)
+    P.zscale = (float)(4294967296.0 / (double)nl->box[2]);
+    P.colw = std::max(P.colwx, P.colwy);
     P.slot_cap = nl->slot_cap;
     P.ent_cap = nl->ent_cap;
-    int warps_per_block = 4;
-    int blocks = (nl->clu_cap + warps_per_block - 1) / warps_per_block;
-    k_search<<<blocks, 32 * warps_per_block, 0, s>>>(
+    {
+        const int nyw = P.fully ? P.ncy : 2 * P.nyr + 1, nxw = P.fullx ? P.ncx : 2 * P.nxr + 1;
+        P.max_ranges = 2 * nyw * nxw;
+    }
+    const size_t search_smem = sizeof(int) * SB_SEARCH_WARPS * (2 * (size_t)P.max_ranges + 1);
+    if (search_smem > 200 * 1024) {
+        sb_set_error("neighbor search: %d column ranges per cluster exceed shared memory",
+                     P.max_ranges);
+        return SB_ERR_ARG;
+    }
+    if (search_smem > 48 * 1024)
+        cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)search_smem);
+    const int warps_per_block = SB_SEARCH_WARPS;
+    const int blocks = (nl->clu_cap + warps_per_block - 1) / warps_per_block;
+    k_search<<<blocks, 32 * warps_per_block, search_smem, s>>>(
         P, nl->col_start, nl->col_count, nl->slot_u, nl->slot_atom, nl->excl_lo, nl->excl_hi,
         es, en, el, nl->zbin, nl->cl_count, nl->cl_ent, nl->meta, dflag);
     SB_CHECK_LAUNCH();
