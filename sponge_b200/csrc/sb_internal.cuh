@@ -236,8 +236,9 @@ int sb_lj_fused_pair(sb_lennard_jones* lj, sb_neighbor_list* nl, float pme_beta,
                      int need_atom_energy, float* d_atom_energy, int need_virial,
                      float* d_atom_lj_virial, float* d_atom_direct_pme_energy, cudaStream_t s);
 // reciprocal part in two pieces: the grid chain (spread of the packed slots, FFT, convolution,
-// inverse FFT into d_theta) and the finish (gather + fixed-point finalisation into d_frc, energy
-// and virial sums), which must follow the pair and exclusion kernels
+// inverse FFT into d_theta, gather of the slot forces into the list's fixed-point buffer) and
+// the finish (finalisation of that buffer into d_frc, energy and virial sums), which must follow
+// the pair and exclusion kernels
 int sb_pme_fused_grid(sb_pme* pme, sb_neighbor_list* nl, int want_energy, cudaStream_t s);
 int sb_pme_fused_finish(sb_pme* pme, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
                         int need_virial, int need_energy, float* d_virial, float* d_potential,

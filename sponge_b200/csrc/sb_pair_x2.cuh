@@ -94,8 +94,8 @@ __device__ __forceinline__ void pair_walk_x2(
                 dz = f2add(zj2, nz[p]);
             }
             const float2 r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
-            const bool a0 = ((m >> (2 * p)) & 1u) && r2.x < rc2.x;
-            const bool a1 = ((m >> (2 * p + 1)) & 1u) && r2.y < rc2.y;
+            const bool a0 = (m & (1u << (2 * p))) != 0u && r2.x < rc2.x;
+            const bool a1 = (m & (2u << (2 * p))) != 0u && r2.y < rc2.y;
             // evaluated on every slot and discarded by a select where inactive
             const float2 ri = make_float2(sb_rsqrt(r2.x), sb_rsqrt(r2.y));
             const float2 ri2 = f2mul(ri, ri);
@@ -132,11 +132,11 @@ __device__ __forceinline__ void pair_walk_x2(
                 }
             }
         }
-        const float fjx = -(gx.x + gx.y), fjy = -(gy.x + gy.y), fjz = -(gz.x + gz.y);
-        if (valid && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
-            red_fix(&fix[j], fjx);
-            red_fix(&fix[P.slot_cap + j], fjy);
-            red_fix(&fix[2 * P.slot_cap + j], fjz);
+        // red_fix skips components that round to zero, so no test of the sums is needed here
+        if (valid) {
+            red_fix(&fix[j], -(gx.x + gx.y));
+            red_fix(&fix[P.slot_cap + j], -(gy.x + gy.y));
+            red_fix(&fix[2 * P.slot_cap + j], -(gz.x + gz.y));
         }
     }
 }
@@ -205,41 +205,53 @@ __global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
         pair_walk_x2<EV, false>(P, cnt, ents, xq, stype, ctab, fix, base, lane, rx, ry, rz, nx,
                                 ny, nz, nq, fx, fy, fz, ei, vi, di);
 
-    // reduce each i atom's sums over the 32 lanes; lane 0 ends with the totals
-    float fxi[8], fyi[8], fzi[8];
+    // i forces: transpose-reduce the 24 per-lane sums (x, y, z of 8 atoms, padded to 32) over the
+    // warp; each of the 5 steps halves the values a lane holds, after which lane l holds the
+    // total of value l (component l / 8 of cluster slot l % 8): 31 shuffles instead of 120
+    float v[32];
 #pragma unroll
     for (int p = 0; p < 4; p++) {
-        fxi[2 * p] = fx[p].x, fxi[2 * p + 1] = fx[p].y;
-        fyi[2 * p] = fy[p].x, fyi[2 * p + 1] = fy[p].y;
-        fzi[2 * p] = fz[p].x, fzi[2 * p + 1] = fz[p].y;
+        v[2 * p] = fx[p].x, v[2 * p + 1] = fx[p].y;
+        v[8 + 2 * p] = fy[p].x, v[9 + 2 * p] = fy[p].y;
+        v[16 + 2 * p] = fz[p].x, v[17 + 2 * p] = fz[p].y;
     }
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
+    for (int k = 24; k < 32; k++) v[k] = 0.f;
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            fxi[k] += __shfl_xor_sync(0xffffffffu, fxi[k], o);
-            fyi[k] += __shfl_xor_sync(0xffffffffu, fyi[k], o);
-            fzi[k] += __shfl_xor_sync(0xffffffffu, fzi[k], o);
-            if (EV) {
+    for (int o = 16, n = 16; o >= 1; o >>= 1, n >>= 1) {
+        const bool upper = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < n; k++) {
+            const float send = upper ? v[k] : v[k + n];
+            const float keep = upper ? v[k + n] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    if (lane < 24) {
+        const int k = lane & 7, comp = lane >> 3;
+        if (slot_atom[base + k] >= 0) red_fix(&fix[(size_t)comp * P.slot_cap + base + k], v[0]);
+    }
+    if (EV) {
+        // energy and virial terms (energy/virial steps only): butterfly sums, lane 0 writes
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) {
                 ei[k] += __shfl_xor_sync(0xffffffffu, ei[k], o);
                 vi[k] += __shfl_xor_sync(0xffffffffu, vi[k], o);
                 di[k] += __shfl_xor_sync(0xffffffffu, di[k], o);
             }
         }
-    }
-    if (lane == 0) {
+        if (lane == 0) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int s = base + k;
-            const int a = slot_atom[s];
-            if (a >= 0) {
-                red_fix(&fix[s], fxi[k]);
-                red_fix(&fix[P.slot_cap + s], fyi[k]);
-                red_fix(&fix[2 * P.slot_cap + s], fzi[k]);
-                if (EV & SB_EV_ENERGY) atom_energy[a] += ei[k];
-                if (EV & SB_EV_VIRIAL) {
-                    atom_virial[a] += vi[k];
-                    atom_direct[a] = di[k];
+            for (int k = 0; k < 8; k++) {
+                const int a = slot_atom[base + k];
+                if (a >= 0) {
+                    if (EV & SB_EV_ENERGY) atom_energy[a] += ei[k];
+                    if (EV & SB_EV_VIRIAL) {
+                        atom_virial[a] += vi[k];
+                        atom_direct[a] = di[k];
+                    }
                 }
             }
         }

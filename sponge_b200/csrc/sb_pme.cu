@@ -839,71 +839,63 @@ __global__ void k_spread_slot(const int* __restrict__ meta, const uint4* __restr
     }
 }
 
-// reciprocal force gather per slot, fused with the conversion of the slot's fixed-point
-// accumulators (pair + exclusion forces) into the caller's float forces; clears the buffer
-__global__ void k_gather_finalize(const int* __restrict__ meta, const int* __restrict__ slot_atom,
-                                  const uint4* __restrict__ xq, const float* __restrict__ theta,
-                                  int K0, int K1, int K2, float ix, float iy, float iz,
-                                  long long* __restrict__ fix, int slot_cap,
-                                  float* __restrict__ frc) {
+// reciprocal force gather per slot into the list's slot-order fixed-point accumulators (the
+// buffer the pair and exclusion kernels add to, possibly at the same time: integer adds commute)
+__global__ void k_gather_slot(const int* __restrict__ meta, const uint4* __restrict__ xq,
+                              const float* __restrict__ theta, int K0, int K1, int K2, float ix,
+                              float iy, float iz, long long* __restrict__ fix, int slot_cap) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     if (sl >= meta[3]) return;
-    const long long ax = fix[sl], ay = fix[slot_cap + sl], az = fix[2 * slot_cap + sl];
-    if (ax | ay | az) {
-        fix[sl] = 0;
-        fix[slot_cap + sl] = 0;
-        fix[2 * slot_cap + sl] = 0;
-    }
-    const int a = slot_atom[sl];
-    if (a < 0) return;
     const uint4 v = xq[sl];
-    const float q = __uint_as_float(v.w);
+    const float q = __uint_as_float(v.w);  // padding slots carry charge 0
+    if (q == 0.f) return;
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(v.x, K0, b0, f0);
+    grid_coord(v.y, K1, b1, f1);
+    grid_coord(v.z, K2, b2, f2);
+    float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    bspline4d(f0, dx);
+    bspline4d(f1, dy);
+    bspline4d(f2, dz);
+    int gz[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int g = b2 - k;
+        gz[k] = g < 0 ? g + K2 : g;
+    }
     float Fx = 0.f, Fy = 0.f, Fz = 0.f;
-    if (q != 0.f) {
-        int b0, b1, b2;
-        float f0, f1, f2;
-        grid_coord(v.x, K0, b0, f0);
-        grid_coord(v.y, K1, b1, f1);
-        grid_coord(v.z, K2, b2, f2);
-        float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
-        bspline4(f0, wx);
-        bspline4(f1, wy);
-        bspline4(f2, wz);
-        bspline4d(f0, dx);
-        bspline4d(f1, dy);
-        bspline4d(f2, dz);
-        int gz[4];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int g = b2 - k;
-            gz[k] = g < 0 ? g + K2 : g;
-        }
+    for (int kx = 0; kx < 4; kx++) {
+        int gx = b0 - kx;
+        if (gx < 0) gx += K0;
 #pragma unroll
-        for (int kx = 0; kx < 4; kx++) {
-            int gx = b0 - kx;
-            if (gx < 0) gx += K0;
+        for (int ky = 0; ky < 4; ky++) {
+            int gy = b1 - ky;
+            if (gy < 0) gy += K1;
+            const float* row = theta + ((size_t)gx * K1 + gy) * K2;
+            float sw = 0.f, sd = 0.f;
 #pragma unroll
-            for (int ky = 0; ky < 4; ky++) {
-                int gy = b1 - ky;
-                if (gy < 0) gy += K1;
-                const float* row = theta + ((size_t)gx * K1 + gy) * K2;
-                float sw = 0.f, sd = 0.f;
-#pragma unroll
-                for (int kz = 0; kz < 4; kz++) {
-                    const float t = row[gz[kz]];
-                    sw = fmaf(t, wz[kz], sw);
-                    sd = fmaf(t, dz[kz], sd);
-                }
-                Fx = fmaf(dx[kx] * wy[ky], sw, Fx);
-                Fy = fmaf(wx[kx] * dy[ky], sw, Fy);
-                Fz = fmaf(wx[kx] * wy[ky], sd, Fz);
+            for (int kz = 0; kz < 4; kz++) {
+                const float t = row[gz[kz]];
+                sw = fmaf(t, wz[kz], sw);
+                sd = fmaf(t, dz[kz], sd);
             }
+            Fx = fmaf(dx[kx] * wy[ky], sw, Fx);
+            Fy = fmaf(wx[kx] * dy[ky], sw, Fy);
+            Fz = fmaf(wx[kx] * wy[ky], sd, Fz);
         }
     }
     const float sq = -q;
-    frc[3 * a] += (float)((double)ax * SB_FORCE_UNSCALE) + sq * Fx * ix;
-    frc[3 * a + 1] += (float)((double)ay * SB_FORCE_UNSCALE) + sq * Fy * iy;
-    frc[3 * a + 2] += (float)((double)az * SB_FORCE_UNSCALE) + sq * Fz * iz;
+    const long long fx = __float2ll_rn(sq * Fx * ix * SB_FORCE_SCALE);
+    const long long fy = __float2ll_rn(sq * Fy * iy * SB_FORCE_SCALE);
+    const long long fz = __float2ll_rn(sq * Fz * iz * SB_FORCE_SCALE);
+    atomicAdd((unsigned long long*)&fix[sl], (unsigned long long)fx);
+    atomicAdd((unsigned long long*)&fix[slot_cap + sl], (unsigned long long)fy);
+    atomicAdd((unsigned long long*)&fix[2 * slot_cap + sl], (unsigned long long)fz);
 }
 
 int sb_pme_fused_excluded(sb_pme* p, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
@@ -933,17 +925,18 @@ int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStre
     SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
     SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_energy, s,
                              &p->rec_nparts));
-    return sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s);
+    SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+    k_gather_slot<<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
+        nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0], (float)K1 / p->box[1],
+        (float)K2 / p->box[2], nl->fix, nl->slot_cap);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
 }
 
 int sb_pme_fused_finish(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
                         int need_virial, int need_energy, float* d_virial, float* d_potential,
                         cudaStream_t s) {
-    const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
-    k_gather_finalize<<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
-        nl->meta, nl->slot_atom, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
-        (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, d_frc);
-    SB_CHECK_LAUNCH();
+    SB_TRY(sb_nl_finalize_forces(nl, d_frc, s));
     if (need_virial > 0 || need_energy > 0) {
         k_pme_energy_finish<<<1, 1024, 0, s>>>(p->n, d_charge, p->d_epart, p->rec_nparts,
                                                p->d_direct_atom_energy,
