@@ -279,6 +279,8 @@ def main():
     ap.add_argument("--form", default="fixed", choices=["fixed", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--pair-shape", type=int, default=0, choices=[0, 1, 2, 4, 8],
+                    help="pair-kernel shape (sb_lj_set_kernel_variant); 0 = pick by timing")
     ap.add_argument("--workload", default="solvated96k", choices=["solvated96k", "fep48"],
                     help="fep48: the 48 batched FEP/TI lambda windows (parity case, reported "
                          "separately from the headline line)")
@@ -309,9 +311,15 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     eng.update_list(forced=1)
     eng.to_uint()
-    # autotuner: time each pair-kernel shape on this list and keep the fastest
-    pair_shape = eng.lj.tune(eng.nl, eng.uint_crd, eng.charge, eng.pme.beta) \
-        if form == FORM_FIXED else None
+    # autotuner: time each pair-kernel shape on this list and keep the fastest (or the shape
+    # given on the command line, e.g. for a profiler run, whose timings would mislead the tuner)
+    pair_shape = None
+    if form == FORM_FIXED:
+        if args.pair_shape:
+            eng.lj.set_kernel_variant(args.pair_shape)
+            pair_shape = args.pair_shape
+        else:
+            pair_shape = eng.lj.tune(eng.nl, eng.uint_crd, eng.charge, eng.pme.beta)
 
     if form == FORM_FIXED:
         # the force part is a fixed launch sequence: captured once, replayed every step after

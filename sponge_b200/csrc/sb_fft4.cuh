@@ -148,30 +148,44 @@ struct F4 {
     static constexpr int T = N1 > N2 ? N1 : N2;  // threads per line
 };
 
+// Global loads and stores of the passes run as unrolled loops with a compile-time trip count
+// (the tile divides evenly among the threads), so that a thread issues all of its loads before
+// the first use and one memory latency covers the tile.
+
 template <int N1, int N2, bool INV>
 __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_ypass4(
     const float2* __restrict__ twy, float2* __restrict__ spec, int K0, int H) {
-    constexpr int K1 = N1 * N2, NL = SB_F4_NL;
+    constexpr int K1 = N1 * N2, NL = SB_F4_NL, NT = NL * F4<N1, N2>::T, IT = K1 * NL / NT;
+    static_assert(K1 * NL % NT == 0, "tile must divide among the threads");
     __shared__ float2 tw[K1];
     __shared__ float2 D[K1 * NL];
     __shared__ long long cbase[NL];
     const int nlines = K0 * H;
     const int l0 = blockIdx.x * NL;
-    for (int t = threadIdx.x; t < K1; t += blockDim.x) tw[t] = twy[t];
+    for (int t = threadIdx.x; t < K1; t += NT) tw[t] = twy[t];
     if (threadIdx.x < NL) {
         const int l = l0 + threadIdx.x;
         const int x = l / H, kz = l - x * H;
         cbase[threadIdx.x] = l < nlines ? (long long)x * K1 * H + kz : -1;
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < K1 * NL; t += blockDim.x) {
-        const int p = t / NL, c = t - p * NL;
-        const long long cb = cbase[c];
-        D[t] = cb >= 0 ? spec[cb + (size_t)p * H] : make_float2(0.f, 0.f);
+    {
+        float2 r[IT];
+#pragma unroll
+        for (int i = 0; i < IT; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int p = t / NL, c = t - p * NL;
+            const long long cb = cbase[c];
+            r[i] = cb >= 0 ? spec[cb + (size_t)p * H] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < IT; i++) D[threadIdx.x + i * NT] = r[i];
     }
     __syncthreads();
     line_fft4<N1, N2, NL, INV>(D, 1, NL, tw);
-    for (int t = threadIdx.x; t < K1 * NL; t += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < IT; i++) {
+        const int t = threadIdx.x + i * NT;
         const int p = t / NL, c = t - p * NL;
         const long long cb = cbase[c];
         if (cb >= 0) spec[cb + (size_t)p * H] = D[t];
@@ -182,14 +196,15 @@ template <int N1, int N2>
 __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_xconv4(
     const float2* __restrict__ twx, float2* __restrict__ spec, const float* __restrict__ bc,
     double* __restrict__ epart, int K1, int H, int K2) {
-    constexpr int K0 = N1 * N2, NL = SB_F4_NL, NT = NL * F4<N1, N2>::T;
+    constexpr int K0 = N1 * N2, NL = SB_F4_NL, NT = NL * F4<N1, N2>::T, IT = K0 * NL / NT;
+    static_assert(K0 * NL % NT == 0, "tile must divide among the threads");
     __shared__ float2 tw[K0];
     __shared__ float2 D[K0 * NL];
     __shared__ int cbase[NL], ckz[NL];
     __shared__ double red[NT];
     const int nlines = K1 * H;
     const int l0 = blockIdx.x * NL;
-    for (int t = threadIdx.x; t < K0; t += blockDim.x) tw[t] = twx[t];
+    for (int t = threadIdx.x; t < K0; t += NT) tw[t] = twx[t];
     if (threadIdx.x < NL) {
         const int l = l0 + threadIdx.x;
         const int y = l / H, kz = l - y * H;
@@ -198,31 +213,43 @@ __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_xconv4(
     }
     __syncthreads();
     const size_t pstride = (size_t)K1 * H;
-    for (int t = threadIdx.x; t < K0 * NL; t += blockDim.x) {
-        const int p = t / NL, c = t - p * NL;
-        const int cb = cbase[c];
-        D[t] = cb >= 0 ? spec[(size_t)p * pstride + cb] : make_float2(0.f, 0.f);
+    // the Green's function values of this thread's points, loaded with the spectrum
+    float g[IT];
+    {
+        float2 r[IT];
+#pragma unroll
+        for (int i = 0; i < IT; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int p = t / NL, c = t - p * NL;
+            const int cb = cbase[c];
+            r[i] = cb >= 0 ? spec[(size_t)p * pstride + cb] : make_float2(0.f, 0.f);
+            g[i] = cb >= 0 ? bc[(size_t)p * pstride + cb] : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < IT; i++) D[threadIdx.x + i * NT] = r[i];
     }
     __syncthreads();
     line_fft4<N1, N2, NL, false>(D, 1, NL, tw);
     double e = 0.0;
-    for (int t = threadIdx.x; t < K0 * NL; t += blockDim.x) {
-        const int kx = t / NL, c = t - kx * NL;
-        const int cb = cbase[c];
-        if (cb >= 0) {
-            const float g = bc[(size_t)kx * pstride + cb];
+#pragma unroll
+    for (int i = 0; i < IT; i++) {
+        const int t = threadIdx.x + i * NT;
+        const int c = t % NL;
+        if (cbase[c] >= 0) {
             const float2 v = D[t];
             if (epart) {
                 const int kz = ckz[c];
                 const double w = (kz == 0 || 2 * kz == K2) ? 1.0 : 2.0;
-                e += w * (double)g * ((double)v.x * v.x + (double)v.y * v.y);
+                e += w * (double)g[i] * ((double)v.x * v.x + (double)v.y * v.y);
             }
-            D[t] = make_float2(v.x * g, v.y * g);
+            D[t] = make_float2(v.x * g[i], v.y * g[i]);
         }
     }
     __syncthreads();
     line_fft4<N1, N2, NL, true>(D, 1, NL, tw);
-    for (int t = threadIdx.x; t < K0 * NL; t += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < IT; i++) {
+        const int t = threadIdx.x + i * NT;
         const int p = t / NL, c = t - p * NL;
         const int cb = cbase[c];
         if (cb >= 0) spec[(size_t)p * pstride + cb] = D[t];
@@ -249,30 +276,38 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zfwd4(
     const float2* __restrict__ twz, const float2* __restrict__ post,
     long long* __restrict__ qfix, float2* __restrict__ spec, int nrows) {
     constexpr int M = N1 * N2, K2 = 2 * M, H = M + 1, NL = SB_F4_ZR;
+    constexpr int NT = NL * F4<N1, N2>::T, IT = NL * K2 / NT, ITO = (NL * H + NT - 1) / NT;
+    static_assert(NL * K2 % NT == 0, "tile must divide among the threads");
     __shared__ float2 tw[M], ps[M];
     __shared__ float2 D[NL * H];
     float* Df = reinterpret_cast<float*>(D);
-    for (int t = threadIdx.x; t < M; t += blockDim.x) {
+    for (int t = threadIdx.x; t < M; t += NT) {
         tw[t] = twz[t];
         ps[t] = post[t];
     }
     const int r0 = blockIdx.x * NL;
     const int nr = min(NL, nrows - r0);
     long long* q = qfix + (size_t)r0 * K2;
-    for (int t = threadIdx.x; t < NL * K2; t += blockDim.x) {
-        const int r = t / K2, col = t - r * K2;
-        long long v = 0;
-        if (r < nr) {
-            v = q[t];
-            if (v) q[t] = 0;
+    {
+        long long v[IT];
+#pragma unroll
+        for (int i = 0; i < IT; i++) {
+            const int t = threadIdx.x + i * NT;
+            v[i] = t < nr * K2 ? q[t] : 0ll;
         }
-        Df[2 * r * H + col] = (float)v * SB_GRID_UNSCALE;
+#pragma unroll
+        for (int i = 0; i < IT; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int r = t / K2, col = t - r * K2;
+            if (v[i]) q[t] = 0;  // the grid is left zero for the next spread
+            Df[2 * r * H + col] = (float)v[i] * SB_GRID_UNSCALE;
+        }
     }
     __syncthreads();
     line_fft4<N1, N2, NL, false>(D, H, 1, tw);
     // X[k] = E[k] + W_K2^k O[k], k = 0..M, from Z = FFT_M(x_even + i x_odd)
     constexpr int half = M / 2;
-    for (int t = threadIdx.x; t < NL * (half + 1); t += blockDim.x) {
+    for (int t = threadIdx.x; t < NL * (half + 1); t += NT) {
         const int k = t / NL, r = t - k * NL;
         float2* row = D + r * H;
         if (k == 0) {
@@ -298,7 +333,11 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zfwd4(
     }
     __syncthreads();
     float2* out = spec + (size_t)r0 * H;
-    for (int t = threadIdx.x; t < nr * H; t += blockDim.x) out[t] = D[t];
+#pragma unroll
+    for (int i = 0; i < ITO; i++) {
+        const int t = threadIdx.x + i * NT;
+        if (t < nr * H) out[t] = D[t];
+    }
 }
 
 // complex-to-real along z: half-spectrum rows -> real rows
@@ -307,22 +346,35 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zinv4(
     const float2* __restrict__ twz, const float2* __restrict__ post,
     const float2* __restrict__ spec, float* __restrict__ real, int nrows) {
     constexpr int M = N1 * N2, K2 = 2 * M, H = M + 1, NL = SB_F4_ZR;
+    constexpr int NT = NL * F4<N1, N2>::T, ITI = (NL * H + NT - 1) / NT, IT = NL * K2 / NT;
+    static_assert(NL * K2 % NT == 0, "tile must divide among the threads");
     __shared__ float2 tw[M], ps[M];
     __shared__ float2 D[NL * H];
     const float* Df = reinterpret_cast<const float*>(D);
-    for (int t = threadIdx.x; t < M; t += blockDim.x) {
+    for (int t = threadIdx.x; t < M; t += NT) {
         tw[t] = twz[t];
         ps[t] = post[t];
     }
     const int r0 = blockIdx.x * NL;
     const int nr = min(NL, nrows - r0);
     const float2* in = spec + (size_t)r0 * H;
-    for (int t = threadIdx.x; t < NL * H; t += blockDim.x)
-        D[t] = t < nr * H ? in[t] : make_float2(0.f, 0.f);
+    {
+        float2 r[ITI];
+#pragma unroll
+        for (int i = 0; i < ITI; i++) {
+            const int t = threadIdx.x + i * NT;
+            r[i] = t < nr * H ? in[t] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < ITI; i++) {
+            const int t = threadIdx.x + i * NT;
+            if (t < NL * H) D[t] = r[i];
+        }
+    }
     __syncthreads();
     // Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_K2^{-k}, k = 0..M-1
     constexpr int half = M / 2;
-    for (int t = threadIdx.x; t < NL * (half + 1); t += blockDim.x) {
+    for (int t = threadIdx.x; t < NL * (half + 1); t += NT) {
         const int k = t / NL, r = t - k * NL;
         float2* row = D + r * H;
         const int k2 = M - k;
@@ -344,9 +396,11 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zinv4(
     __syncthreads();
     line_fft4<N1, N2, NL, true>(D, H, 1, tw);
     float* o = real + (size_t)r0 * K2;
-    for (int t = threadIdx.x; t < nr * K2; t += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < IT; i++) {
+        const int t = threadIdx.x + i * NT;
         const int r = t / K2, col = t - r * K2;
-        o[t] = Df[2 * r * H + col];
+        if (t < nr * K2) o[t] = Df[2 * r * H + col];
     }
 }
 
