@@ -50,6 +50,11 @@ __device__ __forceinline__ void red_fix(long long* p, float v) {
     long long q = __float2ll_rn(v * SB_FORCE_SCALE);
     if (q) atomicAdd((unsigned long long*)p, (unsigned long long)q);
 }
+// the same without the zero test: on the per-entry j forces of the pair kernels the test costs
+// more issue slots than the atomics it saves (adding zero leaves the sum unchanged)
+__device__ __forceinline__ void add_fix(long long* p, float v) {
+    atomicAdd((unsigned long long*)p, (unsigned long long)__float2ll_rn(v * SB_FORCE_SCALE));
+}
 
 #include "sb_pair_fixed.cuh"
 #include "sb_pair_compact.cuh"

@@ -98,10 +98,10 @@ __device__ __forceinline__ void pair_walk(
             fjy += __shfl_xor_sync(0xffffffffu, fjy, 1);
             fjz += __shfl_xor_sync(0xffffffffu, fjz, 1);
         }
-        if (valid && h == 0 && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
-            red_fix(&fix[j], fjx);
-            red_fix(&fix[P.slot_cap + j], fjy);
-            red_fix(&fix[2 * P.slot_cap + j], fjz);
+        if (valid && h == 0) {
+            add_fix(&fix[j], fjx);
+            add_fix(&fix[P.slot_cap + j], fjy);
+            add_fix(&fix[2 * P.slot_cap + j], fjz);
         }
     }
 }

@@ -132,11 +132,10 @@ __device__ __forceinline__ void pair_walk_x2(
                 }
             }
         }
-        // red_fix skips components that round to zero, so no test of the sums is needed here
         if (valid) {
-            red_fix(&fix[j], -(gx.x + gx.y));
-            red_fix(&fix[P.slot_cap + j], -(gy.x + gy.y));
-            red_fix(&fix[2 * P.slot_cap + j], -(gz.x + gz.y));
+            add_fix(&fix[j], -(gx.x + gx.y));
+            add_fix(&fix[P.slot_cap + j], -(gy.x + gy.y));
+            add_fix(&fix[2 * P.slot_cap + j], -(gz.x + gz.y));
         }
     }
 }
