@@ -1,0 +1,142 @@
+"""Real-system fixture from the reference's own input files (SPONGE/covid-tip4p/) and the
+reference's forces on it (test infrastructure).
+
+SPONGE ships one real system, a 98,282-atom protein in TIP4P water (virtual M sites included as
+charged particles), with no expected outputs. Two steps make it a parity case:
+
+    python tests/golden/make_covid.py inputs      # here: reads the reference tree, writes
+                                                  #   covid_tip4p_inputs.npz (coordinates,
+                                                  #   charges, LJ tables and types, exclusions)
+    python tests/golden/make_covid.py reference [out.npz]
+                                                  # on a GPU machine with oracle/_ref built:
+                                                  #   runs the reference's unchanged modules,
+                                                  #   writes reference_covid_tip4p.npz
+
+The inputs follow the reference's file formats (SPONGE/MD_core/MD_core.cu:1213-1257 coordinates
+with the box on the line after them, :1051-1080 charges, :308-351 exclusions as per-atom
+"count j1 j2 ..." lists of later atoms; SPONGE/Lennard_Jones_force/Lennard_Jones_force.cu
+:1082-1105 "N T", then A and B over the T(T+1)/2 type pairs, then the N types). The cut-off
+(10 A), skin (2 A) and Ewald tolerance (1e-5) are SPONGE's defaults; the PME grid is the one
+Get_Fft_Patameter picks for the box. Only LJ + PME forces are compared: the bonded terms, 1-4 terms and the
+virtual-site force redistribution are outside the hot path.
+"""
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+INPUTS = os.path.join(HERE, "covid_tip4p_inputs.npz")
+REFERENCE = os.path.join(HERE, "reference_covid_tip4p.npz")
+SOURCE = "/root/reference/SPONGE/covid-tip4p"
+# Get_Fft_Patameter's grid for the fixture's box (108.43 x 91.25 x 84.41 A)
+FFT = (112, 96, 96)
+
+
+def _numbers(path):
+    with open(path) as f:
+        return f.read().split()
+
+
+def read_reference_files(src=SOURCE, prefix="covid-tip4p", coordinates="npt_coordinate.txt"):
+    """The LJ + PME inputs of the reference's covid-tip4p system, as arrays. The coordinates are
+    the equilibrated ones the reference ships beside the topology (npt_coordinate.txt): the
+    starting structure (covid-tip4p_coordinate.txt) still has clashes of 0.34 A between
+    non-excluded atoms, whose 1e12 kcal/mol/A forces would swamp any comparison."""
+    # first line: the atom count (and, in a written restart, the simulation time); then one
+    # "x y z" line per atom; then "Lx Ly Lz alpha beta gamma"
+    with open(os.path.join(src, coordinates)) as f:
+        lines = f.read().split("\n")
+    n = int(lines[0].split()[0])
+    crd = np.array(" ".join(lines[1:1 + n]).split(), np.float64).reshape(n, 3)
+    box = np.array(lines[1 + n].split()[:3], np.float64)
+    tok = _numbers(os.path.join(src, prefix + "_charge.txt"))
+    assert int(tok[0]) == n
+    charge = np.array(tok[1:1 + n], np.float32)
+    tok = _numbers(os.path.join(src, prefix + "_lj.txt"))
+    assert int(tok[0]) == n
+    t = int(tok[1])
+    npair = t * (t + 1) // 2
+    A = np.array(tok[2:2 + npair], np.float32)
+    B = np.array(tok[2 + npair:2 + 2 * npair], np.float32)
+    lj_type = np.array(tok[2 + 2 * npair:2 + 2 * npair + n], np.int32)
+    tok = _numbers(os.path.join(src, prefix + "_exclude.txt"))
+    assert int(tok[0]) == n
+    total = int(tok[1])
+    numbers = np.zeros(n, np.int32)
+    lists = []
+    p = 2
+    for i in range(n):
+        c = int(tok[p])
+        numbers[i] = c
+        lists.append(np.array(tok[p + 1:p + 1 + c], np.int32))
+        p += 1 + c
+    excl_list = np.concatenate(lists) if lists else np.zeros(0, np.int32)
+    assert excl_list.size == total
+    return dict(crd=crd.astype(np.float32), box=box.astype(np.float32), charge=charge,
+                lj_A=A, lj_B=B, lj_type=lj_type, n_types=np.int32(t), excl_numbers=numbers,
+                excl_list=excl_list)
+
+
+def load_system(path=INPUTS):
+    """The fixture as a system dict of the form sponge_b200.systems builds."""
+    z = np.load(path)
+    n = z["charge"].size
+    numbers = z["excl_numbers"].astype(np.int32)
+    start = np.zeros(n, np.int32)
+    start[1:] = np.cumsum(numbers)[:-1]
+    box = z["box"].astype(np.float32)
+    crd = np.mod(z["crd"].astype(np.float64), box.astype(np.float64)).astype(np.float32)
+    crd = np.where(crd >= box, np.float32(0.0), crd).astype(np.float32)
+    return dict(
+        name="covid_tip4p", crd=crd, charge=z["charge"].astype(np.float32),
+        lj_type=z["lj_type"].astype(np.int32), n_types=int(z["n_types"]),
+        lj_A=z["lj_A"].astype(np.float32), lj_B=z["lj_B"].astype(np.float32),
+        excl_start=start, excl_numbers=numbers, excl_list=z["excl_list"].astype(np.int32),
+        box=box, cutoff=10.0, skin=2.0, fft=FFT, tolerance=1e-5)
+
+
+def write_inputs():
+    r = read_reference_files()
+    np.savez_compressed(INPUTS, crd=r["crd"], box=r["box"], charge=r["charge"],
+                        lj_A=r["lj_A"], lj_B=r["lj_B"], lj_type=r["lj_type"].astype(np.int8),
+                        n_types=r["n_types"], excl_numbers=r["excl_numbers"].astype(np.int16),
+                        excl_list=r["excl_list"].astype(np.int32))
+    print(INPUTS, os.path.getsize(INPUTS))
+
+
+def write_reference(path=REFERENCE):
+    sys.path.insert(0, ROOT)
+    import oracle  # noqa: E402
+    from oracle.ref_harness import run as refrun  # noqa: E402
+    s = load_system()
+    uc = oracle.crd_to_uint(oracle.periodic_map(s["crd"], s["box"]), s["box"])
+    keys = oracle.pairs(uc, s, "cells")
+    r = refrun.run(s, uc, keys)
+    ref_pairs = r["pairs"]
+    out = dict(
+        frc=r["frc"],
+        frc_plain=r["frc_plain"],
+        n_pairs=np.int64(ref_pairs.size),
+        pairs_sha256=hashlib.sha256(np.sort(ref_pairs).tobytes()).hexdigest(),
+        pairs_only_ref=np.setdiff1d(ref_pairs, keys),
+        pairs_only_oracle=np.setdiff1d(keys, ref_pairs),
+        capacities=np.array(r["capacities"], np.int64),
+    )
+    for k, v in r["summary"].items():
+        out["summary_" + k] = np.float64(v)
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "pairs", ref_pairs.size)
+
+
+if __name__ == "__main__":
+    what = sys.argv[1] if len(sys.argv) > 1 else "inputs"
+    if what == "inputs":
+        write_inputs()
+    elif what == "reference":
+        write_reference(sys.argv[2] if len(sys.argv) > 2 else REFERENCE)
+    else:
+        raise SystemExit("usage: make_covid.py inputs|reference")
