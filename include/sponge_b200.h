@@ -277,6 +277,52 @@ SB_API int sb_nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme
  * (integer accumulation); a graph captured from the caller's stream holds both branches. */
 SB_API int sb_nonbonded_set_overlap(sb_pme* pme, int on);
 
+/* ------------------------------------------------------------------------------------------
+ * NON_BOND_14 (SPONGE/nb14/nb14.cuh:41-86): scaled 1-4 LJ and Coulomb pairs
+ * ---------------------------------------------------------------------------------------- */
+typedef struct sb_nb14 sb_nb14;
+
+/* NON_BOND_14::Initial (nb14.cu:172-246) from arrays: pair atoms a, b; per-pair A (x12) and B
+ * (x6), i.e. lj_scale * LJ_A[type pair] as Initial computes them from the LJ tables, and the
+ * Coulomb scale factor. */
+SB_API int sb_nb14_create(int atom_numbers, int nb14_numbers, const int* h_atom_a,
+                          const int* h_atom_b, const float* h_A, const float* h_B,
+                          const float* h_cf_scale, sb_nb14** out);
+SB_API int sb_nb14_destroy(sb_nb14* nb14);
+/* Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial (nb14.cu:467-480): frc += on both atoms,
+ * atom_energy / atom_virial += on the first atom of each pair (either may be NULL). */
+SB_API int sb_nb14_force(sb_nb14* nb14, const uint32_t* d_uint_crd, const float* d_charge,
+                         const float scaler[3], float* d_frc, float* d_atom_energy,
+                         float* d_atom_virial, void* stream);
+/* Get_14_LJ_Energy / Get_14_CF_Energy (nb14.cu:482-520), summed in FP64; either output may be
+ * NULL. Synchronises the stream. */
+SB_API int sb_nb14_energy(sb_nb14* nb14, const uint32_t* d_uint_crd, const float* d_charge,
+                          const float scaler[3], double* h_lj_energy, double* h_cf_energy,
+                          void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * VIRTUAL_INFORMATION (SPONGE/virtual_atoms/virtual_atoms.cuh:86-142): virtual atoms of types
+ * 0 (mirror of atom 1 in z = h), 1 (r_1 + a r_21), 2 (r_1 + a r_21 + b r_31) and 3
+ * (r_1 + d (r_21 + k r_32)/|r_21 + k r_32|)
+ * ---------------------------------------------------------------------------------------- */
+typedef struct sb_vsite sb_vsite;
+
+/* VIRTUAL_INFORMATION::Initial (virtual_atoms.cu:181-490) from arrays: per record its type,
+ * atoms[4] = {virtual atom, from_1, from_2, from_3} (unused parents ignored) and param[2] = the
+ * type's numbers as the virtual_atom_in_file line gives them (type 0: h; 1: a; 2: a, b; 3: d,
+ * k). Levels (a virtual atom built from virtual atoms sits one level above them) are computed
+ * here. */
+SB_API int sb_vsite_create(int atom_numbers, int virtual_numbers, const int* h_type,
+                           const int* h_atoms, const float* h_param, sb_vsite** out);
+SB_API int sb_vsite_destroy(sb_vsite* vsite);
+/* Coordinate_Refresh: crd of every virtual atom from its parents, lowest level first. */
+SB_API int sb_vsite_coordinate_refresh(sb_vsite* vsite, const uint32_t* d_uint_crd,
+                                       const float scaler[3], float* d_crd, void* stream);
+/* Force_Redistribute: the force on each virtual atom moves to its parents and the virtual
+ * atom's force is zeroed, highest level first. */
+SB_API int sb_vsite_force_redistribute(sb_vsite* vsite, const uint32_t* d_uint_crd,
+                                       const float scaler[3], float* d_frc, void* stream);
+
 /* Crd_To_Uint_Crd (SPONGE/common.cu:264-287) with the quarter coefficient 0.25*2^32/L, as
  * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */
 SB_API int sb_crd_to_uint_crd(int atom_numbers, const float box_length[3], const float* d_crd,

@@ -22,6 +22,11 @@
 //                                    :367-550 (grid points, spread, gather), :553-566 + :753-771
 //                                    (reciprocal and self energies)
 //   * FFT grid size                  SPONGE/common.cu:467-534 (Get_Fft_Patameter)
+//   * 1-4 pairs                      SPONGE/nb14/nb14.cu:92-170 (force, energy, virial),
+//                                    :5-91 (energies), :203-217 (per-pair A, B)
+//   * virtual atoms                  SPONGE/virtual_atoms/virtual_atoms.cu:2-73 (positions),
+//                                    :75-180 (force redistribution), :246-290 + :495-530
+//                                    (levels and their order)
 //
 // Pair-set criterion. The reference decides list membership with an FP32 expression whose
 // evaluation order (and FMA contraction) is chosen by its compiler. This build pins ONE order:
@@ -886,6 +891,128 @@ void orc_ti_cross(int n, const uint32_t* uc, const float* q, const float* dq, co
     out[0] = rec;
     out[1] = -2.0 * beta / std::sqrt(M_PI) * sqq + 2.0 * nf * sq * sdq;
     out[2] = corr;
+}
+
+// 1-4 pairs in FP64 (nb14.cu:92-170): dr = r_b - r_a (minimum image); F/r = -A r^-14 + B r^-8
+// - cf q_a q_b r^-3 with charges below 1e-10 clamped to 1e-10 (nb14.cu:77-82); F r_hat added to
+// a and subtracted from b; E = cf q_a q_b / r + A/12 r^-12 - B/6 r^-6 and the virial -F.dr to
+// atom a. out[0] = sum of the LJ parts, out[1] = sum of the Coulomb parts.
+void orc_nb14(int n, int n14, const uint32_t* uc, const float* q, const float* box,
+              const int* a14, const int* b14, const float* A, const float* B, const float* cf,
+              double* frc, double* atom_energy, double* atom_virial, double* out) {
+    float s[3];
+    scaler_of(box, s);
+    double elj = 0.0, ecf = 0.0;
+    for (int p = 0; p < n14; p++) {
+        const int i = a14[p], j = b14[p];
+        double dr[3];
+        dr_f64(uc + 3 * (size_t)i, uc + 3 * (size_t)j, s, dr);
+        const double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+        const double ri2 = 1.0 / r2, ri = std::sqrt(ri2);
+        double qi = q[i], qj = q[j];
+        if (std::fabs(qi) < 1e-10) qi = (double)1e-10f;
+        if (std::fabs(qj) < 1e-10) qj = (double)1e-10f;
+        const double ri6 = ri2 * ri2 * ri2;
+        const double fs = -(double)A[p] * ri6 * ri6 * ri2 + (double)B[p] * ri6 * ri2 -
+                          (double)cf[p] * qi * qj * ri2 * ri;
+        for (int d = 0; d < 3; d++) {
+            frc[3 * (size_t)i + d] += fs * dr[d];
+            frc[3 * (size_t)j + d] -= fs * dr[d];
+        }
+        const double el = (double)A[p] / 12.0 * ri6 * ri6 - (double)B[p] / 6.0 * ri6;
+        const double ec = (double)cf[p] * qi * qj * ri;
+        atom_energy[i] += el + ec;
+        atom_virial[i] -= fs * r2;
+        elj += el;
+        ecf += ec;
+    }
+    out[0] = elj;
+    out[1] = ecf;
+}
+
+// Virtual atoms in FP64. Records: type[v], atoms[4v..4v+3] = {virtual, from_1, from_2, from_3},
+// param[2v..2v+1] as the input line gives them (type 0: h; 1: a; 2: a, b; 3: d, k); level[]
+// gives each record's level (1 = built from real atoms only). Displacements are the minimum-image
+// ones of the fixed-point coordinates, positions are the parent's position plus the displacement
+// (virtual_atoms.cu:2-73). mode 0: refresh crd (lowest level first); mode 1: move each virtual
+// atom's force to its parents and zero it (highest level first, virtual_atoms.cu:75-180).
+static void vs_dr(const uint32_t* uc, int from, int to, const float s[3], double d[3]) {
+    dr_f64(uc + 3 * (size_t)from, uc + 3 * (size_t)to, s, d);
+}
+
+void orc_vsite(int nv, const int* type, const int* atoms, const float* param, const int* level,
+               int maxlevel, const uint32_t* uc, const float* box, int mode, double* crd,
+               double* frc) {
+    float s[3];
+    scaler_of(box, s);
+    for (int li = 0; li < maxlevel; li++) {
+        const int L = mode == 0 ? li + 1 : maxlevel - li;
+        for (int r = 0; r < nv; r++) {
+            if (level[r] != L) continue;
+            const int t = type[r];
+            const int v = atoms[4 * r], f1 = atoms[4 * r + 1], f2 = atoms[4 * r + 2],
+                      f3 = atoms[4 * r + 3];
+            const double p0 = param[2 * r], p1 = param[2 * r + 1];
+            if (mode == 0) {
+                double x[3] = {crd[3 * (size_t)f1], crd[3 * (size_t)f1 + 1], crd[3 * (size_t)f1 + 2]};
+                if (t == 0) {
+                    x[2] = 2.0 * p0 - x[2];  // mirror in the plane z = h
+                } else if (t == 1) {
+                    double d[3];
+                    vs_dr(uc, f1, f2, s, d);
+                    for (int k = 0; k < 3; k++) x[k] += p0 * d[k];
+                } else if (t == 2) {
+                    double d1[3], d2[3];
+                    vs_dr(uc, f1, f2, s, d1);
+                    vs_dr(uc, f1, f3, s, d2);
+                    for (int k = 0; k < 3; k++) x[k] += p0 * d1[k] + p1 * d2[k];
+                } else {
+                    double r21[3], r32[3], tt[3];
+                    vs_dr(uc, f1, f2, s, r21);
+                    vs_dr(uc, f2, f3, s, r32);
+                    for (int k = 0; k < 3; k++) tt[k] = r21[k] + p1 * r32[k];
+                    const double f = p0 / std::sqrt(tt[0] * tt[0] + tt[1] * tt[1] + tt[2] * tt[2]);
+                    for (int k = 0; k < 3; k++) x[k] += f * tt[k];
+                }
+                for (int k = 0; k < 3; k++) crd[3 * (size_t)v + k] = x[k];
+            } else {
+                double fv[3] = {frc[3 * (size_t)v], frc[3 * (size_t)v + 1], frc[3 * (size_t)v + 2]};
+                if (t == 0) {
+                    frc[3 * (size_t)f1] += fv[0];
+                    frc[3 * (size_t)f1 + 1] += fv[1];
+                    frc[3 * (size_t)f1 + 2] -= fv[2];
+                } else if (t == 1) {
+                    for (int k = 0; k < 3; k++) {
+                        frc[3 * (size_t)f1 + k] += p0 * fv[k];
+                        frc[3 * (size_t)f2 + k] += (1.0 - p0) * fv[k];
+                    }
+                } else if (t == 2) {
+                    for (int k = 0; k < 3; k++) {
+                        frc[3 * (size_t)f1 + k] += (1.0 - p0 - p1) * fv[k];
+                        frc[3 * (size_t)f2 + k] += p0 * fv[k];
+                        frc[3 * (size_t)f3 + k] += p1 * fv[k];
+                    }
+                } else {
+                    double r21[3], r32[3], rv1[3], tt[3];
+                    vs_dr(uc, f1, f2, s, r21);
+                    vs_dr(uc, f2, f3, s, r32);
+                    vs_dr(uc, f1, v, s, rv1);
+                    for (int k = 0; k < 3; k++) tt[k] = r21[k] + p1 * r32[k];
+                    const double factor =
+                        p0 / std::sqrt(tt[0] * tt[0] + tt[1] * tt[1] + tt[2] * tt[2]);
+                    const double proj = (rv1[0] * fv[0] + rv1[1] * fv[1] + rv1[2] * fv[2]) /
+                                        (rv1[0] * rv1[0] + rv1[1] * rv1[1] + rv1[2] * rv1[2]);
+                    for (int k = 0; k < 3; k++) {
+                        const double tk = factor * (fv[k] - proj * rv1[k]);
+                        frc[3 * (size_t)f1 + k] += fv[k] - tk;
+                        frc[3 * (size_t)f2 + k] += (1.0 - p1) * tk;
+                        frc[3 * (size_t)f3 + k] += p1 * tk;
+                    }
+                }
+                for (int k = 0; k < 3; k++) frc[3 * (size_t)v + k] = 0.0;
+            }
+        }
+    }
 }
 
 }  // extern "C"

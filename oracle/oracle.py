@@ -73,6 +73,10 @@ def lib():
                                    ctypes.c_long, _f64p, _f64p]
         L.orc_ti_cross.argtypes = [ctypes.c_int, _u32p, _f32p, _f32p, _f32p, _i32p,
                                    ctypes.c_double, _i32p, _i32p, _i32p, _f64p]
+        L.orc_nb14.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _f32p, _i32p, _i32p,
+                               _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f64p]
+        L.orc_vsite.argtypes = [ctypes.c_int, _i32p, _i32p, _f32p, _i32p, ctypes.c_int, _u32p,
+                                _f32p, ctypes.c_int, _f64p, _f64p]
         L.orc_threads.restype = ctypes.c_int
         L.orc_set_threads.argtypes = [ctypes.c_int]
         _LIB = L
@@ -384,3 +388,56 @@ def fep_reference(sys, uc=None, lam=None):
                 e_rec=erec, e_lrc=flrc / V, dhdl_lj=p["dhdl_lj"], dhdl_direct=p["dhdl_direct"],
                 cross_rec=x["rec"], cross_self=x["self"], cross_corr=x["corr"],
                 dhdl_lrc=flrc_ti / V)
+
+
+def nb14(uc, box, charge, atom_a, atom_b, A, B, cf):
+    """1-4 pairs in FP64 (SPONGE/nb14/nb14.cu:92-170). A, B per pair (x12, x6).
+    Returns (frc [N,3], atom_energy [N], atom_virial [N], e_lj, e_cf)."""
+    n = uc.shape[0]
+    a = np.ascontiguousarray(atom_a, np.int32)
+    frc = np.zeros(3 * n, np.float64)
+    ae = np.zeros(n, np.float64)
+    av = np.zeros(n, np.float64)
+    out = np.zeros(2, np.float64)
+    lib().orc_nb14(n, a.size, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                   np.ascontiguousarray(charge, np.float32), np.ascontiguousarray(box, np.float32),
+                   a, np.ascontiguousarray(atom_b, np.int32), np.ascontiguousarray(A, np.float32),
+                   np.ascontiguousarray(B, np.float32), np.ascontiguousarray(cf, np.float32), frc,
+                   ae, av, out)
+    return frc.reshape(n, 3), ae, av, float(out[0]), float(out[1])
+
+
+def vsite_levels(n, types, atoms):
+    """Level of each virtual-atom record: one above its highest parent (virtual_atoms.cu:
+    246-290), iterated to a fixed point so that the record order does not matter."""
+    npar = {0: 1, 1: 2, 2: 3, 3: 3}
+    atoms = np.asarray(atoms, np.int64).reshape(-1, 4)
+    level = np.zeros(n, np.int64)
+    for _ in range(len(types) + 1):
+        changed = False
+        for r, t in enumerate(types):
+            lv = max(level[atoms[r, k]] for k in range(1, npar[int(t)] + 1)) + 1
+            if level[atoms[r, 0]] != lv:
+                level[atoms[r, 0]] = lv
+                changed = True
+        if not changed:
+            break
+    return np.array([level[atoms[r, 0]] for r in range(len(types))], np.int32)
+
+
+def vsite(uc, box, types, atoms, params, crd=None, frc=None):
+    """Virtual atoms in FP64: with ``crd`` [N,3], returns the refreshed coordinates
+    (Coordinate_Refresh); with ``frc`` [N,3], returns the redistributed forces
+    (Force_Redistribute)."""
+    n = uc.shape[0]
+    t = np.ascontiguousarray(types, np.int32)
+    a = np.ascontiguousarray(atoms, np.int32).reshape(-1)
+    p = np.ascontiguousarray(params, np.float32).reshape(-1)
+    lv = vsite_levels(n, t, a)
+    ml = int(lv.max()) if lv.size else 0
+    mode = 0 if crd is not None else 1
+    c = np.ascontiguousarray(crd if crd is not None else np.zeros((n, 3)), np.float64).reshape(-1).copy()
+    f = np.ascontiguousarray(frc if frc is not None else np.zeros((n, 3)), np.float64).reshape(-1).copy()
+    lib().orc_vsite(t.size, t, a, p, lv, ml, np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                    np.ascontiguousarray(box, np.float32), mode, c, f)
+    return (c if mode == 0 else f).reshape(n, 3)

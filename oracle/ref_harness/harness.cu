@@ -9,9 +9,15 @@
 //         max_atom_in_grid_numbers; float box[3], cutoff, skin, tolerance;
 //         float crd[3N], charge[N]; int32 type[N]; float A[T(T+1)/2], B[...] (unscaled);
 //         int32 excl_start[N], excl_numbers[N], excl_list[nexcl]
+//         optional, after that: int32 n14, a[n14], b[n14], float lj_scale[n14], cf[n14];
+//         int32 nv, type[nv], atoms[4 nv], float param[2 nv] (the 1-4 pairs and virtual atoms,
+//         run through NON_BOND_14 and VIRTUAL_INFORMATION when present)
 // outputs (outdir): frc.f32 [3N] force of one evaluation with energy and virial requested,
 //         frc_plain.f32 [3N] force-only evaluation, pairs.i64 (sorted keys i*N+j),
-//         summary.txt (key value lines)
+//         summary.txt (key value lines); with 1-4 pairs: nb14_frc.f32 [3N], nb14_ae.f32 [N],
+//         nb14_av.f32 [N] (Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial from zero);
+//         with virtual atoms: vs_frc.f32 [3N] (frc.f32 after Force_Redistribute),
+//         vs_crd.f32 [3N] (the wrapped coordinates after Coordinate_Refresh)
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -24,7 +30,9 @@
 #include "control.cuh"
 #include "Lennard_Jones_force/Lennard_Jones_force.cuh"
 #include "PME_force/PME_force.cuh"
+#include "nb14/nb14.cuh"
 #include "neighbor_list/neighbor_list.cuh"
+#include "virtual_atoms/virtual_atoms.cuh"
 
 #define CK(x)                                                                      \
     do {                                                                           \
@@ -88,6 +96,28 @@ int main(int argc, char** argv) {
     rd(f, es.data(), es.size());
     rd(f, en.data(), en.size());
     rd(f, el.data(), NE);
+    // optional 1-4 pairs and virtual atoms
+    int n14 = 0, nv = 0;
+    std::vector<int> a14, b14, vtype, vatoms;
+    std::vector<float> ljs14, cf14, vparam;
+    if (fread(&n14, sizeof(int), 1, f) == 1 && n14 > 0) {
+        a14.resize(n14);
+        b14.resize(n14);
+        ljs14.resize(n14);
+        cf14.resize(n14);
+        rd(f, a14.data(), n14);
+        rd(f, b14.data(), n14);
+        rd(f, ljs14.data(), n14);
+        rd(f, cf14.data(), n14);
+    }
+    if (fread(&nv, sizeof(int), 1, f) == 1 && nv > 0) {
+        vtype.resize(nv);
+        vatoms.resize(4 * (size_t)nv);
+        vparam.resize(2 * (size_t)nv);
+        rd(f, vtype.data(), nv);
+        rd(f, vatoms.data(), vatoms.size());
+        rd(f, vparam.data(), vparam.size());
+    }
     fclose(f);
     el.resize(NE);
 
@@ -118,6 +148,32 @@ int main(int argc, char** argv) {
     controller.Set_Command("neighbor_list_max_neighbor_numbers", buf);
     snprintf(buf, sizeof(buf), "%d", hdr[8]);
     controller.Set_Command("neighbor_list_max_atom_in_grid_numbers", buf);
+    // nb14_in_file (nb14.cu:179-187, :203-206) and virtual_atom_in_file (virtual_atoms.cu:
+    // 192-200) in the reference's text formats
+    char nb14path[1024], vspath[1024];
+    if (n14 > 0) {
+        snprintf(nb14path, sizeof(nb14path), "%s/nb14_in.txt", argv[2]);
+        FILE* nf = fopen(nb14path, "w");
+        fprintf(nf, "%d\n", n14);
+        for (int i = 0; i < n14; i++)
+            fprintf(nf, "%d %d %.9g %.9g\n", a14[i], b14[i], ljs14[i], cf14[i]);
+        fclose(nf);
+        controller.Set_Command("nb14_in_file", nb14path);
+    }
+    if (nv > 0) {
+        snprintf(vspath, sizeof(vspath), "%s/vatom_in.txt", argv[2]);
+        FILE* vf = fopen(vspath, "w");
+        const int npar[4] = {1, 2, 3, 3};
+        for (int i = 0; i < nv; i++) {
+            fprintf(vf, "%d", vtype[i]);
+            for (int k = 0; k <= npar[vtype[i]]; k++) fprintf(vf, " %d", vatoms[4 * i + k]);
+            fprintf(vf, " %.9g", vparam[2 * i]);
+            if (vtype[i] >= 2) fprintf(vf, " %.9g", vparam[2 * i + 1]);
+            fprintf(vf, "\n");
+        }
+        fclose(vf);
+        controller.Set_Command("virtual_atom_in_file", vspath);
+    }
 
     VECTOR box = {fh[0], fh[1], fh[2]};
     const float cutoff = fh[3], skin = fh[4];
@@ -217,6 +273,44 @@ int main(int argc, char** argv) {
     std::sort(keys.begin(), keys.end());
     wr(argv[2], "pairs.i64", keys.data(), sizeof(long long) * keys.size());
 
+    // 1-4 pairs and virtual atoms (SPONGE/main.cu:81, :127, :195, :207, :375)
+    float e14_lj = 0.f, e14_cf = 0.f;
+    if (n14 > 0) {
+        NON_BOND_14 nb14;
+        nb14.Initial(&controller, lj.h_LJ_A, lj.h_LJ_B, lj.h_atom_LJ_type);
+        cudaMemset(d_frc, 0, sizeof(VECTOR) * N);
+        cudaMemset(d_ae, 0, sizeof(float) * N);
+        cudaMemset(d_av, 0, sizeof(float) * N);
+        nb14.Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial(d_uc, d_q, scaler, (VECTOR*)d_frc,
+                                                                 d_ae, d_av);
+        CK(cudaDeviceSynchronize());
+        std::vector<float> f14(3 * (size_t)N), e14(N), v14(N);
+        CK(cudaMemcpy(f14.data(), d_frc, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(e14.data(), d_ae, sizeof(float) * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(v14.data(), d_av, sizeof(float) * N, cudaMemcpyDeviceToHost));
+        wr(argv[2], "nb14_frc.f32", f14.data(), sizeof(float) * f14.size());
+        wr(argv[2], "nb14_ae.f32", e14.data(), sizeof(float) * e14.size());
+        wr(argv[2], "nb14_av.f32", v14.data(), sizeof(float) * v14.size());
+        e14_lj = nb14.Get_14_LJ_Energy(d_uc, scaler);
+        e14_cf = nb14.Get_14_CF_Energy(d_uc, d_q, scaler);
+    }
+    if (nv > 0) {
+        VIRTUAL_INFORMATION vatom;
+        int freedom = 3 * N;
+        vatom.Initial(&controller, N, &freedom);
+        // the LJ + PME forces of the energy/virial evaluation, redistributed
+        CK(cudaMemcpy(d_frc, h.data(), sizeof(float) * 3 * N, cudaMemcpyHostToDevice));
+        vatom.Force_Redistribute(d_uc, scaler, (VECTOR*)d_frc);
+        CK(cudaDeviceSynchronize());
+        std::vector<float> fv(3 * (size_t)N), cv(3 * (size_t)N);
+        CK(cudaMemcpy(fv.data(), d_frc, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost));
+        wr(argv[2], "vs_frc.f32", fv.data(), sizeof(float) * fv.size());
+        vatom.Coordinate_Refresh(d_uc, scaler, (VECTOR*)d_crd);
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpy(cv.data(), d_crd, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost));
+        wr(argv[2], "vs_crd.f32", cv.data(), sizeof(float) * cv.size());
+    }
+
     double ms_step = -1, ms_force = -1;
     if (timing_steps > 0) {
         cudaEvent_t a, b;
@@ -257,6 +351,8 @@ int main(int argc, char** argv) {
             lj.long_range_factor, keys.size(), overflow);
     fprintf(s, "ms_force_only %.6f\nms_step %.6f\ntiming_steps %d\n", ms_force, ms_step,
             timing_steps);
+    fprintf(s, "nb14_pairs %d\nnb14_lj %.9g\nnb14_cf %.9g\nvirtual_atoms %d\n", n14, e14_lj,
+            e14_cf, nv);
     fclose(s);
     printf("harness done: %d atoms, %zu pairs\n", N, keys.size());
     return 0;

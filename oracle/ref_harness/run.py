@@ -53,6 +53,20 @@ def write_input(path, system, max_nb, max_grid, refresh_interval=20):
         np.asarray(system["excl_start"], np.int32).tofile(f)
         np.asarray(system["excl_numbers"], np.int32).tofile(f)
         el.tofile(f)
+        # optional 1-4 pairs and virtual atoms
+        a14 = np.asarray(system.get("nb14_a", np.zeros(0)), np.int32)
+        np.array([a14.size], np.int32).tofile(f)
+        if a14.size:
+            a14.tofile(f)
+            np.asarray(system["nb14_b"], np.int32).tofile(f)
+            np.asarray(system["nb14_lj_scale"], np.float32).tofile(f)
+            np.asarray(system["nb14_cf"], np.float32).tofile(f)
+        vt = np.asarray(system.get("vs_type", np.zeros(0)), np.int32)
+        np.array([vt.size], np.int32).tofile(f)
+        if vt.size:
+            vt.tofile(f)
+            np.asarray(system["vs_atoms"], np.int32).reshape(-1).tofile(f)
+            np.asarray(system["vs_param"], np.float32).reshape(-1).tofile(f)
 
 
 def run(system, uc, pair_keys, timing_steps=0, outdir=None, timeout=900):
@@ -71,8 +85,14 @@ def run(system, uc, pair_keys, timing_steps=0, outdir=None, timeout=900):
     for line in open(os.path.join(outdir, "summary.txt")):
         k, v = line.split()
         summ[k] = float(v)
-    return dict(
+    out = dict(
         frc=np.fromfile(os.path.join(outdir, "frc.f32"), np.float32).reshape(n, 3),
         frc_plain=np.fromfile(os.path.join(outdir, "frc_plain.f32"), np.float32).reshape(n, 3),
         pairs=np.fromfile(os.path.join(outdir, "pairs.i64"), np.int64),
         summary=summ, capacities=(max_nb, max_grid), outdir=outdir)
+    for name, shape in (("nb14_frc", (n, 3)), ("nb14_ae", (n,)), ("nb14_av", (n,)),
+                        ("vs_frc", (n, 3)), ("vs_crd", (n, 3))):
+        path = os.path.join(outdir, name + ".f32")
+        if os.path.exists(path):
+            out[name] = np.fromfile(path, np.float32).reshape(shape)
+    return out

@@ -91,6 +91,14 @@ _SIGS = {
     "sb_sc_dh_dlambda": [_vp, _vp, _vp, _vp, _f, _vp, _vp],
     "sb_pme_ti_cross": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "sb_fep_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_nb14_create": [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_nb14_destroy": [_vp],
+    "sb_nb14_force": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_nb14_energy": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_vsite_create": [_i, _i, _vp, _vp, _vp, _vp],
+    "sb_vsite_destroy": [_vp],
+    "sb_vsite_coordinate_refresh": [_vp, _vp, _vp, _vp, _vp],
+    "sb_vsite_force_redistribute": [_vp, _vp, _vp, _vp, _vp],
 }
 
 
@@ -519,3 +527,102 @@ def fep_step(nl, sc, pme, uint_crd, charge, excl, frc, dudl=None, stream=None):
     _check(lib().sb_fep_step(nl.handle, sc.handle, pme.handle, _ptr(uint_crd), _ptr(charge),
                              _ptr(es), _ptr(el), _ptr(en), _ptr(frc), _ptr(dudl),
                              _stream(stream)))
+
+
+def nb14_pair_tables(atom_a, atom_b, lj_scale, lj_A, lj_B, lj_type):
+    """Per-pair A (x12) and B (x6) of the 1-4 pairs as NON_BOND_14::Initial builds them
+    (SPONGE/nb14/nb14.cu:203-217): lj_scale times the LJ tables' entry of the pair's types
+    (lower-triangle index max(ti,tj)(max+1)/2 + min). lj_A / lj_B are the LJ module's tables
+    already scaled by 12 and 6."""
+    ta = np.asarray(lj_type, np.int64)[np.asarray(atom_a, np.int64)]
+    tb = np.asarray(lj_type, np.int64)[np.asarray(atom_b, np.int64)]
+    hi, lo = np.maximum(ta, tb), np.minimum(ta, tb)
+    k = hi * (hi + 1) // 2 + lo
+    scale = np.asarray(lj_scale, np.float32)
+    return ((scale * np.asarray(lj_A, np.float32)[k]).astype(np.float32),
+            (scale * np.asarray(lj_B, np.float32)[k]).astype(np.float32))
+
+
+class NonBond14:
+    """NON_BOND_14 from arrays (pair atoms, per-pair A/B as nb14_pair_tables gives them, Coulomb
+    scale factors)."""
+
+    def __init__(self, atom_numbers, atom_a, atom_b, A, B, cf_scale):
+        _require_cuda()
+        self.atom_numbers = int(atom_numbers)
+        a = np.ascontiguousarray(atom_a, np.int32)
+        b = np.ascontiguousarray(atom_b, np.int32)
+        A = np.ascontiguousarray(A, np.float32)
+        B = np.ascontiguousarray(B, np.float32)
+        cf = np.ascontiguousarray(cf_scale, np.float32)
+        self.nb14_numbers = int(a.size)
+        self.handle = ctypes.c_void_p()
+        _check(lib().sb_nb14_create(self.atom_numbers, self.nb14_numbers, a.ctypes.data,
+                                    b.ctypes.data, A.ctypes.data, B.ctypes.data, cf.ctypes.data,
+                                    ctypes.byref(self.handle)))
+
+    def Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial(self, uint_crd, charge, scaler, frc,
+                                                             atom_energy=None, atom_virial=None,
+                                                             stream=None):
+        _check(lib().sb_nb14_force(self.handle, _ptr(uint_crd), _ptr(charge), _box3(scaler),
+                                   _ptr(frc), _ptr(atom_energy), _ptr(atom_virial),
+                                   _stream(stream)))
+
+    def Get_14_LJ_Energy(self, uint_crd, scaler, stream=None):
+        e = ctypes.c_double()
+        _check(lib().sb_nb14_energy(self.handle, _ptr(uint_crd), None, _box3(scaler),
+                                    ctypes.byref(e), None, _stream(stream)))
+        return e.value
+
+    def Get_14_CF_Energy(self, uint_crd, charge, scaler, stream=None):
+        e = ctypes.c_double()
+        _check(lib().sb_nb14_energy(self.handle, _ptr(uint_crd), _ptr(charge), _box3(scaler),
+                                    None, ctypes.byref(e), _stream(stream)))
+        return e.value
+
+    def Clear(self):
+        if self.handle:
+            lib().sb_nb14_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+
+class VirtualAtoms:
+    """VIRTUAL_INFORMATION from arrays: ``types`` [V], ``atoms`` [V, 4] (virtual atom, from_1,
+    from_2, from_3; unused parents may be anything in range), ``params`` [V, 2] as the
+    virtual_atom_in_file line gives them."""
+
+    def __init__(self, atom_numbers, types, atoms, params):
+        _require_cuda()
+        self.atom_numbers = int(atom_numbers)
+        t = np.ascontiguousarray(types, np.int32)
+        a = np.ascontiguousarray(atoms, np.int32).reshape(-1, 4)
+        p = np.ascontiguousarray(params, np.float32).reshape(-1, 2)
+        self.virtual_numbers = int(t.size)
+        self.handle = ctypes.c_void_p()
+        _check(lib().sb_vsite_create(self.atom_numbers, self.virtual_numbers, t.ctypes.data,
+                                     a.ctypes.data, p.ctypes.data, ctypes.byref(self.handle)))
+
+    def Coordinate_Refresh(self, uint_crd, scaler, crd, stream=None):
+        _check(lib().sb_vsite_coordinate_refresh(self.handle, _ptr(uint_crd), _box3(scaler),
+                                                 _ptr(crd), _stream(stream)))
+
+    def Force_Redistribute(self, uint_crd, scaler, frc, stream=None):
+        _check(lib().sb_vsite_force_redistribute(self.handle, _ptr(uint_crd), _box3(scaler),
+                                                 _ptr(frc), _stream(stream)))
+
+    def Clear(self):
+        if self.handle:
+            lib().sb_vsite_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass

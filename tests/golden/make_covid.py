@@ -2,7 +2,8 @@
 reference's forces on it (test infrastructure).
 
 SPONGE ships one real system, a 98,282-atom protein in TIP4P water (virtual M sites included as
-charged particles), with no expected outputs. Two steps make it a parity case:
+charged particles), with no expected outputs. Two steps make it a parity case for the nonbonded
+path and for the two modules beside it, the 1-4 pairs and the virtual atoms:
 
     python tests/golden/make_covid.py inputs      # here: reads the reference tree, writes
                                                   #   covid_tip4p_inputs.npz (coordinates,
@@ -17,8 +18,9 @@ with the box on the line after them, :1051-1080 charges, :308-351 exclusions as 
 "count j1 j2 ..." lists of later atoms; SPONGE/Lennard_Jones_force/Lennard_Jones_force.cu
 :1082-1105 "N T", then A and B over the T(T+1)/2 type pairs, then the N types). The cut-off
 (10 A), skin (2 A) and Ewald tolerance (1e-5) are SPONGE's defaults; the PME grid is the one
-Get_Fft_Patameter picks for the box. Only LJ + PME forces are compared: the bonded terms, 1-4 terms and the
-virtual-site force redistribution are outside the hot path.
+Get_Fft_Patameter picks for the box. The 1-4 pairs (covid-tip4p_nb14.txt: "count", then
+"a b lj_scale cf_scale") and virtual atoms (covid-tip4p_vatom.txt: one "type v from... params" line
+each) come from the same directory; the bonded terms are not part of the comparison.
 """
 
 import hashlib
@@ -76,9 +78,31 @@ def read_reference_files(src=SOURCE, prefix="covid-tip4p", coordinates="npt_coor
         p += 1 + c
     excl_list = np.concatenate(lists) if lists else np.zeros(0, np.int32)
     assert excl_list.size == total
+    # 1-4 pairs (nb14.cu:179-206): "count", then "a b lj_scale cf_scale" per pair
+    tok = _numbers(os.path.join(src, prefix + "_nb14.txt"))
+    n14 = int(tok[0])
+    rows = np.array(tok[1:1 + 4 * n14], np.float64).reshape(n14, 4)
+    # virtual atoms (virtual_atoms.cu:246-290): "type v from... params" per line
+    vt, va, vp = [], [], []
+    npar = {0: 1, 1: 2, 2: 3, 3: 3}
+    with open(os.path.join(src, prefix + "_vatom.txt")) as f:
+        for line in f:
+            w = line.split()
+            if len(w) < 2:
+                continue
+            vtype = int(w[0])
+            k = npar[vtype]
+            idx = [int(x) for x in w[1:2 + k]]
+            par = [float(x) for x in w[2 + k:]] + [0.0]
+            vt.append(vtype)
+            va.append(idx + [idx[1]] * (4 - len(idx)))
+            vp.append(par[:2])
     return dict(crd=crd.astype(np.float32), box=box.astype(np.float32), charge=charge,
                 lj_A=A, lj_B=B, lj_type=lj_type, n_types=np.int32(t), excl_numbers=numbers,
-                excl_list=excl_list)
+                excl_list=excl_list, nb14_a=rows[:, 0].astype(np.int32),
+                nb14_b=rows[:, 1].astype(np.int32), nb14_lj_scale=rows[:, 2].astype(np.float32),
+                nb14_cf=rows[:, 3].astype(np.float32), vs_type=np.array(vt, np.int32),
+                vs_atoms=np.array(va, np.int32), vs_param=np.array(vp, np.float32))
 
 
 def load_system(path=INPUTS):
@@ -96,7 +120,11 @@ def load_system(path=INPUTS):
         lj_type=z["lj_type"].astype(np.int32), n_types=int(z["n_types"]),
         lj_A=z["lj_A"].astype(np.float32), lj_B=z["lj_B"].astype(np.float32),
         excl_start=start, excl_numbers=numbers, excl_list=z["excl_list"].astype(np.int32),
-        box=box, cutoff=10.0, skin=2.0, fft=FFT, tolerance=1e-5)
+        box=box, cutoff=10.0, skin=2.0, fft=FFT, tolerance=1e-5,
+        nb14_a=z["nb14_a"].astype(np.int32), nb14_b=z["nb14_b"].astype(np.int32),
+        nb14_lj_scale=z["nb14_lj_scale"].astype(np.float32),
+        nb14_cf=z["nb14_cf"].astype(np.float32), vs_type=z["vs_type"].astype(np.int32),
+        vs_atoms=z["vs_atoms"].astype(np.int32), vs_param=z["vs_param"].astype(np.float32))
 
 
 def write_inputs():
@@ -104,8 +132,27 @@ def write_inputs():
     np.savez_compressed(INPUTS, crd=r["crd"], box=r["box"], charge=r["charge"],
                         lj_A=r["lj_A"], lj_B=r["lj_B"], lj_type=r["lj_type"].astype(np.int8),
                         n_types=r["n_types"], excl_numbers=r["excl_numbers"].astype(np.int16),
-                        excl_list=r["excl_list"].astype(np.int32))
+                        excl_list=r["excl_list"].astype(np.int32), nb14_a=r["nb14_a"],
+                        nb14_b=r["nb14_b"], nb14_lj_scale=r["nb14_lj_scale"],
+                        nb14_cf=r["nb14_cf"], vs_type=r["vs_type"].astype(np.int8),
+                        vs_atoms=r["vs_atoms"], vs_param=r["vs_param"])
     print(INPUTS, os.path.getsize(INPUTS))
+
+
+def compact_modules(r, s):
+    """The 1-4 and virtual-atom outputs stored compactly: the 1-4 arrays only on the atoms of
+    1-4 pairs (nb14_atoms), the refreshed coordinates only of the virtual atoms; the
+    redistributed forces in full."""
+    out = {}
+    if "nb14_frc" in r:
+        atoms = np.unique(np.concatenate([s["nb14_a"], s["nb14_b"]])).astype(np.int32)
+        out["nb14_atoms"] = atoms
+        for k in ("nb14_frc", "nb14_ae", "nb14_av"):
+            out[k] = np.asarray(r[k], np.float32)[atoms]
+    if "vs_frc" in r:
+        out["vs_frc"] = np.asarray(r["vs_frc"], np.float32)
+        out["vs_crd"] = np.asarray(r["vs_crd"], np.float32)[s["vs_atoms"][:, 0]]
+    return out
 
 
 def write_reference(path=REFERENCE):
@@ -119,13 +166,13 @@ def write_reference(path=REFERENCE):
     ref_pairs = r["pairs"]
     out = dict(
         frc=r["frc"],
-        frc_plain=r["frc_plain"],
         n_pairs=np.int64(ref_pairs.size),
         pairs_sha256=hashlib.sha256(np.sort(ref_pairs).tobytes()).hexdigest(),
         pairs_only_ref=np.setdiff1d(ref_pairs, keys),
         pairs_only_oracle=np.setdiff1d(keys, ref_pairs),
         capacities=np.array(r["capacities"], np.int64),
     )
+    out.update(compact_modules(r, s))
     for k, v in r["summary"].items():
         out["summary_" + k] = np.float64(v)
     np.savez_compressed(path, **out)
@@ -140,3 +187,13 @@ if __name__ == "__main__":
         write_reference(sys.argv[2] if len(sys.argv) > 2 else REFERENCE)
     else:
         raise SystemExit("usage: make_covid.py inputs|reference")
+
+
+def compact_file(src, dst=REFERENCE):
+    """Rewrites a reference file whose 1-4 and virtual-atom arrays are stored in full."""
+    z = dict(np.load(src))
+    z.pop("frc_plain", None)  # within FP32 rounding of frc; not kept for this system
+    s = load_system()
+    r = {k: z.pop(k) for k in ("nb14_frc", "nb14_ae", "nb14_av", "vs_frc", "vs_crd") if k in z}
+    z.update(compact_modules(r, s))
+    np.savez_compressed(dst, **z)

@@ -89,6 +89,8 @@ def test_pair_list_matches_reference(case):
 def test_reference_forces_match_oracle(case):
     name, s, uc, ref, g = case
     for key in ("frc", "frc_plain"):
+        if key not in g.files:  # the real system keeps only the energy/virial evaluation
+            continue
         f = g[key].astype(np.float64)
         err = np.sqrt(((f - ref["f_total"]) ** 2).sum() / (ref["f_total"] ** 2).sum())
         assert err < 1e-5, (key, err)
@@ -116,3 +118,35 @@ def test_reference_energies_match_oracle(case):
     # per-atom energy sum = LJ + direct Coulomb
     assert get("atom_energy_sum") == pytest.approx(ref["e_lj"] + ref["e_direct"], rel=1e-4,
                                                     abs=1e-2)
+
+
+def test_reference_nb14_and_virtual_atoms_match_oracle(oracle_lib):
+    """The reference's NON_BOND_14 and VIRTUAL_INFORMATION on the real system against the FP64
+    oracle (tests/golden/make_covid.py): 1-4 forces, per-atom energies and virials, the 1-4
+    energy sums, the redistributed nonbonded forces and the refreshed virtual-atom positions."""
+    from sponge_b200 import nb14_pair_tables
+    s = covid_tip4p()
+    g = fixture("covid_tip4p")
+    uc = oracle_lib.crd_to_uint(oracle_lib.periodic_map(s["crd"], s["box"]), s["box"])
+    A, B = nb14_pair_tables(s["nb14_a"], s["nb14_b"], s["nb14_lj_scale"],
+                            np.float32(12.0) * s["lj_A"], np.float32(6.0) * s["lj_B"],
+                            s["lj_type"])
+    f, ae, av, elj, ecf = oracle_lib.nb14(uc, s["box"], s["charge"], s["nb14_a"], s["nb14_b"],
+                                          A, B, s["nb14_cf"])
+    at = g["nb14_atoms"]
+    rel = lambda a, b: float(np.sqrt(((np.asarray(a, np.float64) - b) ** 2).sum()  # noqa: E731
+                                     / (np.asarray(b, np.float64) ** 2).sum()))
+    assert rel(g["nb14_frc"], f[at]) < 1e-5
+    assert rel(g["nb14_ae"], ae[at]) < 1e-5
+    assert rel(g["nb14_av"], av[at]) < 1e-5
+    assert float(g["summary_nb14_lj"]) == pytest.approx(elj, rel=1e-5)
+    assert float(g["summary_nb14_cf"]) == pytest.approx(ecf, rel=1e-5)
+    fv = oracle_lib.vsite(uc, s["box"], s["vs_type"], s["vs_atoms"], s["vs_param"],
+                          frc=g["frc"].astype(np.float64))
+    assert rel(g["vs_frc"], fv) < 1e-6
+    crd = oracle_lib.periodic_map(s["crd"], s["box"]).astype(np.float64)
+    cv = oracle_lib.vsite(uc, s["box"], s["vs_type"], s["vs_atoms"], s["vs_param"], crd=crd)
+    L = np.asarray(s["box"], np.float64)
+    d = g["vs_crd"].astype(np.float64) - cv[s["vs_atoms"][:, 0]]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 1e-4

@@ -5,7 +5,8 @@ PME 112 x 96 x 96; tests/golden/make_covid.py).
 Checked: the pair set bit-exact against the oracle; LJ + PME forces of the fused step and of the
 module calls against the FP64 oracle (relative RMS <= 1e-5) and against the forces the
 reference's own CUDA modules produced on this input (tests/golden/reference_covid_tip4p.npz,
-<= 2e-5: both sides are FP32 within 1e-5 of FP64); energies and virial; bit-identical repeats.
+<= 2e-5: both sides are FP32 within 1e-5 of FP64); energies and virial; bit-identical repeats;
+the 1-4 pairs and virtual atoms against the oracle and the reference's modules.
 The grid's x size (112 = 2^4 7) has no register transform, so the generic FFT kernels run on
 that axis.
 """
@@ -110,4 +111,75 @@ def test_plain_form(covid, oracle_lib):
     pe.to_uint()
     f = _forces(pe, ("direct", "lrc", "excluded", "reciprocal"))
     assert rel_rms(f, ref["f_total"]) < 1e-5
-    assert rel_rms(f, golden["frc_plain"]) < 2e-5
+    assert rel_rms(f, golden["frc"]) < 2e-5
+
+
+# --- the modules beside the nonbonded path: 1-4 pairs and virtual atoms (SPONGE/main.cu:195,
+# :207, :375) ----------------------------------------------------------------------------------
+
+def _nb14_tables(s):
+    from sponge_b200 import nb14_pair_tables
+    return nb14_pair_tables(s["nb14_a"], s["nb14_b"], s["nb14_lj_scale"],
+                            np.float32(12.0) * s["lj_A"], np.float32(6.0) * s["lj_B"],
+                            s["lj_type"])
+
+
+def test_nb14(covid, oracle_lib):
+    s, eng, ref, golden, torch = covid
+    from sponge_b200 import NonBond14
+    A, B = _nb14_tables(s)
+    m = NonBond14(len(s["charge"]), s["nb14_a"], s["nb14_b"], A, B, s["nb14_cf"])
+    uc = eng.uint_crd.cpu().numpy().view(np.uint32)
+    f0, ae0, av0, elj, ecf = oracle_lib.nb14(uc, s["box"], s["charge"], s["nb14_a"],
+                                             s["nb14_b"], A, B, s["nb14_cf"])
+    n = len(s["charge"])
+    runs = []
+    for _ in range(2):
+        frc = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        ae = torch.zeros(n, dtype=torch.float32, device="cuda")
+        av = torch.zeros(n, dtype=torch.float32, device="cuda")
+        m.Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial(eng.uint_crd, eng.charge,
+                                                               eng.scaler, frc, ae, av)
+        runs.append((frc.cpu().numpy().astype(np.float64), ae.cpu().numpy().astype(np.float64),
+                     av.cpu().numpy().astype(np.float64)))
+    assert all(np.array_equal(x, y) for x, y in zip(runs[0], runs[1]))
+    f, ae, av = runs[0]
+    assert rel_rms(f, f0) < 1e-6
+    assert rel_rms(ae, ae0) < 1e-6
+    assert rel_rms(av, av0) < 1e-6
+    assert rel_rms(f[golden["nb14_atoms"]], golden["nb14_frc"]) < 1e-5
+    assert m.Get_14_LJ_Energy(eng.uint_crd, eng.scaler) == pytest.approx(elj, rel=1e-6)
+    assert m.Get_14_CF_Energy(eng.uint_crd, eng.charge, eng.scaler) == pytest.approx(ecf,
+                                                                                      rel=1e-6)
+
+
+def test_virtual_atoms(covid, oracle_lib):
+    s, eng, ref, golden, torch = covid
+    from sponge_b200 import VirtualAtoms
+    n = len(s["charge"])
+    vs = VirtualAtoms(n, s["vs_type"], s["vs_atoms"], s["vs_param"])
+    uc = eng.uint_crd.cpu().numpy().view(np.uint32)
+    # forces: the nonbonded forces with the virtual atoms' shares moved to their parents
+    frc = torch.tensor(ref["f_total"].astype(np.float32), device="cuda")
+    vs.Force_Redistribute(eng.uint_crd, eng.scaler, frc)
+    f = frc.cpu().numpy().astype(np.float64)
+    f0 = oracle_lib.vsite(uc, s["box"], s["vs_type"], s["vs_atoms"], s["vs_param"],
+                          frc=ref["f_total"].astype(np.float32).astype(np.float64))
+    assert rel_rms(f, f0) < 1e-6
+    assert np.all(f[s["vs_atoms"][:, 0]] == 0.0)
+    fg = oracle_lib.vsite(uc, s["box"], s["vs_type"], s["vs_atoms"], s["vs_param"],
+                          frc=golden["frc"].astype(np.float64))
+    assert rel_rms(golden["vs_frc"], fg) < 1e-6
+    # coordinates (compared modulo the box: a virtual atom sits beside its parent's image)
+    crd = eng.crd.clone()
+    vs.Coordinate_Refresh(eng.uint_crd, eng.scaler, crd)
+    c = crd.cpu().numpy().astype(np.float64)
+    c0 = oracle_lib.vsite(uc, s["box"], s["vs_type"], s["vs_atoms"], s["vs_param"],
+                          crd=eng.crd.cpu().numpy().astype(np.float64))
+    L = np.asarray(s["box"], np.float64)
+    d = c - c0
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 1e-4
+    dg = golden["vs_crd"].astype(np.float64) - c0[s["vs_atoms"][:, 0]]
+    dg -= L * np.round(dg / L)
+    assert np.abs(dg).max() < 1e-4
