@@ -1,5 +1,6 @@
-"""Writers for SPONGE's text input formats, so that a generated system can be run by an unchanged
-SPONGE driver (with the stock modules or with the sponge_b200 drop-ins).
+"""Readers and writers for SPONGE's text input formats: a generated system can be run by an
+unchanged SPONGE driver (with the stock modules or with the sponge_b200 drop-ins), and a SPONGE
+system (such as the reference's covid-tip4p) can be read into the system dict the engine takes.
 
 Formats (SPONGE/MD_core/MD_core.cu:1213-1257 coordinates, :1051-1080 charge, :308-351 exclude;
 SPONGE/Lennard_Jones_force/Lennard_Jones_force.cu:1082-1105 LJ; bond and residue files as in
@@ -113,3 +114,131 @@ def write_mdin(path, files, system, steps=10000, dt=0.002, refresh_interval=20,
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
     return path
+
+
+# ---------------------------------------------------------------------------------------------
+# readers
+# ---------------------------------------------------------------------------------------------
+def read_coordinate(path):
+    """Coordinate or restart file (MD_core.cu:1213-1257): first line "N" or "N time", N lines of
+    "x y z", then "Lx Ly Lz alpha beta gamma". Returns (crd [N,3] float32, box [3] float32)."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    n = int(lines[0].split()[0])
+    crd = np.array(" ".join(lines[1:1 + n]).split(), np.float64).reshape(n, 3)
+    box = np.array(lines[1 + n].split()[:3], np.float64)
+    return crd.astype(np.float32), box.astype(np.float32)
+
+
+def read_values(path):
+    """Per-atom value file (mass, charge; MD_core.cu:1051-1080): "N", then N numbers."""
+    tok = open(path).read().split()
+    n = int(tok[0])
+    return np.array(tok[1:1 + n], np.float32)
+
+
+def read_lj(path):
+    """LJ file (Lennard_Jones_force.cu:1082-1105): "N T", A and B over the T(T+1)/2 type pairs,
+    then the N types. Returns (A, B, types, T)."""
+    tok = open(path).read().split()
+    n, t = int(tok[0]), int(tok[1])
+    npair = t * (t + 1) // 2
+    A = np.array(tok[2:2 + npair], np.float32)
+    B = np.array(tok[2 + npair:2 + 2 * npair], np.float32)
+    types = np.array(tok[2 + 2 * npair:2 + 2 * npair + n], np.int32)
+    return A, B, types, t
+
+
+def read_exclude(path):
+    """Exclusion file (MD_core.cu:308-351): "N total", then per atom "count j1 j2 ...".
+    Returns the CSR (start, numbers, list)."""
+    tok = open(path).read().split()
+    n, total = int(tok[0]), int(tok[1])
+    numbers = np.zeros(n, np.int32)
+    lists = []
+    p = 2
+    for i in range(n):
+        c = int(tok[p])
+        numbers[i] = c
+        lists.append(np.array(tok[p + 1:p + 1 + c], np.int32))
+        p += 1 + c
+    lst = np.concatenate(lists) if lists else np.zeros(0, np.int32)
+    if lst.size != total:
+        raise ValueError("%s: %d exclusions listed, header says %d" % (path, lst.size, total))
+    start = np.zeros(n, np.int32)
+    start[1:] = np.cumsum(numbers)[:-1]
+    return start, numbers, lst.astype(np.int32)
+
+
+def read_nb14(path):
+    """1-4 file (nb14.cu:179-206): "count", then "a b lj_scale cf_scale" per pair.
+    Returns (a, b, lj_scale, cf_scale)."""
+    tok = open(path).read().split()
+    n = int(tok[0])
+    rows = np.array(tok[1:1 + 4 * n], np.float64).reshape(n, 4)
+    return (rows[:, 0].astype(np.int32), rows[:, 1].astype(np.int32),
+            rows[:, 2].astype(np.float32), rows[:, 3].astype(np.float32))
+
+
+def read_vatom(path):
+    """Virtual-atom file (virtual_atoms.cu:246-290): one "type v from_1 [from_2 from_3] params"
+    line per virtual atom. Returns (types [V], atoms [V,4], params [V,2]) as
+    sponge_b200.VirtualAtoms takes them (unused parents repeat from_1, unused params are 0)."""
+    npar = {0: 1, 1: 2, 2: 3, 3: 3}
+    nparam = {0: 1, 1: 1, 2: 2, 3: 2}
+    types, atoms, params = [], [], []
+    with open(path) as f:
+        for line in f:
+            w = line.split()
+            if len(w) < 2:
+                continue
+            t = int(w[0])
+            k = npar[t]
+            idx = [int(x) for x in w[1:2 + k]]
+            par = [float(x) for x in w[2 + k:2 + k + nparam[t]]]
+            types.append(t)
+            atoms.append(idx + [idx[1]] * (4 - len(idx)))
+            params.append(par + [0.0] * (2 - len(par)))
+    return (np.array(types, np.int32), np.array(atoms, np.int32).reshape(-1, 4),
+            np.array(params, np.float32).reshape(-1, 2))
+
+
+def write_nb14(path, a, b, lj_scale, cf_scale):
+    with open(path, "w") as f:
+        f.write("%d\n" % len(a))
+        for row in zip(a, b, lj_scale, cf_scale):
+            f.write("%d %d %.9g %.9g\n" % row)
+
+
+def write_vatom(path, types, atoms, params):
+    npar = {0: 1, 1: 2, 2: 3, 3: 3}
+    nparam = {0: 1, 1: 1, 2: 2, 3: 2}
+    with open(path, "w") as f:
+        for t, a, p in zip(types, np.asarray(atoms).reshape(-1, 4), np.asarray(params).reshape(-1, 2)):
+            t = int(t)
+            f.write(" ".join([str(t)] + [str(int(x)) for x in a[:1 + npar[t]]] +
+                             ["%.9g" % x for x in p[:nparam[t]]]) + "\n")
+
+
+def read_system(directory, prefix, coordinate=None, cutoff=10.0, skin=2.0, tolerance=1e-5,
+                fft=None):
+    """A SPONGE input set (prefix_coordinate/charge/LJ/exclude[/nb14/vatom].txt) as the system
+    dict sponge_b200.systems builds; ``coordinate`` overrides the coordinate file (a restart).
+    Files that are absent are left out (no 1-4 pairs or virtual atoms)."""
+    p = lambda name: os.path.join(directory, "%s_%s.txt" % (prefix, name))  # noqa: E731
+    crd, box = read_coordinate(coordinate or p("coordinate"))
+    charge = read_values(p("charge"))
+    lj = p("LJ") if os.path.exists(p("LJ")) else p("lj")
+    A, B, types, t = read_lj(lj)
+    start, numbers, lst = read_exclude(p("exclude"))
+    box64 = box.astype(np.float64)
+    crd = np.mod(crd.astype(np.float64), box64)
+    crd = np.where(crd >= box64, 0.0, crd).astype(np.float32)
+    s = dict(name=prefix, crd=crd, charge=charge, lj_type=types, n_types=t, lj_A=A, lj_B=B,
+             excl_start=start, excl_numbers=numbers, excl_list=lst, box=box,
+             cutoff=float(cutoff), skin=float(skin), fft=fft, tolerance=float(tolerance))
+    if os.path.exists(p("nb14")):
+        s["nb14_a"], s["nb14_b"], s["nb14_lj_scale"], s["nb14_cf"] = read_nb14(p("nb14"))
+    if os.path.exists(p("vatom")):
+        s["vs_type"], s["vs_atoms"], s["vs_param"] = read_vatom(p("vatom"))
+    return s

@@ -38,71 +38,25 @@ SOURCE = "/root/reference/SPONGE/covid-tip4p"
 FFT = (112, 96, 96)
 
 
-def _numbers(path):
-    with open(path) as f:
-        return f.read().split()
-
-
 def read_reference_files(src=SOURCE, prefix="covid-tip4p", coordinates="npt_coordinate.txt"):
-    """The LJ + PME inputs of the reference's covid-tip4p system, as arrays. The coordinates are
-    the equilibrated ones the reference ships beside the topology (npt_coordinate.txt): the
-    starting structure (covid-tip4p_coordinate.txt) still has clashes of 0.34 A between
-    non-excluded atoms, whose 1e12 kcal/mol/A forces would swamp any comparison."""
-    # first line: the atom count (and, in a written restart, the simulation time); then one
-    # "x y z" line per atom; then "Lx Ly Lz alpha beta gamma"
-    with open(os.path.join(src, coordinates)) as f:
-        lines = f.read().split("\n")
-    n = int(lines[0].split()[0])
-    crd = np.array(" ".join(lines[1:1 + n]).split(), np.float64).reshape(n, 3)
-    box = np.array(lines[1 + n].split()[:3], np.float64)
-    tok = _numbers(os.path.join(src, prefix + "_charge.txt"))
-    assert int(tok[0]) == n
-    charge = np.array(tok[1:1 + n], np.float32)
-    tok = _numbers(os.path.join(src, prefix + "_lj.txt"))
-    assert int(tok[0]) == n
-    t = int(tok[1])
-    npair = t * (t + 1) // 2
-    A = np.array(tok[2:2 + npair], np.float32)
-    B = np.array(tok[2 + npair:2 + 2 * npair], np.float32)
-    lj_type = np.array(tok[2 + 2 * npair:2 + 2 * npair + n], np.int32)
-    tok = _numbers(os.path.join(src, prefix + "_exclude.txt"))
-    assert int(tok[0]) == n
-    total = int(tok[1])
-    numbers = np.zeros(n, np.int32)
-    lists = []
-    p = 2
-    for i in range(n):
-        c = int(tok[p])
-        numbers[i] = c
-        lists.append(np.array(tok[p + 1:p + 1 + c], np.int32))
-        p += 1 + c
-    excl_list = np.concatenate(lists) if lists else np.zeros(0, np.int32)
-    assert excl_list.size == total
-    # 1-4 pairs (nb14.cu:179-206): "count", then "a b lj_scale cf_scale" per pair
-    tok = _numbers(os.path.join(src, prefix + "_nb14.txt"))
-    n14 = int(tok[0])
-    rows = np.array(tok[1:1 + 4 * n14], np.float64).reshape(n14, 4)
-    # virtual atoms (virtual_atoms.cu:246-290): "type v from... params" per line
-    vt, va, vp = [], [], []
-    npar = {0: 1, 1: 2, 2: 3, 3: 3}
-    with open(os.path.join(src, prefix + "_vatom.txt")) as f:
-        for line in f:
-            w = line.split()
-            if len(w) < 2:
-                continue
-            vtype = int(w[0])
-            k = npar[vtype]
-            idx = [int(x) for x in w[1:2 + k]]
-            par = [float(x) for x in w[2 + k:]] + [0.0]
-            vt.append(vtype)
-            va.append(idx + [idx[1]] * (4 - len(idx)))
-            vp.append(par[:2])
-    return dict(crd=crd.astype(np.float32), box=box.astype(np.float32), charge=charge,
-                lj_A=A, lj_B=B, lj_type=lj_type, n_types=np.int32(t), excl_numbers=numbers,
-                excl_list=excl_list, nb14_a=rows[:, 0].astype(np.int32),
-                nb14_b=rows[:, 1].astype(np.int32), nb14_lj_scale=rows[:, 2].astype(np.float32),
-                nb14_cf=rows[:, 3].astype(np.float32), vs_type=np.array(vt, np.int32),
-                vs_atoms=np.array(va, np.int32), vs_param=np.array(vp, np.float32))
+    """The LJ + PME inputs of the reference's covid-tip4p system, as arrays, read with
+    sponge_b200.sponge_io. The coordinates are the equilibrated ones the reference ships beside
+    the topology (npt_coordinate.txt): the starting structure (covid-tip4p_coordinate.txt) still
+    has clashes of 0.34 A between non-excluded atoms, whose 1e12 kcal/mol/A forces would swamp any
+    comparison."""
+    sys.path.insert(0, ROOT)
+    from sponge_b200 import sponge_io
+    p = lambda name: os.path.join(src, "%s_%s.txt" % (prefix, name))  # noqa: E731
+    crd, box = sponge_io.read_coordinate(os.path.join(src, coordinates))
+    charge = sponge_io.read_values(p("charge"))
+    A, B, lj_type, t = sponge_io.read_lj(p("lj"))
+    _, numbers, excl_list = sponge_io.read_exclude(p("exclude"))
+    a14, b14, ljs14, cf14 = sponge_io.read_nb14(p("nb14"))
+    vt, va, vp = sponge_io.read_vatom(p("vatom"))
+    return dict(crd=crd, box=box, charge=charge, lj_A=A, lj_B=B, lj_type=lj_type,
+                n_types=np.int32(t), excl_numbers=numbers, excl_list=excl_list, nb14_a=a14,
+                nb14_b=b14, nb14_lj_scale=ljs14, nb14_cf=cf14, vs_type=vt, vs_atoms=va,
+                vs_param=vp)
 
 
 def load_system(path=INPUTS):
