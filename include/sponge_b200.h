@@ -323,6 +323,46 @@ SB_API int sb_vsite_coordinate_refresh(sb_vsite* vsite, const uint32_t* d_uint_c
 SB_API int sb_vsite_force_redistribute(sb_vsite* vsite, const uint32_t* d_uint_crd,
                                        const float scaler[3], float* d_frc, void* stream);
 
+/* ------------------------------------------------------------------------------------------
+ * Integration with rigid-water constraints: the NVE leap-frog of MD_INFORMATION
+ * (SPONGE/MD_core/MD_core.cu:13-32) and SETTLE (SPONGE/constrain/SETTLE.cuh:33-64), in
+ * Main_Iteration's order (SPONGE/main.cu:283-325). dt is the integrator's internal time step
+ * (MD_INFORMATION::dt: the mdin dt in ps times SPONGE's time unit conversion).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct sb_settle sb_settle;
+
+/* SETTLE::Initial (SETTLE.cu:183-354) from CONSTRAIN's pair list (atom i, atom j, length r, in
+ * CONSTRAIN's order; CONSTRAIN::Add_HBond_To_Constrain_Pair puts there every bond with an atom
+ * lighter than 3.3): closed triangles of constrained pairs become rigid triangles, isolated
+ * pairs rigid pairs, the rest is left to another constraint scheme (counted by sb_settle_info).
+ * exp_gamma is the thermostat's velocity factor (1 for NVE), as CONSTRAIN::Initial_Constrain
+ * takes it. */
+SB_API int sb_settle_create(int atom_numbers, int constrain_pair_numbers, const int* h_pair_i,
+                            const int* h_pair_j, const float* h_pair_r, const float* h_mass,
+                            float dt, float exp_gamma, sb_settle** out);
+SB_API int sb_settle_destroy(sb_settle* settle);
+SB_API int sb_settle_info(sb_settle* settle, int* h_triangles, int* h_pairs, int* h_remaining);
+/* SETTLE::Remember_Last_Coordinates: edge vectors of the step start (fixed point). */
+SB_API int sb_settle_remember(sb_settle* settle, const uint32_t* d_uint_crd,
+                              const float scaler[3], void* stream);
+/* SETTLE::Do_SETTLE: constrain crd and vel after the integrator; with need_pressure the
+ * constraint virial / (3V) is added to *d_pressure. */
+SB_API int sb_settle_apply(sb_settle* settle, const float* d_mass, float* d_crd,
+                           const float box[3], float* d_vel, int need_pressure,
+                           float* d_pressure, void* stream);
+/* MD_INFORMATION::NVE_iteration::Leap_Frog (MD_core.cu:1535-1547): acc = F/m, vel += dt acc,
+ * crd += dt vel (d_acc may be NULL). */
+SB_API int sb_md_leap_frog(int atom_numbers, const float* d_inverse_mass, const float* d_frc,
+                           float* d_vel, float* d_crd, float* d_acc, float dt, void* stream);
+/* Remember + leap-frog + SETTLE in one launch (no reference counterpart as one call; the
+ * same bits as the three calls in sequence). Refuses a system whose constraints are not all
+ * rigid triangles or pairs. */
+SB_API int sb_md_nve_settle_step(sb_settle* settle, const uint32_t* d_uint_crd,
+                                 const float scaler[3], const float* d_inverse_mass,
+                                 const float* d_mass, const float* d_frc, float* d_vel,
+                                 float* d_crd, float* d_acc, const float box[3],
+                                 int need_pressure, float* d_pressure, void* stream);
+
 /* Crd_To_Uint_Crd (SPONGE/common.cu:264-287) with the quarter coefficient 0.25*2^32/L, as
  * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */
 SB_API int sb_crd_to_uint_crd(int atom_numbers, const float box_length[3], const float* d_crd,

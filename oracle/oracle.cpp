@@ -24,6 +24,9 @@
 //   * FFT grid size                  SPONGE/common.cu:467-534 (Get_Fft_Patameter)
 //   * 1-4 pairs                      SPONGE/nb14/nb14.cu:92-170 (force, energy, virial),
 //                                    :5-91 (energies), :203-217 (per-pair A, B)
+//   * NVE leap-frog + SETTLE         SPONGE/MD_core/MD_core.cu:13-32, SPONGE/constrain/SETTLE.cu
+//                                    :7-41 (triangle geometry), :93-176 (triangle), :183-305
+//                                    (rigid triangles and pairs), :349-414 (kernels)
 //   * virtual atoms                  SPONGE/virtual_atoms/virtual_atoms.cu:2-73 (positions),
 //                                    :75-180 (force redistribution), :246-290 + :495-530
 //                                    (levels and their order)
@@ -47,6 +50,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <vector>
 #include <thread>
 #include <vector>
 
@@ -1013,6 +1017,205 @@ void orc_vsite(int nv, const int* type, const int* atoms, const float* param, co
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// NVE leap-frog + SETTLE in FP64 (one step): crd, vel updated in place; acc written; the
+// constraint virial sum returned in out[0]. Constraint pairs (i, j, r) in CONSTRAIN's order.
+// ---------------------------------------------------------------------------------------------
+struct OTri { int A, B, C; double ra, rb, rc, rd, re; };
+struct OPair { int i, j; double r, k; };
+
+static void o_rabcde(double rAB, double rAC, double rBC, double mA, double mB, double mC,
+                     double& ra, double& rb, double& rc, double& rd, double& re) {
+    const double mT = mA + mB + mC;
+    double Ax = 0, Ay = 0, Bx = -rAB, By = 0;
+    double c = (rBC * rBC - rAC * rAC - rAB * rAB) / (2 * rAC * rAB);
+    double Cx = rAC * c, Cy = rAC * std::sqrt(1.0 - c * c);
+    const double Ox = (Bx * mB + Cx * mC) / mT, Oy = Cy * mC / mT;
+    Ax -= Ox; Ay -= Oy; Bx -= Ox; By -= Oy; Cx -= Ox; Cy -= Oy;
+    c = 1.0 / std::sqrt(1.0 + Ax * Ax / Ay / Ay);
+    const double sn = c * Ax / Ay;
+    ra = Ax * sn + Ay * c;
+    rc = Bx * c - By * sn;
+    rb = Bx * sn + By * c;
+    rd = Cx * c - Cy * sn;
+    re = Cx * sn + Cy * c;
+    if (ra < 0) { ra = -ra; rb = -rb; re = -re; }
+}
+
+static inline void o_fdisp(const double* a, const double* b, const double* L, double d[3]) {
+    for (int k = 0; k < 3; k++) {
+        d[k] = a[k] - b[k];
+        d[k] -= std::floor(d[k] / L[k] + 0.5) * L[k];
+    }
+}
+static inline void o_cross(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+static inline double o_dot(const double* a, const double* b) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+static inline void o_unit(double* a) {
+    const double r = 1.0 / std::sqrt(o_dot(a, a));
+    for (int k = 0; k < 3; k++) a[k] *= r;
+}
+
+int orc_nve_settle(int n, int np, const int* pi, const int* pj, const float* pr,
+                   const float* mass, const uint32_t* uc, const float* box, double dt,
+                   double exp_gamma, const double* frc, double* crd, double* vel, double* acc,
+                   double* out) {
+    // SETTLE::Initial (SETTLE.cu:194-305)
+    std::vector<int> num(n, 0), link(2 * (size_t)n, -1);
+    std::vector<double> lr(3 * (size_t)n, 0.0);
+    for (int p = 0; p < np; p++) {
+        const int a = pi[p], b = pj[p];
+        if (num[a] < 2 && num[b] < 2) {
+            link[2 * a + num[a]] = b; link[2 * b + num[b]] = a;
+            lr[3 * a + num[a]] = pr[p]; lr[3 * b + num[b]] = pr[p];
+            num[a]++; num[b]++;
+        } else { num[a] = 3; num[b] = 3; }
+    }
+    for (int i = 0; i < n; i++) {
+        if (num[i] == 2) {
+            const int a = link[2 * i], b = link[2 * i + 1];
+            if (num[a] == 2 && num[b] == 2 &&
+                ((link[2 * a] == i && link[2 * a + 1] == b) || (link[2 * a + 1] == i && link[2 * a] == b))) {
+                num[a] = -2; num[b] = -2;
+                lr[3 * i + 2] = link[2 * a + 1] == b ? lr[3 * a + 1] : lr[3 * a];
+            } else { num[i] = 3; num[a] = 3; num[b] = 3; }
+        } else if (num[i] == 1) {
+            const int a = link[2 * i];
+            if (num[a] == 1) num[a] = -1;
+            else { num[i] = 3; num[a] = 3; }
+        }
+    }
+    std::vector<OTri> tri;
+    std::vector<OPair> prs;
+    for (int i = 0; i < n; i++) {
+        if (num[i] == 2) {
+            OTri T;
+            T.A = i; T.B = link[2 * i]; T.C = link[2 * i + 1];
+            o_rabcde(lr[3 * i], lr[3 * i + 1], lr[3 * i + 2], mass[T.A], mass[T.B], mass[T.C],
+                     T.ra, T.rb, T.rc, T.rd, T.re);
+            tri.push_back(T);
+            num[i] = -2;
+        }
+        if (num[i] == 1) {
+            OPair P;
+            P.i = i; P.j = link[2 * i]; P.r = lr[3 * i];
+            P.k = 1.0 / ((double)mass[P.i] + (double)mass[P.j]);
+            prs.push_back(P);
+            num[i] = -1;
+        }
+    }
+    float s[3];
+    scaler_of(box, s);
+    const double L[3] = {box[0], box[1], box[2]};
+    // Remember_Last_Coordinates (SETTLE.cu:355-395)
+    std::vector<double> last(6 * tri.size() + 3 * prs.size());
+    for (size_t t = 0; t < tri.size(); t++) {
+        dr_f64(uc + 3 * (size_t)tri[t].A, uc + 3 * (size_t)tri[t].B, s, &last[6 * t]);
+        dr_f64(uc + 3 * (size_t)tri[t].A, uc + 3 * (size_t)tri[t].C, s, &last[6 * t + 3]);
+    }
+    for (size_t p = 0; p < prs.size(); p++)
+        dr_f64(uc + 3 * (size_t)prs[p].i, uc + 3 * (size_t)prs[p].j, s, &last[6 * tri.size() + 3 * p]);
+    // leap-frog (MD_core.cu:13-32)
+    for (int i = 0; i < n; i++) {
+        const double im = mass[i] > 0 ? 1.0 / (double)mass[i] : 0.0;
+        for (int k = 0; k < 3; k++) {
+            const double a = im * frc[3 * (size_t)i + k];
+            acc[3 * (size_t)i + k] = a;
+            vel[3 * (size_t)i + k] += dt * a;
+            crd[3 * (size_t)i + k] += dt * vel[3 * (size_t)i + k];
+        }
+    }
+    const double vf = exp_gamma, xf = 0.5 * (1.0 + exp_gamma);
+    double vir = 0.0;
+    // settle_pair (SETTLE.cu:381-414)
+    for (size_t p = 0; p < prs.size(); p++) {
+        const OPair& P = prs[p];
+        const double* r2 = &last[6 * tri.size() + 3 * p];
+        double r1[3];
+        o_fdisp(&crd[3 * (size_t)P.j], &crd[3 * (size_t)P.i], L, r1);
+        const double mA = mass[P.i], mB = mass[P.j];
+        const double r0r0 = P.r * P.r, r1r1 = o_dot(r1, r1), r1r2 = o_dot(r1, r2), r2r2 = o_dot(r2, r2);
+        const double k = (std::sqrt(r1r2 * r1r2 - r1r1 * r2r2 + r2r2 * r0r0) - r1r2) / r2r2;
+        const double kv = vf / dt / xf;
+        for (int d = 0; d < 3; d++) {
+            const double kr2 = k * r2[d];
+            const double di = -mB * P.k * kr2, dj = mA * P.k * kr2;
+            crd[3 * (size_t)P.i + d] += di;
+            crd[3 * (size_t)P.j + d] += dj;
+            vel[3 * (size_t)P.i + d] += kv * di;
+            vel[3 * (size_t)P.j + d] += kv * dj;
+            vir += (kv * mB / dt / vf * dj) * r2[d];
+        }
+    }
+    // settle_triangle (SETTLE.cu:349-380) + SETTLE_DO_TRIANGLE (:93-176)
+    for (size_t t = 0; t < tri.size(); t++) {
+        const OTri& T = tri[t];
+        const double* rB0 = &last[6 * t];
+        const double* rC0 = &last[6 * t + 3];
+        double rA[3], rB[3], rC[3], rO[3];
+        for (int d = 0; d < 3; d++) rA[d] = crd[3 * (size_t)T.A + d];
+        o_fdisp(&crd[3 * (size_t)T.B], rA, L, rB);
+        o_fdisp(&crd[3 * (size_t)T.C], rA, L, rC);
+        const double mA = mass[T.A], mB = mass[T.B], mC = mass[T.C];
+        for (int d = 0; d < 3; d++) {
+            rO[d] = (mB * rB[d] + mC * rC[d]) / (mA + mB + mC) + rA[d];
+            rA[d] -= rO[d];
+            rB[d] += rA[d];
+            rC[d] += rA[d];
+        }
+        double bz[3], bx[3], by[3];
+        o_cross(rB0, rC0, bz);
+        o_cross(rA, bz, bx);
+        o_cross(bz, bx, by);
+        o_unit(bx); o_unit(by); o_unit(bz);
+        const double B0x = o_dot(bx, rB0), B0y = o_dot(by, rB0);
+        const double C0x = o_dot(bx, rC0), C0y = o_dot(by, rC0);
+        const double A1z = o_dot(bz, rA);
+        const double B1x = o_dot(bx, rB), B1y = o_dot(by, rB), B1z = o_dot(bz, rB);
+        const double C1x = o_dot(bx, rC), C1y = o_dot(by, rC), C1z = o_dot(bz, rC);
+        const double sinphi = A1z / T.ra, cosphi = std::sqrt(1.0 - sinphi * sinphi);
+        const double sinpsi = (B1z - C1z - (T.rb - T.re) * sinphi) / ((T.rd - T.rc) * cosphi);
+        const double cospsi = std::sqrt(1.0 - sinpsi * sinpsi);
+        const double A2y = T.ra * cosphi;
+        const double B2x = T.rc * cospsi, B2y = T.rb * cosphi + T.rc * sinpsi * sinphi;
+        const double C2x = T.rd * cospsi, C2y = T.re * cosphi + T.rd * sinpsi * sinphi;
+        const double alpha = B2x * B0x + C2x * C0x + B2y * B0y + C2y * C0y;
+        const double beta = -B2x * B0y - C2x * C0y + B2y * B0x + C2y * C0x;
+        const double gamma = B1y * B0x - B1x * B0y + C1y * C0x - C1x * C0y;
+        const double ab = alpha * alpha + beta * beta;
+        const double st = (alpha * gamma - beta * std::sqrt(ab - gamma * gamma)) / ab;
+        const double ct = std::sqrt(1.0 - st * st);
+        const double A3[3] = {-A2y * st, A2y * ct, A1z};
+        const double B3[3] = {B2x * ct - B2y * st, B2x * st + B2y * ct, B1z};
+        const double C3[3] = {C2x * ct - C2y * st, C2x * st + C2y * ct, C1z};
+        double nA[3], nB[3], nC[3];
+        for (int d = 0; d < 3; d++) {
+            nA[d] = A3[0] * bx[d] + A3[1] * by[d] + A3[2] * bz[d];
+            nB[d] = B3[0] * bx[d] + B3[1] * by[d] + B3[2] * bz[d];
+            nC[d] = C3[0] * bx[d] + C3[1] * by[d] + C3[2] * bz[d];
+        }
+        const double kv = vf / dt / xf, kf = 1.0 / dt / dt / xf;
+        for (int d = 0; d < 3; d++) {
+            vel[3 * (size_t)T.A + d] += kv * (nA[d] - rA[d]);
+            vel[3 * (size_t)T.B + d] += kv * (nB[d] - rB[d]);
+            vel[3 * (size_t)T.C + d] += kv * (nC[d] - rC[d]);
+            vir += kf * mB * (nB[d] - rB[d]) * rB0[d] + kf * mC * (nC[d] - rC[d]) * rC0[d];
+            crd[3 * (size_t)T.A + d] = nA[d] + rO[d];
+            crd[3 * (size_t)T.B + d] = nB[d] + rO[d];
+            crd[3 * (size_t)T.C + d] = nC[d] + rO[d];
+        }
+    }
+    out[0] = vir;
+    out[1] = (double)tri.size();
+    out[2] = (double)prs.size();
+    return 0;
 }
 
 }  // extern "C"

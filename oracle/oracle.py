@@ -77,6 +77,9 @@ def lib():
                                _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f64p]
         L.orc_vsite.argtypes = [ctypes.c_int, _i32p, _i32p, _f32p, _i32p, ctypes.c_int, _u32p,
                                 _f32p, ctypes.c_int, _f64p, _f64p]
+        L.orc_nve_settle.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f32p, _f32p,
+                                     _u32p, _f32p, ctypes.c_double, ctypes.c_double, _f64p,
+                                     _f64p, _f64p, _f64p, _f64p]
         L.orc_threads.restype = ctypes.c_int
         L.orc_set_threads.argtypes = [ctypes.c_int]
         _LIB = L
@@ -441,3 +444,22 @@ def vsite(uc, box, types, atoms, params, crd=None, frc=None):
     lib().orc_vsite(t.size, t, a, p, lv, ml, np.ascontiguousarray(uc, np.uint32).reshape(-1),
                     np.ascontiguousarray(box, np.float32), mode, c, f)
     return (c if mode == 0 else f).reshape(n, 3)
+
+
+def nve_settle(uc, box, pair_i, pair_j, pair_r, mass, dt, frc, crd, vel, exp_gamma=1.0):
+    """One NVE leap-frog step with SETTLE in FP64 (SPONGE/MD_core/MD_core.cu:13-32,
+    SPONGE/constrain/SETTLE.cu). Returns (crd, vel, acc, constraint virial, triangles, pairs)."""
+    n = uc.shape[0]
+    c = np.ascontiguousarray(crd, np.float64).reshape(-1).copy()
+    v = np.ascontiguousarray(vel, np.float64).reshape(-1).copy()
+    a = np.zeros(3 * n, np.float64)
+    out = np.zeros(3, np.float64)
+    i = np.ascontiguousarray(pair_i, np.int32)
+    lib().orc_nve_settle(n, i.size, i, np.ascontiguousarray(pair_j, np.int32),
+                         np.ascontiguousarray(pair_r, np.float32),
+                         np.ascontiguousarray(mass, np.float32),
+                         np.ascontiguousarray(uc, np.uint32).reshape(-1),
+                         np.ascontiguousarray(box, np.float32), float(dt), float(exp_gamma),
+                         np.ascontiguousarray(frc, np.float64).reshape(-1), c, v, a, out)
+    return (c.reshape(n, 3), v.reshape(n, 3), a.reshape(n, 3), float(out[0]), int(out[1]),
+            int(out[2]))

@@ -11,13 +11,18 @@
 //         int32 excl_start[N], excl_numbers[N], excl_list[nexcl]
 //         optional, after that: int32 n14, a[n14], b[n14], float lj_scale[n14], cf[n14];
 //         int32 nv, type[nv], atoms[4 nv], float param[2 nv] (the 1-4 pairs and virtual atoms,
-//         run through NON_BOND_14 and VIRTUAL_INFORMATION when present)
+//         run through NON_BOND_14 and VIRTUAL_INFORMATION when present); int32 nbond,
+//         a[nbond], b[nbond], float r0[nbond], mass[N], vel[3N], dt (internal unit), with
+//         which CONSTRAIN (bonds to atoms lighter than 3.3) and SETTLE run one NVE step on the
+//         nonbonded forces (after the virtual-atom redistribution when there are virtual atoms)
 // outputs (outdir): frc.f32 [3N] force of one evaluation with energy and virial requested,
 //         frc_plain.f32 [3N] force-only evaluation, pairs.i64 (sorted keys i*N+j),
 //         summary.txt (key value lines); with 1-4 pairs: nb14_frc.f32 [3N], nb14_ae.f32 [N],
 //         nb14_av.f32 [N] (Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial from zero);
 //         with virtual atoms: vs_frc.f32 [3N] (frc.f32 after Force_Redistribute),
-//         vs_crd.f32 [3N] (the wrapped coordinates after Coordinate_Refresh)
+//         vs_crd.f32 [3N] (the wrapped coordinates after Coordinate_Refresh); with bonds:
+//         settle_crd.f32 / settle_vel.f32 [3N] after Remember_Last_Coordinates, the leap-frog
+//         of MD_core.cu:13-32 and Do_SETTLE, and settle_pressure in summary.txt
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -29,6 +34,8 @@
 #include "common.cuh"
 #include "control.cuh"
 #include "Lennard_Jones_force/Lennard_Jones_force.cuh"
+#include "constrain/SETTLE.cuh"
+#include "constrain/constrain.cuh"
 #include "PME_force/PME_force.cuh"
 #include "nb14/nb14.cuh"
 #include "neighbor_list/neighbor_list.cuh"
@@ -70,6 +77,24 @@ static void wr(const char* dir, const char* name, const void* p, size_t bytes) {
     }
     fwrite(p, 1, bytes, f);
     fclose(f);
+}
+
+// MD_Iteration_Leap_Frog (SPONGE/MD_core/MD_core.cu:13-32) is file-static in the reference, so
+// the harness states it again, operation for operation
+__global__ void harness_leap_frog(const int atom_numbers, VECTOR* vel, VECTOR* crd, VECTOR* frc,
+                                  VECTOR* acc, const float* inverse_mass, const float dt) {
+    int i = blockDim.x * blockIdx.x + threadIdx.x;
+    if (i < atom_numbers) {
+        acc[i].x = inverse_mass[i] * frc[i].x;
+        acc[i].y = inverse_mass[i] * frc[i].y;
+        acc[i].z = inverse_mass[i] * frc[i].z;
+        vel[i].x = vel[i].x + dt * acc[i].x;
+        vel[i].y = vel[i].y + dt * acc[i].y;
+        vel[i].z = vel[i].z + dt * acc[i].z;
+        crd[i].x = crd[i].x + dt * vel[i].x;
+        crd[i].y = crd[i].y + dt * vel[i].y;
+        crd[i].z = crd[i].z + dt * vel[i].z;
+    }
 }
 
 int main(int argc, char** argv) {
@@ -117,6 +142,23 @@ int main(int argc, char** argv) {
         rd(f, vtype.data(), nv);
         rd(f, vatoms.data(), vatoms.size());
         rd(f, vparam.data(), vparam.size());
+    }
+    int nbond = 0;
+    std::vector<int> bond_a, bond_b;
+    std::vector<float> bond_r, mass, vel;
+    float md_dt = 0.f;
+    if (fread(&nbond, sizeof(int), 1, f) == 1 && nbond > 0) {
+        bond_a.resize(nbond);
+        bond_b.resize(nbond);
+        bond_r.resize(nbond);
+        mass.resize(N);
+        vel.resize(3 * (size_t)N);
+        rd(f, bond_a.data(), nbond);
+        rd(f, bond_b.data(), nbond);
+        rd(f, bond_r.data(), nbond);
+        rd(f, mass.data(), N);
+        rd(f, vel.data(), vel.size());
+        rd(f, &md_dt, 1);
     }
     fclose(f);
     el.resize(NE);
@@ -309,6 +351,44 @@ int main(int argc, char** argv) {
         CK(cudaDeviceSynchronize());
         CK(cudaMemcpy(cv.data(), d_crd, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost));
         wr(argv[2], "vs_crd.f32", cv.data(), sizeof(float) * cv.size());
+        h = fv;  // the integrator below takes the redistributed forces
+    }
+    float settle_pressure = 0.f;
+    if (nbond > 0) {
+        // CONSTRAIN + SETTLE as main.cu:92-103 set them up for an NVE run (exp_gamma 1)
+        CONSTRAIN constrain;
+        constrain.Add_HBond_To_Constrain_Pair(&controller, nbond, bond_a.data(), bond_b.data(),
+                                              bond_r.data(), mass.data());
+        // no angle constraints: main.cu:95 adds them only under the constrain_angle command
+        int freedom = 3 * N;
+        constrain.Initial_Constrain(&controller, N, md_dt, box, 1.0f, 0, mass.data(), &freedom);
+        SETTLE settle;
+        settle.Initial(&controller, &constrain, mass.data());
+        // the coordinates of this evaluation (wrapped), their fixed point, the forces h
+        CK(cudaMemcpy(d_crd, crd.data(), sizeof(float) * 3 * N, cudaMemcpyHostToDevice));
+        Crd_Periodic_Map<<<(N + 127) / 128, 128>>>(N, d_crd, box);
+        Crd_To_Uint_Crd<<<(N + 127) / 128, 128>>>(N, quarter, d_crd, d_uc);
+        std::vector<float> inv(N);
+        for (int i = 0; i < N; i++) inv[i] = mass[i] == 0 ? 0.0f : (float)(1.0 / mass[i]);  // MD_core.cu:952-955
+        float* d_mass = dev_copy(mass);
+        float* d_inv = dev_copy(inv);
+        float* d_vel = dev_copy(vel);
+        float* d_f = dev_copy(h);
+        float* d_acc = nullptr;
+        CK(cudaMalloc((void**)&d_acc, sizeof(float) * 3 * N));
+        cudaMemset(d_pot, 0, sizeof(float));
+        settle.Remember_Last_Coordinates(d_uc, scaler);
+        harness_leap_frog<<<(N + 127) / 128, 128>>>(N, (VECTOR*)d_vel, (VECTOR*)d_crd,
+                                                     (VECTOR*)d_f, (VECTOR*)d_acc, d_inv, md_dt);
+        settle.Do_SETTLE(d_mass, (VECTOR*)d_crd, box, (VECTOR*)d_vel, 1, d_pot);
+        CK(cudaDeviceSynchronize());
+        std::vector<float> sc(3 * (size_t)N), sv(3 * (size_t)N);
+        CK(cudaMemcpy(sc.data(), d_crd, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(sv.data(), d_vel, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&settle_pressure, d_pot, sizeof(float), cudaMemcpyDeviceToHost));
+        wr(argv[2], "settle_crd.f32", sc.data(), sizeof(float) * sc.size());
+        wr(argv[2], "settle_vel.f32", sv.data(), sizeof(float) * sv.size());
+        printf("settle: %d triangles, %d pairs\n", settle.triangle_numbers, settle.pair_numbers);
     }
 
     double ms_step = -1, ms_force = -1;
@@ -353,6 +433,7 @@ int main(int argc, char** argv) {
             timing_steps);
     fprintf(s, "nb14_pairs %d\nnb14_lj %.9g\nnb14_cf %.9g\nvirtual_atoms %d\n", n14, e14_lj,
             e14_cf, nv);
+    fprintf(s, "bonds %d\nsettle_pressure %.9g\n", nbond, settle_pressure);
     fclose(s);
     printf("harness done: %d atoms, %zu pairs\n", N, keys.size());
     return 0;

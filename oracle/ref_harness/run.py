@@ -67,6 +67,16 @@ def write_input(path, system, max_nb, max_grid, refresh_interval=20):
             vt.tofile(f)
             np.asarray(system["vs_atoms"], np.int32).reshape(-1).tofile(f)
             np.asarray(system["vs_param"], np.float32).reshape(-1).tofile(f)
+        # optional bonds, masses, velocities and time step for one CONSTRAIN + SETTLE step
+        ba = np.asarray(system.get("bond_a", np.zeros(0)), np.int32)
+        np.array([ba.size], np.int32).tofile(f)
+        if ba.size:
+            ba.tofile(f)
+            np.asarray(system["bond_b"], np.int32).tofile(f)
+            np.asarray(system["bond_r"], np.float32).tofile(f)
+            np.asarray(system["mass"], np.float32).tofile(f)
+            np.asarray(system["vel"], np.float32).reshape(-1).tofile(f)
+            np.array([system["md_dt"]], np.float32).tofile(f)
 
 
 def run(system, uc, pair_keys, timing_steps=0, outdir=None, timeout=900):
@@ -91,7 +101,8 @@ def run(system, uc, pair_keys, timing_steps=0, outdir=None, timeout=900):
         pairs=np.fromfile(os.path.join(outdir, "pairs.i64"), np.int64),
         summary=summ, capacities=(max_nb, max_grid), outdir=outdir)
     for name, shape in (("nb14_frc", (n, 3)), ("nb14_ae", (n,)), ("nb14_av", (n,)),
-                        ("vs_frc", (n, 3)), ("vs_crd", (n, 3))):
+                        ("vs_frc", (n, 3)), ("vs_crd", (n, 3)), ("settle_crd", (n, 3)),
+                        ("settle_vel", (n, 3))):
         path = os.path.join(outdir, name + ".f32")
         if os.path.exists(path):
             out[name] = np.fromfile(path, np.float32).reshape(shape)

@@ -99,6 +99,13 @@ _SIGS = {
     "sb_vsite_destroy": [_vp],
     "sb_vsite_coordinate_refresh": [_vp, _vp, _vp, _vp, _vp],
     "sb_vsite_force_redistribute": [_vp, _vp, _vp, _vp, _vp],
+    "sb_settle_create": [_i, _i, _vp, _vp, _vp, _vp, _f, _f, _vp],
+    "sb_settle_destroy": [_vp],
+    "sb_settle_info": [_vp, _vp, _vp, _vp],
+    "sb_settle_remember": [_vp, _vp, _vp, _vp],
+    "sb_settle_apply": [_vp, _vp, _vp, _vp, _vp, _i, _vp, _vp],
+    "sb_md_leap_frog": [_i, _vp, _vp, _vp, _vp, _vp, _f, _vp],
+    "sb_md_nve_settle_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp],
 }
 
 
@@ -619,6 +626,78 @@ class VirtualAtoms:
     def Clear(self):
         if self.handle:
             lib().sb_vsite_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+
+TIME_CONVERSION = 20.455  # SPONGE's internal time unit per ps (CONSTANT_TIME_CONVERTION)
+
+
+def constrain_pairs_from_bonds(bond_a, bond_b, bond_r, mass, constrain_mass=3.3):
+    """CONSTRAIN::Add_HBond_To_Constrain_Pair (SPONGE/constrain/constrain.cu:81-112): the bonds
+    with an atom lighter than ``constrain_mass`` (and heavier than 0), in bond order.
+    Returns (i, j, r)."""
+    a = np.asarray(bond_a, np.int64)
+    b = np.asarray(bond_b, np.int64)
+    m = np.asarray(mass, np.float32)
+    ma, mb = m[a], m[b]
+    keep = ((ma < constrain_mass) & (ma > 0)) | ((mb < constrain_mass) & (mb > 0))
+    return (a[keep].astype(np.int32), b[keep].astype(np.int32),
+            np.asarray(bond_r, np.float32)[keep])
+
+
+def md_leap_frog(atom_numbers, inverse_mass, frc, vel, crd, dt, acc=None, stream=None):
+    """MD_INFORMATION::NVE_iteration::Leap_Frog: acc = F/m, vel += dt acc, crd += dt vel
+    (dt in SPONGE's internal unit, TIME_CONVERSION per ps)."""
+    _check(lib().sb_md_leap_frog(int(atom_numbers), _ptr(inverse_mass), _ptr(frc), _ptr(vel),
+                                 _ptr(crd), _ptr(acc), float(dt), _stream(stream)))
+
+
+class Settle:
+    """SETTLE over CONSTRAIN's pair list (see constrain_pairs_from_bonds): rigid triangles and
+    rigid pairs; ``dt`` in SPONGE's internal unit; ``exp_gamma`` 1 for NVE."""
+
+    def __init__(self, atom_numbers, pair_i, pair_j, pair_r, mass, dt, exp_gamma=1.0):
+        _require_cuda()
+        self.atom_numbers = int(atom_numbers)
+        i = np.ascontiguousarray(pair_i, np.int32)
+        j = np.ascontiguousarray(pair_j, np.int32)
+        r = np.ascontiguousarray(pair_r, np.float32)
+        m = np.ascontiguousarray(mass, np.float32)
+        self.handle = ctypes.c_void_p()
+        _check(lib().sb_settle_create(self.atom_numbers, int(i.size), i.ctypes.data,
+                                      j.ctypes.data, r.ctypes.data, m.ctypes.data, float(dt),
+                                      float(exp_gamma), ctypes.byref(self.handle)))
+        t, p, rest = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().sb_settle_info(self.handle, ctypes.byref(t), ctypes.byref(p),
+                                    ctypes.byref(rest)))
+        self.triangle_numbers, self.pair_numbers, self.remaining_pairs = t.value, p.value, rest.value
+
+    def Remember_Last_Coordinates(self, uint_crd, scaler, stream=None):
+        _check(lib().sb_settle_remember(self.handle, _ptr(uint_crd), _box3(scaler),
+                                        _stream(stream)))
+
+    def Do_SETTLE(self, mass, crd, box_length, vel, need_pressure=0, pressure=None, stream=None):
+        _check(lib().sb_settle_apply(self.handle, _ptr(mass), _ptr(crd), _box3(box_length),
+                                     _ptr(vel), int(need_pressure), _ptr(pressure),
+                                     _stream(stream)))
+
+    def nve_step(self, uint_crd, scaler, inverse_mass, mass, frc, vel, crd, box_length,
+                 acc=None, need_pressure=0, pressure=None, stream=None):
+        """Remember + leap-frog + SETTLE in one launch (the same bits as the three calls)."""
+        _check(lib().sb_md_nve_settle_step(self.handle, _ptr(uint_crd), _box3(scaler),
+                                           _ptr(inverse_mass), _ptr(mass), _ptr(frc), _ptr(vel),
+                                           _ptr(crd), _ptr(acc), _box3(box_length),
+                                           int(need_pressure), _ptr(pressure), _stream(stream)))
+
+    def Clear(self):
+        if self.handle:
+            lib().sb_settle_destroy(self.handle)
             self.handle = ctypes.c_void_p()
 
     def __del__(self):

@@ -16,7 +16,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsponge_b200.so")
 SOURCES = ["sb_api.cu", "sb_neighbor.cu", "sb_pair.cu", "sb_pme.cu", "sb_fft.cu",
-           "sb_adjoint.cu", "sb_softcore.cu", "sb_nb14.cu"]
+           "sb_adjoint.cu", "sb_softcore.cu", "sb_nb14.cu",
+           "sb_md.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -34,6 +34,20 @@ def _waters(system):
     return first, (n - first) // 3
 
 
+def bonds_and_masses(system):
+    """The rigid-water bonds (O-H1, O-H2, H1-H2 per water, as the bond file lists them) and the
+    per-atom masses of a generated system. Returns (bond_a, bond_b, bond_r0, mass)."""
+    n = len(system["charge"])
+    first, nw = _waters(system)
+    mass = np.full(n, MASS_SOLUTE, np.float32)
+    o = first + 3 * np.arange(nw, dtype=np.int32)
+    mass[o], mass[o + 1], mass[o + 2] = MASS_O, MASS_H, MASS_H
+    a = np.stack([o, o, o + 1], 1).reshape(-1).astype(np.int32)
+    b = np.stack([o + 1, o + 2, o + 2], 1).reshape(-1).astype(np.int32)
+    r = np.tile(np.array([0.9572, 0.9572, R_HH], np.float32), nw)
+    return a, b, r, mass
+
+
 def write_inputs(system, outdir, prefix="sys"):
     os.makedirs(outdir, exist_ok=True)
     n = len(system["charge"])
@@ -128,6 +142,24 @@ def read_coordinate(path):
     crd = np.array(" ".join(lines[1:1 + n]).split(), np.float64).reshape(n, 3)
     box = np.array(lines[1 + n].split()[:3], np.float64)
     return crd.astype(np.float32), box.astype(np.float32)
+
+
+def read_velocity(path):
+    """Velocity restart file: "N [time]", then N lines of "vx vy vz" (A per internal time
+    unit). Returns vel [N,3] float32."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    n = int(lines[0].split()[0])
+    return np.array(" ".join(lines[1:1 + n]).split(), np.float32).reshape(n, 3)
+
+
+def read_bond(path):
+    """Bond file: "count", then "a b k r0" per bond. Returns (a, b, k, r0)."""
+    tok = open(path).read().split()
+    n = int(tok[0])
+    rows = np.array(tok[1:1 + 4 * n], np.float64).reshape(n, 4)
+    return (rows[:, 0].astype(np.int32), rows[:, 1].astype(np.int32),
+            rows[:, 2].astype(np.float32), rows[:, 3].astype(np.float32))
 
 
 def read_values(path):

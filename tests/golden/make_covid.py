@@ -20,7 +20,10 @@ with the box on the line after them, :1051-1080 charges, :308-351 exclusions as 
 (10 A), skin (2 A) and Ewald tolerance (1e-5) are SPONGE's defaults; the PME grid is the one
 Get_Fft_Patameter picks for the box. The 1-4 pairs (covid-tip4p_nb14.txt: "count", then
 "a b lj_scale cf_scale") and virtual atoms (covid-tip4p_vatom.txt: one "type v from... params" line
-each) come from the same directory; the bonded terms are not part of the comparison.
+each) come from the same directory. For one NVE step with SETTLE the bonds (covid-tip4p_bond.txt:
+"count", then "a b k r0"; only the pairs CONSTRAIN keeps are used), the masses
+(covid-tip4p_mass.txt) and the equilibrated velocities (npt_velocity.txt) are added, with a
+2 fs step; the bonded forces are not part of the comparison.
 """
 
 import hashlib
@@ -36,6 +39,11 @@ REFERENCE = os.path.join(HERE, "reference_covid_tip4p.npz")
 SOURCE = "/root/reference/SPONGE/covid-tip4p"
 # Get_Fft_Patameter's grid for the fixture's box (108.43 x 91.25 x 84.41 A)
 FFT = (112, 96, 96)
+# the MD step: 2 fs in SPONGE's internal time unit (MD_core.cu reads dt in ps and multiplies by
+# CONSTANT_TIME_CONVERTION = 20.455 in FP32)
+MD_DT = np.float32(np.float32(0.002) * np.float32(20.455))
+# atoms whose SETTLE outputs are stored (a seeded sample, so the file stays small)
+SETTLE_SAMPLE = 8192
 
 
 def read_reference_files(src=SOURCE, prefix="covid-tip4p", coordinates="npt_coordinate.txt"):
@@ -53,10 +61,13 @@ def read_reference_files(src=SOURCE, prefix="covid-tip4p", coordinates="npt_coor
     _, numbers, excl_list = sponge_io.read_exclude(p("exclude"))
     a14, b14, ljs14, cf14 = sponge_io.read_nb14(p("nb14"))
     vt, va, vp = sponge_io.read_vatom(p("vatom"))
+    ba, bb, _, br = sponge_io.read_bond(p("bond"))
+    mass = sponge_io.read_values(p("mass"))
+    vel = sponge_io.read_velocity(os.path.join(src, "npt_velocity.txt"))
     return dict(crd=crd, box=box, charge=charge, lj_A=A, lj_B=B, lj_type=lj_type,
                 n_types=np.int32(t), excl_numbers=numbers, excl_list=excl_list, nb14_a=a14,
                 nb14_b=b14, nb14_lj_scale=ljs14, nb14_cf=cf14, vs_type=vt, vs_atoms=va,
-                vs_param=vp)
+                vs_param=vp, bond_a=ba, bond_b=bb, bond_r=br, mass=mass, vel=vel)
 
 
 def load_system(path=INPUTS):
@@ -78,7 +89,15 @@ def load_system(path=INPUTS):
         nb14_a=z["nb14_a"].astype(np.int32), nb14_b=z["nb14_b"].astype(np.int32),
         nb14_lj_scale=z["nb14_lj_scale"].astype(np.float32),
         nb14_cf=z["nb14_cf"].astype(np.float32), vs_type=z["vs_type"].astype(np.int32),
-        vs_atoms=z["vs_atoms"].astype(np.int32), vs_param=z["vs_param"].astype(np.float32))
+        vs_atoms=z["vs_atoms"].astype(np.int32), vs_param=z["vs_param"].astype(np.float32),
+        bond_a=z["bond_a"].astype(np.int32), bond_b=z["bond_b"].astype(np.int32),
+        bond_r=z["bond_r"].astype(np.float32), mass=z["mass"].astype(np.float32),
+        vel=z["vel"].astype(np.float32), md_dt=MD_DT)
+
+
+def settle_sample(n):
+    """The atoms whose SETTLE step outputs the reference file keeps."""
+    return np.sort(np.random.default_rng(2024).choice(n, SETTLE_SAMPLE, replace=False))
 
 
 def write_inputs():
@@ -89,7 +108,8 @@ def write_inputs():
                         excl_list=r["excl_list"].astype(np.int32), nb14_a=r["nb14_a"],
                         nb14_b=r["nb14_b"], nb14_lj_scale=r["nb14_lj_scale"],
                         nb14_cf=r["nb14_cf"], vs_type=r["vs_type"].astype(np.int8),
-                        vs_atoms=r["vs_atoms"], vs_param=r["vs_param"])
+                        vs_atoms=r["vs_atoms"], vs_param=r["vs_param"], bond_a=r["bond_a"],
+                        bond_b=r["bond_b"], bond_r=r["bond_r"], mass=r["mass"], vel=r["vel"])
     print(INPUTS, os.path.getsize(INPUTS))
 
 
@@ -106,6 +126,11 @@ def compact_modules(r, s):
     if "vs_frc" in r:
         out["vs_frc"] = np.asarray(r["vs_frc"], np.float32)
         out["vs_crd"] = np.asarray(r["vs_crd"], np.float32)[s["vs_atoms"][:, 0]]
+    if "settle_crd" in r:
+        atoms = settle_sample(len(s["charge"]))
+        out["settle_atoms"] = atoms.astype(np.int32)
+        out["settle_crd"] = np.asarray(r["settle_crd"], np.float32)[atoms]
+        out["settle_vel"] = np.asarray(r["settle_vel"], np.float32)[atoms]
     return out
 
 
