@@ -51,6 +51,7 @@ _SIGS = {
     "sb_nl_pair_count": [_vp, _vp, _vp],
     "sb_nl_export_pairs": [_vp, _vp, ctypes.c_int64, _vp, _vp],
     "sb_nl_status": [_vp, _vp, _vp],
+    "sb_nl_set_prune": [_vp, _f, _i],
     "sb_nl_uint_crd": [_vp, _vp],
     "sb_lj_create": [_i, _i, _vp, _vp, _vp, _f, _vp, _i, _vp],
     "sb_lj_destroy": [_vp],
@@ -240,6 +241,10 @@ class NeighborList:
         f = ctypes.c_int()
         _check(lib().sb_nl_status(self.handle, ctypes.byref(f), _stream(None)))
         return f.value
+
+    def set_prune(self, prune_buffer, prune_interval=0):
+        """Pruned pair list for the packed pair kernel (sb_nl_set_prune; 0 turns it off)."""
+        _check(lib().sb_nl_set_prune(self.handle, float(prune_buffer), int(prune_interval)))
 
     def uint_crd(self):
         torch = _require_cuda()

@@ -152,11 +152,21 @@ struct sb_neighbor_list {
     int* cl_count = nullptr;        // [clu_cap]
     uint32_t* cl_ent = nullptr;     // [clu_cap * ent_cap]
     int* meta = nullptr;            // [0] clusters, [1] status flags, [2] refresh flag,
-                                    // [3] padded slots, [4..5] pair count (int64)
+                                    // [3] padded slots, [4..5] pair count (int64),
+                                    // [6] prune request, [7] pruned by the last pair launch
     // per force call packed data
     uint4* xq = nullptr;            // [slot_cap]
     int* stype = nullptr;           // [slot_cap]
     long long* fix = nullptr;       // [3*slot_cap] x,y,z planes
+    // pruned list (sb_nl_set_prune): the entries of cl_ent with an active slot within
+    // cutoff + prune_buffer at the last prune, written by the packed pair kernel when meta[6] is
+    // set (by a rebuild, by k_pack when an atom has moved more than prune_buffer / 2 since the
+    // last prune, or every prune_interval updates) and read by it in the other steps
+    float prune_buffer = 0.f;
+    int prune_interval = 0, prune_count = 0;
+    int* cl_count_in = nullptr;     // [clu_cap]
+    uint32_t* cl_ent_in = nullptr;  // [clu_cap * ent_cap]
+    uint4* xq_prune = nullptr;      // [slot_cap] packed coordinates at the last prune
     // ATOM_GROUP compatibility export
     void* ag = nullptr;             // ATOM_GROUP[N]
     int* ag_serial = nullptr;       // [N * max_neighbor_numbers]
@@ -222,6 +232,7 @@ int sb_nl_ensure_built(sb_neighbor_list* nl);
 int sb_nl_pack(sb_neighbor_list* nl, const uint32_t* d_uint_crd, const float* d_charge,
                const int* d_type, cudaStream_t s);
 int sb_nl_finalize_forces(sb_neighbor_list* nl, float* d_frc, cudaStream_t s);
+int sb_nl_retire_prune(sb_neighbor_list* nl, cudaStream_t s);
 int sb_nl_build_atom_group(sb_neighbor_list* nl, cudaStream_t s);
 
 // fused fixed-form step pieces: the pair kernel and the exclusion correction accumulate into the

@@ -590,10 +590,14 @@ __global__ void k_ag_clamp(int n, SbAtomGroup* __restrict__ ag, int maxnb) {
     if (i < n && ag[i].atom_numbers > maxnb) ag[i].atom_numbers = maxnb;
 }
 
+// slot-order coordinates, charges and types for the pair kernels; with a pruned list
+// (xq_prune given) also the displacement test against the coordinates of the last prune: an atom
+// that moved more than half the prune buffer requests a new prune (prune_req = meta + 6)
 __global__ void k_pack(const int* __restrict__ meta, const int* __restrict__ slot_atom,
                        const uint32_t* __restrict__ uc, const float* __restrict__ q,
                        const int* __restrict__ type, uint4* __restrict__ xq,
-                       int* __restrict__ stype) {
+                       int* __restrict__ stype, const uint4* __restrict__ xq_prune, float sx,
+                       float sy, float sz, float move2, int* __restrict__ prune_req) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= meta[3]) return;
     int a = slot_atom[s];
@@ -605,14 +609,27 @@ __global__ void k_pack(const int* __restrict__ meta, const int* __restrict__ slo
         v.z = uc[3 * a + 2];
         v.w = q ? __float_as_uint(q[a]) : 0u;
         t = type ? type[a] : 0;
+        if (xq_prune) {
+            const uint4 o = xq_prune[s];
+            const float dx = __int2float_rn((int)(v.x - o.x)) * sx;
+            const float dy = __int2float_rn((int)(v.y - o.y)) * sy;
+            const float dz = __int2float_rn((int)(v.z - o.z)) * sz;
+            if (dx * dx + dy * dy + dz * dz > move2) prune_req[0] = 1;
+        }
     }
     xq[s] = v;
     stype[s] = t;
 }
 
-__global__ void k_finalize(const int* __restrict__ meta, const int* __restrict__ slot_atom,
+// fixed-point forces to the caller's float array (slot order -> atom order), clearing the
+// accumulator; also retires a prune request that the pair launch before it served (meta[6..7])
+__global__ void k_finalize(int* __restrict__ meta, const int* __restrict__ slot_atom,
                            long long* __restrict__ fix, int slot_cap, float* __restrict__ frc) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0 && meta[7]) {
+        meta[6] = 0;
+        meta[7] = 0;
+    }
     if (s >= meta[3]) return;
     int a = slot_atom[s];
     long long fx = fix[s], fy = fix[slot_cap + s], fz = fix[2 * slot_cap + s];
@@ -688,7 +705,7 @@ static int nl_alloc(sb_neighbor_list* nl) {
     SB_TRY(sb_malloc((void**)&nl->xq, sizeof(uint4) * nl->slot_cap, "xq"));
     SB_TRY(sb_malloc((void**)&nl->stype, sizeof(int) * nl->slot_cap, "stype"));
     SB_TRY(sb_malloc((void**)&nl->fix, sizeof(long long) * 3 * nl->slot_cap, "force fix"));
-    SB_CHECK_CUDA(cudaMemset(nl->meta, 0, sizeof(int) * 8));
+    SB_CHECK_CUDA(cudaMemset(nl->meta, 0, sizeof(int) * 8));  // no prune requested
     SB_CHECK_CUDA(cudaMemset(nl->fix, 0, sizeof(long long) * 3 * nl->slot_cap));
     SB_CHECK_CUDA(cudaMemset(nl->cl_count, 0, sizeof(int) * nl->clu_cap));
     SB_CHECK_CUDA(cudaMemset(nl->slot_atom, 0xff, sizeof(int) * nl->slot_cap));
@@ -699,7 +716,8 @@ static void nl_free(sb_neighbor_list* nl) {
     void* ps[] = {nl->old_crd, nl->ucrd, nl->col_of, nl->col_rank, nl->col_count, nl->col_start,
                   nl->sort_tmp, nl->slot_atom, nl->atom_slot, nl->slot_u, nl->excl_lo,
                   nl->excl_hi, nl->cl_count, nl->cl_ent, nl->meta, nl->xq, nl->stype, nl->fix,
-                  nl->ag, nl->ag_serial, nl->zbin};
+                  nl->ag, nl->ag_serial, nl->zbin, nl->cl_count_in, nl->cl_ent_in,
+                  nl->xq_prune};
     for (void* p : ps) sb_free(p);
 }
 
@@ -819,6 +837,11 @@ static int nl_rebuild(sb_neighbor_list* nl, float* d_crd, const int* es, const i
         P, nl->col_start, nl->col_count, nl->slot_u, nl->slot_atom, nl->excl_lo, nl->excl_hi,
         es, en, el, nl->zbin, nl->cl_count, nl->cl_ent, nl->meta, dflag);
     SB_CHECK_LAUNCH();
+    if (nl->prune_buffer > 0.f) {
+        // the slots changed: the pruned list is rebuilt by the next pair launch
+        SB_CHECK_CUDA(cudaMemsetAsync(nl->meta + 6, 1, sizeof(int), s));
+        nl->prune_count = 0;
+    }
     nl->ag_valid = 0;
     nl->build_id++;
     return SB_OK;
@@ -849,9 +872,12 @@ extern "C" int sb_nl_update(sb_neighbor_list* nl, float* d_crd, const int* es, c
         int* flag = nl->meta + 2;
         SB_CHECK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
         int tb = 128;
+        // with a pruned list the outer list must hold every pair within cutoff + prune buffer,
+        // so the skin left for motion is skin - prune_buffer
+        const float hs = 0.5f * (nl->skin - nl->prune_buffer);
         k_refresh_check<<<(nl->n + tb - 1) / tb, tb, 0, s>>>(
             nl->n, d_crd, nl->old_crd, nl->box[0], nl->box[1], nl->box[2],
-            nl->skin_permit * nl->skin_permit * nl->half_skin_square, flag);
+            nl->skin_permit * nl->skin_permit * hs * hs, flag);
         SB_CHECK_LAUNCH();
         int h = 0;
         SB_CHECK_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -862,7 +888,41 @@ extern "C" int sb_nl_update(sb_neighbor_list* nl, float* d_crd, const int* es, c
         SB_TRY(nl_rebuild(nl, d_crd, es, el, en, nullptr, s));
         nl->built = 1;
         nl->needs_rebuild = 0;
+    } else if (nl->prune_buffer > 0.f && nl->prune_interval > 0 &&
+               ++nl->prune_count >= nl->prune_interval) {
+        SB_CHECK_CUDA(cudaMemsetAsync(nl->meta + 6, 1, sizeof(int), s));
+        nl->prune_count = 0;
     }
+    return SB_OK;
+}
+
+extern "C" int sb_nl_set_prune(sb_neighbor_list* nl, float prune_buffer, int prune_interval) {
+    if (!nl || !(prune_buffer >= 0.f) || prune_buffer > nl->skin || prune_interval < 0) {
+        sb_set_error("sb_nl_set_prune: buffer must be in [0, skin] and the interval >= 0");
+        return SB_ERR_ARG;
+    }
+    cudaDeviceSynchronize();
+    if (prune_buffer > 0.f) {
+        if (!nl->cl_count_in) {
+            SB_TRY(sb_malloc((void**)&nl->cl_count_in, sizeof(int) * nl->clu_cap,
+                             "pruned counts"));
+            SB_CHECK_CUDA(cudaMemset(nl->cl_count_in, 0, sizeof(int) * nl->clu_cap));
+        }
+        if (!nl->cl_ent_in)
+            SB_TRY(sb_malloc((void**)&nl->cl_ent_in,
+                             sizeof(uint32_t) * (size_t)nl->clu_cap * nl->ent_cap, "pruned list"));
+        if (!nl->xq_prune) {
+            SB_TRY(sb_malloc((void**)&nl->xq_prune, sizeof(uint4) * nl->slot_cap,
+                             "prune coordinates"));
+            SB_CHECK_CUDA(cudaMemset(nl->xq_prune, 0, sizeof(uint4) * nl->slot_cap));
+        }
+    }
+    nl->prune_buffer = prune_buffer;
+    nl->prune_interval = prune_interval;
+    nl->prune_count = 0;
+    // meta[6] = prune requested (the first pair launch builds the pruned list), meta[7] = 0
+    SB_CHECK_CUDA(cudaMemset(nl->meta + 6, 0, 2 * sizeof(int)));
+    if (prune_buffer > 0.f) SB_CHECK_CUDA(cudaMemset(nl->meta + 6, 1, 1));
     return SB_OK;
 }
 
@@ -888,8 +948,28 @@ int sb_nl_ensure_built(sb_neighbor_list* nl) {
 int sb_nl_pack(sb_neighbor_list* nl, const uint32_t* d_uint_crd, const float* d_charge,
                const int* d_type, cudaStream_t s) {
     int tb = 256;
-    k_pack<<<(nl->slot_cap + tb - 1) / tb, tb, 0, s>>>(nl->meta, nl->slot_atom, d_uint_crd,
-                                                       d_charge, d_type, nl->xq, nl->stype);
+    const bool pr = nl->prune_buffer > 0.f;
+    const float half = 0.5f * nl->prune_buffer;
+    k_pack<<<(nl->slot_cap + tb - 1) / tb, tb, 0, s>>>(
+        nl->meta, nl->slot_atom, d_uint_crd, d_charge, d_type, nl->xq, nl->stype,
+        pr ? nl->xq_prune : nullptr, (1.0f / 4294967296.0f) * nl->box[0],
+        (1.0f / 4294967296.0f) * nl->box[1], (1.0f / 4294967296.0f) * nl->box[2], half * half,
+        nl->meta + 6);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+__global__ void k_retire_prune(int* __restrict__ meta) {
+    if (meta[7]) {
+        meta[6] = 0;
+        meta[7] = 0;
+    }
+}
+
+// retires a prune request served by a pair launch that no k_finalize follows (timing runs)
+int sb_nl_retire_prune(sb_neighbor_list* nl, cudaStream_t s) {
+    if (nl->prune_buffer <= 0.f) return SB_OK;
+    k_retire_prune<<<1, 1, 0, s>>>(nl->meta);
     SB_CHECK_LAUNCH();
     return SB_OK;
 }

@@ -41,6 +41,12 @@ struct PairParams {
     int nt;
     int slot_cap;
     int ent_cap;
+    // pruned list (packed kernel only): rb2 = (rc + prune buffer)^2, 0 without one
+    float rb2;
+    int* prune;                // meta + 6: [0] prune requested, [1] set by a pruning launch
+    int* cl_count_in;
+    uint32_t* cl_ent_in;
+    uint4* xq_prune;
 };
 
 #define SB_EV_ENERGY 1
@@ -283,6 +289,13 @@ static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list
     P.nt = lj->ntypes;
     P.slot_cap = nl->slot_cap;
     P.ent_cap = nl->ent_cap;
+    const bool pruned = nl->prune_buffer > 0.f && nl->cl_ent_in;
+    const float rb = lj->cutoff + nl->prune_buffer;
+    P.rb2 = pruned ? rb * rb : 0.f;
+    P.prune = nl->meta + 6;
+    P.cl_count_in = nl->cl_count_in;
+    P.cl_ent_in = nl->cl_ent_in;
+    P.xq_prune = nl->xq_prune;
     return P;
 }
 
@@ -550,6 +563,8 @@ extern "C" int sb_lj_tune(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint
     for (int c = 0; c < 4; c++) {
         lj->ipl = cand[c];
         SB_TRY(launch_pair_fixed(lj, nl, pme_beta, 0, nullptr, nullptr, nullptr, s));
+        // a pruned list is built by the first packed launch; the timed ones walk it
+        SB_TRY(sb_nl_retire_prune(nl, s));
         SB_CHECK_CUDA(cudaEventRecord(a, s));
         for (int r = 0; r < 3; r++)
             SB_TRY(launch_pair_fixed(lj, nl, pme_beta, 0, nullptr, nullptr, nullptr, s));

@@ -44,6 +44,73 @@ __device__ __forceinline__ float2 ewald_nG2(float2 z, const float* gp) {
     return f2mul(p, make_float2(sb_rcp(q.x), sb_rcp(q.y)));
 }
 
+// Pruning pass over the full list of one cluster: keeps, in order, the entries with an active
+// slot (mask bit set) whose r^2 — computed exactly as pair_walk_x2 computes it — is below
+// (rc + prune buffer)^2, and writes them to `out`. Every entry the walk would find inside the
+// cut-off at these coordinates is kept. Returns the number kept.
+template <bool EXACT>
+__device__ __forceinline__ int prune_walk_x2(
+    const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
+    uint32_t* __restrict__ out, const uint4* __restrict__ xq, const int base, const int lane,
+    const uint32_t rx, const uint32_t ry, const uint32_t rz, const float2 (&nx)[4],
+    const float2 (&ny)[4], const float2 (&nz)[4]) {
+    const float2 rb2 = f2(P.rb2);
+    int kept = 0;
+    // four batches of 32 entries per step, with the next step's entries loaded while this step's
+    // j coordinates arrive: the test itself is short, so more loads are kept in flight than in
+    // the walk (past the end an entry reads as 0: mask 0, never kept)
+    constexpr int G = 4;
+    uint32_t vn[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) vn[g] = lane + 32 * g < cnt ? ents[lane + 32 * g] : 0u;
+    for (int e0 = 0; e0 < cnt; e0 += 32 * G) {
+        uint32_t v[G];
+        uint4 xj[G];
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            v[g] = vn[g];
+            xj[g] = xq[v[g] & 0xffffffu];
+        }
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int e = e0 + 32 * (G + g) + lane;
+            vn[g] = e < cnt ? ents[e] : 0u;
+        }
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const uint32_t m = v[g] >> 24;
+            const float2 xj2 = f2(__int2float_rn((int)(xj[g].x - rx)) * P.sx);
+            const float2 yj2 = f2(__int2float_rn((int)(xj[g].y - ry)) * P.sy);
+            const float2 zj2 = f2(__int2float_rn((int)(xj[g].z - rz)) * P.sz);
+            bool keep = false;
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                float2 dx, dy, dz;
+                if (EXACT) {
+                    const uint4 xa = xq[base + 2 * p], xb = xq[base + 2 * p + 1];
+                    dx = make_float2(__int2float_rn((int)(xj[g].x - xa.x)) * P.sx,
+                                     __int2float_rn((int)(xj[g].x - xb.x)) * P.sx);
+                    dy = make_float2(__int2float_rn((int)(xj[g].y - xa.y)) * P.sy,
+                                     __int2float_rn((int)(xj[g].y - xb.y)) * P.sy);
+                    dz = make_float2(__int2float_rn((int)(xj[g].z - xa.z)) * P.sz,
+                                     __int2float_rn((int)(xj[g].z - xb.z)) * P.sz);
+                } else {
+                    dx = f2add(xj2, nx[p]);
+                    dy = f2add(yj2, ny[p]);
+                    dz = f2add(zj2, nz[p]);
+                }
+                const float2 r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
+                keep |= ((m & (1u << (2 * p))) != 0u && r2.x < rb2.x) ||
+                        ((m & (2u << (2 * p))) != 0u && r2.y < rb2.y);
+            }
+            const unsigned b = __ballot_sync(0xffffffffu, keep);
+            if (keep) out[kept + __popc(b & ((1u << lane) - 1u))] = v[g];
+            kept += __popc(b);
+        }
+    }
+    return kept;
+}
+
 template <int EV, bool EXACT>
 __device__ __forceinline__ void pair_walk_x2(
     const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
@@ -54,9 +121,11 @@ __device__ __forceinline__ void pair_walk_x2(
     float2 (&fz)[4], float (&ei)[8], float (&vi)[8], float (&di)[8]) {
     const float2 rc2 = f2(P.rc2);
     const float2 b2 = f2(P.beta2);
-    // two-deep software pipeline as in the scalar kernel: entries two batches ahead, j data one
-    uint32_t v1 = lane < cnt ? ents[lane] : 0u;
-    uint32_t v2 = lane + 32 < cnt ? ents[lane + 32] : 0u;
+    // two-deep software pipeline as in the scalar kernel: entries two batches ahead, j data one.
+    // Entries are read through L2 (ld.global.cg): a pruning launch reads the list it has just
+    // written.
+    uint32_t v1 = lane < cnt ? __ldcg(ents + lane) : 0u;
+    uint32_t v2 = lane + 32 < cnt ? __ldcg(ents + lane + 32) : 0u;
     uint4 xj1 = xq[v1 & 0xffffffu];
     int tj1 = stype[v1 & 0xffffffu];
     for (int e0 = 0; e0 < cnt; e0 += 32) {
@@ -66,7 +135,7 @@ __device__ __forceinline__ void pair_walk_x2(
         const uint4 xj = xj1;
         const int tj = tj1;
         v1 = v2;
-        v2 = e + 64 < cnt ? ents[e + 64] : 0u;
+        v2 = e + 64 < cnt ? __ldcg(ents + e + 64) : 0u;
         xj1 = xq[v1 & 0xffffffu];
         tj1 = stype[v1 & 0xffffffu];
         const int j = (int)(v & 0xffffffu);
@@ -194,9 +263,31 @@ __global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
     for (int k = 0; k < 8; k++) ei[k] = vi[k] = di[k] = 0.f;
     __syncwarp();
 
-    const int cntf = cl_count[c];
-    const int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
+    int cntf = cl_count[c];
+    int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
     const uint32_t* ents = cl_ent + (size_t)c * P.ent_cap;
+    if (P.rb2 > 0.f) {
+        // pruned list: rebuilt from the full list on request, then walked in both cases, so the
+        // forces do not depend on whether this launch pruned
+        uint32_t* in_ents = P.cl_ent_in + (size_t)c * P.ent_cap;
+        if (P.prune[0]) {
+            cnt = (cntf & SB_CL_EXACT)
+                      ? prune_walk_x2<true>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz, nx,
+                                            ny, nz)
+                      : prune_walk_x2<false>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz,
+                                             nx, ny, nz);
+            if (lane == 0) {
+                P.cl_count_in[c] = cnt | (cntf & ~SB_CL_COUNT_MASK);
+                if (c == 0) P.prune[1] = 1;  // k_finalize retires the request
+            }
+            if (lane < SB_CLUSTER) P.xq_prune[base + lane] = my;
+            __syncwarp();
+        } else {
+            cntf = P.cl_count_in[c];
+            cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
+        }
+        ents = in_ents;
+    }
     if (cntf & SB_CL_EXACT)
         pair_walk_x2<EV, true>(P, cnt, ents, xq, stype, ctab, fix, base, lane, rx, ry, rz, nx, ny,
                                nz, nq, fx, fy, fz, ei, vi, di);

@@ -21,8 +21,13 @@ def scaled_lj_tables(system):
 
 
 class NonbondedEngine:
+    """``prune_buffer`` / ``prune_interval``: the pruned pair list of the fixed form
+    (NeighborList.set_prune): the pair kernel walks the entries within cutoff + 0.5 A of the last
+    prune, renewed after each rebuild, when an atom has moved 0.25 A, and every 5 list updates
+    (the rate the reference's own 2 A skin over 20 steps allows for 0.5 A). 0 turns it off."""
+
     def __init__(self, system, form=FORM_FIXED, refresh_interval=20, max_neighbor_numbers=1200,
-                 device="cuda"):
+                 device="cuda", prune_buffer=0.5, prune_interval=5):
         torch = _require_cuda()
         self.torch = torch
         self.system = system
@@ -39,6 +44,8 @@ class NonbondedEngine:
         A12, B6 = scaled_lj_tables(system)
         self.nl = NeighborList(n, self.box, system["cutoff"], system["skin"], refresh_interval,
                                max_neighbor_numbers=max_neighbor_numbers, form=form)
+        if form == FORM_FIXED and prune_buffer:
+            self.nl.set_prune(min(float(prune_buffer), float(system["skin"])), prune_interval)
         self.lj = LennardJones(n, system["n_types"], A12, B6, system["lj_type"],
                                system["cutoff"], self.box, form=form)
         fft = system.get("fft") or (-1, -1, -1)
