@@ -34,9 +34,10 @@ if ROOT not in sys.path:
 DT_FS = 2.0
 FLOP_PER_PAIR = 50.0       # in-cutoff pair: dr 3, r^2 5, rsqrt 1, powers 4, LJ 3, Ewald 26, scale 3, accumulate 6
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal at max SM clock
-# DRAM bytes read + written by one launch of the pair kernel on this workload, from an ncu
-# capture (profiles/k_pair_fixed_solvated96k.md): the list plus the packed coordinates
-PAIR_DRAM_BYTES = 32.63e6
+# DRAM bytes read + written by one launch of the pair kernel walking the pruned list on this
+# workload, from an ncu capture (profiles/k_pair_x2_solvated96k.md): the list plus the packed
+# coordinates
+PAIR_DRAM_BYTES = 25.01e6
 # pair-kernel shape (sb_lj_set_kernel_variant) -> kernel name
 PAIR_KERNEL = {2: "k_pair_x2", 8: "k_pair_fixed<8>", 4: "k_pair_fixed<4>", 1: "k_pair_compact"}
 

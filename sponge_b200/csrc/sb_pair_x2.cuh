@@ -118,14 +118,12 @@ __device__ __forceinline__ void pair_walk_x2(
     long long* __restrict__ fix, const int base, const int lane, const uint32_t rx,
     const uint32_t ry, const uint32_t rz, const float2 (&nx)[4], const float2 (&ny)[4],
     const float2 (&nz)[4], const float2 (&nq)[4], float2 (&fx)[4], float2 (&fy)[4],
-    float2 (&fz)[4], float (&ei)[8], float (&vi)[8], float (&di)[8]) {
+    float2 (&fz)[4], float (&ei)[8], float (&vi)[8], float (&di)[8], uint32_t v1, uint32_t v2) {
     const float2 rc2 = f2(P.rc2);
     const float2 b2 = f2(P.beta2);
-    // two-deep software pipeline as in the scalar kernel: entries two batches ahead, j data one.
-    // Entries are read through L2 (ld.global.cg): a pruning launch reads the list it has just
-    // written.
-    uint32_t v1 = lane < cnt ? __ldcg(ents + lane) : 0u;
-    uint32_t v2 = lane + 32 < cnt ? __ldcg(ents + lane + 32) : 0u;
+    // two-deep software pipeline as in the scalar kernel: entries two batches ahead (the first
+    // two batches, v1 and v2, are loaded by the caller), j data one. Entries are read through L2
+    // (ld.global.cg): a pruning launch reads the list it has just written.
     uint4 xj1 = xq[v1 & 0xffffffu];
     int tj1 = stype[v1 & 0xffffffu];
     for (int e0 = 0; e0 < cnt; e0 += 32) {
@@ -223,8 +221,27 @@ __global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
     const int c = blockIdx.x;
     if (c >= meta[0]) return;
     const int base = c * SB_CLUSTER;
+    // the loads that start a cluster are issued together: list counts (full and pruned), the
+    // prune request, the cluster's atoms; then the first two batches of entries, which arrive
+    // while the LJ table is built
+    const bool pruned = P.rb2 > 0.f;
+    const int req = pruned ? P.prune[0] : 0;
+    int cntf = cl_count[c];
+    const int cntf_in = pruned ? P.cl_count_in[c] : 0;
     const uint4 my = lane < SB_CLUSTER ? xq[base + lane] : make_uint4(0, 0, 0, 0);
     const int myt = lane < SB_CLUSTER ? stype[base + lane] : 0;
+    const uint32_t* ents = cl_ent + (size_t)c * P.ent_cap;
+    uint32_t* in_ents = pruned ? P.cl_ent_in + (size_t)c * P.ent_cap : nullptr;
+    if (pruned && !req) {
+        cntf = cntf_in;
+        ents = in_ents;
+    }
+    int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
+    uint32_t v1 = 0u, v2 = 0u;
+    if (!req) {
+        v1 = lane < cnt ? __ldcg(ents + lane) : 0u;
+        v2 = lane + 32 < cnt ? __ldcg(ents + lane + 32) : 0u;
+    }
     // cluster LJ table: entry (tj, p) = (-A(t_2p,tj), -A(t_2p+1,tj), B(t_2p,tj), B(t_2p+1,tj))
     const int nt = P.nt;
     {
@@ -263,37 +280,30 @@ __global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
     for (int k = 0; k < 8; k++) ei[k] = vi[k] = di[k] = 0.f;
     __syncwarp();
 
-    int cntf = cl_count[c];
-    int cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
-    const uint32_t* ents = cl_ent + (size_t)c * P.ent_cap;
-    if (P.rb2 > 0.f) {
-        // pruned list: rebuilt from the full list on request, then walked in both cases, so the
-        // forces do not depend on whether this launch pruned
-        uint32_t* in_ents = P.cl_ent_in + (size_t)c * P.ent_cap;
-        if (P.prune[0]) {
-            cnt = (cntf & SB_CL_EXACT)
-                      ? prune_walk_x2<true>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz, nx,
-                                            ny, nz)
-                      : prune_walk_x2<false>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz,
-                                             nx, ny, nz);
-            if (lane == 0) {
-                P.cl_count_in[c] = cnt | (cntf & ~SB_CL_COUNT_MASK);
-                if (c == 0) P.prune[1] = 1;  // k_finalize retires the request
-            }
-            if (lane < SB_CLUSTER) P.xq_prune[base + lane] = my;
-            __syncwarp();
-        } else {
-            cntf = P.cl_count_in[c];
-            cnt = min(cntf & SB_CL_COUNT_MASK, P.ent_cap);
+    if (req) {
+        // pruned list: rebuilt from the full list on request, then walked as in the other
+        // launches, so the forces do not depend on whether this launch pruned
+        cnt = (cntf & SB_CL_EXACT)
+                  ? prune_walk_x2<true>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz, nx, ny,
+                                        nz)
+                  : prune_walk_x2<false>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz, nx,
+                                         ny, nz);
+        if (lane == 0) {
+            P.cl_count_in[c] = cnt | (cntf & ~SB_CL_COUNT_MASK);
+            if (c == 0) P.prune[1] = 1;  // k_finalize retires the request
         }
+        if (lane < SB_CLUSTER) P.xq_prune[base + lane] = my;
+        __syncwarp();
         ents = in_ents;
+        v1 = lane < cnt ? __ldcg(ents + lane) : 0u;
+        v2 = lane + 32 < cnt ? __ldcg(ents + lane + 32) : 0u;
     }
     if (cntf & SB_CL_EXACT)
         pair_walk_x2<EV, true>(P, cnt, ents, xq, stype, ctab, fix, base, lane, rx, ry, rz, nx, ny,
-                               nz, nq, fx, fy, fz, ei, vi, di);
+                               nz, nq, fx, fy, fz, ei, vi, di, v1, v2);
     else
         pair_walk_x2<EV, false>(P, cnt, ents, xq, stype, ctab, fix, base, lane, rx, ry, rz, nx,
-                                ny, nz, nq, fx, fy, fz, ei, vi, di);
+                                ny, nz, nq, fx, fy, fz, ei, vi, di, v1, v2);
 
     // i forces: transpose-reduce the 24 per-lane sums (x, y, z of 8 atoms, padded to 32) over the
     // warp; each of the 5 steps halves the values a lane holds, after which lane l holds the
