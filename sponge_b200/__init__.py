@@ -29,7 +29,7 @@ FORM_PLAIN = 1
 
 PME_TOTAL, PME_DIRECT, PME_RECIPROCAL, PME_CORRECTION, PME_SELF = range(5)
 
-FFT_AUTO, FFT_GENERIC = range(2)
+FFT_AUTO, FFT_GENERIC, FFT_LINES = range(3)
 
 STATUS_LIST_OVERFLOW = 1
 STATUS_COLUMN_OVERFLOW = 2
@@ -374,8 +374,10 @@ class ParticleMeshEwald:
 
     def set_fft_variant(self, variant):
         """FFT kernel family of the fixed-point form: FFT_AUTO (register line transforms where
-        the axis size has one, the default) or FFT_GENERIC (stage kernels only); a fixed rule,
-        same results to FP32 rounding. Synchronises."""
+        the axis size has one, with the y and x passes fused per kz plane for square planes; the
+        default), FFT_LINES (the register transforms pass by pass: the same bits as FFT_AUTO) or
+        FFT_GENERIC (stage kernels only); a fixed rule, same results to FP32 rounding.
+        Synchronises."""
         _check(lib().sb_pme_set_fft_variant(self.handle, int(variant)))
 
     def set_overlap(self, on):

@@ -621,10 +621,15 @@ static void xconv4(int n, int blocks, const float2* tw, float2* spec, const floa
 }
 
 static void zfwd4(int m, int blocks, const float2* tw, const float2* post, long long* qfix,
-                  float2* spec, int rows, cudaStream_t s) {
+                  float2* spec, int rows, bool tr, cudaStream_t s) {
 #define SB_F4_ZF(N_, A_, B_)                                                                 \
     case N_:                                                                                 \
-        k_zfwd4<A_, B_><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, qfix, spec, rows); \
+        if (tr)                                                                              \
+            k_zfwd4<A_, B_, true><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, qfix, \
+                                                                             spec, rows);    \
+        else                                                                                 \
+            k_zfwd4<A_, B_, false><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, qfix, \
+                                                                              spec, rows);   \
         break;
     switch (m) {
         SB_FFT4_ZSIZES(SB_F4_ZF)
@@ -634,10 +639,15 @@ static void zfwd4(int m, int blocks, const float2* tw, const float2* post, long 
 }
 
 static void zinv4(int m, int blocks, const float2* tw, const float2* post, const float2* spec,
-                  float* real, int rows, cudaStream_t s) {
+                  float* real, int rows, bool tr, cudaStream_t s) {
 #define SB_F4_ZI(N_, A_, B_)                                                                 \
     case N_:                                                                                 \
-        k_zinv4<A_, B_><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, spec, real, rows); \
+        if (tr)                                                                              \
+            k_zinv4<A_, B_, true><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, spec, \
+                                                                             real, rows);    \
+        else                                                                                 \
+            k_zinv4<A_, B_, false><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, spec, \
+                                                                              real, rows);   \
         break;
     switch (m) {
         SB_FFT4_ZSIZES(SB_F4_ZI)
@@ -646,12 +656,47 @@ static void zinv4(int m, int blocks, const float2* tw, const float2* post, const
 #undef SB_F4_ZI
 }
 
+// plane sizes fused by k_plane4 (square x-y planes)
+#define SB_F4_PL_HAS(K_, A_, B_, NL_) \
+    case K_:                          \
+        return true;
+static bool f4_has_plane(int k) {
+    switch (k) {
+        SB_FFT4_PLANE_SIZES(SB_F4_PL_HAS)
+        default: return false;
+    }
+}
+#undef SB_F4_PL_HAS
+
+static size_t plane4_smem(int k) { return sizeof(float2) * ((size_t)k + (size_t)k * (k + 1)); }
+
+static int plane4(int k, int blocks, const float2* tw, float2* spec, const float* bc,
+                  double* epart, int H, int K2, cudaStream_t s) {
+    const size_t sm = plane4_smem(k);
+#define SB_F4_PL(K_, A_, B_, NL_)                                                             \
+    case K_:                                                                                  \
+        if (sm > 48 * 1024)                                                                   \
+            SB_CHECK_CUDA(cudaFuncSetAttribute(k_plane4<A_, B_, NL_>,                         \
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                               (int)sm));                                     \
+        k_plane4<A_, B_, NL_><<<blocks, NL_ * F4<A_, B_>::T, sm, s>>>(tw, spec, bc, epart, H, \
+                                                                     K2);                     \
+        break;
+    switch (k) {
+        SB_FFT4_PLANE_SIZES(SB_F4_PL)
+        default: break;
+    }
+#undef SB_F4_PL
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
 static int launch_zfwd(const SbFftPlan* p, long long* d_qfix, float2* d_spec, int zt,
                        cudaStream_t s) {
     const int rows = p->K[0] * p->K[1];
     if (zt == 0)
         zfwd4(p->K[2] / 2, (rows + SB_F4_ZR - 1) / SB_F4_ZR, p->z.d_tw, p->d_post, d_qfix,
-              d_spec, rows, s);
+              d_spec, rows, p->fused != 0, s);
     else
         k_zfwd<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
             axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_qfix, d_spec, rows, p->K[2]);
@@ -664,7 +709,7 @@ static int launch_zinv(const SbFftPlan* p, const float2* d_spec, float* d_real, 
     const int rows = p->K[0] * p->K[1];
     if (zt == 0)
         zinv4(p->K[2] / 2, (rows + SB_F4_ZR - 1) / SB_F4_ZR, p->z.d_tw, p->d_post, d_spec,
-              d_real, rows, s);
+              d_real, rows, p->fused != 0, s);
     else
         k_zinv<<<(rows + SB_ZROWS - 1) / SB_ZROWS, 256, p->plane_smem, s>>>(
             axis_dev(p->z), p->z.d_iperm, p->z.d_tw, p->d_post, d_spec, d_real, rows, p->K[2]);
@@ -746,6 +791,10 @@ int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream
     p->yt = reg && f4_has(p->K[1]) ? 0 : 16;
     p->xt = reg && f4_has(p->K[0]) ? 0 : 16;
     p->zt = reg && f4_has_z(p->K[2] / 2) ? 0 : 32;
+    // square planes with register transforms on every axis: the y and x passes fused per plane
+    // (same line transforms, same bits)
+    p->fused = p->variant == SB_FFT_AUTO && p->zt == 0 && p->K[0] == p->K[1] &&
+               f4_has_plane(p->K[0]);
     if (p->yt && p->xt) return SB_OK;
     cudaEvent_t a, b;
     SB_CHECK_CUDA(cudaEventCreate(&a));
@@ -777,6 +826,7 @@ int sb_fft_plan_tune(SbFftPlan* p, float2* d_spec, const float* d_bc, cudaStream
 
 int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, cudaStream_t s) {
     SB_TRY(launch_zfwd(p, d_qfix, d_spec, p->zt, s));
+    if (p->fused) return SB_OK;  // the y pass runs inside k_plane4
     return launch_ypass(p, d_spec, 0, p->yt, s);
 }
 
@@ -787,11 +837,17 @@ int sb_fft_xconv_parts(const SbFftPlan* p) {
 
 int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
                       int want_energy, cudaStream_t s, int* nparts_out) {
+    if (p->fused) {
+        // y forward, x forward, x BC, x inverse, y inverse: one block per kz plane
+        if (nparts_out) *nparts_out = p->H;
+        return plane4(p->K[0], p->H, p->x.d_tw, d_spec, d_bc, want_energy ? d_epart : nullptr,
+                      p->H, p->K[2], s);
+    }
     return launch_xconv(p, d_spec, d_bc, want_energy ? d_epart : nullptr, p->xt, s, nparts_out);
 }
 
 int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real,
                          cudaStream_t s) {
-    SB_TRY(launch_ypass(p, const_cast<float2*>(d_spec), 1, p->yt, s));
+    if (!p->fused) SB_TRY(launch_ypass(p, const_cast<float2*>(d_spec), 1, p->yt, s));
     return launch_zinv(p, d_spec, d_real, p->zt, s);
 }

@@ -270,8 +270,9 @@ __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_xconv4(
     }
 }
 
-// real-to-complex along z: int64 grid rows (cleared behind) -> half-spectrum rows
-template <int N1, int N2>
+// real-to-complex along z: int64 grid rows (cleared behind) -> half-spectrum rows; with TR the
+// spectrum is stored plane by plane ([kz][row], for k_plane4) instead of row by row ([row][kz])
+template <int N1, int N2, bool TR>
 __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zfwd4(
     const float2* __restrict__ twz, const float2* __restrict__ post,
     long long* __restrict__ qfix, float2* __restrict__ spec, int nrows) {
@@ -332,16 +333,26 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zfwd4(
         }
     }
     __syncthreads();
-    float2* out = spec + (size_t)r0 * H;
+    if (TR) {
+        // consecutive threads take consecutive rows of one kz plane (coalesced)
 #pragma unroll
-    for (int i = 0; i < ITO; i++) {
-        const int t = threadIdx.x + i * NT;
-        if (t < nr * H) out[t] = D[t];
+        for (int i = 0; i < ITO; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int kz = t / NL, r = t - kz * NL;
+            if (t < NL * H && r < nr) spec[(size_t)kz * nrows + r0 + r] = D[r * H + kz];
+        }
+    } else {
+        float2* out = spec + (size_t)r0 * H;
+#pragma unroll
+        for (int i = 0; i < ITO; i++) {
+            const int t = threadIdx.x + i * NT;
+            if (t < nr * H) out[t] = D[t];
+        }
     }
 }
 
-// complex-to-real along z: half-spectrum rows -> real rows
-template <int N1, int N2>
+// complex-to-real along z: half-spectrum rows -> real rows (TR: spectrum stored plane by plane)
+template <int N1, int N2, bool TR>
 __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zinv4(
     const float2* __restrict__ twz, const float2* __restrict__ post,
     const float2* __restrict__ spec, float* __restrict__ real, int nrows) {
@@ -357,8 +368,23 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zinv4(
     }
     const int r0 = blockIdx.x * NL;
     const int nr = min(NL, nrows - r0);
-    const float2* in = spec + (size_t)r0 * H;
-    {
+    if (TR) {
+        float2 r[ITI];
+#pragma unroll
+        for (int i = 0; i < ITI; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int kz = t / NL, rr = t - kz * NL;
+            r[i] = t < NL * H && rr < nr ? spec[(size_t)kz * nrows + r0 + rr]
+                                         : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < ITI; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int kz = t / NL, rr = t - kz * NL;
+            if (t < NL * H) D[rr * H + kz] = r[i];
+        }
+    } else {
+        const float2* in = spec + (size_t)r0 * H;
         float2 r[ITI];
 #pragma unroll
         for (int i = 0; i < ITI; i++) {
@@ -403,6 +429,88 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zinv4(
         if (t < nr * K2) o[t] = Df[2 * r * H + col];
     }
 }
+
+// The y forward, x forward, Green's function, x inverse and y inverse passes of one kz plane in
+// one block, for square planes (K0 = K1 = K = N1 N2) whose K x K complex points fit in shared
+// memory: the spectrum is stored plane by plane ([kz][x][y], written so by k_zfwd4<TR>), the
+// block loads its plane once, runs the same line transforms as k_ypass4 / k_xconv4 (so the same
+// bits), and stores it once. One block per kz: few blocks, each long, which leaves most SMs to
+// the pair kernel that runs beside the reciprocal chain. Dynamic shared memory: the twiddles (K)
+// and the plane with a row pitch of K + 1 (conflict-free for lines in both directions).
+template <int N1, int N2, int NL>
+__global__ void __launch_bounds__(NL * F4<N1, N2>::T) k_plane4(
+    const float2* __restrict__ tw_in, float2* __restrict__ spec, const float* __restrict__ bc,
+    double* __restrict__ epart, int H, int K2) {
+    constexpr int K = N1 * N2, P = K + 1, NT = NL * F4<N1, N2>::T, IT = K * K / NT;
+    static_assert(K * K % NT == 0 && K % NL == 0, "plane must divide among the threads");
+    extern __shared__ float2 smem_plane[];
+    float2* tw = smem_plane;
+    float2* D = smem_plane + K;
+    __shared__ double red[NT];
+    const int kz = blockIdx.x;
+    float2* plane = spec + (size_t)kz * K * K;
+    for (int t = threadIdx.x; t < K; t += NT) tw[t] = tw_in[t];
+    {
+        float2 r[IT];
+#pragma unroll
+        for (int i = 0; i < IT; i++) r[i] = plane[threadIdx.x + i * NT];
+#pragma unroll
+        for (int i = 0; i < IT; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int x = t / K, y = t - x * K;
+            D[x * P + y] = r[i];
+        }
+    }
+    __syncthreads();
+    for (int l0 = 0; l0 < K; l0 += NL) line_fft4<N1, N2, NL, false>(D + l0 * P, P, 1, tw);
+    for (int l0 = 0; l0 < K; l0 += NL) line_fft4<N1, N2, NL, false>(D + l0, 1, P, tw);
+    const double wkz = (kz == 0 || 2 * kz == K2) ? 1.0 : 2.0;
+    double e = 0.0;
+    {
+        float g[IT];
+#pragma unroll
+        for (int i = 0; i < IT; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int x = t / K, y = t - x * K;
+            g[i] = bc[((size_t)x * K + y) * H + kz];
+        }
+#pragma unroll
+        for (int i = 0; i < IT; i++) {
+            const int t = threadIdx.x + i * NT;
+            const int x = t / K, y = t - x * K;
+            const float2 v = D[x * P + y];
+            if (epart) e += wkz * (double)g[i] * ((double)v.x * v.x + (double)v.y * v.y);
+            D[x * P + y] = make_float2(v.x * g[i], v.y * g[i]);
+        }
+    }
+    __syncthreads();
+    for (int l0 = 0; l0 < K; l0 += NL) line_fft4<N1, N2, NL, true>(D + l0, 1, P, tw);
+    for (int l0 = 0; l0 < K; l0 += NL) line_fft4<N1, N2, NL, true>(D + l0 * P, P, 1, tw);
+#pragma unroll
+    for (int i = 0; i < IT; i++) {
+        const int t = threadIdx.x + i * NT;
+        const int x = t / K, y = t - x * K;
+        plane[t] = D[x * P + y];
+    }
+    if (epart) {
+        // deterministic block reduction (fixed tree over a power-of-two prefix)
+        red[threadIdx.x] = e;
+        __syncthreads();
+        int m = 1;
+        while (m * 2 <= NT) m *= 2;
+        if (threadIdx.x >= m) red[threadIdx.x - m] += red[threadIdx.x];
+        __syncthreads();
+        for (int o = m / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) epart[kz] = 0.5 * red[0];
+    }
+}
+
+// square plane sizes fused by k_plane4: X(K, N1, N2, NL)
+#define SB_FFT4_PLANE_SIZES(X) \
+    X(32, 4, 8, 32) X(48, 6, 8, 16) X(64, 8, 8, 32) X(80, 8, 10, 16) X(96, 8, 12, 32) X(128, 8, 16, 32)
 
 // sizes with a register line transform: X(N, N1, N2). The z passes (half length M = K2 / 2)
 // take the sizes whose 32-row tile fits the static shared-memory limit.

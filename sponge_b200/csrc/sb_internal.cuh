@@ -97,7 +97,9 @@ struct SbFftPlan {
     int yt = 16;
     int xt = 16;
     int zt = 32;
-    int variant = 0;           // SB_FFT_AUTO / SB_FFT_GENERIC
+    int variant = 0;           // SB_FFT_AUTO / SB_FFT_GENERIC / SB_FFT_LINES
+    int fused = 0;             // 1: y and x passes fused per kz plane (k_plane4), spectrum
+                               // stored plane by plane [kz][x][y]
 };
 
 // sets the kernel shape of every pass for the plan's variant, timing the stage kernels' line

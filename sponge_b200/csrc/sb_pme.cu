@@ -463,8 +463,8 @@ extern "C" int sb_pme_set_fft_variant(sb_pme* p, int variant) {
         sb_set_error("sb_pme_set_fft_variant: null handle");
         return SB_ERR_ARG;
     }
-    if (variant != SB_FFT_AUTO && variant != SB_FFT_GENERIC) {
-        sb_set_error("sb_pme_set_fft_variant: variant %d is not AUTO or GENERIC", variant);
+    if (variant != SB_FFT_AUTO && variant != SB_FFT_GENERIC && variant != SB_FFT_LINES) {
+        sb_set_error("sb_pme_set_fft_variant: variant %d is not AUTO, GENERIC or LINES", variant);
         return SB_ERR_ARG;
     }
     if (p->form != SB_FORM_FIXED) return SB_OK;  // the plain form runs the library FFT

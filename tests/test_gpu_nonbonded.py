@@ -125,9 +125,11 @@ def test_reciprocal_force(case):
     name, s, eng, ref = case
     import sponge_b200
     out = {}
-    # both FFT kernel families (register line transforms exist for every grid here); the
-    # default (register) stays in place for the other tests
-    for v in (sponge_b200.FFT_GENERIC, sponge_b200.FFT_AUTO):
+    # every FFT kernel family (register line transforms exist for every grid here; the grids
+    # are square, so the default fuses the y and x passes per plane); the default stays in place
+    # for the other tests
+    energies = {}
+    for v in (sponge_b200.FFT_GENERIC, sponge_b200.FFT_LINES, sponge_b200.FFT_AUTO):
         eng.pme.set_fft_variant(v)
         out[v] = _forces(eng, ("reciprocal",))
         assert rel_rms(out[v], ref["f_rec"]) < FORCE_TOL
@@ -135,7 +137,12 @@ def test_reciprocal_force(case):
         e, parts = eng.pme.Get_Energy(eng.uint_crd, eng.charge, eng.nl, eng.scaler, *eng.excl,
                                       which_part=sponge_b200.PME_TOTAL, parts=True)
         assert parts["reciprocal"] == pytest.approx(ref["e_rec"], rel=1e-5)
+        energies[v] = parts["reciprocal"]
     assert rel_rms(out[sponge_b200.FFT_AUTO], out[sponge_b200.FFT_GENERIC]) < 1e-6
+    # the fused plane kernel runs the same line transforms as the pass-by-pass kernels
+    assert np.array_equal(out[sponge_b200.FFT_AUTO], out[sponge_b200.FFT_LINES])
+    assert energies[sponge_b200.FFT_AUTO] == pytest.approx(energies[sponge_b200.FFT_LINES],
+                                                           rel=1e-12)
 
 
 def test_total_force(case):
