@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(NL * F4<N1, N2>::T) k_plane4(
 
 // square plane sizes fused by k_plane4: X(K, N1, N2, NL)
 #define SB_FFT4_PLANE_SIZES(X) \
-    X(32, 4, 8, 32) X(48, 6, 8, 16) X(64, 8, 8, 32) X(80, 8, 10, 16) X(96, 8, 12, 32) X(128, 8, 16, 32)
+    X(32, 4, 8, 32) X(48, 6, 8, 16) X(64, 8, 8, 64) X(80, 8, 10, 16) X(96, 8, 12, 48) X(128, 8, 16, 64)
 
 // sizes with a register line transform: X(N, N1, N2). The z passes (half length M = K2 / 2)
 // take the sizes whose 32-row tile fits the static shared-memory limit.

@@ -193,6 +193,7 @@ struct sb_lennard_jones {
     double* d_red = nullptr;        // FP64 reduction scratch
     float* d_energy_atom = nullptr; // [N] scratch for Get_Energy
     int ipl = 2;                    // pair kernel shape: 8 or 4 i atoms per lane, 2 = packed
+
                                     // FP32x2 slot pairs, 1 = compacted in-cutoff pairs
 };
 

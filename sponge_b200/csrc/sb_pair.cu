@@ -330,10 +330,13 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
     } while (0)
 #define SB_LAUNCH_X2(EVV)                                                                     \
     do {                                                                                      \
-        k_pair_x2<EVV><<<nl->clu_cap, 32, sizeof(float4) * 4 * lj->ntypes, s>>>(              \
+        k_pair_x2<EVV><<<x2_blocks, 32, sizeof(float4) * 4 * lj->ntypes, s>>>(                \
             P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
             nl->slot_atom, nl->fix, ae, av, ad);                                              \
     } while (0)
+    // packed kernel: one block per cluster (a grid of fewer blocks looping over the clusters
+    // ran slower)
+    const int x2_blocks = nl->clu_cap;
     if (lj->ipl == 2 && !P.wide) {
         switch (ev) {
             case 0: SB_LAUNCH_X2(0); break;

@@ -207,19 +207,15 @@ __device__ __forceinline__ void pair_walk_x2(
     }
 }
 
-// One-warp blocks (see k_pair_fixed); dynamic shared memory: the cluster's LJ table, 4 nt float4.
+// one cluster c (the body of k_pair_x2)
 template <int EV>
-__global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
-    PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
-    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
-    const int* __restrict__ stype, const float2* __restrict__ AB,
+__device__ __forceinline__ void x2_cluster(
+    const PairParams& P, const int c, const int lane, float4* ctab,
+    const int* __restrict__ cl_count, const uint32_t* __restrict__ cl_ent,
+    const uint4* __restrict__ xq, const int* __restrict__ stype, const float2* __restrict__ AB,
     const int* __restrict__ slot_atom, long long* __restrict__ fix,
     float* __restrict__ atom_energy, float* __restrict__ atom_virial,
     float* __restrict__ atom_direct) {
-    extern __shared__ float4 ctab[];
-    const int lane = threadIdx.x & 31;
-    const int c = blockIdx.x;
-    if (c >= meta[0]) return;
     const int base = c * SB_CLUSTER;
     // the loads that start a cluster are issued together: list counts (full and pruned), the
     // prune request, the cluster's atoms; then the first two batches of entries, which arrive
@@ -355,5 +351,27 @@ __global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
                 }
             }
         }
+    }
+}
+
+// One-warp blocks; a block takes clusters blockIdx.x, blockIdx.x + gridDim.x, ... (one each when
+// the grid has a block per cluster). Every cluster's forces go to fixed-point accumulators and
+// its energies to its own atoms, so the assignment does not change a bit. Dynamic shared memory:
+// the cluster's LJ table, 4 nt float4.
+template <int EV>
+__global__ void __launch_bounds__(32, EV ? 12 : 16) k_pair_x2(
+    PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
+    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
+    const int* __restrict__ stype, const float2* __restrict__ AB,
+    const int* __restrict__ slot_atom, long long* __restrict__ fix,
+    float* __restrict__ atom_energy, float* __restrict__ atom_virial,
+    float* __restrict__ atom_direct) {
+    extern __shared__ float4 ctab[];
+    const int lane = threadIdx.x & 31;
+    const int ncl = meta[0];
+    for (int c = blockIdx.x; c < ncl; c += gridDim.x) {
+        x2_cluster<EV>(P, c, lane, ctab, cl_count, cl_ent, xq, stype, AB, slot_atom, fix,
+                       atom_energy, atom_virial, atom_direct);
+        __syncwarp();  // the next cluster rewrites the LJ table
     }
 }
