@@ -363,3 +363,24 @@ def test_config1_full_size(torch_cuda, oracle_lib):
     err = rel_rms(f, fr)
     print("config1 total force rel RMS vs FP64: %.3e" % err)
     assert err < FORCE_TOL
+
+
+@pytest.mark.parametrize("K", [48, 64, 80, 96, 128])
+def test_plane_fft_sizes(K, torch_cuda, oracle_lib):
+    """Every square plane size the fused y-x kernel serves (lines per round 16, 64, 16, 48, 64):
+    the same bits as the pass-by-pass register transforms, and the FP64 reciprocal force."""
+    import sponge_b200
+    from sponge_b200 import NonbondedEngine
+    s = dict(systems.config0(), fft=(K, K, K))
+    eng = NonbondedEngine(s)
+    eng.update_list(forced=1)
+    eng.to_uint()
+    out = {}
+    for v in (sponge_b200.FFT_LINES, sponge_b200.FFT_AUTO):
+        eng.pme.set_fft_variant(v)
+        out[v] = _forces(eng, ("reciprocal",))
+    assert np.array_equal(out[sponge_b200.FFT_AUTO], out[sponge_b200.FFT_LINES])
+    uc = eng.uint_crd.cpu().numpy().view(np.uint32)
+    beta = oracle_lib.get_beta(s["cutoff"], s["tolerance"])
+    f_rec = oracle_lib.pme(uc, s, beta, fft=(K, K, K))[0]
+    assert rel_rms(out[sponge_b200.FFT_AUTO], f_rec) < FORCE_TOL
