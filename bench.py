@@ -399,7 +399,9 @@ def main():
     flops = FLOP_PER_PAIR * n_cut
     achieved = flops / (pair_ms * 1e-3) / 1e12
     rebuilds_per_step = 1.0 / 20
-    launches_force = 11  # pack, pair, exclusion, spread, 5 FFT passes, gather, finalize
+    # pack, pair, spread, z R2C, fused y-x plane pass, z C2R, gather (with the exclusion
+    # correction), finalize
+    launches_force = 8
     launches_rebuild = 6
     line = {
         "metric": METRIC,

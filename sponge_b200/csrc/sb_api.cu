@@ -83,10 +83,10 @@ static int nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* p
             SB_CHECK_CUDA(cudaEventRecord(pme->ev_fork, s));
             SB_CHECK_CUDA(cudaStreamWaitEvent(g, pme->ev_fork, 0));
         }
-        // the per-atom correction energy is only read on energy/virial steps
-        int st = sb_pme_fused_excluded(pme, nl, d_uint_crd, d_charge, es, el, en,
-                                       ev ? d_corr : nullptr, g);
-        if (!st) st = sb_pme_fused_grid(pme, nl, ev, g);
+        // the exclusion correction runs inside the reciprocal gather; the per-atom correction
+        // energy is only read on energy/virial steps
+        int st = sb_pme_zero_atom_energy(pme, ev ? d_corr : nullptr, g);
+        if (!st) st = sb_pme_fused_grid(pme, nl, ev, g, es, el, en, ev ? d_corr : nullptr);
         if (fork) {
             // join even after a failed launch so that a capture in progress stays well formed
             SB_CHECK_CUDA(cudaEventRecord(pme->ev_join, g));

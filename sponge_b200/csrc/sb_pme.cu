@@ -841,9 +841,26 @@ __global__ void k_spread_slot(const int* __restrict__ meta, const uint4* __restr
 
 // reciprocal force gather per slot into the list's slot-order fixed-point accumulators (the
 // buffer the pair and exclusion kernels add to, possibly at the same time: integer adds commute)
+// With EXCL the thread also does the Ewald exclusion correction of its atom (k_excluded_slot's
+// arithmetic on the packed coordinates and charges, which hold the same values): the correction
+// runs at the end of the reciprocal chain instead of in a launch of its own. Its i force enters
+// the slot's accumulator as the same int64 value added to the gather's, so the sums are the same
+// bits.
+struct SbExclPass {
+    const int* slot_atom;
+    const int* atom_slot;
+    const int* es;
+    const int* el;
+    const int* en;
+    float sx, sy, sz, beta, beta2, beta3;
+    float* ene;  // per-atom correction energy (energy steps) or null
+};
+
+template <bool EXCL>
 __global__ void k_gather_slot(const int* __restrict__ meta, const uint4* __restrict__ xq,
                               const float* __restrict__ theta, int K0, int K1, int K2, float ix,
-                              float iy, float iz, long long* __restrict__ fix, int slot_cap) {
+                              float iy, float iz, long long* __restrict__ fix, int slot_cap,
+                              SbExclPass X) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     if (sl >= meta[3]) return;
     const uint4 v = xq[sl];
@@ -890,9 +907,46 @@ __global__ void k_gather_slot(const int* __restrict__ meta, const uint4* __restr
         }
     }
     const float sq = -q;
-    const long long fx = __float2ll_rn(sq * Fx * ix * SB_FORCE_SCALE);
-    const long long fy = __float2ll_rn(sq * Fy * iy * SB_FORCE_SCALE);
-    const long long fz = __float2ll_rn(sq * Fz * iz * SB_FORCE_SCALE);
+    long long fx = __float2ll_rn(sq * Fx * ix * SB_FORCE_SCALE);
+    long long fy = __float2ll_rn(sq * Fy * iy * SB_FORCE_SCALE);
+    long long fz = __float2ll_rn(sq * Fz * iz * SB_FORCE_SCALE);
+    if (EXCL) {
+        // an uncharged atom (returned above) has only zero exclusion terms
+        const int a = X.slot_atom[sl];
+        const int cnt = X.en[a];
+        if (cnt > 0) {
+            const int s0 = X.es[a];
+            float ex = 0.f, ey = 0.f, ez = 0.f, e = 0.f;
+            for (int k = s0; k < s0 + cnt; k++) {
+                const int sj = X.atom_slot[X.el[k]];
+                const uint4 w = xq[sj];
+                const float ddx = __int2float_rn((int)(w.x - v.x)) * X.sx;
+                const float ddy = __int2float_rn((int)(w.y - v.y)) * X.sy;
+                const float ddz = __int2float_rn((int)(w.z - v.z)) * X.sz;
+                const float r2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+                const float qq = q * __uint_as_float(w.w);
+                const float fs = qq * X.beta3 * sb_ewald_G(X.beta2 * r2);
+                const float tx = fs * ddx, ty = fs * ddy, tz = fs * ddz;
+                ex += tx;
+                ey += ty;
+                ez += tz;
+                if (X.ene) {
+                    const float r = sqrtf(r2);
+                    e -= qq * erff(X.beta * r) / r;
+                }
+                atomicAdd((unsigned long long*)&fix[sj],
+                          (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
+                atomicAdd((unsigned long long*)&fix[slot_cap + sj],
+                          (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
+                atomicAdd((unsigned long long*)&fix[2 * slot_cap + sj],
+                          (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
+            }
+            fx += __float2ll_rn(ex * SB_FORCE_SCALE);
+            fy += __float2ll_rn(ey * SB_FORCE_SCALE);
+            fz += __float2ll_rn(ez * SB_FORCE_SCALE);
+            if (X.ene) atomicAdd(&X.ene[a], e);
+        }
+    }
     atomicAdd((unsigned long long*)&fix[sl], (unsigned long long)fx);
     atomicAdd((unsigned long long*)&fix[slot_cap + sl], (unsigned long long)fy);
     atomicAdd((unsigned long long*)&fix[2 * slot_cap + sl], (unsigned long long)fz);
@@ -917,7 +971,16 @@ int sb_pme_fused_excluded(sb_pme* p, sb_neighbor_list* nl, const uint32_t* d_uin
     return SB_OK;
 }
 
-int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s) {
+int sb_pme_zero_atom_energy(sb_pme* p, float* d_atom_energy, cudaStream_t s) {
+    if (d_atom_energy) {
+        k_zero_f<<<(p->n + 1023) / 1024, 1024, 0, s>>>(p->n, d_atom_energy);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s,
+                      const int* es, const int* el, const int* en, float* d_excl_energy) {
     const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
     k_spread_slot<<<(4 * nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->meta, nl->xq, K0, K1, K2,
                                                                  p->d_qfix);
@@ -926,9 +989,21 @@ int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStre
     SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_energy, s,
                              &p->rec_nparts));
     SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
-    k_gather_slot<<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
-        nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0], (float)K1 / p->box[1],
-        (float)K2 / p->box[2], nl->fix, nl->slot_cap);
+    SbExclPass X{};
+    const bool excl = es && el && en;
+    if (excl) {
+        const float b = p->beta;
+        X = SbExclPass{nl->slot_atom, nl->atom_slot, es, el, en,
+                       (1.0f / 4294967296.0f) * p->box[0], (1.0f / 4294967296.0f) * p->box[1],
+                       (1.0f / 4294967296.0f) * p->box[2], b, b * b, b * b * b, d_excl_energy};
+        k_gather_slot<true><<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
+            nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
+            (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, X);
+    } else {
+        k_gather_slot<false><<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
+            nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
+            (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, X);
+    }
     SB_CHECK_LAUNCH();
     return SB_OK;
 }
