@@ -65,6 +65,20 @@ void NEIGHBOR_LIST::Initial(CONTROLLER *controller, int md_atom_numbers, VECTOR 
     Sponge_B200_Check(sb_nl_create(atom_numbers, box, cutoff, skin, refresh_interval, permit,
                                    max_neighbor_numbers, SB_FORM_FIXED, &handle),
                       "NEIGHBOR_LIST::Initial");
+    // pruned pair list (sb_nl_set_prune; off unless neighbor_list_prune_buffer is given)
+    float prune_buffer = 0.f;
+    int prune_interval = 0;
+    if (controller[0].Command_Exist(this->module_name, "prune_buffer"))
+        prune_buffer = atof(controller[0].Command(this->module_name, "prune_buffer"));
+    if (controller[0].Command_Exist(this->module_name, "prune_interval"))
+        prune_interval = atoi(controller[0].Command(this->module_name, "prune_interval"));
+    if (prune_buffer > 0.f)
+    {
+        Sponge_B200_Check(sb_nl_set_prune(handle, prune_buffer, prune_interval),
+                          "NEIGHBOR_LIST::Initial (prune)");
+        controller[0].printf("    pruned pair list: cutoff + %.2f, renewed every %d updates and on moves of %.2f\n",
+                             prune_buffer, prune_interval, 0.5f * prune_buffer);
+    }
     const uint32_t *uc = NULL;
     sb_nl_uint_crd(handle, &uc);
     uint_crd = (UNSIGNED_INT_VECTOR *)uc;

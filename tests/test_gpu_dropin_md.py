@@ -1,0 +1,110 @@
+"""The drop-in modules inside the reference's own MD driver.
+
+oracle/ref_harness/build_sponge.sh builds SPONGE's unchanged main.cu and modules twice into
+oracle/_ref/: `sponge_stock` (the reference as shipped) and `sponge_b200` (NEIGHBOR_LIST,
+LENNARD_JONES_INFORMATION and Particle_Mesh_Ewald replaced by sponge_b200/dropin, linked to
+libsponge_b200.so). Both run the same generated water box (3,000 atoms, rc 8 A, PME 32^3, harmonic
+bonds, NVE, 1 fs) from the same input files for 40 steps, and the energies they print every
+10 steps (potential, LJ, PME, bond, temperature) agree within 2e-4 of their size: the printed PME
+energy of the stock build sits about 1.5e-4 from the FP64 value (its B-spline moduli and energy
+sums are FP32; the reference's own energies meet the FP64 oracle only to 1e-4 in
+tests/test_golden.py), while the drop-in's match FP64 to 1e-5. The drop-in with the pruned pair
+list (neighbor_list_prune_buffer 0.5, prune_interval 5) prints the same energies as without it.
+Skipped where the two binaries have not been built.
+"""
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from sponge_b200 import sponge_io, systems
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+STOCK = os.path.join(ROOT, "oracle", "_ref", "sponge_stock")
+B200 = os.path.join(ROOT, "oracle", "_ref", "sponge_b200")
+
+
+def _mdin(paths, outdir, extra=""):
+    return """water box, drop-in parity run
+mode = NVE
+dt = 1e-3
+step_limit = 40
+write_information_interval = 10
+cutoff = 8.0
+skin = 2.0
+neighbor_list_refresh_interval = 10
+neighbor_list_max_neighbor_numbers = 1200
+PME_fftx = 32
+PME_ffty = 32
+PME_fftz = 32
+coordinate_in_file = {coordinate}
+mass_in_file = {mass}
+charge_in_file = {charge}
+LJ_in_file = {LJ}
+exclude_in_file = {exclude}
+bond_in_file = {bond}
+residue_in_file = {residue}
+mdout = {out}/mdout.txt
+mdinfo = {out}/mdinfo.txt
+box = {out}/mdbox.txt
+crd = {out}/mdcrd.dat
+rst = {out}/restart
+end_pause = 0
+dont_check_input = 1
+device = 0
+{extra}
+""".format(out=outdir, extra=extra, **paths)
+
+
+def _run(binary, paths, outdir, extra=""):
+    os.makedirs(outdir, exist_ok=True)
+    mdin = os.path.join(outdir, "mdin.txt")
+    with open(mdin, "w") as f:
+        f.write(_mdin(paths, outdir, extra))
+    r = subprocess.run([binary, "-mdin", mdin], cwd=outdir, stdin=subprocess.DEVNULL,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    lines = [l.split() for l in open(os.path.join(outdir, "mdout.txt")) if l.strip()]
+    head = lines[0]
+    rows = np.array([[float(x) for x in l] for l in lines[1:]], np.float64)
+    return {k: rows[:, i] for i, k in enumerate(head)}
+
+
+@pytest.fixture(scope="module")
+def runs(tmp_path_factory):
+    if not (os.path.exists(STOCK) and os.path.exists(B200)):
+        pytest.skip("oracle/_ref/sponge_stock and sponge_b200 not built "
+                    "(oracle/ref_harness/build_sponge.sh both)")
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    base = tmp_path_factory.mktemp("dropin_md")
+    paths = sponge_io.write_inputs(systems.config0(), str(base / "inputs"), prefix="water")
+    out = {
+        "stock": _run(STOCK, paths, str(base / "stock")),
+        "b200": _run(B200, paths, str(base / "b200")),
+        "b200_pruned": _run(B200, paths, str(base / "b200_pruned"),
+                            "neighbor_list_prune_buffer = 0.5\nneighbor_list_prune_interval = 5"),
+    }
+    return out
+
+
+def test_drop_in_matches_stock_driver(runs):
+    a, b = runs["stock"], runs["b200"]
+    assert len(a["step"]) >= 4 and list(a["step"]) == list(b["step"])
+    for key in ("potential", "LJ", "PME", "bond"):
+        scale = np.abs(a[key]).max()
+        err = np.abs(a[key] - b[key]).max()
+        print("%-10s stock %s b200 %s" % (key, a[key], b[key]))
+        assert err <= 2e-4 * scale + 0.05, key
+    assert np.allclose(a["temperature"], b["temperature"], rtol=1e-3, atol=0.05)
+
+
+def test_pruned_list_in_driver(runs):
+    b, p = runs["b200"], runs["b200_pruned"]
+    for key in ("potential", "LJ", "PME", "bond", "temperature"):
+        assert np.allclose(b[key], p[key], rtol=1e-5, atol=0.02), key
