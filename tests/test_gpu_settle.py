@@ -54,7 +54,8 @@ class Case:
         self.mass = np.asarray(mass, np.float32)
         self.n = self.mass.size
         self.dt = dt
-        inv = np.where(self.mass == 0, 0.0, 1.0 / self.mass.astype(np.float64)).astype(np.float32)
+        m64 = self.mass.astype(np.float64)
+        inv = np.divide(1.0, m64, out=np.zeros_like(m64), where=m64 != 0).astype(np.float32)
         dev = lambda x: torch.tensor(np.ascontiguousarray(x), device="cuda")  # noqa: E731
         self.vel0, self.crd0 = dev(np.asarray(vel, np.float32)), dev(np.asarray(crd, np.float32))
         self.uc = dev(np.ascontiguousarray(uc, np.uint32).view(np.int32))
