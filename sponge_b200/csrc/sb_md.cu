@@ -104,19 +104,25 @@ __device__ __forceinline__ float3 fdisp(float3 a, float3 b, float3 L) {
     return d;
 }
 
-// MD_Iteration_Leap_Frog (MD_core.cu:13-32): a = F/m; v += dt a; x += dt v
+// MD_Iteration_Leap_Frog (MD_core.cu:13-32) on values in registers: a = F/m; v += dt a;
+// x += dt v
+__device__ __forceinline__ void leap_frog_regs(float im, float3 f, float3& v, float3& x,
+                                               float3& a, float dt) {
+    a = f3(im * f.x, im * f.y, im * f.z);
+    v = f3(v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z);
+    x = f3(x.x + dt * v.x, x.y + dt * v.y, x.z + dt * v.z);
+}
+
+// the same on atom i in memory
 __device__ __forceinline__ void leap_frog_atom(int i, const float* __restrict__ inv_mass,
                                                const float* __restrict__ frc, float* __restrict__ vel,
                                                float* __restrict__ crd, float* __restrict__ acc,
                                                float dt) {
-    const float im = inv_mass[i];
-    const float3 a = f3(im * frc[3 * i], im * frc[3 * i + 1], im * frc[3 * i + 2]);
+    float3 v = ld3(vel, i), x = ld3(crd, i), a;
+    leap_frog_regs(inv_mass[i], ld3(frc, i), v, x, a, dt);
     if (acc) st3(acc, i, a);
-    float3 v = ld3(vel, i);
-    v = f3(v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z);
     st3(vel, i, v);
-    const float3 x = ld3(crd, i);
-    st3(crd, i, f3(x.x + dt * v.x, x.y + dt * v.y, x.z + dt * v.z));
+    st3(crd, i, x);
 }
 
 // SETTLE_DO_TRIANGLE (SETTLE.cu:93-176): positions relative to the centre of mass
@@ -171,25 +177,38 @@ __device__ __forceinline__ void settle_do_triangle(float3 rB0, float3 rC0, float
 }
 
 // settle_triangle (SETTLE.cu:349-380) on one triangle whose edge vectors at the step start are
-// BA, CA
+// BA, CA, on positions and velocities in registers (updated in place)
+__device__ __forceinline__ void settle_triangle_regs(const SbTri& T, float3 BA, float3 CA,
+                                                     float mA, float mB, float mC, float3& xA,
+                                                     float3& xB, float3& xC, float3& vA,
+                                                     float3& vB, float3& vC, float3 L, float dt,
+                                                     float vf, float xf, float& vir) {
+    float3 rA = xA;
+    float3 rB = fdisp(xB, rA, L);
+    float3 rC = fdisp(xC, rA, L);
+    const float3 rO = (1.0f / (mA + mB + mC)) * (mB * rB + mC * rC) + rA;
+    rA = rA - rO;
+    rB = rB + rA;
+    rC = rC + rA;
+    settle_do_triangle(BA, CA, rA, rB, rC, T, mB, mC, dt, xf, vf, vA, vB, vC, vir);
+    xA = rA + rO;
+    xB = rB + rO;
+    xC = rC + rO;
+}
+
+// the same on a triangle in memory
 __device__ __forceinline__ void settle_triangle_one(const SbTri& T, float3 BA, float3 CA,
                                                     const float* __restrict__ mass,
                                                     float* __restrict__ crd, float* __restrict__ vel,
                                                     float3 L, float dt, float vf, float xf,
                                                     float& vir) {
-    float3 rA = ld3(crd, T.A);
-    float3 rB = fdisp(ld3(crd, T.B), rA, L);
-    float3 rC = fdisp(ld3(crd, T.C), rA, L);
-    const float mA = mass[T.A], mB = mass[T.B], mC = mass[T.C];
-    const float3 rO = (1.0f / (mA + mB + mC)) * (mB * rB + mC * rC) + rA;
-    rA = rA - rO;
-    rB = rB + rA;
-    rC = rC + rA;
+    float3 xA = ld3(crd, T.A), xB = ld3(crd, T.B), xC = ld3(crd, T.C);
     float3 vA = ld3(vel, T.A), vB = ld3(vel, T.B), vC = ld3(vel, T.C);
-    settle_do_triangle(BA, CA, rA, rB, rC, T, mB, mC, dt, xf, vf, vA, vB, vC, vir);
-    st3(crd, T.A, rA + rO);
-    st3(crd, T.B, rB + rO);
-    st3(crd, T.C, rC + rO);
+    settle_triangle_regs(T, BA, CA, mass[T.A], mass[T.B], mass[T.C], xA, xB, xC, vA, vB, vC, L,
+                         dt, vf, xf, vir);
+    st3(crd, T.A, xA);
+    st3(crd, T.B, xB);
+    st3(crd, T.C, xC);
     st3(vel, T.A, vA);
     st3(vel, T.B, vB);
     st3(vel, T.C, vC);
@@ -265,12 +284,31 @@ __global__ void k_md_step(int ntri, int npair, int nfree, const SbTri* __restric
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     float v = 0.f;
     if (t < ntri) {
+        // every load of the triangle is issued before the arithmetic, which then runs on
+        // registers (the same operations as the separate calls)
         const SbTri T = tri[t];
         const float3 BA = udisp(uc, T.B, T.A, s), CA = udisp(uc, T.C, T.A, s);
-        leap_frog_atom(T.A, inv_mass, frc, vel, crd, acc, dt);
-        leap_frog_atom(T.B, inv_mass, frc, vel, crd, acc, dt);
-        leap_frog_atom(T.C, inv_mass, frc, vel, crd, acc, dt);
-        settle_triangle_one(T, BA, CA, mass, crd, vel, L, dt, vf, xf, v);
+        float3 xA = ld3(crd, T.A), xB = ld3(crd, T.B), xC = ld3(crd, T.C);
+        float3 vA = ld3(vel, T.A), vB = ld3(vel, T.B), vC = ld3(vel, T.C);
+        const float3 fA = ld3(frc, T.A), fB = ld3(frc, T.B), fC = ld3(frc, T.C);
+        const float iA = inv_mass[T.A], iB = inv_mass[T.B], iC = inv_mass[T.C];
+        const float mA = mass[T.A], mB = mass[T.B], mC = mass[T.C];
+        float3 aA, aB, aC;
+        leap_frog_regs(iA, fA, vA, xA, aA, dt);
+        leap_frog_regs(iB, fB, vB, xB, aB, dt);
+        leap_frog_regs(iC, fC, vC, xC, aC, dt);
+        if (acc) {
+            st3(acc, T.A, aA);
+            st3(acc, T.B, aB);
+            st3(acc, T.C, aC);
+        }
+        settle_triangle_regs(T, BA, CA, mA, mB, mC, xA, xB, xC, vA, vB, vC, L, dt, vf, xf, v);
+        st3(crd, T.A, xA);
+        st3(crd, T.B, xB);
+        st3(crd, T.C, xC);
+        st3(vel, T.A, vA);
+        st3(vel, T.B, vB);
+        st3(vel, T.C, vC);
         vir[t] = v;
     } else if (t < ntri + npair) {
         const SbCPair P = pr[t - ntri];
