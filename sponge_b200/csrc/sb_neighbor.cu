@@ -293,7 +293,6 @@ __global__ void __launch_bounds__(32 * SB_SEARCH_WARPS) k_search(
         s_hi[SB_SEARCH_WARPS][SB_CLUSTER];
     __shared__ uint32_t s_u[SB_SEARCH_WARPS][SB_CLUSTER], s_v[SB_SEARCH_WARPS][SB_CLUSTER],
         s_w[SB_SEARCH_WARPS][SB_CLUSTER];
-    __shared__ float4 s_r[SB_SEARCH_WARPS][SB_CLUSTER];
     extern __shared__ int s_ranges[];  // per warp: max_ranges starts, max_ranges + 1 prefixes
     if (refresh_flag && refresh_flag[0] == 0) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -340,7 +339,18 @@ __global__ void __launch_bounds__(32 * SB_SEARCH_WARPS) k_search(
     ex = __shfl_sync(0xffffffffu, ex, 0);
     ey = __shfl_sync(0xffffffffu, ey, 0);
     ez = __shfl_sync(0xffffffffu, ez, 0);
-    if (lane < SB_CLUSTER) s_r[wid][lane] = make_float4(mxr, myr, mzr, 0.f);
+    // the cluster's relative coordinates, negated, as slot pairs (2p, 2p+1) in every lane: the
+    // candidate tests run on packed FP32x2 arithmetic (each half rounds as the scalar operation)
+    float2 nrx[SB_CLUSTER / 2], nry[SB_CLUSTER / 2], nrz[SB_CLUSTER / 2];
+#pragma unroll
+    for (int p = 0; p < SB_CLUSTER / 2; p++) {
+        nrx[p] = make_float2(-__shfl_sync(0xffffffffu, mxr, 2 * p),
+                             -__shfl_sync(0xffffffffu, mxr, 2 * p + 1));
+        nry[p] = make_float2(-__shfl_sync(0xffffffffu, myr, 2 * p),
+                             -__shfl_sync(0xffffffffu, myr, 2 * p + 1));
+        nrz[p] = make_float2(-__shfl_sync(0xffffffffu, mzr, 2 * p),
+                             -__shfl_sync(0xffffffffu, mzr, 2 * p + 1));
+    }
     __syncwarp();
     // exact-path flag: the cluster-relative float frame of the pair kernel is a faithful
     // minimum image only while cs + (extent of the cluster from its first atom) < L/2
@@ -450,13 +460,18 @@ __global__ void __launch_bounds__(32 * SB_SEARCH_WARPS) k_search(
                 const float yj = __int2float_rn((int)(jv - v0)) * P.sy;
                 const float zj = __int2float_rn((int)(jw - w0)) * P.sz;
                 unsigned notfar = 0;
+                const float2 xj2 = make_float2(xj, xj), yj2 = make_float2(yj, yj),
+                             zj2 = make_float2(zj, zj);
 #pragma unroll
-                for (int k = 0; k < SB_CLUSTER; k++) {
-                    const float4 rk = s_r[wid][k];
-                    const float ddx = xj - rk.x, ddy = yj - rk.y, ddz = zj - rk.z;
-                    const float r2a = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
-                    near |= (r2a < cs2_lo ? 1u : 0u) << k;
-                    notfar |= (r2a <= cs2_hi ? 1u : 0u) << k;
+                for (int p = 0; p < SB_CLUSTER / 2; p++) {
+                    // xj + (-r) rounds as xj - r
+                    const float2 ddx = __fadd2_rn(xj2, nrx[p]), ddy = __fadd2_rn(yj2, nry[p]),
+                                 ddz = __fadd2_rn(zj2, nrz[p]);
+                    const float2 r2a =
+                        __ffma2_rn(ddx, ddx, __ffma2_rn(ddy, ddy, __fmul2_rn(ddz, ddz)));
+                    near |= ((r2a.x < cs2_lo ? 1u : 0u) | (r2a.y < cs2_lo ? 2u : 0u)) << (2 * p);
+                    notfar |= ((r2a.x <= cs2_hi ? 1u : 0u) | (r2a.y <= cs2_hi ? 2u : 0u))
+                              << (2 * p);
                 }
                 border = notfar & ~near;
             }
