@@ -271,6 +271,21 @@ def run_fep(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def hbm_view(traffic_bytes, ms):
+    """The pair kernel's DRAM traffic rate against the measured HBM copy rate of this GPU type
+    (MEASURED_PEAKS.json beside this file), or the pool's earlier measurement where that file is
+    absent."""
+    peak, src = 6650.0, "fallback"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, src = float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        pass
+    achieved = traffic_bytes / (ms * 1e-3) / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": src}
+
+
 def time_integrator(eng, s, flush, stream, reps=20):
     """Device time of the fused NVE leap-frog + SETTLE launch (sb_md_nve_settle_step) on the
     bench box (waters rigid by SETTLE, solute atoms free), with zero forces and velocities so the
@@ -459,7 +474,10 @@ def main():
                      "kernel": "%s (LJ + Ewald direct; timed with its pack kernel)"
                                % PAIR_KERNEL.get(pair_shape, "k_pair_fixed"),
                      "kernel_ms": pair_ms, "pairs_in_cutoff": n_cut, "pairs_in_list": n_list,
-                     "peak_note": "nominal FP32 peak 148 SM x 128 lanes x 2 x 1.965 GHz"},
+                     "peak_note": "nominal FP32 peak 148 SM x 128 lanes x 2 x 1.965 GHz (the "
+                                  "measured peaks cover HBM copy and bf16 tensor throughput "
+                                  "only); the kernel is bound by instruction issue",
+                     "hbm": hbm_view(PAIR_DRAM_BYTES, pair_ms)},
         "integrator": None if md_ms is None else {
             "kernel": "k_md_step: NVE leap-frog + SETTLE of 31,000 rigid waters and 3,000 free "
                       "atoms in one launch (the call after the force step; not in the step above)",
