@@ -73,10 +73,10 @@ static int nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* p
         SB_TRY(sb_nl_ensure_built(nl));
         cudaStream_t s = sb_stream(stream);
         const int ev = need_energy > 0 || need_virial > 0;
-        SB_TRY(sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s));
-        // the exclusion correction and the reciprocal grid chain depend only on the packed
-        // slots; with overlap on they run on the module's side stream while the pair kernel
-        // runs here (the force buffer takes integer adds, so the order cannot change a bit)
+        // the reciprocal grid chain (with the exclusion correction in its gather) reads the
+        // atom-order coordinates and charges, so it needs no packing: with overlap on it runs on
+        // the module's side stream from the start while the packing and the pair kernel run
+        // here (the force buffer takes integer adds, so the order cannot change a bit)
         const bool fork = pme->overlap && pme->side;
         cudaStream_t g = fork ? pme->side : s;
         if (fork) {
@@ -86,12 +86,17 @@ static int nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* p
         // the exclusion correction runs inside the reciprocal gather; the per-atom correction
         // energy is only read on energy/virial steps
         int st = sb_pme_zero_atom_energy(pme, ev ? d_corr : nullptr, g);
-        if (!st) st = sb_pme_fused_grid(pme, nl, ev, g, es, el, en, ev ? d_corr : nullptr);
+        if (!st)
+            st = sb_pme_fused_grid_atoms(pme, nl, ev, g, d_uint_crd, d_charge, es, el, en,
+                                         ev ? d_corr : nullptr);
         if (fork) {
             // join even after a failed launch so that a capture in progress stays well formed
             SB_CHECK_CUDA(cudaEventRecord(pme->ev_join, g));
         }
-        int st2 = sb_lj_fused_pair(lj, nl, pme->beta, need_energy, d_atom_energy, need_virial,
+        // the pair kernel's packed slots (issued after the fork, so the side chain starts first)
+        int st2 = sb_nl_pack(nl, d_uint_crd, d_charge, lj->d_type, s);
+        if (!st2)
+            st2 = sb_lj_fused_pair(lj, nl, pme->beta, need_energy, d_atom_energy, need_virial,
                                    d_atom_virial, d_direct, s);
         if (!st2)
             st2 = sb_lj_long_range_correction(lj, need_virial, d_virial, need_energy,

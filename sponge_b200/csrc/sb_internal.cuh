@@ -253,12 +253,14 @@ int sb_lj_fused_pair(sb_lennard_jones* lj, sb_neighbor_list* nl, float pme_beta,
 // inverse FFT into d_theta, gather of the slot forces into the list's fixed-point buffer) and
 // the finish (finalisation of that buffer into d_frc, energy and virial sums), which must follow
 // the pair and exclusion kernels
-// spread, FFT, convolution and gather of the packed slots into the slot accumulators; with the
-// exclusion CSR given, the gather also does the exclusion correction (d_excl_energy: per-atom
-// correction energy, zeroed first by sb_pme_zero_atom_energy, or null)
-int sb_pme_fused_grid(sb_pme* pme, sb_neighbor_list* nl, int want_energy, cudaStream_t s,
-                      const int* es = nullptr, const int* el = nullptr, const int* en = nullptr,
-                      float* d_excl_energy = nullptr);
+// spread, FFT, convolution and gather of the packed slots into the slot accumulators
+int sb_pme_fused_grid(sb_pme* pme, sb_neighbor_list* nl, int want_energy, cudaStream_t s);
+// the same from the atom-order fixed-point coordinates and charges (no packing needed), the gather
+// also doing the exclusion correction when the CSR is given (d_excl_energy: per-atom correction
+// energy, zeroed first by sb_pme_zero_atom_energy, or null)
+int sb_pme_fused_grid_atoms(sb_pme* pme, sb_neighbor_list* nl, int want_energy, cudaStream_t s,
+                            const uint32_t* d_uint_crd, const float* d_charge, const int* es,
+                            const int* el, const int* en, float* d_excl_energy);
 int sb_pme_zero_atom_energy(sb_pme* pme, float* d_atom_energy, cudaStream_t s);
 int sb_pme_fused_finish(sb_pme* pme, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
                         int need_virial, int need_energy, float* d_virial, float* d_potential,

@@ -841,11 +841,8 @@ __global__ void k_spread_slot(const int* __restrict__ meta, const uint4* __restr
 
 // reciprocal force gather per slot into the list's slot-order fixed-point accumulators (the
 // buffer the pair and exclusion kernels add to, possibly at the same time: integer adds commute)
-// With EXCL the thread also does the Ewald exclusion correction of its atom (k_excluded_slot's
-// arithmetic on the packed coordinates and charges, which hold the same values): the correction
-// runs at the end of the reciprocal chain instead of in a launch of its own. Its i force enters
-// the slot's accumulator as the same int64 value added to the gather's, so the sums are the same
-// bits.
+// Ewald exclusion correction of one atom inside a reciprocal gather (k_gather_atom):
+// k_excluded_slot's arithmetic, its terms added to the slot accumulators as the same int64 values
 struct SbExclPass {
     const int* slot_atom;
     const int* atom_slot;
@@ -856,11 +853,9 @@ struct SbExclPass {
     float* ene;  // per-atom correction energy (energy steps) or null
 };
 
-template <bool EXCL>
 __global__ void k_gather_slot(const int* __restrict__ meta, const uint4* __restrict__ xq,
                               const float* __restrict__ theta, int K0, int K1, int K2, float ix,
-                              float iy, float iz, long long* __restrict__ fix, int slot_cap,
-                              SbExclPass X) {
+                              float iy, float iz, long long* __restrict__ fix, int slot_cap) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     if (sl >= meta[3]) return;
     const uint4 v = xq[sl];
@@ -907,46 +902,9 @@ __global__ void k_gather_slot(const int* __restrict__ meta, const uint4* __restr
         }
     }
     const float sq = -q;
-    long long fx = __float2ll_rn(sq * Fx * ix * SB_FORCE_SCALE);
-    long long fy = __float2ll_rn(sq * Fy * iy * SB_FORCE_SCALE);
-    long long fz = __float2ll_rn(sq * Fz * iz * SB_FORCE_SCALE);
-    if (EXCL) {
-        // an uncharged atom (returned above) has only zero exclusion terms
-        const int a = X.slot_atom[sl];
-        const int cnt = X.en[a];
-        if (cnt > 0) {
-            const int s0 = X.es[a];
-            float ex = 0.f, ey = 0.f, ez = 0.f, e = 0.f;
-            for (int k = s0; k < s0 + cnt; k++) {
-                const int sj = X.atom_slot[X.el[k]];
-                const uint4 w = xq[sj];
-                const float ddx = __int2float_rn((int)(w.x - v.x)) * X.sx;
-                const float ddy = __int2float_rn((int)(w.y - v.y)) * X.sy;
-                const float ddz = __int2float_rn((int)(w.z - v.z)) * X.sz;
-                const float r2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
-                const float qq = q * __uint_as_float(w.w);
-                const float fs = qq * X.beta3 * sb_ewald_G(X.beta2 * r2);
-                const float tx = fs * ddx, ty = fs * ddy, tz = fs * ddz;
-                ex += tx;
-                ey += ty;
-                ez += tz;
-                if (X.ene) {
-                    const float r = sqrtf(r2);
-                    e -= qq * erff(X.beta * r) / r;
-                }
-                atomicAdd((unsigned long long*)&fix[sj],
-                          (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
-                atomicAdd((unsigned long long*)&fix[slot_cap + sj],
-                          (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
-                atomicAdd((unsigned long long*)&fix[2 * slot_cap + sj],
-                          (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
-            }
-            fx += __float2ll_rn(ex * SB_FORCE_SCALE);
-            fy += __float2ll_rn(ey * SB_FORCE_SCALE);
-            fz += __float2ll_rn(ez * SB_FORCE_SCALE);
-            if (X.ene) atomicAdd(&X.ene[a], e);
-        }
-    }
+    const long long fx = __float2ll_rn(sq * Fx * ix * SB_FORCE_SCALE);
+    const long long fy = __float2ll_rn(sq * Fy * iy * SB_FORCE_SCALE);
+    const long long fz = __float2ll_rn(sq * Fz * iz * SB_FORCE_SCALE);
     atomicAdd((unsigned long long*)&fix[sl], (unsigned long long)fx);
     atomicAdd((unsigned long long*)&fix[slot_cap + sl], (unsigned long long)fy);
     atomicAdd((unsigned long long*)&fix[2 * slot_cap + sl], (unsigned long long)fz);
@@ -979,8 +937,7 @@ int sb_pme_zero_atom_energy(sb_pme* p, float* d_atom_energy, cudaStream_t s) {
     return SB_OK;
 }
 
-int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s,
-                      const int* es, const int* el, const int* en, float* d_excl_energy) {
+int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s) {
     const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
     k_spread_slot<<<(4 * nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->meta, nl->xq, K0, K1, K2,
                                                                  p->d_qfix);
@@ -989,21 +946,128 @@ int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStre
     SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_energy, s,
                              &p->rec_nparts));
     SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
-    SbExclPass X{};
-    const bool excl = es && el && en;
-    if (excl) {
-        const float b = p->beta;
-        X = SbExclPass{nl->slot_atom, nl->atom_slot, es, el, en,
-                       (1.0f / 4294967296.0f) * p->box[0], (1.0f / 4294967296.0f) * p->box[1],
-                       (1.0f / 4294967296.0f) * p->box[2], b, b * b, b * b * b, d_excl_energy};
-        k_gather_slot<true><<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
-            nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
-            (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, X);
-    } else {
-        k_gather_slot<false><<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
-            nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
-            (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, X);
+    k_gather_slot<<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
+        nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0], (float)K1 / p->box[1],
+        (float)K2 / p->box[2], nl->fix, nl->slot_cap);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+// reciprocal gather of atom i (atom order, from the fixed-point coordinates and charges) into its
+// slot's fixed-point accumulator, followed by the atom's exclusion correction: the same int64
+// terms as k_gather_slot + k_excluded_slot, from data that needs no packing
+__global__ void k_gather_atom(int n, const uint32_t* __restrict__ uc, const float* __restrict__ qa,
+                              const float* __restrict__ theta, int K0, int K1, int K2, float ix,
+                              float iy, float iz, long long* __restrict__ fix, int slot_cap,
+                              SbExclPass X) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float q = qa[i];
+    if (q == 0.f) return;  // an uncharged atom has zero reciprocal force and exclusion terms
+    const uint32_t ux = uc[3 * i], uy = uc[3 * i + 1], uz = uc[3 * i + 2];
+    const int sl = X.atom_slot[i];
+    int b0, b1, b2;
+    float f0, f1, f2;
+    grid_coord(ux, K0, b0, f0);
+    grid_coord(uy, K1, b1, f1);
+    grid_coord(uz, K2, b2, f2);
+    float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+    bspline4(f0, wx);
+    bspline4(f1, wy);
+    bspline4(f2, wz);
+    bspline4d(f0, dx);
+    bspline4d(f1, dy);
+    bspline4d(f2, dz);
+    int gz[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int g = b2 - k;
+        gz[k] = g < 0 ? g + K2 : g;
     }
+    float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+#pragma unroll
+    for (int kx = 0; kx < 4; kx++) {
+        int gx = b0 - kx;
+        if (gx < 0) gx += K0;
+#pragma unroll
+        for (int ky = 0; ky < 4; ky++) {
+            int gy = b1 - ky;
+            if (gy < 0) gy += K1;
+            const float* row = theta + ((size_t)gx * K1 + gy) * K2;
+            float sw = 0.f, sd = 0.f;
+#pragma unroll
+            for (int kz = 0; kz < 4; kz++) {
+                const float t = row[gz[kz]];
+                sw = fmaf(t, wz[kz], sw);
+                sd = fmaf(t, dz[kz], sd);
+            }
+            Fx = fmaf(dx[kx] * wy[ky], sw, Fx);
+            Fy = fmaf(wx[kx] * dy[ky], sw, Fy);
+            Fz = fmaf(wx[kx] * wy[ky], sd, Fz);
+        }
+    }
+    const float sq = -q;
+    long long fx = __float2ll_rn(sq * Fx * ix * SB_FORCE_SCALE);
+    long long fy = __float2ll_rn(sq * Fy * iy * SB_FORCE_SCALE);
+    long long fz = __float2ll_rn(sq * Fz * iz * SB_FORCE_SCALE);
+    const int cnt = X.en ? X.en[i] : 0;
+    if (cnt > 0) {
+        const int s0 = X.es[i];
+        float ex = 0.f, ey = 0.f, ez = 0.f, e = 0.f;
+        for (int k = s0; k < s0 + cnt; k++) {
+            const int j = X.el[k];
+            const int sj = X.atom_slot[j];
+            const float ddx = __int2float_rn((int)(uc[3 * j] - ux)) * X.sx;
+            const float ddy = __int2float_rn((int)(uc[3 * j + 1] - uy)) * X.sy;
+            const float ddz = __int2float_rn((int)(uc[3 * j + 2] - uz)) * X.sz;
+            const float r2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+            const float qq = q * qa[j];
+            const float fs = qq * X.beta3 * sb_ewald_G(X.beta2 * r2);
+            const float tx = fs * ddx, ty = fs * ddy, tz = fs * ddz;
+            ex += tx;
+            ey += ty;
+            ez += tz;
+            if (X.ene) {
+                const float r = sqrtf(r2);
+                e -= qq * erff(X.beta * r) / r;
+            }
+            atomicAdd((unsigned long long*)&fix[sj],
+                      (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
+            atomicAdd((unsigned long long*)&fix[slot_cap + sj],
+                      (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
+            atomicAdd((unsigned long long*)&fix[2 * slot_cap + sj],
+                      (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
+        }
+        fx += __float2ll_rn(ex * SB_FORCE_SCALE);
+        fy += __float2ll_rn(ey * SB_FORCE_SCALE);
+        fz += __float2ll_rn(ez * SB_FORCE_SCALE);
+        if (X.ene) atomicAdd(&X.ene[i], e);
+    }
+    atomicAdd((unsigned long long*)&fix[sl], (unsigned long long)fx);
+    atomicAdd((unsigned long long*)&fix[slot_cap + sl], (unsigned long long)fy);
+    atomicAdd((unsigned long long*)&fix[2 * slot_cap + sl], (unsigned long long)fz);
+}
+
+int sb_pme_fused_grid_atoms(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s,
+                            const uint32_t* d_uint_crd, const float* d_charge, const int* es,
+                            const int* el, const int* en, float* d_excl_energy) {
+    const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2], n = p->n;
+    k_spread<true><<<(4 * n + 255) / 256, 256, 0, s>>>(n, d_uint_crd, d_charge, K0, K1, K2,
+                                                       p->d_qfix, nullptr);
+    SB_CHECK_LAUNCH();
+    SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
+    SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_energy, s,
+                             &p->rec_nparts));
+    SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+    const float b = p->beta;
+    const bool excl = es && el && en;
+    const SbExclPass X{nl->slot_atom, nl->atom_slot, excl ? es : nullptr, excl ? el : nullptr,
+                       excl ? en : nullptr, (1.0f / 4294967296.0f) * p->box[0],
+                       (1.0f / 4294967296.0f) * p->box[1], (1.0f / 4294967296.0f) * p->box[2],
+                       b, b * b, b * b * b, d_excl_energy};
+    k_gather_atom<<<(n + 127) / 128, 128, 0, s>>>(
+        n, d_uint_crd, d_charge, p->d_theta, K0, K1, K2, (float)K0 / p->box[0],
+        (float)K1 / p->box[1], (float)K2 / p->box[2], nl->fix, nl->slot_cap, X);
     SB_CHECK_LAUNCH();
     return SB_OK;
 }
