@@ -318,6 +318,92 @@ def time_integrator(eng, s, flush, stream, reps=20):
     return float(np.mean([a.elapsed_time(b) for a, b in ev]))
 
 
+MODULES_METRIC = "us per call, SPONGE's covid-tip4p modules beside the nonbonded path, 1 B200"
+
+
+def run_modules(args, rank, world, local):
+    """Device time per call of the modules beside the nonbonded path on the reference's own real
+    system (covid-tip4p, 98,282 atoms; tests/golden fixture): the 1-4 pairs (force, atom energy
+    and virial), the virtual atoms (coordinate refresh, force redistribution), and the NVE
+    leap-frog with SETTLE as separate module calls (the system keeps constraint pairs that SETTLE
+    leaves to another scheme, so the fused launch does not apply). CUDA events, L2 flushed before
+    every call. Rank 0 only."""
+    import importlib.util
+    import torch
+    from sponge_b200 import (NonBond14, NonbondedEngine, Settle, VirtualAtoms,
+                             constrain_pairs_from_bonds, md_leap_frog, nb14_pair_tables)
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    spec = importlib.util.spec_from_file_location(
+        "make_covid", os.path.join(ROOT, "tests", "golden", "make_covid.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    s = mod.load_system()
+    n = len(s["charge"])
+    eng = NonbondedEngine(s)
+    eng.update_list(forced=1)
+    eng.to_uint()
+    dev = lambda x: torch.tensor(np.ascontiguousarray(x), device="cuda")  # noqa: E731
+    A, B = nb14_pair_tables(s["nb14_a"], s["nb14_b"], s["nb14_lj_scale"],
+                            np.float32(12.0) * s["lj_A"], np.float32(6.0) * s["lj_B"],
+                            s["lj_type"])
+    nb14 = NonBond14(n, s["nb14_a"], s["nb14_b"], A, B, s["nb14_cf"])
+    vs = VirtualAtoms(n, s["vs_type"], s["vs_atoms"], s["vs_param"])
+    pi, pj, pr = constrain_pairs_from_bonds(s["bond_a"], s["bond_b"], s["bond_r"], s["mass"])
+    dt = float(s["md_dt"])
+    st = Settle(n, pi, pj, pr, s["mass"], dt)
+    m64 = s["mass"].astype(np.float64)
+    inv = dev(np.divide(1.0, m64, out=np.zeros_like(m64), where=m64 != 0).astype(np.float32))
+    mass = dev(s["mass"])
+    frc = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    ae = torch.zeros(n, dtype=torch.float32, device="cuda")
+    av = torch.zeros(n, dtype=torch.float32, device="cuda")
+    vel = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    crd = eng.crd.clone()
+    acc = torch.zeros_like(vel)
+    press = torch.zeros(1, dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    calls = {
+        "nb14_force_energy_virial": lambda: nb14.Non_Bond_14_LJ_CF_Force_With_Atom_Energy_And_Virial(
+            eng.uint_crd, eng.charge, eng.scaler, frc, ae, av),
+        "vsite_coordinate_refresh": lambda: vs.Coordinate_Refresh(eng.uint_crd, eng.scaler, crd),
+        "vsite_force_redistribute": lambda: vs.Force_Redistribute(eng.uint_crd, eng.scaler, frc),
+        "settle_remember": lambda: st.Remember_Last_Coordinates(eng.uint_crd, eng.scaler),
+        "leap_frog": lambda: md_leap_frog(n, inv, frc, vel, crd, 0.0, acc=acc),
+        "settle_apply": lambda: st.Do_SETTLE(mass, crd, eng.box, vel, 1, press),
+    }
+    out = {}
+    for name, fn in calls.items():
+        for _ in range(max(3, args.warmup)):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            fn()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        out[name] = 1e3 * float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    line = {
+        "metric": MODULES_METRIC, "value": sum(out.values()), "unit": "us",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+        "scaling": "none", "vs_baseline": None,
+        "dtype": "f32 arithmetic, int64 fixed-point accumulation (1-4 pairs)",
+        "data": "SPONGE covid-tip4p inputs (tests/golden/covid_tip4p_inputs.npz)",
+        "config": {"workload": "covid-tip4p: %d atoms, %d 1-4 pairs, %d virtual atoms, %d rigid "
+                               "waters and %d rigid pairs (SETTLE), %d constraint pairs left"
+                               % (n, len(s["nb14_a"]), len(s["vs_type"]), st.triangle_numbers,
+                                  st.pair_numbers, st.remaining_pairs),
+                   "l2": "flushed (256 MiB write) before every timed call",
+                   "leap_frog": "dt 0 so the coordinates stay as read (same arithmetic)"},
+        "us_per_call": out,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -329,9 +415,11 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--pair-shape", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="pair-kernel shape (sb_lj_set_kernel_variant); 0 = pick by timing")
-    ap.add_argument("--workload", default="solvated96k", choices=["solvated96k", "fep48"],
+    ap.add_argument("--workload", default="solvated96k",
+                    choices=["solvated96k", "fep48", "modules"],
                     help="fep48: the 48 batched FEP/TI lambda windows (parity case, reported "
-                         "separately from the headline line)")
+                         "separately from the headline line); modules: the 1-4 pair, virtual "
+                         "atom and integrator/SETTLE calls on covid-tip4p (reported separately)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -339,6 +427,9 @@ def main():
         return
     if args.workload == "fep48":
         run_fep(args, rank, world, local)
+        return
+    if args.workload == "modules":
+        run_modules(args, rank, world, local)
         return
 
     import torch
