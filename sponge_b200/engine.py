@@ -128,6 +128,36 @@ class NonbondedEngine:
         self.update_list()
         self._graph.replay()
 
+    def md_step(self, settle, inverse_mass, mass, vel, acc=None):
+        """One NVE step as Main_Calculate_Force + Main_Iteration run it (SPONGE/main.cu:162-329,
+        :376), eagerly: fixed-point coordinates, forces (list as it stands), then the fused
+        leap-frog + SETTLE launch (``settle``: a Settle handle with no constraint pairs left)."""
+        crd_to_uint_crd(self.crd, self.box, out=self.uint_crd)
+        self.frc.zero_()
+        self.force()
+        settle.nve_step(self.uint_crd, self.scaler, inverse_mass, mass, self.frc, vel, self.crd,
+                        self.box, acc=acc)
+
+    def capture_md_graph(self, settle, inverse_mass, mass, vel, acc=None):
+        """Capture ``md_step`` once as a CUDA graph (the integrator and SETTLE behind the force
+        graph); ``md_step_graph`` replays it after the list update by its policy. The buffers
+        passed here are the ones every replay uses. Call ``md_step`` once eagerly first (lazy
+        per-list buffers)."""
+        torch = self.torch
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream()
+        with torch.cuda.graph(g, stream=side):
+            self.md_step(settle, inverse_mass, mass, vel, acc)
+        self._md_graph = g
+        return g
+
+    def md_step_graph(self):
+        """List update by its policy (eager, wraps the coordinates on rebuilds), then the captured
+        MD step."""
+        self.update_list()
+        self._md_graph.replay()
+
     def potential(self):
         """Total potential as MD_core sums it: sum(atom_energy) + d_potential (FP64 sum)."""
         return float(self.atom_energy.double().sum().item() + self.d_potential.double().item())

@@ -181,3 +181,43 @@ def test_covid_module_calls(covid, oracle_lib):
         assert float(p[0]) == pytest.approx(float(golden["summary_settle_pressure"]), rel=1e-4)
     with pytest.raises(SpongeError):
         case.fused(st)
+
+
+def test_md_step_graph_matches_eager(torch, oracle_lib):
+    """The NVE step (force, then the fused leap-frog + SETTLE launch) captured in one CUDA graph
+    behind the force part gives the eager step's bits, through list rebuilds (every 3 steps) and
+    the pruned list's renewals; the rigid waters keep their geometry."""
+    from sponge_b200 import NonbondedEngine, Settle, constrain_pairs_from_bonds, sponge_io
+    from sponge_b200 import systems as sysmod
+    s = sysmod.config0()
+    a, b, r, mass = sponge_io.bonds_and_masses(s)
+    pi, pj, pr = constrain_pairs_from_bonds(a, b, r, mass)
+    n = len(mass)
+    dt = float(np.float32(np.float32(0.0005) * np.float32(20.455)))
+    m64 = mass.astype(np.float64)
+    inv = torch.tensor(np.divide(1.0, m64, out=np.zeros_like(m64), where=m64 != 0)
+                       .astype(np.float32), device="cuda")
+    m_t = torch.tensor(mass, device="cuda")
+    engines, vels, settles = [], [], []
+    for _ in range(2):
+        eng = NonbondedEngine(s, refresh_interval=3)
+        eng.update_list(forced=1)
+        vel = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        st = Settle(n, pi, pj, pr, mass, dt)
+        eng.md_step(st, inv, m_t, vel)
+        engines.append(eng)
+        vels.append(vel)
+        settles.append(st)
+    eager, graphed = engines
+    graphed.capture_md_graph(settles[1], inv, m_t, vels[1])
+    for _ in range(7):
+        eager.update_list()
+        eager.md_step(settles[0], inv, m_t, vels[0])
+        graphed.md_step_graph()
+    torch.cuda.synchronize()
+    assert np.array_equal(eager.crd.cpu().numpy(), graphed.crd.cpu().numpy())
+    assert np.array_equal(vels[0].cpu().numpy(), vels[1].cpu().numpy())
+    c = graphed.crd.cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(c))
+    d = H.distances(c, s["box"], pi, pj)
+    assert np.abs(d - pr).max() < 5e-5
