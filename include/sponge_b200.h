@@ -205,9 +205,9 @@ SB_API int sb_pme_atom_energy_arrays(sb_pme* pme, float** d_direct_atom_energy,
 /* FFT kernel family of the fixed-point form (no reference counterpart; a tuning knob):
  * SB_FFT_AUTO (the default) runs the register line transforms on every axis whose size has one
  * (N = N1 * N2 with small 2/3/5-smooth factors) and the generic mixed-radix stage kernels on the
- * others, and, for square x-y planes (32, 48, 64, 80, 96, 128) with register transforms on every
- * axis, fuses the y and x passes of each kz plane into one block (same transforms, same bits as
- * SB_FFT_LINES); SB_FFT_LINES runs the register line transforms pass by pass; SB_FFT_GENERIC runs
+ * others, and, for square x-y planes (30, 32, 36, 40, 48, 50, 54, 60, 64, 80, 96, 128) with
+ * register transforms on every axis, fuses the y and x passes of each kz plane into one block
+ * (same transforms, same bits as SB_FFT_LINES); SB_FFT_LINES runs the register line transforms pass by pass; SB_FFT_GENERIC runs
  * only the stage kernels. The choice is a fixed rule, not a timing, so the same grid gives the
  * same bits in every process. Synchronises the device and clears the spectrum buffer; call it
  * outside stream capture. The register and generic families agree to FP32 rounding. */

@@ -508,9 +508,12 @@ __global__ void __launch_bounds__(NL * F4<N1, N2>::T) k_plane4(
     }
 }
 
-// square plane sizes fused by k_plane4: X(K, N1, N2, NL)
-#define SB_FFT4_PLANE_SIZES(X) \
-    X(32, 4, 8, 32) X(48, 6, 8, 16) X(64, 8, 8, 64) X(80, 8, 10, 16) X(96, 8, 12, 48) X(128, 8, 16, 64)
+// square plane sizes fused by k_plane4: X(K, N1, N2, NL) (the even 2-3-5-smooth sizes of about
+// 1 A grids on 30-64 A boxes, and 80, 96, 128)
+#define SB_FFT4_PLANE_SIZES(X)                                                                   \
+    X(30, 5, 6, 30) X(32, 4, 8, 32) X(36, 6, 6, 36) X(40, 5, 8, 40) X(48, 6, 8, 16)             \
+    X(50, 5, 10, 50) X(54, 6, 9, 54) X(60, 6, 10, 60) X(64, 8, 8, 64) X(80, 8, 10, 16)          \
+    X(96, 8, 12, 48) X(128, 8, 16, 64)
 
 // sizes with a register line transform: X(N, N1, N2). The z passes (half length M = K2 / 2)
 // take the sizes whose 32-row tile fits the static shared-memory limit.

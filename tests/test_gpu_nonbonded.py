@@ -365,9 +365,9 @@ def test_config1_full_size(torch_cuda, oracle_lib):
     assert err < FORCE_TOL
 
 
-@pytest.mark.parametrize("K", [48, 64, 80, 96, 128])
+@pytest.mark.parametrize("K", [30, 36, 40, 48, 50, 54, 60, 64, 80, 96, 128])
 def test_plane_fft_sizes(K, torch_cuda, oracle_lib):
-    """Every square plane size the fused y-x kernel serves (lines per round 16, 64, 16, 48, 64):
+    """Every square plane size the fused y-x kernel serves besides 32 (config0's own grid):
     the same bits as the pass-by-pass register transforms, and the FP64 reciprocal force."""
     import sponge_b200
     from sponge_b200 import NonbondedEngine
