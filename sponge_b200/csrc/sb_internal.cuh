@@ -249,15 +249,12 @@ int sb_lj_fused_direct(sb_lennard_jones* lj, sb_neighbor_list* nl, const uint32_
 int sb_lj_fused_pair(sb_lennard_jones* lj, sb_neighbor_list* nl, float pme_beta,
                      int need_atom_energy, float* d_atom_energy, int need_virial,
                      float* d_atom_lj_virial, float* d_atom_direct_pme_energy, cudaStream_t s);
-// reciprocal part in two pieces: the grid chain (spread of the packed slots, FFT, convolution,
-// inverse FFT into d_theta, gather of the slot forces into the list's fixed-point buffer) and
-// the finish (finalisation of that buffer into d_frc, energy and virial sums), which must follow
-// the pair and exclusion kernels
-// spread, FFT, convolution and gather of the packed slots into the slot accumulators
-int sb_pme_fused_grid(sb_pme* pme, sb_neighbor_list* nl, int want_energy, cudaStream_t s);
-// the same from the atom-order fixed-point coordinates and charges (no packing needed), the gather
-// also doing the exclusion correction when the CSR is given (d_excl_energy: per-atom correction
-// energy, zeroed first by sb_pme_zero_atom_energy, or null)
+// reciprocal part in two pieces: the grid chain (spread from the atom-order fixed-point
+// coordinates and charges, FFT, convolution, inverse FFT into d_theta, gather of the forces into
+// the list's slot-order fixed-point buffer, with the exclusion correction when the CSR is given;
+// d_excl_energy: per-atom correction energy, zeroed first by sb_pme_zero_atom_energy, or null)
+// and the finish (finalisation of that buffer into d_frc, energy and virial sums), which must
+// follow the pair kernel
 int sb_pme_fused_grid_atoms(sb_pme* pme, sb_neighbor_list* nl, int want_energy, cudaStream_t s,
                             const uint32_t* d_uint_crd, const float* d_charge, const int* es,
                             const int* el, const int* en, float* d_excl_energy);
@@ -265,12 +262,11 @@ int sb_pme_zero_atom_energy(sb_pme* pme, float* d_atom_energy, cudaStream_t s);
 int sb_pme_fused_finish(sb_pme* pme, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
                         int need_virial, int need_energy, float* d_virial, float* d_potential,
                         cudaStream_t s);
-int sb_pme_fused_excluded(sb_pme* pme, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
-                          const float* d_charge, const int* es, const int* el, const int* en,
-                          float* d_atom_energy, cudaStream_t s);
-int sb_pme_fused_reciprocal(sb_pme* pme, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
-                            int need_virial, int need_energy, float* d_virial, float* d_potential,
-                            cudaStream_t s);
+// grid chain and finish in one call (the exclusion correction included when the CSR is given)
+int sb_pme_fused_reciprocal(sb_pme* pme, sb_neighbor_list* nl, float* d_frc,
+                            const uint32_t* d_uint_crd, const float* d_charge, const int* es,
+                            const int* el, const int* en, int need_virial, int need_energy,
+                            float* d_virial, float* d_potential, cudaStream_t s);
 
 // FEP step: PME cross terms of dU/dlambda after sb_pme_fused_reciprocal (acc[0] reciprocal,
 // acc[1] exclusion correction, 2^32 fixed point)

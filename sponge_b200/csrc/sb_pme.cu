@@ -751,98 +751,12 @@ extern "C" int sb_pme_get_energy(sb_pme* p, sb_neighbor_list* nl, const uint32_t
 }
 
 // ---------------------------------------------------------------------------------------------
-// fused fixed-form step: slot-order kernels sharing the neighbor list's packed data and its
-// fixed-point force buffer (x, y, z planes of slot_cap int64 each)
+// fused fixed-form step: reciprocal kernels adding into the neighbor list's fixed-point force
+// buffer (x, y, z planes of slot_cap int64 each)
 // ---------------------------------------------------------------------------------------------
 
-// exclusion correction as k_excluded<true>, accumulating at the atoms' slots
-__global__ void k_excluded_slot(int n, const uint32_t* __restrict__ uc, float sx, float sy,
-                                float sz, const float* __restrict__ q, float beta2, float beta3,
-                                float beta, const int* __restrict__ es,
-                                const int* __restrict__ el, const int* __restrict__ en,
-                                const int* __restrict__ atom_slot, int slot_cap,
-                                long long* __restrict__ fix, float* __restrict__ ene) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int cnt = en[i];
-    if (cnt <= 0) return;
-    const int s0 = es[i];
-    const uint32_t ux = uc[3 * i], uy = uc[3 * i + 1], uz = uc[3 * i + 2];
-    const float qi = q[i];
-    float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f;
-    for (int k = s0; k < s0 + cnt; k++) {
-        const int j = el[k];
-        const float dx = __int2float_rn((int)(uc[3 * j] - ux)) * sx;
-        const float dy = __int2float_rn((int)(uc[3 * j + 1] - uy)) * sy;
-        const float dz = __int2float_rn((int)(uc[3 * j + 2] - uz)) * sz;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float qq = qi * q[j];
-        const float fs = qq * beta3 * sb_ewald_G(beta2 * r2);
-        const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
-        fx += tx;
-        fy += ty;
-        fz += tz;
-        if (ene) {
-            const float r = sqrtf(r2);
-            e -= qq * erff(beta * r) / r;
-        }
-        const int sj = atom_slot[j];
-        atomicAdd((unsigned long long*)&fix[sj], (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
-        atomicAdd((unsigned long long*)&fix[slot_cap + sj], (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
-        atomicAdd((unsigned long long*)&fix[2 * slot_cap + sj], (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
-    }
-    const int si = atom_slot[i];
-    atomicAdd((unsigned long long*)&fix[si], (unsigned long long)__float2ll_rn(fx * SB_FORCE_SCALE));
-    atomicAdd((unsigned long long*)&fix[slot_cap + si], (unsigned long long)__float2ll_rn(fy * SB_FORCE_SCALE));
-    atomicAdd((unsigned long long*)&fix[2 * slot_cap + si], (unsigned long long)__float2ll_rn(fz * SB_FORCE_SCALE));
-    if (ene) atomicAdd(&ene[i], e);
-}
-
-// charge spread from the packed slot data {ux, uy, uz, q}; 4 threads per slot, one per z offset,
-// so that the four lanes of a slot hit four adjacent grid words of one z row (one 32-byte
-// sector) at every (x, y) offset instead of four different x planes. The value added at each
-// point is the same product, in the same order, as the atom-order spread computes.
-__global__ void k_spread_slot(const int* __restrict__ meta, const uint4* __restrict__ xq, int K0,
-                              int K1, int K2, long long* __restrict__ gfix) {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int sl = gt >> 2, kz = gt & 3;
-    if (sl >= meta[3]) return;
-    const uint4 v = xq[sl];
-    const float q = __uint_as_float(v.w);
-    if (q == 0.f) return;  // padding slots and uncharged atoms add nothing
-    int b0, b1, b2;
-    float f0, f1, f2;
-    grid_coord(v.x, K0, b0, f0);
-    grid_coord(v.y, K1, b1, f1);
-    grid_coord(v.z, K2, b2, f2);
-    float wx[4], wy[4], wz[4];
-    bspline4(f0, wx);
-    bspline4(f1, wy);
-    bspline4(f2, wz);
-    int gz = b2 - kz;
-    if (gz < 0) gz += K2;
-    const float wzk = kz == 0 ? wz[0] : kz == 1 ? wz[1] : kz == 2 ? wz[2] : wz[3];
-#pragma unroll
-    for (int kx = 0; kx < 4; kx++) {
-        int gx = b0 - kx;
-        if (gx < 0) gx += K0;
-        const float qw = q * wx[kx];
-#pragma unroll
-        for (int ky = 0; ky < 4; ky++) {
-            int gy = b1 - ky;
-            if (gy < 0) gy += K1;
-            const long long f = __float2ll_rn(qw * wy[ky] * wzk * SB_GRID_SCALE);
-            if (f)
-                atomicAdd((unsigned long long*)&gfix[((size_t)gx * K1 + gy) * K2 + gz],
-                          (unsigned long long)f);
-        }
-    }
-}
-
-// reciprocal force gather per slot into the list's slot-order fixed-point accumulators (the
-// buffer the pair and exclusion kernels add to, possibly at the same time: integer adds commute)
-// Ewald exclusion correction of one atom inside a reciprocal gather (k_gather_atom):
-// k_excluded_slot's arithmetic, its terms added to the slot accumulators as the same int64 values
+// Ewald exclusion correction of one atom inside a reciprocal gather (k_gather_atom): the
+// arithmetic of k_excluded<true>, its int64 terms added to the atoms' slot accumulators
 struct SbExclPass {
     const int* slot_atom;
     const int* atom_slot;
@@ -853,82 +767,6 @@ struct SbExclPass {
     float* ene;  // per-atom correction energy (energy steps) or null
 };
 
-__global__ void k_gather_slot(const int* __restrict__ meta, const uint4* __restrict__ xq,
-                              const float* __restrict__ theta, int K0, int K1, int K2, float ix,
-                              float iy, float iz, long long* __restrict__ fix, int slot_cap) {
-    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sl >= meta[3]) return;
-    const uint4 v = xq[sl];
-    const float q = __uint_as_float(v.w);  // padding slots carry charge 0
-    if (q == 0.f) return;
-    int b0, b1, b2;
-    float f0, f1, f2;
-    grid_coord(v.x, K0, b0, f0);
-    grid_coord(v.y, K1, b1, f1);
-    grid_coord(v.z, K2, b2, f2);
-    float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
-    bspline4(f0, wx);
-    bspline4(f1, wy);
-    bspline4(f2, wz);
-    bspline4d(f0, dx);
-    bspline4d(f1, dy);
-    bspline4d(f2, dz);
-    int gz[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int g = b2 - k;
-        gz[k] = g < 0 ? g + K2 : g;
-    }
-    float Fx = 0.f, Fy = 0.f, Fz = 0.f;
-#pragma unroll
-    for (int kx = 0; kx < 4; kx++) {
-        int gx = b0 - kx;
-        if (gx < 0) gx += K0;
-#pragma unroll
-        for (int ky = 0; ky < 4; ky++) {
-            int gy = b1 - ky;
-            if (gy < 0) gy += K1;
-            const float* row = theta + ((size_t)gx * K1 + gy) * K2;
-            float sw = 0.f, sd = 0.f;
-#pragma unroll
-            for (int kz = 0; kz < 4; kz++) {
-                const float t = row[gz[kz]];
-                sw = fmaf(t, wz[kz], sw);
-                sd = fmaf(t, dz[kz], sd);
-            }
-            Fx = fmaf(dx[kx] * wy[ky], sw, Fx);
-            Fy = fmaf(wx[kx] * dy[ky], sw, Fy);
-            Fz = fmaf(wx[kx] * wy[ky], sd, Fz);
-        }
-    }
-    const float sq = -q;
-    const long long fx = __float2ll_rn(sq * Fx * ix * SB_FORCE_SCALE);
-    const long long fy = __float2ll_rn(sq * Fy * iy * SB_FORCE_SCALE);
-    const long long fz = __float2ll_rn(sq * Fz * iz * SB_FORCE_SCALE);
-    atomicAdd((unsigned long long*)&fix[sl], (unsigned long long)fx);
-    atomicAdd((unsigned long long*)&fix[slot_cap + sl], (unsigned long long)fy);
-    atomicAdd((unsigned long long*)&fix[2 * slot_cap + sl], (unsigned long long)fz);
-}
-
-int sb_pme_fused_excluded(sb_pme* p, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
-                          const float* d_charge, const int* es, const int* el, const int* en,
-                          float* d_atom_energy, cudaStream_t s) {
-    const int n = p->n;
-    if (d_atom_energy) {
-        k_zero_f<<<(n + 1023) / 1024, 1024, 0, s>>>(n, d_atom_energy);
-        SB_CHECK_LAUNCH();
-    }
-    if (!es || !el || !en) return SB_OK;
-    const float b = p->beta;
-    const float sx = (1.0f / 4294967296.0f) * p->box[0], sy = (1.0f / 4294967296.0f) * p->box[1],
-                sz = (1.0f / 4294967296.0f) * p->box[2];
-    k_excluded_slot<<<(n + 127) / 128, 128, 0, s>>>(n, d_uint_crd, sx, sy, sz, d_charge, b * b,
-                                                    b * b * b, b, es, el, en, nl->atom_slot,
-                                                    nl->slot_cap, nl->fix, d_atom_energy);
-    SB_CHECK_LAUNCH();
-    return SB_OK;
-}
-
 int sb_pme_zero_atom_energy(sb_pme* p, float* d_atom_energy, cudaStream_t s) {
     if (d_atom_energy) {
         k_zero_f<<<(p->n + 1023) / 1024, 1024, 0, s>>>(p->n, d_atom_energy);
@@ -937,25 +775,9 @@ int sb_pme_zero_atom_energy(sb_pme* p, float* d_atom_energy, cudaStream_t s) {
     return SB_OK;
 }
 
-int sb_pme_fused_grid(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s) {
-    const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2];
-    k_spread_slot<<<(4 * nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->meta, nl->xq, K0, K1, K2,
-                                                                 p->d_qfix);
-    SB_CHECK_LAUNCH();
-    SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
-    SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_energy, s,
-                             &p->rec_nparts));
-    SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
-    k_gather_slot<<<(nl->slot_cap + 127) / 128, 128, 0, s>>>(
-        nl->meta, nl->xq, p->d_theta, K0, K1, K2, (float)K0 / p->box[0], (float)K1 / p->box[1],
-        (float)K2 / p->box[2], nl->fix, nl->slot_cap);
-    SB_CHECK_LAUNCH();
-    return SB_OK;
-}
-
 // reciprocal gather of atom i (atom order, from the fixed-point coordinates and charges) into its
-// slot's fixed-point accumulator, followed by the atom's exclusion correction: the same int64
-// terms as k_gather_slot + k_excluded_slot, from data that needs no packing
+// slot's fixed-point accumulator, followed by the atom's exclusion correction; reads nothing the
+// pair kernel's packing produces, so it can run beside it
 __global__ void k_gather_atom(int n, const uint32_t* __restrict__ uc, const float* __restrict__ qa,
                               const float* __restrict__ theta, int K0, int K1, int K2, float ix,
                               float iy, float iz, long long* __restrict__ fix, int slot_cap,
@@ -1087,10 +909,12 @@ int sb_pme_fused_finish(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const flo
     return SB_OK;
 }
 
-int sb_pme_fused_reciprocal(sb_pme* p, sb_neighbor_list* nl, float* d_frc, const float* d_charge,
-                            int need_virial, int need_energy, float* d_virial, float* d_potential,
-                            cudaStream_t s) {
-    SB_TRY(sb_pme_fused_grid(p, nl, need_virial > 0 || need_energy > 0, s));
+int sb_pme_fused_reciprocal(sb_pme* p, sb_neighbor_list* nl, float* d_frc,
+                            const uint32_t* d_uint_crd, const float* d_charge, const int* es,
+                            const int* el, const int* en, int need_virial, int need_energy,
+                            float* d_virial, float* d_potential, cudaStream_t s) {
+    SB_TRY(sb_pme_fused_grid_atoms(p, nl, need_virial > 0 || need_energy > 0, s, d_uint_crd,
+                                   d_charge, es, el, en, nullptr));
     return sb_pme_fused_finish(p, nl, d_frc, d_charge, need_virial, need_energy, d_virial,
                                d_potential, s);
 }

@@ -815,8 +815,8 @@ extern "C" int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
     }
     SB_TRY(sc_launch_fixed(sc, nl, d_uint_crd, d_charge, pme->beta, 0, dh, nullptr, nullptr,
                            nullptr, s));
-    SB_TRY(sb_pme_fused_excluded(pme, nl, d_uint_crd, d_charge, es, el, en, nullptr, s));
-    SB_TRY(sb_pme_fused_reciprocal(pme, nl, d_frc, d_charge, 0, 0, nullptr, nullptr, s));
+    SB_TRY(sb_pme_fused_reciprocal(pme, nl, d_frc, d_uint_crd, d_charge, es, el, en, 0, 0,
+                                   nullptr, nullptr, s));
     if (dh) {
         SB_TRY(sb_pme_ti_terms_slot(pme, nl, sc->d_slot_dq, d_uint_crd, d_charge, sc->d_dq, es,
                                     el, en, sc->d_hfix + 2, s));
