@@ -227,6 +227,7 @@ struct sb_pme {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int overlap = 1;
+    int num_sms = 148;             // SMs of the device (grids of the side-stream kernels)
     int rec_nparts = 0;             // energy partials written by the last grid chain
 };
 

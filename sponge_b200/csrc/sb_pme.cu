@@ -23,6 +23,7 @@
 #include "sb_ewald.cuh"
 #include "sb_internal.cuh"
 
+
 __device__ __forceinline__ void grid_coord(uint32_t u, int K, int& base, float& fr) {
     const unsigned long long p = (unsigned long long)u * (unsigned)K;
     base = (int)(p >> 32);
@@ -45,16 +46,16 @@ __device__ __forceinline__ void bspline4d(float f, float d[4]) {
     d[3] = -0.5f * f2 + f - 0.5f;
 }
 
-// 4 threads per atom; thread t handles x-offset t and the 16 (y, z) points
 // 4 threads per atom, one per z offset: the four lanes of an atom update adjacent words of one
-// z row at each (x, y) offset
+// z row at each (x, y) offset. Grid-stride, so that the fused step can run it on a small grid
+// beside the pair kernel.
 template <bool FIXED>
 __global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __restrict__ q,
                          int K0, int K1, int K2, long long* __restrict__ gfix,
                          float* __restrict__ gf) {
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int gt = blockIdx.x * blockDim.x + threadIdx.x; gt < 4 * n;
+         gt += gridDim.x * blockDim.x) {
     const int i = gt >> 2, kz = gt & 3;
-    if (i >= n) return;
     int b0, b1, b2;
     float f0, f1, f2;
     grid_coord(uc[3 * i], K0, b0, f0);
@@ -86,6 +87,7 @@ __global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __
                 atomicAdd(&gf[at], v);
             }
         }
+    }
     }
 }
 
@@ -393,6 +395,13 @@ extern "C" int sb_pme_create(int atom_numbers, const float box_length[3], float 
     }
     sb_pme* p = new sb_pme();
     p->n = atom_numbers;
+    {
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            sms > 0)
+            p->num_sms = sms;
+    }
     p->form = form;
     for (int d = 0; d < 3; d++) p->box[d] = box_length[d];
     p->cutoff = cutoff;
@@ -778,12 +787,12 @@ int sb_pme_zero_atom_energy(sb_pme* p, float* d_atom_energy, cudaStream_t s) {
 // reciprocal gather of atom i (atom order, from the fixed-point coordinates and charges) into its
 // slot's fixed-point accumulator, followed by the atom's exclusion correction; reads nothing the
 // pair kernel's packing produces, so it can run beside it
-__global__ void k_gather_atom(int n, const uint32_t* __restrict__ uc, const float* __restrict__ qa,
-                              const float* __restrict__ theta, int K0, int K1, int K2, float ix,
-                              float iy, float iz, long long* __restrict__ fix, int slot_cap,
-                              SbExclPass X) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ __forceinline__ void gather_atom_one(int i, const uint32_t* __restrict__ uc,
+                                                const float* __restrict__ qa,
+                                                const float* __restrict__ theta, int K0, int K1,
+                                                int K2, float ix, float iy, float iz,
+                                                long long* __restrict__ fix, int slot_cap,
+                                                const SbExclPass& X) {
     const float q = qa[i];
     if (q == 0.f) return;  // an uncharged atom has zero reciprocal force and exclusion terms
     const uint32_t ux = uc[3 * i], uy = uc[3 * i + 1], uz = uc[3 * i + 2];
@@ -870,12 +879,24 @@ __global__ void k_gather_atom(int n, const uint32_t* __restrict__ uc, const floa
     atomicAdd((unsigned long long*)&fix[2 * slot_cap + sl], (unsigned long long)fz);
 }
 
+// thread per atom (grid-stride; a grid of fewer blocks, as for the spread, was slower here: the
+// gather ends the side chain)
+__global__ void k_gather_atom(int n, const uint32_t* __restrict__ uc, const float* __restrict__ qa,
+                              const float* __restrict__ theta, int K0, int K1, int K2, float ix,
+                              float iy, float iz, long long* __restrict__ fix, int slot_cap,
+                              SbExclPass X) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        gather_atom_one(i, uc, qa, theta, K0, K1, K2, ix, iy, iz, fix, slot_cap, X);
+}
+
 int sb_pme_fused_grid_atoms(sb_pme* p, sb_neighbor_list* nl, int want_energy, cudaStream_t s,
                             const uint32_t* d_uint_crd, const float* d_charge, const int* es,
                             const int* el, const int* en, float* d_excl_energy) {
     const int K0 = p->K[0], K1 = p->K[1], K2 = p->K[2], n = p->n;
-    k_spread<true><<<(4 * n + 255) / 256, 256, 0, s>>>(n, d_uint_crd, d_charge, K0, K1, K2,
-                                                       p->d_qfix, nullptr);
+    // a small grid (4 blocks per SM) looping over the atoms: the spread then holds few SM
+    // resources beside the pair kernel (137.4 -> 134.1 us per step on the 96k-atom box)
+    k_spread<true><<<std::min((4 * n + 255) / 256, 4 * p->num_sms), 256, 0, s>>>(
+        n, d_uint_crd, d_charge, K0, K1, K2, p->d_qfix, nullptr);
     SB_CHECK_LAUNCH();
     SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
     SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, want_energy, s,
