@@ -1,18 +1,22 @@
 #!/usr/bin/env python
 """Benchmark: ns/day of the nonbonded hot path on the 96,000-atom solvated PME box.
 
-One step = what one MD step of SPONGE spends in the path (SPONGE/main.cu:162-210, :376): the
-neighbor-list update by its policy (rebuild every 20 steps), LJ + PME direct, the long-range
-correction, the exclusion correction and PME reciprocal space, for 96,000 atoms (31,000 rigid
-waters + 3,000 solute atoms, 98.6 A box, rc 10 A, skin 2 A, PME 96^3). ns/day = steps/s * 2 fs *
-86400 / 1e6. The integrator and constraints are not part of the path and are not timed.
+One step = one NVE MD step as SPONGE's driver runs it (SPONGE/main.cu:162-210, :283-329, :376)
+with the nonbonded path on the GPU: the neighbor-list update by its policy (rebuild every 20
+steps), fixed-point coordinates, LJ + PME direct, the long-range correction, the exclusion
+correction, PME reciprocal space, then the leap-frog and SETTLE of the rigid waters, for 96,000
+atoms (31,000 rigid waters + 3,000 solute atoms, 98.6 A box, rc 10 A, skin 2 A, PME 96^3) on
+moving coordinates (Maxwell-Boltzmann velocities at 300 K after a steepest-descent relaxation
+of the free solute atoms). ns/day = steps/s * 2 fs * 86400 / 1e6.
 
-  value   device time per step (CUDA events on the launching stream), inputs resident in HBM,
+  value   device time per MD step (CUDA events on the launching stream), state resident in HBM,
           L2 flushed (256 MiB write) before every timed step
-  e2e     the same through the public C-ABI call with HOST buffers: pinned coordinates copied
-          in, fixed-point conversion, step, forces copied out, every step
+  e2e     the same MD steps with the state owned by the host: every step the coordinates are
+          copied in from pinned host memory and the new coordinates copied back
+  force_only  the list update + force graph on frozen coordinates (no integrator)
   --impl reference  the CPU baseline: the FP64 multithreaded restatement of the same path
           (SPONGE has no CPU implementation) on the host cores, one full evaluation per step
+  --workload water1m  the 1,000,512-atom water box with PME 216^3, both forms
 
 Multi-GPU: independent replicas (one system per rank, no collective in the data path).
 """
@@ -35,8 +39,7 @@ DT_FS = 2.0
 FLOP_PER_PAIR = 50.0       # in-cutoff pair: dr 3, r^2 5, rsqrt 1, powers 4, LJ 3, Ewald 26, scale 3, accumulate 6
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal at max SM clock
 # DRAM bytes read + written by one launch of the pair kernel walking the pruned list on this
-# workload, from an ncu capture (profiles/k_pair_x2_solvated96k.md): the list plus the packed
-# coordinates
+# workload, from an ncu capture of that kernel: the list plus the packed coordinates
 PAIR_DRAM_BYTES = 25.01e6
 # pair-kernel shape (sb_lj_set_kernel_variant) -> kernel name
 PAIR_KERNEL = {2: "k_pair_x2", 8: "k_pair_fixed<8>", 4: "k_pair_fixed<4>", 1: "k_pair_compact"}
@@ -168,9 +171,22 @@ METRIC = "ns/day, 96k-atom PME water, 1 B200 (nonbonded path, fixed-point form)"
 def workload_config():
     return {"workload": "solvated96k_pme96: 31,000 rigid waters + 3,000 solute atoms (20 LJ "
                         "types), 98.6 A cube, rc 10 A, skin 2 A, PME 96^3, list rebuilt every "
-                        "20 steps, dt 2 fs; pair kernel on the list pruned to rc + 0.5 A (renewed "
-                        "after each rebuild, on any 0.25 A move and every 5 steps)",
+                        "20 steps, dt 2 fs, NVE leap-frog + SETTLE on moving coordinates; pair "
+                        "kernel on the list pruned to rc + 0.5 A (renewed after each rebuild, on "
+                        "any 0.25 A move and every 5 steps)",
             "atoms": 96000, "l2": "flushed (256 MiB write) before every timed step",
+            "parallelism": "replicas"}
+
+
+WATER1M_METRIC = "ns/day, 1,000,512-atom PME water (216^3), 1 B200: chosen vs plain form"
+
+
+def water1m_config():
+    return {"workload": "water1m_pme216: 333,504 rigid waters (70^3 lattice minus 9,496 sites), "
+                        "215.3 A cube, rc 10 A, skin 2 A, PME 216^3, list rebuilt every 20 "
+                        "steps, dt 2 fs, NVE leap-frog + SETTLE; pair kernel on the list pruned "
+                        "to rc + 0.5 A",
+            "atoms": 1000512, "l2": "flushed (256 MiB write) before every timed step",
             "parallelism": "replicas"}
 
 
@@ -286,38 +302,6 @@ def hbm_view(traffic_bytes, ms):
             "peak_source": src}
 
 
-def time_integrator(eng, s, flush, stream, reps=20):
-    """Device time of the fused NVE leap-frog + SETTLE launch (sb_md_nve_settle_step) on the
-    bench box (waters rigid by SETTLE, solute atoms free), with zero forces and velocities so the
-    geometry stays as built while the arithmetic is the same."""
-    import torch
-    from sponge_b200 import TIME_CONVERSION, Settle, constrain_pairs_from_bonds, sponge_io
-    ba, bb, br, mass = sponge_io.bonds_and_masses(s)
-    pi, pj, pr = constrain_pairs_from_bonds(ba, bb, br, mass)
-    dt = float(np.float32(np.float32(DT_FS * 1e-3) * np.float32(TIME_CONVERSION)))
-    st = Settle(eng.n, pi, pj, pr, mass, dt)
-    m64 = mass.astype(np.float64)
-    inv = torch.tensor(np.divide(1.0, m64, out=np.zeros_like(m64), where=m64 != 0)
-                       .astype(np.float32), device="cuda")
-    m_t = torch.tensor(mass, device="cuda")
-    frc = torch.zeros_like(eng.frc)
-    vel = torch.zeros_like(eng.crd)
-    crd = eng.crd.clone()
-    acc = torch.zeros_like(eng.crd)
-    for _ in range(3):
-        st.nve_step(eng.uint_crd, eng.scaler, inv, m_t, frc, vel, crd, eng.box, acc=acc)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(reps)]
-    for k in range(reps):
-        flush.fill_(float(k))
-        ev[k][0].record(stream)
-        st.nve_step(eng.uint_crd, eng.scaler, inv, m_t, frc, vel, crd, eng.box, acc=acc)
-        ev[k][1].record(stream)
-    torch.cuda.synchronize()
-    st.Clear()
-    return float(np.mean([a.elapsed_time(b) for a, b in ev]))
-
-
 MODULES_METRIC = "us per call, SPONGE's covid-tip4p modules beside the nonbonded path, 1 B200"
 
 
@@ -404,6 +388,95 @@ def run_modules(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def setup_md(eng, s, seed, relax_iters=300, temperature=300.0):
+    """Untimed MD set-up on the device. The seeded generators place the free (unconstrained)
+    solute atoms by random sequential addition at >= 2.2 A, which leaves LJ overlaps of several
+    thousand kcal/mol/A: those atoms are first relaxed by steepest descent (every free atom moves
+    along its force by at most 0.02 A per iteration, the waters stay as built), then velocities
+    are drawn from the Maxwell-Boltzmann distribution at ``temperature`` (seeded), with the
+    centre-of-mass momentum removed. Returns the buffers of the NVE leap-frog + SETTLE step."""
+    import torch
+    from sponge_b200 import TIME_CONVERSION, Settle, constrain_pairs_from_bonds, sponge_io
+    ba, bb, br, mass = sponge_io.bonds_and_masses(s)
+    pi, pj, pr = constrain_pairs_from_bonds(ba, bb, br, mass)
+    n = eng.n
+    constrained = np.zeros(n, bool)
+    constrained[np.asarray(pi, np.int64)] = True
+    constrained[np.asarray(pj, np.int64)] = True
+    free = torch.tensor(np.nonzero(~constrained)[0], device="cuda")
+    if free.numel():
+        for it in range(relax_iters):
+            eng.update_list(forced=1 if it % 20 == 0 else 0)
+            eng.to_uint()
+            eng.frc.zero_()
+            eng.force()
+            f = eng.frc[free]
+            fn = f.norm(dim=1, keepdim=True)
+            step = 0.02 * f / torch.clamp(fn, min=50.0)
+            eng.crd[free] += step
+    dt = float(np.float32(np.float32(DT_FS * 1e-3) * np.float32(TIME_CONVERSION)))
+    settle = Settle(n, pi, pj, pr, mass, dt)
+    m64 = mass.astype(np.float64)
+    inv = np.divide(1.0, m64, out=np.zeros_like(m64), where=m64 != 0)
+    rng = np.random.default_rng(seed)
+    kT = 0.0019872041 * temperature  # kcal/mol
+    vel = rng.normal(size=(n, 3)) * np.sqrt(kT * inv)[:, None]
+    vel -= (m64[:, None] * vel).sum(0) / m64.sum()
+    inv_t = torch.tensor(inv.astype(np.float32), device="cuda")
+    mass_t = torch.tensor(mass.astype(np.float32), device="cuda")
+    vel_t = torch.tensor(vel.astype(np.float32), device="cuda")
+    acc_t = torch.zeros_like(vel_t)
+    eng.update_list(forced=1)
+    return settle, inv_t, mass_t, vel_t, acc_t
+
+
+def timed_steps(fn, steps, flush, stream, dist=None):
+    """Per-step device time (CUDA events on the launching stream), L2 flushed (256 MiB write)
+    before every step outside the events; a barrier and a synchronize on both sides."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        fn()
+        ev[k][1].record(stream)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def kernel_times(eng, flush, stream, reps=10):
+    """Device time of the parts of one force step, each called alone through its module entry
+    point (CUDA events, L2 flushed before each call): the pair kernel with its pack and finalize
+    (LJ + Ewald direct), the reciprocal chain (spread, FFTs with the convolution, gather) and a
+    list rebuild (the whole sequence: fixed point, column sort, search)."""
+    import torch
+    out = {}
+    parts = {"pair": lambda: eng.forces(parts=("direct",)),
+             "reciprocal": lambda: eng.forces(parts=("reciprocal",)),
+             "rebuild": lambda: eng.update_list(forced=1)}
+    for name, fn in parts.items():
+        fn()
+        torch.cuda.synchronize()
+        out[name] = float(np.mean(timed_steps(fn, reps, flush, stream)))
+    eng.frc.zero_()
+    return out
+
+
+def pme_bytes(n_atoms, fft):
+    """Algorithmic HBM bytes of one reciprocal evaluation: per atom 16 B read (coordinates,
+    charge), 12 B force written, 16 B read again by the gather; per grid point 4 B x (zero,
+    spread write, gather read) and 4 B x (2 real-to-complex, 2 complex-to-real, 2 Green's-function
+    multiply) for the FFTs and the convolution."""
+    G = int(np.prod(fft))
+    return n_atoms * 44 + G * 4 * 9
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,10 +489,11 @@ def main():
     ap.add_argument("--pair-shape", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="pair-kernel shape (sb_lj_set_kernel_variant); 0 = pick by timing")
     ap.add_argument("--workload", default="solvated96k",
-                    choices=["solvated96k", "fep48", "modules"],
-                    help="fep48: the 48 batched FEP/TI lambda windows (parity case, reported "
-                         "separately from the headline line); modules: the 1-4 pair, virtual "
-                         "atom and integrator/SETTLE calls on covid-tip4p (reported separately)")
+                    choices=["solvated96k", "water1m", "fep48", "modules"],
+                    help="water1m: the 1,000,512-atom water box with PME 216^3 (both forms, "
+                         "per-kernel roofline; reported separately from the headline line); "
+                         "fep48: the 48 batched FEP/TI lambda windows; modules: the 1-4 pair, "
+                         "virtual atom and integrator/SETTLE calls on covid-tip4p")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -431,9 +505,16 @@ def main():
     if args.workload == "modules":
         run_modules(args, rank, world, local)
         return
+    run_md(args, rank, world, local)
 
+
+def run_md(args, rank, world, local):
+    """The headline (and the water1m line): NVE MD steps of the chosen form on moving
+    coordinates, each the list update by its policy (rebuild every 20 steps; the pruned pair list
+    renewed on 0.25 A moves and every 5 steps) followed by one captured CUDA graph of fixed
+    point, force step and the fused leap-frog + SETTLE launch."""
     import torch
-    import sponge_b200
+    import sponge_b200  # noqa: F401  (fails loudly without the library)
     from sponge_b200 import FORM_FIXED, FORM_PLAIN, NonbondedEngine, systems
 
     torch.cuda.set_device(local)
@@ -443,107 +524,94 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    s = systems.config1()
+    big = args.workload == "water1m"
+    s = systems.config2() if big else systems.config1()
+    cfg = water1m_config() if big else workload_config()
+    metric = WATER1M_METRIC if big else METRIC
     form = FORM_FIXED if args.form == "fixed" else FORM_PLAIN
-    eng = NonbondedEngine(s, form=form, refresh_interval=20)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    eng.update_list(forced=1)
-    eng.to_uint()
-    # autotuner: time each pair-kernel shape on this list and keep the fastest (or the shape
-    # given on the command line, e.g. for a profiler run, whose timings would mislead the tuner)
-    pair_shape = None
-    if form == FORM_FIXED:
-        if args.pair_shape:
-            eng.lj.set_kernel_variant(args.pair_shape)
-            pair_shape = args.pair_shape
-        else:
-            pair_shape = eng.lj.tune(eng.nl, eng.uint_crd, eng.charge, eng.pme.beta)
 
-    if form == FORM_FIXED:
-        # the force part is a fixed launch sequence: captured once, replayed every step after
-        # the list update by its policy
-        eng.capture_force_graph()
+    def make(form_):
+        eng = NonbondedEngine(s, form=form_, refresh_interval=20)
+        eng.update_list(forced=1)
+        eng.to_uint()
+        shape = None
+        if form_ == FORM_FIXED:
+            # autotuner: time each pair-kernel shape on this list and keep the fastest (or the
+            # shape given on the command line, e.g. for a profiler run)
+            if args.pair_shape:
+                eng.lj.set_kernel_variant(args.pair_shape)
+                shape = args.pair_shape
+            else:
+                shape = eng.lj.tune(eng.nl, eng.uint_crd, eng.charge, eng.pme.beta)
+        md = setup_md(eng, s, seed=2000 + rank)
+        eng.md_step(*md)
+        eng.capture_md_graph(*md)
+        return eng, md, shape
 
-        def one_step():
-            eng.step_graph()
-    else:
-        def one_step():
-            eng.frc.zero_()
-            eng.step(need_energy=0, need_virial=0)
-
+    eng, md, pair_shape = make(form)
     for _ in range(max(3, args.warmup)):
-        one_step()
+        eng.md_step_graph()
     torch.cuda.synchronize()
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
 
     clocks = ClockSampler(local)
     clocks.start()
-    barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
     t_wall = time.perf_counter()
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        ev[k][0].record(stream)
-        one_step()
-        ev[k][1].record(stream)
-    barrier()
+    dev = timed_steps(eng.md_step_graph, args.steps, flush, stream, dist)
     t_wall = time.perf_counter() - t_wall
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
 
-    # e2e through the public API with host buffers
-    crd_host = torch.from_numpy(s["crd"].copy()).pin_memory()
-    frc_host = torch.empty((eng.n, 3), dtype=torch.float32).pin_memory()
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        ev2[k][0].record(stream)
+    # e2e through the public API with host buffers: every step the caller's coordinates are
+    # copied in from pinned host memory, the MD step runs, and the new coordinates are copied
+    # back (the host owns the state: step k + 1 starts from what step k returned)
+    crd_host = torch.empty((eng.n, 3), dtype=torch.float32).pin_memory()
+    crd_host.copy_(eng.crd)
+
+    def e2e_step():
         eng.crd.copy_(crd_host, non_blocking=True)
-        eng.to_uint()
-        one_step()
-        frc_host.copy_(eng.frc, non_blocking=True)
-        ev2[k][1].record(stream)
-    barrier()
+        eng.md_step_graph()
+        crd_host.copy_(eng.crd, non_blocking=True)
+    e2e = timed_steps(e2e_step, args.steps, flush, stream, dist)
     clk = clocks.stop()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in ev2)
 
-    # roofline of the dominant kernel (LJ + Ewald direct pair kernel), timed in isolation
-    evp = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(20)]
-    for k in range(20):
-        flush.fill_(float(k))
-        evp[k][0].record(stream)
-        eng.forces(parts=("direct",))
-        evp[k][1].record(stream)
-    torch.cuda.synchronize()
-    pair_ms = float(np.mean([a.elapsed_time(b) for a, b in evp]))
-    md_ms = time_integrator(eng, s, flush, stream) if form == FORM_FIXED else None
+    # force-only step on frozen coordinates (the previous headline): list update + force graph
+    eng.capture_force_graph()
+    for _ in range(3):
+        eng.step_graph()
+    fo = timed_steps(eng.step_graph, args.steps, flush, stream, dist)
+    kt = kernel_times(eng, flush, stream)
+    crd_scratch = eng.crd.clone()
+    md_ms = float(np.mean(timed_steps(
+        lambda: md[0].nve_step(eng.uint_crd, eng.scaler, md[1], md[2], eng.frc, md[3],
+                               crd_scratch, eng.box, acc=md[4]), 10, flush, stream)))
 
-    ms, e2e_step_ms = max_over_ranks([dev_ms / args.steps, e2e_ms / args.steps], dist, "cuda")
+    ms, e2e_ms, fo_ms = max_over_ranks([float(np.mean(dev)), float(np.mean(e2e)),
+                                        float(np.mean(fo))], dist, "cuda")
+    # the chosen form's forces at the current coordinates (list rebuilt), for the force error
+    eng.update_list(forced=1)
+    eng.to_uint()
+    eng.frc.zero_()
+    eng.force()
+    crd_snapshot = eng.crd.clone()
+    uc = eng.uint_crd.cpu().numpy().view(np.uint32)
+    f_fixed = eng.frc.cpu().numpy()
     if rank != 0:
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()
         return
 
-    uc = eng.uint_crd.cpu().numpy().view(np.uint32)
     n_list, n_cut = pair_counts(s, uc)
-    # algorithmic work: the pairs inside the cut-off (list pairs beyond it are overhead)
     flops = FLOP_PER_PAIR * n_cut
+    pair_ms = kt["pair"]
     achieved = flops / (pair_ms * 1e-3) / 1e12
-    rebuilds_per_step = 1.0 / 20
-    # pack, pair, spread, z R2C, fused y-x plane pass, z C2R, gather (with the exclusion
-    # correction), finalize
-    launches_force = 8
-    launches_rebuild = 6
+    rb = pme_bytes(eng.n, (eng.pme.fftx, eng.pme.ffty, eng.pme.fftz))
+    hbm_peak = hbm_view(0, 1.0)["peak"]
+    # launches per MD step: fixed point, the 8 of the force step, the integrator; a rebuild (6)
+    # every 20 steps
+    launches = 10 if form == FORM_FIXED else None
     line = {
-        "metric": METRIC,
+        "metric": metric,
         "value": world * ns_per_day(ms * 1e-3),
         "unit": "ns/day",
         "n_gpus": world,
@@ -555,64 +623,82 @@ def main():
         "vs_baseline": None,
         "dtype": "f32 pair math, int64 fixed-point accumulation, f64 energies" if form == FORM_FIXED
                  else "f32 float atomics",
-        "data": "synthetic (seeded generator, sponge_b200.systems.config1)",
-        "config": dict(workload_config(), form=args.form, pair_kernel_shape=pair_shape),
-        "e2e": {"value": world * ns_per_day(e2e_step_ms * 1e-3), "unit": "ns/day",
+        "data": "synthetic (seeded generator, sponge_b200.systems.%s; free solute atoms relaxed "
+                "by steepest descent, Maxwell-Boltzmann velocities at 300 K)"
+                % ("config2" if big else "config1"),
+        "config": dict(cfg, form=args.form, pair_kernel_shape=pair_shape),
+        "e2e": {"value": world * ns_per_day(e2e_ms * 1e-3), "unit": "ns/day",
                 "h2d_bytes_per_step": int(eng.n * 12), "d2h_bytes_per_step": int(eng.n * 12)},
-        "gpu_launches": int(round(args.steps * (launches_force + launches_rebuild * rebuilds_per_step))),
+        "gpu_launches": None if launches is None else
+            int(round(args.steps * (launches + 6 / 20.0))),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
-                     "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS, "traffic": PAIR_DRAM_BYTES,
-                     "kernel": "%s (LJ + Ewald direct; timed with its pack kernel)"
+                     "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS,
+                     "traffic": PAIR_DRAM_BYTES if not big else None,
+                     "kernel": "%s (LJ + Ewald direct; timed with its pack and finalize)"
                                % PAIR_KERNEL.get(pair_shape, "k_pair_fixed"),
                      "kernel_ms": pair_ms, "pairs_in_cutoff": n_cut, "pairs_in_list": n_list,
                      "peak_note": "nominal FP32 peak 148 SM x 128 lanes x 2 x 1.965 GHz (the "
                                   "measured peaks cover HBM copy and bf16 tensor throughput "
-                                  "only); the kernel is bound by instruction issue",
-                     "hbm": hbm_view(PAIR_DRAM_BYTES, pair_ms)},
-        "integrator": None if md_ms is None else {
-            "kernel": "k_md_step: NVE leap-frog + SETTLE of 31,000 rigid waters and 3,000 free "
-                      "atoms in one launch (the call after the force step; not in the step above)",
-            "ms": md_ms},
+                                  "only); the kernel is bound by instruction issue"},
+        "kernels": {
+            "pair_ms": pair_ms,
+            "reciprocal": {"ms": kt["reciprocal"], "algorithmic_bytes": rb,
+                           "achieved_gbs": rb / (kt["reciprocal"] * 1e-3) / 1e9,
+                           "peak_gbs": hbm_peak,
+                           "frac": rb / (kt["reciprocal"] * 1e-3) / 1e9 / hbm_peak},
+            "rebuild_ms": kt["rebuild"],
+            "integrator_ms": md_ms,
+        },
+        "force_only": {"value": world * ns_per_day(fo_ms * 1e-3), "unit": "ns/day",
+                       "ms_per_step": fo_ms,
+                       "what": "list update by its policy + force graph on frozen coordinates"},
         "clocks": clk,
         "wall_s": t_wall,
     }
-    if not args.no_plain and form == FORM_FIXED:
-        del eng
-        torch.cuda.synchronize()
-        pe = NonbondedEngine(s, form=FORM_PLAIN, refresh_interval=20)
-        pe.update_list(forced=1)
-        pe.to_uint()
-        # the plain form's force part is captured the same way (graph replay per step)
-        pe.capture_force_graph()
-        for _ in range(5):
-            pe.step_graph()
-        torch.cuda.synchronize()
-        evq = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(min(args.steps, 100))]
-        for k in range(len(evq)):
-            flush.fill_(float(k))
-            evq[k][0].record(stream)
-            pe.step_graph()
-            evq[k][1].record(stream)
-        torch.cuda.synchronize()
-        pms = float(np.mean([a.elapsed_time(b) for a, b in evq]))
-        line["plain_form"] = {"value": ns_per_day(pms * 1e-3), "unit": "ns/day",
-                              "ms_per_step": pms,
-                              "speedup_fixed_over_plain": pms / ms}
+    if not big:
+        line["roofline"]["hbm"] = hbm_view(PAIR_DRAM_BYTES, pair_ms)
+    import oracle
+    beta = oracle.get_beta(s["cutoff"])
+    ref_f = None
     if not args.no_cpu_baseline:
-        import oracle
-        beta = oracle.get_beta(s["cutoff"])
         t = time.perf_counter()
-        oracle.nonbonded(uc, s, beta)
+        ref_f, _, _ = oracle.nonbonded(uc, s, beta)
         sec = time.perf_counter() - t
         line["cpu_baseline"] = {"value": ns_per_day(sec), "unit": "ns/day",
                                 "cores": oracle.threads(), "kind": "port",
-                                "sample": "one full FP64 evaluation of the same 96,000-atom path "
-                                          "(%.2f s)" % sec}
+                                "sample": "one full FP64 evaluation of the same %d-atom path "
+                                          "(%.2f s)" % (eng.n, sec)}
+        line["force_error_vs_fp64"] = {args.form: rel_rms(f_fixed, ref_f)}
+    if not args.no_plain and form == FORM_FIXED:
+        del eng, md
+        torch.cuda.synchronize()
+        pe, pmd, _ = make(FORM_PLAIN)
+        for _ in range(max(3, args.warmup)):
+            pe.md_step_graph()
+        pdev = timed_steps(pe.md_step_graph, min(args.steps, 100), flush, stream)
+        pms = float(np.mean(pdev))
+        plain = {"value": ns_per_day(pms * 1e-3), "unit": "ns/day", "ms_per_step": pms,
+                 "speedup_fixed_over_plain": pms / ms}
+        if ref_f is not None:
+            # the plain form's forces at the same coordinates
+            pe.crd.copy_(crd_snapshot)
+            pe.update_list(forced=1)
+            pe.to_uint()
+            assert np.array_equal(pe.uint_crd.cpu().numpy().view(np.uint32), uc)
+            pe.frc.zero_()
+            pe.force()
+            line["force_error_vs_fp64"]["plain"] = rel_rms(pe.frc.cpu().numpy(), ref_f)
+        line["plain_form"] = plain
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
 if __name__ == "__main__":

@@ -233,8 +233,11 @@ SB_API int sb_pme_reciprocal_force(sb_pme* pme, const uint32_t* d_uint_crd, cons
                             float* d_potential, void* stream);
 
 /* Particle_Mesh_Ewald::Get_Energy (PME_force.cu:892-994). which_part is SB_PME_*. The DIRECT
- * part is evaluated over the list of `nl` (may be NULL for other parts). h_parts (optional,
- * 5 doubles) receives total, direct, reciprocal, correction, self as computed (FP64). */
+ * part is evaluated over the list of `nl` (may be NULL for other parts; it must hold as many
+ * atoms as `pme`). h_parts (optional, 5 doubles) receives total, direct, reciprocal, correction,
+ * self as computed (FP64). The forces that the reciprocal and exclusion passes produce on the
+ * way are discarded into a 3N-float array of the module, allocated on the first call and kept
+ * until sb_pme_destroy. */
 SB_API int sb_pme_get_energy(sb_pme* pme, sb_neighbor_list* nl, const uint32_t* d_uint_crd,
                       const float* d_charge, const float scaler[3],
                       const int* d_excluded_list_start, const int* d_excluded_list,
@@ -244,12 +247,16 @@ SB_API int sb_pme_get_energy(sb_pme* pme, sb_neighbor_list* nl, const uint32_t* 
 /* Allocation-free variant of sb_pme_get_energy (no counterpart in the reference). Same
  * arguments and results. sb_pme_get_energy allocates and frees a 3N-float array on every call
  * for the forces its reciprocal and exclusion passes produce and then discard; this variant uses
- * a fixed 1.5 MiB device block that the library reserves when it is loaded, for callers that
- * cannot allocate: programs whose device memory is all handed to their own pool allocator, and
- * loops that must not pay for cudaFree, which waits for the whole device.
- *   - at most 131072 atoms (larger modules are rejected with SB_ERR_ARG);
+ * a fixed 1.5 MiB device block of the library instead, for callers that cannot allocate:
+ * programs whose device memory is all handed to their own pool allocator, and loops that must
+ * not pay for cudaFree, which waits for the whole device. The block exists on a device once the
+ * library's device code is loaded there, which happens at the latest in sb_pme_create.
+ *   - at most 131072 atoms (larger modules are rejected with SB_ERR_ARG); `nl` must hold as many
+ *     atoms as `pme` when the DIRECT part (or TOTAL) is asked for (else SB_ERR_ARG);
  *   - the first call on each device looks up the block's device address (with that device
- *     current); make that first call before beginning any stream capture;
+ *     current) and keeps it for the life of the process; make that first call before beginning
+ *     any stream capture. The kept address does not survive cudaDeviceReset or anything else
+ *     that destroys the device's primary context: do not call this entry point after that;
  *   - the DIRECT part (and TOTAL) reads the list's ATOM_GROUP export, which allocates on first
  *     use: call sb_nl_atom_group once beforehand, or the call fails with SB_ERR_STATE;
  *   - every call on a device shares the one block: calls whose GPU work overlaps (other streams,

@@ -219,6 +219,7 @@ struct sb_pme {
     float* d_direct_atom_energy = nullptr;
     float* d_correction_atom_energy = nullptr;
     long long* d_fix = nullptr;     // [3N] exclusion-correction accumulator (original order)
+    float* energy_scratch = nullptr; // [3N] discarded forces of energy queries (first query)
     void* cufft_r2c = nullptr;      // plain form: cuFFT handles (stored as int)
     void* cufft_c2r = nullptr;
     int cufft_ok = 0;

@@ -946,8 +946,20 @@ extern "C" int sb_nl_update_volume(sb_neighbor_list* nl, const float box_length[
         sb_set_error("sb_nl_update_volume: null argument");
         return SB_ERR_ARG;
     }
+    for (int d = 0; d < 3; d++) {
+        if (!(box_length[d] > 0.f)) {
+            sb_set_error("sb_nl_update_volume: box lengths must be positive");
+            return SB_ERR_ARG;
+        }
+    }
     for (int d = 0; d < 3; d++) nl->box[d] = box_length[d];
-    // the column grid keeps its counts (as the reference keeps its cell counts); widths change
+    // the column grid keeps its counts (as the reference keeps its cell counts); the widths
+    // change, so the number of columns the search window spans is recomputed (a shrinking box
+    // needs more of them). The capacities keep their sizes; an overflow at the new density sets
+    // the status flags like any other.
+    const double cwx = (double)nl->box[0] / nl->ncx, cwy = (double)nl->box[1] / nl->ncy;
+    nl->nxr = (int)ceil(nl->cs / cwx);
+    nl->nyr = (int)ceil(nl->cs / cwy);
     nl->needs_rebuild = 1;
     return SB_OK;
 }

@@ -497,7 +497,8 @@ extern "C" int sb_pme_destroy(sb_pme* p) {
         cufftDestroy((cufftHandle)(intptr_t)p->cufft_c2r);
     }
     void* ps[] = {p->d_qfix, p->d_qf, p->d_spec, p->d_theta, p->d_bc, p->d_epart, p->d_ered,
-                  p->d_direct_atom_energy, p->d_correction_atom_energy, p->d_fix};
+                  p->d_direct_atom_energy, p->d_correction_atom_energy, p->d_fix,
+                  p->energy_scratch};
     for (void* x : ps) sb_free(x);
     delete p;
     return SB_OK;
@@ -678,51 +679,46 @@ extern "C" int sb_pme_get_energy(sb_pme* p, sb_neighbor_list* nl, const uint32_t
     cudaStream_t s = sb_stream(stream);
     const int n = p->n;
     const int all = which_part == SB_PME_TOTAL;
-    int nparts = 0;
-    float* scratch_frc = nullptr;
-    if (all || which_part == SB_PME_RECIPROCAL) {
-        // the reciprocal energy comes with a force evaluation into a scratch array
-        SB_TRY(sb_malloc((void**)&scratch_frc, sizeof(float) * 3 * n, "energy scratch"));
-        cudaMemsetAsync(scratch_frc, 0, sizeof(float) * 3 * n, s);
-        int st = reciprocal(p, d_uint_crd, d_charge, scratch_frc, 1, s, &nparts);
-        if (st) {
-            sb_free(scratch_frc);
-            return st;
-        }
-    }
-    float* direct = nullptr;
-    float* corr = nullptr;
-    if (all || which_part == SB_PME_DIRECT) {
+    const int want_rec = all || which_part == SB_PME_RECIPROCAL;
+    const int want_dir = all || which_part == SB_PME_DIRECT;
+    const int want_cor = all || which_part == SB_PME_CORRECTION;
+    if (want_dir) {
         if (!nl) {
-            sb_free(scratch_frc);
             sb_set_error("sb_pme_get_energy: the DIRECT part needs the neighbor list");
             return SB_ERR_ARG;
         }
-        int st = sb_nl_build_atom_group(nl, s);
-        if (st) {
-            sb_free(scratch_frc);
-            return st;
+        if (nl->n != n) {
+            sb_set_error("sb_pme_get_energy: the neighbor list holds %d atoms, the PME module %d",
+                         nl->n, n);
+            return SB_ERR_ARG;
         }
+    }
+    int nparts = 0;
+    if ((want_rec || want_cor) && !p->energy_scratch) {
+        // the reciprocal and exclusion passes produce forces that the energy query discards:
+        // they go to an array of the module, allocated on the first query and kept
+        SB_TRY(sb_malloc((void**)&p->energy_scratch, sizeof(float) * 3 * n, "energy scratch"));
+    }
+    if (want_rec || want_cor)
+        SB_CHECK_CUDA(cudaMemsetAsync(p->energy_scratch, 0, sizeof(float) * 3 * n, s));
+    if (want_rec) SB_TRY(reciprocal(p, d_uint_crd, d_charge, p->energy_scratch, 1, s, &nparts));
+    float* direct = nullptr;
+    float* corr = nullptr;
+    if (want_dir) {
+        SB_TRY(sb_nl_build_atom_group(nl, s));
         k_direct_energy_list<<<(n + 127) / 128, 128, 0, s>>>(n, nl->ag, d_uint_crd, d_charge,
                                                              scaler[0], scaler[1], scaler[2],
                                                              p->beta, p->cutoff * p->cutoff,
                                                              p->d_direct_atom_energy);
+        SB_CHECK_LAUNCH();
         direct = p->d_direct_atom_energy;
     }
-    if (all || which_part == SB_PME_CORRECTION) {
+    if (want_cor) {
         k_zero_f<<<(n + 1023) / 1024, 1024, 0, s>>>(n, p->d_correction_atom_energy);
-        if (!scratch_frc) {
-            SB_TRY(sb_malloc((void**)&scratch_frc, sizeof(float) * 3 * n, "energy scratch"));
-            cudaMemsetAsync(scratch_frc, 0, sizeof(float) * 3 * n, s);
-        }
-        if (es && el && en) {
-            int st = excluded_force(p, d_uint_crd, scaler, d_charge, es, el, en, scratch_frc,
-                                    p->d_correction_atom_energy, s);
-            if (st) {
-                sb_free(scratch_frc);
-                return st;
-            }
-        }
+        SB_CHECK_LAUNCH();
+        if (es && el && en)
+            SB_TRY(excluded_force(p, d_uint_crd, scaler, d_charge, es, el, en, p->energy_scratch,
+                                  p->d_correction_atom_energy, s));
         corr = p->d_correction_atom_energy;
     }
     k_pme_energy_finish<<<1, 1024, 0, s>>>(n, d_charge, p->d_epart, nparts, direct, corr,
@@ -733,7 +729,6 @@ extern "C" int sb_pme_get_energy(sb_pme* p, sb_neighbor_list* nl, const uint32_t
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(parts, p->d_ered, sizeof(double) * 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    sb_free(scratch_frc);
     if (e != cudaSuccess) {
         sb_set_error("sb_pme_get_energy: %s", cudaGetErrorString(e));
         return SB_ERR_CUDA;
@@ -1144,7 +1139,8 @@ extern "C" int sb_pme_ti_cross(sb_pme* p, const uint32_t* d_uint_crd, const floa
 // cudaFree on every call. Some callers cannot do that: a host program whose device memory is
 // fully handed to its own pool allocator, or a driver loop that must not pay for cudaFree, which
 // waits for the whole device. sb_pme_get_energy_noalloc takes that array from a fixed block of
-// device memory that this library reserves at load time instead.
+// device memory of this library instead (it exists on a device once the library's device code
+// is loaded there: at the latest in sb_pme_create).
 // ---------------------------------------------------------------------------------------------
 #define SB_NOALLOC_MAX_ATOMS 131072  // 3 x 131072 floats = 1.5 MiB, held by every GPU that loads
                                      // the library until the process exits
@@ -1153,7 +1149,10 @@ extern "C" int sb_pme_ti_cross(sb_pme* p, const uint32_t* d_uint_crd, const floa
 static __device__ __align__(256) float g_noalloc_frc[3 * SB_NOALLOC_MAX_ATOMS];
 
 // Host code may not hand g_noalloc_frc itself to a kernel (on the host it only names a stand-in
-// object); its device address is looked up once per device, with that device current.
+// object); its device address is looked up once per device, with that device current, and kept
+// for the life of the process. A kept address is stale after cudaDeviceReset (or anything else
+// that destroys the device's primary context); the header says callers must not call the entry
+// point after that.
 static float* g_noalloc_frc_addr[SB_NOALLOC_MAX_DEVICES];
 static std::mutex g_noalloc_mu;
 
@@ -1210,6 +1209,11 @@ extern "C" int sb_pme_get_energy_noalloc(sb_pme* p, sb_neighbor_list* nl,
     if (want_dir) {
         if (!nl) {
             sb_set_error("sb_pme_get_energy_noalloc: the DIRECT part needs the neighbor list");
+            return SB_ERR_ARG;
+        }
+        if (nl->n != n) {
+            sb_set_error("sb_pme_get_energy_noalloc: the neighbor list holds %d atoms, the PME "
+                         "module %d", nl->n, n);
             return SB_ERR_ARG;
         }
         if (!nl->ag) {

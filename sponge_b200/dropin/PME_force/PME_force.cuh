@@ -2,8 +2,8 @@
 // same struct, the public members the MD driver reads (beta, fft sizes, d_direct_atom_energy,
 // d_correction_atom_energy, energy parts) and method signatures; spread, FFT, convolution and
 // gather are libsponge_b200's, reached through the C ABI. The cuFFT plans and per-atom stencil
-// arrays of the reference are internal to the library and not exposed (TI_CORE reads them;
-// see INTEGRATION.md).
+// arrays of the reference are internal to the library and not exposed; the TI cross terms
+// that TI_CORE derives from them are computed by sb_pme_ti_cross.
 #ifndef PME_FORCE_CUH
 #define PME_FORCE_CUH
 #include "../common.cuh"

@@ -1,7 +1,7 @@
 // Drop-in replacement for SPONGE's NEIGHBOR_LIST (SPONGE/neighbor_list/neighbor_list.cuh:44-106).
 // Same struct name, public members read by other modules and method signatures; the work is done
 // by libsponge_b200 through its C ABI (include/sponge_b200.h). Place this directory over
-// SPONGE/neighbor_list and link libsponge_b200.so (INTEGRATION.md).
+// SPONGE/neighbor_list and link libsponge_b200.so.
 #ifndef NEIGHBOR_LIST_CUH
 #define NEIGHBOR_LIST_CUH
 #include "../common.cuh"

@@ -57,6 +57,8 @@ class NonbondedEngine:
         self.d_virial = torch.zeros(1, dtype=torch.float32, device=dev)
         self.d_potential = torch.zeros(1, dtype=torch.float32, device=dev)
         self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
+        self._graph = None
+        self._md_graph = None
 
     @property
     def excl(self):
@@ -108,9 +110,25 @@ class NonbondedEngine:
                         self.frc, need_energy, need_virial, self.atom_energy, self.atom_virial,
                         self.d_virial, self.d_potential, stream=stream)
 
+    def update_box(self, box_length):
+        """Box change as Main_Box_Length_Change / Main_Volume_Change call it (SPONGE/main.cu:438-460)
+        after the caller has scaled the coordinates: NEIGHBOR_LIST::Update_Volume (the next list
+        update rebuilds), LENNARD_JONES_INFORMATION::Update_Volume and
+        Particle_Mesh_Ewald::Update_Box_Length. Captured graphs hold the old box's scale factors
+        as kernel arguments, so they are dropped here and captured again at their next replay."""
+        box = np.asarray(box_length, np.float32).reshape(3)
+        self.nl.Update_Volume(box)
+        self.lj.Update_Volume(box)
+        self.pme.Update_Box_Length(box)
+        self.box = box
+        self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
+        self._graph = None
+        self._md_graph = None
+
     def capture_force_graph(self):
         """Capture (frc = 0; force part) once as a CUDA graph; ``step_graph`` replays it after
-        the list update by its policy. Call once eagerly first (lazy per-list buffers)."""
+        the list update by its policy. Call once eagerly first (lazy per-list buffers). A box
+        change (``update_box``) drops the graph; ``step_graph`` then captures it again."""
         torch = self.torch
         self.frc.zero_()
         self.force()
@@ -124,8 +142,11 @@ class NonbondedEngine:
         return g
 
     def step_graph(self):
-        """List update by its policy (eager), then the captured force graph."""
+        """List update by its policy (eager), then the captured force graph (captured again
+        first when the box changed since the last capture)."""
         self.update_list()
+        if self._graph is None:
+            self.capture_force_graph()
         self._graph.replay()
 
     def md_step(self, settle, inverse_mass, mass, vel, acc=None):
@@ -150,12 +171,17 @@ class NonbondedEngine:
         with torch.cuda.graph(g, stream=side):
             self.md_step(settle, inverse_mass, mass, vel, acc)
         self._md_graph = g
+        self._md_args = (settle, inverse_mass, mass, vel, acc)
         return g
 
     def md_step_graph(self):
         """List update by its policy (eager, wraps the coordinates on rebuilds), then the captured
-        MD step."""
+        MD step (captured again, with the buffers of the last capture, after a box change)."""
         self.update_list()
+        if self._md_graph is None:
+            self.md_step(*self._md_args)
+            self.capture_md_graph(*self._md_args)
+            return
         self._md_graph.replay()
 
     def potential(self):

@@ -36,7 +36,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 INPUTS = os.path.join(HERE, "covid_tip4p_inputs.npz")
 REFERENCE = os.path.join(HERE, "reference_covid_tip4p.npz")
-SOURCE = "/root/reference/SPONGE/covid-tip4p"
+# the reference tree is read where the harness scripts read it (REF, as in
+# oracle/ref_harness/build_all.sh)
+SOURCE = os.path.join(os.environ.get("REF", "/root/reference/SPONGE"), "covid-tip4p")
 # Get_Fft_Patameter's grid for the fixture's box (108.43 x 91.25 x 84.41 A)
 FFT = (112, 96, 96)
 # the MD step: 2 fs in SPONGE's internal time unit (MD_core.cu reads dt in ps and multiplies by

@@ -3,12 +3,13 @@
 sb_pme_get_energy allocates (and frees) a throwaway force array on every call. Callers that
 cannot allocate device memory at that point -- a host program whose GPU memory is all owned by
 its own pool allocator, or a tight driver loop that cannot afford cudaFree's device-wide wait --
-use sb_pme_get_energy_noalloc, which takes that array from a fixed block the library reserves
-when it is loaded (up to 131072 atoms). This file checks, through the C ABI, that it returns the
-same energy parts as sb_pme_get_energy on two calls in a row (energies within 1e-5 relative, the
-energy tolerance of the other GPU tests), and that it refuses what it cannot do without
-allocating. It is collected last so that a run stopping at the first failure has already run
-every other test; it creates its own modules and passes alone or after the other tests.
+use sb_pme_get_energy_noalloc, which takes that array from a fixed block of the library's device
+memory (up to 131072 atoms). This file checks, through the C ABI, that it returns the same energy
+parts as sb_pme_get_energy on two calls in a row (energies within 1e-5 relative, the energy
+tolerance of the other GPU tests), that further calls leave the device's free memory unchanged,
+and that it refuses what it cannot do without allocating. It is collected last so that a run
+stopping at the first failure has already run every other test; it creates its own modules and
+passes alone or after the other tests.
 """
 
 import ctypes
@@ -67,6 +68,27 @@ def test_noalloc_energy_matches_allocating_query(engine):
             assert np.all(p[~nz] == 0), (which, call, p)
 
 
+def test_noalloc_leaves_device_memory_unchanged(engine):
+    """The property the entry point exists for: after its first call on the device, further
+    calls take no device memory (free memory as the driver reports it does not move)."""
+    import torch
+    import sponge_b200
+    from sponge_b200 import PME_TOTAL
+    L = sponge_b200.lib()
+    eng = engine
+    eng.nl.d_nl
+    st, _, _ = _parts(L.sb_pme_get_energy_noalloc, eng, PME_TOTAL)
+    assert st == 0, L.sb_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(4):
+        st, _, _ = _parts(L.sb_pme_get_energy_noalloc, eng, PME_TOTAL)
+        assert st == 0, L.sb_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_refuses_what_would_allocate():
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
@@ -88,3 +110,11 @@ def test_noalloc_refuses_what_would_allocate():
                                      None, _stream(None))
     assert st == 1 and b"maximum" in L.sb_last_error()
     big.Clear()
+    # a list of another system (another atom count) is refused before any launch
+    other = NonbondedEngine(systems.small_water(n_side=3))
+    other.update_list(forced=1)
+    other.nl.d_nl
+    st = L.sb_pme_get_energy_noalloc(eng.pme.handle, other.nl.handle, _ptr(eng.uint_crd),
+                                     _ptr(eng.charge), _box3(eng.scaler), None, None, None,
+                                     PME_DIRECT, None, None, _stream(None))
+    assert st == 1 and b"holds" in L.sb_last_error()
