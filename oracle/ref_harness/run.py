@@ -107,3 +107,61 @@ def run(system, uc, pair_keys, timing_steps=0, outdir=None, timeout=900):
         if os.path.exists(path):
             out[name] = np.fromfile(path, np.float32).reshape(shape)
     return out
+
+
+SC_BIN = os.path.join(os.path.dirname(HERE), "_ref", "sc_harness")
+
+
+def sc_available():
+    return os.path.exists(SC_BIN)
+
+
+def write_sc_input(path, system, max_nb, max_grid):
+    """Input of sc_harness for an FEP box of sponge_b200.systems.fep_box (charges at lambda)."""
+    n = len(system["charge"])
+    TA, TB = int(system["n_types"]), int(system["n_types_B"])
+    fft = system["fft"]
+    el = np.asarray(system["excl_list"], np.int32)
+    with open(path, "wb") as f:
+        np.array([n, TA, TB, el.size, fft[0], fft[1], fft[2], max_nb, max_grid],
+                 np.int32).tofile(f)
+        np.array([*system["box"], system["cutoff"], system["skin"], system["tolerance"],
+                  system["lam"], system["sc_alpha"], system["sc_p"], system["sc_sigma"],
+                  system["sc_sigma_min"]], np.float32).tofile(f)
+        np.asarray(system["crd"], np.float32).tofile(f)
+        np.asarray(system["charge"], np.float32).tofile(f)
+        np.asarray(system["dq"], np.float32).tofile(f)
+        np.asarray(system["lj_type"], np.int32).tofile(f)
+        np.asarray(system["lj_type_B"], np.int32).tofile(f)
+        np.asarray(system["mask"], np.int32).tofile(f)
+        np.asarray(system["lj_A"], np.float32).tofile(f)
+        np.asarray(system["lj_B"], np.float32).tofile(f)
+        np.asarray(system["lj_A_B"], np.float32).tofile(f)
+        np.asarray(system["lj_B_B"], np.float32).tofile(f)
+        np.asarray(system["excl_start"], np.int32).tofile(f)
+        np.asarray(system["excl_numbers"], np.int32).tofile(f)
+        el.tofile(f)
+
+
+def run_softcore(system, uc, pair_keys, outdir=None, timeout=600):
+    """Runs sc_harness on an FEP box; returns dict(frc, ae, av, adir, pairs, summary). The list
+    capacities are computed from the system as in run()."""
+    max_nb, max_grid = safe_capacities(system, uc, pair_keys)
+    outdir = outdir or tempfile.mkdtemp(prefix="refsc_")
+    os.makedirs(outdir, exist_ok=True)
+    inp = os.path.join(outdir, "in.bin")
+    write_sc_input(inp, system, max_nb, max_grid)
+    r = subprocess.run([SC_BIN, inp, outdir], stdin=subprocess.DEVNULL, capture_output=True,
+                       text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("soft-core harness failed (%d): %s" % (r.returncode, r.stderr[-2000:]))
+    n = len(system["charge"])
+    summ = {}
+    for line in open(os.path.join(outdir, "summary.txt")):
+        k, v = line.split()
+        summ[k] = float(v)
+    rdf = lambda name, shape: np.fromfile(os.path.join(outdir, name), np.float32).reshape(shape)  # noqa: E731
+    return dict(frc=rdf("sc_frc.f32", (n, 3)), ae=rdf("sc_ae.f32", (n,)),
+                av=rdf("sc_av.f32", (n,)), adir=rdf("sc_adir.f32", (n,)),
+                pairs=np.fromfile(os.path.join(outdir, "pairs.i64"), np.int64), summary=summ,
+                capacities=(max_nb, max_grid))

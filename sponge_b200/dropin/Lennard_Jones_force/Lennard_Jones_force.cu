@@ -4,6 +4,8 @@
 #include "../neighbor_list/neighbor_list.cuh"
 #include "sponge_b200.h"
 
+#include <vector>
+
 // helpers other modules link against (nb14 declares them too)
 __device__ __host__ VECTOR Get_Periodic_Displacement(const UINT_VECTOR_LJ_TYPE uvec_a, const UINT_VECTOR_LJ_TYPE uvec_b, const VECTOR scaler)
 {
@@ -130,11 +132,97 @@ void LENNARD_JONES_INFORMATION::Initial(CONTROLLER *controller, float cutoff, VE
     controller[0].printf("END INITIALIZING LENNARD JONES INFORMATION\n\n");
 }
 
+// AMBER parm7 sections are "%FLAG NAME", one "%FORMAT(...)" line, then the values as
+// whitespace-separated fields. Reads `count` values of the current section into `out`; returns
+// the number read.
+static int parm7_read_doubles(FILE *fp, double *out, int count)
+{
+    int got = 0;
+    while (got < count && fscanf(fp, "%lf", out + got) == 1)
+        got++;
+    return got;
+}
+
+// LENNARD_JONES_INFORMATION::Initial_From_AMBER_Parm (Lennard_Jones_force.cu:1201-1276): the
+// atom count and type count from POINTERS (its first two values), the per-atom type index
+// (ATOM_TYPE_INDEX, 1-based in the file) and the pair tables LENNARD_JONES_ACOEF / _BCOEF, read
+// in file order as the lower-triangular type-pair tables and scaled by 12 and 6 in double
+// before rounding to float, as the reference reads them.
 void LENNARD_JONES_INFORMATION::Initial_From_AMBER_Parm(const char *file_name, CONTROLLER controller)
 {
-    fprintf(stderr, "sponge_b200: LJ parameters from amber_parm7 (%s) are not read by this drop-in; "
-                    "provide LJ_in_file\n", file_name);
-    exit(1);
+    FILE *fp = NULL;
+    Open_File_Safely(&fp, file_name, "r");
+    controller.printf("    Start reading LJ information from AMBER file:\n");
+    char line[CHAR_LENGTH_MAX];
+    int have_pointers = 0, have_types = 0, have_a = 0, have_b = 0;
+    std::vector<double> vals;
+    while (fgets(line, CHAR_LENGTH_MAX, fp))
+    {
+        char flag[CHAR_LENGTH_MAX], name[CHAR_LENGTH_MAX];
+        if (sscanf(line, "%s %s", flag, name) != 2 || strcmp(flag, "%FLAG") != 0)
+            continue;
+        const int pointers = strcmp(name, "POINTERS") == 0;
+        const int types = strcmp(name, "ATOM_TYPE_INDEX") == 0;
+        const int acoef = strcmp(name, "LENNARD_JONES_ACOEF") == 0;
+        const int bcoef = strcmp(name, "LENNARD_JONES_BCOEF") == 0;
+        if (!(pointers || types || acoef || bcoef))
+            continue;
+        if (!fgets(line, CHAR_LENGTH_MAX, fp))  // the %FORMAT line
+            break;
+        if (pointers)
+        {
+            vals.resize(2);
+            if (parm7_read_doubles(fp, vals.data(), 2) != 2)
+                break;
+            atom_numbers = (int)vals[0];
+            atom_type_numbers = (int)vals[1];
+            pair_type_numbers = atom_type_numbers * (atom_type_numbers + 1) / 2;
+            controller.printf("        atom_numbers is %d\n        atom_LJ_type_number is %d\n",
+                              atom_numbers, atom_type_numbers);
+            LJ_Malloc();
+            have_pointers = 1;
+        }
+        else if (!have_pointers)
+        {
+            break;  // the tables are sized by POINTERS, which comes first in a parm7 file
+        }
+        else if (types)
+        {
+            vals.resize(atom_numbers);
+            have_types = parm7_read_doubles(fp, vals.data(), atom_numbers) == atom_numbers;
+            for (int i = 0; i < atom_numbers && have_types; i++)
+                h_atom_LJ_type[i] = (int)vals[i] - 1;
+        }
+        else
+        {
+            vals.resize(pair_type_numbers);
+            const int ok = parm7_read_doubles(fp, vals.data(), pair_type_numbers) == pair_type_numbers;
+            float *dst = acoef ? h_LJ_A : h_LJ_B;
+            const double scale = acoef ? 12.0 : 6.0;
+            for (int i = 0; i < pair_type_numbers && ok; i++)
+                dst[i] = (float)(scale * vals[i]);
+            (acoef ? have_a : have_b) = ok;
+        }
+    }
+    fclose(fp);
+    if (!(have_pointers && have_types && have_a && have_b))
+    {
+        fprintf(stderr, "sponge_b200: %s lacks POINTERS, ATOM_TYPE_INDEX or the LJ A/B tables, "
+                        "or one of them is truncated\n", file_name);
+        exit(1);
+    }
+    for (int i = 0; i < atom_numbers; i++)
+    {
+        if (h_atom_LJ_type[i] < 0 || h_atom_LJ_type[i] >= atom_type_numbers)
+        {
+            fprintf(stderr, "sponge_b200: %s: atom %d has LJ type %d of %d\n", file_name, i,
+                    h_atom_LJ_type[i] + 1, atom_type_numbers);
+            exit(1);
+        }
+    }
+    controller.printf("    End reading LJ information from AMBER file\n");
+    Parameter_Host_To_Device();
+    is_initialized = 1;
 }
 
 void LENNARD_JONES_INFORMATION::Clear()

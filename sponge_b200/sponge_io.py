@@ -133,6 +133,45 @@ def write_mdin(path, files, system, steps=10000, dt=0.002, refresh_interval=20,
 # ---------------------------------------------------------------------------------------------
 # readers
 # ---------------------------------------------------------------------------------------------
+def _parm7_section(f, name, fmt, values, per_line, width, conv):
+    f.write("%%FLAG %s\n%%FORMAT(%s)\n" % (name, fmt))
+    values = list(values)
+    for k in range(0, len(values), per_line):
+        f.write("".join(conv(v).rjust(width) for v in values[k:k + per_line]) + "\n")
+    if not values:
+        f.write("\n")
+
+
+def write_amber_parm7(path, system):
+    """The LJ part of an AMBER parm7 topology for ``system``: POINTERS (NATOM, NTYPES, the other
+    counts 0), ATOM_TYPE_INDEX (1-based), NONBONDED_PARM_INDEX and LENNARD_JONES_ACOEF / _BCOEF
+    (unscaled A = 4 eps sigma^12, B = 4 eps sigma^6, lower-triangular type-pair order). SPONGE's
+    LJ module reads exactly these when an mdin names ``amber_parm7`` and no ``LJ_in_file``
+    (Lennard_Jones_force.cu:1201-1276); the other modules read their own ``*_in_file`` first, and
+    with the counts 0 the angle, dihedral, 1-4 and CMAP readers initialise nothing."""
+    n = len(system["charge"])
+    T = int(system["n_types"])
+    A = np.asarray(system["lj_A"], np.float32)
+    B = np.asarray(system["lj_B"], np.float32)
+    ico = np.zeros(T * T, np.int64)
+    for i in range(T):
+        for j in range(T):
+            hi, lo = max(i, j), min(i, j)
+            ico[i * T + j] = hi * (hi + 1) // 2 + lo + 1
+    pointers = [n, T] + [0] * 29
+    e16 = lambda v: "%.8E" % float(v)  # noqa: E731  (9 significant digits: exact for float32)
+    with open(path, "w") as f:
+        f.write("%VERSION  VERSION_STAMP = V0001.000\n")
+        _parm7_section(f, "TITLE", "20a4", [], 20, 4, str)
+        _parm7_section(f, "POINTERS", "10I8", pointers, 10, 8, str)
+        _parm7_section(f, "ATOM_TYPE_INDEX", "10I8",
+                       (np.asarray(system["lj_type"], np.int64) + 1).tolist(), 10, 8, str)
+        _parm7_section(f, "NONBONDED_PARM_INDEX", "10I8", ico.tolist(), 10, 8, str)
+        _parm7_section(f, "LENNARD_JONES_ACOEF", "5E16.8", A.tolist(), 5, 16, e16)
+        _parm7_section(f, "LENNARD_JONES_BCOEF", "5E16.8", B.tolist(), 5, 16, e16)
+    return path
+
+
 def read_coordinate(path):
     """Coordinate or restart file (MD_core.cu:1213-1257): first line "N" or "N time", N lines of
     "x y z", then "Lx Ly Lz alpha beta gamma". Returns (crd [N,3] float32, box [3] float32)."""

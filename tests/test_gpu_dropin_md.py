@@ -9,7 +9,9 @@ bonds, NVE, 1 fs) from the same input files for 40 steps, and the energies they 
 energy of the stock build sits about 1.5e-4 from the FP64 value (its B-spline moduli and energy
 sums are FP32; the reference's own energies meet the FP64 oracle only to 1e-4 in
 tests/test_golden.py), while the drop-in's match FP64 to 1e-5. The drop-in with the pruned pair
-list (neighbor_list_prune_buffer 0.5, prune_interval 5) prints the same energies as without it.
+list (neighbor_list_prune_buffer 0.5, prune_interval 5) prints the same energies as without it,
+and so do both builds with the LJ parameters read from an AMBER parm7 topology (amber_parm7)
+instead of LJ_in_file.
 Skipped where the two binaries have not been built.
 """
 
@@ -29,7 +31,7 @@ B200 = os.path.join(ROOT, "oracle", "_ref", "sponge_b200")
 
 
 def _mdin(paths, outdir, extra=""):
-    return """water box, drop-in parity run
+    text = """water box, drop-in parity run
 mode = NVE
 dt = 1e-3
 step_limit = 40
@@ -58,6 +60,26 @@ dont_check_input = 1
 device = 0
 {extra}
 """.format(out=outdir, extra=extra, **paths)
+    if paths.get("LJ") is None:  # LJ from amber_parm7 (in `extra`) instead of LJ_in_file
+        text = "\n".join(l for l in text.split("\n") if not l.startswith("LJ_in_file"))
+    if "mode =" in extra:  # another mode replaces the NVE default
+        text = "\n".join(l for l in text.split("\n") if l != "mode = NVE")
+    return text
+
+
+# NPT with the Berendsen barostat every 2 steps (deterministic, so the two builds see the same
+# box moves up to the rounding of their pressures): every move calls Main_Volume_Change
+# (main.cu:438-448), that is NEIGHBOR_LIST::Update_Volume, LENNARD_JONES_INFORMATION::Update_Volume
+# and Particle_Mesh_Ewald::Update_Volume on the drop-ins, and the pressure reads their virial.
+NPT = """mode = NPT
+thermostat = berendsen_thermostat
+berendsen_thermostat_tau = 0.1
+target_temperature = 300
+barostat = berendsen_barostat
+target_pressure = 1.0
+berendsen_barostat_tau = 0.1
+berendsen_barostat_compressibility = 4.5e-5
+berendsen_barostat_update_interval = 2"""
 
 
 def _run(binary, paths, outdir, extra=""):
@@ -84,11 +106,17 @@ def runs(tmp_path_factory):
         pytest.skip("no CUDA device")
     base = tmp_path_factory.mktemp("dropin_md")
     paths = sponge_io.write_inputs(systems.config0(), str(base / "inputs"), prefix="water")
+    parm7 = sponge_io.write_amber_parm7(str(base / "inputs" / "water.parm7"), systems.config0())
+    no_lj = dict(paths, LJ=None)
     out = {
         "stock": _run(STOCK, paths, str(base / "stock")),
         "b200": _run(B200, paths, str(base / "b200")),
         "b200_pruned": _run(B200, paths, str(base / "b200_pruned"),
                             "neighbor_list_prune_buffer = 0.5\nneighbor_list_prune_interval = 5"),
+        "stock_parm7": _run(STOCK, no_lj, str(base / "stock_parm7"), "amber_parm7 = " + parm7),
+        "b200_parm7": _run(B200, no_lj, str(base / "b200_parm7"), "amber_parm7 = " + parm7),
+        "stock_npt": _run(STOCK, paths, str(base / "stock_npt"), NPT),
+        "b200_npt": _run(B200, paths, str(base / "b200_npt"), NPT),
     }
     return out
 
@@ -108,3 +136,33 @@ def test_pruned_list_in_driver(runs):
     b, p = runs["b200"], runs["b200_pruned"]
     for key in ("potential", "LJ", "PME", "bond", "temperature"):
         assert np.allclose(b[key], p[key], rtol=1e-5, atol=0.02), key
+
+
+def test_lj_from_amber_parm7(runs):
+    """LENNARD_JONES_INFORMATION::Initial_From_AMBER_Parm: with the LJ tables and types read from
+    an AMBER parm7 topology instead of LJ_in_file, the drop-in prints the energies of its
+    LJ_in_file run, and the stock build does the same with its own reader."""
+    for a, b in ((runs["b200"], runs["b200_parm7"]), (runs["stock"], runs["stock_parm7"])):
+        assert list(a["step"]) == list(b["step"])
+        for key in ("potential", "LJ", "PME", "bond", "temperature"):
+            assert np.allclose(a[key], b[key], rtol=1e-5, atol=0.02), key
+    a, b = runs["stock_parm7"], runs["b200_parm7"]
+    for key in ("potential", "LJ", "PME", "bond"):
+        scale = np.abs(a[key]).max()
+        assert np.abs(a[key] - b[key]).max() <= 2e-4 * scale + 0.05, key
+
+
+def test_npt_box_moves_in_driver(runs):
+    """Berendsen NPT: the box changes every 2 steps through the modules' Update_Volume; the
+    drop-in prints the stock build's density, pressure and energies (the pressure within the
+    rounding of the stock build's FP32 PME energy, about 1.5e-4 of the Coulomb virial)."""
+    a, b = runs["stock_npt"], runs["b200_npt"]
+    assert list(a["step"]) == list(b["step"])
+    assert "density" in a and "pressure" in a
+    assert np.ptp(a["density"]) > 0  # the box did move
+    assert np.allclose(a["density"], b["density"], rtol=2e-5, atol=0)
+    assert np.allclose(a["pressure"], b["pressure"], rtol=1e-3, atol=10.0)
+    for key in ("potential", "LJ", "PME", "bond"):
+        scale = np.abs(a[key]).max()
+        assert np.abs(a[key] - b[key]).max() <= 2e-4 * scale + 0.05, key
+    assert np.allclose(a["temperature"], b["temperature"], rtol=1e-3, atol=0.05)
