@@ -7,7 +7,8 @@ steps), fixed-point coordinates, LJ + PME direct, the long-range correction, the
 correction, PME reciprocal space, then the leap-frog and SETTLE of the rigid waters, for 96,000
 atoms (31,000 rigid waters + 3,000 solute atoms, 98.6 A box, rc 10 A, skin 2 A, PME 96^3) on
 moving coordinates (Maxwell-Boltzmann velocities at 300 K after a steepest-descent relaxation
-of the free solute atoms). ns/day = steps/s * 2 fs * 86400 / 1e6.
+of the free solute atoms, then 300 equilibration steps with velocity rescaling).
+ns/day = steps/s * 2 fs * 86400 / 1e6.
 
   value   device time per MD step (CUDA events on the launching stream), state resident in HBM,
           L2 flushed (256 MiB write) before every timed step
@@ -162,7 +163,40 @@ def run_reference(args, rank, world):
                                    "(cell list + LJ/Ewald direct + exclusions + SPME 96^3)"},
         "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    rc = reference_cuda(s, uc, args.steps)
+    if rc is not None:
+        line["reference_cuda"] = rc
     print(json.dumps(line), flush=True)
+
+
+def reference_cuda(s, uc, steps):
+    """The reference's own CUDA modules (NEIGHBOR_LIST, LENNARD_JONES_INFORMATION,
+    Particle_Mesh_Ewald as shipped, built for sm_100a from the reference's sources into
+    oracle/_ref by oracle/ref_harness) on the same system and GPU: CUDA-event time of a force step
+    (list update every 20 steps + LJ/PME direct + long-range correction + exclusion correction +
+    PME reciprocal) on frozen coordinates, as oracle/ref_harness/harness.cu times it. None where
+    the harness binary or a GPU is absent."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except ImportError:
+        return None
+    import oracle
+    from oracle.ref_harness import run as refrun
+    if not refrun.available():
+        return None
+    keys = oracle.pairs(uc, s, "cells")
+    r = refrun.run(s, uc, keys, timing_steps=max(20, steps))
+    ms_step = float(r["summary"]["ms_step"])
+    ms_force = float(r["summary"]["ms_force_only"])
+    return {"kind": "the reference's CUDA modules, built for sm_100a from its sources",
+            "ms_per_step": ms_step, "ns_per_day": ns_per_day(ms_step * 1e-3),
+            "ms_per_force_evaluation": ms_force,
+            "what": "list update every 20 steps + LJ/PME direct + long-range correction + "
+                    "exclusion correction + PME reciprocal on frozen coordinates (compare with "
+                    "the force_only field of the chosen form's line)",
+            "timing_steps": max(20, steps)}
 
 
 METRIC = "ns/day, 96k-atom PME water, 1 B200 (nonbonded path, fixed-point form)"
@@ -388,13 +422,14 @@ def run_modules(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
-def setup_md(eng, s, seed, relax_iters=300, temperature=300.0):
+def setup_md(eng, s, seed, relax_iters=300, temperature=300.0, equil_steps=300):
     """Untimed MD set-up on the device. The seeded generators place the free (unconstrained)
     solute atoms by random sequential addition at >= 2.2 A, which leaves LJ overlaps of several
     thousand kcal/mol/A: those atoms are first relaxed by steepest descent (every free atom moves
     along its force by at most 0.02 A per iteration, the waters stay as built), then velocities
     are drawn from the Maxwell-Boltzmann distribution at ``temperature`` (seeded), with the
-    centre-of-mass momentum removed. Returns the buffers of the NVE leap-frog + SETTLE step."""
+    centre-of-mass momentum removed, and the system is equilibrated by `equil_steps` MD steps with
+    velocity rescaling. Returns the buffers of the NVE leap-frog + SETTLE step."""
     import torch
     from sponge_b200 import TIME_CONVERSION, Settle, constrain_pairs_from_bonds, sponge_io
     ba, bb, br, mass = sponge_io.bonds_and_masses(s)
@@ -418,14 +453,24 @@ def setup_md(eng, s, seed, relax_iters=300, temperature=300.0):
     settle = Settle(n, pi, pj, pr, mass, dt)
     m64 = mass.astype(np.float64)
     inv = np.divide(1.0, m64, out=np.zeros_like(m64), where=m64 != 0)
-    rng = np.random.default_rng(seed)
-    kT = 0.0019872041 * temperature  # kcal/mol
-    vel = rng.normal(size=(n, 3)) * np.sqrt(kT * inv)[:, None]
-    vel -= (m64[:, None] * vel).sum(0) / m64.sum()
+    vel = sponge_io.maxwell_boltzmann(m64, temperature, seed)
     inv_t = torch.tensor(inv.astype(np.float32), device="cuda")
     mass_t = torch.tensor(mass.astype(np.float32), device="cuda")
     vel_t = torch.tensor(vel.astype(np.float32), device="cuda")
     acc_t = torch.zeros_like(vel_t)
+    eng.update_list(forced=1)
+    # equilibration: the generated waters start with random orientations, so their first steps
+    # carry the excess energy of close contacts; `equil_steps` NVE steps with the velocities
+    # rescaled to `temperature` every 10 steps (a Berendsen thermostat with tau = dt) bring the
+    # system to the motion of an equilibrated run before anything is timed
+    ke_target = 0.5 * (3 * n - 3 * len(pi)) * 0.0019872041 * temperature  # rigid constraints
+    for k in range(equil_steps):
+        eng.update_list()
+        eng.md_step(settle, inv_t, mass_t, vel_t, acc_t)
+        if k % 10 == 9:
+            ke = 0.5 * float((mass_t[:, None] * vel_t * vel_t).double().sum())
+            if ke > 0:
+                vel_t.mul_(float(np.sqrt(ke_target / ke)))
     eng.update_list(forced=1)
     return settle, inv_t, mass_t, vel_t, acc_t
 
@@ -558,7 +603,9 @@ def run_md(args, rank, world, local):
     clocks = ClockSampler(local)
     clocks.start()
     t_wall = time.perf_counter()
-    dev = timed_steps(eng.md_step_graph, args.steps, flush, stream, dist)
+    # the NVTX range marks the timed MD steps for a profiler's launch list (no cost without one)
+    with torch.cuda.nvtx.range("md_steps"):
+        dev = timed_steps(eng.md_step_graph, args.steps, flush, stream, dist)
     t_wall = time.perf_counter() - t_wall
 
     # e2e through the public API with host buffers: every step the caller's coordinates are
@@ -624,7 +671,8 @@ def run_md(args, rank, world, local):
         "dtype": "f32 pair math, int64 fixed-point accumulation, f64 energies" if form == FORM_FIXED
                  else "f32 float atomics",
         "data": "synthetic (seeded generator, sponge_b200.systems.%s; free solute atoms relaxed "
-                "by steepest descent, Maxwell-Boltzmann velocities at 300 K)"
+                "by steepest descent, Maxwell-Boltzmann velocities at 300 K, 300 equilibration "
+                "steps with velocity rescaling)"
                 % ("config2" if big else "config1"),
         "config": dict(cfg, form=args.form, pair_kernel_shape=pair_shape),
         "e2e": {"value": world * ns_per_day(e2e_ms * 1e-3), "unit": "ns/day",

@@ -172,16 +172,6 @@ SB_API int sb_lj_update_volume(sb_lennard_jones* lj, const float box_length[3]);
  * Results are identical to FP32 rounding whichever shape runs. */
 SB_API int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane);
 
-/* Schedule of the packed pair kernel (atoms_per_lane 2; no counterpart in the reference, whose
- * LJ kernel has one fixed launch shape). warps_per_block 0 (the default) launches one one-warp
- * block per 8-atom cluster. Otherwise a persistent grid of blocks_per_sm blocks of
- * warps_per_block warps per SM runs, each warp taking clusters_per_grab consecutive clusters at
- * a time from a launch-wide counter of the module until none are left. The forces are the same
- * bits either way. With a persistent schedule, launches of one module must not overlap in time
- * (they share the counter). */
-SB_API int sb_lj_set_pair_schedule(sb_lennard_jones* lj, int warps_per_block, int blocks_per_sm,
-                                   int clusters_per_grab);
-
 /* Autotuner: times each pair-kernel shape on the current list and keeps the fastest; writes the
  * choice to *h_chosen. Synchronises the stream; leaves d_frc untouched. The shapes sum in
  * different orders, so a process that needs the same bits as another sets the shape explicitly
@@ -276,6 +266,12 @@ SB_API int sb_pme_get_energy_noalloc(sb_pme* pme, sb_neighbor_list* nl,
                       const int* d_excluded_list_start, const int* d_excluded_list,
                       const int* d_excluded_numbers, int which_part, float* h_energy,
                       double* h_parts, void* stream);
+
+/* The member PME_BC of Particle_Mesh_Ewald (PME_force.cu:253-286), which TI_CORE reads: the
+ * device address of the module's Green's-function table (B-spline moduli included, built in
+ * FP64), float [fftx][ffty][fftz/2+1] in the layout of a real-to-complex transform's half
+ * spectrum, element [0] = 0. Owned by the module; sb_pme_update_box rewrites it in place. */
+SB_API int sb_pme_bc_table(sb_pme* pme, const float** d_bc);
 
 /* Particle_Mesh_Ewald::Update_Box_Length / Update_Volume (PME_force.cu:996-1042) */
 SB_API int sb_pme_update_box(sb_pme* pme, const float box_length[3]);

@@ -1,9 +1,12 @@
 #!/bin/bash
-# Builds the unchanged SPONGE MD driver (SPONGE/main.cu and every module it links, per the
-# reference's Makefile object list) twice, into oracle/_ref/ (git-ignored, travels to the GPU box):
-#   sponge_stock   the reference exactly as shipped (target sm_100a, -include cfloat)
-#   sponge_b200    the same driver with neighbor_list/, Lennard_Jones_force.cu/.cuh and
-#                  PME_force/ replaced by sponge_b200/dropin and linked to libsponge_b200.so
+# Builds the unchanged SPONGE drivers (SPONGE/main.cu, main_fep.cu and main_ti.cu with every
+# module they link, per the reference's Makefile object lists) twice, into oracle/_ref/
+# (git-ignored, travels to the GPU box):
+#   sponge_stock, sponge_fep_stock, sponge_ti_stock   the reference exactly as shipped (target
+#                  sm_100a, -include cfloat)
+#   sponge_b200, sponge_fep_b200, sponge_ti_b200      the same drivers with neighbor_list/,
+#                  Lennard_Jones_force.cu/.cuh and PME_force/ replaced by sponge_b200/dropin and
+#                  linked to libsponge_b200.so
 # Sources are compiled where they lie through a shadow tree of symlinks; nothing is copied.
 # usage: oracle/ref_harness/build_sponge.sh [stock|b200|both]   (needs the reference tree)
 set -e
@@ -22,6 +25,12 @@ thermostats/Berendsen_thermostat thermostats/nose_hoover_chain barostats/MC_baro
 barostats/Berendsen_barostat barostats/andersen_barostat restrain/restrain constrain/constrain
 constrain/simple_constrain constrain/SETTLE constrain/SHAKE virtual_atoms/virtual_atoms
 crd_molecular_map/crd_molecular_map"
+FEP_OBJS="main_fep common control FEP_core/FEP_core bond/bond bond/bond_soft angle/angle
+dihedral/dihedral nb14/nb14 neighbor_list/neighbor_list Lennard_Jones_force/LJ_soft_core
+PME_force/PME_force"
+TI_OBJS="main_ti common control TI_core/TI_core bond/bond bond/bond_soft angle/angle
+dihedral/dihedral nb14/nb14 neighbor_list/neighbor_list Lennard_Jones_force/LJ_soft_core
+PME_force/PME_force"
 
 shadow() {  # $1 = variant dir
     local S=$1
@@ -48,12 +57,20 @@ build_variant() {  # $1 = stock|b200
         LINK="-L$REPO/sponge_b200 -lsponge_b200 -Xlinker -rpath=$REPO/sponge_b200 -Xlinker -rpath=\$ORIGIN/../../sponge_b200"
     fi
     mkdir -p "$S/obj"
-    echo $OBJS | tr ' ' '\n' | xargs -P "$JOBS" -I{} sh -c \
+    echo $OBJS $FEP_OBJS $TI_OBJS | tr ' ' '\n' | sort -u | xargs -P "$JOBS" -I{} sh -c \
         "mkdir -p \$(dirname '$S/obj/{}.o') && $NVCC $FLAGS -I$REPO/include -c '$S/{}.cu' -o '$S/obj/{}.o'"
     local OL=""
     for o in $OBJS; do OL="$OL $S/obj/$o.o"; done
     $NVCC -arch=sm_100a -rdc=true -o "$OUT/sponge_$V" $OL -lcufft -lcudadevrt $LINK
     echo "built $OUT/sponge_$V"
+    OL=""
+    for o in $FEP_OBJS; do OL="$OL $S/obj/$o.o"; done
+    $NVCC -arch=sm_100a -rdc=true -o "$OUT/sponge_fep_$V" $OL -lcufft -lcudadevrt $LINK
+    echo "built $OUT/sponge_fep_$V"
+    OL=""
+    for o in $TI_OBJS; do OL="$OL $S/obj/$o.o"; done
+    $NVCC -arch=sm_100a -rdc=true -o "$OUT/sponge_ti_$V" $OL -lcufft -lcudadevrt $LINK
+    echo "built $OUT/sponge_ti_$V"
 }
 
 mkdir -p "$OUT"

@@ -61,7 +61,6 @@ _SIGS = {
     "sb_lj_update_volume": [_vp, _vp],
     "sb_lj_long_range_factor": [_vp, _vp],
     "sb_lj_set_kernel_variant": [_vp, _i],
-    "sb_lj_set_pair_schedule": [_vp, _i, _i, _i],
     "sb_lj_tune": [_vp, _vp, _vp, _vp, _f, _vp, _vp],
     "sb_pme_create": [_i, _vp, _f, _f, _i, _i, _i, _i, _vp],
     "sb_pme_destroy": [_vp],
@@ -74,6 +73,7 @@ _SIGS = {
     "sb_pme_get_energy": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp],
     "sb_pme_get_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp],
     "sb_pme_update_box": [_vp, _vp],
+    "sb_pme_bc_table": [_vp, _vp],
     "sb_nonbonded_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp,
                           _vp, _vp, _vp],
     "sb_crd_to_uint_crd": [_i, _vp, _vp, _vp, _vp],
@@ -323,13 +323,6 @@ class LennardJones:
         FP32x2 slot pairs (the default), or 1 for the compacted kernel (one in-cutoff pair per
         lane); a tuning knob with the same results to FP32 rounding."""
         _check(lib().sb_lj_set_kernel_variant(self.handle, int(atoms_per_lane)))
-
-    def set_pair_schedule(self, warps_per_block=0, blocks_per_sm=3, clusters_per_grab=1):
-        """Schedule of the packed pair kernel: 0 warps per block = one one-warp block per
-        cluster (the default); otherwise a persistent grid whose warps take
-        ``clusters_per_grab`` clusters at a time from a counter. Same forces either way."""
-        _check(lib().sb_lj_set_pair_schedule(self.handle, int(warps_per_block),
-                                             int(blocks_per_sm), int(clusters_per_grab)))
 
     def tune(self, nl, uint_crd, charge, pme_beta, stream=None):
         """Time each pair-kernel shape on the current list and keep the fastest."""

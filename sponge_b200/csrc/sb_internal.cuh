@@ -194,12 +194,6 @@ struct sb_lennard_jones {
     float* d_energy_atom = nullptr; // [N] scratch for Get_Energy
     int ipl = 2;                    // pair kernel shape: 8 or 4 i atoms per lane, 2 = packed
                                     // FP32x2 slot pairs, 1 = compacted in-cutoff pairs
-    // schedule of the packed kernel: 0 warps = one one-warp block per cluster; else a
-    // persistent grid of `sched_bps` blocks per SM of `sched_warps` warps taking `sched_chunk`
-    // clusters per grab from the counters d_work[2]
-    int sched_warps = 0, sched_bps = 3, sched_chunk = 1;
-    int* d_work = nullptr;
-    int num_sms = 148;
 };
 
 struct sb_pme {

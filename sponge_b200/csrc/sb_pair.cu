@@ -239,18 +239,9 @@ extern "C" int sb_lj_create(int atom_numbers, int atom_type_numbers, const float
         (st = sb_malloc((void**)&lj->d_AB, sizeof(float2) * nt * nt, "LJ_AB")) ||
         (st = sb_malloc((void**)&lj->d_type, sizeof(int) * atom_numbers, "LJ type")) ||
         (st = sb_malloc((void**)&lj->d_red, sizeof(double) * 8, "LJ reduce")) ||
-        (st = sb_malloc((void**)&lj->d_energy_atom, sizeof(float) * atom_numbers, "LJ energy")) ||
-        (st = sb_malloc((void**)&lj->d_work, sizeof(int) * 2, "pair work counters"))) {
+        (st = sb_malloc((void**)&lj->d_energy_atom, sizeof(float) * atom_numbers, "LJ energy"))) {
         sb_lj_destroy(lj);
         return st;
-    }
-    cudaMemset(lj->d_work, 0, sizeof(int) * 2);
-    {
-        int dev = 0, sms = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-            sms > 0)
-            lj->num_sms = sms;
     }
     cudaMemcpy(lj->d_A, h_A, sizeof(float) * np, cudaMemcpyHostToDevice);
     cudaMemcpy(lj->d_B, h_B, sizeof(float) * np, cudaMemcpyHostToDevice);
@@ -274,7 +265,6 @@ extern "C" int sb_lj_destroy(sb_lennard_jones* lj) {
     sb_free(lj->d_type);
     sb_free(lj->d_red);
     sb_free(lj->d_energy_atom);
-    sb_free(lj->d_work);
     delete lj;
     return SB_OK;
 }
@@ -340,20 +330,9 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
     } while (0)
 #define SB_LAUNCH_X2(EVV)                                                                     \
     do {                                                                                      \
-        if (lj->sched_warps > 0) {                                                            \
-            const size_t sm_dyn = sizeof(float4) * 4 * lj->ntypes * lj->sched_warps;          \
-            if (sm_dyn > 48 * 1024)                                                           \
-                cudaFuncSetAttribute(k_pair_x2_dyn<EVV>,                                      \
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dyn); \
-            k_pair_x2_dyn<EVV><<<lj->num_sms * lj->sched_bps, 32 * lj->sched_warps, sm_dyn,   \
-                                 s>>>(P, lj->d_work, lj->sched_chunk, nl->meta, nl->cl_count, \
-                                      nl->cl_ent, nl->xq, nl->stype, lj->d_AB,                \
-                                      nl->slot_atom, nl->fix, ae, av, ad);                    \
-        } else {                                                                              \
-            k_pair_x2<EVV><<<x2_blocks, 32, sizeof(float4) * 4 * lj->ntypes, s>>>(            \
-                P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,           \
-                nl->slot_atom, nl->fix, ae, av, ad);                                          \
-        }                                                                                     \
+        k_pair_x2<EVV><<<x2_blocks, 32, sizeof(float4) * 4 * lj->ntypes, s>>>(                \
+            P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
+            nl->slot_atom, nl->fix, ae, av, ad);                                              \
     } while (0)
     // packed kernel: one block per cluster (a grid of fewer blocks looping over the clusters
     // ran slower)
@@ -562,27 +541,6 @@ extern "C" int sb_lj_set_kernel_variant(sb_lennard_jones* lj, int atoms_per_lane
         return SB_ERR_ARG;
     }
     lj->ipl = atoms_per_lane;
-    return SB_OK;
-}
-
-extern "C" int sb_lj_set_pair_schedule(sb_lennard_jones* lj, int warps_per_block,
-                                       int blocks_per_sm, int clusters_per_grab) {
-    if (!lj || warps_per_block < 0 || warps_per_block > 8 ||
-        (warps_per_block > 0 && (blocks_per_sm < 1 || clusters_per_grab < 1 ||
-                                 blocks_per_sm * warps_per_block > 32))) {
-        sb_set_error("sb_lj_set_pair_schedule: warps_per_block in [0, 8], blocks_per_sm >= 1 "
-                     "with at most 32 warps per SM, clusters_per_grab >= 1");
-        return SB_ERR_ARG;
-    }
-    if (warps_per_block > 0 && 4 * (size_t)lj->ntypes * warps_per_block * sizeof(float4) >
-                                   200 * 1024) {
-        sb_set_error("sb_lj_set_pair_schedule: %d LJ types x %d warps exceed shared memory",
-                     lj->ntypes, warps_per_block);
-        return SB_ERR_ARG;
-    }
-    lj->sched_warps = warps_per_block;
-    lj->sched_bps = blocks_per_sm;
-    lj->sched_chunk = clusters_per_grab;
     return SB_OK;
 }
 

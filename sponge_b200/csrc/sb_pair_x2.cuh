@@ -378,43 +378,3 @@ __global__ void __launch_bounds__(32, EV ? 12 : 24) k_pair_x2(
     }
 }
 
-// Persistent form of the same kernel: a grid of a few blocks per SM, W warps each; every warp
-// takes `chunk` consecutive clusters at a time from a launch-wide counter (one atomic by lane 0
-// per grab) until the clusters run out, so that no SM idles at the tail of the launch and no
-// block launch is paid per cluster; consecutive clusters of one grab share most of their j
-// atoms in L1. The last warp to run out re-arms the counters for the next launch (work[0] the
-// next cluster, work[1] the warps done). The forces are the bits of k_pair_x2: the fixed-point
-// sums do not depend on which warp takes which cluster.
-template <int EV>
-__global__ void __launch_bounds__(256, EV ? 2 : 3) k_pair_x2_dyn(
-    PairParams P, int* __restrict__ work, int chunk, const int* __restrict__ meta,
-    const int* __restrict__ cl_count, const uint32_t* __restrict__ cl_ent,
-    const uint4* __restrict__ xq, const int* __restrict__ stype, const float2* __restrict__ AB,
-    const int* __restrict__ slot_atom, long long* __restrict__ fix,
-    float* __restrict__ atom_energy, float* __restrict__ atom_virial,
-    float* __restrict__ atom_direct) {
-    extern __shared__ float4 ctab_all[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float4* ctab = ctab_all + (size_t)wid * 4 * P.nt;
-    const int ncl = meta[0];
-    for (;;) {
-        int c0 = 0;
-        if (lane == 0) c0 = atomicAdd(&work[0], chunk);
-        c0 = __shfl_sync(0xffffffffu, c0, 0);
-        if (c0 >= ncl) break;
-        const int c1 = min(c0 + chunk, ncl);
-        for (int c = c0; c < c1; c++) {
-            x2_cluster<EV>(P, c, lane, ctab, cl_count, cl_ent, xq, stype, AB, slot_atom, fix,
-                           atom_energy, atom_virial, atom_direct);
-            __syncwarp();  // the next cluster rewrites the LJ table
-        }
-    }
-    if (lane == 0) {
-        const int warps = gridDim.x * (blockDim.x >> 5);
-        if (atomicAdd(&work[1], 1) == warps - 1) {
-            // every warp of this launch has taken its last grab
-            work[0] = 0;
-            work[1] = 0;
-        }
-    }
-}

@@ -627,6 +627,15 @@ extern "C" int sb_pme_reciprocal_force(sb_pme* p, const uint32_t* d_uint_crd,
     return SB_OK;
 }
 
+extern "C" int sb_pme_bc_table(sb_pme* p, const float** d_bc) {
+    if (!p || !d_bc) {
+        sb_set_error("sb_pme_bc_table: null argument");
+        return SB_ERR_ARG;
+    }
+    *d_bc = p->d_bc;
+    return SB_OK;
+}
+
 extern "C" int sb_pme_update_box(sb_pme* p, const float box_length[3]) {
     if (!p || !box_length) {
         sb_set_error("sb_pme_update_box: null argument");

@@ -4,6 +4,176 @@
 #include "../neighbor_list/neighbor_list.cuh"
 #include "sponge_b200.h"
 
+// ---------------------------------------------------------------------------------------------
+// The reference-layout PME internals for TI_CORE (see PME_force.cuh). The kernels keep the
+// reference header's contracts: a grid coordinate u = uint * K / 2^32 in FP32, base = (int)u,
+// fraction u - base; the 64 stencil points (base - k) mod K of the 4th-order B-spline; charge
+// spread with float atomics; the half spectrum times the Green's function table; a dot product
+// summed by one block.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float ti_bspline4(int k, float f)
+{
+    // weight of stencil offset k (0..3) at fraction f: the cardinal cubic B-spline pieces
+    const float f2 = f * f, f3 = f2 * f;
+    switch (k)
+    {
+    case 0: return f3 * (1.0f / 6.0f);
+    case 1: return -0.5f * f3 + 0.5f * f2 + 0.5f * f + (1.0f / 6.0f);
+    case 2: return 0.5f * f3 - f2 + (2.0f / 3.0f);
+    default: return -f3 * (1.0f / 6.0f) + 0.5f * f2 - 0.5f * f + (1.0f / 6.0f);
+    }
+}
+
+__global__ void PME_Atom_Near(const UNSIGNED_INT_VECTOR *uint_crd, int **PME_atom_near, const int PME_Nin,
+    const float periodic_factor_inverse_x, const float periodic_factor_inverse_y, const float periodic_factor_inverse_z,
+    const int atom_numbers, const int fftx, const int ffty, const int fftz,
+    const UNSIGNED_INT_VECTOR *PME_kxyz, UNSIGNED_INT_VECTOR *PME_uxyz, VECTOR *PME_frxyz)
+{
+    const int i = blockDim.x * blockIdx.x + threadIdx.x;
+    if (i >= atom_numbers)
+        return;
+    const float ux = (float)uint_crd[i].uint_x * periodic_factor_inverse_x;
+    const float uy = (float)uint_crd[i].uint_y * periodic_factor_inverse_y;
+    const float uz = (float)uint_crd[i].uint_z * periodic_factor_inverse_z;
+    const int bx = (int)ux, by = (int)uy, bz = (int)uz;
+    PME_frxyz[i].x = ux - bx;
+    PME_frxyz[i].y = uy - by;
+    PME_frxyz[i].z = uz - bz;
+    UNSIGNED_INT_VECTOR last = PME_uxyz[i];
+    if ((int)last.uint_x == bx && (int)last.uint_y == by && (int)last.uint_z == bz)
+        return;  // same base cell as the last call: the stencil indices stand
+    PME_uxyz[i].uint_x = bx;
+    PME_uxyz[i].uint_y = by;
+    PME_uxyz[i].uint_z = bz;
+    int *near = PME_atom_near[i];
+    for (int k = 0; k < 64; k++)
+    {
+        const UNSIGNED_INT_VECTOR o = PME_kxyz[k];
+        int gx = bx - (int)o.uint_x, gy = by - (int)o.uint_y, gz = bz - (int)o.uint_z;
+        gx += gx < 0 ? fftx : (gx >= fftx ? -fftx : 0);
+        gy += gy < 0 ? ffty : (gy >= ffty ? -ffty : 0);
+        gz += gz < 0 ? fftz : (gz >= fftz ? -fftz : 0);
+        near[k] = gx * PME_Nin + gy * fftz + gz;
+    }
+}
+
+__global__ void PME_Q_Spread(int **PME_atom_near, const float *charge, const VECTOR *PME_frxyz,
+    float *PME_Q, const UNSIGNED_INT_VECTOR *PME_kxyz, const int atom_numbers)
+{
+    const int i = blockDim.x * blockIdx.x + threadIdx.x;
+    if (i >= atom_numbers)
+        return;
+    const int *near = PME_atom_near[i];
+    const VECTOR f = PME_frxyz[i];
+    const float q = charge[i];
+    for (int k = threadIdx.y; k < 64; k += blockDim.y)
+    {
+        const UNSIGNED_INT_VECTOR o = PME_kxyz[k];
+        const float w = q * ti_bspline4(o.uint_x, f.x) * ti_bspline4(o.uint_y, f.y) *
+                        ti_bspline4(o.uint_z, f.z);
+        atomicAdd(&PME_Q[near[k]], w);
+    }
+}
+
+__global__ void PME_BCFQ(cufftComplex *PME_FQ, float *PME_BC, int PME_Nfft)
+{
+    const int i = blockDim.x * blockIdx.x + threadIdx.x;
+    if (i < PME_Nfft)
+    {
+        const float b = PME_BC[i];
+        PME_FQ[i].x *= b;
+        PME_FQ[i].y *= b;
+    }
+}
+
+__global__ void PME_Energy_Product(const int element_number, const float *list1, const float *list2, float *sum)
+{
+    // one block: a strided partial per thread, a warp-shuffle and shared-memory tree, one store
+    __shared__ float part[32];
+    float v = 0.f;
+    for (int i = threadIdx.x; i < element_number; i += blockDim.x)
+        v += list1[i] * list2[i];
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0)
+        part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        v = threadIdx.x < (blockDim.x + 31) / 32 ? part[threadIdx.x] : 0.f;
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0)
+            sum[0] = v;
+    }
+}
+
+__global__ static void ti_fill_kxyz(UNSIGNED_INT_VECTOR *kxyz, UNSIGNED_INT_VECTOR *uxyz, int n,
+                                    int **near, int *block)
+{
+    const int i = blockDim.x * blockIdx.x + threadIdx.x;
+    if (i < 64)
+    {
+        kxyz[i].uint_x = i >> 4;
+        kxyz[i].uint_y = (i >> 2) & 3;
+        kxyz[i].uint_z = i & 3;
+    }
+    if (i < n)
+    {
+        // no base cell yet: the first PME_Atom_Near computes every stencil
+        uxyz[i].uint_x = uxyz[i].uint_y = uxyz[i].uint_z = 1u << 30;
+        near[i] = block + 64 * (size_t)i;
+    }
+}
+
+void Particle_Mesh_Ewald::Initial_TI_Internals()
+{
+    if (ti_internals)
+        return;
+    Cuda_Malloc_Safely((void **)&PME_kxyz, sizeof(UNSIGNED_INT_VECTOR) * 64);
+    Cuda_Malloc_Safely((void **)&PME_uxyz, sizeof(UNSIGNED_INT_VECTOR) * atom_numbers);
+    Cuda_Malloc_Safely((void **)&PME_frxyz, sizeof(VECTOR) * atom_numbers);
+    Cuda_Malloc_Safely((void **)&PME_Q, sizeof(float) * PME_Nall);
+    Cuda_Malloc_Safely((void **)&PME_FBCFQ, sizeof(float) * PME_Nall);
+    Cuda_Malloc_Safely((void **)&PME_FQ, sizeof(cufftComplex) * PME_Nfft);
+    Cuda_Malloc_Safely((void **)&PME_atom_near, sizeof(int *) * atom_numbers);
+    Cuda_Malloc_Safely((void **)&PME_atom_near_block, sizeof(int) * 64 * (size_t)atom_numbers);
+    Cuda_Malloc_Safely((void **)&charge_sum, sizeof(float));
+    const int n = atom_numbers > 64 ? atom_numbers : 64;
+    ti_fill_kxyz<<<(n + 255) / 256, 256>>>(PME_kxyz, PME_uxyz, atom_numbers, PME_atom_near,
+                                           PME_atom_near_block);
+    if (cufftPlan3d(&PME_plan_r2c, fftx, ffty, fftz, CUFFT_R2C) != CUFFT_SUCCESS ||
+        cufftPlan3d(&PME_plan_c2r, fftx, ffty, fftz, CUFFT_C2R) != CUFFT_SUCCESS)
+    {
+        fprintf(stderr, "sponge_b200: cuFFT plans of the TI internals could not be created\n");
+        exit(1);
+    }
+    const float *bc = NULL;
+    Sponge_B200_Check(sb_pme_bc_table(handle, &bc), "Particle_Mesh_Ewald::Initial_TI_Internals");
+    PME_BC = (float *)bc;
+    ti_internals = 1;
+}
+
+void Particle_Mesh_Ewald::Clear_TI_Internals()
+{
+    if (!ti_internals)
+        return;
+    cufftDestroy(PME_plan_r2c);
+    cufftDestroy(PME_plan_c2r);
+    void *ps[] = {PME_kxyz, PME_uxyz, PME_frxyz, PME_Q, PME_FBCFQ, PME_FQ, PME_atom_near,
+                  PME_atom_near_block, charge_sum};
+    for (void *q : ps)
+        cudaFree(q);
+    PME_kxyz = PME_uxyz = NULL;
+    PME_frxyz = NULL;
+    PME_Q = PME_FBCFQ = charge_sum = NULL;
+    PME_FQ = NULL;
+    PME_atom_near = NULL;
+    PME_atom_near_block = NULL;
+    PME_BC = NULL;
+    ti_internals = 0;
+}
+
 void Particle_Mesh_Ewald::Initial(CONTROLLER *controller, int atom_numbers, VECTOR boxlength, float cutoff, const char *module_name)
 {
     if (module_name == NULL)
@@ -49,6 +219,8 @@ void Particle_Mesh_Ewald::Initial(CONTROLLER *controller, int atom_numbers, VECT
     cudaMemset(d_direct_ene, 0, sizeof(float));
     controller[0].printf("    fftx: %d\n    ffty: %d\n    fftz: %d\n    beta: %f\n", fftx, ffty, fftz, beta);
     is_initialized = 1;
+    if (controller[0].Command_Exist("charge_pertubated") && atoi(controller[0].Command("charge_pertubated")) != 0)
+        Initial_TI_Internals();
     if (!is_controller_printf_initialized)
     {
         controller[0].Step_Print_Initial(this->module_name, "%.2f");
@@ -62,6 +234,7 @@ void Particle_Mesh_Ewald::Clear()
 {
     if (is_initialized)
     {
+        Clear_TI_Internals();
         is_initialized = 0;
         sb_pme_destroy(handle);
         handle = NULL;

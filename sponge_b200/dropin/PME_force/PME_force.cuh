@@ -1,11 +1,19 @@
 // Drop-in replacement for SPONGE's Particle_Mesh_Ewald (SPONGE/PME_force/PME_force.cuh:25-123):
 // same struct, the public members the MD driver reads (beta, fft sizes, d_direct_atom_energy,
 // d_correction_atom_energy, energy parts) and method signatures; spread, FFT, convolution and
-// gather are libsponge_b200's, reached through the C ABI. The cuFFT plans and per-atom stencil
-// arrays of the reference are internal to the library and not exposed; the TI cross terms
-// that TI_CORE derives from them are computed by sb_pme_ti_cross.
+// gather are libsponge_b200's, reached through the C ABI.
+//
+// TI_CORE::Get_Cross_PME_Partial_H_Partial_Lambda (TI_core.cu:670-730) works on the reference's
+// own PME internals: it launches PME_Atom_Near, PME_Q_Spread, PME_BCFQ and PME_Energy_Product on
+// the members PME_atom_near, PME_kxyz, PME_uxyz, PME_frxyz, PME_Q, PME_FQ, PME_FBCFQ, PME_BC and
+// the cuFFT plans. The same members and kernels are declared here (with the reference header's
+// names and signatures, which TI_core.cu compiles against); Initial allocates them only for runs
+// whose mdin perturbs charges (charge_pertubated), PME_BC is the library's FP64-built Green's
+// function table, and the kernels are this drop-in's own (PME_force.cu).
 #ifndef PME_FORCE_CUH
 #define PME_FORCE_CUH
+#include <cufft.h>
+
 #include "../common.cuh"
 #include "../control.cuh"
 
@@ -50,6 +58,22 @@ struct Particle_Mesh_Ewald
 
     sb_pme *handle = NULL;
 
+    // the internals TI_CORE reads (allocated by Initial when the mdin perturbs charges)
+    dim3 thread_PME = {8, 8};
+    cufftHandle PME_plan_r2c = 0;
+    cufftHandle PME_plan_c2r = 0;
+    int ti_internals = 0;
+    float *PME_BC = NULL;  // the library's table, [fftx][ffty][fftz/2+1]
+    UNSIGNED_INT_VECTOR *PME_kxyz = NULL;
+    UNSIGNED_INT_VECTOR *PME_uxyz = NULL;
+    VECTOR *PME_frxyz = NULL;
+    float *PME_Q = NULL;
+    float *PME_FBCFQ = NULL;
+    cufftComplex *PME_FQ = NULL;
+    int **PME_atom_near = NULL;
+    int *PME_atom_near_block = NULL;
+    float *charge_sum = NULL;
+
     enum PME_ENERGY_PART
     {
         TOTAL = 0,
@@ -71,6 +95,18 @@ struct Particle_Mesh_Ewald
         const int *excluded_list_start, const int *excluded_list, const int *excluded_atom_numbers, int which_part = 0, int is_download = 1);
     void Update_Volume(VECTOR boxlength);
     void Update_Box_Length(VECTOR boxlength);
+    void Initial_TI_Internals();
+    void Clear_TI_Internals();
 };
+
+// kernels of the reference header that TI_CORE launches on the members above
+__global__ void PME_Atom_Near(const UNSIGNED_INT_VECTOR *uint_crd, int **PME_atom_near, const int PME_Nin,
+    const float periodic_factor_inverse_x, const float periodic_factor_inverse_y, const float periodic_factor_inverse_z,
+    const int atom_numbers, const int fftx, const int ffty, const int fftz,
+    const UNSIGNED_INT_VECTOR *PME_kxyz, UNSIGNED_INT_VECTOR *PME_uxyz, VECTOR *PME_frxyz);
+__global__ void PME_Q_Spread(int **PME_atom_near, const float *charge, const VECTOR *PME_frxyz,
+    float *PME_Q, const UNSIGNED_INT_VECTOR *PME_kxyz, const int atom_numbers);
+__global__ void PME_Energy_Product(const int element_number, const float *list1, const float *list2, float *sum);
+__global__ void PME_BCFQ(cufftComplex *PME_FQ, float *PME_BC, int PME_Nfft);
 
 #endif

@@ -192,6 +192,139 @@ def read_velocity(path):
     return np.array(" ".join(lines[1:1 + n]).split(), np.float32).reshape(n, 3)
 
 
+def write_velocity(path, vel):
+    """Velocity file as velocity_in_file reads it (MD_core.cu:867-892): "N", then N lines
+    "vx vy vz" in A per internal time unit."""
+    vel = np.asarray(vel, np.float64).reshape(-1, 3)
+    with open(path, "w") as f:
+        f.write("%d\n" % vel.shape[0])
+        np.savetxt(f, vel, fmt="%.7f")
+    return path
+
+
+def maxwell_boltzmann(mass, temperature, seed):
+    """Velocities (A per internal time unit) drawn at ``temperature`` K for ``mass`` (amu),
+    centre-of-mass momentum removed: sqrt(kB T / m) per component, kB in kcal/mol/K."""
+    m = np.asarray(mass, np.float64)
+    inv = np.divide(1.0, m, out=np.zeros_like(m), where=m != 0)
+    rng = np.random.default_rng(seed)
+    vel = rng.normal(size=(m.size, 3)) * np.sqrt(0.0019872041 * temperature * inv)[:, None]
+    vel -= (m[:, None] * vel).sum(0) / m.sum()
+    return vel
+
+
+def append_crd_traj(path, crd):
+    """One frame of the binary coordinate trajectory (`crd`, mdcrd.dat), as
+    Append_Crd_Traj_File writes it (MD_core.cu:1347-1357): N x 3 float32, no header, frames
+    appended one after another. Also the layout of the velocity and force trajectories."""
+    with open(path, "ab") as f:
+        np.ascontiguousarray(crd, np.float32).reshape(-1, 3).tofile(f)
+
+
+def read_crd_traj(path, atom_numbers):
+    """All frames of a binary coordinate (or velocity, force) trajectory: [F, N, 3] float32."""
+    a = np.fromfile(path, np.float32)
+    per = 3 * int(atom_numbers)
+    if a.size % per:
+        raise ValueError("%s: %d floats is not a whole number of %d-atom frames"
+                         % (path, a.size, atom_numbers))
+    return a.reshape(-1, int(atom_numbers), 3)
+
+
+def append_box_traj(path, box):
+    """One line of the box trajectory (`box`, mdbox.txt) as Append_Box_Traj_File writes it
+    (MD_core.cu:1398-1408): "Lx Ly Lz 90 90 90" with %f lengths."""
+    b = np.asarray(box, np.float32).reshape(3)
+    with open(path, "a") as f:
+        f.write("%f %f %f %.0f %.0f %.0f\n" % (b[0], b[1], b[2], 90.0, 90.0, 90.0))
+
+
+def read_box_traj(path):
+    """The box lengths of every frame of a box trajectory: [F, 3] float32."""
+    rows = [l.split() for l in open(path) if l.strip()]
+    return np.array([[float(x) for x in r[:3]] for r in rows], np.float32).reshape(-1, 3)
+
+
+def write_restart(prefix, crd, vel, box, time_ps=0.0):
+    """SPONGE's own restart pair as Export_Restart_File writes it without an AMBER restart
+    (MD_core.cu:1466-1486): "<prefix>_coordinate.txt" ("N time", N lines "%12.7f %12.7f
+    %12.7f", the box line) and "<prefix>_velocity.txt" ("N time", N velocity lines)."""
+    crd = np.asarray(crd, np.float32).reshape(-1, 3)
+    vel = np.asarray(vel, np.float32).reshape(-1, 3)
+    b = np.asarray(box, np.float32).reshape(3)
+    n = crd.shape[0]
+    with open(prefix + "_coordinate.txt", "w") as f:
+        f.write("%d %.3f\n" % (n, time_ps))
+        for x in crd:
+            f.write("%12.7f %12.7f %12.7f\n" % tuple(x))
+        f.write("%12.7f %12.7f %12.7f %12.7f %12.7f %12.7f" % (b[0], b[1], b[2], 90.0, 90.0, 90.0))
+    with open(prefix + "_velocity.txt", "w") as f:
+        f.write("%d %.3f\n" % (n, time_ps))
+        for v in vel:
+            f.write("%12.7f %12.7f %12.7f\n" % tuple(v))
+    return prefix + "_coordinate.txt", prefix + "_velocity.txt"
+
+
+def read_restart(prefix):
+    """The restart pair of `write_restart` (or of a SPONGE run with `rst = <prefix>`):
+    (crd [N,3], vel [N,3], box [3], time in ps)."""
+    crd, box = read_coordinate(prefix + "_coordinate.txt")
+    vel = read_velocity(prefix + "_velocity.txt")
+    with open(prefix + "_coordinate.txt") as f:
+        head = f.readline().split()
+    return crd, vel, box, float(head[1]) if len(head) > 1 else 0.0
+
+
+def write_fep_inputs(system, outdir, frames, prefix="fep"):
+    """Inputs of SPONGE's FEP and TI drivers (main_fep.cu, main_ti.cu) for an FEP box of
+    ``sponge_b200.systems.fep_box`` and a list of coordinate frames (same box each):
+
+    * charge_in_file (the charges at the box's lambda), chargeA_in_file, chargeB_in_file
+      (TI_core.cu:421-470), subsys_division_in_file (the perturbed-atom mask,
+      LJ_soft_core.cu:1549-1575), exclude_in_file;
+    * LJ_soft_core_in_file: "N TA TB", the A state's A and B tables, the B state's, then
+      "typeA typeB" per atom (LJ_soft_core.cu:1491-1547), unscaled;
+    * the binary coordinate trajectory and the box trajectory that the drivers read frame by
+      frame (``crd`` and ``box``).
+    Returns a dict of paths."""
+    os.makedirs(outdir, exist_ok=True)
+    n = len(system["charge"])
+    p = lambda name: os.path.join(outdir, "%s_%s" % (prefix, name))  # noqa: E731
+
+    def values(path, v, fmt):
+        with open(path, "w") as f:
+            f.write("%d\n" % n)
+            np.savetxt(f, np.asarray(v).reshape(-1), fmt=fmt)
+        return path
+
+    out = {
+        "charge": values(p("charge.txt"), np.asarray(system["charge"], np.float64), "%.9g"),
+        "chargeA": values(p("chargeA.txt"), np.asarray(system["charge_A"], np.float64), "%.9g"),
+        "chargeB": values(p("chargeB.txt"), np.asarray(system["charge_B"], np.float64), "%.9g"),
+        "subsys": values(p("subsys.txt"), np.asarray(system["mask"], np.int64), "%d"),
+    }
+    es, en, el = system["excl_start"], system["excl_numbers"], system["excl_list"]
+    out["exclude"] = p("exclude.txt")
+    with open(out["exclude"], "w") as f:
+        f.write("%d %d\n" % (n, len(el)))
+        for i in range(n):
+            f.write(" ".join([str(en[i])] + [str(x) for x in el[es[i]:es[i] + en[i]]]) + "\n")
+    out["lj_soft"] = p("LJ_soft_core.txt")
+    with open(out["lj_soft"], "w") as f:
+        f.write("%d %d %d\n" % (n, int(system["n_types"]), int(system["n_types_B"])))
+        for key in ("lj_A", "lj_B", "lj_A_B", "lj_B_B"):
+            np.savetxt(f, np.asarray(system[key], np.float64), fmt="%.9e")
+        np.savetxt(f, np.stack([system["lj_type"], system["lj_type_B"]], 1), fmt="%d")
+    out["crd"], out["box"] = p("crd.dat"), p("box.txt")
+    for path in (out["crd"], out["box"]):
+        if os.path.exists(path):
+            os.remove(path)
+    for fr in frames:
+        append_crd_traj(out["crd"], fr)
+        append_box_traj(out["box"], system["box"])
+    return out
+
+
 def read_bond(path):
     """Bond file: "count", then "a b k r0" per bond. Returns (a, b, k, r0)."""
     tok = open(path).read().split()

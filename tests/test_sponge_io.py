@@ -60,3 +60,27 @@ def test_round_trip_nb14_and_virtual_atoms(tmp_path):
     rt, ratoms, rp = sponge_io.read_vatom(pv)
     assert np.array_equal(rt, types) and np.array_equal(ratoms, atoms)
     assert np.allclose(rp, params)
+
+
+def test_trajectory_and_restart_round_trip(tmp_path):
+    """The binary coordinate trajectory (float32 frames appended, MD_core.cu:1347-1357), the box
+    trajectory (one "Lx Ly Lz 90 90 90" line per frame, :1398-1408) and SPONGE's own restart
+    pair (:1466-1486): written frames read back, restart values to the 1e-7 of %12.7f."""
+    rng = np.random.default_rng(3)
+    n = 17
+    frames = rng.uniform(0, 30, (3, n, 3)).astype(np.float32)
+    boxes = np.array([[30.0, 30.5, 31.0], [30.1, 30.6, 31.1], [29.9, 30.4, 30.9]], np.float32)
+    traj = os.path.join(str(tmp_path), "mdcrd.dat")
+    boxf = os.path.join(str(tmp_path), "mdbox.txt")
+    for f, b in zip(frames, boxes):
+        sponge_io.append_crd_traj(traj, f)
+        sponge_io.append_box_traj(boxf, b)
+    assert os.path.getsize(traj) == frames.nbytes
+    assert np.array_equal(sponge_io.read_crd_traj(traj, n), frames)
+    assert np.allclose(sponge_io.read_box_traj(boxf), boxes, atol=1e-6)
+    vel = rng.normal(0, 0.5, (n, 3)).astype(np.float32)
+    prefix = os.path.join(str(tmp_path), "restart")
+    sponge_io.write_restart(prefix, frames[2], vel, boxes[2], time_ps=12.5)
+    c, v, b, t = sponge_io.read_restart(prefix)
+    assert np.allclose(c, frames[2], atol=6e-8 * 30) and np.allclose(v, vel, atol=1e-7)
+    assert np.allclose(b, boxes[2], atol=1e-6) and t == 12.5
