@@ -4,17 +4,19 @@
 
 so that the Coulomb part of the pair force scalar is  qq * (1/r^3 - beta^3 G(beta^2 r^2))
 (equal to qq [erfc(br) + 2br/sqrt(pi) e^{-b^2r^2}] / r^3) and the exclusion correction is
--qq beta^3 G.  G is entire and even in x; on z in [0, 12] (beta*r <= 3.46) a degree-(5,5)
-rational P(z)/Q(z), Q(0) = 1, fitted by linearised least squares with Loeb reweighting and an
-error-proportional weight, has max |error| 1.5e-8 in FP64 and 1.1e-7 when evaluated in FP32
-(Horner, FP32 coefficients). Run this file to regenerate the coefficients printed into
-sb_ewald_rational.cuh.
+-qq beta^3 G.  G is entire and even in x; on z in [0, 9] (beta*r <= 3; an Ewald tolerance of
+1e-5 puts beta*rc near 2.8) a degree-(5,4) rational P(z)/Q(z), Q(0) = 1, fitted by linearised
+least squares with Loeb reweighting and an error-proportional weight, has max |error| 3.3e-8 in
+FP64 and 1.1e-7 when evaluated in FP32 (Horner, FP32 coefficients), the floor of FP32 Horner
+evaluation here, with one multiply-add fewer than a (5,5) fit on [0, 12]; its denominator has no
+zero for z >= 0. Run this file to regenerate the coefficients written into sb_ewald.cuh and
+sb_pair_x2.cuh.
 """
 import numpy as np
 from math import factorial
 from scipy.special import erf
 
-ZMAX = 12.0
+ZMAX = 9.0
 
 
 def G(z):
@@ -32,7 +34,7 @@ def G(z):
     return out
 
 
-def fit(m=5, n=5, iters=30):
+def fit(m=5, n=4, iters=40):
     z = np.linspace(0, ZMAX, 20001)
     g = G(z)
     w = np.ones_like(z)

@@ -18,21 +18,21 @@ __device__ __forceinline__ float sb_fdiv(float a, float b) {
 // G(z) = [erf(x) - 2x e^{-x^2}/sqrt(pi)] / x^3 with x = sqrt(z) = beta*r.
 // Coulomb part of the pair force scalar:   qq * (1/r^3 - beta^3 G(beta^2 r^2))
 // exclusion-correction force scalar:       qq * beta^3 G(beta^2 r^2)
-// Rational (5,5) fit on z in [0, 12] (fit_ewald_rational.py): max |error| 1.5e-8 in FP64,
-// ~1.1e-7 in FP32 Horner evaluation. Beyond z = 12 (beta*r > 3.46) the exact expression is used.
+// Rational (5,4) fit on z in [0, 9] (fit_ewald_rational.py): max |error| 3.3e-8 in FP64,
+// 1.1e-7 in FP32 Horner evaluation; the denominator has no zero for z >= 0. Beyond z = 9
+// (beta*r > 3) the exact expression is used.
 __device__ __forceinline__ float sb_ewald_G(float z) {
-    if (z <= 12.0f) {
-        float p = -4.234642899e-07f;
-        p = fmaf(p, z, 3.557744695e-05f);
-        p = fmaf(p, z, -2.489903094e-05f);
-        p = fmaf(p, z, 1.708683818e-02f);
-        p = fmaf(p, z, -2.884509870e-02f);
-        p = fmaf(p, z, 7.522527883e-01f);
-        float q = 1.255407394e-04f;
-        q = fmaf(q, z, 2.169710712e-03f);
-        q = fmaf(q, z, 2.242775561e-02f);
-        q = fmaf(q, z, 1.454184461e-01f);
-        q = fmaf(q, z, 5.616555609e-01f);
+    if (z <= 9.0f) {
+        float p = -1.034988821e-06f;
+        p = fmaf(p, z, 5.361237187e-05f);
+        p = fmaf(p, z, -1.155735711e-03f);
+        p = fmaf(p, z, 1.953816643e-02f);
+        p = fmaf(p, z, -8.191096247e-02f);
+        p = fmaf(p, z, 7.522527569e-01f);
+        float q = 7.681388070e-04f;
+        q = fmaf(q, z, 1.258269309e-02f);
+        q = fmaf(q, z, 1.063599183e-01f);
+        q = fmaf(q, z, 4.911114809e-01f);
         q = fmaf(q, z, 1.0f);
         return __fdividef(p, q);
     }
@@ -41,16 +41,16 @@ __device__ __forceinline__ float sb_ewald_G(float z) {
 }
 
 // The numerator coefficients of G, in Horner order (highest degree first).
-#define SB_EWALD_P5 -4.234642899e-07
-#define SB_EWALD_P4 3.557744695e-05
-#define SB_EWALD_P3 -2.489903094e-05
-#define SB_EWALD_P2 1.708683818e-02
-#define SB_EWALD_P1 -2.884509870e-02
-#define SB_EWALD_P0 7.522527883e-01
+#define SB_EWALD_P5 -1.034988821e-06
+#define SB_EWALD_P4 5.361237187e-05
+#define SB_EWALD_P3 -1.155735711e-03
+#define SB_EWALD_P2 1.953816643e-02
+#define SB_EWALD_P1 -8.191096247e-02
+#define SB_EWALD_P0 7.522527569e-01
 
-// beta^3 G(z) by the rational alone, no branch: valid for z <= 12. The pair kernel uses it when
-// (beta rc)^2 <= 12 (every tolerance above ~1e-7), where in-cutoff pairs never leave the fitted
-// range and out-of-range values only reach pairs that are discarded.
+// beta^3 G(z) by the rational alone, no branch: valid for z <= 9. The pair kernel uses it when
+// (beta rc)^2 <= 8.9 (an Ewald tolerance of 1e-5 gives beta rc near 2.8), where in-cutoff pairs
+// never leave the fitted range and out-of-range values only reach pairs that are discarded.
 __device__ __forceinline__ float sb_ewald_G_rational(float z, const float* gp) {
     float p = gp[0];
     p = fmaf(p, z, gp[1]);
@@ -58,11 +58,10 @@ __device__ __forceinline__ float sb_ewald_G_rational(float z, const float* gp) {
     p = fmaf(p, z, gp[3]);
     p = fmaf(p, z, gp[4]);
     p = fmaf(p, z, gp[5]);
-    float q = 1.255407394e-04f;
-    q = fmaf(q, z, 2.169710712e-03f);
-    q = fmaf(q, z, 2.242775561e-02f);
-    q = fmaf(q, z, 1.454184461e-01f);
-    q = fmaf(q, z, 5.616555609e-01f);
+    float q = 7.681388070e-04f;
+    q = fmaf(q, z, 1.258269309e-02f);
+    q = fmaf(q, z, 1.063599183e-01f);
+    q = fmaf(q, z, 4.911114809e-01f);
     q = fmaf(q, z, 1.0f);
     return sb_fdiv(p, q);
 }
@@ -70,18 +69,17 @@ __device__ __forceinline__ float sb_ewald_G_rational(float z, const float* gp) {
 // beta^3 G(z) with the numerator coefficients pre-multiplied by beta^3 (gp[0] = beta^3 P5 ...
 // gp[5] = beta^3 P0, filled on the host), one multiply fewer per pair.
 __device__ __forceinline__ float sb_ewald_G_scaled(float z, const float* gp) {
-    if (z <= 12.0f) {
+    if (z <= 9.0f) {
         float p = gp[0];
         p = fmaf(p, z, gp[1]);
         p = fmaf(p, z, gp[2]);
         p = fmaf(p, z, gp[3]);
         p = fmaf(p, z, gp[4]);
         p = fmaf(p, z, gp[5]);
-        float q = 1.255407394e-04f;
-        q = fmaf(q, z, 2.169710712e-03f);
-        q = fmaf(q, z, 2.242775561e-02f);
-        q = fmaf(q, z, 1.454184461e-01f);
-        q = fmaf(q, z, 5.616555609e-01f);
+        float q = 7.681388070e-04f;
+        q = fmaf(q, z, 1.258269309e-02f);
+        q = fmaf(q, z, 1.063599183e-01f);
+        q = fmaf(q, z, 4.911114809e-01f);
         q = fmaf(q, z, 1.0f);
         return __fdividef(p, q);
     }

@@ -285,7 +285,7 @@ static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list
                           SB_EWALD_P2, SB_EWALD_P1, SB_EWALD_P0};
     for (int k = 0; k < 6; k++) P.gp[k] = (float)(b3 * pc[k]);
     const double brc = (double)beta * lj->cutoff;
-    P.wide = brc * brc > 11.9;
+    P.wide = brc * brc > 8.9;
     P.nt = lj->ntypes;
     P.slot_cap = nl->slot_cap;
     P.ent_cap = nl->ent_cap;

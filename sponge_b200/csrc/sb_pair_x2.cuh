@@ -26,8 +26,8 @@ __device__ __forceinline__ float sb_rcp(float x) {
     return y;
 }
 
-// -beta^3 G(z) on a pair of slots by the (5,5) rational of sb_ewald_G_rational (valid for
-// z <= 12); gp holds the numerator coefficients pre-multiplied by beta^3, highest degree first
+// -beta^3 G(z) on a pair of slots by the (5,4) rational of sb_ewald_G_rational (valid for
+// z <= 9); gp holds the numerator coefficients pre-multiplied by beta^3, highest degree first
 __device__ __forceinline__ float2 ewald_nG2(float2 z, const float* gp) {
     float2 p = f2(-gp[0]);
     p = f2fma(p, z, f2(-gp[1]));
@@ -35,11 +35,10 @@ __device__ __forceinline__ float2 ewald_nG2(float2 z, const float* gp) {
     p = f2fma(p, z, f2(-gp[3]));
     p = f2fma(p, z, f2(-gp[4]));
     p = f2fma(p, z, f2(-gp[5]));
-    float2 q = f2(1.255407394e-04f);
-    q = f2fma(q, z, f2(2.169710712e-03f));
-    q = f2fma(q, z, f2(2.242775561e-02f));
-    q = f2fma(q, z, f2(1.454184461e-01f));
-    q = f2fma(q, z, f2(5.616555609e-01f));
+    float2 q = f2(7.681388070e-04f);
+    q = f2fma(q, z, f2(1.258269309e-02f));
+    q = f2fma(q, z, f2(1.063599183e-01f));
+    q = f2fma(q, z, f2(4.911114809e-01f));
     q = f2fma(q, z, f2(1.0f));
     return f2mul(p, make_float2(sb_rcp(q.x), sb_rcp(q.y)));
 }

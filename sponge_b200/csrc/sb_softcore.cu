@@ -468,7 +468,7 @@ static ScParams sc_params(const sb_softcore* sc, const sb_neighbor_list* nl, flo
                           SB_EWALD_P0};
     for (int k = 0; k < 6; k++) P.gp[k] = (float)(b3 * pc[k]);
     const double brc = (double)beta * sc->cutoff;
-    P.wide = brc * brc > 11.9;
+    P.wide = brc * brc > 8.9;
     P.ntA = sc->ntA;
     P.ntB = sc->ntB;
     P.slot_cap = nl->slot_cap;
