@@ -461,6 +461,32 @@ SB_API int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
                        const int* d_excluded_list_start, const int* d_excluded_list,
                        const int* d_excluded_numbers, float* d_frc, double* d_dudl, void* stream);
 
+/* Many FEP windows stepped together (the loop over lambda windows of a SPONGE_FEP / SPONGE_TI
+ * campaign, main_fep.cu:56-132, one process per window there): sb_fep_step of every box, one
+ * launch per stage over all boxes (pack, soft-core pair, spread, gather, finalize, dU/dlambda
+ * finish) plus one launch per FFT stage per group of equal grid sizes. Box k reads
+ * d_uint_crd[k], d_charge[k] and its exclusion lists, adds its forces into d_frc[k] and writes
+ * its dU/dlambda to d_dudl[k] (d_dudl: n_boxes device doubles, or NULL for forces only). Each
+ * box gets the same bits as its own sb_fep_step.
+ * The batch records the modules' buffers, capacities, boxes and lambdas at creation: after a
+ * box or lambda change (sb_*_update_volume, sb_sc_set_lambda) or sb_nl_set_prune, create it
+ * again (sb_fep_batch_step refuses with SB_ERR_STATE). Every list must be built before
+ * sb_fep_batch_create; later list updates (same capacities) need nothing. The caller's arrays
+ * (d_uint_crd, d_charge, ...) are read through device pointers stored at creation, so a captured
+ * CUDA graph of sb_fep_batch_step stays valid as long as those buffers do. */
+typedef struct sb_fep_batch sb_fep_batch;
+SB_API int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
+                               sb_softcore* const* scs, sb_pme* const* pmes,
+                               const uint32_t* const* d_uint_crd, const float* const* d_charge,
+                               const int* const* d_excluded_list_start,
+                               const int* const* d_excluded_list,
+                               const int* const* d_excluded_numbers, float* const* d_frc,
+                               double* d_dudl, sb_fep_batch** out);
+SB_API int sb_fep_batch_step(sb_fep_batch* batch, void* stream);
+/* kernel launches of one sb_fep_batch_step */
+SB_API int sb_fep_batch_launches(const sb_fep_batch* batch);
+SB_API int sb_fep_batch_destroy(sb_fep_batch* batch);
+
 /* ------------------------------------------------------------------------------------------
  * Differentiation for force-field fitting (no reference counterpart: SPONGE has no gradients
  * with respect to parameters). Fixed-point form of all three modules only.

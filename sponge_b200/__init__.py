@@ -93,6 +93,10 @@ _SIGS = {
     "sb_sc_dh_dlambda": [_vp, _vp, _vp, _vp, _f, _vp, _vp],
     "sb_pme_ti_cross": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "sb_fep_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_fep_batch_create": [_i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_fep_batch_step": [_vp, _vp],
+    "sb_fep_batch_launches": [_vp],
+    "sb_fep_batch_destroy": [_vp],
     "sb_nb14_create": [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp],
     "sb_nb14_destroy": [_vp],
     "sb_nb14_force": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
@@ -533,6 +537,41 @@ def pme_ti_cross(pme, uint_crd, charge, charge_B_A, excl, stream=None):
     _check(lib().sb_pme_ti_cross(pme.handle, _ptr(uint_crd), _ptr(charge), _ptr(charge_B_A),
                                  _ptr(es), _ptr(el), _ptr(en), h, _stream(stream)))
     return tuple(h)
+
+
+class FepBatchStep:
+    """sb_fep_batch_*: the fused FEP step of many boxes in one launch per stage. ``boxes`` is a
+    list of (nl, sc, pme, uint_crd, charge, (excl_start, excl_list, excl_numbers), frc); box k's
+    dU/dlambda goes to dudl[k] (a float64 CUDA tensor of len(boxes) elements, or None). The
+    tensors must outlive the batch (their device addresses are stored at creation)."""
+
+    def __init__(self, boxes, dudl=None):
+        n = len(boxes)
+        arr = lambda: (_vp * n)()
+        nls, scs, pmes, uc, q, es, el, en, frc = (arr() for _ in range(9))
+        for k, (nl, sc, pme, u, c, excl, f) in enumerate(boxes):
+            nls[k], scs[k], pmes[k] = nl.handle, sc.handle, pme.handle
+            uc[k], q[k], frc[k] = _ptr(u), _ptr(c), _ptr(f)
+            es[k], el[k], en[k] = (_ptr(t) for t in excl)
+        if dudl is not None and dudl.numel() < n:
+            raise SpongeError("dudl holds fewer than %d values" % n)
+        self._keep = (boxes, dudl)
+        h = _vp()
+        _check(lib().sb_fep_batch_create(n, nls, scs, pmes, uc, q, es, el, en, frc, _ptr(dudl),
+                                         ctypes.byref(h)))
+        self.handle = h
+
+    @property
+    def launches(self):
+        return int(lib().sb_fep_batch_launches(self.handle))
+
+    def step(self, stream=None):
+        _check(lib().sb_fep_batch_step(self.handle, _stream(stream)))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().sb_fep_batch_destroy(self.handle)
+            self.handle = None
 
 
 def fep_step(nl, sc, pme, uint_crd, charge, excl, frc, dudl=None, stream=None):

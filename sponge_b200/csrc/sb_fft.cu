@@ -594,10 +594,11 @@ static bool f4_has_z(int m) {
 
 template <bool INV>
 static void ypass4(int n, int blocks, const float2* tw, float2* spec, int K0, int H,
-                   cudaStream_t s) {
-#define SB_F4_Y(N_, A_, B_)                                                                  \
-    case N_:                                                                                 \
-        k_ypass4<A_, B_, INV><<<blocks, SB_F4_NL * F4<A_, B_>::T, 0, s>>>(tw, spec, K0, H); \
+                   cudaStream_t s, const SbFftBatchIo* bio = nullptr, int nb = 1) {
+#define SB_F4_Y(N_, A_, B_)                                                                   \
+    case N_:                                                                                  \
+        k_ypass4<A_, B_, INV><<<dim3(blocks, nb), SB_F4_NL * F4<A_, B_>::T, 0, s>>>(          \
+            tw, spec, K0, H, bio);                                                            \
         break;
     switch (n) {
         SB_FFT4_SIZES(SB_F4_Y)
@@ -607,11 +608,12 @@ static void ypass4(int n, int blocks, const float2* tw, float2* spec, int K0, in
 }
 
 static void xconv4(int n, int blocks, const float2* tw, float2* spec, const float* bc,
-                   double* epart, int K1, int H, int K2, cudaStream_t s) {
-#define SB_F4_X(N_, A_, B_)                                                               \
-    case N_:                                                                              \
-        k_xconv4<A_, B_><<<blocks, SB_F4_NL * F4<A_, B_>::T, 0, s>>>(tw, spec, bc, epart, \
-                                                                      K1, H, K2);         \
+                   double* epart, int K1, int H, int K2, cudaStream_t s,
+                   const SbFftBatchIo* bio = nullptr, int nb = 1) {
+#define SB_F4_X(N_, A_, B_)                                                                   \
+    case N_:                                                                                  \
+        k_xconv4<A_, B_><<<dim3(blocks, nb), SB_F4_NL * F4<A_, B_>::T, 0, s>>>(               \
+            tw, spec, bc, epart, K1, H, K2, bio);                                             \
         break;
     switch (n) {
         SB_FFT4_SIZES(SB_F4_X)
@@ -621,15 +623,16 @@ static void xconv4(int n, int blocks, const float2* tw, float2* spec, const floa
 }
 
 static void zfwd4(int m, int blocks, const float2* tw, const float2* post, long long* qfix,
-                  float2* spec, int rows, bool tr, cudaStream_t s) {
-#define SB_F4_ZF(N_, A_, B_)                                                                 \
-    case N_:                                                                                 \
-        if (tr)                                                                              \
-            k_zfwd4<A_, B_, true><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, qfix, \
-                                                                             spec, rows);    \
-        else                                                                                 \
-            k_zfwd4<A_, B_, false><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, qfix, \
-                                                                              spec, rows);   \
+                  float2* spec, int rows, bool tr, cudaStream_t s,
+                  const SbFftBatchIo* bio = nullptr, int nb = 1) {
+#define SB_F4_ZF(N_, A_, B_)                                                                  \
+    case N_:                                                                                  \
+        if (tr)                                                                               \
+            k_zfwd4<A_, B_, true><<<dim3(blocks, nb), SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(      \
+                tw, post, qfix, spec, rows, bio);                                             \
+        else                                                                                  \
+            k_zfwd4<A_, B_, false><<<dim3(blocks, nb), SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(     \
+                tw, post, qfix, spec, rows, bio);                                             \
         break;
     switch (m) {
         SB_FFT4_ZSIZES(SB_F4_ZF)
@@ -639,15 +642,16 @@ static void zfwd4(int m, int blocks, const float2* tw, const float2* post, long 
 }
 
 static void zinv4(int m, int blocks, const float2* tw, const float2* post, const float2* spec,
-                  float* real, int rows, bool tr, cudaStream_t s) {
-#define SB_F4_ZI(N_, A_, B_)                                                                 \
-    case N_:                                                                                 \
-        if (tr)                                                                              \
-            k_zinv4<A_, B_, true><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, spec, \
-                                                                             real, rows);    \
-        else                                                                                 \
-            k_zinv4<A_, B_, false><<<blocks, SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(tw, post, spec, \
-                                                                              real, rows);   \
+                  float* real, int rows, bool tr, cudaStream_t s,
+                  const SbFftBatchIo* bio = nullptr, int nb = 1) {
+#define SB_F4_ZI(N_, A_, B_)                                                                  \
+    case N_:                                                                                  \
+        if (tr)                                                                               \
+            k_zinv4<A_, B_, true><<<dim3(blocks, nb), SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(      \
+                tw, post, spec, real, rows, bio);                                             \
+        else                                                                                  \
+            k_zinv4<A_, B_, false><<<dim3(blocks, nb), SB_F4_ZR * F4<A_, B_>::T, 0, s>>>(     \
+                tw, post, spec, real, rows, bio);                                             \
         break;
     switch (m) {
         SB_FFT4_ZSIZES(SB_F4_ZI)
@@ -671,7 +675,8 @@ static bool f4_has_plane(int k) {
 static size_t plane4_smem(int k) { return sizeof(float2) * ((size_t)k + (size_t)k * (k + 1)); }
 
 static int plane4(int k, int blocks, const float2* tw, float2* spec, const float* bc,
-                  double* epart, int H, int K2, cudaStream_t s) {
+                  double* epart, int H, int K2, cudaStream_t s,
+                  const SbFftBatchIo* bio = nullptr, int nb = 1) {
     const size_t sm = plane4_smem(k);
 #define SB_F4_PL(K_, A_, B_, NL_)                                                             \
     case K_:                                                                                  \
@@ -679,8 +684,8 @@ static int plane4(int k, int blocks, const float2* tw, float2* spec, const float
             SB_CHECK_CUDA(cudaFuncSetAttribute(k_plane4<A_, B_, NL_>,                         \
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,   \
                                                (int)sm));                                     \
-        k_plane4<A_, B_, NL_><<<blocks, NL_ * F4<A_, B_>::T, sm, s>>>(tw, spec, bc, epart, H, \
-                                                                     K2);                     \
+        k_plane4<A_, B_, NL_><<<dim3(blocks, nb), NL_ * F4<A_, B_>::T, sm, s>>>(              \
+            tw, spec, bc, epart, H, K2, bio);                                                 \
         break;
     switch (k) {
         SB_FFT4_PLANE_SIZES(SB_F4_PL)
@@ -850,4 +855,64 @@ int sb_fft_plane_inverse(const SbFftPlan* p, const float2* d_spec, float* d_real
                          cudaStream_t s) {
     if (!p->fused) SB_TRY(launch_ypass(p, const_cast<float2*>(d_spec), 1, p->yt, s));
     return launch_zinv(p, d_spec, d_real, p->zt, s);
+}
+
+// ---------------------------------------------------------------------------------------------
+// batched stages: nb grids of this plan's size, one launch per stage, grid blockIdx.y taking its
+// pointers from entry blockIdx.y of the device table (the same kernels and shapes as a single
+// grid, so each grid gets the bits of its own single launch)
+// ---------------------------------------------------------------------------------------------
+bool sb_fft_batchable(const SbFftPlan* p) {
+    return p->zt == 0 && p->yt == 0 && p->xt == 0 && f4_has_z(p->K[2] / 2) &&
+           (p->fused ? f4_has_plane(p->K[0]) : (f4_has(p->K[1]) && f4_has(p->K[0])));
+}
+
+int sb_fft_batch_forward(const SbFftPlan* p, const SbFftBatchIo* d_io, int nb, cudaStream_t s) {
+    if (!sb_fft_batchable(p) || nb < 1 || nb > 65535) {
+        sb_set_error("sb_fft_batch_forward: plan without a batched form or bad count %d", nb);
+        return SB_ERR_ARG;
+    }
+    const int rows = p->K[0] * p->K[1];
+    zfwd4(p->K[2] / 2, (rows + SB_F4_ZR - 1) / SB_F4_ZR, p->z.d_tw, p->d_post, nullptr, nullptr,
+          rows, p->fused != 0, s, d_io, nb);
+    SB_CHECK_LAUNCH();
+    if (!p->fused) {
+        ypass4<false>(p->K[1], (p->K[0] * p->H + SB_F4_NL - 1) / SB_F4_NL, p->y.d_tw, nullptr,
+                      p->K[0], p->H, s, d_io, nb);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+int sb_fft_batch_convolve(const SbFftPlan* p, const SbFftBatchIo* d_io, int nb, int want_energy,
+                          cudaStream_t s) {
+    (void)want_energy;  // the partials are written either way; the caller reads them or not
+    if (!sb_fft_batchable(p) || nb < 1 || nb > 65535) {
+        sb_set_error("sb_fft_batch_convolve: plan without a batched form or bad count %d", nb);
+        return SB_ERR_ARG;
+    }
+    if (p->fused)
+        return plane4(p->K[0], p->H, p->x.d_tw, nullptr, nullptr, nullptr, p->H, p->K[2], s,
+                      d_io, nb);
+    xconv4(p->K[0], (p->K[1] * p->H + SB_F4_NL - 1) / SB_F4_NL, p->x.d_tw, nullptr, nullptr,
+           nullptr, p->K[1], p->H, p->K[2], s, d_io, nb);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+int sb_fft_batch_inverse(const SbFftPlan* p, const SbFftBatchIo* d_io, int nb, cudaStream_t s) {
+    if (!sb_fft_batchable(p) || nb < 1 || nb > 65535) {
+        sb_set_error("sb_fft_batch_inverse: plan without a batched form or bad count %d", nb);
+        return SB_ERR_ARG;
+    }
+    if (!p->fused) {
+        ypass4<true>(p->K[1], (p->K[0] * p->H + SB_F4_NL - 1) / SB_F4_NL, p->y.d_tw, nullptr,
+                     p->K[0], p->H, s, d_io, nb);
+        SB_CHECK_LAUNCH();
+    }
+    const int rows = p->K[0] * p->K[1];
+    zinv4(p->K[2] / 2, (rows + SB_F4_ZR - 1) / SB_F4_ZR, p->z.d_tw, p->d_post, nullptr, nullptr,
+          rows, p->fused != 0, s, d_io, nb);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
 }

@@ -154,9 +154,11 @@ struct F4 {
 
 template <int N1, int N2, bool INV>
 __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_ypass4(
-    const float2* __restrict__ twy, float2* __restrict__ spec, int K0, int H) {
+    const float2* __restrict__ twy, float2* __restrict__ spec, int K0, int H,
+    const SbFftBatchIo* __restrict__ bio) {
     constexpr int K1 = N1 * N2, NL = SB_F4_NL, NT = NL * F4<N1, N2>::T, IT = K1 * NL / NT;
     static_assert(K1 * NL % NT == 0, "tile must divide among the threads");
+    if (bio) spec = bio[blockIdx.y].spec;
     __shared__ float2 tw[K1];
     __shared__ float2 D[K1 * NL];
     __shared__ long long cbase[NL];
@@ -195,9 +197,14 @@ __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_ypass4(
 template <int N1, int N2>
 __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_xconv4(
     const float2* __restrict__ twx, float2* __restrict__ spec, const float* __restrict__ bc,
-    double* __restrict__ epart, int K1, int H, int K2) {
+    double* __restrict__ epart, int K1, int H, int K2, const SbFftBatchIo* __restrict__ bio) {
     constexpr int K0 = N1 * N2, NL = SB_F4_NL, NT = NL * F4<N1, N2>::T, IT = K0 * NL / NT;
     static_assert(K0 * NL % NT == 0, "tile must divide among the threads");
+    if (bio) {
+        spec = bio[blockIdx.y].spec;
+        bc = bio[blockIdx.y].bc;
+        epart = bio[blockIdx.y].epart;
+    }
     __shared__ float2 tw[K0];
     __shared__ float2 D[K0 * NL];
     __shared__ int cbase[NL], ckz[NL];
@@ -275,10 +282,15 @@ __global__ void __launch_bounds__(SB_F4_NL * F4<N1, N2>::T) k_xconv4(
 template <int N1, int N2, bool TR>
 __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zfwd4(
     const float2* __restrict__ twz, const float2* __restrict__ post,
-    long long* __restrict__ qfix, float2* __restrict__ spec, int nrows) {
+    long long* __restrict__ qfix, float2* __restrict__ spec, int nrows,
+    const SbFftBatchIo* __restrict__ bio) {
     constexpr int M = N1 * N2, K2 = 2 * M, H = M + 1, NL = SB_F4_ZR;
     constexpr int NT = NL * F4<N1, N2>::T, IT = NL * K2 / NT, ITO = (NL * H + NT - 1) / NT;
     static_assert(NL * K2 % NT == 0, "tile must divide among the threads");
+    if (bio) {
+        qfix = bio[blockIdx.y].qfix;
+        spec = bio[blockIdx.y].spec;
+    }
     __shared__ float2 tw[M], ps[M];
     __shared__ float2 D[NL * H];
     float* Df = reinterpret_cast<float*>(D);
@@ -355,10 +367,15 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zfwd4(
 template <int N1, int N2, bool TR>
 __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zinv4(
     const float2* __restrict__ twz, const float2* __restrict__ post,
-    const float2* __restrict__ spec, float* __restrict__ real, int nrows) {
+    const float2* __restrict__ spec, float* __restrict__ real, int nrows,
+    const SbFftBatchIo* __restrict__ bio) {
     constexpr int M = N1 * N2, K2 = 2 * M, H = M + 1, NL = SB_F4_ZR;
     constexpr int NT = NL * F4<N1, N2>::T, ITI = (NL * H + NT - 1) / NT, IT = NL * K2 / NT;
     static_assert(NL * K2 % NT == 0, "tile must divide among the threads");
+    if (bio) {
+        spec = bio[blockIdx.y].spec;
+        real = bio[blockIdx.y].real;
+    }
     __shared__ float2 tw[M], ps[M];
     __shared__ float2 D[NL * H];
     const float* Df = reinterpret_cast<const float*>(D);
@@ -440,9 +457,14 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zinv4(
 template <int N1, int N2, int NL>
 __global__ void __launch_bounds__(NL * F4<N1, N2>::T) k_plane4(
     const float2* __restrict__ tw_in, float2* __restrict__ spec, const float* __restrict__ bc,
-    double* __restrict__ epart, int H, int K2) {
+    double* __restrict__ epart, int H, int K2, const SbFftBatchIo* __restrict__ bio) {
     constexpr int K = N1 * N2, P = K + 1, NT = NL * F4<N1, N2>::T, IT = K * K / NT;
     static_assert(K * K % NT == 0 && K % NL == 0, "plane must divide among the threads");
+    if (bio) {
+        spec = bio[blockIdx.y].spec;
+        bc = bio[blockIdx.y].bc;
+        epart = bio[blockIdx.y].epart;
+    }
     extern __shared__ float2 smem_plane[];
     float2* tw = smem_plane;
     float2* D = smem_plane + K;

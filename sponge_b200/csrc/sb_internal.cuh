@@ -83,6 +83,16 @@ struct SbFftAxis {
     float2* d_tw = nullptr;    // e^{-2 pi i t / n}, t < n (FP64-computed)
 };
 
+// per-grid pointers of a batched FFT launch: grids of one size transformed by one launch, grid
+// blockIdx.y of the launch taking entry blockIdx.y (the twiddles are shared by the size)
+struct SbFftBatchIo {
+    long long* qfix;
+    float2* spec;
+    float* real;
+    const float* bc;
+    double* epart;
+};
+
 struct SbFftPlan {
     int K[3] = {0, 0, 0};
     int H = 0;                 // K2/2 + 1
@@ -111,6 +121,13 @@ void sb_fft_plan_destroy(SbFftPlan* p);
 
 // forward plane pass: int64 charge grid -> half spectrum (z R2C + y forward); clears the grid
 int sb_fft_plane_forward(const SbFftPlan* p, long long* d_qfix, float2* d_spec, cudaStream_t s);
+// the same three stages for `nb` grids of this plan's shape in one launch each (io: a device
+// table of nb entries); SB_ERR_ARG for a plan with a stage-kernel axis (no batched form)
+int sb_fft_batch_forward(const SbFftPlan* p, const SbFftBatchIo* d_io, int nb, cudaStream_t s);
+int sb_fft_batch_convolve(const SbFftPlan* p, const SbFftBatchIo* d_io, int nb, int want_energy,
+                          cudaStream_t s);
+int sb_fft_batch_inverse(const SbFftPlan* p, const SbFftBatchIo* d_io, int nb, cudaStream_t s);
+bool sb_fft_batchable(const SbFftPlan* p);
 // x pass: forward x, multiply by the Green's function table, energy partials, inverse x
 int sb_fft_x_convolve(const SbFftPlan* p, float2* d_spec, const float* d_bc, double* d_epart,
                       int want_energy, cudaStream_t s, int* nparts_out);
@@ -274,6 +291,126 @@ int sb_pme_fused_reciprocal(sb_pme* pme, sb_neighbor_list* nl, float* d_frc,
 int sb_pme_ti_terms_slot(sb_pme* p, sb_neighbor_list* nl, const float* slot_dq,
                          const uint32_t* uc, const float* q, const float* dq, const int* es,
                          const int* el, const int* en, long long* acc, cudaStream_t s);
+
+// slot s of a packed list (k_pack): coordinates, charge bits and type in slot order (zeros in an
+// empty slot); with xq_prune, an atom that moved more than sqrt(move2) since the last prune sets
+// the prune request
+__device__ __forceinline__ void sb_pack_slot(int s, const int* __restrict__ slot_atom,
+                                             const uint32_t* __restrict__ uc,
+                                             const float* __restrict__ q,
+                                             const int* __restrict__ type,
+                                             uint4* __restrict__ xq, int* __restrict__ stype,
+                                             const uint4* __restrict__ xq_prune, float sx,
+                                             float sy, float sz, float move2,
+                                             int* __restrict__ prune_req) {
+    const int a = slot_atom[s];
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    int t = 0;
+    if (a >= 0) {
+        v.x = uc[3 * a];
+        v.y = uc[3 * a + 1];
+        v.z = uc[3 * a + 2];
+        v.w = q ? __float_as_uint(q[a]) : 0u;
+        t = type ? type[a] : 0;
+        if (xq_prune) {
+            const uint4 o = xq_prune[s];
+            const float dx = __int2float_rn((int)(v.x - o.x)) * sx;
+            const float dy = __int2float_rn((int)(v.y - o.y)) * sy;
+            const float dz = __int2float_rn((int)(v.z - o.z)) * sz;
+            if (dx * dx + dy * dy + dz * dz > move2) prune_req[0] = 1;
+        }
+    }
+    xq[s] = v;
+    stype[s] = t;
+}
+
+// slot s of the fixed-point force planes (k_finalize) added to the atom's float force, the
+// accumulator cleared for the next step
+__device__ __forceinline__ void sb_finalize_slot(int s, const int* __restrict__ slot_atom,
+                                                 long long* __restrict__ fix, int slot_cap,
+                                                 float* __restrict__ frc) {
+    const int a = slot_atom[s];
+    const long long fx = fix[s], fy = fix[slot_cap + s], fz = fix[2 * slot_cap + s];
+    if (fx | fy | fz) {
+        fix[s] = 0;
+        fix[slot_cap + s] = 0;
+        fix[2 * slot_cap + s] = 0;
+    }
+    if (a >= 0) {
+        frc[3 * a] += (float)((double)fx * SB_FORCE_UNSCALE);
+        frc[3 * a + 1] += (float)((double)fy * SB_FORCE_UNSCALE);
+        frc[3 * a + 2] += (float)((double)fz * SB_FORCE_UNSCALE);
+    }
+}
+
+// a prune request served by the pair launch before (meta[7] set) is retired
+__device__ __forceinline__ void sb_retire_prune(int* __restrict__ meta) {
+    if (meta[7]) {
+        meta[6] = 0;
+        meta[7] = 0;
+    }
+}
+
+// Ewald exclusion correction of one atom inside a reciprocal gather (k_gather_atom): the
+// arithmetic of k_excluded<true>, its int64 terms added to the atoms' slot accumulators
+struct SbExclPass {
+    const int* slot_atom;
+    const int* atom_slot;
+    const int* es;
+    const int* el;
+    const int* en;
+    float sx, sy, sz, beta, beta2, beta3;
+    float* ene;  // per-atom correction energy (energy steps) or null
+};
+
+// One FEP box of a batched step (sb_fep_batch_*): the device pointers and constants that the
+// batched kernels of every stage read, gathered from the box's list, soft-core and PME modules
+// and from the caller's buffers bound to the batch.
+#define SB_FEP_BATCH_THREADS 256  // threads per block of the batched per-atom and per-slot kernels
+struct SbFepBox {
+    // neighbor list
+    int* meta;
+    const int* cl_count;
+    const uint32_t* cl_ent;
+    uint4* xq;
+    int* stype;
+    const int* slot_atom;
+    long long* fix;
+    const uint4* xq_prune;  // null without a pruned list
+    float move2;            // squared displacement that requests a prune
+    float usx, usy, usz;    // length of one fixed-point coordinate unit in the list's box
+    int slot_cap;
+    // soft core
+    const int* typeA;
+    const int* typeB;
+    const int* mask;
+    const float* dq;
+    int* slot_ext;
+    float* slot_dq;
+    const float2* ABa;
+    const float2* ABb;
+    long long* hfix;  // [4] dH/dlambda parts: LJ, direct, reciprocal, correction
+    // reciprocal space
+    long long* qfix;
+    const float* theta;
+    int K0, K1, K2;
+    float ix, iy, iz;
+    SbExclPass X;
+    // the caller's buffers and the finishing constants
+    const uint32_t* uc;
+    const float* q;
+    float* frc;
+    double* dudl;
+    int n;
+    double self_coef, neutral2, lrc;
+};
+
+// batched stages over all boxes; tab[b] = {box, block of that box} for every launched block
+int sb_pme_batch_spread(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, cudaStream_t s);
+int sb_pme_batch_gather(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, int dh,
+                        cudaStream_t s);
+int sb_pme_batch_slots(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, int dh,
+                       cudaStream_t s);
 
 // FP64 reduction helpers (deterministic: fixed block/thread order)
 int sb_reduce_sum_f32(const float* d_x, int n, double* d_out, cudaStream_t s);

@@ -613,51 +613,19 @@ __global__ void k_pack(const int* __restrict__ meta, const int* __restrict__ slo
                        const int* __restrict__ type, uint4* __restrict__ xq,
                        int* __restrict__ stype, const uint4* __restrict__ xq_prune, float sx,
                        float sy, float sz, float move2, int* __restrict__ prune_req) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= meta[3]) return;
-    int a = slot_atom[s];
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    int t = 0;
-    if (a >= 0) {
-        v.x = uc[3 * a];
-        v.y = uc[3 * a + 1];
-        v.z = uc[3 * a + 2];
-        v.w = q ? __float_as_uint(q[a]) : 0u;
-        t = type ? type[a] : 0;
-        if (xq_prune) {
-            const uint4 o = xq_prune[s];
-            const float dx = __int2float_rn((int)(v.x - o.x)) * sx;
-            const float dy = __int2float_rn((int)(v.y - o.y)) * sy;
-            const float dz = __int2float_rn((int)(v.z - o.z)) * sz;
-            if (dx * dx + dy * dy + dz * dz > move2) prune_req[0] = 1;
-        }
-    }
-    xq[s] = v;
-    stype[s] = t;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < meta[3])
+        sb_pack_slot(s, slot_atom, uc, q, type, xq, stype, xq_prune, sx, sy, sz, move2,
+                     prune_req);
 }
 
 // fixed-point forces to the caller's float array (slot order -> atom order), clearing the
 // accumulator; also retires a prune request that the pair launch before it served (meta[6..7])
 __global__ void k_finalize(int* __restrict__ meta, const int* __restrict__ slot_atom,
                            long long* __restrict__ fix, int slot_cap, float* __restrict__ frc) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s == 0 && meta[7]) {
-        meta[6] = 0;
-        meta[7] = 0;
-    }
-    if (s >= meta[3]) return;
-    int a = slot_atom[s];
-    long long fx = fix[s], fy = fix[slot_cap + s], fz = fix[2 * slot_cap + s];
-    if (fx | fy | fz) {
-        fix[s] = 0;
-        fix[slot_cap + s] = 0;
-        fix[2 * slot_cap + s] = 0;
-    }
-    if (a >= 0) {
-        frc[3 * a] += (float)((double)fx * SB_FORCE_UNSCALE);
-        frc[3 * a + 1] += (float)((double)fy * SB_FORCE_UNSCALE);
-        frc[3 * a + 2] += (float)((double)fz * SB_FORCE_UNSCALE);
-    }
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) sb_retire_prune(meta);
+    if (s < meta[3]) sb_finalize_slot(s, slot_atom, fix, slot_cap, frc);
 }
 
 __global__ void k_crd_to_uint(int n, const float* __restrict__ crd, float cx, float cy, float cz,

@@ -50,11 +50,9 @@ __device__ __forceinline__ void bspline4d(float f, float d[4]) {
 // z row at each (x, y) offset. Grid-stride, so that the fused step can run it on a small grid
 // beside the pair kernel.
 template <bool FIXED>
-__global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __restrict__ q,
-                         int K0, int K1, int K2, long long* __restrict__ gfix,
-                         float* __restrict__ gf) {
-    for (int gt = blockIdx.x * blockDim.x + threadIdx.x; gt < 4 * n;
-         gt += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void spread_one(int gt, const uint32_t* __restrict__ uc,
+                                           const float* __restrict__ q, int K0, int K1, int K2,
+                                           long long* __restrict__ gfix, float* __restrict__ gf) {
     const int i = gt >> 2, kz = gt & 3;
     int b0, b1, b2;
     float f0, f1, f2;
@@ -88,7 +86,15 @@ __global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __
             }
         }
     }
-    }
+}
+
+template <bool FIXED>
+__global__ void k_spread(int n, const uint32_t* __restrict__ uc, const float* __restrict__ q,
+                         int K0, int K1, int K2, long long* __restrict__ gfix,
+                         float* __restrict__ gf) {
+    for (int gt = blockIdx.x * blockDim.x + threadIdx.x; gt < 4 * n;
+         gt += gridDim.x * blockDim.x)
+        spread_one<FIXED>(gt, uc, q, K0, K1, K2, gfix, gf);
 }
 
 // force interpolation (PME_Final, PME_force.cu:485-550); one thread per atom, one writer
@@ -768,17 +774,6 @@ extern "C" int sb_pme_get_energy(sb_pme* p, sb_neighbor_list* nl, const uint32_t
 // buffer (x, y, z planes of slot_cap int64 each)
 // ---------------------------------------------------------------------------------------------
 
-// Ewald exclusion correction of one atom inside a reciprocal gather (k_gather_atom): the
-// arithmetic of k_excluded<true>, its int64 terms added to the atoms' slot accumulators
-struct SbExclPass {
-    const int* slot_atom;
-    const int* atom_slot;
-    const int* es;
-    const int* el;
-    const int* en;
-    float sx, sy, sz, beta, beta2, beta3;
-    float* ene;  // per-atom correction energy (energy steps) or null
-};
 
 int sb_pme_zero_atom_energy(sb_pme* p, float* d_atom_energy, cudaStream_t s) {
     if (d_atom_energy) {
@@ -995,6 +990,17 @@ __device__ __forceinline__ void ti_red(long long* p, float v) {
     }
 }
 
+// dq phi of packed slot s (a slot of an uncharged-change atom or an empty slot gives 0)
+__device__ __forceinline__ float ti_rec_slot(int s, const uint4* __restrict__ xq,
+                                             const float* __restrict__ slot_dq,
+                                             const float* __restrict__ theta, int K0, int K1,
+                                             int K2) {
+    const float d = slot_dq[s];
+    if (d == 0.f) return 0.f;
+    const uint4 u = xq[s];
+    return d * phi_at(u.x, u.y, u.z, theta, K0, K1, K2);
+}
+
 // sum dq phi over atoms in original order (n) or over packed slots (xq != null, n = slots)
 __global__ void k_ti_rec(int n, const int* __restrict__ meta, const uint32_t* __restrict__ uc,
                          const uint4* __restrict__ xq, const float* __restrict__ dq,
@@ -1004,40 +1010,46 @@ __global__ void k_ti_rec(int n, const int* __restrict__ meta, const uint32_t* __
     const int lim = meta ? meta[3] : n;
     float v = 0.f;
     if (i < lim) {
-        const float d = dq[i];
-        if (d != 0.f) {
-            if (xq) {
-                const uint4 u = xq[i];
-                v = d * phi_at(u.x, u.y, u.z, theta, K0, K1, K2);
-            } else {
+        if (xq) {
+            v = ti_rec_slot(i, xq, dq, theta, K0, K1, K2);
+        } else {
+            const float d = dq[i];
+            if (d != 0.f)
                 v = d * phi_at(uc[3 * i], uc[3 * i + 1], uc[3 * i + 2], theta, K0, K1, K2);
-            }
         }
     }
     ti_red(acc, v);
 }
 
-// d/dlambda of the exclusion correction -qq erf(beta r)/r at fixed geometry
+// d/dlambda of atom i's exclusion corrections -qq erf(beta r)/r at fixed geometry
+__device__ __forceinline__ float ti_corr_atom(int i, const uint32_t* __restrict__ uc, float sx,
+                                              float sy, float sz, const float* __restrict__ q,
+                                              const float* __restrict__ dq, float beta,
+                                              const int* __restrict__ es,
+                                              const int* __restrict__ el,
+                                              const int* __restrict__ en) {
+    float v = 0.f;
+    const int cnt = en[i], s0 = es[i];
+    const float qi = q[i], dqi = dq[i];
+    for (int k = s0; k < s0 + cnt; k++) {
+        const int j = el[k];
+        const float dqq = qi * dq[j] + dqi * q[j];
+        if (dqq == 0.f) continue;
+        const float dx = __int2float_rn((int)(uc[3 * j] - uc[3 * i])) * sx;
+        const float dy = __int2float_rn((int)(uc[3 * j + 1] - uc[3 * i + 1])) * sy;
+        const float dz = __int2float_rn((int)(uc[3 * j + 2] - uc[3 * i + 2])) * sz;
+        const float r = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        v -= dqq * erff(beta * r) / r;
+    }
+    return v;
+}
+
 __global__ void k_ti_corr(int n, const uint32_t* __restrict__ uc, float sx, float sy, float sz,
                           const float* __restrict__ q, const float* __restrict__ dq, float beta,
                           const int* __restrict__ es, const int* __restrict__ el,
                           const int* __restrict__ en, long long* __restrict__ acc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    float v = 0.f;
-    if (i < n) {
-        const int cnt = en[i], s0 = es[i];
-        const float qi = q[i], dqi = dq[i];
-        for (int k = s0; k < s0 + cnt; k++) {
-            const int j = el[k];
-            const float dqq = qi * dq[j] + dqi * q[j];
-            if (dqq == 0.f) continue;
-            const float dx = __int2float_rn((int)(uc[3 * j] - uc[3 * i])) * sx;
-            const float dy = __int2float_rn((int)(uc[3 * j + 1] - uc[3 * i + 1])) * sy;
-            const float dz = __int2float_rn((int)(uc[3 * j + 2] - uc[3 * i + 2])) * sz;
-            const float r = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-            v -= dqq * erff(beta * r) / r;
-        }
-    }
+    const float v = i < n ? ti_corr_atom(i, uc, sx, sy, sz, q, dq, beta, es, el, en) : 0.f;
     ti_red(acc, v);
 }
 
@@ -1284,5 +1296,81 @@ extern "C" int sb_pme_get_energy_noalloc(sb_pme* p, sb_neighbor_list* nl,
         h_parts[3] = cor;
         h_parts[4] = self;
     }
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched reciprocal chain of many FEP boxes (sb_fep_batch_*): every launch covers all boxes,
+// block b working for box tab[b].x on its block tab[b].y (blocks never straddle boxes, so a warp
+// belongs to one box). Each thread does what the same thread of the box's own launches does and
+// the sums are fixed point or keep their warps, so every box gets the bits of its single steps.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
+    k_spread_batch(const SbFepBox* __restrict__ B, const int2* __restrict__ tab) {
+    const int2 t = tab[blockIdx.x];
+    const SbFepBox& b = B[t.x];
+    const int gt = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
+    if (gt < 4 * b.n) spread_one<true>(gt, b.uc, b.q, b.K0, b.K1, b.K2, b.qfix, nullptr);
+}
+
+// reciprocal gather with the exclusion correction, and (dH) the exclusion cross term of
+// dU/dlambda summed per warp as k_ti_corr does
+template <bool DH>
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
+    k_gather_batch(const SbFepBox* __restrict__ B, const int2* __restrict__ tab) {
+    const int2 t = tab[blockIdx.x];
+    const SbFepBox& b = B[t.x];
+    const int i = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
+    if (DH && b.X.es) {
+        const float v = i < b.n ? ti_corr_atom(i, b.uc, b.X.sx, b.X.sy, b.X.sz, b.q, b.dq,
+                                               b.X.beta, b.X.es, b.X.el, b.X.en)
+                                : 0.f;
+        ti_red(b.hfix + 3, v);
+    }
+    if (i < b.n)
+        gather_atom_one(i, b.uc, b.q, b.theta, b.K0, b.K1, b.K2, b.ix, b.iy, b.iz, b.fix,
+                        b.slot_cap, b.X);
+}
+
+// fixed-point forces to the boxes' float arrays, and (dH) the reciprocal cross term over slots
+template <bool DH>
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
+    k_slots_batch(const SbFepBox* __restrict__ B, const int2* __restrict__ tab) {
+    const int2 t = tab[blockIdx.x];
+    const SbFepBox& b = B[t.x];
+    const int s = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
+    const int lim = b.meta[3];
+    if (s == 0) sb_retire_prune(b.meta);
+    if (DH) {
+        const float v = s < lim ? ti_rec_slot(s, b.xq, b.slot_dq, b.theta, b.K0, b.K1, b.K2)
+                                : 0.f;
+        ti_red(b.hfix + 2, v);
+    }
+    if (s < lim) sb_finalize_slot(s, b.slot_atom, b.fix, b.slot_cap, b.frc);
+}
+
+int sb_pme_batch_spread(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, cudaStream_t s) {
+    k_spread_batch<<<nblocks, SB_FEP_BATCH_THREADS, 0, s>>>(d_boxes, d_tab);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+int sb_pme_batch_gather(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, int dh,
+                        cudaStream_t s) {
+    if (dh)
+        k_gather_batch<true><<<nblocks, SB_FEP_BATCH_THREADS, 0, s>>>(d_boxes, d_tab);
+    else
+        k_gather_batch<false><<<nblocks, SB_FEP_BATCH_THREADS, 0, s>>>(d_boxes, d_tab);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+int sb_pme_batch_slots(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, int dh,
+                       cudaStream_t s) {
+    if (dh)
+        k_slots_batch<true><<<nblocks, SB_FEP_BATCH_THREADS, 0, s>>>(d_boxes, d_tab);
+    else
+        k_slots_batch<false><<<nblocks, SB_FEP_BATCH_THREADS, 0, s>>>(d_boxes, d_tab);
+    SB_CHECK_LAUNCH();
     return SB_OK;
 }

@@ -133,21 +133,29 @@ __device__ __forceinline__ void red_fix_sc(long long* p, float v, float scale) {
 }
 
 // per-slot B type, mask and charge change
-__global__ void k_sc_pack(const int* __restrict__ meta, const int* __restrict__ slot_atom,
-                          const int* __restrict__ typeB, const int* __restrict__ mask,
-                          const float* __restrict__ dq, int* __restrict__ ext,
-                          float* __restrict__ sdq) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= meta[3]) return;
+__device__ __forceinline__ void sc_pack_slot(int s, const int* __restrict__ slot_atom,
+                                             const int* __restrict__ typeB,
+                                             const int* __restrict__ mask,
+                                             const float* __restrict__ dq, int* __restrict__ ext,
+                                             float* __restrict__ sdq) {
     const int a = slot_atom[s];
     ext[s] = a >= 0 ? (typeB[a] | (mask[a] << 16)) : 0;
     sdq[s] = a >= 0 ? dq[a] : 0.f;
 }
 
-// chosen form: warp per cluster, one lane per list entry, the 8 cluster atoms in registers
+__global__ void k_sc_pack(const int* __restrict__ meta, const int* __restrict__ slot_atom,
+                          const int* __restrict__ typeB, const int* __restrict__ mask,
+                          const float* __restrict__ dq, int* __restrict__ ext,
+                          float* __restrict__ sdq) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < meta[3]) sc_pack_slot(s, slot_atom, typeB, mask, dq, ext, sdq);
+}
+
+// chosen form: warp per cluster, one lane per list entry, the 8 cluster atoms in registers;
+// block `blk` of 4 warps takes clusters 4 blk .. 4 blk + 3
 template <int EV, bool DH>
-__global__ void __launch_bounds__(128) k_pair_sc(
-    ScParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
+__device__ __forceinline__ void pair_sc_block(
+    const ScParams& P, int blk, const int* __restrict__ meta, const int* __restrict__ cl_count,
     const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
     const int* __restrict__ stype, const int* __restrict__ sext, const float* __restrict__ sdq,
     const float2* __restrict__ ABa, const float2* __restrict__ ABb,
@@ -164,7 +172,7 @@ __global__ void __launch_bounds__(128) k_pair_sc(
     const float2* sA = sAB;
     const float2* sB = sAB + na;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int c = blockIdx.x * 4 + w;
+    const int c = blk * 4 + w;
     if (c >= meta[0]) return;
     const int base = c * SB_CLUSTER;
     const uint4 my = lane < SB_CLUSTER ? xq[base + lane] : make_uint4(0, 0, 0, 0);
@@ -287,6 +295,19 @@ __global__ void __launch_bounds__(128) k_pair_sc(
     }
 }
 
+template <int EV, bool DH>
+__global__ void __launch_bounds__(128) k_pair_sc(
+    ScParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,
+    const uint32_t* __restrict__ cl_ent, const uint4* __restrict__ xq,
+    const int* __restrict__ stype, const int* __restrict__ sext, const float* __restrict__ sdq,
+    const float2* __restrict__ ABa, const float2* __restrict__ ABb,
+    const int* __restrict__ slot_atom, long long* __restrict__ fix,
+    long long* __restrict__ hfix, float* __restrict__ atom_energy,
+    float* __restrict__ atom_virial, float* __restrict__ atom_direct) {
+    pair_sc_block<EV, DH>(P, blockIdx.x, meta, cl_count, cl_ent, xq, stype, sext, sdq, ABa, ABb,
+                          slot_atom, fix, hfix, atom_energy, atom_virial, atom_direct);
+}
+
 // plain form: warp per atom over the ATOM_GROUP half list, float atomics (the reference's
 // LJ_Soft_Core_Force_With_Direct_CF_CUDA structure, LJ_soft_core.cu:159-317)
 struct ScAtomGroup {
@@ -372,13 +393,14 @@ __global__ void k_sc_zero(long long* __restrict__ h, int n) {
 }
 
 // PME cross-term and total: hfix [LJ, direct, reciprocal, correction] (fixed point) + self term
-// from FP64 sums of q dq, q, dq + long-range term -> out (FP64); optionally parts[7]
-__global__ void __launch_bounds__(1024) k_fep_finish(int n, const float* __restrict__ q,
-                                                     const float* __restrict__ dq,
-                                                     const long long* __restrict__ hfix,
-                                                     double self_coef, double neutral2,
-                                                     double lrc, double* __restrict__ out,
-                                                     double* __restrict__ parts) {
+// from FP64 sums of q dq, q, dq + long-range term -> out (FP64); optionally parts[7]. One block
+// of 1024 threads.
+__device__ __forceinline__ void fep_finish_block(int n, const float* __restrict__ q,
+                                                 const float* __restrict__ dq,
+                                                 const long long* __restrict__ hfix,
+                                                 double self_coef, double neutral2, double lrc,
+                                                 double* __restrict__ out,
+                                                 double* __restrict__ parts) {
     __shared__ double r1[1024], r2[1024], r3[1024];
     double a = 0, b = 0, c = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -413,6 +435,15 @@ __global__ void __launch_bounds__(1024) k_fep_finish(int n, const float* __restr
             parts[6] = lj + dir + rec + cor + self + lrc;
         }
     }
+}
+
+__global__ void __launch_bounds__(1024) k_fep_finish(int n, const float* __restrict__ q,
+                                                     const float* __restrict__ dq,
+                                                     const long long* __restrict__ hfix,
+                                                     double self_coef, double neutral2,
+                                                     double lrc, double* __restrict__ out,
+                                                     double* __restrict__ parts) {
+    fep_finish_block(n, q, dq, hfix, self_coef, neutral2, lrc, out, parts);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -586,7 +617,7 @@ extern "C" int sb_sc_set_lambda(sb_softcore* sc, float lambda) {
 }
 
 // per-slot extras sized for the list (re-created when a list with more slots comes along)
-static int sc_slots(sb_softcore* sc, sb_neighbor_list* nl, cudaStream_t s) {
+static int sc_slots_alloc(sb_softcore* sc, const sb_neighbor_list* nl) {
     if (sc->slot_cap < nl->slot_cap) {
         sb_free(sc->d_slot_ext);
         sb_free(sc->d_slot_dq);
@@ -597,6 +628,11 @@ static int sc_slots(sb_softcore* sc, sb_neighbor_list* nl, cudaStream_t s) {
         SB_TRY(sb_malloc((void**)&sc->d_slot_dq, sizeof(float) * nl->slot_cap, "soft-core slots"));
         sc->slot_cap = nl->slot_cap;
     }
+    return SB_OK;
+}
+
+static int sc_slots(sb_softcore* sc, sb_neighbor_list* nl, cudaStream_t s) {
+    SB_TRY(sc_slots_alloc(sc, nl));
     k_sc_pack<<<(nl->slot_cap + 255) / 256, 256, 0, s>>>(nl->meta, nl->slot_atom, sc->d_typeB,
                                                          sc->d_mask, sc->d_dq, sc->d_slot_ext,
                                                          sc->d_slot_dq);
@@ -828,4 +864,431 @@ extern "C" int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
         SB_CHECK_LAUNCH();
     }
     return SB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched FEP step: the sb_fep_step of many boxes (windows) in one launch per stage. Each box
+// keeps its own list, soft-core and PME modules; the batch gathers their device pointers and
+// constants into descriptors (SbFepBox, ScParams) and block tables (block -> box, block of box),
+// so that the pack, pair, spread, gather and finalize launches each cover all boxes. The FFTs
+// run one launch per stage per group of equal grid sizes. Every thread does what the same
+// thread of the box's own sb_fep_step does, and all sums are fixed point or keep their warps:
+// each box gets the bits of its own step.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
+    k_fep_pack_batch(const SbFepBox* __restrict__ B, const int2* __restrict__ tab, int dh) {
+    const int2 t = tab[blockIdx.x];
+    const SbFepBox& b = B[t.x];
+    const int s = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
+    if (dh && t.y == 0 && threadIdx.x < 4) b.hfix[threadIdx.x] = 0;
+    if (s >= b.meta[3]) return;
+    sb_pack_slot(s, b.slot_atom, b.uc, b.q, b.typeA, b.xq, b.stype, b.xq_prune, b.usx, b.usy,
+                 b.usz, b.move2, b.meta + 6);
+    sc_pack_slot(s, b.slot_atom, b.typeB, b.mask, b.dq, b.slot_ext, b.slot_dq);
+}
+
+// the ScParams fields that differ between the boxes of one pair launch
+struct ScBoxVar {
+    float sx, sy, sz, l, l_, cA, cB, dcA, dcB;
+    int slot_cap, ent_cap;
+};
+
+// the boxes of one launch share C's other fields, which stay kernel parameters (constant-bank
+// operands, as in k_pair_sc) while the box's own ones are loaded per block
+template <bool DH>
+__global__ void __launch_bounds__(128, 4) k_pair_sc_batch(ScParams C,
+                                                       const ScBoxVar* __restrict__ V,
+                                                       const SbFepBox* __restrict__ B,
+                                                       const int2* __restrict__ tab) {
+    const int2 t = tab[blockIdx.x];
+    const ScBoxVar v = V[t.x];
+    ScParams P = C;
+    P.sx = v.sx;
+    P.sy = v.sy;
+    P.sz = v.sz;
+    P.l = v.l;
+    P.l_ = v.l_;
+    P.cA = v.cA;
+    P.cB = v.cB;
+    P.dcA = v.dcA;
+    P.dcB = v.dcB;
+    P.slot_cap = v.slot_cap;
+    P.ent_cap = v.ent_cap;
+    const SbFepBox& b = B[t.x];
+    pair_sc_block<0, DH>(P, t.y, b.meta, b.cl_count, b.cl_ent, b.xq, b.stype, b.slot_ext,
+                         b.slot_dq, b.ABa, b.ABb, b.slot_atom, b.fix, b.hfix, nullptr, nullptr,
+                         nullptr);
+}
+
+static ScBoxVar sc_box_var(const ScParams& P) {
+    return ScBoxVar{P.sx, P.sy, P.sz, P.l, P.l_, P.cA, P.cB, P.dcA, P.dcB, P.slot_cap,
+                    P.ent_cap};
+}
+
+// the fields a pair launch takes from its first box
+static bool sc_same_common(const ScParams& a, const ScParams& b) {
+    if (a.rc2 != b.rc2 || a.beta != b.beta || a.beta2 != b.beta2 || a.tsp_beta != b.tsp_beta ||
+        a.s6 != b.s6 || a.s6min != b.s6min || a.wide != b.wide || a.ntA != b.ntA ||
+        a.ntB != b.ntB)
+        return false;
+    for (int k = 0; k < 6; k++)
+        if (a.gp[k] != b.gp[k]) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(1024) k_fep_finish_batch(const SbFepBox* __restrict__ B) {
+    const SbFepBox& b = B[blockIdx.x];
+    fep_finish_block(b.n, b.q, b.dq, b.hfix, b.self_coef, b.neutral2, b.lrc, b.dudl, nullptr);
+}
+
+struct SbFftGroup {
+    const SbFftPlan* plan;      // the plan of the group's first box (all share its sizes)
+    std::vector<int> boxes;
+    std::vector<SbFftBatchIo> io;  // what d_io holds
+    SbFftBatchIo* d_io = nullptr;
+    bool batched = false;       // false: the boxes' own plan calls, one after another
+    int fused = 0;
+};
+
+struct sb_fep_batch {
+    int nb = 0;
+    int dh = 0;
+    std::vector<sb_neighbor_list*> nls;
+    std::vector<sb_softcore*> scs;
+    std::vector<sb_pme*> pmes;
+    std::vector<SbFepBox> hbox;   // what the descriptors were built from (staleness check)
+    std::vector<ScParams> hP;
+    std::vector<float> lam;
+    SbFepBox* d_box = nullptr;
+    ScBoxVar* d_var = nullptr;
+    int2* d_tab = nullptr;
+    int off_slot = 0, n_slot = 0, off_spread = 0, n_spread = 0, off_atom = 0, n_atom = 0;
+    // pair launches: boxes with equal common parameters (usually all), their cluster blocks
+    struct PairGroup {
+        int first_box, off, n;
+    };
+    std::vector<PairGroup> pair_groups;
+    size_t smem = 0;              // dynamic shared memory of the pair launch (largest tables)
+    std::vector<SbFftGroup> groups;
+};
+
+static void fep_batch_free(sb_fep_batch* b) {
+    for (auto& g : b->groups) sb_free(g.d_io);
+    sb_free(b->d_box);
+    sb_free(b->d_var);
+    sb_free(b->d_tab);
+    delete b;
+}
+
+static SbFepBox fep_box_desc(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* p, const uint32_t* uc,
+                             const float* q, const int* es, const int* el, const int* en,
+                             float* frc, double* dudl) {
+    SbFepBox d{};
+    d.meta = nl->meta;
+    d.cl_count = nl->cl_count;
+    d.cl_ent = nl->cl_ent;
+    d.xq = nl->xq;
+    d.stype = nl->stype;
+    d.slot_atom = nl->slot_atom;
+    d.fix = nl->fix;
+    const bool pr = nl->prune_buffer > 0.f;
+    d.xq_prune = pr ? nl->xq_prune : nullptr;
+    const float half = 0.5f * nl->prune_buffer;
+    d.move2 = half * half;
+    d.usx = (1.0f / 4294967296.0f) * nl->box[0];
+    d.usy = (1.0f / 4294967296.0f) * nl->box[1];
+    d.usz = (1.0f / 4294967296.0f) * nl->box[2];
+    d.slot_cap = nl->slot_cap;
+    d.typeA = sc->d_typeA;
+    d.typeB = sc->d_typeB;
+    d.mask = sc->d_mask;
+    d.dq = sc->d_dq;
+    d.slot_ext = sc->d_slot_ext;
+    d.slot_dq = sc->d_slot_dq;
+    d.ABa = sc->d_ABa;
+    d.ABb = sc->d_ABb;
+    d.hfix = sc->d_hfix;
+    d.qfix = p->d_qfix;
+    d.theta = p->d_theta;
+    d.K0 = p->K[0];
+    d.K1 = p->K[1];
+    d.K2 = p->K[2];
+    d.ix = (float)p->K[0] / p->box[0];
+    d.iy = (float)p->K[1] / p->box[1];
+    d.iz = (float)p->K[2] / p->box[2];
+    const float be = p->beta;
+    const bool excl = es && el && en;
+    d.X = SbExclPass{nl->slot_atom, nl->atom_slot, excl ? es : nullptr, excl ? el : nullptr,
+                     excl ? en : nullptr, (1.0f / 4294967296.0f) * p->box[0],
+                     (1.0f / 4294967296.0f) * p->box[1], (1.0f / 4294967296.0f) * p->box[2],
+                     be, be * be, be * be * be, nullptr};
+    d.uc = uc;
+    d.q = q;
+    d.frc = frc;
+    d.dudl = dudl;
+    d.n = nl->n;
+    d.self_coef = -2.0 * (double)be / sqrt(M_PI);
+    d.neutral2 = 2.0 * p->neutralizing_factor;
+    const double V = (double)sc->box[0] * sc->box[1] * sc->box[2];
+    d.lrc = sc->lrc_ti / V;
+    return d;
+}
+
+static void fep_tab_add(std::vector<int2>& tab, int box, int blocks) {
+    for (int k = 0; k < blocks; k++) tab.push_back(make_int2(box, k));
+}
+
+extern "C" int sb_fep_batch_destroy(sb_fep_batch* b) {
+    if (!b) return SB_OK;
+    fep_batch_free(b);
+    return SB_OK;
+}
+
+extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
+                                   sb_softcore* const* scs, sb_pme* const* pmes,
+                                   const uint32_t* const* d_uint_crd,
+                                   const float* const* d_charge,
+                                   const int* const* d_excluded_list_start,
+                                   const int* const* d_excluded_list,
+                                   const int* const* d_excluded_numbers, float* const* d_frc,
+                                   double* d_dudl, sb_fep_batch** out) {
+    if (!out || n_boxes < 1 || !nls || !scs || !pmes || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_fep_batch_create: invalid argument");
+        return SB_ERR_ARG;
+    }
+    *out = nullptr;
+    for (int k = 0; k < n_boxes; k++) {
+        sb_neighbor_list* nl = nls[k];
+        sb_softcore* sc = scs[k];
+        sb_pme* p = pmes[k];
+        if (!nl || !sc || !p || !d_uint_crd[k] || !d_charge[k] || !d_frc[k]) {
+            sb_set_error("sb_fep_batch_create: box %d has a null module or buffer", k);
+            return SB_ERR_ARG;
+        }
+        if (nl->n != sc->n || p->n != sc->n) {
+            sb_set_error("sb_fep_batch_create: box %d: modules disagree on the atom count", k);
+            return SB_ERR_ARG;
+        }
+        if (nl->form != SB_FORM_FIXED || sc->form != SB_FORM_FIXED || p->form != SB_FORM_FIXED) {
+            sb_set_error("sb_fep_batch_create: box %d: needs the fixed-point form of all modules",
+                         k);
+            return SB_ERR_ARG;
+        }
+        if (nl->clu_cap > (1 << 30) / 4 || 4 * (long long)nl->n > (1ll << 30)) {
+            sb_set_error("sb_fep_batch_create: box %d is too large", k);
+            return SB_ERR_ARG;
+        }
+        SB_TRY(sb_nl_ensure_built(nl));
+    }
+    sb_fep_batch* b = new sb_fep_batch();
+    b->nb = n_boxes;
+    b->dh = d_dudl != nullptr;
+    std::vector<int2> tab;
+    int st = SB_OK;
+    for (int k = 0; k < n_boxes && !st; k++) {
+        b->nls.push_back(nls[k]);
+        b->scs.push_back(scs[k]);
+        b->pmes.push_back(pmes[k]);
+        st = sc_slots_alloc(scs[k], nls[k]);
+        if (st) break;
+        const int* es = d_excluded_list_start ? d_excluded_list_start[k] : nullptr;
+        const int* el = d_excluded_list ? d_excluded_list[k] : nullptr;
+        const int* en = d_excluded_numbers ? d_excluded_numbers[k] : nullptr;
+        b->hbox.push_back(fep_box_desc(nls[k], scs[k], pmes[k], d_uint_crd[k], d_charge[k], es,
+                                       el, en, d_frc[k], d_dudl ? d_dudl + k : nullptr));
+        b->hP.push_back(sc_params(scs[k], nls[k], pmes[k]->beta));
+        b->lam.push_back(scs[k]->lambda);
+        const size_t sm = sizeof(float2) * (size_t)(scs[k]->ntA * scs[k]->ntA +
+                                                    scs[k]->ntB * scs[k]->ntB);
+        b->smem = std::max(b->smem, sm);
+    }
+    if (!st) {
+        const int T = SB_FEP_BATCH_THREADS;
+        b->off_slot = (int)tab.size();
+        for (int k = 0; k < n_boxes; k++) fep_tab_add(tab, k, (nls[k]->slot_cap + T - 1) / T);
+        b->n_slot = (int)tab.size() - b->off_slot;
+        std::vector<int> pg(n_boxes, -1);
+        for (int k = 0; k < n_boxes; k++) {
+            if (pg[k] >= 0) continue;
+            sb_fep_batch::PairGroup g{k, (int)tab.size(), 0};
+            for (int j = k; j < n_boxes; j++) {
+                if (pg[j] >= 0 || !sc_same_common(b->hP[k], b->hP[j])) continue;
+                pg[j] = (int)b->pair_groups.size();
+                fep_tab_add(tab, j, (nls[j]->clu_cap + 3) / 4);
+            }
+            g.n = (int)tab.size() - g.off;
+            b->pair_groups.push_back(g);
+        }
+        b->off_spread = (int)tab.size();
+        for (int k = 0; k < n_boxes; k++) fep_tab_add(tab, k, (4 * nls[k]->n + T - 1) / T);
+        b->n_spread = (int)tab.size() - b->off_spread;
+        b->off_atom = (int)tab.size();
+        for (int k = 0; k < n_boxes; k++) fep_tab_add(tab, k, (nls[k]->n + T - 1) / T);
+        b->n_atom = (int)tab.size() - b->off_atom;
+        if (b->smem > 200 * 1024) {
+            sb_set_error("sb_fep_batch_create: LJ tables too large for shared memory");
+            st = SB_ERR_ARG;
+        }
+    }
+    // grids of equal sizes and transform family share batched FFT launches
+    for (int k = 0; k < n_boxes && !st; k++) {
+        const SbFftPlan* pl = &pmes[k]->plan;
+        SbFftGroup* g = nullptr;
+        for (auto& h : b->groups) {
+            const SbFftPlan* q = h.plan;
+            if (h.batched && sb_fft_batchable(pl) && q->K[0] == pl->K[0] && q->K[1] == pl->K[1] &&
+                q->K[2] == pl->K[2] && q->fused == pl->fused)
+                g = &h;
+        }
+        if (!g) {
+            b->groups.push_back(SbFftGroup());
+            g = &b->groups.back();
+            g->plan = pl;
+            g->batched = sb_fft_batchable(pl);
+            g->fused = pl->fused;
+        }
+        g->boxes.push_back(k);
+    }
+    for (auto& g : b->groups) {
+        if (st || !g.batched) continue;
+        std::vector<SbFftBatchIo>& io = g.io;
+        for (int k : g.boxes) {
+            sb_pme* p = pmes[k];
+            io.push_back(SbFftBatchIo{p->d_qfix, p->d_spec, p->d_theta, p->d_bc, nullptr});
+        }
+        st = sb_malloc((void**)&g.d_io, sizeof(SbFftBatchIo) * io.size(), "FEP batch FFT table");
+        if (!st && cudaMemcpy(g.d_io, io.data(), sizeof(SbFftBatchIo) * io.size(),
+                              cudaMemcpyHostToDevice) != cudaSuccess) {
+            sb_set_error("sb_fep_batch_create: FFT table upload failed");
+            st = SB_ERR_CUDA;
+        }
+    }
+    if (!st) st = sb_malloc((void**)&b->d_box, sizeof(SbFepBox) * n_boxes, "FEP batch boxes");
+    if (!st) st = sb_malloc((void**)&b->d_var, sizeof(ScBoxVar) * n_boxes, "FEP batch params");
+    std::vector<ScBoxVar> var;
+    for (const ScParams& P : b->hP) var.push_back(sc_box_var(P));
+    if (!st) st = sb_malloc((void**)&b->d_tab, sizeof(int2) * tab.size(), "FEP batch tables");
+    if (!st && (cudaMemcpy(b->d_box, b->hbox.data(), sizeof(SbFepBox) * n_boxes,
+                           cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(b->d_var, var.data(), sizeof(ScBoxVar) * n_boxes,
+                           cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(b->d_tab, tab.data(), sizeof(int2) * tab.size(),
+                           cudaMemcpyHostToDevice) != cudaSuccess)) {
+        sb_set_error("sb_fep_batch_create: descriptor upload failed");
+        st = SB_ERR_CUDA;
+    }
+    if (!st && b->smem > 40 * 1024) {
+        const cudaError_t e1 = cudaFuncSetAttribute(
+            k_pair_sc_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+        const cudaError_t e2 = cudaFuncSetAttribute(
+            k_pair_sc_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            sb_set_error("sb_fep_batch_create: shared memory attribute refused");
+            st = SB_ERR_CUDA;
+        }
+    }
+    if (st) {
+        fep_batch_free(b);
+        return st;
+    }
+    *out = b;
+    return SB_OK;
+}
+
+// the descriptors still describe the modules: same buffers, capacities, box and lambda
+static int fep_batch_current(const sb_fep_batch* b) {
+    for (int k = 0; k < b->nb; k++) {
+        const sb_neighbor_list* nl = b->nls[k];
+        const sb_softcore* sc = b->scs[k];
+        const sb_pme* p = b->pmes[k];
+        const SbFepBox& d = b->hbox[k];
+        const bool pr = nl->prune_buffer > 0.f;
+        const float half = 0.5f * nl->prune_buffer;
+        if (!nl->built || nl->meta != d.meta || nl->cl_ent != d.cl_ent || nl->xq != d.xq ||
+            nl->fix != d.fix || nl->slot_cap != d.slot_cap || nl->ent_cap != b->hP[k].ent_cap ||
+            (pr ? nl->xq_prune : nullptr) != d.xq_prune || half * half != d.move2 ||
+            (1.0f / 4294967296.0f) * nl->box[0] != d.usx ||
+            (1.0f / 4294967296.0f) * nl->box[1] != d.usy ||
+            (1.0f / 4294967296.0f) * nl->box[2] != d.usz || sc->d_slot_ext != d.slot_ext ||
+            sc->d_slot_dq != d.slot_dq || sc->lambda != b->lam[k] || p->d_qfix != d.qfix ||
+            p->d_theta != d.theta || (float)p->K[0] / p->box[0] != d.ix ||
+            (float)p->K[1] / p->box[1] != d.iy || (float)p->K[2] / p->box[2] != d.iz ||
+            p->beta != d.X.beta) {
+            sb_set_error("sb_fep_batch_step: box %d changed (box, lambda, list capacity or "
+                         "pruning) since sb_fep_batch_create; create the batch again", k);
+            return SB_ERR_STATE;
+        }
+    }
+    for (const auto& g : b->groups) {
+        if (!g.batched) continue;
+        for (size_t i = 0; i < g.boxes.size(); i++) {
+            const sb_pme* p = b->pmes[g.boxes[i]];
+            const SbFftBatchIo& io = g.io[i];
+            if (!sb_fft_batchable(&p->plan) || p->plan.fused != g.fused ||
+                p->d_spec != io.spec || p->d_bc != io.bc) {
+                sb_set_error("sb_fep_batch_step: box %d changed its FFT since "
+                             "sb_fep_batch_create; create the batch again", g.boxes[i]);
+                return SB_ERR_STATE;
+            }
+        }
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_fep_batch_step(sb_fep_batch* b, void* stream) {
+    if (!b) {
+        sb_set_error("sb_fep_batch_step: null handle");
+        return SB_ERR_ARG;
+    }
+    SB_TRY(fep_batch_current(b));
+    cudaStream_t s = sb_stream(stream);
+    const int2* tab = b->d_tab;
+    k_fep_pack_batch<<<b->n_slot, SB_FEP_BATCH_THREADS, 0, s>>>(b->d_box, tab + b->off_slot,
+                                                               b->dh);
+    SB_CHECK_LAUNCH();
+    for (const auto& g : b->pair_groups) {
+        const ScParams& C = b->hP[g.first_box];
+        if (b->dh)
+            k_pair_sc_batch<true><<<g.n, 128, b->smem, s>>>(C, b->d_var, b->d_box, tab + g.off);
+        else
+            k_pair_sc_batch<false><<<g.n, 128, b->smem, s>>>(C, b->d_var, b->d_box, tab + g.off);
+        SB_CHECK_LAUNCH();
+    }
+    SB_TRY(sb_pme_batch_spread(b->d_box, tab + b->off_spread, b->n_spread, s));
+    for (const auto& g : b->groups) {
+        if (g.batched) {
+            const int n = (int)g.boxes.size();
+            SB_TRY(sb_fft_batch_forward(g.plan, g.d_io, n, s));
+            SB_TRY(sb_fft_batch_convolve(g.plan, g.d_io, n, 0, s));
+            SB_TRY(sb_fft_batch_inverse(g.plan, g.d_io, n, s));
+        } else {
+            for (int k : g.boxes) {
+                sb_pme* p = b->pmes[k];
+                SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
+                SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, 0, s,
+                                         &p->rec_nparts));
+                SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+            }
+        }
+    }
+    SB_TRY(sb_pme_batch_gather(b->d_box, tab + b->off_atom, b->n_atom, b->dh, s));
+    SB_TRY(sb_pme_batch_slots(b->d_box, tab + b->off_slot, b->n_slot, b->dh, s));
+    if (b->dh) {
+        k_fep_finish_batch<<<b->nb, 1024, 0, s>>>(b->d_box);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_fep_batch_launches(const sb_fep_batch* b) {
+    if (!b) return -1;
+    // pack, spread, gather, slots (+ finish), the pair launches
+    int n = 4 + (b->dh ? 1 : 0) + (int)b->pair_groups.size();
+    for (const auto& g : b->groups) {
+        if (g.batched)
+            n += 3 + (g.plan->fused ? 0 : 2);
+        else
+            n += (int)g.boxes.size() * (g.plan->fused ? 3 : 5);
+    }
+    return n;
 }

@@ -6,16 +6,19 @@ A/B LJ types and tables, the perturbation mask). ``step()`` is one force evaluat
 dU/dlambda (``sb_fep_step``: soft-core LJ + direct, exclusion correction, reciprocal space, PME
 cross terms and the long-range correction, no host synchronisation).
 
-``FepBatch(systems)`` runs many such boxes of uneven size together: every box keeps its own
-modules and list; one force step of all boxes is captured once as a CUDA graph whose branches run
-the boxes concurrently on separate streams, and each step replays it. The number of streams the
-boxes are spread over is picked by timing (``tune``). List rebuilds run between replays.
+``FepBatch(systems)`` runs many such boxes of uneven size together. Each box keeps its own
+modules and list. In the default mode (``mode="kernels"``) one force step of all boxes is
+``sb_fep_batch_step``: one launch per stage over all boxes' slots, clusters and atoms through
+per-box descriptors, plus one launch per FFT stage per group of equal grid sizes; the step is
+captured once as a CUDA graph. ``mode="streams"`` keeps each box's own ``sb_fep_step`` launches
+as concurrent branches of one graph, spread over a tuned number of streams. Both give every box
+the bits of its own step. List rebuilds run between replays.
 """
 
 import numpy as np
 
-from . import (FORM_FIXED, NeighborList, ParticleMeshEwald, SoftCore, _require_cuda,
-               crd_to_uint_crd, fep_step, pme_ti_cross)
+from . import (FORM_FIXED, FepBatchStep, NeighborList, ParticleMeshEwald, SoftCore,
+               _require_cuda, crd_to_uint_crd, fep_step, pme_ti_cross)
 
 
 def _scaled(x, f):
@@ -96,34 +99,60 @@ class FepEngine:
 class FepBatch:
     """Many FEP boxes on one GPU, one captured CUDA graph per force step."""
 
-    def __init__(self, systems, refresh_interval=20):
+    def __init__(self, systems, refresh_interval=20, mode="kernels"):
         torch = _require_cuda()
+        if mode not in ("kernels", "streams"):
+            raise ValueError("mode must be 'kernels' or 'streams'")
         self.torch = torch
+        self.mode = mode
         self.engines = [FepEngine(s, refresh_interval=refresh_interval) for s in systems]
         self.refresh_interval = refresh_interval
         self.dudl = torch.zeros(len(self.engines), dtype=torch.float64, device="cuda")
+        # one force array for all boxes: a single clear per step
+        self.frc = torch.zeros((self.atoms, 3), dtype=torch.float32, device="cuda")
+        o = 0
         for k, e in enumerate(self.engines):
             e.dudl = self.dudl[k:k + 1]
+            e.frc = self.frc[o:o + e.n]
+            o += e.n
         self.graph = None
         self.n_streams = None
+        self.batch = None
         self.count = 0
 
     @property
     def atoms(self):
         return sum(e.n for e in self.engines)
 
+    @property
+    def launches(self):
+        """Kernel launches of one captured step (the force clear included)."""
+        if self.mode == "kernels":
+            return 1 + self.batch.launches
+        return None
+
     def rebuild(self):
         for e in self.engines:
             e.update_list(forced=1)
             e.to_uint()
 
-    def _eager_step(self):
-        for e in self.engines:
-            e.frc.zero_()
-            e.step()
+    def _batch(self):
+        if self.batch is None:
+            self.batch = FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc)
+                                       for e in self.engines], self.dudl)
+        return self.batch
 
-    def capture(self, n_streams):
-        """Capture one force step of every box; box k runs on stream k mod n_streams."""
+    def _eager_step(self):
+        self.frc.zero_()
+        if self.mode == "kernels":
+            self._batch().step()
+        else:
+            for e in self.engines:
+                e.step()
+
+    def capture(self, n_streams=1):
+        """Capture one force step of every box. In streams mode box k runs on stream
+        k mod n_streams."""
         torch = self.torch
         self._eager_step()  # first calls size per-list scratch outside the capture
         torch.cuda.synchronize()
@@ -131,16 +160,19 @@ class FepBatch:
         streams = [torch.cuda.Stream() for _ in range(n_streams)]
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=main):
-            cur = torch.cuda.current_stream()
-            for st in streams:
-                st.wait_stream(cur)
-            for k, e in enumerate(self.engines):
-                st = streams[k % n_streams]
-                with torch.cuda.stream(st):
-                    e.frc.zero_()
-                    e.step(stream=st)
-            for st in streams:
-                cur.wait_stream(st)
+            if self.mode == "kernels":
+                self.frc.zero_()
+                self.batch.step()
+            else:
+                cur = torch.cuda.current_stream()
+                self.frc.zero_()
+                for st in streams:
+                    st.wait_stream(cur)
+                for k, e in enumerate(self.engines):
+                    with torch.cuda.stream(streams[k % n_streams]):
+                        e.step(stream=streams[k % n_streams])
+                for st in streams:
+                    cur.wait_stream(st)
         self.graph = g
         self.n_streams = n_streams
         self._streams = (main, streams)
@@ -153,25 +185,32 @@ class FepBatch:
         self.graph.replay()
         self.count += 1
 
-    def tune(self, candidates=(1, 4, 8, 16, 48), reps=5):
-        """Pick the stream count of the captured step by timing its replay."""
+    def _replay_ms(self, reps):
         torch = self.torch
+        for _ in range(2):
+            self.graph.replay()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            self.graph.replay()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def tune(self, candidates=(1, 4, 8, 16, 48), reps=5):
+        """Capture the step; in streams mode pick the stream count by timing the replay.
+        Returns (streams, ms per replay)."""
+        if self.mode == "kernels":
+            self.capture(1)
+            return 1, self._replay_ms(reps)
         best = None
         for ns in candidates:
             if ns > len(self.engines):
                 continue
             self.capture(ns)
-            for _ in range(2):
-                self.graph.replay()
-            torch.cuda.synchronize()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record()
-            for _ in range(reps):
-                self.graph.replay()
-            b.record()
-            torch.cuda.synchronize()
-            ms = a.elapsed_time(b) / reps
+            ms = self._replay_ms(reps)
             if best is None or ms < best[1]:
                 best = (ns, ms)
         self.capture(best[0])

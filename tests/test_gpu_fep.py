@@ -3,8 +3,9 @@ FP64 oracle, on FEP boxes at several lambda values.
 
 Tolerances: forces relative RMS <= 1e-5 against FP64; dU/dlambda and its parts within 1e-5 of
 the sum of the parts' magnitudes; the fused step against the module sequence to float rounding
-of the final conversion (1e-6) and bit-identical run to run; the batched graph replay identical
-to the boxes stepped one at a time.
+of the final conversion (1e-6) and bit-identical run to run; the batched step (one launch per
+stage over all boxes, and the per-box graph branches) identical to the boxes stepped one at a
+time.
 """
 
 import numpy as np
@@ -130,23 +131,59 @@ def test_plain_form_matches_oracle(name, cuda, oracle_lib):
         assert abs(parts[k] - ref[k]) <= DUDL_TOL * scale, (k, parts[k], ref[k])
 
 
-def test_batched_graph_matches_single_boxes(cuda):
+def _batch_boxes():
+    # three boxes share the 30^3 grid (one batched FFT group of plane kernels), the 2600-water
+    # box runs the pass-by-pass register transforms (a batched group without the plane kernel)
+    # and the 1700-water box the generic stage kernels (its own FFT launches)
+    return [systems.fep_box(n, lam, 100 + k) for k, (n, lam) in
+            enumerate([(500, 0.0), (1700, 0.2), (800, 0.5), (2600, 0.8), (650, 1.0)])]
+
+
+@pytest.mark.parametrize("mode", ["kernels", "streams"])
+def test_batched_graph_matches_single_boxes(cuda, mode):
+    import sponge_b200
     from sponge_b200.fep import FepBatch
-    boxes = [systems.fep_box(n, lam, 100 + k) for k, (n, lam) in
-             enumerate([(500, 0.0), (1700, 0.2), (800, 0.5), (2600, 0.8), (650, 1.0)])]
-    batch = FepBatch(boxes)
+    batch = FepBatch(_batch_boxes(), mode=mode)
+    batch.engines[1].pme.set_fft_variant(sponge_b200.FFT_GENERIC)
+    batch.engines[3].pme.set_fft_variant(sponge_b200.FFT_LINES)
     batch.rebuild()
     # one box at a time, eagerly
-    single = []
     for e in batch.engines:
         e.frc.zero_()
         e.step()
     cuda.cuda.synchronize()
     single = [(e.frc.cpu().numpy().copy(), float(e.dudl.item())) for e in batch.engines]
-    best = batch.tune(candidates=(1, 2, 5), reps=2)
-    assert best[0] in (1, 2, 5)
-    batch.graph.replay()
+    if mode == "kernels":
+        best = batch.tune(reps=2)
+        assert best[0] == 1
+        # pack, pair, spread, gather, finalize, finish, the force clear and the FFTs: 3 for the
+        # plane group, 5 for the pass-by-pass group, 5 for the generic box
+        assert batch.launches == 7 + 3 + 5 + 5, batch.launches
+    else:
+        best = batch.tune(candidates=(1, 2, 5), reps=2)
+        assert best[0] in (1, 2, 5)
+    for rep in range(2):  # the replay leaves every accumulator clear for the next one
+        batch.graph.replay()
+        cuda.cuda.synchronize()
+        for e, (f, d) in zip(batch.engines, single):
+            assert np.array_equal(e.frc.cpu().numpy(), f)
+            assert float(e.dudl.item()) == d
+
+
+def test_batch_refuses_changed_box(cuda):
+    import sponge_b200
+    from sponge_b200 import FepBatchStep
+    from sponge_b200.fep import FepEngine
+    engines = [FepEngine(s) for s in _batch_boxes()[:2]]
+    for e in engines:
+        e.update_list(forced=1)
+        e.to_uint()
+    dudl = cuda.zeros(2, dtype=cuda.float64, device="cuda")
+    b = FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc) for e in engines],
+                     dudl)
+    b.step()
     cuda.cuda.synchronize()
-    for e, (f, d) in zip(batch.engines, single):
-        assert np.array_equal(e.frc.cpu().numpy(), f)
-        assert float(e.dudl.item()) == d
+    assert float(dudl[0].item()) != 0.0
+    engines[1].sc.set_lambda(0.7)
+    with pytest.raises(sponge_b200.SpongeError, match="create the batch again"):
+        b.step()
