@@ -231,9 +231,10 @@ def run_fep(args, rank, world, local):
     """48 uneven water boxes with a vanishing 20-atom solute, one lambda each, batched on each
     GPU: one launch per stage over all boxes (sb_fep_batch_step) under one captured CUDA graph
     (boxes sharded over ranks, the per-window dU/dlambda gathered at the end). Baselines on the
-    same GPU: the per-box steps as concurrent graph branches on tuned streams, the 48 boxes one
-    after another through the fixed-form fused step without the graph, and through the
-    plain-form modules (float atomics, per-atom lists, cuFFT)."""
+    same GPU: the per-box steps as concurrent graph branches on tuned streams (same steps, same
+    list rebuilds), and, as force steps without list rebuilds, the 48 boxes one after another
+    through the fixed-form fused step without the graph and through the plain-form modules
+    (float atomics, per-atom lists, cuFFT)."""
     import torch
     from sponge_b200 import FORM_PLAIN, systems
     from sponge_b200.fep import FepBatch, FepEngine, box_cost, shard_boxes
@@ -277,6 +278,10 @@ def run_fep(args, rank, world, local):
     dudl[torch.tensor(mine, device="cuda")] = batch.dudl
     if dist is not None:
         dist.all_reduce(dudl)
+    # the two parts of a step: the captured force step of all boxes, and the list rebuild of
+    # all boxes (every refresh_interval steps)
+    replay_ms = timed(batch.graph.replay, 20)
+    rebuild_ms = timed(batch.rebuild, 3)
     launches = None
     if batch.launches is not None:
         rebuilds = sum(1 for c in range(batch.count - args.steps, batch.count)
@@ -288,7 +293,8 @@ def run_fep(args, rank, world, local):
             other = FepBatch([boxes[k] for k in mine], mode="streams")
             other.rebuild()
             other.tune()
-            base_streams = timed(other.step, max(10, args.steps // 4)) * len(boxes) / len(mine)
+            # the same steps and rebuild phase as the timed batch
+            base_streams = timed(other.step, args.steps) * len(boxes) / len(mine)
             del other
 
         def fixed_sequential():
@@ -326,9 +332,11 @@ def run_fep(args, rank, world, local):
                                "sigma 3 A, lambda = k/47, rc 9 A, skin 2 A, PME ~1 A grids, "
                                "list rebuilt every 20 steps",
                    "atoms": atoms, "boxes_per_rank": len(mine), "mode": args.fep_mode,
-                   "graph_streams": ns, "parallelism": "boxes sharded over ranks"},
+                   "graph_branches": ns, "parallelism": "boxes sharded over ranks"},
         "gpu_launches": launches,
         "gpu_launches_per_step": batch.launches,
+        "force_step_ms": replay_ms, "rebuild_ms": rebuild_ms,
+        "rebuild_interval": batch.refresh_interval,
         "dudl_per_window": [float(x) for x in dudl.cpu().numpy()],
         "baselines_ns_per_day": {
             "per_box_graph_branches":

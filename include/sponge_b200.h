@@ -422,6 +422,15 @@ SB_API int sb_sc_destroy(sb_softcore* sc);
  * lambda-mixed long-range correction factor. */
 SB_API int sb_sc_set_lambda(sb_softcore* sc, float lambda);
 
+/* The split form of sb_fep_step / sb_fep_batch_step (no reference counterpart): the perturbed
+ * atoms are those with a mask or a charge change, or whose (A, B) type pair makes the B-state
+ * table differ from the A-state table against the other atoms. With at most 512 of them and at
+ * most one atom in eight, the pairs of two unperturbed atoms (whose soft-core energy is their
+ * A-state energy, with no dH/dlambda) run through the packed LJ + Ewald kernel and the pairs with
+ * a perturbed atom through a soft-core pass over the perturbed atoms. *h_split = 1 when the
+ * module uses it, *h_n_perturbed = the perturbed atom count. */
+SB_API int sb_sc_split_form(const sb_softcore* sc, int* h_split, int* h_n_perturbed);
+
 /* LJ_SOFT_CORE::LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial: soft-core LJ + Ewald
  * direct force over the list of `nl` added to d_frc (d_charge holds the charges at lambda), with
  * the per-atom energy / LJ virial / direct energy outputs of sb_lj_pme_direct_force. */
@@ -466,8 +475,10 @@ SB_API int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
  * launch per stage over all boxes (pack, soft-core pair, spread, gather, finalize, dU/dlambda
  * finish) plus one launch per FFT stage per group of equal grid sizes. Box k reads
  * d_uint_crd[k], d_charge[k] and its exclusion lists, adds its forces into d_frc[k] and writes
- * its dU/dlambda to d_dudl[k] (d_dudl: n_boxes device doubles, or NULL for forces only). Each
- * box gets the same bits as its own sb_fep_step.
+ * its dU/dlambda to the device double d_dudl[k] (d_dudl: n_boxes pointers, or NULL for forces
+ * only). Each box gets the same bits as its own sb_fep_step. The pair stage, the soft-core
+ * passes and the reciprocal chain run on library-owned streams forked from and joined back
+ * into `stream` (capturable in a CUDA graph).
  * The batch records the modules' buffers, capacities, boxes and lambdas at creation: after a
  * box or lambda change (sb_*_update_volume, sb_sc_set_lambda) or sb_nl_set_prune, create it
  * again (sb_fep_batch_step refuses with SB_ERR_STATE). Every list must be built before
@@ -481,7 +492,7 @@ SB_API int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
                                const int* const* d_excluded_list_start,
                                const int* const* d_excluded_list,
                                const int* const* d_excluded_numbers, float* const* d_frc,
-                               double* d_dudl, sb_fep_batch** out);
+                               double* const* d_dudl, sb_fep_batch** out);
 SB_API int sb_fep_batch_step(sb_fep_batch* batch, void* stream);
 /* kernel launches of one sb_fep_batch_step */
 SB_API int sb_fep_batch_launches(const sb_fep_batch* batch);

@@ -93,6 +93,7 @@ _SIGS = {
     "sb_sc_dh_dlambda": [_vp, _vp, _vp, _vp, _f, _vp, _vp],
     "sb_pme_ti_cross": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "sb_fep_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sb_sc_split_form": [_vp, _vp, _vp],
     "sb_fep_batch_create": [_i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "sb_fep_batch_step": [_vp, _vp],
     "sb_fep_batch_launches": [_vp],
@@ -490,6 +491,13 @@ class SoftCore:
                                   self.lambda_lj, float(alpha), float(p), float(sigma),
                                   float(sigma_min), int(form), ctypes.byref(self.handle)))
 
+    @property
+    def split_form(self):
+        """(uses the split form, perturbed atom count) of the fused FEP step."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(lib().sb_sc_split_form(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return bool(a.value), int(b.value)
+
     def set_lambda(self, lambda_lj):
         self.lambda_lj = float(lambda_lj)
         _check(lib().sb_sc_set_lambda(self.handle, self.lambda_lj))
@@ -541,24 +549,26 @@ def pme_ti_cross(pme, uint_crd, charge, charge_B_A, excl, stream=None):
 
 class FepBatchStep:
     """sb_fep_batch_*: the fused FEP step of many boxes in one launch per stage. ``boxes`` is a
-    list of (nl, sc, pme, uint_crd, charge, (excl_start, excl_list, excl_numbers), frc); box k's
-    dU/dlambda goes to dudl[k] (a float64 CUDA tensor of len(boxes) elements, or None). The
-    tensors must outlive the batch (their device addresses are stored at creation)."""
+    list of (nl, sc, pme, uint_crd, charge, (excl_start, excl_list, excl_numbers), frc, dudl),
+    dudl a 1-element float64 CUDA tensor receiving the box's dU/dlambda (None in every box for
+    forces only). The tensors must outlive the batch (their device addresses are stored at
+    creation)."""
 
-    def __init__(self, boxes, dudl=None):
+    def __init__(self, boxes):
         n = len(boxes)
         arr = lambda: (_vp * n)()
-        nls, scs, pmes, uc, q, es, el, en, frc = (arr() for _ in range(9))
-        for k, (nl, sc, pme, u, c, excl, f) in enumerate(boxes):
+        nls, scs, pmes, uc, q, es, el, en, frc, du = (arr() for _ in range(10))
+        want = boxes[0][7] is not None
+        for k, (nl, sc, pme, u, c, excl, f, d) in enumerate(boxes):
+            if (d is not None) != want:
+                raise SpongeError("dudl must be given for every box or for none")
             nls[k], scs[k], pmes[k] = nl.handle, sc.handle, pme.handle
-            uc[k], q[k], frc[k] = _ptr(u), _ptr(c), _ptr(f)
+            uc[k], q[k], frc[k], du[k] = _ptr(u), _ptr(c), _ptr(f), _ptr(d)
             es[k], el[k], en[k] = (_ptr(t) for t in excl)
-        if dudl is not None and dudl.numel() < n:
-            raise SpongeError("dudl holds fewer than %d values" % n)
-        self._keep = (boxes, dudl)
+        self._keep = boxes
         h = _vp()
-        _check(lib().sb_fep_batch_create(n, nls, scs, pmes, uc, q, es, el, en, frc, _ptr(dudl),
-                                         ctypes.byref(h)))
+        _check(lib().sb_fep_batch_create(n, nls, scs, pmes, uc, q, es, el, en, frc,
+                                         du if want else None, ctypes.byref(h)))
         self.handle = h
 
     @property

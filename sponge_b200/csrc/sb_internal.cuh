@@ -390,6 +390,18 @@ struct SbFepBox {
     const float2* ABa;
     const float2* ABb;
     long long* hfix;  // [4] dH/dlambda parts: LJ, direct, reciprocal, correction
+    double* sums;     // [3] FP64 sums of q dq, q, dq (self term)
+    // split form (sb_softcore split != 0): the A-state square table with a zero ghost type
+    // (ntA) for the packed kernel, each atom's A type or the ghost type, the perturbed atoms
+    int split;
+    int ghost;
+    const int* tu;
+    const float2* ABu;
+    const int* pert;
+    int npert;
+    int2* ppairs;  // pairs with a perturbed atom found this step: {perturbed index, slot}
+    int* pcount;
+    int pcap;
     // reciprocal space
     long long* qfix;
     const float* theta;
@@ -404,6 +416,19 @@ struct SbFepBox {
     int n;
     double self_coef, neutral2, lrc;
 };
+
+// FEP split form: the packed pair kernel over the unperturbed pairs of a box packed by the FEP
+// step (sb_pair.cu); the batched form over several boxes' clusters, grouped by common parameters
+bool sb_pair_fep_packed(const sb_neighbor_list* nl, float cutoff, float beta);
+int sb_pair_fep(sb_neighbor_list* nl, const float2* d_AB, int ntypes, float cutoff, float beta,
+                cudaStream_t s);
+struct SbX2Batch;
+int sb_pair_batch_create(int nb, const int* box_ids, sb_neighbor_list* const* nls,
+                         const int* ntypes, const float* cutoffs, const float* betas, int n_all,
+                         SbX2Batch** out);
+int sb_pair_batch_launch(const SbX2Batch* x, const SbFepBox* d_boxes, cudaStream_t s);
+int sb_pair_batch_launches(const SbX2Batch* x);
+void sb_pair_batch_destroy(SbX2Batch* x);
 
 // batched stages over all boxes; tab[b] = {box, block of that box} for every launched block
 int sb_pme_batch_spread(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, cudaStream_t s);

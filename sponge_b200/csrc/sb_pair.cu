@@ -269,14 +269,14 @@ extern "C" int sb_lj_destroy(sb_lennard_jones* lj) {
     return SB_OK;
 }
 
-static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list* nl,
-                              float beta) {
+static PairParams pair_params_of(const sb_neighbor_list* nl, int ntypes, float cutoff,
+                                 float beta) {
     PairParams P;
     P.sx = (1.0f / 4294967296.0f) * nl->box[0];
     P.sy = (1.0f / 4294967296.0f) * nl->box[1];
     P.sz = (1.0f / 4294967296.0f) * nl->box[2];
-    P.rc = lj->cutoff;
-    P.rc2 = lj->cutoff * lj->cutoff;
+    P.rc = cutoff;
+    P.rc2 = cutoff * cutoff;
     P.beta = beta;
     P.beta2 = beta * beta;
     P.beta3 = beta * beta * beta;
@@ -284,19 +284,24 @@ static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list
     const double pc[6] = {SB_EWALD_P5, SB_EWALD_P4, SB_EWALD_P3,
                           SB_EWALD_P2, SB_EWALD_P1, SB_EWALD_P0};
     for (int k = 0; k < 6; k++) P.gp[k] = (float)(b3 * pc[k]);
-    const double brc = (double)beta * lj->cutoff;
+    const double brc = (double)beta * cutoff;
     P.wide = brc * brc > 8.9;
-    P.nt = lj->ntypes;
+    P.nt = ntypes;
     P.slot_cap = nl->slot_cap;
     P.ent_cap = nl->ent_cap;
     const bool pruned = nl->prune_buffer > 0.f && nl->cl_ent_in;
-    const float rb = lj->cutoff + nl->prune_buffer;
+    const float rb = cutoff + nl->prune_buffer;
     P.rb2 = pruned ? rb * rb : 0.f;
     P.prune = nl->meta + 6;
     P.cl_count_in = nl->cl_count_in;
     P.cl_ent_in = nl->cl_ent_in;
     P.xq_prune = nl->xq_prune;
     return P;
+}
+
+static PairParams pair_params(const sb_lennard_jones* lj, const sb_neighbor_list* nl,
+                              float beta) {
+    return pair_params_of(nl, lj->ntypes, lj->cutoff, beta);
 }
 
 static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float beta, int ev,
@@ -596,4 +601,167 @@ extern "C" int sb_lj_long_range_factor(sb_lennard_jones* lj, float* h_factor) {
     }
     *h_factor = (float)lj->long_range_factor;
     return SB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// FEP split form: the pairs of two unperturbed atoms of a soft-core box through the packed
+// kernel (force only), with the box's A-state table extended by a zero ghost type that the
+// FEP pack gives the perturbed atoms (their charges packed as 0), so that their pairs add
+// exactly zero here and are left to the soft-core pass over the perturbed atoms.
+// ---------------------------------------------------------------------------------------------
+bool sb_pair_fep_packed(const sb_neighbor_list* nl, float cutoff, float beta) {
+    return !pair_params_of(nl, 1, cutoff, beta).wide;
+}
+
+int sb_pair_fep(sb_neighbor_list* nl, const float2* d_AB, int ntypes, float cutoff, float beta,
+                cudaStream_t s) {
+    const PairParams P = pair_params_of(nl, ntypes, cutoff, beta);
+    if (P.wide) {
+        sb_set_error("sb_pair_fep: beta * cutoff beyond the packed kernel's Ewald fit");
+        return SB_ERR_ARG;
+    }
+    k_pair_x2<0><<<nl->clu_cap, 32, sizeof(float4) * 4 * ntypes, s>>>(
+        P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, d_AB, nl->slot_atom, nl->fix,
+        nullptr, nullptr, nullptr);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+}
+
+// the PairParams fields that differ between the boxes of one batched launch
+struct X2BoxVar {
+    float sx, sy, sz;
+    int nt, slot_cap, ent_cap;
+    float rb2;
+    int* prune;
+    int* cl_count_in;
+    uint32_t* cl_ent_in;
+    uint4* xq_prune;
+};
+
+// one-warp block per cluster of any box: tab[b] = {box, cluster}; C holds the common fields as
+// kernel parameters (constant-bank operands, as in k_pair_x2), the box's own ones are loaded
+__global__ void __launch_bounds__(32, 24) k_pair_x2_batch(PairParams C,
+                                                          const X2BoxVar* __restrict__ V,
+                                                          const SbFepBox* __restrict__ B,
+                                                          const int2* __restrict__ tab) {
+    extern __shared__ float4 ctab[];
+    const int2 t = tab[blockIdx.x];
+    const SbFepBox& b = B[t.x];
+    if (t.y >= b.meta[0]) return;
+    const X2BoxVar v = V[t.x];
+    PairParams P = C;
+    P.sx = v.sx;
+    P.sy = v.sy;
+    P.sz = v.sz;
+    P.nt = v.nt;
+    P.slot_cap = v.slot_cap;
+    P.ent_cap = v.ent_cap;
+    P.rb2 = v.rb2;
+    P.prune = v.prune;
+    P.cl_count_in = v.cl_count_in;
+    P.cl_ent_in = v.cl_ent_in;
+    P.xq_prune = v.xq_prune;
+    x2_cluster<0>(P, t.y, threadIdx.x & 31, ctab, b.cl_count, b.cl_ent, b.xq, b.stype, b.ABu,
+                  b.slot_atom, b.fix, nullptr, nullptr, nullptr);
+}
+
+struct SbX2Batch {
+    struct Group {
+        PairParams C;
+        int off, n;
+    };
+    std::vector<Group> groups;
+    X2BoxVar* d_var = nullptr;
+    int2* d_tab = nullptr;
+    size_t smem = 0;
+};
+
+static bool x2_same_common(const PairParams& a, const PairParams& b) {
+    if (a.rc2 != b.rc2 || a.rc != b.rc || a.beta != b.beta || a.beta2 != b.beta2 ||
+        a.beta3 != b.beta3 || a.wide != b.wide)
+        return false;
+    for (int k = 0; k < 6; k++)
+        if (a.gp[k] != b.gp[k]) return false;
+    return true;
+}
+
+void sb_pair_batch_destroy(SbX2Batch* x) {
+    if (!x) return;
+    sb_free(x->d_var);
+    sb_free(x->d_tab);
+    delete x;
+}
+
+int sb_pair_batch_create(int nb, const int* box_ids, sb_neighbor_list* const* nls,
+                         const int* ntypes, const float* cutoffs, const float* betas,
+                         int n_all, SbX2Batch** out) {
+    *out = nullptr;
+    SbX2Batch* x = new SbX2Batch();
+    std::vector<PairParams> P(nb);
+    std::vector<X2BoxVar> var(n_all);
+    for (int i = 0; i < nb; i++) {
+        P[i] = pair_params_of(nls[i], ntypes[i], cutoffs[i], betas[i]);
+        if (P[i].wide) {
+            sb_set_error("sb_pair_batch_create: box %d beyond the packed kernel's Ewald fit",
+                         box_ids[i]);
+            delete x;
+            return SB_ERR_ARG;
+        }
+        const PairParams& q = P[i];
+        var[box_ids[i]] = X2BoxVar{q.sx, q.sy, q.sz, q.nt, q.slot_cap, q.ent_cap, q.rb2,
+                                   q.prune, q.cl_count_in, q.cl_ent_in, q.xq_prune};
+        x->smem = std::max(x->smem, sizeof(float4) * 4 * (size_t)ntypes[i]);
+    }
+    std::vector<int2> tab;
+    std::vector<char> done(nb, 0);
+    for (int i = 0; i < nb; i++) {
+        if (done[i]) continue;
+        SbX2Batch::Group g{P[i], (int)tab.size(), 0};
+        for (int j = i; j < nb; j++) {
+            if (done[j] || !x2_same_common(P[i], P[j])) continue;
+            done[j] = 1;
+            for (int c = 0; c < nls[j]->clu_cap; c++) tab.push_back(make_int2(box_ids[j], c));
+        }
+        g.n = (int)tab.size() - g.off;
+        x->groups.push_back(g);
+    }
+    int st = SB_OK;
+    if (!tab.empty()) {
+        st = sb_malloc((void**)&x->d_var, sizeof(X2BoxVar) * var.size(), "x2 batch params");
+        if (!st) st = sb_malloc((void**)&x->d_tab, sizeof(int2) * tab.size(), "x2 batch table");
+        if (!st && (cudaMemcpy(x->d_var, var.data(), sizeof(X2BoxVar) * var.size(),
+                               cudaMemcpyHostToDevice) != cudaSuccess ||
+                    cudaMemcpy(x->d_tab, tab.data(), sizeof(int2) * tab.size(),
+                               cudaMemcpyHostToDevice) != cudaSuccess)) {
+            sb_set_error("sb_pair_batch_create: upload failed");
+            st = SB_ERR_CUDA;
+        }
+    }
+    if (!st && x->smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_pair_x2_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)x->smem) != cudaSuccess) {
+        sb_set_error("sb_pair_batch_create: shared memory attribute refused");
+        st = SB_ERR_CUDA;
+    }
+    if (st) {
+        sb_pair_batch_destroy(x);
+        return st;
+    }
+    *out = x;
+    return SB_OK;
+}
+
+int sb_pair_batch_launch(const SbX2Batch* x, const SbFepBox* d_boxes, cudaStream_t s) {
+    for (const auto& g : x->groups) {
+        if (!g.n) continue;
+        k_pair_x2_batch<<<g.n, 32, x->smem, s>>>(g.C, x->d_var, d_boxes, x->d_tab + g.off);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+int sb_pair_batch_launches(const SbX2Batch* x) {
+    int n = 0;
+    for (const auto& g : x->groups) n += g.n ? 1 : 0;
+    return n;
 }

@@ -52,7 +52,27 @@ struct sb_softcore {
     long long* d_hfix = nullptr;   // [4] fixed-point dH/dlambda: LJ, direct, reciprocal, correction
     double* d_red = nullptr;       // [8] FP64 scratch
     float* d_scratch_frc = nullptr;  // [3N] plain-form dH/dlambda pass (forces discarded)
+    // split form of the fused FEP step (split != 0): the pairs of two unperturbed atoms go
+    // through the packed LJ + Ewald kernel with the A-state table (for them the soft-core
+    // energy is the A-state energy and adds nothing to dH/dlambda), the pairs with a perturbed
+    // atom through a soft-core pass over the perturbed atoms
+    int npert = 0;
+    int split = 0;
+    int* d_pert = nullptr;         // [npert] perturbed atoms, ascending
+    int* d_tu = nullptr;           // [N] A type, or the ghost type ntA for a perturbed atom
+    float2* d_ABu = nullptr;       // [(ntA+1)^2] A-state square table, zero ghost row/column
+    double* d_sums = nullptr;      // [3] sums of q dq, q, dq of the last FEP step
+    int2* d_ppairs = nullptr;      // [pcap] pairs with a perturbed atom found by the step
+    int* d_pcount = nullptr;       // their count
+    int pcap = 0;
 };
+
+// pairs with a perturbed atom held per perturbed atom (more raise SB_STATUS_LIST_OVERFLOW)
+#define SB_SC_PAIRS_PER_ATOM 2048
+
+// at most this many perturbed atoms (and at most one in eight atoms) for the split form: its
+// soft-core pass tests every atom against every perturbed atom
+#define SB_SC_SPLIT_MAX 512
 
 struct ScParams {
     float sx, sy, sz, rc2;
@@ -392,15 +412,10 @@ __global__ void k_sc_zero(long long* __restrict__ h, int n) {
     if (t < n) h[t] = 0;
 }
 
-// PME cross-term and total: hfix [LJ, direct, reciprocal, correction] (fixed point) + self term
-// from FP64 sums of q dq, q, dq + long-range term -> out (FP64); optionally parts[7]. One block
-// of 1024 threads.
-__device__ __forceinline__ void fep_finish_block(int n, const float* __restrict__ q,
-                                                 const float* __restrict__ dq,
-                                                 const long long* __restrict__ hfix,
-                                                 double self_coef, double neutral2, double lrc,
-                                                 double* __restrict__ out,
-                                                 double* __restrict__ parts) {
+// FP64 sums of q dq, q and dq over the box (one block of 1024 threads, fixed order) -> out[0..2]
+__device__ __forceinline__ void fep_self_sums(int n, const float* __restrict__ q,
+                                              const float* __restrict__ dq,
+                                              double* __restrict__ out) {
     __shared__ double r1[1024], r2[1024], r3[1024];
     double a = 0, b = 0, c = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -421,29 +436,43 @@ __device__ __forceinline__ void fep_finish_block(int n, const float* __restrict_
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        const double lj = (double)hfix[0] * SB_DHDL_UNSCALE, dir = (double)hfix[1] * SB_DHDL_UNSCALE;
-        const double rec = (double)hfix[2] * SB_DHDL_UNSCALE, cor = (double)hfix[3] * SB_DHDL_UNSCALE;
-        const double self = self_coef * r1[0] + neutral2 * r2[0] * r3[0];
-        if (out) out[0] = lj + dir + rec + cor + self + lrc;
-        if (parts) {
-            parts[0] = lj;
-            parts[1] = dir;
-            parts[2] = rec;
-            parts[3] = self;
-            parts[4] = cor;
-            parts[5] = lrc;
-            parts[6] = lj + dir + rec + cor + self + lrc;
-        }
+        out[0] = r1[0];
+        out[1] = r2[0];
+        out[2] = r3[0];
     }
 }
 
-__global__ void __launch_bounds__(1024) k_fep_finish(int n, const float* __restrict__ q,
-                                                     const float* __restrict__ dq,
-                                                     const long long* __restrict__ hfix,
-                                                     double self_coef, double neutral2,
-                                                     double lrc, double* __restrict__ out,
-                                                     double* __restrict__ parts) {
-    fep_finish_block(n, q, dq, hfix, self_coef, neutral2, lrc, out, parts);
+// dU/dlambda: hfix [LJ, direct, reciprocal, correction] (fixed point) + the self term from the
+// sums of fep_self_sums + the long-range term -> out (FP64); optionally the parts[7]
+__device__ __forceinline__ void fep_combine(const long long* __restrict__ hfix,
+                                            const double* __restrict__ sums, double self_coef,
+                                            double neutral2, double lrc, double* __restrict__ out,
+                                            double* __restrict__ parts) {
+    const double lj = (double)hfix[0] * SB_DHDL_UNSCALE, dir = (double)hfix[1] * SB_DHDL_UNSCALE;
+    const double rec = (double)hfix[2] * SB_DHDL_UNSCALE, cor = (double)hfix[3] * SB_DHDL_UNSCALE;
+    const double self = self_coef * sums[0] + neutral2 * sums[1] * sums[2];
+    if (out) out[0] = lj + dir + rec + cor + self + lrc;
+    if (parts) {
+        parts[0] = lj;
+        parts[1] = dir;
+        parts[2] = rec;
+        parts[3] = self;
+        parts[4] = cor;
+        parts[5] = lrc;
+        parts[6] = lj + dir + rec + cor + self + lrc;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_fep_self(int n, const float* __restrict__ q,
+                                                   const float* __restrict__ dq,
+                                                   double* __restrict__ sums) {
+    fep_self_sums(n, q, dq, sums);
+}
+
+__global__ void k_fep_combine(const long long* __restrict__ hfix, const double* __restrict__ sums,
+                              double self_coef, double neutral2, double lrc,
+                              double* __restrict__ out) {
+    if (threadIdx.x == 0) fep_combine(hfix, sums, self_coef, neutral2, lrc, out, nullptr);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -512,7 +541,8 @@ extern "C" int sb_sc_destroy(sb_softcore* sc) {
     cudaDeviceSynchronize();
     void* ps[] = {sc->d_ABa, sc->d_ABb, sc->d_Aa, sc->d_Ba, sc->d_Ab, sc->d_Bb, sc->d_typeA,
                   sc->d_typeB, sc->d_mask, sc->d_dq, sc->d_slot_ext, sc->d_slot_dq, sc->d_hfix,
-                  sc->d_red, sc->d_scratch_frc};
+                  sc->d_red, sc->d_scratch_frc, sc->d_pert, sc->d_tu, sc->d_ABu,
+                  sc->d_ppairs, sc->d_pcount, sc->d_sums};
     for (void* x : ps) sb_free(x);
     delete sc;
     return SB_OK;
@@ -527,6 +557,62 @@ static std::vector<float2> square_table(int nt, const float* A, const float* B) 
             t[(size_t)a * nt + b] = make_float2(A[k], B[k]);
         }
     return t;
+}
+
+// The perturbed atoms of the split form: every atom with a mask or a charge change, and every
+// atom whose (A type, B type) pair is not interchangeable with the other unperturbed atoms' (the
+// A table between two unperturbed atoms must equal the B table between them, coefficient for
+// coefficient, so that the lambda-mixed pair is the A-state pair); the rest are unperturbed.
+static int sc_split_setup(sb_softcore* sc, const int* hmask, const float* hdq) {
+    const int n = sc->n, ntA = sc->ntA, ntB = sc->ntB;
+    std::vector<char> pert(n);
+    for (int i = 0; i < n; i++) pert[i] = hmask[i] != 0 || hdq[i] != 0.f;
+    auto tri = [](int a, int b) { return a > b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; };
+    for (bool changed = true; changed;) {
+        changed = false;
+        std::vector<char> seen((size_t)ntA * ntB, 0);
+        std::vector<int> combos;
+        for (int i = 0; i < n; i++) {
+            const int c = sc->htA[i] * ntB + sc->htB[i];
+            if (!pert[i] && !seen[c]) seen[c] = 1, combos.push_back(c);
+        }
+        std::vector<char> bad((size_t)ntA * ntB, 0);
+        for (int c1 : combos)
+            for (int c2 : combos) {
+                const int ka = tri(c1 / ntB, c2 / ntB), kb = tri(c1 % ntB, c2 % ntB);
+                if (sc->hA12a[ka] != sc->hA12b[kb] || sc->hB6a[ka] != sc->hB6b[kb]) bad[c1] = 1;
+            }
+        for (int i = 0; i < n; i++)
+            if (!pert[i] && bad[sc->htA[i] * ntB + sc->htB[i]]) pert[i] = 1, changed = true;
+    }
+    std::vector<int> plist;
+    for (int i = 0; i < n; i++)
+        if (pert[i]) plist.push_back(i);
+    sc->npert = (int)plist.size();
+    sc->split = sc->npert > 0 && sc->npert <= SB_SC_SPLIT_MAX && 8 * (long long)sc->npert <= n;
+    if (!sc->split) return SB_OK;
+    std::vector<int> tu(n);
+    for (int i = 0; i < n; i++) tu[i] = pert[i] ? ntA : sc->htA[i];
+    const int nu = ntA + 1;
+    std::vector<float2> abu((size_t)nu * nu, make_float2(0.f, 0.f));
+    for (int a = 0; a < ntA; a++)
+        for (int b = 0; b < ntA; b++) {
+            const int k = tri(a, b);
+            abu[(size_t)a * nu + b] = make_float2(sc->hA12a[k], sc->hB6a[k]);
+        }
+    SB_TRY(sb_malloc((void**)&sc->d_pert, sizeof(int) * plist.size(), "perturbed atoms"));
+    SB_TRY(sb_malloc((void**)&sc->d_tu, sizeof(int) * n, "split types"));
+    SB_TRY(sb_malloc((void**)&sc->d_ABu, sizeof(float2) * abu.size(), "split table"));
+    sc->pcap = sc->npert * std::min(n, SB_SC_PAIRS_PER_ATOM);
+    SB_TRY(sb_malloc((void**)&sc->d_ppairs, sizeof(int2) * sc->pcap, "perturbed pairs"));
+    SB_TRY(sb_malloc((void**)&sc->d_pcount, sizeof(int), "perturbed pair count"));
+    SB_CHECK_CUDA(cudaMemset(sc->d_pcount, 0, sizeof(int)));
+    SB_CHECK_CUDA(cudaMemcpy(sc->d_pert, plist.data(), sizeof(int) * plist.size(),
+                             cudaMemcpyHostToDevice));
+    SB_CHECK_CUDA(cudaMemcpy(sc->d_tu, tu.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    SB_CHECK_CUDA(cudaMemcpy(sc->d_ABu, abu.data(), sizeof(float2) * abu.size(),
+                             cudaMemcpyHostToDevice));
+    return SB_OK;
 }
 
 extern "C" int sb_sc_create(int n, int ntA, const float* hAA, const float* hAB, int ntB,
@@ -582,7 +668,8 @@ extern "C" int sb_sc_create(int n, int ntA, const float* hAA, const float* hAB, 
         (st = sb_malloc((void**)&sc->d_mask, sizeof(int) * n, "soft-core mask")) ||
         (st = sb_malloc((void**)&sc->d_dq, sizeof(float) * n, "soft-core dq")) ||
         (st = sb_malloc((void**)&sc->d_hfix, sizeof(long long) * 4, "dH/dlambda")) ||
-        (st = sb_malloc((void**)&sc->d_red, sizeof(double) * 8, "soft-core reduce"))) {
+        (st = sb_malloc((void**)&sc->d_red, sizeof(double) * 8, "soft-core reduce")) ||
+        (st = sb_malloc((void**)&sc->d_sums, sizeof(double) * 3, "FEP self sums"))) {
         sb_sc_destroy(sc);
         return st;
     }
@@ -602,7 +689,21 @@ extern "C" int sb_sc_create(int n, int ntA, const float* hAA, const float* hAB, 
         return SB_ERR_CUDA;
     }
     sc_lrc(sc);
+    if ((st = sc_split_setup(sc, hmask, hdq))) {
+        sb_sc_destroy(sc);
+        return st;
+    }
     *out = sc;
+    return SB_OK;
+}
+
+extern "C" int sb_sc_split_form(const sb_softcore* sc, int* h_split, int* h_n_perturbed) {
+    if (!sc || !h_split || !h_n_perturbed) {
+        sb_set_error("sb_sc_split_form: null argument");
+        return SB_ERR_ARG;
+    }
+    *h_split = sc->split;
+    *h_n_perturbed = sc->npert;
     return SB_OK;
 }
 
@@ -641,11 +742,8 @@ static int sc_slots(sb_softcore* sc, sb_neighbor_list* nl, cudaStream_t s) {
 }
 
 // fixed form: pack + soft-core pair kernel into the list's fixed-point force buffer
-static int sc_launch_fixed(sb_softcore* sc, sb_neighbor_list* nl, const uint32_t* uc,
-                           const float* q, float beta, int ev, bool dh, float* ae, float* av,
-                           float* ad, cudaStream_t s) {
-    SB_TRY(sb_nl_pack(nl, uc, q, sc->d_typeA, s));
-    SB_TRY(sc_slots(sc, nl, s));
+static int sc_pair_fixed(sb_softcore* sc, sb_neighbor_list* nl, float beta, int ev, bool dh,
+                         float* ae, float* av, float* ad, cudaStream_t s) {
     const ScParams P = sc_params(sc, nl, beta);
     const size_t smem = sizeof(float2) * (size_t)(sc->ntA * sc->ntA + sc->ntB * sc->ntB);
     const int blocks = (nl->clu_cap + 3) / 4;
@@ -676,6 +774,14 @@ static int sc_launch_fixed(sb_softcore* sc, sb_neighbor_list* nl, const uint32_t
 #undef SB_LAUNCH_SC
     SB_CHECK_LAUNCH();
     return SB_OK;
+}
+
+static int sc_launch_fixed(sb_softcore* sc, sb_neighbor_list* nl, const uint32_t* uc,
+                           const float* q, float beta, int ev, bool dh, float* ae, float* av,
+                           float* ad, cudaStream_t s) {
+    SB_TRY(sb_nl_pack(nl, uc, q, sc->d_typeA, s));
+    SB_TRY(sc_slots(sc, nl, s));
+    return sc_pair_fixed(sc, nl, beta, ev, dh, ae, av, ad, s);
 }
 
 // plain form: ATOM_GROUP walk with float atomics; dH/dlambda into d_red (float pair [0..1])
@@ -826,158 +932,230 @@ extern "C" int sb_sc_dh_dlambda(sb_softcore* sc, sb_neighbor_list* nl, const uin
     return SB_OK;
 }
 
-extern "C" int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
-                           const uint32_t* d_uint_crd, const float* d_charge, const int* es,
-                           const int* el, const int* en, float* d_frc, double* d_dudl,
-                           void* stream) {
-    if (!nl || !sc || !pme || !d_uint_crd || !d_charge || !d_frc) {
-        sb_set_error("sb_fep_step: null argument");
-        return SB_ERR_ARG;
-    }
-    if (nl->n != sc->n || pme->n != sc->n) {
-        sb_set_error("sb_fep_step: modules disagree on the atom count");
-        return SB_ERR_ARG;
-    }
-    if (nl->form != SB_FORM_FIXED || sc->form != SB_FORM_FIXED || pme->form != SB_FORM_FIXED) {
-        sb_set_error("sb_fep_step: needs the fixed-point form of all modules");
-        return SB_ERR_ARG;
-    }
-    SB_TRY(sb_nl_ensure_built(nl));
-    cudaStream_t s = sb_stream(stream);
-    const bool dh = d_dudl != nullptr;
-    if (dh) {
-        k_sc_zero<<<1, 32, 0, s>>>(sc->d_hfix, 4);
-        SB_CHECK_LAUNCH();
-    }
-    SB_TRY(sc_launch_fixed(sc, nl, d_uint_crd, d_charge, pme->beta, 0, dh, nullptr, nullptr,
-                           nullptr, s));
-    SB_TRY(sb_pme_fused_reciprocal(pme, nl, d_frc, d_uint_crd, d_charge, es, el, en, 0, 0,
-                                   nullptr, nullptr, s));
-    if (dh) {
-        SB_TRY(sb_pme_ti_terms_slot(pme, nl, sc->d_slot_dq, d_uint_crd, d_charge, sc->d_dq, es,
-                                    el, en, sc->d_hfix + 2, s));
-        const double V = (double)sc->box[0] * sc->box[1] * sc->box[2];
-        k_fep_finish<<<1, 1024, 0, s>>>(sc->n, d_charge, sc->d_dq, sc->d_hfix,
-                                        -2.0 * (double)pme->beta / sqrt(M_PI),
-                                        2.0 * pme->neutralizing_factor, sc->lrc_ti / V, d_dudl,
-                                        nullptr);
-        SB_CHECK_LAUNCH();
-    }
-    return SB_OK;
-}
-
 // ---------------------------------------------------------------------------------------------
-// Batched FEP step: the sb_fep_step of many boxes (windows) in one launch per stage. Each box
-// keeps its own list, soft-core and PME modules; the batch gathers their device pointers and
-// constants into descriptors (SbFepBox, ScParams) and block tables (block -> box, block of box),
-// so that the pack, pair, spread, gather and finalize launches each cover all boxes. The FFTs
-// run one launch per stage per group of equal grid sizes. Every thread does what the same
-// thread of the box's own sb_fep_step does, and all sums are fixed point or keep their warps:
-// each box gets the bits of its own step.
+// The fused FEP step of one box (sb_fep_step) and of many boxes (sb_fep_batch_*). Both run the
+// same device code on a descriptor of the box (SbFepBox): the pack (slot-order coordinates,
+// charges and types, the soft-core slot extras, dH/dlambda accumulators cleared), the pair
+// stage, the reciprocal chain, the finalize and the dU/dlambda finish. In the split form the
+// pair stage is the packed LJ + Ewald kernel over the unperturbed pairs (the perturbed atoms
+// packed as an uncharged ghost type) plus the soft-core pass over the perturbed atoms; without
+// it, the soft-core cluster kernel over all pairs.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
-    k_fep_pack_batch(const SbFepBox* __restrict__ B, const int2* __restrict__ tab, int dh) {
-    const int2 t = tab[blockIdx.x];
-    const SbFepBox& b = B[t.x];
-    const int s = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
-    if (dh && t.y == 0 && threadIdx.x < 4) b.hfix[threadIdx.x] = 0;
-    if (s >= b.meta[3]) return;
-    sb_pack_slot(s, b.slot_atom, b.uc, b.q, b.typeA, b.xq, b.stype, b.xq_prune, b.usx, b.usy,
-                 b.usz, b.move2, b.meta + 6);
+__device__ __forceinline__ void fep_pack_one(int s, const SbFepBox& b) {
+    const int a = b.slot_atom[s];
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    int t = 0;
+    if (a >= 0) {
+        v.x = b.uc[3 * a];
+        v.y = b.uc[3 * a + 1];
+        v.z = b.uc[3 * a + 2];
+        t = b.split ? b.tu[a] : b.typeA[a];
+        v.w = (b.split && t == b.ghost) ? 0u : __float_as_uint(b.q[a]);
+        if (b.xq_prune) {
+            const uint4 o = b.xq_prune[s];
+            const float dx = __int2float_rn((int)(v.x - o.x)) * b.usx;
+            const float dy = __int2float_rn((int)(v.y - o.y)) * b.usy;
+            const float dz = __int2float_rn((int)(v.z - o.z)) * b.usz;
+            if (dx * dx + dy * dy + dz * dz > b.move2) b.meta[6] = 1;
+        }
+    }
+    b.xq[s] = v;
+    b.stype[s] = t;
     sc_pack_slot(s, b.slot_atom, b.typeB, b.mask, b.dq, b.slot_ext, b.slot_dq);
 }
 
-// the ScParams fields that differ between the boxes of one pair launch
-struct ScBoxVar {
-    float sx, sy, sz, l, l_, cA, cB, dcA, dcB;
-    int slot_cap, ent_cap;
-};
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS) k_fep_pack(SbFepBox b, int dh) {
+    const int s = blockIdx.x * SB_FEP_BATCH_THREADS + threadIdx.x;
+    if (dh && blockIdx.x == 0 && threadIdx.x < 4) b.hfix[threadIdx.x] = 0;
+    if (b.split && blockIdx.x == 0 && threadIdx.x == 4) b.pcount[0] = 0;
+    if (s < b.meta[3]) fep_pack_one(s, b);
+}
 
-// the boxes of one launch share C's other fields, which stay kernel parameters (constant-bank
-// operands, as in k_pair_sc) while the box's own ones are loaded per block
+// pair {a < b} is excluded iff b is in a's exclusion list (the list's rule)
+__device__ __forceinline__ bool sc_excluded(int a, int b, const SbExclPass& X) {
+    if (!X.es) return false;
+    const int k0 = X.es[a], k1 = k0 + X.en[a];
+    for (int k = k0; k < k1; k++)
+        if (X.el[k] == b) return true;
+    return false;
+}
+
+// Soft-core pass of the split form, in two launches. The search (block `blk` of 256 list
+// slots, slot order being spatial): for each perturbed atom p (staged in shared memory, 256 at a
+// time) every lane tests its slot's atom j and the hits (pairs inside the cut-off at the current
+// coordinates, not excluded, a pair of two perturbed atoms taken once as p < j) are appended to
+// the box's pair buffer, a warp's hits at once. The evaluation: one pair per thread, forces and
+// dH/dlambda (LJ, direct: hfix[0..1]) converted to fixed point pair by pair, so the result does
+// not depend on the order of the buffer.
+#define SB_SC_PERT_CHUNK 256
+#define SB_SC_EVAL_BLOCKS 32  // evaluation blocks per box (grid-stride over its pairs)
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// squared distance from x to the interval [lo, hi] on one periodic axis of length L, x and the
+// interval being minimum images relative to the same point (so the pair vector is one of x's
+// images shifted by -L, 0 or +L)
+__device__ __forceinline__ float axis_gap2(float x, float lo, float hi, float L) {
+    float g = 3.0e38f;
+#pragma unroll
+    for (int k = -1; k <= 1; k++) {
+        const float y = x + (float)k * L;
+        const float d = fmaxf(fmaxf(lo - y, y - hi), 0.f);
+        g = fminf(g, d);
+    }
+    return g * g;
+}
+
+__device__ __forceinline__ void sc_pert_find(const ScParams& P, int blk, const SbFepBox& b) {
+    constexpr int T = SB_FEP_BATCH_THREADS;
+    __shared__ uint32_t s_u[3][SB_SC_PERT_CHUNK];
+    __shared__ int s_idx[SB_SC_PERT_CHUNK];
+    const int lane = threadIdx.x & 31;
+    const int sj = blk * T + threadIdx.x;
+    const int j = sj < b.meta[3] ? b.slot_atom[sj] : -1;
+    const bool in = j >= 0;
+    uint32_t ux = 0, uy = 0, uz = 0;
+    bool pj = false;
+    if (in) {
+        const uint4 u = b.xq[sj];  // packed by this step
+        ux = u.x;
+        uy = u.y;
+        uz = u.z;
+        pj = b.tu[j] == b.ghost;
+    }
+    // the warp's bounding box, relative to its first atom (minimum images)
+    const unsigned live = __ballot_sync(0xffffffffu, in);
+    const int l0 = live ? __ffs(live) - 1 : 0;
+    const uint32_t rx = __shfl_sync(0xffffffffu, ux, l0);
+    const uint32_t ry = __shfl_sync(0xffffffffu, uy, l0);
+    const uint32_t rz = __shfl_sync(0xffffffffu, uz, l0);
+    const float ox = in ? __int2float_rn((int)(ux - rx)) * P.sx : 0.f;
+    const float oy = in ? __int2float_rn((int)(uy - ry)) * P.sy : 0.f;
+    const float oz = in ? __int2float_rn((int)(uz - rz)) * P.sz : 0.f;
+    const float lox = warp_min(ox), hix = warp_max(ox);
+    const float loy = warp_min(oy), hiy = warp_max(oy);
+    const float loz = warp_min(oz), hiz = warp_max(oz);
+    const float Lx = P.sx * 4294967296.0f, Ly = P.sy * 4294967296.0f, Lz = P.sz * 4294967296.0f;
+    const float cut2 = 1.01f * P.rc2;  // margin over the rounding of the two distance forms
+    for (int c0 = 0; c0 < b.npert; c0 += SB_SC_PERT_CHUNK) {
+        const int nc = min(SB_SC_PERT_CHUNK, b.npert - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nc; t += T) {
+            const int p = b.pert[c0 + t];
+            s_idx[t] = p;
+            s_u[0][t] = b.uc[3 * p];
+            s_u[1][t] = b.uc[3 * p + 1];
+            s_u[2][t] = b.uc[3 * p + 2];
+        }
+        __syncthreads();
+        if (!live) continue;
+        for (int k0 = 0; k0 < nc; k0 += 32) {
+            // lane l screens perturbed atom k0 + l against the warp's box
+            bool near = false;
+            if (k0 + lane < nc) {
+                const int k = k0 + lane;
+                const float px = __int2float_rn((int)(s_u[0][k] - rx)) * P.sx;
+                const float py = __int2float_rn((int)(s_u[1][k] - ry)) * P.sy;
+                const float pz = __int2float_rn((int)(s_u[2][k] - rz)) * P.sz;
+                near = axis_gap2(px, lox, hix, Lx) + axis_gap2(py, loy, hiy, Ly) +
+                           axis_gap2(pz, loz, hiz, Lz) <
+                       cut2;
+            }
+            unsigned cand = __ballot_sync(0xffffffffu, near);
+            while (cand) {
+                const int k = k0 + __ffs(cand) - 1;
+                cand &= cand - 1;
+                const int p = s_idx[k];
+                bool hit = false;
+                if (in && p != j && !(pj && j < p)) {
+                    const float dx = __int2float_rn((int)(ux - s_u[0][k])) * P.sx;
+                    const float dy = __int2float_rn((int)(uy - s_u[1][k])) * P.sy;
+                    const float dz = __int2float_rn((int)(uz - s_u[2][k])) * P.sz;
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    hit = r2 < P.rc2 && !sc_excluded(min(p, j), max(p, j), b.X);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (m) {
+                    int base = 0;
+                    if (lane == 0) base = atomicAdd(b.pcount, __popc(m));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    const int at = base + __popc(m & ((1u << lane) - 1u));
+                    if (hit) {
+                        if (at < b.pcap)
+                            b.ppairs[at] = make_int2(c0 + k, sj);
+                        else
+                            atomicOr(&b.meta[1], SB_STATUS_LIST_OVERFLOW);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// thread e of the box's evaluation blocks takes pairs e, e + stride, ...
 template <bool DH>
-__global__ void __launch_bounds__(128, 4) k_pair_sc_batch(ScParams C,
-                                                       const ScBoxVar* __restrict__ V,
-                                                       const SbFepBox* __restrict__ B,
-                                                       const int2* __restrict__ tab) {
-    const int2 t = tab[blockIdx.x];
-    const ScBoxVar v = V[t.x];
-    ScParams P = C;
-    P.sx = v.sx;
-    P.sy = v.sy;
-    P.sz = v.sz;
-    P.l = v.l;
-    P.l_ = v.l_;
-    P.cA = v.cA;
-    P.cB = v.cB;
-    P.dcA = v.dcA;
-    P.dcB = v.dcB;
-    P.slot_cap = v.slot_cap;
-    P.ent_cap = v.ent_cap;
-    const SbFepBox& b = B[t.x];
-    pair_sc_block<0, DH>(P, t.y, b.meta, b.cl_count, b.cl_ent, b.xq, b.stype, b.slot_ext,
-                         b.slot_dq, b.ABa, b.ABb, b.slot_atom, b.fix, b.hfix, nullptr, nullptr,
-                         nullptr);
+__device__ __forceinline__ void sc_pert_eval(const ScParams& P, int e0, int stride,
+                                             const SbFepBox& b) {
+    const int np = min(b.pcount[0], b.pcap);
+    long long h_lj = 0, h_c = 0;
+    for (int e = e0; e < np; e += stride) {
+        const int2 pr = b.ppairs[e];
+        const int p = b.pert[pr.x], sj = pr.y, j = b.slot_atom[sj];
+        const uint4 uj = b.xq[sj];
+        // d = r_j - r_p: the force on p is fs d, the force on j its opposite
+        const float dx = __int2float_rn((int)(uj.x - b.uc[3 * p])) * P.sx;
+        const float dy = __int2float_rn((int)(uj.y - b.uc[3 * p + 1])) * P.sy;
+        const float dz = __int2float_rn((int)(uj.z - b.uc[3 * p + 2])) * P.sz;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float2 a = b.ABa[b.typeA[p] * P.ntA + b.typeA[j]];
+        const float2 c = b.ABb[b.typeB[p] * P.ntB + b.typeB[j]];
+        const bool soft = sc_is_soft(b.mask[p], b.mask[j], a, c);
+        const float qp = b.q[p], qj = b.q[j];
+        float e1 = 0.f, e2 = 0.f, v1 = 0.f, hl = 0.f, hc = 0.f;
+        const float fs = sc_pair<false, DH>(P, r2, qp * qj, b.dq[j] * qp + qj * b.dq[p], soft,
+                                            a, c, e1, e2, v1, hl, hc);
+        const float tx = fs * dx, ty = fs * dy, tz = fs * dz;
+        const int sp = b.X.atom_slot[p];
+        red_fix_sc(&b.fix[sp], tx, SB_FORCE_SCALE);
+        red_fix_sc(&b.fix[b.slot_cap + sp], ty, SB_FORCE_SCALE);
+        red_fix_sc(&b.fix[2 * b.slot_cap + sp], tz, SB_FORCE_SCALE);
+        red_fix_sc(&b.fix[sj], -tx, SB_FORCE_SCALE);
+        red_fix_sc(&b.fix[b.slot_cap + sj], -ty, SB_FORCE_SCALE);
+        red_fix_sc(&b.fix[2 * b.slot_cap + sj], -tz, SB_FORCE_SCALE);
+        if (DH) {
+            h_lj += __float2ll_rn(hl * SB_DHDL_SCALE);
+            h_c += __float2ll_rn(hc * SB_DHDL_SCALE);
+        }
+    }
+    if (DH) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            h_lj += __shfl_xor_sync(0xffffffffu, h_lj, o);
+            h_c += __shfl_xor_sync(0xffffffffu, h_c, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            if (h_lj) atomicAdd((unsigned long long*)&b.hfix[0], (unsigned long long)h_lj);
+            if (h_c) atomicAdd((unsigned long long*)&b.hfix[1], (unsigned long long)h_c);
+        }
+    }
 }
 
-static ScBoxVar sc_box_var(const ScParams& P) {
-    return ScBoxVar{P.sx, P.sy, P.sz, P.l, P.l_, P.cA, P.cB, P.dcA, P.dcB, P.slot_cap,
-                    P.ent_cap};
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS) k_sc_pert_find(ScParams P, SbFepBox b) {
+    sc_pert_find(P, blockIdx.x, b);
 }
 
-// the fields a pair launch takes from its first box
-static bool sc_same_common(const ScParams& a, const ScParams& b) {
-    if (a.rc2 != b.rc2 || a.beta != b.beta || a.beta2 != b.beta2 || a.tsp_beta != b.tsp_beta ||
-        a.s6 != b.s6 || a.s6min != b.s6min || a.wide != b.wide || a.ntA != b.ntA ||
-        a.ntB != b.ntB)
-        return false;
-    for (int k = 0; k < 6; k++)
-        if (a.gp[k] != b.gp[k]) return false;
-    return true;
-}
-
-__global__ void __launch_bounds__(1024) k_fep_finish_batch(const SbFepBox* __restrict__ B) {
-    const SbFepBox& b = B[blockIdx.x];
-    fep_finish_block(b.n, b.q, b.dq, b.hfix, b.self_coef, b.neutral2, b.lrc, b.dudl, nullptr);
-}
-
-struct SbFftGroup {
-    const SbFftPlan* plan;      // the plan of the group's first box (all share its sizes)
-    std::vector<int> boxes;
-    std::vector<SbFftBatchIo> io;  // what d_io holds
-    SbFftBatchIo* d_io = nullptr;
-    bool batched = false;       // false: the boxes' own plan calls, one after another
-    int fused = 0;
-};
-
-struct sb_fep_batch {
-    int nb = 0;
-    int dh = 0;
-    std::vector<sb_neighbor_list*> nls;
-    std::vector<sb_softcore*> scs;
-    std::vector<sb_pme*> pmes;
-    std::vector<SbFepBox> hbox;   // what the descriptors were built from (staleness check)
-    std::vector<ScParams> hP;
-    std::vector<float> lam;
-    SbFepBox* d_box = nullptr;
-    ScBoxVar* d_var = nullptr;
-    int2* d_tab = nullptr;
-    int off_slot = 0, n_slot = 0, off_spread = 0, n_spread = 0, off_atom = 0, n_atom = 0;
-    // pair launches: boxes with equal common parameters (usually all), their cluster blocks
-    struct PairGroup {
-        int first_box, off, n;
-    };
-    std::vector<PairGroup> pair_groups;
-    size_t smem = 0;              // dynamic shared memory of the pair launch (largest tables)
-    std::vector<SbFftGroup> groups;
-};
-
-static void fep_batch_free(sb_fep_batch* b) {
-    for (auto& g : b->groups) sb_free(g.d_io);
-    sb_free(b->d_box);
-    sb_free(b->d_var);
-    sb_free(b->d_tab);
-    delete b;
+template <bool DH>
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS) k_sc_pert_eval(ScParams P, SbFepBox b) {
+    sc_pert_eval<DH>(P, blockIdx.x * SB_FEP_BATCH_THREADS + threadIdx.x,
+                     gridDim.x * SB_FEP_BATCH_THREADS, b);
 }
 
 static SbFepBox fep_box_desc(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* p, const uint32_t* uc,
@@ -1008,6 +1186,16 @@ static SbFepBox fep_box_desc(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* p, c
     d.ABa = sc->d_ABa;
     d.ABb = sc->d_ABb;
     d.hfix = sc->d_hfix;
+    d.sums = sc->d_sums;
+    d.split = sc->split && sb_pair_fep_packed(nl, sc->cutoff, p->beta);
+    d.ghost = sc->ntA;
+    d.tu = sc->d_tu;
+    d.ABu = sc->d_ABu;
+    d.pert = sc->d_pert;
+    d.npert = sc->npert;
+    d.ppairs = sc->d_ppairs;
+    d.pcount = sc->d_pcount;
+    d.pcap = sc->pcap;
     d.qfix = p->d_qfix;
     d.theta = p->d_theta;
     d.K0 = p->K[0];
@@ -1034,6 +1222,226 @@ static SbFepBox fep_box_desc(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* p, c
     return d;
 }
 
+extern "C" int sb_fep_step(sb_neighbor_list* nl, sb_softcore* sc, sb_pme* pme,
+                           const uint32_t* d_uint_crd, const float* d_charge, const int* es,
+                           const int* el, const int* en, float* d_frc, double* d_dudl,
+                           void* stream) {
+    if (!nl || !sc || !pme || !d_uint_crd || !d_charge || !d_frc) {
+        sb_set_error("sb_fep_step: null argument");
+        return SB_ERR_ARG;
+    }
+    if (nl->n != sc->n || pme->n != sc->n) {
+        sb_set_error("sb_fep_step: modules disagree on the atom count");
+        return SB_ERR_ARG;
+    }
+    if (nl->form != SB_FORM_FIXED || sc->form != SB_FORM_FIXED || pme->form != SB_FORM_FIXED) {
+        sb_set_error("sb_fep_step: needs the fixed-point form of all modules");
+        return SB_ERR_ARG;
+    }
+    SB_TRY(sb_nl_ensure_built(nl));
+    SB_TRY(sc_slots_alloc(sc, nl));
+    cudaStream_t s = sb_stream(stream);
+    const bool dh = d_dudl != nullptr;
+    const SbFepBox d = fep_box_desc(nl, sc, pme, d_uint_crd, d_charge, es, el, en, d_frc, d_dudl);
+    k_fep_pack<<<(nl->slot_cap + SB_FEP_BATCH_THREADS - 1) / SB_FEP_BATCH_THREADS,
+                 SB_FEP_BATCH_THREADS, 0, s>>>(d, dh ? 1 : 0);
+    SB_CHECK_LAUNCH();
+    if (d.split) {
+        SB_TRY(sb_pair_fep(nl, sc->d_ABu, sc->ntA + 1, sc->cutoff, pme->beta, s));
+        const ScParams P = sc_params(sc, nl, pme->beta);
+        const int blocks = (nl->slot_cap + SB_FEP_BATCH_THREADS - 1) / SB_FEP_BATCH_THREADS;
+        k_sc_pert_find<<<blocks, SB_FEP_BATCH_THREADS, 0, s>>>(P, d);
+        SB_CHECK_LAUNCH();
+        if (dh)
+            k_sc_pert_eval<true><<<SB_SC_EVAL_BLOCKS, SB_FEP_BATCH_THREADS, 0, s>>>(P, d);
+        else
+            k_sc_pert_eval<false><<<SB_SC_EVAL_BLOCKS, SB_FEP_BATCH_THREADS, 0, s>>>(P, d);
+        SB_CHECK_LAUNCH();
+    } else {
+        SB_TRY(sc_pair_fixed(sc, nl, pme->beta, 0, dh, nullptr, nullptr, nullptr, s));
+    }
+    SB_TRY(sb_pme_fused_reciprocal(pme, nl, d_frc, d_uint_crd, d_charge, es, el, en, 0, 0,
+                                   nullptr, nullptr, s));
+    if (dh) {
+        SB_TRY(sb_pme_ti_terms_slot(pme, nl, sc->d_slot_dq, d_uint_crd, d_charge, sc->d_dq, es,
+                                    el, en, sc->d_hfix + 2, s));
+        k_fep_self<<<1, 1024, 0, s>>>(sc->n, d_charge, sc->d_dq, sc->d_sums);
+        SB_CHECK_LAUNCH();
+        k_fep_combine<<<1, 32, 0, s>>>(sc->d_hfix, sc->d_sums, d.self_coef, d.neutral2, d.lrc,
+                                       d_dudl);
+        SB_CHECK_LAUNCH();
+    }
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched FEP step: the sb_fep_step of many boxes (windows) in one launch per stage. Each box
+// keeps its own list, soft-core and PME modules; the batch gathers their device pointers and
+// constants into descriptors (SbFepBox) and block tables (block -> box, block of that box), so
+// that each stage's launch covers all boxes. The FFTs run one launch per stage per group of
+// equal grid sizes. Every thread does what the same thread of the box's own sb_fep_step does,
+// and all sums are fixed point or keep their warps: each box gets the bits of its own step.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
+    k_fep_pack_batch(const SbFepBox* __restrict__ B, const int2* __restrict__ tab, int dh) {
+    const int2 t = tab[blockIdx.x];
+    const SbFepBox& b = B[t.x];
+    const int s = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
+    if (dh && t.y == 0 && threadIdx.x < 4) b.hfix[threadIdx.x] = 0;
+    if (b.split && t.y == 0 && threadIdx.x == 4) b.pcount[0] = 0;
+    if (s < b.meta[3]) fep_pack_one(s, b);
+}
+
+// the ScParams fields that differ between the boxes of one launch
+struct ScBoxVar {
+    float sx, sy, sz, l, l_, cA, cB, dcA, dcB;
+    int slot_cap, ent_cap;
+};
+
+// the boxes of one launch share C's other fields, which stay kernel parameters (constant-bank
+// operands, as in the single-box kernels) while the box's own ones are loaded per block
+__device__ __forceinline__ ScParams sc_box_params(const ScParams& C, const ScBoxVar& v) {
+    ScParams P = C;
+    P.sx = v.sx;
+    P.sy = v.sy;
+    P.sz = v.sz;
+    P.l = v.l;
+    P.l_ = v.l_;
+    P.cA = v.cA;
+    P.cB = v.cB;
+    P.dcA = v.dcA;
+    P.dcB = v.dcB;
+    P.slot_cap = v.slot_cap;
+    P.ent_cap = v.ent_cap;
+    return P;
+}
+
+// soft-core cluster kernel over the boxes without the split form
+template <bool DH>
+__global__ void __launch_bounds__(128, 4) k_pair_sc_batch(ScParams C,
+                                                          const ScBoxVar* __restrict__ V,
+                                                          const SbFepBox* __restrict__ B,
+                                                          const int2* __restrict__ tab) {
+    const int2 t = tab[blockIdx.x];
+    const ScParams P = sc_box_params(C, V[t.x]);
+    const SbFepBox& b = B[t.x];
+    pair_sc_block<0, DH>(P, t.y, b.meta, b.cl_count, b.cl_ent, b.xq, b.stype, b.slot_ext,
+                         b.slot_dq, b.ABa, b.ABb, b.slot_atom, b.fix, b.hfix, nullptr, nullptr,
+                         nullptr);
+}
+
+// soft-core pass over the perturbed atoms of the split boxes: the search over their slot
+// blocks, then the evaluation (SB_SC_EVAL_BLOCKS blocks per box)
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS) k_sc_pert_find_batch(
+    ScParams C, const ScBoxVar* __restrict__ V, const SbFepBox* __restrict__ B,
+    const int2* __restrict__ tab) {
+    const int2 t = tab[blockIdx.x];
+    const ScParams P = sc_box_params(C, V[t.x]);
+    sc_pert_find(P, t.y, B[t.x]);
+}
+
+template <bool DH>
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS) k_sc_pert_eval_batch(
+    ScParams C, const ScBoxVar* __restrict__ V, const SbFepBox* __restrict__ B,
+    const int2* __restrict__ tab) {
+    const int2 t = tab[blockIdx.x];
+    const ScParams P = sc_box_params(C, V[t.x]);
+    sc_pert_eval<DH>(P, t.y * SB_FEP_BATCH_THREADS + threadIdx.x,
+                     SB_SC_EVAL_BLOCKS * SB_FEP_BATCH_THREADS, B[t.x]);
+}
+
+static ScBoxVar sc_box_var(const ScParams& P) {
+    return ScBoxVar{P.sx, P.sy, P.sz, P.l, P.l_, P.cA, P.cB, P.dcA, P.dcB, P.slot_cap,
+                    P.ent_cap};
+}
+
+// the fields a launch takes from its first box
+static bool sc_same_common(const ScParams& a, const ScParams& b) {
+    if (a.rc2 != b.rc2 || a.beta != b.beta || a.beta2 != b.beta2 || a.tsp_beta != b.tsp_beta ||
+        a.s6 != b.s6 || a.s6min != b.s6min || a.wide != b.wide || a.ntA != b.ntA ||
+        a.ntB != b.ntB)
+        return false;
+    for (int k = 0; k < 6; k++)
+        if (a.gp[k] != b.gp[k]) return false;
+    return true;
+}
+
+// block per box: the self-term sums (they need only the charges, so they run beside the pair
+// stage); then thread per box: dU/dlambda
+__global__ void __launch_bounds__(1024) k_fep_self_batch(const SbFepBox* __restrict__ B) {
+    const SbFepBox& b = B[blockIdx.x];
+    fep_self_sums(b.n, b.q, b.dq, b.sums);
+}
+
+__global__ void k_fep_combine_batch(const SbFepBox* __restrict__ B, int nb) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nb) {
+        const SbFepBox& b = B[k];
+        fep_combine(b.hfix, b.sums, b.self_coef, b.neutral2, b.lrc, b.dudl, nullptr);
+    }
+}
+
+struct SbFftGroup {
+    const SbFftPlan* plan;         // the plan of the group's first box (all share its sizes)
+    std::vector<int> boxes;
+    std::vector<SbFftBatchIo> io;  // what d_io holds
+    SbFftBatchIo* d_io = nullptr;
+    bool batched = false;          // false: the boxes' own plan calls, one after another
+    int fused = 0;
+};
+
+struct sb_fep_batch {
+    int nb = 0;
+    int dh = 0;
+    std::vector<sb_neighbor_list*> nls;
+    std::vector<sb_softcore*> scs;
+    std::vector<sb_pme*> pmes;
+    std::vector<SbFepBox> hbox;   // what the descriptors were built from (staleness check)
+    std::vector<ScParams> hP;
+    std::vector<float> lam;
+    std::vector<const void*> cl_ent_in;
+    SbFepBox* d_box = nullptr;
+    ScBoxVar* d_var = nullptr;
+    int2* d_tab = nullptr;
+    int off_slot = 0, n_slot = 0, off_spread = 0, n_spread = 0, off_atom = 0, n_atom = 0;
+    // soft-core launches: boxes with equal common parameters (usually all); the cluster blocks
+    // of their boxes without the split form and the atom blocks of their split boxes
+    struct ScGroup {
+        int first_box, off_pair, n_pair, off_pert, n_pert, off_eval, n_eval;
+    };
+    std::vector<ScGroup> sc_groups;
+    SbX2Batch* x2 = nullptr;      // packed pair kernel over the split boxes
+    size_t smem = 0;              // dynamic shared memory of the soft-core cluster launch
+    std::vector<SbFftGroup> groups;
+    // the reciprocal chain (spread, FFT groups, gather) runs beside the pair launches: on `rec`
+    // (highest priority) with the FFT groups spread over `fft` streams, joined by events
+    cudaStream_t rec = nullptr;
+    cudaStream_t pert = nullptr;  // the soft-core passes, beside the packed pair kernel
+    std::vector<cudaStream_t> fft;
+    cudaEvent_t ev_packed = nullptr, ev_spread = nullptr, ev_rec = nullptr, ev_pert = nullptr;
+    std::vector<cudaEvent_t> ev_fft;
+};
+
+#define SB_FEP_FFT_STREAMS 4
+
+static void fep_batch_free(sb_fep_batch* b) {
+    if (b->rec) cudaStreamSynchronize(b->rec);
+    for (cudaStream_t f : b->fft) cudaStreamSynchronize(f);
+    if (b->pert) cudaStreamSynchronize(b->pert);
+    for (cudaStream_t f : b->fft) cudaStreamDestroy(f);
+    if (b->rec) cudaStreamDestroy(b->rec);
+    if (b->pert) cudaStreamDestroy(b->pert);
+    for (cudaEvent_t e : {b->ev_packed, b->ev_spread, b->ev_rec, b->ev_pert})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : b->ev_fft) cudaEventDestroy(e);
+    for (auto& g : b->groups) sb_free(g.d_io);
+    sb_pair_batch_destroy(b->x2);
+    sb_free(b->d_box);
+    sb_free(b->d_var);
+    sb_free(b->d_tab);
+    delete b;
+}
+
 static void fep_tab_add(std::vector<int2>& tab, int box, int blocks) {
     for (int k = 0; k < blocks; k++) tab.push_back(make_int2(box, k));
 }
@@ -1051,7 +1459,7 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
                                    const int* const* d_excluded_list_start,
                                    const int* const* d_excluded_list,
                                    const int* const* d_excluded_numbers, float* const* d_frc,
-                                   double* d_dudl, sb_fep_batch** out) {
+                                   double* const* d_dudl, sb_fep_batch** out) {
     if (!out || n_boxes < 1 || !nls || !scs || !pmes || !d_uint_crd || !d_charge || !d_frc) {
         sb_set_error("sb_fep_batch_create: invalid argument");
         return SB_ERR_ARG;
@@ -1074,15 +1482,17 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
                          k);
             return SB_ERR_ARG;
         }
-        if (nl->clu_cap > (1 << 30) / 4 || 4 * (long long)nl->n > (1ll << 30)) {
-            sb_set_error("sb_fep_batch_create: box %d is too large", k);
-            return SB_ERR_ARG;
-        }
         SB_TRY(sb_nl_ensure_built(nl));
     }
     sb_fep_batch* b = new sb_fep_batch();
     b->nb = n_boxes;
     b->dh = d_dudl != nullptr;
+    for (int k = 0; k < n_boxes && b->dh; k++)
+        if (!d_dudl[k]) {
+            sb_set_error("sb_fep_batch_create: box %d has no dU/dlambda output", k);
+            delete b;
+            return SB_ERR_ARG;
+        }
     std::vector<int2> tab;
     int st = SB_OK;
     for (int k = 0; k < n_boxes && !st; k++) {
@@ -1095,29 +1505,42 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
         const int* el = d_excluded_list ? d_excluded_list[k] : nullptr;
         const int* en = d_excluded_numbers ? d_excluded_numbers[k] : nullptr;
         b->hbox.push_back(fep_box_desc(nls[k], scs[k], pmes[k], d_uint_crd[k], d_charge[k], es,
-                                       el, en, d_frc[k], d_dudl ? d_dudl + k : nullptr));
+                                       el, en, d_frc[k], d_dudl ? d_dudl[k] : nullptr));
         b->hP.push_back(sc_params(scs[k], nls[k], pmes[k]->beta));
         b->lam.push_back(scs[k]->lambda);
-        const size_t sm = sizeof(float2) * (size_t)(scs[k]->ntA * scs[k]->ntA +
-                                                    scs[k]->ntB * scs[k]->ntB);
-        b->smem = std::max(b->smem, sm);
+        b->cl_ent_in.push_back(nls[k]->cl_ent_in);
+        if (!b->hbox.back().split) {
+            const size_t sm = sizeof(float2) * (size_t)(scs[k]->ntA * scs[k]->ntA +
+                                                        scs[k]->ntB * scs[k]->ntB);
+            b->smem = std::max(b->smem, sm);
+        }
     }
     if (!st) {
         const int T = SB_FEP_BATCH_THREADS;
         b->off_slot = (int)tab.size();
         for (int k = 0; k < n_boxes; k++) fep_tab_add(tab, k, (nls[k]->slot_cap + T - 1) / T);
         b->n_slot = (int)tab.size() - b->off_slot;
-        std::vector<int> pg(n_boxes, -1);
+        std::vector<char> done(n_boxes, 0);
         for (int k = 0; k < n_boxes; k++) {
-            if (pg[k] >= 0) continue;
-            sb_fep_batch::PairGroup g{k, (int)tab.size(), 0};
-            for (int j = k; j < n_boxes; j++) {
-                if (pg[j] >= 0 || !sc_same_common(b->hP[k], b->hP[j])) continue;
-                pg[j] = (int)b->pair_groups.size();
-                fep_tab_add(tab, j, (nls[j]->clu_cap + 3) / 4);
-            }
-            g.n = (int)tab.size() - g.off;
-            b->pair_groups.push_back(g);
+            if (done[k]) continue;
+            sb_fep_batch::ScGroup g{k, (int)tab.size(), 0, 0, 0, 0, 0};
+            for (int j = k; j < n_boxes; j++)
+                if (!done[j] && sc_same_common(b->hP[k], b->hP[j]) && !b->hbox[j].split)
+                    fep_tab_add(tab, j, (nls[j]->clu_cap + 3) / 4);
+            g.n_pair = (int)tab.size() - g.off_pair;
+            g.off_pert = (int)tab.size();
+            for (int j = k; j < n_boxes; j++)
+                if (!done[j] && sc_same_common(b->hP[k], b->hP[j]) && b->hbox[j].split)
+                    fep_tab_add(tab, j, (nls[j]->slot_cap + T - 1) / T);
+            g.n_pert = (int)tab.size() - g.off_pert;
+            g.off_eval = (int)tab.size();
+            for (int j = k; j < n_boxes; j++)
+                if (!done[j] && sc_same_common(b->hP[k], b->hP[j])) {
+                    done[j] = 1;
+                    if (b->hbox[j].split) fep_tab_add(tab, j, SB_SC_EVAL_BLOCKS);
+                }
+            g.n_eval = (int)tab.size() - g.off_eval;
+            b->sc_groups.push_back(g);
         }
         b->off_spread = (int)tab.size();
         for (int k = 0; k < n_boxes; k++) fep_tab_add(tab, k, (4 * nls[k]->n + T - 1) / T);
@@ -1129,6 +1552,22 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
             sb_set_error("sb_fep_batch_create: LJ tables too large for shared memory");
             st = SB_ERR_ARG;
         }
+    }
+    if (!st) {
+        std::vector<int> ids, nts;
+        std::vector<sb_neighbor_list*> xl;
+        std::vector<float> cuts, betas;
+        for (int k = 0; k < n_boxes; k++) {
+            if (!b->hbox[k].split) continue;
+            ids.push_back(k);
+            xl.push_back(nls[k]);
+            nts.push_back(scs[k]->ntA + 1);
+            cuts.push_back(scs[k]->cutoff);
+            betas.push_back(pmes[k]->beta);
+        }
+        if (!ids.empty())
+            st = sb_pair_batch_create((int)ids.size(), ids.data(), xl.data(), nts.data(),
+                                      cuts.data(), betas.data(), n_boxes, &b->x2);
     }
     // grids of equal sizes and transform family share batched FFT launches
     for (int k = 0; k < n_boxes && !st; k++) {
@@ -1151,22 +1590,22 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
     }
     for (auto& g : b->groups) {
         if (st || !g.batched) continue;
-        std::vector<SbFftBatchIo>& io = g.io;
         for (int k : g.boxes) {
             sb_pme* p = pmes[k];
-            io.push_back(SbFftBatchIo{p->d_qfix, p->d_spec, p->d_theta, p->d_bc, nullptr});
+            g.io.push_back(SbFftBatchIo{p->d_qfix, p->d_spec, p->d_theta, p->d_bc, nullptr});
         }
-        st = sb_malloc((void**)&g.d_io, sizeof(SbFftBatchIo) * io.size(), "FEP batch FFT table");
-        if (!st && cudaMemcpy(g.d_io, io.data(), sizeof(SbFftBatchIo) * io.size(),
+        st = sb_malloc((void**)&g.d_io, sizeof(SbFftBatchIo) * g.io.size(),
+                       "FEP batch FFT table");
+        if (!st && cudaMemcpy(g.d_io, g.io.data(), sizeof(SbFftBatchIo) * g.io.size(),
                               cudaMemcpyHostToDevice) != cudaSuccess) {
             sb_set_error("sb_fep_batch_create: FFT table upload failed");
             st = SB_ERR_CUDA;
         }
     }
-    if (!st) st = sb_malloc((void**)&b->d_box, sizeof(SbFepBox) * n_boxes, "FEP batch boxes");
-    if (!st) st = sb_malloc((void**)&b->d_var, sizeof(ScBoxVar) * n_boxes, "FEP batch params");
     std::vector<ScBoxVar> var;
     for (const ScParams& P : b->hP) var.push_back(sc_box_var(P));
+    if (!st) st = sb_malloc((void**)&b->d_box, sizeof(SbFepBox) * n_boxes, "FEP batch boxes");
+    if (!st) st = sb_malloc((void**)&b->d_var, sizeof(ScBoxVar) * n_boxes, "FEP batch params");
     if (!st) st = sb_malloc((void**)&b->d_tab, sizeof(int2) * tab.size(), "FEP batch tables");
     if (!st && (cudaMemcpy(b->d_box, b->hbox.data(), sizeof(SbFepBox) * n_boxes,
                            cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -1176,6 +1615,29 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
                            cudaMemcpyHostToDevice) != cudaSuccess)) {
         sb_set_error("sb_fep_batch_create: descriptor upload failed");
         st = SB_ERR_CUDA;
+    }
+    if (!st) {
+        int lo = 0, hi = 0;
+        bool ok = cudaDeviceGetStreamPriorityRange(&lo, &hi) == cudaSuccess &&
+                  cudaStreamCreateWithPriority(&b->rec, cudaStreamNonBlocking, hi) == cudaSuccess &&
+                  cudaStreamCreateWithPriority(&b->pert, cudaStreamNonBlocking, hi) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&b->ev_pert, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&b->ev_packed, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&b->ev_spread, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&b->ev_rec, cudaEventDisableTiming) == cudaSuccess;
+        const int nf = std::min((int)b->groups.size(), SB_FEP_FFT_STREAMS);
+        for (int k = 0; k < nf && ok; k++) {
+            cudaStream_t f = nullptr;
+            cudaEvent_t e = nullptr;
+            ok = cudaStreamCreateWithPriority(&f, cudaStreamNonBlocking, hi) == cudaSuccess;
+            if (ok) b->fft.push_back(f);
+            ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+            if (ok) b->ev_fft.push_back(e);
+        }
+        if (!ok) {
+            sb_set_error("sb_fep_batch_create: stream or event creation failed");
+            st = SB_ERR_CUDA;
+        }
     }
     if (!st && b->smem > 40 * 1024) {
         const cudaError_t e1 = cudaFuncSetAttribute(
@@ -1195,7 +1657,7 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
     return SB_OK;
 }
 
-// the descriptors still describe the modules: same buffers, capacities, box and lambda
+// the descriptors still describe the modules: same buffers, capacities, box, lambda, FFT
 static int fep_batch_current(const sb_fep_batch* b) {
     for (int k = 0; k < b->nb; k++) {
         const sb_neighbor_list* nl = b->nls[k];
@@ -1207,7 +1669,7 @@ static int fep_batch_current(const sb_fep_batch* b) {
         if (!nl->built || nl->meta != d.meta || nl->cl_ent != d.cl_ent || nl->xq != d.xq ||
             nl->fix != d.fix || nl->slot_cap != d.slot_cap || nl->ent_cap != b->hP[k].ent_cap ||
             (pr ? nl->xq_prune : nullptr) != d.xq_prune || half * half != d.move2 ||
-            (1.0f / 4294967296.0f) * nl->box[0] != d.usx ||
+            nl->cl_ent_in != b->cl_ent_in[k] || (1.0f / 4294967296.0f) * nl->box[0] != d.usx ||
             (1.0f / 4294967296.0f) * nl->box[1] != d.usy ||
             (1.0f / 4294967296.0f) * nl->box[2] != d.usz || sc->d_slot_ext != d.slot_ext ||
             sc->d_slot_dq != d.slot_dq || sc->lambda != b->lam[k] || p->d_qfix != d.qfix ||
@@ -1246,35 +1708,76 @@ extern "C" int sb_fep_batch_step(sb_fep_batch* b, void* stream) {
     k_fep_pack_batch<<<b->n_slot, SB_FEP_BATCH_THREADS, 0, s>>>(b->d_box, tab + b->off_slot,
                                                                b->dh);
     SB_CHECK_LAUNCH();
-    for (const auto& g : b->pair_groups) {
-        const ScParams& C = b->hP[g.first_box];
-        if (b->dh)
-            k_pair_sc_batch<true><<<g.n, 128, b->smem, s>>>(C, b->d_var, b->d_box, tab + g.off);
-        else
-            k_pair_sc_batch<false><<<g.n, 128, b->smem, s>>>(C, b->d_var, b->d_box, tab + g.off);
-        SB_CHECK_LAUNCH();
-    }
-    SB_TRY(sb_pme_batch_spread(b->d_box, tab + b->off_spread, b->n_spread, s));
-    for (const auto& g : b->groups) {
+    // reciprocal chain beside the pair launches: both add to the fixed-point force planes
+    // (order-free integer sums); the finalize waits for both
+    SB_CHECK_CUDA(cudaEventRecord(b->ev_packed, s));
+    SB_CHECK_CUDA(cudaStreamWaitEvent(b->rec, b->ev_packed, 0));
+    SB_TRY(sb_pme_batch_spread(b->d_box, tab + b->off_spread, b->n_spread, b->rec));
+    SB_CHECK_CUDA(cudaEventRecord(b->ev_spread, b->rec));
+    const int nf = (int)b->fft.size();
+    for (int k = 0; k < nf; k++) SB_CHECK_CUDA(cudaStreamWaitEvent(b->fft[k], b->ev_spread, 0));
+    for (size_t gi = 0; gi < b->groups.size(); gi++) {
+        const SbFftGroup& g = b->groups[gi];
+        cudaStream_t f = b->fft[gi % nf];
         if (g.batched) {
             const int n = (int)g.boxes.size();
-            SB_TRY(sb_fft_batch_forward(g.plan, g.d_io, n, s));
-            SB_TRY(sb_fft_batch_convolve(g.plan, g.d_io, n, 0, s));
-            SB_TRY(sb_fft_batch_inverse(g.plan, g.d_io, n, s));
+            SB_TRY(sb_fft_batch_forward(g.plan, g.d_io, n, f));
+            SB_TRY(sb_fft_batch_convolve(g.plan, g.d_io, n, 0, f));
+            SB_TRY(sb_fft_batch_inverse(g.plan, g.d_io, n, f));
         } else {
             for (int k : g.boxes) {
                 sb_pme* p = b->pmes[k];
-                SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, s));
-                SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, 0, s,
+                SB_TRY(sb_fft_plane_forward(&p->plan, p->d_qfix, p->d_spec, f));
+                SB_TRY(sb_fft_x_convolve(&p->plan, p->d_spec, p->d_bc, p->d_epart, 0, f,
                                          &p->rec_nparts));
-                SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, s));
+                SB_TRY(sb_fft_plane_inverse(&p->plan, p->d_spec, p->d_theta, f));
             }
         }
     }
-    SB_TRY(sb_pme_batch_gather(b->d_box, tab + b->off_atom, b->n_atom, b->dh, s));
+    for (int k = 0; k < nf; k++) {
+        SB_CHECK_CUDA(cudaEventRecord(b->ev_fft[k], b->fft[k]));
+        SB_CHECK_CUDA(cudaStreamWaitEvent(b->rec, b->ev_fft[k], 0));
+    }
+    SB_TRY(sb_pme_batch_gather(b->d_box, tab + b->off_atom, b->n_atom, b->dh, b->rec));
+    SB_CHECK_CUDA(cudaEventRecord(b->ev_rec, b->rec));
+    SB_CHECK_CUDA(cudaStreamWaitEvent(b->pert, b->ev_packed, 0));
+    for (const auto& g : b->sc_groups) {
+        if (!g.n_pert) continue;
+        const ScParams& C = b->hP[g.first_box];
+        k_sc_pert_find_batch<<<g.n_pert, SB_FEP_BATCH_THREADS, 0, b->pert>>>(
+            C, b->d_var, b->d_box, tab + g.off_pert);
+        SB_CHECK_LAUNCH();
+        if (b->dh)
+            k_sc_pert_eval_batch<true><<<g.n_eval, SB_FEP_BATCH_THREADS, 0, b->pert>>>(
+                C, b->d_var, b->d_box, tab + g.off_eval);
+        else
+            k_sc_pert_eval_batch<false><<<g.n_eval, SB_FEP_BATCH_THREADS, 0, b->pert>>>(
+                C, b->d_var, b->d_box, tab + g.off_eval);
+        SB_CHECK_LAUNCH();
+    }
+    if (b->dh) {
+        k_fep_self_batch<<<b->nb, 1024, 0, b->pert>>>(b->d_box);
+        SB_CHECK_LAUNCH();
+    }
+    SB_CHECK_CUDA(cudaEventRecord(b->ev_pert, b->pert));
+    if (b->x2) SB_TRY(sb_pair_batch_launch(b->x2, b->d_box, s));
+    for (const auto& g : b->sc_groups) {
+        const ScParams& C = b->hP[g.first_box];
+        if (g.n_pair) {
+            if (b->dh)
+                k_pair_sc_batch<true><<<g.n_pair, 128, b->smem, s>>>(C, b->d_var, b->d_box,
+                                                                      tab + g.off_pair);
+            else
+                k_pair_sc_batch<false><<<g.n_pair, 128, b->smem, s>>>(C, b->d_var, b->d_box,
+                                                                       tab + g.off_pair);
+            SB_CHECK_LAUNCH();
+        }
+    }
+    SB_CHECK_CUDA(cudaStreamWaitEvent(s, b->ev_pert, 0));
+    SB_CHECK_CUDA(cudaStreamWaitEvent(s, b->ev_rec, 0));
     SB_TRY(sb_pme_batch_slots(b->d_box, tab + b->off_slot, b->n_slot, b->dh, s));
     if (b->dh) {
-        k_fep_finish_batch<<<b->nb, 1024, 0, s>>>(b->d_box);
+        k_fep_combine_batch<<<(b->nb + 127) / 128, 128, 0, s>>>(b->d_box, b->nb);
         SB_CHECK_LAUNCH();
     }
     return SB_OK;
@@ -1282,8 +1785,9 @@ extern "C" int sb_fep_batch_step(sb_fep_batch* b, void* stream) {
 
 extern "C" int sb_fep_batch_launches(const sb_fep_batch* b) {
     if (!b) return -1;
-    // pack, spread, gather, slots (+ finish), the pair launches
-    int n = 4 + (b->dh ? 1 : 0) + (int)b->pair_groups.size();
+    // pack, spread, gather, slots (+ self sums, combine), the pair launches
+    int n = 4 + (b->dh ? 2 : 0) + (b->x2 ? sb_pair_batch_launches(b->x2) : 0);
+    for (const auto& g : b->sc_groups) n += (g.n_pair ? 1 : 0) + (g.n_pert ? 2 : 0);
     for (const auto& g : b->groups) {
         if (g.batched)
             n += 3 + (g.plan->fused ? 0 : 2);

@@ -27,7 +27,7 @@ def _scaled(x, f):
 
 class FepEngine:
     def __init__(self, system, form=FORM_FIXED, refresh_interval=20, max_neighbor_numbers=1200,
-                 device="cuda"):
+                 device="cuda", prune_buffer=0.5, prune_interval=5):
         torch = _require_cuda()
         self.torch = torch
         self.system = s = system
@@ -53,6 +53,10 @@ class FepEngine:
                            n_types_A=s["n_types"], n_types_B=s["n_types_B"])
         self.pme = ParticleMeshEwald(n, self.box, s["cutoff"], s["tolerance"], s["fft"],
                                      form=form)
+        # the split form's packed pair kernel walks a pruned list (rc + 0.5 A, pruned again
+        # when an atom has moved 0.25 A or every 5 list updates)
+        if form == FORM_FIXED and prune_buffer > 0 and self.sc.split_form[0]:
+            self.nl.set_prune(prune_buffer, prune_interval)
         self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
         self.form = form
 
@@ -117,7 +121,7 @@ class FepBatch:
             o += e.n
         self.graph = None
         self.n_streams = None
-        self.batch = None
+        self._batches = {}  # sub-batch count -> list of FepBatchStep
         self.count = 0
 
     @property
@@ -127,52 +131,68 @@ class FepBatch:
     @property
     def launches(self):
         """Kernel launches of one captured step (the force clear included)."""
-        if self.mode == "kernels":
-            return 1 + self.batch.launches
+        if self.mode == "kernels" and self.n_streams in self._batches:
+            return 1 + sum(b.launches for b in self._batches[self.n_streams])
         return None
 
-    def rebuild(self):
-        for e in self.engines:
-            e.update_list(forced=1)
-            e.to_uint()
+    def rebuild(self, n_streams=8):
+        """List rebuild of every box, the boxes spread over n_streams streams."""
+        torch = self.torch
+        if getattr(self, "_rb_streams", None) is None or len(self._rb_streams) != n_streams:
+            self._rb_streams = [torch.cuda.Stream() for _ in range(n_streams)]
+        cur = torch.cuda.current_stream()
+        for st in self._rb_streams:
+            st.wait_stream(cur)
+        for k, e in enumerate(self.engines):
+            st = self._rb_streams[k % n_streams]
+            with torch.cuda.stream(st):
+                e.update_list(forced=1, stream=st)
+                e.to_uint(stream=st)
+        for st in self._rb_streams:
+            cur.wait_stream(st)
 
-    def _batch(self):
-        if self.batch is None:
-            self.batch = FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc)
-                                       for e in self.engines], self.dudl)
-        return self.batch
+    def _sub_batches(self, n):
+        """The boxes in n sub-batches of balanced cost, one sb_fep_batch each."""
+        if n not in self._batches:
+            parts = shard_boxes([box_cost(e.system) for e in self.engines], n)
+            self._batches[n] = [
+                FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc, e.dudl)
+                              for e in (self.engines[k] for k in part)])
+                for part in parts if part]
+        return self._batches[n]
 
-    def _eager_step(self):
+    def _eager_step(self, n=1):
         self.frc.zero_()
         if self.mode == "kernels":
-            self._batch().step()
+            for b in self._sub_batches(n):
+                b.step()
         else:
             for e in self.engines:
                 e.step()
 
     def capture(self, n_streams=1):
-        """Capture one force step of every box. In streams mode box k runs on stream
-        k mod n_streams."""
+        """Capture one force step of every box: in kernels mode n_streams sub-batches of
+        batched launches, in streams mode each box's own launches, box k on stream
+        k mod n_streams; the branches run concurrently."""
         torch = self.torch
-        self._eager_step()  # first calls size per-list scratch outside the capture
+        self._eager_step(n_streams)  # first calls size per-list scratch outside the capture
         torch.cuda.synchronize()
         main = torch.cuda.Stream()
         streams = [torch.cuda.Stream() for _ in range(n_streams)]
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=main):
+            cur = torch.cuda.current_stream()
+            self.frc.zero_()
+            for st in streams:
+                st.wait_stream(cur)
             if self.mode == "kernels":
-                self.frc.zero_()
-                self.batch.step()
+                for k, b in enumerate(self._sub_batches(n_streams)):
+                    b.step(stream=streams[k])
             else:
-                cur = torch.cuda.current_stream()
-                self.frc.zero_()
-                for st in streams:
-                    st.wait_stream(cur)
                 for k, e in enumerate(self.engines):
-                    with torch.cuda.stream(streams[k % n_streams]):
-                        e.step(stream=streams[k % n_streams])
-                for st in streams:
-                    cur.wait_stream(st)
+                    e.step(stream=streams[k % n_streams])
+            for st in streams:
+                cur.wait_stream(st)
         self.graph = g
         self.n_streams = n_streams
         self._streams = (main, streams)
@@ -199,12 +219,11 @@ class FepBatch:
         torch.cuda.synchronize()
         return a.elapsed_time(b) / reps
 
-    def tune(self, candidates=(1, 4, 8, 16, 48), reps=5):
-        """Capture the step; in streams mode pick the stream count by timing the replay.
-        Returns (streams, ms per replay)."""
-        if self.mode == "kernels":
-            self.capture(1)
-            return 1, self._replay_ms(reps)
+    def tune(self, candidates=None, reps=5):
+        """Capture the step with the branch count (sub-batches in kernels mode, streams in
+        streams mode) whose replay is fastest. Returns (count, ms per replay)."""
+        if candidates is None:
+            candidates = (1, 2, 3, 4, 6) if self.mode == "kernels" else (1, 4, 8, 16, 48)
         best = None
         for ns in candidates:
             if ns > len(self.engines):

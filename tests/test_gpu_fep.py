@@ -134,9 +134,21 @@ def test_plain_form_matches_oracle(name, cuda, oracle_lib):
 def _batch_boxes():
     # three boxes share the 30^3 grid (one batched FFT group of plane kernels), the 2600-water
     # box runs the pass-by-pass register transforms (a batched group without the plane kernel)
-    # and the 1700-water box the generic stage kernels (its own FFT launches)
+    # and the 1700-water box the generic stage kernels (its own FFT launches); the last box has
+    # too many perturbed atoms for the split form and runs the soft-core cluster kernel
+    many = systems.fep_box(500, 0.3, 106)
+    many["mask"] = np.asarray(many["mask"]).copy()
+    many["mask"][:300] = 1  # 280 water atoms join the 20 solute atoms in the perturbed group
     return [systems.fep_box(n, lam, 100 + k) for k, (n, lam) in
-            enumerate([(500, 0.0), (1700, 0.2), (800, 0.5), (2600, 0.8), (650, 1.0)])]
+            enumerate([(500, 0.0), (1700, 0.2), (800, 0.5), (2600, 0.8), (650, 1.0)])] + [many]
+
+
+def test_split_form_chosen(cuda):
+    from sponge_b200.fep import FepEngine
+    boxes = _batch_boxes()
+    assert FepEngine(boxes[0]).sc.split_form == (True, 20)
+    split, npert = FepEngine(boxes[-1]).sc.split_form
+    assert not split and npert == 300
 
 
 @pytest.mark.parametrize("mode", ["kernels", "streams"])
@@ -153,21 +165,28 @@ def test_batched_graph_matches_single_boxes(cuda, mode):
         e.step()
     cuda.cuda.synchronize()
     single = [(e.frc.cpu().numpy().copy(), float(e.dudl.item())) for e in batch.engines]
+    counts = (1, 2, 5)
     if mode == "kernels":
-        best = batch.tune(reps=2)
-        assert best[0] == 1
-        # pack, pair, spread, gather, finalize, finish, the force clear and the FFTs: 3 for the
-        # plane group, 5 for the pass-by-pass group, 5 for the generic box
-        assert batch.launches == 7 + 3 + 5 + 5, batch.launches
+        best = batch.tune(candidates=(2, 1), reps=2)
+        assert best[0] in (1, 2)
+        counts = (2, 1)
+        batch.capture(1)
+        # the force clear, pack, spread, gather, finalize, self sums, dU/dlambda; the packed
+        # pair kernel and the soft-core search and evaluation of the split boxes, the soft-core
+        # cluster kernel of the other; the FFTs: 3 for the plane group, 5 for the pass-by-pass
+        # group, 5 for the generic box
+        assert batch.launches == 7 + 4 + 3 + 5 + 5, batch.launches
     else:
         best = batch.tune(candidates=(1, 2, 5), reps=2)
         assert best[0] in (1, 2, 5)
-    for rep in range(2):  # the replay leaves every accumulator clear for the next one
-        batch.graph.replay()
-        cuda.cuda.synchronize()
-        for e, (f, d) in zip(batch.engines, single):
-            assert np.array_equal(e.frc.cpu().numpy(), f)
-            assert float(e.dudl.item()) == d
+    for n in counts:  # sub-batches (kernels) or streams (per-box branches)
+        batch.capture(n)
+        for rep in range(2):  # the replay leaves every accumulator clear for the next one
+            batch.graph.replay()
+            cuda.cuda.synchronize()
+            for e, (f, d) in zip(batch.engines, single):
+                assert np.array_equal(e.frc.cpu().numpy(), f), n
+                assert float(e.dudl.item()) == d, n
 
 
 def test_batch_refuses_changed_box(cuda):
@@ -179,8 +198,8 @@ def test_batch_refuses_changed_box(cuda):
         e.update_list(forced=1)
         e.to_uint()
     dudl = cuda.zeros(2, dtype=cuda.float64, device="cuda")
-    b = FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc) for e in engines],
-                     dudl)
+    b = FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc, dudl[k:k + 1])
+                      for k, e in enumerate(engines)])
     b.step()
     cuda.cuda.synchronize()
     assert float(dudl[0].item()) != 0.0
