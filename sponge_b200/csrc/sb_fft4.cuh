@@ -25,8 +25,11 @@ __host__ __device__ constexpr int sb_spf(int n) {
     return n % 2 == 0 ? 2 : n % 3 == 0 ? 3 : n % 5 == 0 ? 5 : n % 7 == 0 ? 7 : n;
 }
 
+// Every product that meets a sum is written out as an explicit fused multiply-add or an unfused
+// multiply (__fmul_rn), so the compiler has no contraction to choose: the plane kernel and the
+// pass-by-pass kernels, which inline these helpers in different surroundings, round alike.
 __device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_float2(fmaf(a.x, b.x, -__fmul_rn(a.y, b.y)), fmaf(a.x, b.y, __fmul_rn(a.y, b.x)));
 }
 
 // in-place N-point DFT of x (natural order in and out)
@@ -51,8 +54,8 @@ __device__ __forceinline__ void rdft(float2 (&x)[N]) {
         const float c = -0.5f, s = INV ? -0.86602540378443865f : 0.86602540378443865f;
         const float2 a = x[0], b = x[1], d = x[2];
         const float2 t1 = make_float2(b.x + d.x, b.y + d.y), t2 = make_float2(b.x - d.x, b.y - d.y);
-        const float2 m = make_float2(a.x + c * t1.x, a.y + c * t1.y);
-        const float2 st = make_float2(s * t2.y, -s * t2.x);
+        const float2 m = make_float2(fmaf(c, t1.x, a.x), fmaf(c, t1.y, a.y));
+        const float2 st = make_float2(__fmul_rn(s, t2.y), __fmul_rn(-s, t2.x));
         x[0] = make_float2(a.x + t1.x, a.y + t1.y);
         x[1] = make_float2(m.x + st.x, m.y + st.y);
         x[2] = make_float2(m.x - st.x, m.y - st.y);
@@ -330,16 +333,16 @@ __global__ void __launch_bounds__(SB_F4_ZR * F4<N1, N2>::T) k_zfwd4(
         } else {
             const int k2 = M - k;
             const float2 a = row[k], b = row[k2];
-            const float2 Ek = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
-            const float2 Ok = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
+            const float2 Ek = make_float2(__fmul_rn(0.5f, a.x + b.x), __fmul_rn(0.5f, a.y - b.y));
+            const float2 Ok = make_float2(__fmul_rn(0.5f, a.y + b.y), __fmul_rn(-0.5f, a.x - b.x));
             const float2 pk = ps[k];
-            const float2 Xk = make_float2(Ek.x + pk.x * Ok.x - pk.y * Ok.y,
-                                          Ek.y + pk.x * Ok.y + pk.y * Ok.x);
+            const float2 pO = c_mul(pk, Ok);
+            const float2 Xk = make_float2(Ek.x + pO.x, Ek.y + pO.y);
             if (k2 != k) {
                 const float2 w2 = make_float2(-pk.x, pk.y);
                 const float2 cE = make_float2(Ek.x, -Ek.y), cO = make_float2(Ok.x, -Ok.y);
-                row[k2] = make_float2(cE.x + w2.x * cO.x - w2.y * cO.y,
-                                      cE.y + w2.x * cO.y + w2.y * cO.x);
+                const float2 wO = c_mul(w2, cO);
+                row[k2] = make_float2(cE.x + wO.x, cE.y + wO.y);
             }
             row[k] = Xk;
         }
