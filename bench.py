@@ -17,7 +17,11 @@ ns/day = steps/s * 2 fs * 86400 / 1e6.
   force_only  the list update + force graph on frozen coordinates (no integrator)
   --impl reference  the CPU baseline: the FP64 multithreaded restatement of the same path
           (SPONGE has no CPU implementation) on the host cores, one full evaluation per step
+  fep48   beside the headline: the 48 batched FEP/TI lambda windows (618,180 atoms, soft core,
+          dU/dlambda every step) as --workload fep48 times them, 40 steps (--no-fep skips it)
   --workload water1m  the 1,000,512-atom water box with PME 216^3, both forms
+  --workload fep48    the 48 windows with their baselines (per-window graph branches, windows
+          one after another in both forms)
 
 Multi-GPU: independent replicas (one system per rank, no collective in the data path).
 """
@@ -227,7 +231,7 @@ def water1m_config():
 FEP_METRIC = "aggregate ns/day, %d FEP/TI lambda windows (soft-core), 1 B200"
 
 
-def run_fep(args, rank, world, local):
+def run_fep(args, rank, world, local, dist=None, emit=True):
     """48 uneven water boxes with a vanishing 20-atom solute, one lambda each, batched on each
     GPU: one launch per stage over all boxes (sb_fep_batch_step) under one captured CUDA graph
     (boxes sharded over ranks, the per-window dU/dlambda gathered at the end). Baselines on the
@@ -239,11 +243,12 @@ def run_fep(args, rank, world, local):
     from sponge_b200 import FORM_PLAIN, systems
     from sponge_b200.fep import FepBatch, FepEngine, box_cost, shard_boxes
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
+    own = False  # the process group is this function's (standalone run) or the caller's
+    if world > 1 and dist is None:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        own = True
     nbox = args.fep_boxes  # 48 for the workload; fewer (its first windows) for profiling
     boxes = [systems.config4(k) for k in range(nbox)]
     mine = shard_boxes([box_cost(b) for b in boxes], world)[rank]
@@ -317,9 +322,9 @@ def run_fep(args, rank, world, local):
     if dist is not None:
         dist.barrier()
     if rank != 0:
-        if dist is not None:
+        if own:
             dist.destroy_process_group()
-        return
+        return None
     atoms = sum(len(b["charge"]) for b in boxes)
     value = nbox * ns_per_day(ms * 1e-3)
     line = {
@@ -348,9 +353,11 @@ def run_fep(args, rank, world, local):
             "fixed_form_sequential_no_graph":
                 nbox * ns_per_day(base_seq * 1e-3) if base_seq else None},
     }
-    print(json.dumps(line), flush=True)
-    if dist is not None:
+    if emit:
+        print(json.dumps(line), flush=True)
+    if own:
         dist.destroy_process_group()
+    return line
 
 
 def hbm_view(traffic_bytes, ms):
@@ -563,6 +570,8 @@ def main():
     ap.add_argument("--form", default="fixed", choices=["fixed", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-fep", action="store_true",
+                    help="headline run: skip the batched FEP windows reported beside it")
     ap.add_argument("--fep-boxes", type=int, default=48,
                     help="fep48: number of windows (the first ones; 48 is the workload)")
     ap.add_argument("--fep-mode", default="kernels", choices=["kernels", "streams"],
@@ -652,6 +661,7 @@ def run_md(args, rank, world, local):
 
     def e2e_step():
         eng.crd.copy_(crd_host, non_blocking=True)
+        eng.to_uint()  # the caller's coordinates, converted as the step's input
         eng.md_step_graph()
         crd_host.copy_(eng.crd, non_blocking=True)
     e2e = timed_steps(e2e_step, args.steps, flush, stream, dist)
@@ -678,6 +688,12 @@ def run_md(args, rank, world, local):
     crd_snapshot = eng.crd.clone()
     uc = eng.uint_crd.cpu().numpy().view(np.uint32)
     f_fixed = eng.frc.cpu().numpy()
+    # the batched FEP/TI windows (config 4) on the same GPU, reported beside the headline
+    fep = None
+    if not big and not args.no_fep:
+        fa = argparse.Namespace(**vars(args))
+        fa.fep_boxes, fa.fep_mode, fa.steps, fa.warmup, fa.no_plain = 48, "kernels", 40, 5, True
+        fep = run_fep(fa, rank, world, local, dist=dist, emit=False)
     if rank != 0:
         if dist is not None:
             dist.barrier()
@@ -690,9 +706,10 @@ def run_md(args, rank, world, local):
     achieved = flops / (pair_ms * 1e-3) / 1e12
     rb = pme_bytes(eng.n, (eng.pme.fftx, eng.pme.ffty, eng.pme.fftz))
     hbm_peak = hbm_view(0, 1.0)["peak"]
-    # launches per MD step: fixed point, the 8 of the force step, the integrator; a rebuild (6)
-    # every 20 steps
-    launches = 10 if form == FORM_FIXED else None
+    # launches per MD step: the 7 of the accumulated force step (pack, pair, spread, z R2C,
+    # plane, z C2R, gather) and the integrator, which also writes the fixed-point coordinates;
+    # a rebuild (6, and the coordinate conversion after it) every 20 steps
+    launches = 8 if form == FORM_FIXED else None
     line = {
         "metric": metric,
         "value": world * ns_per_day(ms * 1e-3),
@@ -714,7 +731,7 @@ def run_md(args, rank, world, local):
         "e2e": {"value": world * ns_per_day(e2e_ms * 1e-3), "unit": "ns/day",
                 "h2d_bytes_per_step": int(eng.n * 12), "d2h_bytes_per_step": int(eng.n * 12)},
         "gpu_launches": None if launches is None else
-            int(round(args.steps * (launches + 6 / 20.0))),
+            int(round(args.steps * (launches + 7 / 20.0))),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
                      "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS,
                      "traffic": PAIR_DRAM_BYTES if not big else None,
@@ -773,6 +790,10 @@ def run_md(args, rank, world, local):
             pe.force()
             line["force_error_vs_fp64"]["plain"] = rel_rms(pe.frc.cpu().numpy(), ref_f)
         line["plain_form"] = plain
+    if fep is not None:
+        line["fep48"] = {k: fep[k] for k in ("metric", "value", "unit", "ms_per_step", "steps",
+                                            "force_step_ms", "rebuild_ms", "rebuild_interval",
+                                            "gpu_launches_per_step", "config")}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
