@@ -661,7 +661,6 @@ def run_md(args, rank, world, local):
 
     def e2e_step():
         eng.crd.copy_(crd_host, non_blocking=True)
-        eng.to_uint()  # the caller's coordinates, converted as the step's input
         eng.md_step_graph()
         crd_host.copy_(eng.crd, non_blocking=True)
     e2e = timed_steps(e2e_step, args.steps, flush, stream, dist)
@@ -706,10 +705,9 @@ def run_md(args, rank, world, local):
     achieved = flops / (pair_ms * 1e-3) / 1e12
     rb = pme_bytes(eng.n, (eng.pme.fftx, eng.pme.ffty, eng.pme.fftz))
     hbm_peak = hbm_view(0, 1.0)["peak"]
-    # launches per MD step: the 7 of the accumulated force step (pack, pair, spread, z R2C,
-    # plane, z C2R, gather) and the integrator, which also writes the fixed-point coordinates;
-    # a rebuild (6, and the coordinate conversion after it) every 20 steps
-    launches = 8 if form == FORM_FIXED else None
+    # launches per MD step: fixed point, the 8 of the force step, the integrator; a rebuild (6)
+    # every 20 steps
+    launches = 10 if form == FORM_FIXED else None
     line = {
         "metric": metric,
         "value": world * ns_per_day(ms * 1e-3),
@@ -731,7 +729,7 @@ def run_md(args, rank, world, local):
         "e2e": {"value": world * ns_per_day(e2e_ms * 1e-3), "unit": "ns/day",
                 "h2d_bytes_per_step": int(eng.n * 12), "d2h_bytes_per_step": int(eng.n * 12)},
         "gpu_launches": None if launches is None else
-            int(round(args.steps * (launches + 7 / 20.0))),
+            int(round(args.steps * (launches + 6 / 20.0))),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS,
                      "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS,
                      "traffic": PAIR_DRAM_BYTES if not big else None,

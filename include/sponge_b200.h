@@ -392,29 +392,6 @@ SB_API int sb_md_nve_settle_step(sb_settle* settle, const uint32_t* d_uint_crd,
                                  float* d_crd, float* d_acc, const float box[3],
                                  int need_pressure, float* d_pressure, void* stream);
 
-/* The MD step of the fixed form without the float force array: sb_nonbonded_force_accumulate
- * runs the fused force part (no energies or virial) and leaves the forces in the list's
- * fixed-point accumulator; sb_md_nve_settle_step_accumulated then reads and clears it (the
- * force each atom gets is the one sb_nonbonded_force's finalize would have added to a zeroed
- * d_frc, plus d_frc itself when not NULL), runs sb_md_nve_settle_step's leap-frog + SETTLE and
- * writes the new fixed-point coordinates into d_uint_crd (Crd_To_Uint_Crd of the new d_crd).
- * Two launches fewer per step than force + finalize + Crd_To_Uint_Crd + integrator. After a
- * list rebuild (which wraps d_crd in place) the caller converts the coordinates again
- * (sb_crd_to_uint_crd); sb_nl_build_count counts the rebuilds. */
-SB_API int sb_nonbonded_force_accumulate(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* pme,
-                                         const uint32_t* d_uint_crd, const float* d_charge,
-                                         const int* d_excluded_list_start,
-                                         const int* d_excluded_list,
-                                         const int* d_excluded_numbers, void* stream);
-SB_API int sb_md_nve_settle_step_accumulated(sb_settle* m, sb_neighbor_list* nl,
-                                             uint32_t* d_uint_crd, const float scaler[3],
-                                             const float* d_inverse_mass, const float* d_mass,
-                                             const float* d_frc, float* d_vel, float* d_crd,
-                                             float* d_acc, const float box[3], int need_pressure,
-                                             float* d_pressure, void* stream);
-/* Number of list rebuilds so far (host-side counter; no synchronisation). */
-SB_API int sb_nl_build_count(sb_neighbor_list* nl, int64_t* h_count);
-
 /* Crd_To_Uint_Crd (SPONGE/common.cu:264-287) with the quarter coefficient 0.25*2^32/L, as
  * MD_INFORMATION::MD_Information_Crd_To_Uint_Crd produces md_info.uint_crd. */
 SB_API int sb_crd_to_uint_crd(int atom_numbers, const float box_length[3], const float* d_crd,

@@ -113,10 +113,6 @@ _SIGS = {
     "sb_settle_apply": [_vp, _vp, _vp, _vp, _vp, _i, _vp, _vp],
     "sb_md_leap_frog": [_i, _vp, _vp, _vp, _vp, _vp, _f, _vp],
     "sb_md_nve_settle_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp],
-    "sb_md_nve_settle_step_accumulated": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                          _i, _vp, _vp],
-    "sb_nonbonded_force_accumulate": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
-    "sb_nl_build_count": [_vp, _vp],
 }
 
 
@@ -251,12 +247,6 @@ class NeighborList:
         f = ctypes.c_int()
         _check(lib().sb_nl_status(self.handle, ctypes.byref(f), _stream(None)))
         return f.value
-
-    def build_count(self):
-        """Rebuilds so far (host-side counter)."""
-        c = ctypes.c_int64()
-        _check(lib().sb_nl_build_count(self.handle, ctypes.byref(c)))
-        return c.value
 
     def set_prune(self, prune_buffer, prune_interval=0):
         """Pruned pair list for the packed pair kernel (sb_nl_set_prune; 0 turns it off)."""
@@ -458,15 +448,6 @@ def nonbonded_step(nl, lj, pme, crd, uint_crd, charge, excl, frc, need_energy=0,
                                    int(need_energy), int(need_virial), _ptr(atom_energy),
                                    _ptr(atom_virial), _ptr(d_virial), _ptr(d_potential),
                                    _stream(stream)))
-
-
-def nonbonded_force_accumulate(nl, lj, pme, uint_crd, charge, excl, stream=None):
-    """The fused force part leaving the forces in the list's fixed-point accumulator for
-    ``Settle.nve_step_accumulated`` (sb_nonbonded_force_accumulate); capturable."""
-    es, el, en = excl
-    _check(lib().sb_nonbonded_force_accumulate(nl.handle, lj.handle, pme.handle, _ptr(uint_crd),
-                                               _ptr(charge), _ptr(es), _ptr(el), _ptr(en),
-                                               _stream(stream)))
 
 
 def nonbonded_force(nl, lj, pme, uint_crd, charge, excl, frc, need_energy=0, need_virial=0,
@@ -770,17 +751,6 @@ class Settle:
                                            _ptr(inverse_mass), _ptr(mass), _ptr(frc), _ptr(vel),
                                            _ptr(crd), _ptr(acc), _box3(box_length),
                                            int(need_pressure), _ptr(pressure), _stream(stream)))
-
-    def nve_step_accumulated(self, nl, uint_crd, scaler, inverse_mass, mass, vel, crd,
-                             box_length, frc=None, acc=None, need_pressure=0, pressure=None,
-                             stream=None):
-        """``nve_step`` on the forces left in ``nl``'s accumulator by
-        ``nonbonded_force_accumulate`` (plus ``frc`` if given); writes the new fixed-point
-        coordinates into ``uint_crd`` (sb_md_nve_settle_step_accumulated)."""
-        _check(lib().sb_md_nve_settle_step_accumulated(
-            self.handle, nl.handle, _ptr(uint_crd), _box3(scaler), _ptr(inverse_mass),
-            _ptr(mass), _ptr(frc), _ptr(vel), _ptr(crd), _ptr(acc), _box3(box_length),
-            int(need_pressure), _ptr(pressure), _stream(stream)))
 
     def Clear(self):
         if self.handle:

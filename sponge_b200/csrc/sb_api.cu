@@ -62,8 +62,7 @@ static int nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* p
                            const uint32_t* d_uint_crd, const float* d_charge, const int* es,
                            const int* el, const int* en, float* d_frc, int need_energy,
                            int need_virial, float* d_atom_energy, float* d_atom_virial,
-                           float* d_virial, float* d_potential, void* stream,
-                           bool finalize = true) {
+                           float* d_virial, float* d_potential, void* stream) {
     float* d_direct = nullptr;
     float* d_corr = nullptr;
     SB_TRY(sb_pme_atom_energy_arrays(pme, &d_direct, &d_corr));
@@ -105,7 +104,6 @@ static int nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb_pme* p
         if (fork) SB_CHECK_CUDA(cudaStreamWaitEvent(s, pme->ev_join, 0));
         if (st) return st;
         if (st2) return st2;
-        if (!finalize) return SB_OK;  // the forces stay in the list's accumulator
         return sb_pme_fused_finish(pme, nl, d_frc, d_charge, need_virial, need_energy, d_virial,
                                    d_potential, s);
     }
@@ -164,31 +162,4 @@ extern "C" int sb_nonbonded_force(sb_neighbor_list* nl, sb_lennard_jones* lj, sb
     return nonbonded_force(nl, lj, pme, d_uint_crd, d_charge, es, el, en, d_frc, need_energy,
                            need_virial, d_atom_energy, d_atom_virial, d_virial, d_potential,
                            stream);
-}
-
-extern "C" int sb_nonbonded_force_accumulate(sb_neighbor_list* nl, sb_lennard_jones* lj,
-                                             sb_pme* pme, const uint32_t* d_uint_crd,
-                                             const float* d_charge, const int* es, const int* el,
-                                             const int* en, void* stream) {
-    if (!nl || !lj || !pme || !d_uint_crd || !d_charge) {
-        sb_set_error("sb_nonbonded_force_accumulate: null argument");
-        return SB_ERR_ARG;
-    }
-    if (lj->form != SB_FORM_FIXED || pme->form != SB_FORM_FIXED || nl->form != SB_FORM_FIXED ||
-        lj->n != nl->n || pme->n != nl->n) {
-        sb_set_error("sb_nonbonded_force_accumulate: needs the fixed-point form of all modules "
-                     "on one atom count");
-        return SB_ERR_ARG;
-    }
-    return nonbonded_force(nl, lj, pme, d_uint_crd, d_charge, es, el, en, nullptr, 0, 0, nullptr,
-                           nullptr, nullptr, nullptr, stream, false);
-}
-
-extern "C" int sb_nl_build_count(sb_neighbor_list* nl, int64_t* h_count) {
-    if (!nl || !h_count) {
-        sb_set_error("sb_nl_build_count: null argument");
-        return SB_ERR_ARG;
-    }
-    *h_count = (int64_t)nl->build_id;
-    return SB_OK;
 }

@@ -273,66 +273,15 @@ __global__ void k_settle_apply(int ntri, int npair, const SbTri* __restrict__ tr
     }
 }
 
-// The forces left in a neighbor list's slot-order fixed-point accumulator by the fused force
-// step (sb_nonbonded_force_accumulate), read and cleared the way k_finalize does it, plus the
-// caller's float forces when given: the force k_finalize would have left in frc.
-struct SbFixForces {
-    const int* atom_slot;  // null: the forces are in frc alone
-    long long* fix;
-    int slot_cap;
-    int* meta;             // the list's meta (a served prune request is retired here)
-    uint32_t* uc_out;      // the new fixed-point coordinates (Crd_To_Uint_Crd of crd)
-    float3 cu;             // its factors, 2^30 / box
-};
-
-__device__ __forceinline__ float3 md_force(const SbFixForces& F, const float* __restrict__ frc,
-                                           int a) {
-    if (!F.atom_slot) return ld3(frc, a);
-    const int sl = F.atom_slot[a];
-    const long long fx = F.fix[sl], fy = F.fix[F.slot_cap + sl], fz = F.fix[2 * F.slot_cap + sl];
-    if (fx | fy | fz) {
-        F.fix[sl] = 0;
-        F.fix[F.slot_cap + sl] = 0;
-        F.fix[2 * F.slot_cap + sl] = 0;
-    }
-    const float3 f = f3((float)((double)fx * SB_FORCE_UNSCALE), (float)((double)fy * SB_FORCE_UNSCALE),
-                        (float)((double)fz * SB_FORCE_UNSCALE));
-    return frc ? ld3(frc, a) + f : f;
-}
-
-__device__ __forceinline__ void md_uint(const SbFixForces& F, int a, float3 x) {
-    if (!F.uc_out) return;
-    F.uc_out[3 * a] = ((uint32_t)(int)__fmul_rn(x.x, F.cu.x)) << 2;
-    F.uc_out[3 * a + 1] = ((uint32_t)(int)__fmul_rn(x.y, F.cu.y)) << 2;
-    F.uc_out[3 * a + 2] = ((uint32_t)(int)__fmul_rn(x.z, F.cu.z)) << 2;
-}
-
-// leap_frog_atom with the force of md_force
-__device__ __forceinline__ void leap_frog_atom_f(const SbFixForces& F, int i,
-                                                 const float* __restrict__ inv_mass,
-                                                 const float* __restrict__ frc,
-                                                 float* __restrict__ vel, float* __restrict__ crd,
-                                                 float* __restrict__ acc, float dt) {
-    float3 v = ld3(vel, i), x = ld3(crd, i), a;
-    leap_frog_regs(inv_mass[i], md_force(F, frc, i), v, x, a, dt);
-    if (acc) st3(acc, i, a);
-    st3(vel, i, v);
-    st3(crd, i, x);
-}
-
-// the three calls in one launch: triangles, pairs, then the unconstrained atoms; with F.fix the
-// forces come from the list's accumulator (which this launch clears) and the new fixed-point
-// coordinates are written (every atom belongs to one thread, which reads its atoms'
-// step-start fixed-point coordinates before it writes the new ones)
+// the three calls in one launch: triangles, pairs, then the unconstrained atoms
 __global__ void k_md_step(int ntri, int npair, int nfree, const SbTri* __restrict__ tri,
                           const SbCPair* __restrict__ pr, const int* __restrict__ free_atoms,
-                          const uint32_t* uc, float3 s,
+                          const uint32_t* __restrict__ uc, float3 s,
                           const float* __restrict__ inv_mass, const float* __restrict__ mass,
                           const float* __restrict__ frc, float* __restrict__ vel,
                           float* __restrict__ crd, float* __restrict__ acc, float3 L, float dt,
-                          float vf, float xf, float* __restrict__ vir, SbFixForces F) {
+                          float vf, float xf, float* __restrict__ vir) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t == 0 && F.meta) sb_retire_prune(F.meta);
     float v = 0.f;
     if (t < ntri) {
         // every load of the triangle is issued before the arithmetic, which then runs on
@@ -341,8 +290,7 @@ __global__ void k_md_step(int ntri, int npair, int nfree, const SbTri* __restric
         const float3 BA = udisp(uc, T.B, T.A, s), CA = udisp(uc, T.C, T.A, s);
         float3 xA = ld3(crd, T.A), xB = ld3(crd, T.B), xC = ld3(crd, T.C);
         float3 vA = ld3(vel, T.A), vB = ld3(vel, T.B), vC = ld3(vel, T.C);
-        const float3 fA = md_force(F, frc, T.A), fB = md_force(F, frc, T.B),
-                     fC = md_force(F, frc, T.C);
+        const float3 fA = ld3(frc, T.A), fB = ld3(frc, T.B), fC = ld3(frc, T.C);
         const float iA = inv_mass[T.A], iB = inv_mass[T.B], iC = inv_mass[T.C];
         const float mA = mass[T.A], mB = mass[T.B], mC = mass[T.C];
         float3 aA, aB, aC;
@@ -361,23 +309,16 @@ __global__ void k_md_step(int ntri, int npair, int nfree, const SbTri* __restric
         st3(vel, T.A, vA);
         st3(vel, T.B, vB);
         st3(vel, T.C, vC);
-        md_uint(F, T.A, xA);
-        md_uint(F, T.B, xB);
-        md_uint(F, T.C, xC);
         vir[t] = v;
     } else if (t < ntri + npair) {
         const SbCPair P = pr[t - ntri];
         const float3 AB = udisp(uc, P.j, P.i, s);
-        leap_frog_atom_f(F, P.i, inv_mass, frc, vel, crd, acc, dt);
-        leap_frog_atom_f(F, P.j, inv_mass, frc, vel, crd, acc, dt);
+        leap_frog_atom(P.i, inv_mass, frc, vel, crd, acc, dt);
+        leap_frog_atom(P.j, inv_mass, frc, vel, crd, acc, dt);
         settle_pair_one(P, AB, mass, crd, vel, L, dt, vf, xf, v);
-        md_uint(F, P.i, ld3(crd, P.i));
-        md_uint(F, P.j, ld3(crd, P.j));
         vir[t] = v;
     } else if (t < ntri + npair + nfree) {
-        const int a = free_atoms[t - ntri - npair];
-        leap_frog_atom_f(F, a, inv_mass, frc, vel, crd, acc, dt);
-        md_uint(F, a, ld3(crd, a));
+        leap_frog_atom(free_atoms[t - ntri - npair], inv_mass, frc, vel, crd, acc, dt);
     }
 }
 
@@ -591,29 +532,6 @@ extern "C" int sb_md_leap_frog(int atom_numbers, const float* d_inverse_mass, co
     return SB_OK;
 }
 
-static int md_step_launch(sb_settle* m, const uint32_t* d_uint_crd, const float scaler[3],
-                          const float* d_inverse_mass, const float* d_mass, const float* d_frc,
-                          float* d_vel, float* d_crd, float* d_acc, const float box[3],
-                          int need_pressure, float* d_pressure, const SbFixForces& F,
-                          cudaStream_t s) {
-    if (m->nrest > 0) {
-        sb_set_error("sb_md_nve_settle_step: %d constrained pairs need another constraint scheme",
-                     m->nrest);
-        return SB_ERR_STATE;
-    }
-    const int nt = m->ntri + m->npair + m->nfree;
-    if (nt > 0) {
-        k_md_step<<<(nt + 127) / 128, 128, 0, s>>>(
-            m->ntri, m->npair, m->nfree, m->d_tri, m->d_pair, m->d_free, d_uint_crd,
-            make_float3(scaler[0], scaler[1], scaler[2]), d_inverse_mass, d_mass, d_frc, d_vel,
-            d_crd, d_acc, make_float3(box[0], box[1], box[2]), m->dt, m->v_factor, m->x_factor,
-            m->d_vir, F);
-        SB_CHECK_LAUNCH();
-    }
-    if (need_pressure) SB_TRY(add_pressure(m, box, d_pressure, s));
-    return SB_OK;
-}
-
 extern "C" int sb_md_nve_settle_step(sb_settle* m, const uint32_t* d_uint_crd,
                                      const float scaler[3], const float* d_inverse_mass,
                                      const float* d_mass, const float* d_frc, float* d_vel,
@@ -624,33 +542,21 @@ extern "C" int sb_md_nve_settle_step(sb_settle* m, const uint32_t* d_uint_crd,
         sb_set_error("sb_md_nve_settle_step: null argument");
         return SB_ERR_ARG;
     }
-    const SbFixForces F{nullptr, nullptr, 0, nullptr, nullptr, make_float3(0.f, 0.f, 0.f)};
-    return md_step_launch(m, d_uint_crd, scaler, d_inverse_mass, d_mass, d_frc, d_vel, d_crd,
-                          d_acc, box, need_pressure, d_pressure, F, sb_stream(stream));
-}
-
-extern "C" int sb_md_nve_settle_step_accumulated(sb_settle* m, sb_neighbor_list* nl,
-                                                 uint32_t* d_uint_crd, const float scaler[3],
-                                                 const float* d_inverse_mass, const float* d_mass,
-                                                 const float* d_frc, float* d_vel, float* d_crd,
-                                                 float* d_acc, const float box[3],
-                                                 int need_pressure, float* d_pressure,
-                                                 void* stream) {
-    if (!m || !nl || !d_uint_crd || !scaler || !d_inverse_mass || !d_mass || !d_vel || !d_crd ||
-        !box || (need_pressure && !d_pressure)) {
-        sb_set_error("sb_md_nve_settle_step_accumulated: null argument");
-        return SB_ERR_ARG;
+    if (m->nrest > 0) {
+        sb_set_error("sb_md_nve_settle_step: %d constrained pairs need another constraint scheme",
+                     m->nrest);
+        return SB_ERR_STATE;
     }
-    if (nl->n != m->n || nl->form != SB_FORM_FIXED) {
-        sb_set_error("sb_md_nve_settle_step_accumulated: needs a fixed-form list of %d atoms",
-                     m->n);
-        return SB_ERR_ARG;
+    cudaStream_t s = sb_stream(stream);
+    const int nt = m->ntri + m->npair + m->nfree;
+    if (nt > 0) {
+        k_md_step<<<(nt + 127) / 128, 128, 0, s>>>(
+            m->ntri, m->npair, m->nfree, m->d_tri, m->d_pair, m->d_free, d_uint_crd,
+            make_float3(scaler[0], scaler[1], scaler[2]), d_inverse_mass, d_mass, d_frc, d_vel,
+            d_crd, d_acc, make_float3(box[0], box[1], box[2]), m->dt, m->v_factor, m->x_factor,
+            m->d_vir);
+        SB_CHECK_LAUNCH();
     }
-    SB_TRY(sb_nl_ensure_built(nl));
-    float cu[3];
-    for (int d = 0; d < 3; d++) cu[d] = (0.25f * 4294967296.0f) / box[d];
-    const SbFixForces F{nl->atom_slot, nl->fix, nl->slot_cap, nl->meta, d_uint_crd,
-                        make_float3(cu[0], cu[1], cu[2])};
-    return md_step_launch(m, d_uint_crd, scaler, d_inverse_mass, d_mass, d_frc, d_vel, d_crd,
-                          d_acc, box, need_pressure, d_pressure, F, sb_stream(stream));
+    if (need_pressure) SB_TRY(add_pressure(m, box, d_pressure, s));
+    return SB_OK;
 }

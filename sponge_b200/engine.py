@@ -10,7 +10,7 @@ neighbor list. The engine owns device copies of one system's arrays (from
 import numpy as np
 
 from . import (FORM_FIXED, LennardJones, NeighborList, ParticleMeshEwald, _require_cuda,
-               crd_to_uint_crd, nonbonded_force, nonbonded_force_accumulate, nonbonded_step)
+               crd_to_uint_crd, nonbonded_force, nonbonded_step)
 
 
 def scaled_lj_tables(system):
@@ -57,10 +57,8 @@ class NonbondedEngine:
         self.d_virial = torch.zeros(1, dtype=torch.float32, device=dev)
         self.d_potential = torch.zeros(1, dtype=torch.float32, device=dev)
         self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
-        self.form = form
         self._graph = None
         self._md_graph = None
-        self._md_builds = None  # list rebuilds seen by the captured MD step
 
     @property
     def excl(self):
@@ -126,7 +124,6 @@ class NonbondedEngine:
         self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
         self._graph = None
         self._md_graph = None
-        self._md_builds = None
 
     def capture_force_graph(self):
         """Capture (frc = 0; force part) once as a CUDA graph; ``step_graph`` replays it after
@@ -152,71 +149,39 @@ class NonbondedEngine:
             self.capture_force_graph()
         self._graph.replay()
 
-    def md_step(self, settle, inverse_mass, mass, vel, acc=None, accumulated=None):
+    def md_step(self, settle, inverse_mass, mass, vel, acc=None):
         """One NVE step as Main_Calculate_Force + Main_Iteration run it (SPONGE/main.cu:162-329,
         :376), eagerly: fixed-point coordinates, forces (list as it stands), then the fused
-        leap-frog + SETTLE launch (``settle``: a Settle handle with no constraint pairs left).
-        ``accumulated`` (default: on in the fixed form): the forces stay in the list's
-        fixed-point accumulator and the integrator launch reads them and writes the new
-        fixed-point coordinates (sb_nonbonded_force_accumulate +
-        sb_md_nve_settle_step_accumulated: the same forces, two launches fewer); ``self.frc``
-        then holds no forces."""
-        if accumulated is None:
-            accumulated = self.form == FORM_FIXED
+        leap-frog + SETTLE launch (``settle``: a Settle handle with no constraint pairs left)."""
         crd_to_uint_crd(self.crd, self.box, out=self.uint_crd)
-        if accumulated:
-            self.md_step_accumulated(settle, inverse_mass, mass, vel, acc)
-            return
         self.frc.zero_()
         self.force()
         settle.nve_step(self.uint_crd, self.scaler, inverse_mass, mass, self.frc, vel, self.crd,
                         self.box, acc=acc)
 
-    def md_step_accumulated(self, settle, inverse_mass, mass, vel, acc=None):
-        """The accumulated MD step from fixed-point coordinates already in ``uint_crd``."""
-        nonbonded_force_accumulate(self.nl, self.lj, self.pme, self.uint_crd, self.charge,
-                                   self.excl)
-        settle.nve_step_accumulated(self.nl, self.uint_crd, self.scaler, inverse_mass, mass, vel,
-                                    self.crd, self.box, acc=acc)
-
-    def capture_md_graph(self, settle, inverse_mass, mass, vel, acc=None, accumulated=None):
+    def capture_md_graph(self, settle, inverse_mass, mass, vel, acc=None):
         """Capture ``md_step`` once as a CUDA graph (the integrator and SETTLE behind the force
         graph); ``md_step_graph`` replays it after the list update by its policy. The buffers
         passed here are the ones every replay uses. Call ``md_step`` once eagerly first (lazy
-        per-list buffers). In the accumulated form the graph starts from ``uint_crd`` (written
-        by the previous step's integrator launch), and ``md_step_graph`` converts the
-        coordinates again only after a list rebuild, which wraps them in place."""
+        per-list buffers)."""
         torch = self.torch
-        if accumulated is None:
-            accumulated = self.form == FORM_FIXED
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         side = torch.cuda.Stream()
         with torch.cuda.graph(g, stream=side):
-            if accumulated:
-                self.md_step_accumulated(settle, inverse_mass, mass, vel, acc)
-            else:
-                self.md_step(settle, inverse_mass, mass, vel, acc, accumulated=False)
+            self.md_step(settle, inverse_mass, mass, vel, acc)
         self._md_graph = g
-        self._md_args = (settle, inverse_mass, mass, vel, acc, accumulated)
-        self._md_builds = self.nl.build_count() if accumulated else None
+        self._md_args = (settle, inverse_mass, mass, vel, acc)
         return g
 
     def md_step_graph(self):
         """List update by its policy (eager, wraps the coordinates on rebuilds), then the captured
-        MD step (captured again, with the buffers of the last capture, after a box change). In
-        the accumulated form a caller that writes ``self.crd`` between steps converts it with
-        ``to_uint()`` before the next one."""
+        MD step (captured again, with the buffers of the last capture, after a box change)."""
         self.update_list()
         if self._md_graph is None:
             self.md_step(*self._md_args)
             self.capture_md_graph(*self._md_args)
             return
-        if self._md_builds is not None:
-            b = self.nl.build_count()
-            if b != self._md_builds:
-                self.to_uint()  # the rebuild wrapped the coordinates
-                self._md_builds = b
         self._md_graph.replay()
 
     def potential(self):

@@ -221,37 +221,3 @@ def test_md_step_graph_matches_eager(torch, oracle_lib):
     assert np.all(np.isfinite(c))
     d = H.distances(c, s["box"], pi, pj)
     assert np.abs(d - pr).max() < 5e-5
-
-
-def test_accumulated_md_step_matches_separate_calls(torch):
-    """The accumulated MD step (forces left in the list's fixed-point accumulator, read and
-    cleared by the integrator launch, which also writes the new fixed-point coordinates) gives
-    the bits of force + finalize + Crd_To_Uint_Crd + integrator, through a list rebuild."""
-    from sponge_b200 import NonbondedEngine, Settle, constrain_pairs_from_bonds, sponge_io
-    from sponge_b200 import systems as sysmod
-    s = sysmod.config0()
-    a, b, r, mass = sponge_io.bonds_and_masses(s)
-    pi, pj, pr = constrain_pairs_from_bonds(a, b, r, mass)
-    n = len(mass)
-    dt = float(np.float32(np.float32(0.0005) * np.float32(20.455)))
-    m64 = mass.astype(np.float64)
-    inv = torch.tensor(np.divide(1.0, m64, out=np.zeros_like(m64), where=m64 != 0)
-                       .astype(np.float32), device="cuda")
-    m_t = torch.tensor(mass, device="cuda")
-    runs = []
-    for accumulated in (True, False):
-        eng = NonbondedEngine(s, refresh_interval=3)
-        eng.update_list(forced=1)
-        vel = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
-        st = Settle(n, pi, pj, pr, mass, dt)
-        for _ in range(5):
-            eng.update_list()
-            eng.md_step(st, inv, m_t, vel, accumulated=accumulated)
-        torch.cuda.synchronize()
-        if accumulated:
-            uc = eng.uint_crd.cpu().numpy().copy()  # written by the integrator launch
-            eng.to_uint()
-            assert np.array_equal(uc, eng.uint_crd.cpu().numpy())
-        runs.append((eng.crd.cpu().numpy(), vel.cpu().numpy()))
-    assert np.array_equal(runs[0][0], runs[1][0])
-    assert np.array_equal(runs[0][1], runs[1][1])
