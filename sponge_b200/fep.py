@@ -135,8 +135,7 @@ class FepBatch:
             return 1 + sum(b.launches for b in self._batches[self.n_streams])
         return None
 
-    def rebuild(self, n_streams=8):
-        """List rebuild of every box, the boxes spread over n_streams streams."""
+    def _rebuild_all(self, n_streams):
         torch = self.torch
         if getattr(self, "_rb_streams", None) is None or len(self._rb_streams) != n_streams:
             self._rb_streams = [torch.cuda.Stream() for _ in range(n_streams)]
@@ -150,6 +149,22 @@ class FepBatch:
                 e.to_uint(stream=st)
         for st in self._rb_streams:
             cur.wait_stream(st)
+
+    def rebuild(self, n_streams=8):
+        """List rebuild of every box (a forced update: no host synchronisation), the boxes spread
+        over n_streams streams. The first call runs eagerly and captures the same launches as a
+        CUDA graph, which the later calls replay (the host would otherwise spend longer issuing
+        the seven launches of each box than the device spends running them)."""
+        torch = self.torch
+        if getattr(self, "_rb_graph", None) is not None:
+            self._rb_graph.replay()
+            return
+        self._rebuild_all(n_streams)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=torch.cuda.Stream()):
+            self._rebuild_all(n_streams)
+        self._rb_graph = g
 
     def _sub_batches(self, n):
         """The boxes in n sub-batches of balanced cost, one sb_fep_batch each."""

@@ -182,6 +182,8 @@ def test_batched_graph_matches_single_boxes(cuda, mode):
     for n in counts:  # sub-batches (kernels) or streams (per-box branches)
         batch.capture(n)
         for rep in range(2):  # the replay leaves every accumulator clear for the next one
+            if rep:
+                batch.rebuild()  # the captured rebuild of all lists: the same lists again
             batch.graph.replay()
             cuda.cuda.synchronize()
             for e, (f, d) in zip(batch.engines, single):
