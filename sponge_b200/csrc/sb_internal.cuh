@@ -424,9 +424,9 @@ int sb_pair_fep(sb_neighbor_list* nl, const float2* d_AB, int ntypes, float cuto
                 cudaStream_t s);
 struct SbX2Batch;
 int sb_pair_batch_create(int nb, const int* box_ids, sb_neighbor_list* const* nls,
-                         const int* ntypes, const float* cutoffs, const float* betas, int n_all,
-                         SbX2Batch** out);
-int sb_pair_batch_launch(const SbX2Batch* x, const SbFepBox* d_boxes, cudaStream_t s);
+                         const float2* const* tables, const int* ntypes, const float* cutoffs,
+                         const float* betas, SbX2Batch** out);
+int sb_pair_batch_launch(const SbX2Batch* x, cudaStream_t s);
 int sb_pair_batch_launches(const SbX2Batch* x);
 void sb_pair_batch_destroy(SbX2Batch* x);
 

@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "sb_ewald.cuh"
@@ -638,41 +639,63 @@ struct X2BoxVar {
     uint4* xq_prune;
 };
 
-// one-warp block per cluster of any box: tab[b] = {box, cluster}; C holds the common fields as
-// kernel parameters (constant-bank operands, as in k_pair_x2), the box's own ones are loaded
-__global__ void __launch_bounds__(32, 24) k_pair_x2_batch(PairParams C,
-                                                          const X2BoxVar* __restrict__ V,
-                                                          const SbFepBox* __restrict__ B,
-                                                          const int2* __restrict__ tab) {
+// One one-warp block per cluster of any window. The windows' pointers and constants travel in
+// the kernel parameters (a constant-bank block read with a block-uniform index; the fields that
+// all windows of a launch share stay plain PairParams operands, as in k_pair_x2), and a block
+// finds its window by a binary search over the windows' first blocks: a table entry and a
+// descriptor in global memory, which each block waited for before its cluster's own loads, made
+// the launch 2 % slower on fep48.
+#define SB_X2_BATCH_MAX 96  // windows per launch
+struct X2Box {
+    const int* meta;
+    const int* cl_count;
+    const uint32_t* cl_ent;
+    const uint4* xq;
+    const int* stype;
+    const float2* AB;
+    const int* slot_atom;
+    long long* fix;
+    X2BoxVar v;
+};
+struct X2BatchParams {
+    PairParams C;
+    int nbox;
+    int first[SB_X2_BATCH_MAX + 1];  // first block of each window; first[nbox] = grid size
+    X2Box box[SB_X2_BATCH_MAX];
+};
+
+__global__ void __launch_bounds__(32, 24) k_pair_x2_batch(const __grid_constant__ X2BatchParams B) {
     extern __shared__ float4 ctab[];
-    const int2 t = tab[blockIdx.x];
-    const SbFepBox& b = B[t.x];
-    if (t.y >= b.meta[0]) return;
-    const X2BoxVar v = V[t.x];
-    PairParams P = C;
-    P.sx = v.sx;
-    P.sy = v.sy;
-    P.sz = v.sz;
-    P.nt = v.nt;
-    P.slot_cap = v.slot_cap;
-    P.ent_cap = v.ent_cap;
-    P.rb2 = v.rb2;
-    P.prune = v.prune;
-    P.cl_count_in = v.cl_count_in;
-    P.cl_ent_in = v.cl_ent_in;
-    P.xq_prune = v.xq_prune;
-    x2_cluster<0>(P, t.y, threadIdx.x & 31, ctab, b.cl_count, b.cl_ent, b.xq, b.stype, b.ABu,
-                  b.slot_atom, b.fix, nullptr, nullptr, nullptr);
+    const int b = blockIdx.x;
+    int lo = 0, hi = B.nbox - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (B.first[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const X2Box& w = B.box[lo];
+    const int c = b - B.first[lo];
+    if (c >= w.meta[0]) return;
+    PairParams P = B.C;
+    P.sx = w.v.sx;
+    P.sy = w.v.sy;
+    P.sz = w.v.sz;
+    P.nt = w.v.nt;
+    P.slot_cap = w.v.slot_cap;
+    P.ent_cap = w.v.ent_cap;
+    P.rb2 = w.v.rb2;
+    P.prune = w.v.prune;
+    P.cl_count_in = w.v.cl_count_in;
+    P.cl_ent_in = w.v.cl_ent_in;
+    P.xq_prune = w.v.xq_prune;
+    x2_cluster<0>(P, c, threadIdx.x & 31, ctab, w.cl_count, w.cl_ent, w.xq, w.stype, w.AB,
+                  w.slot_atom, w.fix, nullptr, nullptr, nullptr);
 }
 
 struct SbX2Batch {
-    struct Group {
-        PairParams C;
-        int off, n;
-    };
-    std::vector<Group> groups;
-    X2BoxVar* d_var = nullptr;
-    int2* d_tab = nullptr;
+    std::vector<X2BatchParams> launches;  // windows with equal common fields, up to 96 a launch
     size_t smem = 0;
 };
 
@@ -685,83 +708,67 @@ static bool x2_same_common(const PairParams& a, const PairParams& b) {
     return true;
 }
 
-void sb_pair_batch_destroy(SbX2Batch* x) {
-    if (!x) return;
-    sb_free(x->d_var);
-    sb_free(x->d_tab);
-    delete x;
-}
+void sb_pair_batch_destroy(SbX2Batch* x) { delete x; }
 
 int sb_pair_batch_create(int nb, const int* box_ids, sb_neighbor_list* const* nls,
-                         const int* ntypes, const float* cutoffs, const float* betas,
-                         int n_all, SbX2Batch** out) {
+                         const float2* const* tables, const int* ntypes, const float* cutoffs,
+                         const float* betas, SbX2Batch** out) {
     *out = nullptr;
-    SbX2Batch* x = new SbX2Batch();
     std::vector<PairParams> P(nb);
-    std::vector<X2BoxVar> var(n_all);
+    size_t smem = 0;
     for (int i = 0; i < nb; i++) {
         P[i] = pair_params_of(nls[i], ntypes[i], cutoffs[i], betas[i]);
         if (P[i].wide) {
             sb_set_error("sb_pair_batch_create: box %d beyond the packed kernel's Ewald fit",
                          box_ids[i]);
-            delete x;
             return SB_ERR_ARG;
         }
-        const PairParams& q = P[i];
-        var[box_ids[i]] = X2BoxVar{q.sx, q.sy, q.sz, q.nt, q.slot_cap, q.ent_cap, q.rb2,
-                                   q.prune, q.cl_count_in, q.cl_ent_in, q.xq_prune};
-        x->smem = std::max(x->smem, sizeof(float4) * 4 * (size_t)ntypes[i]);
+        smem = std::max(smem, sizeof(float4) * 4 * (size_t)ntypes[i]);
     }
-    std::vector<int2> tab;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_pair_x2_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+        sb_set_error("sb_pair_batch_create: shared memory attribute refused");
+        return SB_ERR_CUDA;
+    }
+    SbX2Batch* x = new SbX2Batch();
+    x->smem = smem;
     std::vector<char> done(nb, 0);
     for (int i = 0; i < nb; i++) {
         if (done[i]) continue;
-        SbX2Batch::Group g{P[i], (int)tab.size(), 0};
+        X2BatchParams L;
+        memset(&L, 0, sizeof(L));
+        L.C = P[i];
         for (int j = i; j < nb; j++) {
             if (done[j] || !x2_same_common(P[i], P[j])) continue;
             done[j] = 1;
-            for (int c = 0; c < nls[j]->clu_cap; c++) tab.push_back(make_int2(box_ids[j], c));
+            if (L.nbox == SB_X2_BATCH_MAX) {
+                x->launches.push_back(L);
+                memset(&L.box, 0, sizeof(L.box));
+                L.nbox = 0;
+                L.first[0] = 0;
+            }
+            sb_neighbor_list* nl = nls[j];
+            const PairParams& q = P[j];
+            L.box[L.nbox] = X2Box{nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype,
+                                  tables[j], nl->slot_atom, nl->fix,
+                                  X2BoxVar{q.sx, q.sy, q.sz, q.nt, q.slot_cap, q.ent_cap, q.rb2,
+                                           q.prune, q.cl_count_in, q.cl_ent_in, q.xq_prune}};
+            L.first[L.nbox + 1] = L.first[L.nbox] + nl->clu_cap;
+            L.nbox++;
         }
-        g.n = (int)tab.size() - g.off;
-        x->groups.push_back(g);
-    }
-    int st = SB_OK;
-    if (!tab.empty()) {
-        st = sb_malloc((void**)&x->d_var, sizeof(X2BoxVar) * var.size(), "x2 batch params");
-        if (!st) st = sb_malloc((void**)&x->d_tab, sizeof(int2) * tab.size(), "x2 batch table");
-        if (!st && (cudaMemcpy(x->d_var, var.data(), sizeof(X2BoxVar) * var.size(),
-                               cudaMemcpyHostToDevice) != cudaSuccess ||
-                    cudaMemcpy(x->d_tab, tab.data(), sizeof(int2) * tab.size(),
-                               cudaMemcpyHostToDevice) != cudaSuccess)) {
-            sb_set_error("sb_pair_batch_create: upload failed");
-            st = SB_ERR_CUDA;
-        }
-    }
-    if (!st && x->smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k_pair_x2_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)x->smem) != cudaSuccess) {
-        sb_set_error("sb_pair_batch_create: shared memory attribute refused");
-        st = SB_ERR_CUDA;
-    }
-    if (st) {
-        sb_pair_batch_destroy(x);
-        return st;
+        if (L.nbox) x->launches.push_back(L);
     }
     *out = x;
     return SB_OK;
 }
 
-int sb_pair_batch_launch(const SbX2Batch* x, const SbFepBox* d_boxes, cudaStream_t s) {
-    for (const auto& g : x->groups) {
-        if (!g.n) continue;
-        k_pair_x2_batch<<<g.n, 32, x->smem, s>>>(g.C, x->d_var, d_boxes, x->d_tab + g.off);
+int sb_pair_batch_launch(const SbX2Batch* x, cudaStream_t s) {
+    for (const auto& L : x->launches) {
+        k_pair_x2_batch<<<L.first[L.nbox], 32, x->smem, s>>>(L);
         SB_CHECK_LAUNCH();
     }
     return SB_OK;
 }
 
-int sb_pair_batch_launches(const SbX2Batch* x) {
-    int n = 0;
-    for (const auto& g : x->groups) n += g.n ? 1 : 0;
-    return n;
-}
+int sb_pair_batch_launches(const SbX2Batch* x) { return (int)x->launches.size(); }

@@ -1556,18 +1556,20 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
     if (!st) {
         std::vector<int> ids, nts;
         std::vector<sb_neighbor_list*> xl;
+        std::vector<const float2*> tabs;
         std::vector<float> cuts, betas;
         for (int k = 0; k < n_boxes; k++) {
             if (!b->hbox[k].split) continue;
             ids.push_back(k);
             xl.push_back(nls[k]);
+            tabs.push_back(scs[k]->d_ABu);
             nts.push_back(scs[k]->ntA + 1);
             cuts.push_back(scs[k]->cutoff);
             betas.push_back(pmes[k]->beta);
         }
         if (!ids.empty())
-            st = sb_pair_batch_create((int)ids.size(), ids.data(), xl.data(), nts.data(),
-                                      cuts.data(), betas.data(), n_boxes, &b->x2);
+            st = sb_pair_batch_create((int)ids.size(), ids.data(), xl.data(), tabs.data(),
+                                      nts.data(), cuts.data(), betas.data(), &b->x2);
     }
     // grids of equal sizes and transform family share batched FFT launches
     for (int k = 0; k < n_boxes && !st; k++) {
@@ -1760,7 +1762,7 @@ extern "C" int sb_fep_batch_step(sb_fep_batch* b, void* stream) {
         SB_CHECK_LAUNCH();
     }
     SB_CHECK_CUDA(cudaEventRecord(b->ev_pert, b->pert));
-    if (b->x2) SB_TRY(sb_pair_batch_launch(b->x2, b->d_box, s));
+    if (b->x2) SB_TRY(sb_pair_batch_launch(b->x2, s));
     for (const auto& g : b->sc_groups) {
         const ScParams& C = b->hP[g.first_box];
         if (g.n_pair) {
