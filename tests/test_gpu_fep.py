@@ -208,3 +208,26 @@ def test_batch_refuses_changed_box(cuda):
     engines[1].sc.set_lambda(0.7)
     with pytest.raises(sponge_b200.SpongeError, match="create the batch again"):
         b.step()
+
+
+def test_batch_beyond_one_pair_launch(cuda):
+    """98 windows: the packed pair kernel carries at most 96 windows' descriptors per launch, so
+    the batch issues two; every window still gets the bits of its own step."""
+    from sponge_b200.fep import FepBatch
+    boxes = [systems.fep_box(500, k / 97.0, 300 + k) for k in range(98)]
+    batch = FepBatch(boxes)
+    batch.rebuild()
+    for e in batch.engines:
+        e.frc.zero_()
+        e.step()
+    cuda.cuda.synchronize()
+    single = [(e.frc.cpu().numpy().copy(), float(e.dudl.item())) for e in batch.engines]
+    batch.capture(1)
+    # the force clear, pack, spread, gather, finalize, self sums, dU/dlambda; two packed pair
+    # launches; the soft-core search and evaluation; the three FFT stages of the one grid size
+    assert batch.launches == 7 + 2 + 2 + 3, batch.launches
+    batch.graph.replay()
+    cuda.cuda.synchronize()
+    for e, (f, d) in zip(batch.engines, single):
+        assert np.array_equal(e.frc.cpu().numpy(), f)
+        assert float(e.dudl.item()) == d
