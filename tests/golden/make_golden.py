@@ -29,6 +29,7 @@ from sponge_b200 import systems  # noqa: E402
 CASES = {
     "small": lambda: systems.small_water(),
     "config0": systems.config0,
+    "config1": systems.config1,
     "config3": systems.config3,
 }
 

@@ -33,6 +33,7 @@ def covid_tip4p():
 CASES = {
     "small": lambda: systems.small_water(),
     "config0": systems.config0,
+    "config1": systems.config1,
     "config3": systems.config3,
     "covid_tip4p": covid_tip4p,
 }
