@@ -231,3 +231,33 @@ def test_batch_beyond_one_pair_launch(cuda):
     for e, (f, d) in zip(batch.engines, single):
         assert np.array_equal(e.frc.cpu().numpy(), f)
         assert float(e.dudl.item()) == d
+
+
+def test_batch_forces_only(cuda):
+    """Without dU/dlambda outputs the batch runs the force-only kernels: the forces are the
+    bits of each window's own force-only step; a batch asking dU/dlambda of only some windows is
+    refused."""
+    import sponge_b200
+    from sponge_b200 import FepBatchStep
+    from sponge_b200.fep import FepEngine
+    engines = [FepEngine(s) for s in _batch_boxes()[:3] + _batch_boxes()[-1:]]
+    for e in engines:
+        e.update_list(forced=1)
+        e.to_uint()
+    single = []
+    for e in engines:
+        e.frc.zero_()
+        e.step(want_dudl=False)
+        cuda.cuda.synchronize()
+        single.append(e.frc.cpu().numpy().copy())
+    b = FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc, None)
+                      for e in engines])
+    for e in engines:
+        e.frc.zero_()
+    b.step()
+    cuda.cuda.synchronize()
+    for e, f in zip(engines, single):
+        assert np.array_equal(e.frc.cpu().numpy(), f)
+    with pytest.raises(sponge_b200.SpongeError):
+        FepBatchStep([(e.nl, e.sc, e.pme, e.uint_crd, e.charge, e.excl, e.frc,
+                       e.dudl if k == 0 else None) for k, e in enumerate(engines)])
