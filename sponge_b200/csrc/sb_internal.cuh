@@ -180,11 +180,14 @@ struct sb_neighbor_list {
     // pruned list (sb_nl_set_prune): the entries of cl_ent with an active slot within
     // cutoff + prune_buffer at the last prune, written by the packed pair kernel when meta[6] is
     // set (by a rebuild, by k_pack when an atom has moved more than prune_buffer / 2 since the
-    // last prune, or every prune_interval updates) and read by it in the other steps
+    // last prune, or every prune_interval updates) and read by it in the other steps. Its masks
+    // keep only the slots within that radius, and each cluster's entries are sorted by which
+    // slot pairs they use (the packed kernel skips a slot pair that no entry of a batch uses).
     float prune_buffer = 0.f;
     int prune_interval = 0, prune_count = 0;
     int* cl_count_in = nullptr;     // [clu_cap]
     uint32_t* cl_ent_in = nullptr;  // [clu_cap * ent_cap]
+    uint32_t* cl_ent_tmp = nullptr; // [clu_cap * ent_cap] a prune's entries before the sort
     uint4* xq_prune = nullptr;      // [slot_cap] packed coordinates at the last prune
     // ATOM_GROUP compatibility export
     void* ag = nullptr;             // ATOM_GROUP[N]

@@ -700,7 +700,7 @@ static void nl_free(sb_neighbor_list* nl) {
                   nl->sort_tmp, nl->slot_atom, nl->atom_slot, nl->slot_u, nl->excl_lo,
                   nl->excl_hi, nl->cl_count, nl->cl_ent, nl->meta, nl->xq, nl->stype, nl->fix,
                   nl->ag, nl->ag_serial, nl->zbin, nl->cl_count_in, nl->cl_ent_in,
-                  nl->xq_prune};
+                  nl->cl_ent_tmp, nl->xq_prune};
     for (void* p : ps) sb_free(p);
 }
 
@@ -894,6 +894,10 @@ extern "C" int sb_nl_set_prune(sb_neighbor_list* nl, float prune_buffer, int pru
         if (!nl->cl_ent_in)
             SB_TRY(sb_malloc((void**)&nl->cl_ent_in,
                              sizeof(uint32_t) * (size_t)nl->clu_cap * nl->ent_cap, "pruned list"));
+        if (!nl->cl_ent_tmp)
+            SB_TRY(sb_malloc((void**)&nl->cl_ent_tmp,
+                             sizeof(uint32_t) * (size_t)nl->clu_cap * nl->ent_cap,
+                             "prune scratch"));
         if (!nl->xq_prune) {
             SB_TRY(sb_malloc((void**)&nl->xq_prune, sizeof(uint4) * nl->slot_cap,
                              "prune coordinates"));

@@ -47,6 +47,7 @@ struct PairParams {
     int* prune;                // meta + 6: [0] prune requested, [1] set by a pruning launch
     int* cl_count_in;
     uint32_t* cl_ent_in;
+    uint32_t* cl_ent_tmp;
     uint4* xq_prune;
 };
 
@@ -66,6 +67,11 @@ __device__ __forceinline__ void add_fix(long long* p, float v) {
 #include "sb_pair_fixed.cuh"
 #include "sb_pair_compact.cuh"
 #include "sb_pair_x2.cuh"
+
+// dynamic shared memory of a packed-kernel block: the cluster's LJ table and the prune's counts
+static size_t x2_smem(int ntypes) {
+    return sizeof(float4) * 4 * (size_t)ntypes + sizeof(int) * SB_PAT_COUNTS;
+}
 
 // ---------------------------------------------------------------------------------------------
 // plain form: reference structure (warp per atom, float atomics), Lennard_Jones_force.cu:47-158
@@ -290,12 +296,13 @@ static PairParams pair_params_of(const sb_neighbor_list* nl, int ntypes, float c
     P.nt = ntypes;
     P.slot_cap = nl->slot_cap;
     P.ent_cap = nl->ent_cap;
-    const bool pruned = nl->prune_buffer > 0.f && nl->cl_ent_in;
+    const bool pruned = nl->prune_buffer > 0.f && nl->cl_ent_in && nl->cl_ent_tmp;
     const float rb = cutoff + nl->prune_buffer;
     P.rb2 = pruned ? rb * rb : 0.f;
     P.prune = nl->meta + 6;
     P.cl_count_in = nl->cl_count_in;
     P.cl_ent_in = nl->cl_ent_in;
+    P.cl_ent_tmp = nl->cl_ent_tmp;
     P.xq_prune = nl->xq_prune;
     return P;
 }
@@ -336,7 +343,7 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
     } while (0)
 #define SB_LAUNCH_X2(EVV)                                                                     \
     do {                                                                                      \
-        k_pair_x2<EVV><<<x2_blocks, 32, sizeof(float4) * 4 * lj->ntypes, s>>>(                \
+        k_pair_x2<EVV><<<x2_blocks, 32, x2_smem(lj->ntypes), s>>>(                            \
             P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
             nl->slot_atom, nl->fix, ae, av, ad);                                              \
     } while (0)
@@ -621,7 +628,7 @@ int sb_pair_fep(sb_neighbor_list* nl, const float2* d_AB, int ntypes, float cuto
         sb_set_error("sb_pair_fep: beta * cutoff beyond the packed kernel's Ewald fit");
         return SB_ERR_ARG;
     }
-    k_pair_x2<0><<<nl->clu_cap, 32, sizeof(float4) * 4 * ntypes, s>>>(
+    k_pair_x2<0><<<nl->clu_cap, 32, x2_smem(ntypes), s>>>(
         P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, d_AB, nl->slot_atom, nl->fix,
         nullptr, nullptr, nullptr);
     SB_CHECK_LAUNCH();
@@ -636,6 +643,7 @@ struct X2BoxVar {
     int* prune;
     int* cl_count_in;
     uint32_t* cl_ent_in;
+    uint32_t* cl_ent_tmp;
     uint4* xq_prune;
 };
 
@@ -689,6 +697,7 @@ __global__ void __launch_bounds__(32, 24) k_pair_x2_batch(const __grid_constant_
     P.prune = w.v.prune;
     P.cl_count_in = w.v.cl_count_in;
     P.cl_ent_in = w.v.cl_ent_in;
+    P.cl_ent_tmp = w.v.cl_ent_tmp;
     P.xq_prune = w.v.xq_prune;
     x2_cluster<0>(P, c, threadIdx.x & 31, ctab, w.cl_count, w.cl_ent, w.xq, w.stype, w.AB,
                   w.slot_atom, w.fix, nullptr, nullptr, nullptr);
@@ -723,7 +732,7 @@ int sb_pair_batch_create(int nb, const int* box_ids, sb_neighbor_list* const* nl
                          box_ids[i]);
             return SB_ERR_ARG;
         }
-        smem = std::max(smem, sizeof(float4) * 4 * (size_t)ntypes[i]);
+        smem = std::max(smem, x2_smem(ntypes[i]));
     }
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(k_pair_x2_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -753,7 +762,8 @@ int sb_pair_batch_create(int nb, const int* box_ids, sb_neighbor_list* const* nl
             L.box[L.nbox] = X2Box{nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype,
                                   tables[j], nl->slot_atom, nl->fix,
                                   X2BoxVar{q.sx, q.sy, q.sz, q.nt, q.slot_cap, q.ent_cap, q.rb2,
-                                           q.prune, q.cl_count_in, q.cl_ent_in, q.xq_prune}};
+                                           q.prune, q.cl_count_in, q.cl_ent_in, q.cl_ent_tmp,
+                                           q.xq_prune}};
             L.first[L.nbox + 1] = L.first[L.nbox] + nl->clu_cap;
             L.nbox++;
         }

@@ -43,17 +43,44 @@ __device__ __forceinline__ float2 ewald_nG2(float2 z, const float* gp) {
     return f2mul(p, make_float2(sb_rcp(q.x), sb_rcp(q.y)));
 }
 
-// Pruning pass over the full list of one cluster: keeps, in order, the entries with an active
-// slot (mask bit set) whose r^2 — computed exactly as pair_walk_x2 computes it — is below
-// (rc + prune buffer)^2, and writes them to `out`. Every entry the walk would find inside the
-// cut-off at these coordinates is kept. Returns the number kept.
+// Slot-pair patterns of a pruned entry: bit p is set when slot pair p (i atoms 2p and 2p + 1)
+// has an active slot within the prune radius. A prune sorts each cluster's entries by the rank
+// of their pattern, in the order below, so that entries needing the same slot pairs share the
+// walk's batches of 32 and a batch more often has slot pairs that none of its entries needs,
+// which the whole warp then skips. The order was found by a search over the patterns of the
+// 96,000-atom solvated box's clusters (rc 10 A, prune radius 10.5 A): sorted, its batches
+// evaluate 80.5 % of the slot pairs that unsorted batches do.
+//   rank:    0  1  2  3  4  5  6   7   8   9  10  11  12  13  14
+//   pattern: 1  3  2  6  7  5  9  13  15  11  10  14  12   4   8
+// Nibble k of SB_PAT_RANK is the rank of pattern k (pattern 0, never kept, has rank 15).
+#define SB_PAT_RANK 0x8b7c9a6e435d120full
+#define SB_PAT_COUNTS 16
+__device__ __forceinline__ int pat_rank(uint32_t mask8) {
+    const uint32_t a = (mask8 | (mask8 >> 1)) & 0x55u;
+    const uint32_t k = (a & 1u) | ((a >> 1) & 2u) | ((a >> 2) & 4u) | ((a >> 3) & 8u);
+    return (int)((SB_PAT_RANK >> (4 * k)) & 15ull);
+}
+
+// Pruning pass over the full list of one cluster: keeps the entries with an active slot (mask
+// bit set) whose r^2 — computed exactly as pair_walk_x2 computes it — is below
+// (rc + prune buffer)^2, with the mask reduced to those slots, and writes them to `out` sorted by
+// pattern rank (a counting sort: the kept entries go to `tmp` in list order while `rcnt`, 16 ints
+// of the block's shared memory, counts the ranks; then they are scattered to their rank's range
+// in list order, so the sorted list does not depend on the order of the counting atomics). Every slot the walk would find inside the cut-off before the next prune keeps its bit
+// (an atom that moves more than half the buffer requests a prune), and the forces are
+// fixed-point sums, so neither the dropped slots nor the order changes a bit. Returns the number
+// kept.
 template <bool EXACT>
 __device__ __forceinline__ int prune_walk_x2(
     const PairParams& P, const int cnt, const uint32_t* __restrict__ ents,
-    uint32_t* __restrict__ out, const uint4* __restrict__ xq, const int base, const int lane,
-    const uint32_t rx, const uint32_t ry, const uint32_t rz, const float2 (&nx)[4],
-    const float2 (&ny)[4], const float2 (&nz)[4]) {
+    uint32_t* __restrict__ out, uint32_t* __restrict__ tmp, int* rcnt,
+    const uint4* __restrict__ xq, const int base, const int lane, const uint32_t rx,
+    const uint32_t ry, const uint32_t rz, const float2 (&nx)[4], const float2 (&ny)[4],
+    const float2 (&nz)[4]) {
     const float2 rb2 = f2(P.rb2);
+    const unsigned lt = (1u << lane) - 1u;
+    if (lane < SB_PAT_COUNTS) rcnt[lane] = 0;
+    __syncwarp();
     int kept = 0;
     // four batches of 32 entries per step, with the next step's entries loaded while this step's
     // j coordinates arrive: the test itself is short, so more loads are kept in flight than in
@@ -77,11 +104,10 @@ __device__ __forceinline__ int prune_walk_x2(
         }
 #pragma unroll
         for (int g = 0; g < G; g++) {
-            const uint32_t m = v[g] >> 24;
             const float2 xj2 = f2(__int2float_rn((int)(xj[g].x - rx)) * P.sx);
             const float2 yj2 = f2(__int2float_rn((int)(xj[g].y - ry)) * P.sy);
             const float2 zj2 = f2(__int2float_rn((int)(xj[g].z - rz)) * P.sz);
-            bool keep = false;
+            uint32_t near = 0u;
 #pragma unroll
             for (int p = 0; p < 4; p++) {
                 float2 dx, dy, dz;
@@ -99,12 +125,52 @@ __device__ __forceinline__ int prune_walk_x2(
                     dz = f2add(zj2, nz[p]);
                 }
                 const float2 r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
-                keep |= ((m & (1u << (2 * p))) != 0u && r2.x < rb2.x) ||
-                        ((m & (2u << (2 * p))) != 0u && r2.y < rb2.y);
+                near |= (r2.x < rb2.x ? 1u << (2 * p) : 0u) | (r2.y < rb2.y ? 2u << (2 * p) : 0u);
             }
+            const uint32_t act = near & (v[g] >> 24);
+            const bool keep = act != 0u;
             const unsigned b = __ballot_sync(0xffffffffu, keep);
-            if (keep) out[kept + __popc(b & ((1u << lane) - 1u))] = v[g];
+            if (keep) {
+                tmp[kept + __popc(b & lt)] = (v[g] & 0xffffffu) | (act << 24);
+                atomicAdd(&rcnt[pat_rank(act)], 1);
+            }
             kept += __popc(b);
+        }
+    }
+    __syncwarp();
+    // each rank's first position, then the scatter (the entries of one rank keep their order);
+    // the kept entries are read eight batches at a time, so that their loads overlap
+    const int c = lane < SB_PAT_COUNTS ? rcnt[lane] : 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < SB_PAT_COUNTS; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __syncwarp();
+    if (lane < SB_PAT_COUNTS) rcnt[lane] = incl - c;
+    __syncwarp();
+    constexpr int S = 8;
+    for (int e0 = 0; e0 < kept; e0 += 32 * S) {
+        uint32_t vs[S];
+#pragma unroll
+        for (int g = 0; g < S; g++) {
+            const int e = e0 + 32 * g + lane;
+            vs[g] = e < kept ? __ldcg(tmp + e) : 0u;  // a kept entry is never 0 (mask != 0)
+        }
+#pragma unroll
+        for (int g = 0; g < S; g++) {
+            if (e0 + 32 * g >= kept) break;
+            const bool valid = vs[g] != 0u;
+            const int r = valid ? pat_rank(vs[g] >> 24) : SB_PAT_COUNTS;
+            const unsigned grp = __match_any_sync(0xffffffffu, r);
+            const int pos = valid ? rcnt[r] + __popc(grp & lt) : 0;
+            __syncwarp();
+            if (valid) {
+                out[pos] = vs[g];
+                if ((grp & lt) == 0u) rcnt[r] += __popc(grp);
+            }
+            __syncwarp();
         }
     }
     return kept;
@@ -137,14 +203,16 @@ __device__ __forceinline__ void pair_walk_x2(
         tj1 = stype[v1 & 0xffffffu];
         const int j = (int)(v & 0xffffffu);
         const uint32_t m = v >> 24;
+        // the slots that some entry of this batch uses
+        const uint32_t mu = __reduce_or_sync(0xffffffffu, m);
         const float2 xj2 = f2(__int2float_rn((int)(xj.x - rx)) * P.sx);
         const float2 yj2 = f2(__int2float_rn((int)(xj.y - ry)) * P.sy);
         const float2 zj2 = f2(__int2float_rn((int)(xj.z - rz)) * P.sz);
         const float2 qj2 = f2(__uint_as_float(xj.w));
         const float4* trow = ctab + tj * 4;
         float2 gx = f2(0.f), gy = f2(0.f), gz = f2(0.f);
-#pragma unroll
-        for (int p = 0; p < 4; p++) {
+        // slot pair p of this lane's entry (a skipped pair would add exactly zero)
+        auto slot_pair = [&](const int p) {
             float2 dx, dy, dz;
             if (EXACT) {
                 const uint4 xa = xq[base + 2 * p], xb = xq[base + 2 * p + 1];
@@ -197,6 +265,17 @@ __device__ __forceinline__ void pair_walk_x2(
                     }
                 }
             }
+        };
+        // a batch that uses every slot pair runs the four interleaved; otherwise the warp takes
+        // only the pairs some entry uses (the prune sorts the entries to make such batches)
+        const uint32_t need = (mu | (mu >> 1)) & 0x55u;
+        if (need == 0x55u) {
+#pragma unroll
+            for (int p = 0; p < 4; p++) slot_pair(p);
+        } else {
+#pragma unroll
+            for (int p = 0; p < 4; p++)
+                if (need & (1u << (2 * p))) slot_pair(p);
         }
         if (valid) {
             add_fix(&fix[j], -(gx.x + gx.y));
@@ -278,11 +357,13 @@ __device__ __forceinline__ void x2_cluster(
     if (req) {
         // pruned list: rebuilt from the full list on request, then walked as in the other
         // launches, so the forces do not depend on whether this launch pruned
+        uint32_t* tmp = P.cl_ent_tmp + (size_t)c * P.ent_cap;
+        int* rcnt = (int*)(ctab + 4 * nt);
         cnt = (cntf & SB_CL_EXACT)
-                  ? prune_walk_x2<true>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz, nx, ny,
-                                        nz)
-                  : prune_walk_x2<false>(P, cnt, ents, in_ents, xq, base, lane, rx, ry, rz, nx,
-                                         ny, nz);
+                  ? prune_walk_x2<true>(P, cnt, ents, in_ents, tmp, rcnt, xq, base, lane, rx, ry,
+                                        rz, nx, ny, nz)
+                  : prune_walk_x2<false>(P, cnt, ents, in_ents, tmp, rcnt, xq, base, lane, rx, ry,
+                                         rz, nx, ny, nz);
         if (lane == 0) {
             P.cl_count_in[c] = cnt | (cntf & ~SB_CL_COUNT_MASK);
             if (c == 0) P.prune[1] = 1;  // k_finalize retires the request
@@ -358,7 +439,7 @@ __device__ __forceinline__ void x2_cluster(
 // SM): 85 us against 88 us at 128 registers on the 96k-atom box, for a few spilled bytes outside
 // the pair loop. Every cluster's forces go to fixed-point accumulators and
 // its energies to its own atoms, so the assignment does not change a bit. Dynamic shared memory:
-// the cluster's LJ table, 4 nt float4.
+// the cluster's LJ table, 4 nt float4, then the prune's SB_PAT_COUNTS rank counts.
 template <int EV>
 __global__ void __launch_bounds__(32, EV ? 12 : 24) k_pair_x2(
     PairParams P, const int* __restrict__ meta, const int* __restrict__ cl_count,

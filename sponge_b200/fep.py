@@ -27,7 +27,7 @@ def _scaled(x, f):
 
 class FepEngine:
     def __init__(self, system, form=FORM_FIXED, refresh_interval=20, max_neighbor_numbers=1200,
-                 device="cuda", prune_buffer=0.5, prune_interval=5):
+                 device="cuda", prune_buffer=0.5, prune_interval=0):
         torch = _require_cuda()
         self.torch = torch
         self.system = s = system
@@ -54,7 +54,7 @@ class FepEngine:
         self.pme = ParticleMeshEwald(n, self.box, s["cutoff"], s["tolerance"], s["fft"],
                                      form=form)
         # the split form's packed pair kernel walks a pruned list (rc + 0.5 A, pruned again
-        # when an atom has moved 0.25 A or every 5 list updates)
+        # after a rebuild and when an atom has moved 0.25 A)
         if form == FORM_FIXED and prune_buffer > 0 and self.sc.split_form[0]:
             self.nl.set_prune(prune_buffer, prune_interval)
         self.scaler = (np.float32(1.0) / np.float32(4294967296.0)) * self.box
