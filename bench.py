@@ -210,8 +210,8 @@ def workload_config():
     return {"workload": "solvated96k_pme96: 31,000 rigid waters + 3,000 solute atoms (20 LJ "
                         "types), 98.6 A cube, rc 10 A, skin 2 A, PME 96^3, list rebuilt every "
                         "20 steps, dt 2 fs, NVE leap-frog + SETTLE on moving coordinates; pair "
-                        "kernel on the list pruned to rc + 0.5 A (renewed after each rebuild, on "
-                        "any 0.25 A move and every 5 steps)",
+                        "kernel on the list pruned to rc + 0.5 A (renewed after each rebuild and on "
+                        "any 0.25 A move)",
             "atoms": 96000, "l2": "flushed (256 MiB write) before every timed step",
             "parallelism": "replicas"}
 
@@ -601,7 +601,7 @@ def main():
 def run_md(args, rank, world, local):
     """The headline (and the water1m line): NVE MD steps of the chosen form on moving
     coordinates, each the list update by its policy (rebuild every 20 steps; the pruned pair list
-    renewed on 0.25 A moves and every 5 steps) followed by one captured CUDA graph of fixed
+    renewed on 0.25 A moves) followed by one captured CUDA graph of fixed
     point, force step and the fused leap-frog + SETTLE launch."""
     import torch
     import sponge_b200  # noqa: F401  (fails loudly without the library)

@@ -112,9 +112,12 @@ SB_API int sb_nl_export_pairs(sb_neighbor_list* nl, int64_t* h_keys, int64_t cap
  * cutoff + prune_buffer at the last prune, instead of the full cutoff + skin list. A prune runs
  * inside the pair launch after every rebuild, when an atom has moved more than prune_buffer / 2
  * since the last prune (tested while packing coordinates), and every prune_interval list updates
- * (0: never on a count). Every pair within the cut-off stays in the walked list, so the pair set
- * evaluated is unchanged; the i-atom sums run over fewer entries, so forces may differ from the
- * unpruned walk in FP32 rounding, and do not depend on whether a launch pruned. With the
+ * (0: never on a count, which the displacement test makes safe; a count only adds prunes). A
+ * prune keeps in each entry only the slots within that radius and sorts each cluster's entries
+ * by the slot pairs they use, so that the walk can skip slot pairs a whole batch does not use.
+ * Every pair within the cut-off stays in the walked list, so the pair set evaluated is
+ * unchanged; the i-atom sums run over other entries in another order, so forces may differ from
+ * the unpruned walk in FP32 rounding, and do not depend on whether a launch pruned. With the
  * displacement-check policy (refresh_interval 0) the skin left for motion before a rebuild
  * becomes skin - prune_buffer. Requires 0 <= prune_buffer <= skin; 0 turns pruning off. */
 SB_API int sb_nl_set_prune(sb_neighbor_list* nl, float prune_buffer, int prune_interval);
