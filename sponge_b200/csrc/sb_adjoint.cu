@@ -303,7 +303,7 @@ __global__ void k_adj_spread_q(int n, const uint32_t* __restrict__ uc, const flo
             int gz = b2 - kz;
             if (gz < 0) gz += K2;
             const long long f = __float2ll_rn(qw * wy[ky] * wz[kz] * SB_GRID_SCALE);
-            if (f) atomicAdd((unsigned long long*)&gfix[row + gz], (unsigned long long)f);
+            if (f) sb_red_add(&gfix[row + gz], f);
         }
     }
 }
@@ -351,7 +351,7 @@ __global__ void k_adj_spread_p(int n, const uint32_t* __restrict__ uc, const flo
             if (gz < 0) gz += K2;
             const float v = a * wz[kz] + b * dz[kz];
             const long long f = __float2ll_rn(v * SB_GRID_SCALE);
-            if (f) atomicAdd((unsigned long long*)&gfix[row + gz], (unsigned long long)f);
+            if (f) sb_red_add(&gfix[row + gz], f);
         }
     }
 }

@@ -295,6 +295,13 @@ int sb_pme_ti_terms_slot(sb_pme* p, sb_neighbor_list* nl, const float* slot_dq,
                          const uint32_t* uc, const float* q, const float* dq, const int* es,
                          const int* el, const int* en, long long* acc, cudaStream_t s);
 
+// 64-bit integer add to global memory with no value returned (PTX red): the fixed-point grid and
+// force sums, where a returned value would only make the thread wait for the atomic's round trip
+__device__ __forceinline__ void sb_red_add(long long* p, long long v) {
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)),
+                 "l"(v));
+}
+
 // slot s of a packed list (k_pack): coordinates, charge bits and type in slot order (zeros in an
 // empty slot); with xq_prune, an atom that moved more than sqrt(move2) since the last prune sets
 // the prune request

@@ -43,7 +43,7 @@ __device__ __forceinline__ float3 nb14_disp(const uint32_t* uc, int i, int j, fl
 }
 
 __device__ __forceinline__ void nb14_add(long long* p, float v) {
-    atomicAdd((unsigned long long*)p, (unsigned long long)__float2ll_rn(v * SB_FORCE_SCALE));
+    sb_red_add(p, __float2ll_rn(v * SB_FORCE_SCALE));
 }
 
 // Dihedral_14_LJ_CF_Force_With_Atom_Energy_And_Virial_Cuda (nb14.cu:92-170): force on the pair,

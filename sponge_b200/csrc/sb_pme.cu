@@ -80,7 +80,7 @@ __device__ __forceinline__ void spread_one(int gt, const uint32_t* __restrict__ 
             const float v = qw * wy[ky] * wzk;
             if (FIXED) {
                 const long long f = __float2ll_rn(v * SB_GRID_SCALE);
-                if (f) atomicAdd((unsigned long long*)&gfix[at], (unsigned long long)f);
+                if (f) sb_red_add(&gfix[at], f);
             } else {
                 atomicAdd(&gf[at], v);
             }
@@ -213,9 +213,9 @@ __global__ void k_excluded(int n, const uint32_t* __restrict__ uc, float sx, flo
         fz += tz;
         e -= qq * erff(beta * r) / r;
         if (FIXED) {
-            atomicAdd((unsigned long long*)&fix[3 * j], (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
-            atomicAdd((unsigned long long*)&fix[3 * j + 1], (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
-            atomicAdd((unsigned long long*)&fix[3 * j + 2], (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
+            sb_red_add(&fix[3 * j], __float2ll_rn(-tx * SB_FORCE_SCALE));
+            sb_red_add(&fix[3 * j + 1], __float2ll_rn(-ty * SB_FORCE_SCALE));
+            sb_red_add(&fix[3 * j + 2], __float2ll_rn(-tz * SB_FORCE_SCALE));
         } else {
             atomicAdd(&frc[3 * j], -tx);
             atomicAdd(&frc[3 * j + 1], -ty);
@@ -223,9 +223,9 @@ __global__ void k_excluded(int n, const uint32_t* __restrict__ uc, float sx, flo
         }
     }
     if (FIXED) {
-        atomicAdd((unsigned long long*)&fix[3 * i], (unsigned long long)__float2ll_rn(fx * SB_FORCE_SCALE));
-        atomicAdd((unsigned long long*)&fix[3 * i + 1], (unsigned long long)__float2ll_rn(fy * SB_FORCE_SCALE));
-        atomicAdd((unsigned long long*)&fix[3 * i + 2], (unsigned long long)__float2ll_rn(fz * SB_FORCE_SCALE));
+        sb_red_add(&fix[3 * i], __float2ll_rn(fx * SB_FORCE_SCALE));
+        sb_red_add(&fix[3 * i + 1], __float2ll_rn(fy * SB_FORCE_SCALE));
+        sb_red_add(&fix[3 * i + 2], __float2ll_rn(fz * SB_FORCE_SCALE));
     } else {
         atomicAdd(&frc[3 * i], fx);
         atomicAdd(&frc[3 * i + 1], fy);
@@ -861,21 +861,18 @@ __device__ __forceinline__ void gather_atom_one(int i, const uint32_t* __restric
                 const float r = sqrtf(r2);
                 e -= qq * erff(X.beta * r) / r;
             }
-            atomicAdd((unsigned long long*)&fix[sj],
-                      (unsigned long long)__float2ll_rn(-tx * SB_FORCE_SCALE));
-            atomicAdd((unsigned long long*)&fix[slot_cap + sj],
-                      (unsigned long long)__float2ll_rn(-ty * SB_FORCE_SCALE));
-            atomicAdd((unsigned long long*)&fix[2 * slot_cap + sj],
-                      (unsigned long long)__float2ll_rn(-tz * SB_FORCE_SCALE));
+            sb_red_add(&fix[sj], __float2ll_rn(-tx * SB_FORCE_SCALE));
+            sb_red_add(&fix[slot_cap + sj], __float2ll_rn(-ty * SB_FORCE_SCALE));
+            sb_red_add(&fix[2 * slot_cap + sj], __float2ll_rn(-tz * SB_FORCE_SCALE));
         }
         fx += __float2ll_rn(ex * SB_FORCE_SCALE);
         fy += __float2ll_rn(ey * SB_FORCE_SCALE);
         fz += __float2ll_rn(ez * SB_FORCE_SCALE);
         if (X.ene) atomicAdd(&X.ene[i], e);
     }
-    atomicAdd((unsigned long long*)&fix[sl], (unsigned long long)fx);
-    atomicAdd((unsigned long long*)&fix[slot_cap + sl], (unsigned long long)fy);
-    atomicAdd((unsigned long long*)&fix[2 * slot_cap + sl], (unsigned long long)fz);
+    sb_red_add(&fix[sl], fx);
+    sb_red_add(&fix[slot_cap + sl], fy);
+    sb_red_add(&fix[2 * slot_cap + sl], fz);
 }
 
 // thread per atom (grid-stride; a grid of fewer blocks, as for the spread, was slower here: the

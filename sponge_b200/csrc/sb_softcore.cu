@@ -149,7 +149,7 @@ __device__ __forceinline__ bool sc_is_soft(int mi, int mj, float2 a, float2 b) {
 
 __device__ __forceinline__ void red_fix_sc(long long* p, float v, float scale) {
     const long long q = __float2ll_rn(v * scale);
-    if (q) atomicAdd((unsigned long long*)p, (unsigned long long)q);
+    if (q) sb_red_add(p, q);
 }
 
 // per-slot B type, mask and charge change
