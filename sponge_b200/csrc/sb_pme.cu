@@ -1313,7 +1313,7 @@ __global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
 // reciprocal gather with the exclusion correction, and (dH) the exclusion cross term of
 // dU/dlambda summed per warp as k_ti_corr does
 template <bool DH>
-__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
+__global__ void __launch_bounds__(SB_FEP_BATCH_THREADS, 4)
     k_gather_batch(const SbFepBox* __restrict__ B, const int2* __restrict__ tab) {
     const int2 t = tab[blockIdx.x];
     const SbFepBox& b = B[t.x];
