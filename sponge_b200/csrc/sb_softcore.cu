@@ -1418,7 +1418,8 @@ struct sb_fep_batch {
     cudaStream_t rec = nullptr;
     cudaStream_t pert = nullptr;  // the soft-core passes, beside the packed pair kernel
     std::vector<cudaStream_t> fft;
-    cudaEvent_t ev_packed = nullptr, ev_spread = nullptr, ev_rec = nullptr, ev_pert = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_packed = nullptr, ev_spread = nullptr, ev_rec = nullptr,
+                ev_pert = nullptr;
     std::vector<cudaEvent_t> ev_fft;
 };
 
@@ -1431,7 +1432,7 @@ static void fep_batch_free(sb_fep_batch* b) {
     for (cudaStream_t f : b->fft) cudaStreamDestroy(f);
     if (b->rec) cudaStreamDestroy(b->rec);
     if (b->pert) cudaStreamDestroy(b->pert);
-    for (cudaEvent_t e : {b->ev_packed, b->ev_spread, b->ev_rec, b->ev_pert})
+    for (cudaEvent_t e : {b->ev_start, b->ev_packed, b->ev_spread, b->ev_rec, b->ev_pert})
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : b->ev_fft) cudaEventDestroy(e);
     for (auto& g : b->groups) sb_free(g.d_io);
@@ -1624,6 +1625,7 @@ extern "C" int sb_fep_batch_create(int n_boxes, sb_neighbor_list* const* nls,
                   cudaStreamCreateWithPriority(&b->rec, cudaStreamNonBlocking, hi) == cudaSuccess &&
                   cudaStreamCreateWithPriority(&b->pert, cudaStreamNonBlocking, hi) == cudaSuccess &&
                   cudaEventCreateWithFlags(&b->ev_pert, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) == cudaSuccess &&
                   cudaEventCreateWithFlags(&b->ev_packed, cudaEventDisableTiming) == cudaSuccess &&
                   cudaEventCreateWithFlags(&b->ev_spread, cudaEventDisableTiming) == cudaSuccess &&
                   cudaEventCreateWithFlags(&b->ev_rec, cudaEventDisableTiming) == cudaSuccess;
@@ -1707,13 +1709,17 @@ extern "C" int sb_fep_batch_step(sb_fep_batch* b, void* stream) {
     SB_TRY(fep_batch_current(b));
     cudaStream_t s = sb_stream(stream);
     const int2* tab = b->d_tab;
+    // reciprocal chain beside the pack and the pair launches: the spread reads the atom-order
+    // coordinates and charges (and the grid the last forward FFT left zero), so it starts with
+    // the pack; the gather, which adds to the dU/dlambda sums the pack zeroes, waits for it. Both
+    // chains add to the fixed-point force planes (order-free integer sums); the finalize waits
+    // for both.
+    SB_CHECK_CUDA(cudaEventRecord(b->ev_start, s));
+    SB_CHECK_CUDA(cudaStreamWaitEvent(b->rec, b->ev_start, 0));
     k_fep_pack_batch<<<b->n_slot, SB_FEP_BATCH_THREADS, 0, s>>>(b->d_box, tab + b->off_slot,
                                                                b->dh);
     SB_CHECK_LAUNCH();
-    // reciprocal chain beside the pair launches: both add to the fixed-point force planes
-    // (order-free integer sums); the finalize waits for both
     SB_CHECK_CUDA(cudaEventRecord(b->ev_packed, s));
-    SB_CHECK_CUDA(cudaStreamWaitEvent(b->rec, b->ev_packed, 0));
     SB_TRY(sb_pme_batch_spread(b->d_box, tab + b->off_spread, b->n_spread, b->rec));
     SB_CHECK_CUDA(cudaEventRecord(b->ev_spread, b->rec));
     const int nf = (int)b->fft.size();
@@ -1740,6 +1746,7 @@ extern "C" int sb_fep_batch_step(sb_fep_batch* b, void* stream) {
         SB_CHECK_CUDA(cudaEventRecord(b->ev_fft[k], b->fft[k]));
         SB_CHECK_CUDA(cudaStreamWaitEvent(b->rec, b->ev_fft[k], 0));
     }
+    SB_CHECK_CUDA(cudaStreamWaitEvent(b->rec, b->ev_packed, 0));
     SB_TRY(sb_pme_batch_gather(b->d_box, tab + b->off_atom, b->n_atom, b->dh, b->rec));
     SB_CHECK_CUDA(cudaEventRecord(b->ev_rec, b->rec));
     SB_CHECK_CUDA(cudaStreamWaitEvent(b->pert, b->ev_packed, 0));
