@@ -303,17 +303,17 @@ __device__ __forceinline__ void sb_red_add(long long* p, long long v) {
 }
 
 // slot s of a packed list (k_pack): coordinates, charge bits and type in slot order (zeros in an
-// empty slot); with xq_prune, an atom that moved more than sqrt(move2) since the last prune sets
-// the prune request
-__device__ __forceinline__ void sb_pack_slot(int s, const int* __restrict__ slot_atom,
+// empty slot); with a pruned list (pruned), an atom that moved more than sqrt(move2) since the
+// last prune (its packed coordinates then: o) sets the prune request. The slot's atom a and o
+// are loaded by the caller, beside the slot count (the packing kernels run a thread per slot of
+// the allocation, so these loads need not wait for the count).
+__device__ __forceinline__ void sb_pack_slot(int s, int a, uint4 o,
                                              const uint32_t* __restrict__ uc,
                                              const float* __restrict__ q,
                                              const int* __restrict__ type,
                                              uint4* __restrict__ xq, int* __restrict__ stype,
-                                             const uint4* __restrict__ xq_prune, float sx,
-                                             float sy, float sz, float move2,
-                                             int* __restrict__ prune_req) {
-    const int a = slot_atom[s];
+                                             bool pruned, float sx, float sy, float sz,
+                                             float move2, int* __restrict__ prune_req) {
     uint4 v = make_uint4(0u, 0u, 0u, 0u);
     int t = 0;
     if (a >= 0) {
@@ -322,8 +322,7 @@ __device__ __forceinline__ void sb_pack_slot(int s, const int* __restrict__ slot
         v.z = uc[3 * a + 2];
         v.w = q ? __float_as_uint(q[a]) : 0u;
         t = type ? type[a] : 0;
-        if (xq_prune) {
-            const uint4 o = xq_prune[s];
+        if (pruned) {
             const float dx = __int2float_rn((int)(v.x - o.x)) * sx;
             const float dy = __int2float_rn((int)(v.y - o.y)) * sy;
             const float dz = __int2float_rn((int)(v.z - o.z)) * sz;
@@ -335,12 +334,11 @@ __device__ __forceinline__ void sb_pack_slot(int s, const int* __restrict__ slot
 }
 
 // slot s of the fixed-point force planes (k_finalize) added to the atom's float force, the
-// accumulator cleared for the next step
-__device__ __forceinline__ void sb_finalize_slot(int s, const int* __restrict__ slot_atom,
-                                                 long long* __restrict__ fix, int slot_cap,
-                                                 float* __restrict__ frc) {
-    const int a = slot_atom[s];
-    const long long fx = fix[s], fy = fix[slot_cap + s], fz = fix[2 * slot_cap + s];
+// accumulator cleared for the next step; the slot's atom a and its sums fx, fy, fz are loaded by
+// the caller, beside the slot count
+__device__ __forceinline__ void sb_finalize_slot(int s, int a, long long fx, long long fy,
+                                                 long long fz, long long* __restrict__ fix,
+                                                 int slot_cap, float* __restrict__ frc) {
     if (fx | fy | fz) {
         fix[s] = 0;
         fix[slot_cap + s] = 0;

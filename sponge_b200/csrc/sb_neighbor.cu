@@ -612,10 +612,14 @@ __global__ void k_pack(const int* __restrict__ meta, const int* __restrict__ slo
                        const uint32_t* __restrict__ uc, const float* __restrict__ q,
                        const int* __restrict__ type, uint4* __restrict__ xq,
                        int* __restrict__ stype, const uint4* __restrict__ xq_prune, float sx,
-                       float sy, float sz, float move2, int* __restrict__ prune_req) {
+                       float sy, float sz, float move2, int* __restrict__ prune_req,
+                       int slot_cap) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slot_cap) return;
+    const int a = slot_atom[s];
+    const uint4 o = xq_prune ? xq_prune[s] : make_uint4(0u, 0u, 0u, 0u);
     if (s < meta[3])
-        sb_pack_slot(s, slot_atom, uc, q, type, xq, stype, xq_prune, sx, sy, sz, move2,
+        sb_pack_slot(s, a, o, uc, q, type, xq, stype, xq_prune != nullptr, sx, sy, sz, move2,
                      prune_req);
 }
 
@@ -625,7 +629,10 @@ __global__ void k_finalize(int* __restrict__ meta, const int* __restrict__ slot_
                            long long* __restrict__ fix, int slot_cap, float* __restrict__ frc) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s == 0) sb_retire_prune(meta);
-    if (s < meta[3]) sb_finalize_slot(s, slot_atom, fix, slot_cap, frc);
+    if (s >= slot_cap) return;
+    const int a = slot_atom[s];
+    const long long fx = fix[s], fy = fix[slot_cap + s], fz = fix[2 * slot_cap + s];
+    if (s < meta[3]) sb_finalize_slot(s, a, fx, fy, fz, fix, slot_cap, frc);
 }
 
 __global__ void k_crd_to_uint(int n, const float* __restrict__ crd, float cx, float cy, float cz,
@@ -953,7 +960,7 @@ int sb_nl_pack(sb_neighbor_list* nl, const uint32_t* d_uint_crd, const float* d_
         nl->meta, nl->slot_atom, d_uint_crd, d_charge, d_type, nl->xq, nl->stype,
         pr ? nl->xq_prune : nullptr, (1.0f / 4294967296.0f) * nl->box[0],
         (1.0f / 4294967296.0f) * nl->box[1], (1.0f / 4294967296.0f) * nl->box[2], half * half,
-        nl->meta + 6);
+        nl->meta + 6, nl->slot_cap);
     SB_CHECK_LAUNCH();
     return SB_OK;
 }

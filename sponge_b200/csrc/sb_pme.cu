@@ -1336,14 +1336,27 @@ __global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
     const int2 t = tab[blockIdx.x];
     const SbFepBox& b = B[t.x];
     const int s = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
+    // the slot's data are loaded beside the slot count (the blocks cover the allocation)
+    const bool in = s < b.slot_cap;
+    const int a = in ? b.slot_atom[s] : -1;
+    long long fx = 0, fy = 0, fz = 0;
+    if (in) {
+        fx = b.fix[s];
+        fy = b.fix[b.slot_cap + s];
+        fz = b.fix[2 * b.slot_cap + s];
+    }
+    const float d = DH && in ? b.slot_dq[s] : 0.f;
     const int lim = b.meta[3];
     if (s == 0) sb_retire_prune(b.meta);
     if (DH) {
-        const float v = s < lim ? ti_rec_slot(s, b.xq, b.slot_dq, b.theta, b.K0, b.K1, b.K2)
-                                : 0.f;
+        float v = 0.f;
+        if (s < lim && d != 0.f) {
+            const uint4 u = b.xq[s];
+            v = d * phi_at(u.x, u.y, u.z, b.theta, b.K0, b.K1, b.K2);
+        }
         ti_red(b.hfix + 2, v);
     }
-    if (s < lim) sb_finalize_slot(s, b.slot_atom, b.fix, b.slot_cap, b.frc);
+    if (s < lim) sb_finalize_slot(s, a, fx, fy, fz, b.fix, b.slot_cap, b.frc);
 }
 
 int sb_pme_batch_spread(const SbFepBox* d_boxes, const int2* d_tab, int nblocks, cudaStream_t s) {

@@ -941,8 +941,9 @@ extern "C" int sb_sc_dh_dlambda(sb_softcore* sc, sb_neighbor_list* nl, const uin
 // packed as an uncharged ghost type) plus the soft-core pass over the perturbed atoms; without
 // it, the soft-core cluster kernel over all pairs.
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void fep_pack_one(int s, const SbFepBox& b) {
-    const int a = b.slot_atom[s];
+// slot s (< slot_cap) of a box; its atom a and prune snapshot o are loaded by the caller, beside
+// the slot count
+__device__ __forceinline__ void fep_pack_one(int s, int a, uint4 o, const SbFepBox& b) {
     uint4 v = make_uint4(0u, 0u, 0u, 0u);
     int t = 0;
     if (a >= 0) {
@@ -952,7 +953,6 @@ __device__ __forceinline__ void fep_pack_one(int s, const SbFepBox& b) {
         t = b.split ? b.tu[a] : b.typeA[a];
         v.w = (b.split && t == b.ghost) ? 0u : __float_as_uint(b.q[a]);
         if (b.xq_prune) {
-            const uint4 o = b.xq_prune[s];
             const float dx = __int2float_rn((int)(v.x - o.x)) * b.usx;
             const float dy = __int2float_rn((int)(v.y - o.y)) * b.usy;
             const float dz = __int2float_rn((int)(v.z - o.z)) * b.usz;
@@ -961,14 +961,22 @@ __device__ __forceinline__ void fep_pack_one(int s, const SbFepBox& b) {
     }
     b.xq[s] = v;
     b.stype[s] = t;
-    sc_pack_slot(s, b.slot_atom, b.typeB, b.mask, b.dq, b.slot_ext, b.slot_dq);
+    b.slot_ext[s] = a >= 0 ? (b.typeB[a] | (b.mask[a] << 16)) : 0;
+    b.slot_dq[s] = a >= 0 ? b.dq[a] : 0.f;
+}
+
+__device__ __forceinline__ void fep_pack_slot(int s, const SbFepBox& b) {
+    if (s >= b.slot_cap) return;
+    const int a = b.slot_atom[s];
+    const uint4 o = b.xq_prune ? b.xq_prune[s] : make_uint4(0u, 0u, 0u, 0u);
+    if (s < b.meta[3]) fep_pack_one(s, a, o, b);
 }
 
 __global__ void __launch_bounds__(SB_FEP_BATCH_THREADS) k_fep_pack(SbFepBox b, int dh) {
     const int s = blockIdx.x * SB_FEP_BATCH_THREADS + threadIdx.x;
     if (dh && blockIdx.x == 0 && threadIdx.x < 4) b.hfix[threadIdx.x] = 0;
     if (b.split && blockIdx.x == 0 && threadIdx.x == 4) b.pcount[0] = 0;
-    if (s < b.meta[3]) fep_pack_one(s, b);
+    fep_pack_slot(s, b);
 }
 
 // pair {a < b} is excluded iff b is in a's exclusion list (the list's rule)
@@ -1289,7 +1297,7 @@ __global__ void __launch_bounds__(SB_FEP_BATCH_THREADS)
     const int s = t.y * SB_FEP_BATCH_THREADS + threadIdx.x;
     if (dh && t.y == 0 && threadIdx.x < 4) b.hfix[threadIdx.x] = 0;
     if (b.split && t.y == 0 && threadIdx.x == 4) b.pcount[0] = 0;
-    if (s < b.meta[3]) fep_pack_one(s, b);
+    fep_pack_slot(s, b);
 }
 
 // the ScParams fields that differ between the boxes of one launch
