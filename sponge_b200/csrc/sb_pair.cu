@@ -343,6 +343,9 @@ static int launch_pair_fixed(sb_lennard_jones* lj, sb_neighbor_list* nl, float b
     } while (0)
 #define SB_LAUNCH_X2(EVV)                                                                     \
     do {                                                                                      \
+        if (x2_smem(lj->ntypes) > 48 * 1024)                                                  \
+            cudaFuncSetAttribute(k_pair_x2<EVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)x2_smem(lj->ntypes));                                   \
         k_pair_x2<EVV><<<x2_blocks, 32, x2_smem(lj->ntypes), s>>>(                            \
             P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, lj->d_AB,               \
             nl->slot_atom, nl->fix, ae, av, ad);                                              \
@@ -628,6 +631,9 @@ int sb_pair_fep(sb_neighbor_list* nl, const float2* d_AB, int ntypes, float cuto
         sb_set_error("sb_pair_fep: beta * cutoff beyond the packed kernel's Ewald fit");
         return SB_ERR_ARG;
     }
+    if (x2_smem(ntypes) > 48 * 1024)
+        cudaFuncSetAttribute(k_pair_x2<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)x2_smem(ntypes));
     k_pair_x2<0><<<nl->clu_cap, 32, x2_smem(ntypes), s>>>(
         P, nl->meta, nl->cl_count, nl->cl_ent, nl->xq, nl->stype, d_AB, nl->slot_atom, nl->fix,
         nullptr, nullptr, nullptr);
