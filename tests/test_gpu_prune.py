@@ -1,7 +1,9 @@
 """The pruned pair list (sb_nl_set_prune) on the GPU.
 
 The packed pair kernel walks only the entries with a pair within cutoff + buffer at the last
-prune. Checked on the 3,000-atom water box (rc 8 A, skin 2 A, buffer 0.5 A):
+prune, each with its mask reduced to the slots within that radius and the entries of a cluster
+sorted by the slot pairs they use (a batch skips the slot pairs none of its entries uses).
+Checked on the 3,000-atom water box (rc 8 A, skin 2 A, buffer 0.5 A):
 
 * at the coordinates of the build, the pruned walk evaluates the same pairs as the full walk:
   forces agree per atom to FP32 rounding of the i-atom sums (a single missing pair near the
