@@ -209,9 +209,9 @@ METRIC = "ns/day, 96k-atom PME water, 1 B200 (nonbonded path, fixed-point form)"
 def workload_config():
     return {"workload": "solvated96k_pme96: 31,000 rigid waters + 3,000 solute atoms (20 LJ "
                         "types), 98.6 A cube, rc 10 A, skin 2 A, PME 96^3, list rebuilt every "
-                        "20 steps, dt 2 fs, NVE leap-frog + SETTLE on moving coordinates; pair "
-                        "kernel on the list pruned to rc + 0.5 A (renewed after each rebuild and on "
-                        "any 0.25 A move)",
+                        "20 steps, dt 2 fs, NVE leap-frog + SETTLE at 300 K on moving coordinates; pair "
+                        "kernel on the list pruned to rc + 1 A (renewed after each rebuild and on "
+                        "any 0.5 A move)",
             "atoms": 96000, "l2": "flushed (256 MiB write) before every timed step",
             "parallelism": "replicas"}
 
@@ -222,8 +222,8 @@ WATER1M_METRIC = "ns/day, 1,000,512-atom PME water (216^3), 1 B200: chosen vs pl
 def water1m_config():
     return {"workload": "water1m_pme216: 333,504 rigid waters (70^3 lattice minus 9,496 sites), "
                         "215.3 A cube, rc 10 A, skin 2 A, PME 216^3, list rebuilt every 20 "
-                        "steps, dt 2 fs, NVE leap-frog + SETTLE; pair kernel on the list pruned "
-                        "to rc + 0.5 A",
+                        "steps, dt 2 fs, NVE leap-frog + SETTLE at 300 K; pair kernel on the list "
+                        "pruned to rc + 1 A",
             "atoms": 1000512, "l2": "flushed (256 MiB write) before every timed step",
             "parallelism": "replicas"}
 
@@ -502,7 +502,9 @@ def setup_md(eng, s, seed, relax_iters=300, temperature=300.0, equil_steps=300):
     # carry the excess energy of close contacts; `equil_steps` NVE steps with the velocities
     # rescaled to `temperature` every 10 steps (a Berendsen thermostat with tau = dt) bring the
     # system to the motion of an equilibrated run before anything is timed
-    ke_target = 0.5 * (3 * n - 3 * len(pi)) * 0.0019872041 * temperature  # rigid constraints
+    # degrees of freedom: 3 per atom, less one per distance constraint and the three of the
+    # removed centre-of-mass momentum
+    ke_target = 0.5 * (3 * n - len(pi) - 3) * 0.0019872041 * temperature
     for k in range(equil_steps):
         eng.update_list()
         eng.md_step(settle, inv_t, mass_t, vel_t, acc_t)
@@ -601,7 +603,7 @@ def main():
 def run_md(args, rank, world, local):
     """The headline (and the water1m line): NVE MD steps of the chosen form on moving
     coordinates, each the list update by its policy (rebuild every 20 steps; the pruned pair list
-    renewed on 0.25 A moves) followed by one captured CUDA graph of fixed
+    renewed on 0.5 A moves) followed by one captured CUDA graph of fixed
     point, force step and the fused leap-frog + SETTLE launch."""
     import torch
     import sponge_b200  # noqa: F401  (fails loudly without the library)

@@ -22,14 +22,15 @@ def scaled_lj_tables(system):
 
 class NonbondedEngine:
     """``prune_buffer`` / ``prune_interval``: the pruned pair list of the fixed form
-    (NeighborList.set_prune): the pair kernel walks the entries within cutoff + 0.5 A of the last
-    prune, renewed after each rebuild and when an atom has moved 0.25 A (which keeps every pair
-    inside the cut-off in it), plus every ``prune_interval`` list updates when that is > 0 (on
-    the 96,000-atom box's MD steps a prune interval of 3, 5 or 10 updates cost 3-4 us per step
-    more than none). A buffer of 0 turns the pruned list off."""
+    (NeighborList.set_prune): the pair kernel walks the entries within cutoff + prune_buffer of
+    the last prune, renewed after each rebuild and when an atom has moved half the buffer (which
+    keeps every pair inside the cut-off in it), plus every ``prune_interval`` list updates when
+    that is > 0 (a count only adds prunes). The default 1 A buffer is the fastest of 0.5-1.5 A
+    for MD of the 96,000-atom water box at 300 K (a prune about every fourth step). A buffer of 0
+    turns the pruned list off."""
 
     def __init__(self, system, form=FORM_FIXED, refresh_interval=20, max_neighbor_numbers=1200,
-                 device="cuda", prune_buffer=0.5, prune_interval=0):
+                 device="cuda", prune_buffer=1.0, prune_interval=0):
         torch = _require_cuda()
         self.torch = torch
         self.system = system
