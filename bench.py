@@ -461,6 +461,12 @@ def run_modules(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def md_degrees_of_freedom(n_atoms, n_constraints):
+    """3 per atom, less one per distance constraint (a rigid water holds three) and the three of
+    the removed centre-of-mass momentum."""
+    return 3 * int(n_atoms) - int(n_constraints) - 3
+
+
 def setup_md(eng, s, seed, relax_iters=300, temperature=300.0, equil_steps=300):
     """Untimed MD set-up on the device. The seeded generators place the free (unconstrained)
     solute atoms by random sequential addition at >= 2.2 A, which leaves LJ overlaps of several
@@ -502,9 +508,7 @@ def setup_md(eng, s, seed, relax_iters=300, temperature=300.0, equil_steps=300):
     # carry the excess energy of close contacts; `equil_steps` NVE steps with the velocities
     # rescaled to `temperature` every 10 steps (a Berendsen thermostat with tau = dt) bring the
     # system to the motion of an equilibrated run before anything is timed
-    # degrees of freedom: 3 per atom, less one per distance constraint and the three of the
-    # removed centre-of-mass momentum
-    ke_target = 0.5 * (3 * n - len(pi) - 3) * 0.0019872041 * temperature
+    ke_target = 0.5 * md_degrees_of_freedom(n, len(pi)) * 0.0019872041 * temperature
     for k in range(equil_steps):
         eng.update_list()
         eng.md_step(settle, inv_t, mass_t, vel_t, acc_t)
